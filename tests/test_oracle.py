@@ -1,0 +1,93 @@
+"""The oracle is pinned before it is trusted: against the golden fixtures (an independent
+Fock-space evaluation), the reference's structure counts and Rumer property, and cofactor
+identities checked against explicit deleted minors (as the reference's
+tests/vbscf/unit/test_cofactor_differential.cpp does)."""
+
+import itertools
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden_cases, load_golden
+
+# the reference's structure-test tolerances (test_structure_tiles.cpp:310-319)
+H_TOL = 2e-10
+S_TOL = 2e-11
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_oracle_matches_golden(name):
+    z = load_golden(name)
+    n, nel, mult, kw = int(z["n"]), int(z["n_el"]), int(z["mult"]), str(z["keyword"])
+    structures = O.generate_structures(kw, n, nel, mult)
+    assert np.array_equal(np.array(structures), z["structures"])
+    exp = O.expand(structures, nel, mult)
+    Hs, Ss, _ = O.structure_matrices(n, exp, z["S"], z["h"], z["eri"])
+    scale_h = max(1.0, np.linalg.norm(z["Hs"]))
+    scale_s = max(1.0, np.linalg.norm(z["Ss"]))
+    assert np.linalg.norm(Hs - z["Hs"]) <= H_TOL * scale_h
+    assert np.linalg.norm(Ss - z["Ss"]) <= S_TOL * scale_s
+    Hd, Sd = O.determinant_matrices(n, exp.det_alpha_occ, exp.det_beta_occ, z["S"], z["h"], z["eri"])
+    assert np.abs(Hd - z["Hd"]).max() <= H_TOL * max(1.0, np.abs(z["Hd"]).max())
+    assert np.abs(Sd - z["Sd"]).max() <= S_TOL * max(1.0, np.abs(z["Sd"]).max())
+
+
+@pytest.mark.parametrize("n", [4, 6, 8, 10, 12, 14])
+def test_covalent_counts_and_rumer(n):
+    structures = O.generate_structures("COV", n, n)
+    expected = math.comb(n, n // 2) - math.comb(n, n // 2 - 1)
+    assert len(structures) == expected
+    rumer = {tuple(sorted(tuple(sorted(b)) for b in p)) for p in O.rumer_pairings(0, n)}
+    got = {tuple(sorted(tuple(sorted((row[2 * i] - 1, row[2 * i + 1] - 1))) for i in range(n // 2)))
+           for row in structures}
+    assert got == rumer
+    exp = O.expand(structures, n)
+    assert exp.n_determinants == math.comb(n, n // 2)
+    assert len(exp.term_structure) == expected * 2 ** (n // 2)
+
+
+@pytest.mark.parametrize("n", [4, 6, 8, 10, 12])
+def test_singly_ionic_counts(n):
+    m = n - 2
+    ionic = n * (n - 1) * (math.comb(m, m // 2) - math.comb(m, m // 2 - 1))
+    assert len(O.generate_structures("ION(1)", n, n)) == ionic
+
+
+def _adjugate(x):
+    k = x.shape[0]
+    return np.array([[(-1) ** (i + j) * np.linalg.det(np.delete(np.delete(x, i, 0), j, 1)) for j in range(k)]
+                     for i in range(k)])
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 7])
+@pytest.mark.parametrize("rank_drop", [0, 1, 2, 3])
+def test_first_and_second_cofactors_against_minors(k, rank_drop):
+    if rank_drop > k:
+        pytest.skip("rank drop larger than the block")
+    rng = np.random.default_rng(100 * k + rank_drop)
+    x = rng.standard_normal((k, k))
+    if rank_drop:
+        u, s, vt = np.linalg.svd(x)
+        s[k - rank_drop:] = 0.0
+        x = (u * s) @ vt
+    det, nullity, _, cof = O.resolve(x)
+    assert nullity == rank_drop or (k <= 1 and rank_drop == 1)
+    scale = max(1.0, np.abs(x).max()) ** max(0, k - 1)
+    if k > 1 and nullity <= 1:
+        assert np.abs(cof - _adjugate(x)).max() <= 1e-12 * scale
+    if k >= 2 and nullity <= 2:
+        for r1, r2 in itertools.combinations(range(k), 2):
+            for c1, c2 in itertools.combinations(range(k), 2):
+                minor = np.delete(np.delete(x, [r1, r2], 0), [c1, c2], 1)
+                ref = (-1) ** (r1 + r2 + c1 + c2) * (np.linalg.det(minor) if minor.size else 1.0)
+                assert abs(O.second_cofactor(x, r1, r2, c1, c2) - ref) <= 1e-12 * scale
+
+
+def test_full_pivot_lu_rank_threshold():
+    x = np.diag([1.0, 1e-6, 1e-13])
+    rank, det, inv = O.full_pivot_lu(x)
+    assert rank == 2 and inv is None
+    rank, det, inv = O.full_pivot_lu(np.diag([1.0, 1e-6, 1e-11]))
+    assert rank == 3 and abs(det - 1e-17) < 1e-30
