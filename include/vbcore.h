@@ -1,0 +1,181 @@
+/*
+ * vbcore: B200-native (sm_100a) VBSCF evaluation core behind a C ABI.
+ *
+ * Drop-in boundary for the determinant-pair / structure-matrix hot path of
+ * Tao-Xia/xmvb-cpp (paths below are relative to that project).  Every entry
+ * point names the reference interface it replaces.  Conventions:
+ *
+ *   - all matrices are column-major (m[col * rows + row]), as the reference's
+ *     src/vbscf/determinants/contracts/types.hpp:13-15;
+ *   - determinant overlap blocks have rows = right determinant, columns = left
+ *     determinant (types.hpp:62-66); cofactor matrices use the same orientation;
+ *   - packed pair index pair(a,b) = hi(hi+1)/2 + lo and packed two-electron
+ *     storage (pq|rs) at pair(pair(p,q), pair(r,s)) (src/core/pair_index.cpp:10-44);
+ *   - status codes instead of exceptions; vb_last_error() gives the message;
+ *   - caller-owned buffers; VB_MEM_HOST pointers are copied through the
+ *     context's stream, VB_MEM_DEVICE pointers are used in place.
+ *
+ * There is no CPU fallback: every numerical entry point runs CUDA kernels and
+ * fails with VB_ERR_CUDA when no usable sm_100 device is present.
+ */
+#ifndef VBCORE_H
+#define VBCORE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int vb_status;
+enum {
+    VB_OK = 0,
+    VB_ERR_INVALID = 1,     /* bad argument or shape (reference: std::invalid_argument) */
+    VB_ERR_CUDA = 2,        /* CUDA runtime failure (reference: check_cuda, context.hpp:20-37) */
+    VB_ERR_BUDGET = 3,      /* HBM budget exceeded (reference: context.hpp:213-218) */
+    VB_ERR_NUMERIC = 4,     /* non-SPD metric, failed eigensolve (reference: cholesky check_info) */
+    VB_ERR_UNSUPPORTED = 5, /* size outside what the kernels implement */
+    VB_ERR_TIMEOUT = 6      /* a bounded device wait gave up */
+};
+
+enum { VB_MEM_HOST = 0, VB_MEM_DEVICE = 1 };
+
+typedef struct vb_context vb_context;
+typedef struct vb_hs_plan vb_hs_plan;
+
+/* ---- context (replaces xmvb::cuda::Context, src/cuda/memory/context.hpp:66-405) ---------- */
+
+/* Create a context on `device` with an HBM byte budget (0 = 90 % of free memory, as
+ * context.hpp:68-104).  The context owns one non-blocking stream unless one is attached. */
+vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** out);
+vb_status vb_context_destroy(vb_context* ctx);
+/* Use the caller's cudaStream_t for all work of this context (NULL restores its own). */
+vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream);
+vb_status vb_context_synchronize(vb_context* ctx);
+/* Last error message of this context (or of the last failed create when ctx is NULL). */
+const char* vb_last_error(const vb_context* ctx);
+/* Bytes currently allocated by the context and the peak (reference: gpu_peak_device_bytes,
+ * src/cli/cuvbscf.cpp:121-190). */
+vb_status vb_context_memory(const vb_context* ctx, size_t* current_bytes, size_t* peak_bytes);
+
+/* ---- structure generation and expansion (host) ------------------------------------------- */
+
+/* Structure-class generation: keyword as the deck's STR= value ("COV", "ION(1)", "COV ION(1)",
+ * "FULL").  Replaces build_generated_raw_structures_from_structure_class
+ * (src/input/loading/generated_structures.cpp:674-716).  rows_out (nullable) receives
+ * n_structures x (n_active_electrons + 2 n_inactive) 1-based orbital labels, row-major. */
+vb_status vb_generate_structures(const char* keyword, int n_active_orbitals, int n_active_electrons,
+                                 int spin_multiplicity, int n_inactive, int64_t* n_structures_out,
+                                 int32_t* rows_out, int64_t rows_capacity);
+
+/* Determinant expansion of raw structures (StructureExpander::expand,
+ * src/vbscf/structures/expansion/expander.cpp:287-557).  Two-call protocol: call with NULL
+ * outputs to get the sizes, then with buffers.  Strings are occupation bit masks sorted
+ * ascending; determinants are ordered by (alpha rank, beta rank); terms are CSR by determinant
+ * with +-1 coefficients. */
+typedef struct {
+    int32_t n_structures;
+    int32_t n_alpha_electrons;
+    int32_t n_beta_electrons;
+    int32_t n_alpha_strings;
+    int32_t n_beta_strings;
+    int64_t n_determinants;
+    int64_t n_terms;
+} vb_expansion_sizes;
+
+vb_status vb_expand_structures(const int32_t* rows, int64_t n_structures, int n_active_electrons,
+                               int spin_multiplicity, int n_inactive, vb_expansion_sizes* sizes,
+                               uint64_t* alpha_strings, uint64_t* beta_strings, int32_t* det_alpha,
+                               int32_t* det_beta, int64_t* term_offsets, int32_t* term_structure,
+                               double* term_coefficient);
+
+/* ---- structure Hamiltonian / overlap (the determinant-pair hot path) --------------------- */
+
+/* A plan holds the orbital-independent topology on the device (string tables, determinant
+ * list, incidence) and the scratch for the spin-pair records, so repeated evaluations at new
+ * orbitals (every optimizer trial) re-upload nothing but S, h and (ij|kl).  It replaces
+ * FullDeterminantStructureHamiltonianOverlapBuilder::build
+ * (src/vbscf/structures/assembly/hamiltonian_overlap.hpp:70-107) with
+ * DeterminantPairEvaluator::{evaluate_same_spin_pair, combine_spin_pair_evaluations}
+ * (src/vbscf/determinants/pairs/evaluator.hpp:81-154) as its inner kernels. */
+typedef struct {
+    int32_t n_orbitals;
+    int32_t n_alpha_electrons;
+    int32_t n_beta_electrons;
+    int32_t n_alpha_strings;
+    int32_t n_beta_strings;
+    const uint64_t* alpha_strings; /* host, sorted ascending occupation masks */
+    const uint64_t* beta_strings;
+    int64_t n_determinants;
+    const int32_t* det_alpha; /* host, string index per determinant */
+    const int32_t* det_beta;
+    int32_t n_structures;
+    const int64_t* term_offsets; /* host CSR by determinant, n_determinants + 1 */
+    const int32_t* term_structure;
+    const double* term_coefficient;
+} vb_expansion;
+
+vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* expansion, vb_hs_plan** out);
+vb_status vb_hs_plan_destroy(vb_hs_plan* plan);
+
+/* Evaluate H and S (n_structures^2 each, column-major, symmetric).  Inputs: active overlap
+ * S_act (n x n), one-electron h (n x n), packed (ij|kl) of length P(P+1)/2 with
+ * P = n(n+1)/2.  mem_space says where all five pointers live.  Stream-ordered; with
+ * VB_MEM_HOST the call returns after the results are on the host. */
+vb_status vb_hs_plan_execute(vb_hs_plan* plan, const double* ovlp_act, const double* h1e_act,
+                             const double* eri_packed, int mem_space, double* hamiltonian_out,
+                             double* overlap_out);
+
+/* Diagnostics of the last execute: spin pairs evaluated, pairs routed to the exact
+ * full-pivot/SVD path, determinant pairs evaluated. */
+typedef struct {
+    int64_t spin_pairs;
+    int64_t careful_spin_pairs;
+    int64_t determinant_pairs;
+    int64_t kernel_launches;
+} vb_hs_stats;
+vb_status vb_hs_plan_stats(const vb_hs_plan* plan, vb_hs_stats* stats);
+
+/* Phase timing with CUDA events on the context stream (the device counterpart of the
+ * reference's XMVB_PHASE_TIMING scoped phases, src/core/timing.hpp:411).  When enabled, every
+ * execute records events around its phases; vb_hs_plan_phase_times synchronizes and returns
+ * the milliseconds of the last execute per phase: [0] integral tables, [1] spin-pair records
+ * (fast + exact kernels), [2] determinant pairs (all bands), [3] band reduction,
+ * [4] structure reduction + symmetrization.  Phases [2] and [3] sum over bands. */
+enum { VB_PHASE_TABLES = 0, VB_PHASE_SPIN_PAIRS = 1, VB_PHASE_DETERMINANT_PAIRS = 2, VB_PHASE_BAND_REDUCE = 3,
+       VB_PHASE_STRUCTURE_REDUCE = 4, VB_PHASE_COUNT = 5 };
+vb_status vb_hs_plan_enable_phase_timing(vb_hs_plan* plan, int enable);
+vb_status vb_hs_plan_phase_times(vb_hs_plan* plan, double* milliseconds, int count);
+
+/* ---- determinant-pair level entry points ---------------------------------------------------- */
+
+/* Batched overlap resolution (DeterminantOverlapResolver::resolve_matrix,
+ * src/vbscf/determinants/algebra/overlap.hpp:53, overlap.cpp:50-109) plus the first-order
+ * cofactor matrix (build_first_order_cofactor_matrix, contractions.cpp:172-237).
+ * blocks: batch x k x k column-major; out det[batch], nullity[batch], cofactor (batch x k x k,
+ * zero for nullity >= 2).  mem_space applies to all pointers. */
+vb_status vb_resolve_overlaps(vb_context* ctx, int k, int64_t batch, const double* blocks, int mem_space,
+                              double* det_out, int32_t* nullity_out, double* cofactor_out);
+
+/* Same-spin pair evaluation for explicit (left, right) occupied lists
+ * (DeterminantPairEvaluator::evaluate_same_spin_pair, evaluator.cpp:297-352).
+ * occ_left/occ_right: batch x k int32 orbital indices (ascending).  out_scalars: batch x 4
+ * {det, one-electron H, total same-spin H, nullity}; cofactor_out (nullable): batch x k x k. */
+vb_status vb_same_spin_pairs(vb_context* ctx, int n_orbitals, int k, int64_t batch, const int32_t* occ_left,
+                             const int32_t* occ_right, const double* ovlp_act, const double* h1e_act,
+                             const double* eri_packed, int mem_space, double* out_scalars,
+                             double* cofactor_out);
+
+/* Full determinant pairs <left|H|right>, <left|right> for a plan's determinant list
+ * (DeterminantPairEvaluator::evaluate, evaluator.cpp:421-466): pairs[2*i] = left index,
+ * pairs[2*i+1] = right index.  Outputs H and S per pair. */
+vb_status vb_hs_plan_determinant_pairs(vb_hs_plan* plan, const double* ovlp_act, const double* h1e_act,
+                                       const double* eri_packed, int64_t n_pairs, const int64_t* pairs,
+                                       int mem_space, double* h_out, double* s_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VBCORE_H */

@@ -1,0 +1,184 @@
+"""GPU parity of the determinant-pair path through the C ABI against the oracle.
+
+Tolerances are the north-star bar for structure matrices: 1e-10 relative on every H/S element
+(relative to max(1, max |H|)), and the reference's own per-pair closeness for the determinant
+level."""
+
+import numpy as np
+import pytest
+
+import oracle as O
+import vbcore
+from vbcore import workloads
+from conftest import golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+REL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = vbcore.Context(0)
+    yield c
+    c.close()
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(1.0, np.abs(b).max())
+
+
+def _plan(ctx, kw, n, nel, mult=1):
+    rows = vbcore.generate_structures(kw, n, nel, mult)
+    ex = vbcore.expand_structures(rows, nel, mult)
+    return vbcore.HsPlan(ctx, ex, n), O.expand(O.generate_structures(kw, n, nel, mult), nel, mult)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_structure_matrices_match_golden(ctx, name):
+    z = load_golden(name)
+    n, nel, mult, kw = int(z["n"]), int(z["n_el"]), int(z["mult"]), str(z["keyword"])
+    plan, _ = _plan(ctx, kw, n, nel, mult)
+    H, S = plan.execute(z["S"], z["h"], z["eri"])
+    assert _rel(H, z["Hs"]) < REL
+    assert _rel(S, z["Ss"]) < REL
+
+
+@pytest.mark.parametrize("kw,n,seed", [("COV", 8, 1), ("COV", 10, 2), ("COV", 12, 3), ("COV ION(1)", 8, 4),
+                                       ("COV ION(1)", 6, 5), ("FULL", 6, 6)])
+def test_structure_matrices_match_oracle(ctx, kw, n, seed):
+    S, h, eri = workloads.active_space(n, 3 * n, seed)
+    plan, ex = _plan(ctx, kw, n, n)
+    H, So = plan.execute(S, h, eri)
+    Hr, Sr, _ = O.structure_matrices(n, ex, S, h, eri)
+    assert _rel(H, Hr) < REL
+    assert _rel(So, Sr) < REL
+    assert np.array_equal(H, H.T) and np.array_equal(So, So.T)
+    st = plan.stats()
+    assert st["spin_pairs"] > 0 and st["kernel_launches"] >= 5
+
+
+def test_open_shell_tables(ctx):
+    # doublet and triplet: alpha and beta string tables differ
+    for n, nel, mult in ((5, 5, 2), (6, 4, 3), (7, 6, 3)):
+        S, h, eri = workloads.active_space(n, 2 * n, 11 + n)
+        plan, ex = _plan(ctx, "COV", n, nel, mult)
+        H, So = plan.execute(S, h, eri)
+        Hr, Sr, _ = O.structure_matrices(n, ex, S, h, eri)
+        assert _rel(H, Hr) < REL and _rel(So, Sr) < REL
+
+
+def test_orthogonal_orbitals_take_the_exact_path(ctx):
+    z = load_golden("orthogonal_n6")
+    plan, _ = _plan(ctx, str(z["keyword"]), int(z["n"]), int(z["n_el"]))
+    H, S = plan.execute(z["S"], z["h"], z["eri"])
+    assert _rel(H, z["Hs"]) < REL and _rel(S, z["Ss"]) < REL
+    st = plan.stats()
+    assert st["careful_spin_pairs"] > 0  # singular blocks (nullity 1, 2, ...) present
+
+
+def test_determinant_pairs_match_oracle(ctx):
+    n = 8
+    S, h, eri = workloads.active_space(n, 24, 7)
+    plan, ex = _plan(ctx, "COV ION(1)", n, n)
+    Hd, Sd = O.determinant_matrices(n, ex.det_alpha_occ, ex.det_beta_occ, S, h, eri)
+    rng = np.random.default_rng(0)
+    pairs = rng.integers(0, ex.n_determinants, size=(4000, 2))
+    ho, so = plan.determinant_pairs(S, h, eri, pairs)
+    assert np.abs(ho - Hd[pairs[:, 0], pairs[:, 1]]).max() < REL * max(1.0, np.abs(Hd).max())
+    assert np.abs(so - Sd[pairs[:, 0], pairs[:, 1]]).max() < REL * max(1.0, np.abs(Sd).max())
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 6, 7, 9])
+def test_resolve_overlaps_reference_semantics(ctx, k):
+    rng = np.random.default_rng(k)
+    blocks = []
+    for drop in range(0, min(k, 3) + 1):
+        for _ in range(6):
+            x = rng.standard_normal((k, k))
+            if drop:
+                u, s, vt = np.linalg.svd(x)
+                s[k - drop:] = 0.0
+                x = (u * s) @ vt
+            blocks.append(x)
+    blocks.append(np.zeros((k, k)))
+    blocks = np.array(blocks)
+    det, nul, cof = ctx.resolve_overlaps(blocks)
+    for i, x in enumerate(blocks):
+        d_ref, n_ref, _, c_ref = O.resolve(x)
+        assert nul[i] == n_ref
+        assert abs(det[i] - d_ref) <= 1e-12 * max(1.0, abs(d_ref))
+        assert np.abs(cof[i] - c_ref).max() <= 1e-11 * max(1.0, np.abs(c_ref).max())
+
+
+def test_same_spin_pairs_match_oracle(ctx):
+    n, k = 10, 5
+    S, h, eri = workloads.active_space(n, 30, 3)
+    rng = np.random.default_rng(5)
+    L = np.array([np.sort(rng.choice(n, k, replace=False)) for _ in range(300)])
+    R = np.array([np.sort(rng.choice(n, k, replace=False)) for _ in range(300)])
+    R[:20] = L[:20]  # diagonal pairs
+    sc, cof = ctx.same_spin_pairs(n, L, R, S, h, eri)
+    for i in range(len(L)):
+        ref = O.spin_pair(n, L[i], R[i], S, h, eri)
+        assert int(sc[i, 3]) == ref["nullity"]
+        for j, key in enumerate(("det", "h1", "htot")):
+            assert abs(sc[i, j] - ref[key]) <= 1e-11 * max(1.0, abs(ref[key]))
+
+
+def test_reproducible_and_device_path(ctx):
+    import torch
+    n = 10
+    S, h, eri = workloads.active_space(n, 30, 9)
+    plan, _ = _plan(ctx, "COV", n, n)
+    H1, S1 = plan.execute(S, h, eri)
+    H2, S2 = plan.execute(S, h, eri)
+    assert np.array_equal(H1, H2) and np.array_equal(S1, S2)
+    dev = torch.device("cuda:0")
+    tS = torch.tensor(S.T.copy(), device=dev)
+    th = torch.tensor(h.T.copy(), device=dev)
+    te = torch.tensor(eri, device=dev)
+    ns = plan.n_structures
+    tH = torch.empty((ns, ns), dtype=torch.float64, device=dev)
+    tSo = torch.empty((ns, ns), dtype=torch.float64, device=dev)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    plan.execute_device(tS.data_ptr(), th.data_ptr(), te.data_ptr(), tH.data_ptr(), tSo.data_ptr())
+    torch.cuda.synchronize()
+    ctx.set_stream(None)
+    assert np.array_equal(tH.cpu().numpy().T, H1) and np.array_equal(tSo.cpu().numpy().T, S1)
+
+
+def _structure_elements_oracle(ex, n, S, h, eri, pairs_IJ):
+    """H_IJ, S_IJ for selected structure pairs from the oracle on the determinants involved."""
+    T = ex.coefficient_matrix()
+    out = []
+    for I, J in pairs_IJ:
+        dets = np.nonzero((T[:, I] != 0) | (T[:, J] != 0))[0]
+        Hd, Sd = O.determinant_matrices(n, ex.det_alpha_occ[dets], ex.det_beta_occ[dets], S, h, eri)
+        cI, cJ = T[dets, I], T[dets, J]
+        out.append((cI @ Hd @ cJ, cI @ Sd @ cJ))
+    return np.array(out)
+
+
+def test_full_size_microbenchmark_properties(ctx):
+    """n_active = 14, 3432 determinants, 429 structures (the microbenchmark shape): sampled
+    elements against the oracle, plus size-independent properties (symmetry, positive metric,
+    linearity of H in (h, (ij|kl)))."""
+    n = 14
+    S, h, eri = workloads.active_space(n, 42, 2026)
+    plan, ex = _plan(ctx, "COV", n, n)
+    H, So = plan.execute(S, h, eri)
+    assert H.shape == (429, 429)
+    rng = np.random.default_rng(1)
+    sample = [(0, 0), (428, 428), (0, 428)] + [tuple(rng.integers(0, 429, 2)) for _ in range(5)]
+    ref = _structure_elements_oracle(ex, n, S, h, eri, sample)
+    scale_h = max(1.0, np.abs(H).max())
+    scale_s = max(1.0, np.abs(So).max())
+    for (I, J), (hr, sr) in zip(sample, ref):
+        assert abs(H[I, J] - hr) <= REL * scale_h
+        assert abs(So[I, J] - sr) <= REL * scale_s
+    assert np.array_equal(H, H.T)
+    assert np.linalg.eigvalsh(So).min() > 0
+    H1, S1 = plan.execute(S, h, np.zeros_like(eri))
+    H2, S2 = plan.execute(S, np.zeros_like(h), eri)
+    assert np.array_equal(S1, So) and np.array_equal(S2, So)
+    assert np.abs(H1 + H2 - H).max() <= 1e-12 * scale_h

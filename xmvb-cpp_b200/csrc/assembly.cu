@@ -1,0 +1,125 @@
+// Structure H/S assembly as HBM streams (sm_100a).
+//
+// The reference accumulates H_IJ = sum_{d in I, e in J} c_dI c_eJ H_de for left <= right
+// structure pairs and mirrors the upper triangle (hamiltonian_overlap.cpp:437-450, 890-1022).
+// Here the determinant matrix is symmetric and only its upper triangle U (d <= e) is produced,
+// in bands of columns.  With U' = U with halved diagonal, H_d = U' + U'^T, so
+//   Z  = T^T U'          (n_str x n_det; one streaming pass over every band, band_reduce)
+//   W  = Z T             (n_str x n_str; structure_reduce)
+//   H  = W + W^T         (symmetrize)
+// Every sum runs in a fixed order (no atomics), so results are bitwise reproducible.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace vbcore {
+namespace {
+
+constexpr int kPad = kBandReduceColumns + 1;
+
+// One CTA per 32 band columns; all rows of the band stream through once.  Warp w owns the
+// structures bucketed to it, so each shared-memory accumulator has exactly one writer.
+__global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(BandReduceArgs a) {
+    extern __shared__ double zsm[];
+    double* zh = zsm;
+    double* zs = zsm + (size_t)a.struct_count * kPad;
+    for (int i = threadIdx.x; i < a.struct_count * kPad; i += blockDim.x) {
+        zh[i] = 0.0;
+        zs[i] = 0.0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long j = (long long)blockIdx.x * kBandReduceColumns + lane;
+    const bool valid = j < a.width;
+    const long long e = a.e0 + j;
+    long long row_end = a.e0 + (long long)blockIdx.x * kBandReduceColumns + kBandReduceColumns;
+    if (row_end > a.e0 + a.width) row_end = a.e0 + a.width;
+    const long long* off = a.woff + (long long)warp * (a.n_det + 1);
+    for (long long d = 0; d < row_end; ++d) {
+        const long long t0 = __ldg(off + d), t1 = __ldg(off + d + 1);
+        if (t0 == t1) continue;
+        double hv = 0.0, sv = 0.0;
+        if (valid && d <= e) {
+            hv = __ldg(a.Hb + d * a.width + j);
+            sv = __ldg(a.Sb + d * a.width + j);
+            if (d == e) {
+                hv *= 0.5;
+                sv *= 0.5;
+            }
+        }
+        for (long long t = t0; t < t1; ++t) {
+            const int I = __ldg(a.wstruct + t) - a.struct_begin;
+            const double c = __ldg(a.wcoef + t);
+            zh[I * kPad + lane] = fma(c, hv, zh[I * kPad + lane]);
+            zs[I * kPad + lane] = fma(c, sv, zs[I * kPad + lane]);
+        }
+    }
+    __syncthreads();
+    const long long col0 = a.e0 + (long long)blockIdx.x * kBandReduceColumns;
+    for (int i = threadIdx.x; i < a.struct_count * kBandReduceColumns; i += blockDim.x) {
+        const int I = i % a.struct_count, l = i / a.struct_count;
+        if ((long long)blockIdx.x * kBandReduceColumns + l >= a.width) continue;
+        const long long col = col0 + l;
+        a.Zh[col * a.n_str + a.struct_begin + I] = zh[I * kPad + l];
+        a.Zs[col * a.n_str + a.struct_begin + I] = zs[I * kPad + l];
+    }
+}
+
+// W[I, J] = sum_{(e, c) in J} c Z[I, e]; one CTA per J, threads over I.
+__global__ void structure_reduce_kernel(StructureReduceArgs a) {
+    const int J = blockIdx.x;
+    const long long t0 = a.str_off[J], t1 = a.str_off[J + 1];
+    for (int I = threadIdx.x; I < a.n_str; I += blockDim.x) {
+        double wh = 0.0, ws = 0.0;
+        for (long long t = t0; t < t1; ++t) {
+            const long long e = __ldg(a.str_det + t);
+            const double c = __ldg(a.str_coef + t);
+            wh = fma(c, __ldg(a.Zh + e * a.n_str + I), wh);
+            ws = fma(c, __ldg(a.Zs + e * a.n_str + I), ws);
+        }
+        a.Wh[(long long)J * a.n_str + I] = wh;
+        a.Ws[(long long)J * a.n_str + I] = ws;
+    }
+}
+
+__global__ void symmetrize_kernel(int n, const double* __restrict__ Wh, const double* __restrict__ Ws,
+                                  double* __restrict__ H, double* __restrict__ S) {
+    const long long total = (long long)n * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long J = t / n, I = t % n;
+        H[t] = Wh[t] + Wh[I * n + J];
+        S[t] = Ws[t] + Ws[I * n + J];
+    }
+}
+
+}  // namespace
+
+size_t band_reduce_smem_bytes(int struct_count) { return sizeof(double) * 2 * (size_t)struct_count * kPad; }
+
+int band_reduce_max_structures() { return (int)((227 * 1024) / (sizeof(double) * 2 * kPad)) / 8 * 8; }
+
+cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches) {
+    const size_t smem = band_reduce_smem_bytes(a.struct_count);
+    cudaError_t err = cudaFuncSetAttribute(band_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    const long long blocks = (a.width + kBandReduceColumns - 1) / kBandReduceColumns;
+    band_reduce_kernel<<<(unsigned)blocks, kBandReduceWarps * 32, smem, stream>>>(a);
+    ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_structure_reduce(const StructureReduceArgs& a, double* H, double* S, cudaStream_t stream,
+                                    int* launches) {
+    structure_reduce_kernel<<<a.n_str, 128, 0, stream>>>(a);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    const long long total = (long long)a.n_str * a.n_str;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 2048) blocks = 2048;
+    symmetrize_kernel<<<(unsigned)blocks, 256, 0, stream>>>(a.n_str, a.Wh, a.Ws, H, S);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+}  // namespace vbcore

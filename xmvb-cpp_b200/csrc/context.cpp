@@ -1,0 +1,132 @@
+// Context, error reporting and budgeted device memory (the role of xmvb::cuda::Context,
+// src/cuda/memory/context.hpp:66-405 in the reference: one device, one stream, a byte budget
+// of 90 % of free HBM by default, allocation counters).
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "internal.h"
+
+namespace {
+std::mutex g_error_mutex;
+std::string g_create_error;
+}  // namespace
+
+namespace vbcore {
+
+vb_status set_error(vb_context* ctx, vb_status code, const std::string& message) {
+    if (ctx) {
+        ctx->last_error = message;
+    } else {
+        std::lock_guard<std::mutex> lock(g_error_mutex);
+        g_create_error = message;
+    }
+    return code;
+}
+
+vb_status cuda_error(vb_context* ctx, cudaError_t err, const char* what) {
+    return set_error(ctx, VB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+void* device_alloc(vb_context* ctx, size_t bytes, vb_status* status) {
+    if (ctx->current + bytes > ctx->budget) {
+        *status = set_error(ctx, VB_ERR_BUDGET,
+                            "device budget exceeded: requested " + std::to_string(bytes) + " bytes with " +
+                                std::to_string(ctx->current) + " of " + std::to_string(ctx->budget) + " in use");
+        return nullptr;
+    }
+    void* p = nullptr;
+    cudaError_t err = cudaMallocAsync(&p, bytes, ctx->stream);
+    if (err != cudaSuccess) {
+        *status = cuda_error(ctx, err, "cudaMallocAsync");
+        return nullptr;
+    }
+    ctx->current += bytes;
+    if (ctx->current > ctx->peak) ctx->peak = ctx->current;
+    *status = VB_OK;
+    return p;
+}
+
+void device_free(vb_context* ctx, void* ptr, size_t bytes) {
+    if (!ptr) return;
+    cudaFreeAsync(ptr, ctx->stream);
+    ctx->current -= bytes;
+}
+
+}  // namespace vbcore
+
+using namespace vbcore;
+
+extern "C" {
+
+vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** out) {
+    if (!out) return set_error(nullptr, VB_ERR_INVALID, "vb_context_create: out is null");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t err = cudaGetDeviceCount(&count);
+    if (err != cudaSuccess || count == 0)
+        return set_error(nullptr, VB_ERR_CUDA,
+                         std::string("no CUDA device available: ") + cudaGetErrorString(err));
+    if (device < 0 || device >= count) return set_error(nullptr, VB_ERR_INVALID, "device index out of range");
+    cudaDeviceProp prop;
+    err = cudaGetDeviceProperties(&prop, device);
+    if (err != cudaSuccess) return set_error(nullptr, VB_ERR_CUDA, "cudaGetDeviceProperties failed");
+    if (prop.major < 10)
+        return set_error(nullptr, VB_ERR_UNSUPPORTED,
+                         std::string("vbcore is built for sm_100a (B200); device is ") + prop.name);
+    err = cudaSetDevice(device);
+    if (err != cudaSuccess) return set_error(nullptr, VB_ERR_CUDA, "cudaSetDevice failed");
+    vb_context* ctx = new (std::nothrow) vb_context();
+    if (!ctx) return set_error(nullptr, VB_ERR_INVALID, "out of host memory");
+    ctx->device = device;
+    err = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) {
+        delete ctx;
+        return set_error(nullptr, VB_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    ctx->stream = ctx->own_stream;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    ctx->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.9 * (double)free_b);
+    *out = ctx;
+    return VB_OK;
+}
+
+vb_status vb_context_destroy(vb_context* ctx) {
+    if (!ctx) return VB_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->own_stream) {
+        cudaStreamSynchronize(ctx->own_stream);
+        cudaStreamDestroy(ctx->own_stream);
+    }
+    delete ctx;
+    return VB_OK;
+}
+
+vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream) {
+    if (!ctx) return VB_ERR_INVALID;
+    ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+    return VB_OK;
+}
+
+vb_status vb_context_synchronize(vb_context* ctx) {
+    if (!ctx) return VB_ERR_INVALID;
+    cudaError_t err = cudaStreamSynchronize(ctx->stream);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "cudaStreamSynchronize");
+    return VB_OK;
+}
+
+const char* vb_last_error(const vb_context* ctx) {
+    if (ctx) return ctx->last_error.c_str();
+    std::lock_guard<std::mutex> lock(g_error_mutex);
+    return g_create_error.c_str();
+}
+
+vb_status vb_context_memory(const vb_context* ctx, size_t* current_bytes, size_t* peak_bytes) {
+    if (!ctx) return VB_ERR_INVALID;
+    if (current_bytes) *current_bytes = ctx->current;
+    if (peak_bytes) *peak_bytes = ctx->peak;
+    return VB_OK;
+}
+
+}  // extern "C"

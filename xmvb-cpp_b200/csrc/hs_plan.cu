@@ -1,0 +1,620 @@
+// Structure H/S plans and the determinant-pair level entry points of the C ABI.
+//
+// A plan uploads the orbital-independent topology once (string tables, determinant list,
+// structure incidence) and owns the spin-pair record scratch; execute() then runs, all
+// stream-ordered on the context's stream:
+//   prepare_tables -> spin_pairs (fast + exact, per distinct spin table)
+//   -> per band of determinant columns: full_pairs -> band_reduce (per structure chunk)
+//   -> structure_reduce + symmetrize.
+// This is the B200 counterpart of FullDeterminantStructureHamiltonianOverlapBuilder::build
+// (src/vbscf/structures/assembly/hamiltonian_overlap.hpp:70-107 in the reference).
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "device_algebra.cuh"
+#include "internal.h"
+#include "kernels.h"
+
+using namespace vbcore;
+
+struct StructureChunk {
+    int begin = 0, count = 0;
+    DeviceBuffer woff, wstruct, wcoef;
+};
+
+struct vb_hs_plan {
+    vb_context* ctx = nullptr;
+    int n = 0, ka = 0, kb = 0, np = 0, gd = 0;
+    int n_str = 0;
+    long long n_det = 0;
+    int Na = 0, Nb = 0;
+    bool shared_tables = false;
+    DeviceBuffer occ_a, occ_b, det_alpha, det_beta;
+    DeviceBuffer rec_a, rec_b;
+    int stride_a = 0, stride_b = 0;
+    long long npairs_a = 0, npairs_b = 0;
+    DeviceBuffer counters, list_a, list_b;
+    DeviceBuffer S_in, h_in, eri_in, gamma, kfull;
+    DeviceBuffer band_h, band_s;
+    long long band_width = 0;
+    DeviceBuffer Zh, Zs, Wh, Ws, Hout, Sout;
+    DeviceBuffer str_off, str_det, str_coef;
+    std::vector<StructureChunk> chunks;
+    vb_hs_stats stats{};
+    bool evaluated = false;
+    // phase timing: per phase a pool of (start, stop) event pairs, `used` pairs this execute
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[VB_PHASE_COUNT];
+    int used[VB_PHASE_COUNT] = {0, 0, 0, 0, 0};
+    ~vb_hs_plan() {
+        for (auto& v : events)
+            for (auto& e : v) {
+                cudaEventDestroy(e.first);
+                cudaEventDestroy(e.second);
+            }
+    }
+};
+
+namespace {
+
+vb_status upload(vb_context* ctx, DeviceBuffer& buf, const void* src, size_t bytes) {
+    vb_status st = buf.allocate(ctx, bytes);
+    if (st != VB_OK) return st;
+    if (bytes == 0) return VB_OK;
+    cudaError_t err = cudaMemcpyAsync(buf.ptr, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "cudaMemcpyAsync (plan upload)");
+    return VB_OK;
+}
+
+std::vector<uint64_t> occupation_rows(const uint64_t* masks, int count, int k, int n, std::string* error) {
+    std::vector<uint64_t> rows(2 * (size_t)count, ~uint64_t{0});
+    for (int s = 0; s < count; ++s) {
+        uint8_t bytes[16];
+        std::memset(bytes, 0xFF, sizeof(bytes));
+        int m = 0;
+        for (int o = 0; o < 64; ++o)
+            if ((masks[s] >> o) & 1) {
+                if (m >= 16 || o >= n) {
+                    *error = "string occupation outside the active space or above 16 electrons";
+                    return {};
+                }
+                bytes[m++] = (uint8_t)o;
+            }
+        if (m != k) {
+            *error = "string electron count does not match the spin's electron count";
+            return {};
+        }
+        std::memcpy(&rows[2 * (size_t)s], bytes, 16);
+    }
+    return rows;
+}
+
+// Phase bracket: records a start event on construction and a stop event on close().
+struct PhaseMark {
+    vb_hs_plan* p;
+    int phase;
+    cudaEvent_t stop = nullptr;
+    PhaseMark(vb_hs_plan* plan, int ph) : p(plan), phase(ph) {
+        if (!p->timing) return;
+        auto& pool = p->events[phase];
+        if (p->used[phase] == (int)pool.size()) {
+            cudaEvent_t a, b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            pool.push_back({a, b});
+        }
+        auto& pr = pool[p->used[phase]++];
+        cudaEventRecord(pr.first, p->ctx->stream);
+        stop = pr.second;
+    }
+    void close() {
+        if (stop) cudaEventRecord(stop, p->ctx->stream);
+        stop = nullptr;
+    }
+    ~PhaseMark() { close(); }
+};
+
+int record_stride(int k) {
+    int s = k * k + 4;
+    return (s + 1) / 2 * 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan** out) {
+    if (!ctx || !ex || !out) return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_create: null argument");
+    *out = nullptr;
+    const int n = ex->n_orbitals;
+    if (n <= 0 || n > kMaxOrbitals) return set_error(ctx, VB_ERR_UNSUPPORTED, "n_orbitals must be in 1..64");
+    if (ex->n_alpha_electrons < 0 || ex->n_alpha_electrons > kMaxElectrons || ex->n_beta_electrons < 0 ||
+        ex->n_beta_electrons > kMaxElectrons)
+        return set_error(ctx, VB_ERR_UNSUPPORTED, "electrons per spin must be in 0..16");
+    if (ex->n_determinants <= 0 || ex->n_structures <= 0)
+        return set_error(ctx, VB_ERR_INVALID, "at least one determinant and one structure are required");
+    if (ex->n_alpha_electrons > 0 && (ex->n_alpha_strings <= 0 || !ex->alpha_strings))
+        return set_error(ctx, VB_ERR_INVALID, "alpha string table missing");
+    if (ex->n_beta_electrons > 0 && (ex->n_beta_strings <= 0 || !ex->beta_strings))
+        return set_error(ctx, VB_ERR_INVALID, "beta string table missing");
+    if (!ex->det_alpha || !ex->det_beta || !ex->term_offsets || !ex->term_structure || !ex->term_coefficient)
+        return set_error(ctx, VB_ERR_INVALID, "expansion arrays missing");
+    cudaSetDevice(ctx->device);
+    vb_hs_plan* p = new (std::nothrow) vb_hs_plan();
+    if (!p) return set_error(ctx, VB_ERR_INVALID, "out of host memory");
+    p->ctx = ctx;
+    p->n = n;
+    p->ka = ex->n_alpha_electrons;
+    p->kb = ex->n_beta_electrons;
+    p->np = n * (n + 1) / 2;
+    p->gd = n * (n - 1) / 2;
+    p->n_str = ex->n_structures;
+    p->n_det = ex->n_determinants;
+    p->Na = p->ka > 0 ? ex->n_alpha_strings : 0;
+    p->Nb = p->kb > 0 ? ex->n_beta_strings : 0;
+    auto fail = [&](vb_status st) {
+        delete p;
+        return st;
+    };
+    // validate the determinant list and incidence
+    for (long long d = 0; d < p->n_det; ++d) {
+        if ((p->ka > 0 && (ex->det_alpha[d] < 0 || ex->det_alpha[d] >= p->Na)) ||
+            (p->kb > 0 && (ex->det_beta[d] < 0 || ex->det_beta[d] >= p->Nb)))
+            return fail(set_error(ctx, VB_ERR_INVALID, "determinant string index out of range"));
+    }
+    if (ex->term_offsets[0] != 0) return fail(set_error(ctx, VB_ERR_INVALID, "term offsets must start at 0"));
+    for (long long d = 0; d < p->n_det; ++d)
+        if (ex->term_offsets[d + 1] < ex->term_offsets[d])
+            return fail(set_error(ctx, VB_ERR_INVALID, "term offsets must be non-decreasing"));
+    const long long n_terms = ex->term_offsets[p->n_det];
+    for (long long t = 0; t < n_terms; ++t)
+        if (ex->term_structure[t] < 0 || ex->term_structure[t] >= p->n_str)
+            return fail(set_error(ctx, VB_ERR_INVALID, "term structure index out of range"));
+
+    std::string err;
+    std::vector<uint64_t> occa, occb;
+    if (p->ka > 0) {
+        occa = occupation_rows(ex->alpha_strings, p->Na, p->ka, n, &err);
+        if (occa.empty()) return fail(set_error(ctx, VB_ERR_INVALID, err));
+    }
+    if (p->kb > 0) {
+        occb = occupation_rows(ex->beta_strings, p->Nb, p->kb, n, &err);
+        if (occb.empty()) return fail(set_error(ctx, VB_ERR_INVALID, err));
+    }
+    p->shared_tables = p->ka > 0 && p->ka == p->kb && p->Na == p->Nb &&
+                       std::equal(ex->alpha_strings, ex->alpha_strings + p->Na, ex->beta_strings);
+    vb_status st;
+    if ((st = upload(ctx, p->occ_a, occa.data(), occa.size() * 8)) != VB_OK) return fail(st);
+    if ((st = upload(ctx, p->occ_b, occb.data(), occb.size() * 8)) != VB_OK) return fail(st);
+    if ((st = upload(ctx, p->det_alpha, ex->det_alpha, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
+    if ((st = upload(ctx, p->det_beta, ex->det_beta, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
+
+    // spin-pair records
+    p->stride_a = record_stride(p->ka);
+    p->stride_b = record_stride(p->kb);
+    p->npairs_a = (long long)p->Na * (p->Na + 1) / 2;
+    p->npairs_b = p->shared_tables ? 0 : (long long)p->Nb * (p->Nb + 1) / 2;
+    if ((st = p->rec_a.allocate(ctx, sizeof(double) * p->stride_a * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
+    if ((st = p->list_a.allocate(ctx, sizeof(long long) * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
+    if (!p->shared_tables) {
+        if ((st = p->rec_b.allocate(ctx, sizeof(double) * p->stride_b * std::max(1LL, p->npairs_b))) != VB_OK)
+            return fail(st);
+        if ((st = p->list_b.allocate(ctx, sizeof(long long) * std::max(1LL, p->npairs_b))) != VB_OK) return fail(st);
+    }
+    if ((st = p->counters.allocate(ctx, 4 * sizeof(unsigned long long))) != VB_OK) return fail(st);
+
+    // inputs and derived integral tables
+    if ((st = p->S_in.allocate(ctx, sizeof(double) * n * n)) != VB_OK) return fail(st);
+    if ((st = p->h_in.allocate(ctx, sizeof(double) * n * n)) != VB_OK) return fail(st);
+    if ((st = p->eri_in.allocate(ctx, sizeof(double) * (size_t)p->np * (p->np + 1) / 2)) != VB_OK) return fail(st);
+    if ((st = p->gamma.allocate(ctx, sizeof(double) * std::max(1, p->gd * p->gd))) != VB_OK) return fail(st);
+    if ((st = p->kfull.allocate(ctx, sizeof(double) * p->np * p->np)) != VB_OK) return fail(st);
+
+    // band of determinant columns: keep the two band buffers within ~4 GB and 1/4 of the budget
+    const size_t band_cap = std::min<size_t>((size_t)4 << 30, ctx->budget / 4);
+    long long width = (long long)(band_cap / (16 * (size_t)p->n_det));
+    width = std::max(32LL, std::min(width, p->n_det));
+    p->band_width = width;
+    if ((st = p->band_h.allocate(ctx, sizeof(double) * p->n_det * width)) != VB_OK) return fail(st);
+    if ((st = p->band_s.allocate(ctx, sizeof(double) * p->n_det * width)) != VB_OK) return fail(st);
+    const size_t zbytes = sizeof(double) * (size_t)p->n_str * p->n_det;
+    if ((st = p->Zh.allocate(ctx, zbytes)) != VB_OK) return fail(st);
+    if ((st = p->Zs.allocate(ctx, zbytes)) != VB_OK) return fail(st);
+    const size_t wbytes = sizeof(double) * (size_t)p->n_str * p->n_str;
+    for (DeviceBuffer* b : {&p->Wh, &p->Ws, &p->Hout, &p->Sout})
+        if ((st = b->allocate(ctx, wbytes)) != VB_OK) return fail(st);
+
+    // structure-major incidence (CSC of T)
+    std::vector<long long> soff(p->n_str + 1, 0);
+    for (long long t = 0; t < n_terms; ++t) ++soff[ex->term_structure[t] + 1];
+    for (int I = 0; I < p->n_str; ++I) soff[I + 1] += soff[I];
+    std::vector<long long> sdet(n_terms), next(soff.begin(), soff.end() - 1);
+    std::vector<double> scoef(n_terms);
+    for (long long d = 0; d < p->n_det; ++d)
+        for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t) {
+            const long long pos = next[ex->term_structure[t]]++;
+            sdet[pos] = d;
+            scoef[pos] = ex->term_coefficient[t];
+        }
+    if ((st = upload(ctx, p->str_off, soff.data(), sizeof(long long) * soff.size())) != VB_OK) return fail(st);
+    if ((st = upload(ctx, p->str_det, sdet.data(), sizeof(long long) * std::max<size_t>(1, sdet.size()))) != VB_OK)
+        return fail(st);
+    if ((st = upload(ctx, p->str_coef, scoef.data(), sizeof(double) * std::max<size_t>(1, scoef.size()))) != VB_OK)
+        return fail(st);
+
+    // per structure chunk: determinant-major term lists bucketed by (structure - begin) mod warps
+    const int max_chunk = band_reduce_max_structures();
+    for (int begin = 0; begin < p->n_str; begin += max_chunk) {
+        StructureChunk ch;
+        ch.begin = begin;
+        ch.count = std::min(max_chunk, p->n_str - begin);
+        std::vector<long long> woff((size_t)kBandReduceWarps * (p->n_det + 1), 0);
+        std::vector<int> wstruct;
+        std::vector<double> wcoef;
+        for (int w = 0; w < kBandReduceWarps; ++w) {
+            long long* o = woff.data() + (size_t)w * (p->n_det + 1);
+            o[0] = (long long)wstruct.size();
+            for (long long d = 0; d < p->n_det; ++d) {
+                for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t) {
+                    const int I = ex->term_structure[t];
+                    if (I >= begin && I < begin + ch.count && (I - begin) % kBandReduceWarps == w) {
+                        wstruct.push_back(I);
+                        wcoef.push_back(ex->term_coefficient[t]);
+                    }
+                }
+                o[d + 1] = (long long)wstruct.size();
+            }
+        }
+        if ((st = upload(ctx, ch.woff, woff.data(), sizeof(long long) * woff.size())) != VB_OK) return fail(st);
+        if ((st = upload(ctx, ch.wstruct, wstruct.data(), sizeof(int) * std::max<size_t>(1, wstruct.size()))) != VB_OK)
+            return fail(st);
+        if ((st = upload(ctx, ch.wcoef, wcoef.data(), sizeof(double) * std::max<size_t>(1, wcoef.size()))) != VB_OK)
+            return fail(st);
+        p->chunks.push_back(std::move(ch));
+    }
+    cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    if (e2 != cudaSuccess) return fail(cuda_error(ctx, e2, "plan upload"));
+    *out = p;
+    return VB_OK;
+}
+
+vb_status vb_hs_plan_destroy(vb_hs_plan* plan) {
+    if (!plan) return VB_OK;
+    cudaStreamSynchronize(plan->ctx->stream);
+    delete plan;
+    return VB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+SpinTableArgs table_args(vb_hs_plan* p, bool beta, const double* S, const double* h, const double* eri) {
+    SpinTableArgs a{};
+    a.n = p->n;
+    a.k = beta ? p->kb : p->ka;
+    a.n_strings = beta ? p->Nb : p->Na;
+    a.occ = beta ? p->occ_b.as<uint64_t>() : p->occ_a.as<uint64_t>();
+    a.n_pairs = beta ? p->npairs_b : p->npairs_a;
+    a.S = S;
+    a.h = h;
+    a.gamma = p->gamma.as<double>();
+    a.eri = eri;
+    a.gamma_dim = p->gd;
+    a.records = beta ? p->rec_b.as<double>() : p->rec_a.as<double>();
+    a.rec_stride = beta ? p->stride_b : p->stride_a;
+    a.careful_count = p->counters.as<unsigned long long>() + (beta ? 1 : 0);
+    a.careful_list = beta ? p->list_b.as<long long>() : p->list_a.as<long long>();
+    a.all_careful = 0;
+    return a;
+}
+
+FullPairArgs full_args(vb_hs_plan* p) {
+    FullPairArgs a{};
+    a.n = p->n;
+    a.ka = p->ka;
+    a.kb = p->kb;
+    a.np = p->np;
+    a.n_det = p->n_det;
+    a.det_alpha = p->det_alpha.as<int>();
+    a.det_beta = p->det_beta.as<int>();
+    a.occ_a = p->occ_a.as<uint64_t>();
+    a.occ_b = p->shared_tables ? p->occ_a.as<uint64_t>() : p->occ_b.as<uint64_t>();
+    a.rec_a = p->rec_a.as<double>();
+    a.rec_b = p->shared_tables ? p->rec_a.as<double>() : p->rec_b.as<double>();
+    a.stride_a = p->stride_a;
+    a.stride_b = p->stride_b;
+    a.kfull = p->kfull.as<double>();
+    return a;
+}
+
+// Stage inputs and evaluate the spin-pair records of every distinct table.
+vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem,
+                               const double** dS, const double** dh, const double** deri, int* launches) {
+    vb_context* ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    const size_t n2 = sizeof(double) * p->n * p->n;
+    const size_t ne = sizeof(double) * (size_t)p->np * (p->np + 1) / 2;
+    if (mem == VB_MEM_HOST) {
+        cudaError_t err = cudaMemcpyAsync(p->S_in.ptr, S, n2, cudaMemcpyHostToDevice, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(p->h_in.ptr, h, n2, cudaMemcpyHostToDevice, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(p->eri_in.ptr, eri, ne, cudaMemcpyHostToDevice, s);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "input upload");
+        *dS = p->S_in.as<double>();
+        *dh = p->h_in.as<double>();
+        *deri = p->eri_in.as<double>();
+    } else {
+        *dS = S;
+        *dh = h;
+        *deri = eri;
+    }
+    for (int& u : p->used) u = 0;
+    PhaseMark tables(p, VB_PHASE_TABLES);
+    cudaError_t err = launch_prepare_tables(p->n, *deri, p->gamma.as<double>(), p->kfull.as<double>(), s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "prepare_tables");
+    ++*launches;
+    tables.close();
+    PhaseMark spin(p, VB_PHASE_SPIN_PAIRS);
+    err = cudaMemsetAsync(p->counters.ptr, 0, 4 * sizeof(unsigned long long), s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "cudaMemsetAsync");
+    if (p->ka > 0) {
+        err = launch_spin_pairs(table_args(p, false, *dS, *dh, *deri), s, launches);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs (alpha)");
+    }
+    if (p->kb > 0 && !p->shared_tables) {
+        err = launch_spin_pairs(table_args(p, true, *dS, *dh, *deri), s, launches);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs (beta)");
+    }
+    return VB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem,
+                             double* H_out, double* S_out) {
+    if (!p) return VB_ERR_INVALID;
+    vb_context* ctx = p->ctx;
+    if (!S || !h || !eri || !H_out || !S_out) return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_execute: null pointer");
+    if (mem != VB_MEM_HOST && mem != VB_MEM_DEVICE) return set_error(ctx, VB_ERR_INVALID, "bad memory space");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int launches = 0;
+    const double *dS, *dh, *deri;
+    vb_status st = prepare_spin_records(p, S, h, eri, mem, &dS, &dh, &deri, &launches);
+    if (st != VB_OK) return st;
+    FullPairArgs fa = full_args(p);
+    for (long long e0 = 0; e0 < p->n_det; e0 += p->band_width) {
+        const long long e1 = std::min(p->n_det, e0 + p->band_width);
+        const long long B = e1 - e0;
+        fa.e0 = e0;
+        fa.e1 = e1;
+        fa.n_items = e0 * B + B * (B + 1) / 2;
+        fa.Hb = p->band_h.as<double>();
+        fa.Sb = p->band_s.as<double>();
+        PhaseMark pairs(p, VB_PHASE_DETERMINANT_PAIRS);
+        cudaError_t err = launch_full_pairs(fa, s, &launches);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "full_pairs");
+        pairs.close();
+        PhaseMark reduce(p, VB_PHASE_BAND_REDUCE);
+        for (const StructureChunk& ch : p->chunks) {
+            BandReduceArgs ba{};
+            ba.n_det = p->n_det;
+            ba.n_str = p->n_str;
+            ba.e0 = e0;
+            ba.width = B;
+            ba.Hb = fa.Hb;
+            ba.Sb = fa.Sb;
+            ba.woff = ch.woff.as<long long>();
+            ba.wstruct = ch.wstruct.as<int>();
+            ba.wcoef = ch.wcoef.as<double>();
+            ba.struct_begin = ch.begin;
+            ba.struct_count = ch.count;
+            ba.Zh = p->Zh.as<double>();
+            ba.Zs = p->Zs.as<double>();
+            err = launch_band_reduce(ba, s, &launches);
+            if (err != cudaSuccess) return cuda_error(ctx, err, "band_reduce");
+        }
+    }
+    StructureReduceArgs ra{};
+    ra.n_str = p->n_str;
+    ra.n_det = p->n_det;
+    ra.str_off = p->str_off.as<long long>();
+    ra.str_det = p->str_det.as<long long>();
+    ra.str_coef = p->str_coef.as<double>();
+    ra.Zh = p->Zh.as<double>();
+    ra.Zs = p->Zs.as<double>();
+    ra.Wh = p->Wh.as<double>();
+    ra.Ws = p->Ws.as<double>();
+    double* Hdst = mem == VB_MEM_DEVICE ? H_out : p->Hout.as<double>();
+    double* Sdst = mem == VB_MEM_DEVICE ? S_out : p->Sout.as<double>();
+    PhaseMark sreduce(p, VB_PHASE_STRUCTURE_REDUCE);
+    cudaError_t err = launch_structure_reduce(ra, Hdst, Sdst, s, &launches);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "structure_reduce");
+    sreduce.close();
+    if (mem == VB_MEM_HOST) {
+        const size_t wbytes = sizeof(double) * (size_t)p->n_str * p->n_str;
+        err = cudaMemcpyAsync(H_out, Hdst, wbytes, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(S_out, Sdst, wbytes, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "result download");
+    }
+    p->stats.spin_pairs = p->npairs_a + p->npairs_b;
+    p->stats.determinant_pairs = p->n_det * (p->n_det + 1) / 2;
+    p->stats.kernel_launches = launches;
+    p->evaluated = true;
+    return VB_OK;
+}
+
+vb_status vb_hs_plan_enable_phase_timing(vb_hs_plan* p, int enable) {
+    if (!p) return VB_ERR_INVALID;
+    p->timing = enable != 0;
+    return VB_OK;
+}
+
+vb_status vb_hs_plan_phase_times(vb_hs_plan* p, double* ms, int count) {
+    if (!p || !ms || count < 0) return VB_ERR_INVALID;
+    for (int ph = 0; ph < count && ph < VB_PHASE_COUNT; ++ph) {
+        double total = 0.0;
+        for (int i = 0; i < p->used[ph]; ++i) {
+            auto& pr = p->events[ph][i];
+            cudaError_t err = cudaEventSynchronize(pr.second);
+            if (err != cudaSuccess) return cuda_error(p->ctx, err, "phase timing");
+            float t = 0.f;
+            err = cudaEventElapsedTime(&t, pr.first, pr.second);
+            if (err != cudaSuccess) return cuda_error(p->ctx, err, "phase timing");
+            total += t;
+        }
+        ms[ph] = p->timing ? total : 0.0;
+    }
+    for (int ph = VB_PHASE_COUNT; ph < count; ++ph) ms[ph] = 0.0;
+    return VB_OK;
+}
+
+vb_status vb_hs_plan_stats(const vb_hs_plan* p, vb_hs_stats* stats) {
+    if (!p || !stats) return VB_ERR_INVALID;
+    vb_hs_stats s = p->stats;
+    if (p->evaluated) {
+        unsigned long long c[4] = {0, 0, 0, 0};
+        cudaError_t err = cudaMemcpyAsync(c, p->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, p->ctx->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(p->ctx->stream);
+        if (err != cudaSuccess) return cuda_error(p->ctx, err, "stats download");
+        const bool all_a = p->ka > vbcore::kMaxFastElectrons;
+        const bool all_b = p->kb > vbcore::kMaxFastElectrons;
+        s.careful_spin_pairs = (long long)(all_a ? p->npairs_a : c[0]) + (long long)(all_b ? p->npairs_b : c[1]);
+    }
+    *stats = s;
+    return VB_OK;
+}
+
+vb_status vb_hs_plan_determinant_pairs(vb_hs_plan* p, const double* S, const double* h, const double* eri,
+                                       int64_t n_pairs, const int64_t* pairs, int mem, double* h_out, double* s_out) {
+    if (!p) return VB_ERR_INVALID;
+    vb_context* ctx = p->ctx;
+    if (n_pairs < 0 || (n_pairs > 0 && (!pairs || !h_out || !s_out)))
+        return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_determinant_pairs: bad arguments");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int launches = 0;
+    const double *dS, *dh, *deri;
+    vb_status st = prepare_spin_records(p, S, h, eri, mem, &dS, &dh, &deri, &launches);
+    if (st != VB_OK) return st;
+    if (mem == VB_MEM_HOST)
+        for (int64_t i = 0; i < 2 * n_pairs; ++i)
+            if (pairs[i] < 0 || pairs[i] >= p->n_det)
+                return set_error(ctx, VB_ERR_INVALID, "determinant index out of range");
+    DeviceBuffer dp, dh_o, ds_o;
+    const long long* pp = reinterpret_cast<const long long*>(pairs);
+    double *ho = h_out, *so = s_out;
+    if (mem == VB_MEM_HOST) {
+        if ((st = upload(ctx, dp, pairs, sizeof(int64_t) * 2 * std::max<int64_t>(1, n_pairs))) != VB_OK) return st;
+        if ((st = dh_o.allocate(ctx, sizeof(double) * std::max<int64_t>(1, n_pairs))) != VB_OK) return st;
+        if ((st = ds_o.allocate(ctx, sizeof(double) * std::max<int64_t>(1, n_pairs))) != VB_OK) return st;
+        pp = dp.as<long long>();
+        ho = dh_o.as<double>();
+        so = ds_o.as<double>();
+    }
+    cudaError_t err = launch_listed_pairs(full_args(p), n_pairs, pp, ho, so, s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "listed_pairs");
+    if (mem == VB_MEM_HOST && n_pairs > 0) {
+        err = cudaMemcpyAsync(h_out, ho, sizeof(double) * n_pairs, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(s_out, so, sizeof(double) * n_pairs, cudaMemcpyDeviceToHost, s);
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "listed pairs download");
+    return VB_OK;
+}
+
+vb_status vb_resolve_overlaps(vb_context* ctx, int k, int64_t batch, const double* blocks, int mem, double* det_out,
+                              int32_t* nullity_out, double* cofactor_out) {
+    if (!ctx) return VB_ERR_INVALID;
+    if (k < 1 || k > dev::KMAX || batch < 0 || !blocks || !det_out || !nullity_out)
+        return set_error(ctx, VB_ERR_INVALID, "vb_resolve_overlaps: bad arguments");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    DeviceBuffer db, dd, dn, dc;
+    const double* b = blocks;
+    double* det = det_out;
+    int* nul = nullity_out;
+    double* cof = cofactor_out;
+    vb_status st;
+    const size_t kk = (size_t)k * k;
+    if (mem == VB_MEM_HOST) {
+        if ((st = upload(ctx, db, blocks, sizeof(double) * kk * std::max<int64_t>(1, batch))) != VB_OK) return st;
+        if ((st = dd.allocate(ctx, sizeof(double) * std::max<int64_t>(1, batch))) != VB_OK) return st;
+        if ((st = dn.allocate(ctx, sizeof(int) * std::max<int64_t>(1, batch))) != VB_OK) return st;
+        if (cofactor_out && (st = dc.allocate(ctx, sizeof(double) * kk * std::max<int64_t>(1, batch))) != VB_OK)
+            return st;
+        b = db.as<double>();
+        det = dd.as<double>();
+        nul = dn.as<int>();
+        cof = cofactor_out ? dc.as<double>() : nullptr;
+    }
+    cudaError_t err = launch_resolve_blocks(k, batch, b, det, nul, cof, s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "resolve_blocks");
+    if (mem == VB_MEM_HOST && batch > 0) {
+        err = cudaMemcpyAsync(det_out, det, sizeof(double) * batch, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(nullity_out, nul, sizeof(int) * batch, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess && cofactor_out)
+            err = cudaMemcpyAsync(cofactor_out, cof, sizeof(double) * kk * batch, cudaMemcpyDeviceToHost, s);
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "resolve download");
+    return VB_OK;
+}
+
+vb_status vb_same_spin_pairs(vb_context* ctx, int n, int k, int64_t batch, const int32_t* occ_left,
+                             const int32_t* occ_right, const double* S, const double* h, const double* eri, int mem,
+                             double* out_scalars, double* cofactor_out) {
+    if (!ctx) return VB_ERR_INVALID;
+    if (n < 1 || n > kMaxOrbitals || k < 1 || k > dev::KMAX || k > n || batch < 0 || !occ_left || !occ_right || !S ||
+        !h || !eri || !out_scalars)
+        return set_error(ctx, VB_ERR_INVALID, "vb_same_spin_pairs: bad arguments");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const size_t np = (size_t)n * (n + 1) / 2;
+    const size_t kk = (size_t)k * k;
+    const int64_t nb = std::max<int64_t>(1, batch);
+    DeviceBuffer dl, dr, dS, dh, de, dsc, dc;
+    const int* l = occ_left;
+    const int* r = occ_right;
+    const double *pS = S, *ph = h, *pe = eri;
+    double* sc = out_scalars;
+    double* cof = cofactor_out;
+    vb_status st;
+    if (mem == VB_MEM_HOST) {
+        for (int64_t i = 0; i < batch * k; ++i)
+            if (occ_left[i] < 0 || occ_left[i] >= n || occ_right[i] < 0 || occ_right[i] >= n)
+                return set_error(ctx, VB_ERR_INVALID, "orbital index out of range");
+        if ((st = upload(ctx, dl, occ_left, sizeof(int) * k * nb)) != VB_OK) return st;
+        if ((st = upload(ctx, dr, occ_right, sizeof(int) * k * nb)) != VB_OK) return st;
+        if ((st = upload(ctx, dS, S, sizeof(double) * n * n)) != VB_OK) return st;
+        if ((st = upload(ctx, dh, h, sizeof(double) * n * n)) != VB_OK) return st;
+        if ((st = upload(ctx, de, eri, sizeof(double) * np * (np + 1) / 2)) != VB_OK) return st;
+        if ((st = dsc.allocate(ctx, sizeof(double) * 4 * nb)) != VB_OK) return st;
+        if (cofactor_out && (st = dc.allocate(ctx, sizeof(double) * kk * nb)) != VB_OK) return st;
+        l = dl.as<int>();
+        r = dr.as<int>();
+        pS = dS.as<double>();
+        ph = dh.as<double>();
+        pe = de.as<double>();
+        sc = dsc.as<double>();
+        cof = cofactor_out ? dc.as<double>() : nullptr;
+    }
+    cudaError_t err = launch_same_spin_list(n, k, batch, l, r, pS, ph, pe, sc, cof, s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "same_spin_list");
+    if (mem == VB_MEM_HOST && batch > 0) {
+        err = cudaMemcpyAsync(out_scalars, sc, sizeof(double) * 4 * batch, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess && cofactor_out)
+            err = cudaMemcpyAsync(cofactor_out, cof, sizeof(double) * kk * batch, cudaMemcpyDeviceToHost, s);
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "same-spin download");
+    return VB_OK;
+}
+
+}  // extern "C"

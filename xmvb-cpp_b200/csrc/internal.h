@@ -1,0 +1,105 @@
+// Internal declarations shared by the vbcore host and device translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "vbcore.h"
+
+struct vb_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    size_t budget = 0;
+    size_t current = 0;
+    size_t peak = 0;
+    std::string last_error;
+};
+
+namespace vbcore {
+
+// Linear-dependence threshold of the reference overlap resolver
+// (src/vbscf/determinants/algebra/overlap.hpp:166).
+constexpr double kLinearDependenceThreshold = 1.0e-12;
+
+// Largest electron count per spin handled by the register-resident kernels; larger blocks
+// run on the local-memory exact path only.
+constexpr int kMaxFastElectrons = 8;
+// Largest electron count per spin supported at all, and largest active space.
+constexpr int kMaxElectrons = 16;
+constexpr int kMaxOrbitals = 64;
+
+vb_status set_error(vb_context* ctx, vb_status code, const std::string& message);
+vb_status cuda_error(vb_context* ctx, cudaError_t err, const char* what);
+
+// Budgeted device allocation; returns nullptr (and records VB_ERR_BUDGET / VB_ERR_CUDA) on failure.
+void* device_alloc(vb_context* ctx, size_t bytes, vb_status* status);
+void device_free(vb_context* ctx, void* ptr, size_t bytes);
+
+// RAII device buffer tied to a context.
+struct DeviceBuffer {
+    vb_context* ctx = nullptr;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ctx(o.ctx), ptr(o.ptr), bytes(o.bytes) {
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        if (this != &o) {
+            release();
+            ctx = o.ctx;
+            ptr = o.ptr;
+            bytes = o.bytes;
+            o.ptr = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DeviceBuffer() { release(); }
+    vb_status allocate(vb_context* c, size_t n) {
+        release();
+        ctx = c;
+        vb_status st = VB_OK;
+        if (n == 0) n = 16;
+        ptr = device_alloc(c, n, &st);
+        if (ptr) bytes = n;
+        return st;
+    }
+    void release() {
+        if (ptr) device_free(ctx, ptr, bytes);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+// Host-side structure generation and expansion (structures.cpp).
+struct Expansion {
+    int n_structures = 0;
+    int n_alpha = 0;
+    int n_beta = 0;
+    std::vector<uint64_t> alpha_strings;
+    std::vector<uint64_t> beta_strings;
+    std::vector<int32_t> det_alpha;
+    std::vector<int32_t> det_beta;
+    std::vector<int64_t> offsets;
+    std::vector<int32_t> term_structure;
+    std::vector<double> term_coefficient;
+};
+
+std::vector<std::vector<int>> generate_structures(const std::string& keyword, int n_orb, int n_el, int mult,
+                                                  int n_inactive);
+Expansion expand_structures(const std::vector<std::vector<int>>& rows, int n_el_active, int mult,
+                            int n_inactive);
+
+}  // namespace vbcore

@@ -1,0 +1,351 @@
+"""Python host mirror of the vbcore C ABI (include/vbcore.h).
+
+The names follow the reference's (Tao-Xia/xmvb-cpp) interfaces for the determinant-pair
+path: structure generation (``build_generated_raw_structures_from_structure_class``),
+expansion (``StructureExpander::expand``), the structure H/S builder
+(``FullDeterminantStructureHamiltonianOverlapBuilder::build``), overlap resolution
+(``DeterminantOverlapResolver::resolve_matrix``) and same-spin pair evaluation
+(``DeterminantPairEvaluator::evaluate_same_spin_pair``).  Errors raise ``VbError`` with the
+library's message, as the reference raises ``std::invalid_argument`` / ``std::runtime_error``.
+
+The numerical entry points run CUDA kernels only; there is no CPU path.  Loading the library
+needs no GPU (structure generation and expansion are host work), but creating a ``Context``
+on a machine without an sm_100 device raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_DIR, "lib", "libvbcore.so")
+
+VB_MEM_HOST = 0
+VB_MEM_DEVICE = 1
+
+_STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "HBM budget exceeded", 4: "numerical failure",
+           5: "unsupported", 6: "timeout"}
+
+
+class VbError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"vbcore {_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class _ExpansionSizes(ctypes.Structure):
+    _fields_ = [("n_structures", ctypes.c_int32), ("n_alpha_electrons", ctypes.c_int32),
+                ("n_beta_electrons", ctypes.c_int32), ("n_alpha_strings", ctypes.c_int32),
+                ("n_beta_strings", ctypes.c_int32), ("n_determinants", ctypes.c_int64),
+                ("n_terms", ctypes.c_int64)]
+
+
+class _Expansion(ctypes.Structure):
+    _fields_ = [("n_orbitals", ctypes.c_int32), ("n_alpha_electrons", ctypes.c_int32),
+                ("n_beta_electrons", ctypes.c_int32), ("n_alpha_strings", ctypes.c_int32),
+                ("n_beta_strings", ctypes.c_int32), ("alpha_strings", ctypes.c_void_p),
+                ("beta_strings", ctypes.c_void_p), ("n_determinants", ctypes.c_int64),
+                ("det_alpha", ctypes.c_void_p), ("det_beta", ctypes.c_void_p), ("n_structures", ctypes.c_int32),
+                ("term_offsets", ctypes.c_void_p), ("term_structure", ctypes.c_void_p),
+                ("term_coefficient", ctypes.c_void_p)]
+
+
+class _HsStats(ctypes.Structure):
+    _fields_ = [("spin_pairs", ctypes.c_int64), ("careful_spin_pairs", ctypes.c_int64),
+                ("determinant_pairs", ctypes.c_int64), ("kernel_launches", ctypes.c_int64)]
+
+
+# every symbol include/vbcore.h declares
+EXPORTED_SYMBOLS = (
+    "vb_context_create", "vb_context_destroy", "vb_context_set_stream", "vb_context_synchronize", "vb_last_error",
+    "vb_context_memory", "vb_generate_structures", "vb_expand_structures", "vb_hs_plan_create",
+    "vb_hs_plan_destroy", "vb_hs_plan_execute", "vb_hs_plan_stats", "vb_resolve_overlaps", "vb_same_spin_pairs",
+    "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
+)
+
+PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libvbcore.so (raises when the extension has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise VbError(2, f"native library missing: {path} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    c = ctypes
+    P = c.c_void_p
+    lib.vb_context_create.argtypes = [c.c_int, c.c_size_t, c.POINTER(P)]
+    lib.vb_context_destroy.argtypes = [P]
+    lib.vb_context_set_stream.argtypes = [P, P]
+    lib.vb_context_synchronize.argtypes = [P]
+    lib.vb_last_error.argtypes = [P]
+    lib.vb_last_error.restype = c.c_char_p
+    lib.vb_context_memory.argtypes = [P, c.POINTER(c.c_size_t), c.POINTER(c.c_size_t)]
+    lib.vb_generate_structures.argtypes = [c.c_char_p, c.c_int, c.c_int, c.c_int, c.c_int, c.POINTER(c.c_int64), P,
+                                           c.c_int64]
+    lib.vb_expand_structures.argtypes = [P, c.c_int64, c.c_int, c.c_int, c.c_int, c.POINTER(_ExpansionSizes)] + [P] * 7
+    lib.vb_hs_plan_create.argtypes = [P, c.POINTER(_Expansion), c.POINTER(P)]
+    lib.vb_hs_plan_destroy.argtypes = [P]
+    lib.vb_hs_plan_execute.argtypes = [P, P, P, P, c.c_int, P, P]
+    lib.vb_hs_plan_stats.argtypes = [P, c.POINTER(_HsStats)]
+    lib.vb_hs_plan_determinant_pairs.argtypes = [P, P, P, P, c.c_int64, P, c.c_int, P, P]
+    lib.vb_hs_plan_enable_phase_timing.argtypes = [P, c.c_int]
+    lib.vb_hs_plan_phase_times.argtypes = [P, P, c.c_int]
+    lib.vb_resolve_overlaps.argtypes = [P, c.c_int, c.c_int64, P, c.c_int, P, P, P]
+    lib.vb_same_spin_pairs.argtypes = [P, c.c_int, c.c_int, c.c_int64, P, P, P, P, P, c.c_int, P, P]
+    for name in EXPORTED_SYMBOLS:
+        fn = getattr(lib, name)
+        if name != "vb_last_error" and fn.restype is not c.c_char_p:
+            fn.restype = c.c_int
+    _lib = lib
+    return lib
+
+
+def _check(status: int, ctx_handle=None):
+    if status != 0:
+        msg = load_library().vb_last_error(ctx_handle)
+        raise VbError(status, msg.decode() if msg else "")
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+# ---------------------------------------------------------------------------------------------
+# host-side structure setup (no GPU needed)
+
+
+def generate_structures(keyword: str, n_active_orbitals: int, n_active_electrons: int,
+                        spin_multiplicity: int = 1, n_inactive: int = 0) -> np.ndarray:
+    """Raw structures, one row per structure of 1-based orbital labels (reference row layout)."""
+    lib = load_library()
+    n = ctypes.c_int64()
+    _check(lib.vb_generate_structures(keyword.encode(), n_active_orbitals, n_active_electrons, spin_multiplicity,
+                                      n_inactive, ctypes.byref(n), None, 0))
+    width = n_active_electrons + 2 * n_inactive
+    rows = np.zeros((n.value, width), dtype=np.int32)
+    _check(lib.vb_generate_structures(keyword.encode(), n_active_orbitals, n_active_electrons, spin_multiplicity,
+                                      n_inactive, ctypes.byref(n), _ptr(rows), rows.size))
+    return rows
+
+
+@dataclass
+class Expansion:
+    """Structure -> determinant expansion (StructureExpansion of the reference)."""
+    n_structures: int
+    n_alpha_electrons: int
+    n_beta_electrons: int
+    alpha_strings: np.ndarray  # uint64 occupation masks, ascending
+    beta_strings: np.ndarray
+    det_alpha: np.ndarray  # int32 string index per determinant
+    det_beta: np.ndarray
+    term_offsets: np.ndarray  # int64 CSR by determinant
+    term_structure: np.ndarray  # int32
+    term_coefficient: np.ndarray  # float64
+
+    @property
+    def n_determinants(self) -> int:
+        return len(self.det_alpha)
+
+    def occupations(self, beta: bool = False) -> np.ndarray:
+        strings = self.beta_strings if beta else self.alpha_strings
+        ids = self.det_beta if beta else self.det_alpha
+        k = self.n_beta_electrons if beta else self.n_alpha_electrons
+        occ = np.zeros((len(ids), k), dtype=np.int32)
+        for d, s in enumerate(ids):
+            m = int(strings[s])
+            occ[d] = [i for i in range(64) if (m >> i) & 1]
+        return occ
+
+
+def expand_structures(rows: np.ndarray, n_active_electrons: int, spin_multiplicity: int = 1,
+                      n_inactive: int = 0) -> Expansion:
+    lib = load_library()
+    rows = _c(rows, np.int32)
+    sizes = _ExpansionSizes()
+    _check(lib.vb_expand_structures(_ptr(rows), rows.shape[0], n_active_electrons, spin_multiplicity, n_inactive,
+                                    ctypes.byref(sizes), None, None, None, None, None, None, None))
+    a = np.zeros(sizes.n_alpha_strings, dtype=np.uint64)
+    b = np.zeros(sizes.n_beta_strings, dtype=np.uint64)
+    da = np.zeros(sizes.n_determinants, dtype=np.int32)
+    db = np.zeros(sizes.n_determinants, dtype=np.int32)
+    off = np.zeros(sizes.n_determinants + 1, dtype=np.int64)
+    ts = np.zeros(sizes.n_terms, dtype=np.int32)
+    tc = np.zeros(sizes.n_terms, dtype=np.float64)
+    _check(lib.vb_expand_structures(_ptr(rows), rows.shape[0], n_active_electrons, spin_multiplicity, n_inactive,
+                                    ctypes.byref(sizes), _ptr(a), _ptr(b), _ptr(da), _ptr(db), _ptr(off), _ptr(ts),
+                                    _ptr(tc)))
+    return Expansion(sizes.n_structures, sizes.n_alpha_electrons, sizes.n_beta_electrons, a, b, da, db, off, ts, tc)
+
+
+# ---------------------------------------------------------------------------------------------
+# device context and the H/S plan
+
+
+class Context:
+    """One device, one stream, an HBM budget (xmvb::cuda::Context of the reference)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.vb_context_create(device, hbm_budget_bytes, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_handle: int | None):
+        _check(load_library().vb_context_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)), self._h)
+
+    def synchronize(self):
+        _check(load_library().vb_context_synchronize(self._h), self._h)
+
+    def memory(self):
+        cur, peak = ctypes.c_size_t(), ctypes.c_size_t()
+        _check(load_library().vb_context_memory(self._h, ctypes.byref(cur), ctypes.byref(peak)), self._h)
+        return cur.value, peak.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().vb_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- determinant-pair level entry points ---------------------------------------------------
+
+    def resolve_overlaps(self, blocks: np.ndarray):
+        """blocks: (batch, k, k) -> (det, nullity, cofactor (batch, k, k)), reference semantics."""
+        blocks = np.asarray(blocks, dtype=np.float64)
+        batch, k, _ = blocks.shape
+        colmajor = _c(np.transpose(blocks, (0, 2, 1)), np.float64)
+        det = np.zeros(batch)
+        nul = np.zeros(batch, dtype=np.int32)
+        cof = np.zeros((batch, k, k))
+        _check(load_library().vb_resolve_overlaps(self._h, k, batch, _ptr(colmajor), VB_MEM_HOST, _ptr(det), _ptr(nul),
+                                                  _ptr(cof)), self._h)
+        return det, nul, np.transpose(cof, (0, 2, 1)).copy()
+
+    def same_spin_pairs(self, n_orbitals, occ_left, occ_right, S, h, eri):
+        """Explicit same-spin pairs -> (scalars (batch, 4) = det, h1, htot, nullity; cofactors)."""
+        occ_left = _c(occ_left, np.int32)
+        occ_right = _c(occ_right, np.int32)
+        batch, k = occ_left.shape
+        sc = np.zeros((batch, 4))
+        cof = np.zeros((batch, k, k))
+        Sf = _c(np.asarray(S).T, np.float64)
+        hf = _c(np.asarray(h).T, np.float64)
+        ef = _c(eri, np.float64)
+        _check(load_library().vb_same_spin_pairs(self._h, n_orbitals, k, batch, _ptr(occ_left), _ptr(occ_right),
+                                                 _ptr(Sf), _ptr(hf), _ptr(ef), VB_MEM_HOST, _ptr(sc), _ptr(cof)),
+               self._h)
+        return sc, np.transpose(cof, (0, 2, 1)).copy()
+
+
+class HsPlan:
+    """Structure Hamiltonian/overlap builder with the topology resident on the device."""
+
+    def __init__(self, ctx: Context, expansion: Expansion, n_orbitals: int):
+        self.ctx = ctx
+        self.expansion = expansion
+        self.n_orbitals = n_orbitals
+        e = expansion
+        self._keep = [_c(e.alpha_strings, np.uint64), _c(e.beta_strings, np.uint64), _c(e.det_alpha, np.int32),
+                      _c(e.det_beta, np.int32), _c(e.term_offsets, np.int64), _c(e.term_structure, np.int32),
+                      _c(e.term_coefficient, np.float64)]
+        a, b, da, db, off, ts, tc = self._keep
+        desc = _Expansion(n_orbitals, e.n_alpha_electrons, e.n_beta_electrons, len(a), len(b), _ptr(a).value,
+                          _ptr(b).value, len(da), _ptr(da).value, _ptr(db).value, e.n_structures, _ptr(off).value,
+                          _ptr(ts).value, _ptr(tc).value)
+        h = ctypes.c_void_p()
+        _check(load_library().vb_hs_plan_create(ctx.handle, ctypes.byref(desc), ctypes.byref(h)), ctx.handle)
+        self._h = h
+        self.n_structures = e.n_structures
+
+    def execute(self, S, h, eri):
+        """Host arrays in (S, h as n x n; eri packed), host H and S out."""
+        n = self.n_orbitals
+        Sf = _c(np.asarray(S).T, np.float64)
+        hf = _c(np.asarray(h).T, np.float64)
+        ef = _c(eri, np.float64)
+        if Sf.size != n * n or hf.size != n * n:
+            raise VbError(1, "S and h must be n_orbitals x n_orbitals")
+        np_ = n * (n + 1) // 2
+        if ef.size != np_ * (np_ + 1) // 2:
+            raise VbError(1, "eri must hold P(P+1)/2 packed values")
+        ns = self.n_structures
+        H = np.zeros((ns, ns))
+        So = np.zeros((ns, ns))
+        _check(load_library().vb_hs_plan_execute(self._h, _ptr(Sf), _ptr(hf), _ptr(ef), VB_MEM_HOST, _ptr(H), _ptr(So)),
+               self.ctx.handle)
+        return H.T.copy(), So.T.copy()
+
+    def execute_device(self, S_ptr: int, h_ptr: int, eri_ptr: int, H_ptr: int, S_out_ptr: int):
+        """Device pointers (column-major S/h; packed eri); stream-ordered, no synchronization."""
+        _check(load_library().vb_hs_plan_execute(self._h, ctypes.c_void_p(S_ptr), ctypes.c_void_p(h_ptr),
+                                                 ctypes.c_void_p(eri_ptr), VB_MEM_DEVICE, ctypes.c_void_p(H_ptr),
+                                                 ctypes.c_void_p(S_out_ptr)), self.ctx.handle)
+
+    def execute_host_pointers(self, S_ptr: int, h_ptr: int, eri_ptr: int, H_ptr: int, S_out_ptr: int):
+        """Host pointers (ideally pinned; column-major S/h; packed eri): copies in, evaluates,
+        copies H and S out, and returns when the results are on the host."""
+        _check(load_library().vb_hs_plan_execute(self._h, ctypes.c_void_p(S_ptr), ctypes.c_void_p(h_ptr),
+                                                 ctypes.c_void_p(eri_ptr), VB_MEM_HOST, ctypes.c_void_p(H_ptr),
+                                                 ctypes.c_void_p(S_out_ptr)), self.ctx.handle)
+
+    def determinant_pairs(self, S, h, eri, pairs):
+        """<d|H|e>, <d|e> for an (m, 2) array of determinant index pairs."""
+        pairs = _c(pairs, np.int64)
+        m = pairs.shape[0]
+        ho = np.zeros(m)
+        so = np.zeros(m)
+        Sf = _c(np.asarray(S).T, np.float64)
+        hf = _c(np.asarray(h).T, np.float64)
+        ef = _c(eri, np.float64)
+        _check(load_library().vb_hs_plan_determinant_pairs(self._h, _ptr(Sf), _ptr(hf), _ptr(ef), m, _ptr(pairs),
+                                                           VB_MEM_HOST, _ptr(ho), _ptr(so)), self.ctx.handle)
+        return ho, so
+
+    def stats(self) -> dict:
+        st = _HsStats()
+        _check(load_library().vb_hs_plan_stats(self._h, ctypes.byref(st)), self.ctx.handle)
+        return dict(spin_pairs=st.spin_pairs, careful_spin_pairs=st.careful_spin_pairs,
+                    determinant_pairs=st.determinant_pairs, kernel_launches=st.kernel_launches)
+
+    def enable_phase_timing(self, enable: bool = True):
+        _check(load_library().vb_hs_plan_enable_phase_timing(self._h, int(enable)), self.ctx.handle)
+
+    def phase_times(self) -> dict:
+        """Milliseconds per phase of the last execute (CUDA events on the context stream)."""
+        out = np.zeros(len(PHASES))
+        _check(load_library().vb_hs_plan_phase_times(self._h, _ptr(out), len(PHASES)), self.ctx.handle)
+        return dict(zip(PHASES, out.tolist()))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().vb_hs_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
