@@ -250,7 +250,8 @@ def run_vbcore(args):
     n_det, n_str = ex.n_determinants, ex.n_structures
     ordered = n_det * n_det
     S, h, eri = workloads.active_space(N_ACTIVE, N_AUX, SEED)
-    stream = torch.cuda.current_stream(device)
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
     dS = torch.tensor(np.ascontiguousarray(S.T), device=device)

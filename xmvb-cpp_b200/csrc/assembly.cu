@@ -17,8 +17,12 @@ namespace {
 
 constexpr int kPad = kBandReduceColumns + 1;
 
-// One CTA per 32 band columns; all rows of the band stream through once.  Warp w owns the
-// structures bucketed to it, so each shared-memory accumulator has exactly one writer.
+// One CTA per 32 band columns; every row of the band streams through once.  Warp w owns the
+// structures bucketed to it (local structure index = w mod warps), so each shared-memory
+// accumulator has exactly one writer and the sum order is fixed.  A warp walks its
+// (determinant, structure, coefficient) triples, sorted by determinant, 32 at a time: lane j
+// fetches triple j, then the warp broadcasts them one by one; the band loads of consecutive
+// triples are independent, which keeps many loads in flight.
 __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(BandReduceArgs a) {
     extern __shared__ double zsm[];
     double* zh = zsm;
@@ -34,22 +38,33 @@ __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(Band
     const long long e = a.e0 + j;
     long long row_end = a.e0 + (long long)blockIdx.x * kBandReduceColumns + kBandReduceColumns;
     if (row_end > a.e0 + a.width) row_end = a.e0 + a.width;
-    const long long* off = a.woff + (long long)warp * (a.n_det + 1);
-    for (long long d = 0; d < row_end; ++d) {
-        const long long t0 = __ldg(off + d), t1 = __ldg(off + d + 1);
-        if (t0 == t1) continue;
-        double hv = 0.0, sv = 0.0;
-        if (valid && d <= e) {
-            hv = __ldg(a.Hb + d * a.width + j);
-            sv = __ldg(a.Sb + d * a.width + j);
-            if (d == e) {
-                hv *= 0.5;
-                sv *= 0.5;
-            }
+    const long long t_begin = a.wbegin[warp], t_end = a.wbegin[warp + 1];
+    for (long long base = t_begin; base < t_end; base += 32) {
+        const long long mine = base + lane;
+        int d_l = 0x7fffffff, I_l = 0;
+        double c_l = 0.0;
+        if (mine < t_end) {
+            d_l = __ldg(a.wdet + mine);
+            I_l = __ldg(a.wstruct + mine);
+            c_l = __ldg(a.wcoef + mine);
         }
-        for (long long t = t0; t < t1; ++t) {
-            const int I = __ldg(a.wstruct + t) - a.struct_begin;
-            const double c = __ldg(a.wcoef + t);
+        const int first = __shfl_sync(0xffffffffu, d_l, 0);
+        if (first >= row_end) break;
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q) {
+            const int d = __shfl_sync(0xffffffffu, d_l, q);
+            const int I = __shfl_sync(0xffffffffu, I_l, q);
+            const double c = __shfl_sync(0xffffffffu, c_l, q);
+            if (d >= row_end) break;
+            double hv = 0.0, sv = 0.0;
+            if (valid && d <= e) {
+                hv = __ldg(a.Hb + (long long)d * a.width + j);
+                sv = __ldg(a.Sb + (long long)d * a.width + j);
+                if (d == e) {
+                    hv *= 0.5;
+                    sv *= 0.5;
+                }
+            }
             zh[I * kPad + lane] = fma(c, hv, zh[I * kPad + lane]);
             zs[I * kPad + lane] = fma(c, sv, zs[I * kPad + lane]);
         }

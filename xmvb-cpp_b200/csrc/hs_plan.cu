@@ -22,7 +22,7 @@ using namespace vbcore;
 
 struct StructureChunk {
     int begin = 0, count = 0;
-    DeviceBuffer woff, wstruct, wcoef;
+    DeviceBuffer wbegin, wdet, wstruct, wcoef;
 };
 
 struct vb_hs_plan {
@@ -36,8 +36,13 @@ struct vb_hs_plan {
     DeviceBuffer rec_a, rec_b;
     int stride_a = 0, stride_b = 0;
     long long npairs_a = 0, npairs_b = 0;
-    DeviceBuffer counters, list_a, list_b;
+    DeviceBuffer counters, list_a, list_b, items_a, items_b;
+    int n_items_a = 0, n_items_b = 0;
     DeviceBuffer S_in, h_in, eri_in, gamma, kfull;
+    // pair-kernel factorization: lf[q * np + m], scratch, signs, meta = {r_pos, r_neg} (+ host copy)
+    DeviceBuffer lf, fwork, fcols, fsigns, fmeta;
+    int* meta_host = nullptr;
+    int R = 0, r_pos = 0;
     DeviceBuffer band_h, band_s;
     long long band_width = 0;
     DeviceBuffer Zh, Zs, Wh, Ws, Hout, Sout;
@@ -50,6 +55,7 @@ struct vb_hs_plan {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[VB_PHASE_COUNT];
     int used[VB_PHASE_COUNT] = {0, 0, 0, 0, 0};
     ~vb_hs_plan() {
+        if (meta_host) cudaFreeHost(meta_host);
         for (auto& v : events)
             for (auto& e : v) {
                 cudaEventDestroy(e.first);
@@ -117,9 +123,17 @@ struct PhaseMark {
     ~PhaseMark() { close(); }
 };
 
-int record_stride(int k) {
-    int s = k * k + 4;
+int record_stride(int R) {
+    const int s = R + 4;
     return (s + 1) / 2 * 2;
+}
+
+// Work items of the fast spin-pair kernel: (left string u, first right string v0), v0 >= u.
+std::vector<int2> spin_items(int N) {
+    std::vector<int2> items;
+    for (int u = 0; u < N; ++u)
+        for (int v0 = u; v0 < N; v0 += kSpinBlock) items.push_back(make_int2(u, v0));
+    return items;
 }
 
 }  // namespace
@@ -192,17 +206,27 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     if ((st = upload(ctx, p->det_alpha, ex->det_alpha, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
     if ((st = upload(ctx, p->det_beta, ex->det_beta, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
 
-    // spin-pair records
-    p->stride_a = record_stride(p->ka);
-    p->stride_b = record_stride(p->kb);
+    // spin-pair records, sized for the largest factor rank (np columns)
+    const int max_stride = record_stride(p->np);
     p->npairs_a = (long long)p->Na * (p->Na + 1) / 2;
     p->npairs_b = p->shared_tables ? 0 : (long long)p->Nb * (p->Nb + 1) / 2;
-    if ((st = p->rec_a.allocate(ctx, sizeof(double) * p->stride_a * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
-    if ((st = p->list_a.allocate(ctx, sizeof(long long) * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
-    if (!p->shared_tables) {
-        if ((st = p->rec_b.allocate(ctx, sizeof(double) * p->stride_b * std::max(1LL, p->npairs_b))) != VB_OK)
+    if ((st = p->rec_a.allocate(ctx, sizeof(double) * max_stride * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
+    if ((st = p->list_a.allocate(ctx, sizeof(unsigned long long) * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
+    {
+        std::vector<int2> it = spin_items(p->Na);
+        p->n_items_a = (int)it.size();
+        if ((st = upload(ctx, p->items_a, it.data(), sizeof(int2) * std::max<size_t>(1, it.size()))) != VB_OK)
             return fail(st);
-        if ((st = p->list_b.allocate(ctx, sizeof(long long) * std::max(1LL, p->npairs_b))) != VB_OK) return fail(st);
+    }
+    if (!p->shared_tables) {
+        if ((st = p->rec_b.allocate(ctx, sizeof(double) * max_stride * std::max(1LL, p->npairs_b))) != VB_OK)
+            return fail(st);
+        if ((st = p->list_b.allocate(ctx, sizeof(unsigned long long) * std::max(1LL, p->npairs_b))) != VB_OK)
+            return fail(st);
+        std::vector<int2> it = spin_items(p->Nb);
+        p->n_items_b = (int)it.size();
+        if ((st = upload(ctx, p->items_b, it.data(), sizeof(int2) * std::max<size_t>(1, it.size()))) != VB_OK)
+            return fail(st);
     }
     if ((st = p->counters.allocate(ctx, 4 * sizeof(unsigned long long))) != VB_OK) return fail(st);
 
@@ -212,6 +236,11 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     if ((st = p->eri_in.allocate(ctx, sizeof(double) * (size_t)p->np * (p->np + 1) / 2)) != VB_OK) return fail(st);
     if ((st = p->gamma.allocate(ctx, sizeof(double) * std::max(1, p->gd * p->gd))) != VB_OK) return fail(st);
     if ((st = p->kfull.allocate(ctx, sizeof(double) * p->np * p->np)) != VB_OK) return fail(st);
+    for (DeviceBuffer* b : {&p->lf, &p->fwork, &p->fcols})
+        if ((st = b->allocate(ctx, sizeof(double) * p->np * p->np)) != VB_OK) return fail(st);
+    if ((st = p->fsigns.allocate(ctx, sizeof(int) * p->np)) != VB_OK) return fail(st);
+    if ((st = p->fmeta.allocate(ctx, sizeof(int) * 2)) != VB_OK) return fail(st);
+    if (cudaMallocHost(&p->meta_host, sizeof(int) * 2) != cudaSuccess) return fail(set_error(ctx, VB_ERR_CUDA, "cudaMallocHost"));
 
     // band of determinant columns: keep the two band buffers within ~4 GB and 1/4 of the budget
     const size_t band_cap = std::min<size_t>((size_t)4 << 30, ctx->budget / 4);
@@ -245,30 +274,32 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     if ((st = upload(ctx, p->str_coef, scoef.data(), sizeof(double) * std::max<size_t>(1, scoef.size()))) != VB_OK)
         return fail(st);
 
-    // per structure chunk: determinant-major term lists bucketed by (structure - begin) mod warps
+    // per structure chunk and warp bucket ((structure - begin) mod warps): triples
+    // (determinant, local structure, coefficient) sorted by determinant
     const int max_chunk = band_reduce_max_structures();
     for (int begin = 0; begin < p->n_str; begin += max_chunk) {
         StructureChunk ch;
         ch.begin = begin;
         ch.count = std::min(max_chunk, p->n_str - begin);
-        std::vector<long long> woff((size_t)kBandReduceWarps * (p->n_det + 1), 0);
-        std::vector<int> wstruct;
+        std::vector<long long> wbegin(kBandReduceWarps + 1, 0);
+        std::vector<int> wdet, wstruct;
         std::vector<double> wcoef;
         for (int w = 0; w < kBandReduceWarps; ++w) {
-            long long* o = woff.data() + (size_t)w * (p->n_det + 1);
-            o[0] = (long long)wstruct.size();
-            for (long long d = 0; d < p->n_det; ++d) {
+            wbegin[w] = (long long)wdet.size();
+            for (long long d = 0; d < p->n_det; ++d)
                 for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t) {
                     const int I = ex->term_structure[t];
                     if (I >= begin && I < begin + ch.count && (I - begin) % kBandReduceWarps == w) {
-                        wstruct.push_back(I);
+                        wdet.push_back((int)d);
+                        wstruct.push_back(I - begin);
                         wcoef.push_back(ex->term_coefficient[t]);
                     }
                 }
-                o[d + 1] = (long long)wstruct.size();
-            }
         }
-        if ((st = upload(ctx, ch.woff, woff.data(), sizeof(long long) * woff.size())) != VB_OK) return fail(st);
+        wbegin[kBandReduceWarps] = (long long)wdet.size();
+        if ((st = upload(ctx, ch.wbegin, wbegin.data(), sizeof(long long) * wbegin.size())) != VB_OK) return fail(st);
+        if ((st = upload(ctx, ch.wdet, wdet.data(), sizeof(int) * std::max<size_t>(1, wdet.size()))) != VB_OK)
+            return fail(st);
         if ((st = upload(ctx, ch.wstruct, wstruct.data(), sizeof(int) * std::max<size_t>(1, wstruct.size()))) != VB_OK)
             return fail(st);
         if ((st = upload(ctx, ch.wcoef, wcoef.data(), sizeof(double) * std::max<size_t>(1, wcoef.size()))) != VB_OK)
@@ -304,30 +335,36 @@ SpinTableArgs table_args(vb_hs_plan* p, bool beta, const double* S, const double
     a.gamma = p->gamma.as<double>();
     a.eri = eri;
     a.gamma_dim = p->gd;
+    a.lf = p->lf.as<double>();
+    a.ld = p->np;
+    a.R = p->R;
+    const int chunks = (p->R + kFactorChunk - 1) / kFactorChunk;
+    a.Rs = std::max(1, chunks * kFactorChunk) | 1;
     a.records = beta ? p->rec_b.as<double>() : p->rec_a.as<double>();
-    a.rec_stride = beta ? p->stride_b : p->stride_a;
+    a.rec_stride = record_stride(p->R);
     a.careful_count = p->counters.as<unsigned long long>() + (beta ? 1 : 0);
-    a.careful_list = beta ? p->list_b.as<long long>() : p->list_a.as<long long>();
+    a.careful_list = beta ? p->list_b.as<unsigned long long>() : p->list_a.as<unsigned long long>();
+    a.items = beta ? p->items_b.as<int2>() : p->items_a.as<int2>();
+    a.n_items = beta ? p->n_items_b : p->n_items_a;
     a.all_careful = 0;
     return a;
 }
 
 FullPairArgs full_args(vb_hs_plan* p) {
     FullPairArgs a{};
-    a.n = p->n;
     a.ka = p->ka;
     a.kb = p->kb;
-    a.np = p->np;
     a.n_det = p->n_det;
     a.det_alpha = p->det_alpha.as<int>();
     a.det_beta = p->det_beta.as<int>();
-    a.occ_a = p->occ_a.as<uint64_t>();
-    a.occ_b = p->shared_tables ? p->occ_a.as<uint64_t>() : p->occ_b.as<uint64_t>();
+    a.Na = p->Na;
+    a.Nb = p->shared_tables ? p->Na : p->Nb;
     a.rec_a = p->rec_a.as<double>();
     a.rec_b = p->shared_tables ? p->rec_a.as<double>() : p->rec_b.as<double>();
-    a.stride_a = p->stride_a;
-    a.stride_b = p->stride_b;
-    a.kfull = p->kfull.as<double>();
+    a.stride_a = record_stride(p->R);
+    a.stride_b = record_stride(p->R);
+    a.R = p->R;
+    a.r_pos = p->r_pos;
     return a;
 }
 
@@ -356,6 +393,16 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
     cudaError_t err = launch_prepare_tables(p->n, *deri, p->gamma.as<double>(), p->kfull.as<double>(), s);
     if (err != cudaSuccess) return cuda_error(ctx, err, "prepare_tables");
     ++*launches;
+    err = launch_factor_pair_kernel(p->np, p->kfull.as<double>(), p->fwork.as<double>(), p->fcols.as<double>(),
+                                    p->fsigns.as<int>(), p->lf.as<double>(), p->np, p->fmeta.as<int>(), s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "factor_pair_kernel");
+    ++*launches;
+    // the factor rank sizes the spin-pair launch: one 8-byte read-back per evaluation
+    err = cudaMemcpyAsync(p->meta_host, p->fmeta.ptr, sizeof(int) * 2, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "factor rank read-back");
+    p->r_pos = p->meta_host[0];
+    p->R = p->meta_host[0] + p->meta_host[1];
     tables.close();
     PhaseMark spin(p, VB_PHASE_SPIN_PAIRS);
     err = cudaMemsetAsync(p->counters.ptr, 0, 4 * sizeof(unsigned long long), s);
@@ -409,7 +456,8 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
             ba.width = B;
             ba.Hb = fa.Hb;
             ba.Sb = fa.Sb;
-            ba.woff = ch.woff.as<long long>();
+            ba.wbegin = ch.wbegin.as<long long>();
+            ba.wdet = ch.wdet.as<int>();
             ba.wstruct = ch.wstruct.as<int>();
             ba.wcoef = ch.wcoef.as<double>();
             ba.struct_begin = ch.begin;
@@ -483,8 +531,13 @@ vb_status vb_hs_plan_stats(const vb_hs_plan* p, vb_hs_stats* stats) {
         cudaError_t err = cudaMemcpyAsync(c, p->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, p->ctx->stream);
         if (err == cudaSuccess) err = cudaStreamSynchronize(p->ctx->stream);
         if (err != cudaSuccess) return cuda_error(p->ctx, err, "stats download");
-        const bool all_a = p->ka > vbcore::kMaxFastElectrons;
-        const bool all_b = p->kb > vbcore::kMaxFastElectrons;
+        auto all_exact = [&](int k) {
+            const int chunks = (p->R + kFactorChunk - 1) / kFactorChunk;
+            const int Rs = std::max(1, chunks * kFactorChunk) | 1;
+            return k > vbcore::kMaxFastElectrons || factored_spin_smem_bytes(p->n, k, Rs) > 227 * 1024;
+        };
+        const bool all_a = p->ka > 0 && all_exact(p->ka);
+        const bool all_b = p->kb > 0 && !p->shared_tables && all_exact(p->kb);
         s.careful_spin_pairs = (long long)(all_a ? p->npairs_a : c[0]) + (long long)(all_b ? p->npairs_b : c[1]);
     }
     *stats = s;

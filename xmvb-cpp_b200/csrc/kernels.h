@@ -7,11 +7,16 @@
 
 namespace vbcore {
 
-// One spin-string table and its unordered spin-pair records.
-// Record of pair (u <= v), left = string u, right = string v, stride rec_stride doubles:
-//   [r * k + c] first-order cofactor A(r, c) (rows = right), r, c < k (zero for nullity >= 2)
-//   [k*k + 0] overlap determinant, [+1] same-spin H (1e + 2e), [+2] one-electron part,
-//   [+3] nullity.
+// Opposite-spin factorization of the pair kernel: K[p][q] = (p|q) over packed orbital pairs is
+// written K = sum_m sigma_m l_m l_m^T (pivoted LDL^T, sigma = +1 for the first r_pos columns,
+// -1 for the next r_neg), so the opposite-spin energy of a determinant pair
+// sum A_a(r,c) A_b(r',c') (R_r L_c | R'_r' L'_c') becomes sum_m sigma_m u_a[m] u_b[m] with
+// u[m] = sum_{r,c} A(r,c) l_m[pair(R_r, L_c)] computed once per spin pair.
+//
+// Spin-pair record of the unordered pair (u <= v) of one string table, left = string u, right =
+// string v, at index u N - u (u - 1) / 2 + (v - u), stride rec_stride doubles:
+//   [m] u-vector (m < R), [R + 0] overlap determinant, [R + 1] same-spin H (1e + 2e),
+//   [R + 2] one-electron part, [R + 3] nullity.
 struct SpinTableArgs {
     int n;          // active orbitals
     int k;          // electrons of this spin
@@ -20,28 +25,32 @@ struct SpinTableArgs {
     long long n_pairs;    // N (N + 1) / 2
     const double* S;      // n x n active overlap
     const double* h;      // n x n one-electron integrals
-    const double* gamma;  // gd x gd antisymmetrized two-electron table (k >= 2)
+    const double* gamma;  // gd x gd antisymmetrized table: gamma[rp * gd + cp] = (ij|kl) - (il|kj)
     const double* eri;    // packed (ij|kl)
     int gamma_dim;        // n (n - 1) / 2
+    const double* lf;     // pair-kernel factor, lf[q * ld + m]
+    int ld;               // leading dimension of lf (>= R)
+    int R;                // number of factor columns
+    int Rs;               // shared-memory row stride (odd, >= chunks * 21)
     double* records;
     int rec_stride;
     unsigned long long* careful_count;
-    long long* careful_list;
-    int all_careful;  // 1: every pair takes the exact path (list is implicit 0..n_pairs-1)
+    unsigned long long* careful_list;  // (u << 32) | v
+    const int2* items;                 // fast-kernel work items: (left string u, first right string v0)
+    int n_items;
+    int all_careful;  // 1: every pair takes the exact path
 };
 
 struct FullPairArgs {
-    int n, ka, kb, np;  // np = n (n + 1) / 2
+    int ka, kb;
     long long n_det;
     const int* det_alpha;
     const int* det_beta;
-    const uint64_t* occ_a;
-    const uint64_t* occ_b;
+    int Na, Nb;  // strings per table
     const double* rec_a;
     const double* rec_b;
     int stride_a, stride_b;
-    const double* kfull;  // np x np unpacked pair kernel
-    int kfull_in_smem;
+    int R, r_pos;         // factor columns, positive-sign columns
     long long e0, e1;     // band columns [e0, e1)
     long long n_items;    // determinant pairs (d <= e) in the band
     double* Hb;           // band, row-major: Hb[d * (e1 - e0) + (e - e0)], valid for d <= e
@@ -54,7 +63,8 @@ struct BandReduceArgs {
     long long e0, width;      // band columns
     const double* Hb;
     const double* Sb;
-    const long long* woff;    // per (warp bucket, determinant) CSR offsets of this structure chunk
+    const long long* wbegin;  // per warp bucket: triple range [wbegin[w], wbegin[w + 1])
+    const int* wdet;          // triples sorted by determinant: (determinant, local structure, coef)
     const int* wstruct;
     const double* wcoef;
     int struct_begin, struct_count;
@@ -76,8 +86,13 @@ struct StructureReduceArgs {
 
 constexpr int kBandReduceWarps = 8;
 constexpr int kBandReduceColumns = 32;
+constexpr int kFactorChunk = 21;   // u-vector entries accumulated per pass
+constexpr int kSpinBlock = 128;    // right strings per fast-kernel item (threads per CTA)
 
 cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, double* kfull, cudaStream_t stream);
+cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs,
+                                      double* lf, int ld, int* meta, cudaStream_t stream);
+size_t factored_spin_smem_bytes(int n, int k, int Rs);
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, cudaStream_t stream, int* launches);
 cudaError_t launch_full_pairs(const FullPairArgs& a, cudaStream_t stream, int* launches);
 cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches);

@@ -29,19 +29,12 @@ namespace {
 
 constexpr double kThreshold = 1.0e-12;
 constexpr double kCertificate2 = 1.0e18;  // (1e9)^2 on ||X||_F^2 ||X^-1||_F^2
+constexpr double kFactorTolerance = 1.0e-15;  // relative pivot cut of the pair-kernel factorization
 constexpr int kSms = 148;
 
 __device__ __forceinline__ int occ_byte(const uint64_t* row, int i) {
     const uint64_t w = row[i >> 3];
     return (int)((w >> (8 * (i & 7))) & 0xFFu);
-}
-
-__device__ __forceinline__ void decode_upper(long long t, long long* u, long long* v) {
-    long long vv = (long long)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while (vv * (vv + 1) / 2 > t) --vv;
-    while ((vv + 1) * (vv + 2) / 2 <= t) ++vv;
-    *v = vv;
-    *u = t - vv * (vv + 1) / 2;
 }
 
 __global__ void prepare_tables_kernel(int n, const double* __restrict__ eri, double* __restrict__ gamma,
@@ -73,41 +66,204 @@ __global__ void prepare_tables_kernel(int n, const double* __restrict__ eri, dou
     }
 }
 
+// Pivoted LDL^T of the unpacked pair kernel with diagonal (complete) pivoting, one CTA.
+// Stops when the largest remaining |diagonal| falls to rel_tol times the largest initial one;
+// the dropped remainder then perturbs any opposite-spin energy by at most
+// rel_tol * max|K_pp| * ||p_a||_1 ||p_b||_1.  Columns are emitted positive-sign first.
+__global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* __restrict__ kfull,
+                                                          double* __restrict__ work, double* __restrict__ cols,
+                                                          int* __restrict__ signs, double* __restrict__ lf, int ld,
+                                                          int* __restrict__ meta, double rel_tol) {
+    extern __shared__ unsigned char fsm[];
+    int* used = reinterpret_cast<int*>(fsm);
+    __shared__ double red_v[32];
+    __shared__ int red_i[32];
+    __shared__ double s_piv;
+    __shared__ int s_p;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long n2 = (long long)np * np;
+    for (long long i = tid; i < n2; i += nt) work[i] = kfull[i];
+    for (int i = tid; i < np; i += nt) used[i] = 0;
+    __syncthreads();
+    // largest initial |diagonal|
+    double local = 0.0;
+    for (int i = tid; i < np; i += nt) local = fmax(local, fabs(work[(long long)i * np + i]));
+    for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(0xffffffffu, local, o));
+    if ((tid & 31) == 0) red_v[tid >> 5] = local;
+    __syncthreads();
+    if (tid < 32) {
+        double v = tid < (nt >> 5) ? red_v[tid] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (tid == 0) s_piv = v;
+    }
+    __syncthreads();
+    const double cut = rel_tol * s_piv;
+    int m = 0;
+    for (; m < np; ++m) {
+        double best = -1.0;
+        int bi = -1;
+        for (int i = tid; i < np; i += nt)
+            if (!used[i]) {
+                const double v = fabs(work[(long long)i * np + i]);
+                if (v > best || (v == best && i < bi)) {
+                    best = v;
+                    bi = i;
+                }
+            }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi >= 0 && (bi < 0 || oi < bi))) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if ((tid & 31) == 0) {
+            red_v[tid >> 5] = best;
+            red_i[tid >> 5] = bi;
+        }
+        __syncthreads();
+        if (tid < 32) {
+            double v = tid < (nt >> 5) ? red_v[tid] : -1.0;
+            int vi = tid < (nt >> 5) ? red_i[tid] : -1;
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, vi, o);
+                if (ov > v || (ov == v && oi >= 0 && (vi < 0 || oi < vi))) {
+                    v = ov;
+                    vi = oi;
+                }
+            }
+            if (tid == 0) {
+                s_p = vi;
+                s_piv = vi >= 0 ? work[(long long)vi * np + vi] : 0.0;
+            }
+        }
+        __syncthreads();
+        const int p = s_p;
+        const double piv = s_piv;
+        if (p < 0 || !(fabs(piv) > cut) || fabs(piv) == 0.0) break;
+        const double inv = 1.0 / sqrt(fabs(piv));
+        const int sgn = piv > 0.0 ? 1 : -1;
+        for (int i = tid; i < np; i += nt) cols[(long long)m * np + i] = used[i] ? 0.0 : work[(long long)i * np + p] * inv;
+        if (tid == 0) signs[m] = sgn;
+        __syncthreads();
+        if (tid == 0) used[p] = 1;
+        __syncthreads();
+        const double* l = cols + (long long)m * np;
+        for (long long idx = tid; idx < n2; idx += nt) {
+            const int i = (int)(idx / np), j = (int)(idx % np);
+            if (!used[i] && !used[j]) work[idx] -= (double)sgn * l[i] * l[j];
+        }
+        __syncthreads();
+    }
+    // emit: positive-sign columns first, then negative, zero padding up to ld
+    int pos = 0;
+    for (int c = 0; c < m; ++c) pos += signs[c] > 0 ? 1 : 0;
+    for (long long idx = tid; idx < (long long)np * ld; idx += nt) {
+        const int q = (int)(idx / ld), slot = (int)(idx % ld);
+        double v = 0.0;
+        if (slot < m) {
+            // find the column that lands in `slot`
+            int c = -1, seen_pos = 0, seen_neg = 0;
+            for (int t = 0; t < m; ++t) {
+                if (signs[t] > 0) {
+                    if (seen_pos == slot) { c = t; break; }
+                    ++seen_pos;
+                } else {
+                    if (pos + seen_neg == slot) { c = t; break; }
+                    ++seen_neg;
+                }
+            }
+            if (c >= 0) v = cols[(long long)c * np + q];
+        }
+        lf[idx] = v;
+    }
+    if (tid == 0) {
+        meta[0] = pos;
+        meta[1] = m - pos;
+    }
+}
+
+__device__ __forceinline__ long long record_index(long long u, long long v, long long N) {
+    return u * N - u * (u - 1) / 2 + (v - u);
+}
+
+// One CTA per work item (left string u, right strings v0 .. v0 + 127): the tables restricted to
+// the left string's columns live in shared memory, so every per-lane gather stays inside one
+// row of at most n doubles (conflict-free) and every column index is warp-uniform.
 template <int K>
-__global__ void __launch_bounds__(128) spin_pairs_fast(SpinTableArgs a) {
+__global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a) {
     extern __shared__ double smem[];
+    constexpr int CP = K * (K - 1) / 2;
+    constexpr int CH = kFactorChunk;
     const int n = a.n;
     const int gd = a.gamma_dim;
-    double* sS = smem;
-    double* sh = smem + n * n;
-    double* sG = smem + 2 * n * n;
-    for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
-        sS[i] = a.S[i];
-        sh[i] = a.h[i];
-    }
-    if (K >= 2)
-        for (int i = threadIdx.x; i < gd * gd; i += blockDim.x) sG[i] = a.gamma[i];
-    __syncthreads();
-
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < a.n_pairs; t += stride) {
-        long long u, v;
-        decode_upper(t, &u, &v);
+    const int Rs = a.Rs;
+    double* sS = smem;                      // [c][i] = S(i, L_c)
+    double* sh = sS + K * n;                // [c][i] = h(i, L_c)
+    double* sG = sh + K * n;                // [cp][rp] = gamma(rp, pair(L_c1, L_c2))
+    double* sL = sG + (K >= 2 ? CP * gd : 0);  // [(c n + i) Rs + m] = lf(pair(i, L_c), m)
+    const long long N = a.n_strings;
+    const int nch = (a.R + CH - 1) / CH;
+    for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+        const int2 it = a.items[item];
+        const long long u = it.x;
+        __syncthreads();
         const uint64_t wl = __ldg(a.occ + 2 * u);
-        const uint64_t wr = __ldg(a.occ + 2 * v);
-        int L[K], R[K];
+        int L[K];
 #pragma unroll
-        for (int c = 0; c < K; ++c) {
-            L[c] = (int)((wl >> (8 * c)) & 0xFFu);
-            R[c] = (int)((wr >> (8 * c)) & 0xFFu);
+        for (int c = 0; c < K; ++c) L[c] = (int)((wl >> (8 * c)) & 0xFFu);
+        for (int idx = threadIdx.x; idx < K * n; idx += blockDim.x) {
+            const int c = idx / n, i = idx % n;
+            int lc = 0;
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc)
+                if (cc == c) lc = L[cc];
+            sS[idx] = __ldg(a.S + lc * n + i);
+            sh[idx] = __ldg(a.h + lc * n + i);
         }
+        if (K >= 2) {
+            for (int idx = threadIdx.x; idx < CP * gd; idx += blockDim.x) {
+                const int cp = idx / gd, rp = idx % gd;
+                // cp enumerates (c1 < c2) in the order c2 (c2 - 1) / 2 + c1
+                int c2 = (int)floorf((1.0f + sqrtf(1.0f + 8.0f * cp)) * 0.5f);
+                while (c2 * (c2 - 1) / 2 > cp) --c2;
+                while ((c2 + 1) * c2 / 2 <= cp) ++c2;
+                const int c1 = cp - c2 * (c2 - 1) / 2;
+                int l1 = 0, l2 = 0;
+#pragma unroll
+                for (int cc = 0; cc < K; ++cc) {
+                    if (cc == c1) l1 = L[cc];
+                    if (cc == c2) l2 = L[cc];
+                }
+                sG[idx] = __ldg(a.gamma + (long long)rp * gd + dev::anti_index(l1, l2));
+            }
+        }
+        for (int idx = threadIdx.x; idx < K * n * Rs; idx += blockDim.x) {
+            const int m = idx % Rs, row = idx / Rs;
+            const int c = row / n, i = row % n;
+            int lc = 0;
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc)
+                if (cc == c) lc = L[cc];
+            sL[idx] = m < a.R ? __ldg(a.lf + (long long)dev::pair_index(i, lc) * a.ld + m) : 0.0;
+        }
+        __syncthreads();
+        const long long v = (long long)it.y + threadIdx.x;
+        if (v >= N) continue;
+        const long long t = record_index(u, v, N);
+        const uint64_t wr = __ldg(a.occ + 2 * v);
+        int R[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) R[c] = (int)((wr >> (8 * c)) & 0xFFu);
         double x[K][K];
         double nx2 = 0.0;
 #pragma unroll
         for (int r = 0; r < K; ++r)
 #pragma unroll
             for (int c = 0; c < K; ++c) {
-                x[r][c] = sS[R[r] * n + L[c]];
+                x[r][c] = sS[c * n + R[r]];
                 nx2 = fma(x[r][c], x[r][c], nx2);
             }
         constexpr int K0 = K <= 3 ? K : 1;
@@ -171,13 +327,16 @@ __global__ void __launch_bounds__(128) spin_pairs_fast(SpinTableArgs a) {
         const bool accepted = isfinite(det) && det != 0.0 && (nx2 * ni2 < kCertificate2);
         if (!accepted) {
             const unsigned long long slot = atomicAdd(a.careful_count, 1ull);
-            a.careful_list[slot] = t;
+            a.careful_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
             continue;
         }
         double* rec = a.records + t * (long long)a.rec_stride;
         double h1 = 0.0, h2 = 0.0;
+        // A(row, c): value and right orbital, in the order the u-vector loop visits them
+        int Rp[K];
         if (K <= 3) {
-            // closed-form cofactors and second cofactors (contractions.cpp:187-205, 915-923)
+#pragma unroll
+            for (int j = 0; j < K; ++j) Rp[j] = R[j];
             double cof[K0][K0];
 #pragma unroll
             for (int i = 0; i < K0; ++i)
@@ -193,11 +352,10 @@ __global__ void __launch_bounds__(128) spin_pairs_fast(SpinTableArgs a) {
                         value = fma(x0[rr][cc], x0[ss][dd], -product) - fma(x0[rr][dd], x0[ss][cc], -product);
                     }
                     cof[i][j] = ((i + j) & 1) ? -value : value;
-                    h1 = fma(sh[R[i] * n + L[j]], cof[i][j], h1);
-                    rec[i * K + j] = cof[i][j];
+                    h1 = fma(sh[j * n + R[i]], cof[i][j], h1);
                 }
             if (K == 2) {
-                h2 = sG[dev::anti_index(R[0], R[1]) * gd + dev::anti_index(L[0], L[1])];
+                h2 = sG[dev::anti_index(R[0], R[1])];
             } else if (K == 3) {
 #pragma unroll
                 for (int r1 = 0; r1 < K0; ++r1)
@@ -208,27 +366,39 @@ __global__ void __launch_bounds__(128) spin_pairs_fast(SpinTableArgs a) {
 #pragma unroll
                             for (int c2 = c1 + 1; c2 < K0; ++c2) {
                                 const double sign = ((r1 + r2 + c1 + c2) & 1) ? -1.0 : 1.0;
-                                const double c2nd = sign * x0[3 - r1 - r2][3 - c1 - c2];
-                                h2 = fma(sG[dev::anti_index(R[r1], R[r2]) * gd + dev::anti_index(L[c1], L[c2])], c2nd,
-                                         h2);
+                                const int cp = c2 * (c2 - 1) / 2 + c1;
+                                h2 = fma(sG[cp * gd + dev::anti_index(R[r1], R[r2])],
+                                         sign * x0[3 - r1 - r2][3 - c1 - c2], h2);
                             }
             }
+            // u-vector: u[m] = sum_{r,c} cof(r, c) lf(pair(R_r, L_c), m)
+            for (int ch = 0; ch < nch; ++ch) {
+                double acc[CH];
+#pragma unroll
+                for (int q = 0; q < CH; ++q) acc[q] = 0.0;
+#pragma unroll
+                for (int c = 0; c < K0; ++c)
+#pragma unroll
+                    for (int r = 0; r < K0; ++r) {
+                        const double av = cof[r][c];
+                        const double* row = sL + (c * n + R[r]) * Rs + ch * CH;
+#pragma unroll
+                        for (int q = 0; q < CH; ++q) acc[q] = fma(av, row[q], acc[q]);
+                    }
+#pragma unroll
+                for (int q = 0; q < CH; ++q)
+                    if (ch * CH + q < a.R) rec[ch * CH + q] = acc[q];
+            }
         } else {
-            // x now holds C = (P X)^{-1}; X^{-1}[c][lab[j]] = C[c][j], A(lab[j], c) = det C[c][j].
-            int Rp[K];
+            // x holds C = (P X)^{-1}: X^{-1}[c][lab[j]] = C[c][j], A(lab[j], c) = det C[c][j]
 #pragma unroll
             for (int j = 0; j < K; ++j) Rp[j] = (int)((wr >> (8 * lab[j])) & 0xFFu);
             double acc1 = 0.0;
 #pragma unroll
             for (int j = 0; j < K; ++j)
 #pragma unroll
-                for (int c = 0; c < K; ++c) acc1 = fma(sh[Rp[j] * n + L[c]], x[c][j], acc1);
+                for (int c = 0; c < K; ++c) acc1 = fma(sh[c * n + Rp[j]], x[c][j], acc1);
             h1 = det * acc1;
-            int cidx[K][K];
-#pragma unroll
-            for (int c1 = 0; c1 < K; ++c1)
-#pragma unroll
-                for (int c2 = c1 + 1; c2 < K; ++c2) cidx[c1][c2] = dev::anti_index(L[c1], L[c2]);
             double acc2 = 0.0;
 #pragma unroll
             for (int j1 = 0; j1 < K; ++j1)
@@ -236,29 +406,40 @@ __global__ void __launch_bounds__(128) spin_pairs_fast(SpinTableArgs a) {
                 for (int j2 = j1 + 1; j2 < K; ++j2) {
                     const int ra = Rp[j1], rb = Rp[j2];
                     const bool ordered = ra < rb;
-                    const double* grow = sG + dev::anti_index(ordered ? ra : rb, ordered ? rb : ra) * gd;
+                    const int rp = dev::anti_index(ordered ? ra : rb, ordered ? rb : ra);
                     double part = 0.0;
 #pragma unroll
                     for (int c1 = 0; c1 < K; ++c1)
 #pragma unroll
                         for (int c2 = c1 + 1; c2 < K; ++c2) {
                             const double m2 = fma(x[c1][j1], x[c2][j2], -x[c2][j1] * x[c1][j2]);
-                            part = fma(grow[cidx[c1][c2]], m2, part);
+                            part = fma(sG[(c2 * (c2 - 1) / 2 + c1) * gd + rp], m2, part);
                         }
                     acc2 += ordered ? part : -part;
                 }
             h2 = det * acc2;
+            for (int ch = 0; ch < nch; ++ch) {
+                double acc[CH];
 #pragma unroll
-            for (int j = 0; j < K; ++j) {
-                double* row = rec + lab[j] * K;
+                for (int q = 0; q < CH; ++q) acc[q] = 0.0;
 #pragma unroll
-                for (int c = 0; c < K; ++c) row[c] = det * x[c][j];
+                for (int c = 0; c < K; ++c)
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        const double av = x[c][j];
+                        const double* row = sL + (c * n + Rp[j]) * Rs + ch * CH;
+#pragma unroll
+                        for (int q = 0; q < CH; ++q) acc[q] = fma(av, row[q], acc[q]);
+                    }
+#pragma unroll
+                for (int q = 0; q < CH; ++q)
+                    if (ch * CH + q < a.R) rec[ch * CH + q] = det * acc[q];
             }
         }
-        rec[K * K + 0] = det;
-        rec[K * K + 1] = h1 + h2;
-        rec[K * K + 2] = h1;
-        rec[K * K + 3] = 0.0;
+        rec[a.R + 0] = det;
+        rec[a.R + 1] = h1 + h2;
+        rec[a.R + 2] = h1;
+        rec[a.R + 3] = 0.0;
     }
 }
 
@@ -266,10 +447,29 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
     const long long count = a.all_careful ? a.n_pairs : (long long)(*a.careful_count);
     const long long stride = (long long)gridDim.x * blockDim.x;
     const int k = a.k;
+    const long long N = a.n_strings;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < count; idx += stride) {
-        const long long t = a.all_careful ? idx : a.careful_list[idx];
         long long u, v;
-        decode_upper(t, &u, &v);
+        if (a.all_careful) {
+            // idx enumerates pairs row by row: decode the row-major upper packing
+            long long uu = 0;
+            {
+                // offset(u) = u N - u (u - 1) / 2; solve offset(u) <= idx < offset(u + 1)
+                const double b = 2.0 * (double)N + 1.0;
+                uu = (long long)floor((b - sqrt(fmax(b * b - 8.0 * (double)idx, 0.0))) * 0.5);
+                if (uu < 0) uu = 0;
+                if (uu > N - 1) uu = N - 1;
+                while (uu > 0 && uu * N - uu * (uu - 1) / 2 > idx) --uu;
+                while (uu + 1 < N && (uu + 1) * N - (uu + 1) * uu / 2 <= idx) ++uu;
+            }
+            u = uu;
+            v = u + (idx - (u * N - u * (u - 1) / 2));
+        } else {
+            const unsigned long long w = a.careful_list[idx];
+            u = (long long)(w >> 32);
+            v = (long long)(w & 0xffffffffull);
+        }
+        const long long t = record_index(u, v, N);
         int L[dev::KMAX], R[dev::KMAX];
         for (int c = 0; c < k; ++c) {
             L[c] = occ_byte(a.occ + 2 * u, c);
@@ -285,12 +485,18 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
         double h1 = 0.0, htot = 0.0;
         if (res.nullity < 3) htot = dev::same_spin_exact(a.n, k, L, R, res, cof, a.h, a.eri, &h1);
         double* rec = a.records + t * (long long)a.rec_stride;
-        for (int r = 0; r < k; ++r)
-            for (int c = 0; c < k; ++c) rec[r * k + c] = res.nullity <= 1 ? cof[c * k + r] : 0.0;
-        rec[k * k + 0] = res.det;
-        rec[k * k + 1] = htot;
-        rec[k * k + 2] = h1;
-        rec[k * k + 3] = (double)res.nullity;
+        for (int m = 0; m < a.R; ++m) {
+            double acc = 0.0;
+            if (res.nullity <= 1)
+                for (int c = 0; c < k; ++c)
+                    for (int r = 0; r < k; ++r)
+                        acc = fma(cof[c * k + r], __ldg(a.lf + (long long)dev::pair_index(R[r], L[c]) * a.ld + m), acc);
+            rec[m] = acc;
+        }
+        rec[a.R + 0] = res.det;
+        rec[a.R + 1] = htot;
+        rec[a.R + 2] = h1;
+        rec[a.R + 3] = (double)res.nullity;
     }
 }
 
@@ -313,181 +519,66 @@ __device__ __forceinline__ void band_decode(long long t, long long e0, long long
     *e = *d + (tp - (i * B - i * (i - 1) / 2));
 }
 
-__device__ __forceinline__ long long upper_record(int a, int b) {
-    const long long hi = a > b ? a : b, lo = a > b ? b : a;
-    return hi * (hi + 1) / 2 + lo;
-}
-
-template <int KB>
-__global__ void __launch_bounds__(128) full_pairs_kernel(FullPairArgs a) {
-    extern __shared__ double sK[];
-    const int np = a.np;
-    if (a.kfull_in_smem) {
-        for (int i = threadIdx.x; i < np * np; i += blockDim.x) sK[i] = a.kfull[i];
-        __syncthreads();
-    }
-    const double* K = a.kfull_in_smem ? sK : a.kfull;
-    const long long B = a.e1 - a.e0;
-    const int ka = a.ka;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < a.n_items; t += stride) {
-        long long d, e;
-        band_decode(t, a.e0, a.e1, &d, &e);
+// S_de = S_a S_b, H_de = H_a S_b + H_b S_a + sum_m sigma_m u_a[m] u_b[m] for one determinant pair.
+__device__ __forceinline__ void pair_value(const FullPairArgs& a, long long d, long long e, double* H, double* S) {
+    double sa = 1.0, hsa = 0.0, sb = 1.0, hsb = 0.0, dot = 0.0;
+    const double* ra = nullptr;
+    const double* rb = nullptr;
+    const int R = a.R;
+    if (a.ka > 0) {
         const int ia = __ldg(a.det_alpha + d), ja = __ldg(a.det_alpha + e);
-        const int ib = __ldg(a.det_beta + d), jb = __ldg(a.det_beta + e);
-        const int la = min(ia, ja), ha = max(ia, ja), lb = min(ib, jb), hb = max(ib, jb);
-        const double* ra = a.rec_a + upper_record(la, ha) * a.stride_a;
-        const double* rb = a.rec_b + upper_record(lb, hb) * a.stride_b;
-        const double sa = ra[ka * ka], hsa = ra[ka * ka + 1], nua = ra[ka * ka + 3];
-        const double sb = rb[KB * KB], hsb = rb[KB * KB + 1], nub = rb[KB * KB + 3];
-        double H = fma(hsa, sb, hsb * sa);
-        const double S = sa * sb;
-        if (nua < 1.5 && nub < 1.5) {
-            const uint64_t wbl = __ldg(a.occ_b + 2 * lb), wbr = __ldg(a.occ_b + 2 * hb);
-            double Ab[KB * KB];
-            int qb[KB * KB];
-#pragma unroll
-            for (int r = 0; r < KB; ++r)
-#pragma unroll
-                for (int c = 0; c < KB; ++c) {
-                    Ab[r * KB + c] = rb[r * KB + c];
-                    qb[r * KB + c] = dev::pair_index((int)((wbr >> (8 * r)) & 0xFFu), (int)((wbl >> (8 * c)) & 0xFFu));
-                }
-            const uint64_t* occl = a.occ_a + 2 * la;
-            const uint64_t* occr = a.occ_a + 2 * ha;
-            double opp = 0.0;
-            for (int r = 0; r < ka; ++r) {
-                const int Ra = occ_byte(occr, r);
-                for (int c = 0; c < ka; ++c) {
-                    const double av = ra[r * ka + c];
-                    const double* krow = K + dev::pair_index(Ra, occ_byte(occl, c)) * np;
-                    double tt = 0.0;
-#pragma unroll
-                    for (int i = 0; i < KB * KB; ++i) tt = fma(Ab[i], krow[qb[i]], tt);
-                    opp = fma(av, tt, opp);
-                }
-            }
-            H += opp;
-        }
-        const long long o = d * B + (e - a.e0);
-        a.Hb[o] = H;
-        a.Sb[o] = S;
+        const long long lo = min(ia, ja), hi = max(ia, ja);
+        ra = a.rec_a + record_index(lo, hi, a.Na) * a.stride_a;
+        sa = ra[R];
+        hsa = ra[R + 1];
     }
+    if (a.kb > 0) {
+        const int ib = __ldg(a.det_beta + d), jb = __ldg(a.det_beta + e);
+        const long long lo = min(ib, jb), hi = max(ib, jb);
+        rb = a.rec_b + record_index(lo, hi, a.Nb) * a.stride_b;
+        sb = rb[R];
+        hsb = rb[R + 1];
+    }
+    if (ra && rb) {
+        double pos = 0.0, neg = 0.0;
+        int m = 0;
+        for (; m + 1 < a.r_pos; m += 2) {
+            const double2 x = *reinterpret_cast<const double2*>(ra + m);
+            const double2 y = *reinterpret_cast<const double2*>(rb + m);
+            pos = fma(x.x, y.x, pos);
+            pos = fma(x.y, y.y, pos);
+        }
+        for (; m < a.r_pos; ++m) pos = fma(ra[m], rb[m], pos);
+        for (; m < R; ++m) neg = fma(ra[m], rb[m], neg);
+        dot = pos - neg;
+    }
+    *H = fma(hsa, sb, fma(hsb, sa, dot));
+    *S = sa * sb;
 }
 
-// Generic variant: any k_a, k_b <= 16 (either may be zero); both cofactor blocks streamed.
-__global__ void __launch_bounds__(128) full_pairs_generic(FullPairArgs a) {
-    extern __shared__ double sK[];
-    const int np = a.np;
-    if (a.kfull_in_smem) {
-        for (int i = threadIdx.x; i < np * np; i += blockDim.x) sK[i] = a.kfull[i];
-        __syncthreads();
-    }
-    const double* K = a.kfull_in_smem ? sK : a.kfull;
+__global__ void __launch_bounds__(256) full_pairs_kernel(FullPairArgs a) {
     const long long B = a.e1 - a.e0;
-    const int ka = a.ka, kb = a.kb;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < a.n_items; t += stride) {
         long long d, e;
         band_decode(t, a.e0, a.e1, &d, &e);
-        double sa = 1.0, hsa = 0.0, nua = 0.0, sb = 1.0, hsb = 0.0, nub = 0.0;
-        const double* ra = nullptr;
-        const double* rb = nullptr;
-        int la = 0, ha = 0, lb = 0, hb = 0;
-        if (ka > 0) {
-            const int ia = __ldg(a.det_alpha + d), ja = __ldg(a.det_alpha + e);
-            la = min(ia, ja);
-            ha = max(ia, ja);
-            ra = a.rec_a + upper_record(la, ha) * a.stride_a;
-            sa = ra[ka * ka];
-            hsa = ra[ka * ka + 1];
-            nua = ra[ka * ka + 3];
-        }
-        if (kb > 0) {
-            const int ib = __ldg(a.det_beta + d), jb = __ldg(a.det_beta + e);
-            lb = min(ib, jb);
-            hb = max(ib, jb);
-            rb = a.rec_b + upper_record(lb, hb) * a.stride_b;
-            sb = rb[kb * kb];
-            hsb = rb[kb * kb + 1];
-            nub = rb[kb * kb + 3];
-        }
-        double H = fma(hsa, sb, hsb * sa);
-        const double S = sa * sb;
-        if (ka > 0 && kb > 0 && nua < 1.5 && nub < 1.5) {
-            double opp = 0.0;
-            for (int r = 0; r < ka; ++r) {
-                const int Ra = occ_byte(a.occ_a + 2 * ha, r);
-                for (int c = 0; c < ka; ++c) {
-                    const double av = ra[r * ka + c];
-                    const double* krow = K + dev::pair_index(Ra, occ_byte(a.occ_a + 2 * la, c)) * np;
-                    double tt = 0.0;
-                    for (int r2 = 0; r2 < kb; ++r2) {
-                        const int Rb = occ_byte(a.occ_b + 2 * hb, r2);
-                        for (int c2 = 0; c2 < kb; ++c2)
-                            tt = fma(rb[r2 * kb + c2], krow[dev::pair_index(Rb, occ_byte(a.occ_b + 2 * lb, c2))], tt);
-                    }
-                    opp = fma(av, tt, opp);
-                }
-            }
-            H += opp;
-        }
+        double H, S;
+        pair_value(a, d, e, &H, &S);
         const long long o = d * B + (e - a.e0);
         a.Hb[o] = H;
         a.Sb[o] = S;
     }
 }
 
-// Listed determinant pairs (d, e) in any order, full orientation handled through records.
+// Listed determinant pairs (d, e) in any order.
 __global__ void listed_pairs_kernel(FullPairArgs a, long long n_pairs, const long long* __restrict__ pairs,
                                     double* __restrict__ h_out, double* __restrict__ s_out) {
-    const int np = a.np;
-    const double* K = a.kfull;
-    const int ka = a.ka, kb = a.kb;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n_pairs;
          t += (long long)gridDim.x * blockDim.x) {
-        const long long d = pairs[2 * t], e = pairs[2 * t + 1];
-        double sa = 1.0, hsa = 0.0, nua = 0.0, sb = 1.0, hsb = 0.0, nub = 0.0;
-        const double* ra = nullptr;
-        const double* rb = nullptr;
-        int la = 0, ha = 0, lb = 0, hb = 0;
-        if (ka > 0) {
-            const int ia = a.det_alpha[d], ja = a.det_alpha[e];
-            la = min(ia, ja);
-            ha = max(ia, ja);
-            ra = a.rec_a + upper_record(la, ha) * a.stride_a;
-            sa = ra[ka * ka];
-            hsa = ra[ka * ka + 1];
-            nua = ra[ka * ka + 3];
-        }
-        if (kb > 0) {
-            const int ib = a.det_beta[d], jb = a.det_beta[e];
-            lb = min(ib, jb);
-            hb = max(ib, jb);
-            rb = a.rec_b + upper_record(lb, hb) * a.stride_b;
-            sb = rb[kb * kb];
-            hsb = rb[kb * kb + 1];
-            nub = rb[kb * kb + 3];
-        }
-        double H = fma(hsa, sb, hsb * sa);
-        if (ka > 0 && kb > 0 && nua < 1.5 && nub < 1.5) {
-            double opp = 0.0;
-            for (int r = 0; r < ka; ++r)
-                for (int c = 0; c < ka; ++c) {
-                    const double* krow =
-                        K + dev::pair_index(occ_byte(a.occ_a + 2 * ha, r), occ_byte(a.occ_a + 2 * la, c)) * np;
-                    double tt = 0.0;
-                    for (int r2 = 0; r2 < kb; ++r2)
-                        for (int c2 = 0; c2 < kb; ++c2)
-                            tt = fma(rb[r2 * kb + c2],
-                                     krow[dev::pair_index(occ_byte(a.occ_b + 2 * hb, r2), occ_byte(a.occ_b + 2 * lb, c2))],
-                                     tt);
-                    opp = fma(ra[r * ka + c], tt, opp);
-                }
-            H += opp;
-        }
+        double H, S;
+        pair_value(a, pairs[2 * t], pairs[2 * t + 1], &H, &S);
         h_out[t] = H;
-        s_out[t] = sa * sb;
+        s_out[t] = S;
     }
 }
 
@@ -536,33 +627,31 @@ __global__ void same_spin_list_kernel(int n, int k, long long batch, const int* 
 }
 
 template <int K>
-cudaError_t launch_fast(const SpinTableArgs& a, cudaStream_t stream) {
-    const size_t smem = sizeof(double) * (2 * (size_t)a.n * a.n + (K >= 2 ? (size_t)a.gamma_dim * a.gamma_dim : 0));
+cudaError_t launch_fast(const SpinTableArgs& a, size_t smem, cudaStream_t stream) {
     cudaError_t err = cudaFuncSetAttribute(spin_pairs_fast<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    long long blocks = (a.n_pairs + 127) / 128;
-    if (blocks > kSms * 16) blocks = kSms * 16;
+    int blocks = a.n_items;
+    if (blocks > kSms * 24) blocks = kSms * 24;
     if (blocks < 1) blocks = 1;
-    spin_pairs_fast<K><<<(unsigned)blocks, 128, smem, stream>>>(a);
-    return cudaGetLastError();
-}
-
-template <int KB>
-cudaError_t launch_full(const FullPairArgs& a, size_t smem, cudaStream_t stream) {
-    cudaError_t err = cudaFuncSetAttribute(full_pairs_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    long long blocks = (a.n_items + 127) / 128;
-    if (blocks > kSms * 32) blocks = kSms * 32;
-    if (blocks < 1) blocks = 1;
-    full_pairs_kernel<KB><<<(unsigned)blocks, 128, smem, stream>>>(a);
+    spin_pairs_fast<K><<<blocks, kSpinBlock, smem, stream>>>(a);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t fast_spin_smem_bytes(int n, int k) {
+size_t factored_spin_smem_bytes(int n, int k, int Rs) {
     const size_t gd = (size_t)n * (n - 1) / 2;
-    return sizeof(double) * (2 * (size_t)n * n + (k >= 2 ? gd * gd : 0));
+    const size_t cp = (size_t)k * (k - 1) / 2;
+    return sizeof(double) * (2 * (size_t)k * n + (k >= 2 ? cp * gd : 0) + (size_t)k * n * Rs);
+}
+
+cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs, double* lf,
+                                      int ld, int* meta, cudaStream_t stream) {
+    const size_t smem = sizeof(int) * (size_t)np;
+    cudaError_t err = cudaFuncSetAttribute(factor_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    factor_pair_kernel<<<1, 512, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, kFactorTolerance);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, double* kfull, cudaStream_t stream) {
@@ -578,17 +667,18 @@ cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, doubl
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, cudaStream_t stream, int* launches) {
     if (a.n_pairs <= 0 || a.k <= 0) return cudaSuccess;
     cudaError_t err = cudaSuccess;
-    const bool fast_ok = !a.all_careful && a.k <= 8 && fast_spin_smem_bytes(a.n, a.k) <= 227 * 1024;
+    const size_t smem = factored_spin_smem_bytes(a.n, a.k, a.Rs);
+    const bool fast_ok = !a.all_careful && a.k <= 8 && smem <= 227 * 1024;
     if (fast_ok) {
         switch (a.k) {
-            case 1: err = launch_fast<1>(a, stream); break;
-            case 2: err = launch_fast<2>(a, stream); break;
-            case 3: err = launch_fast<3>(a, stream); break;
-            case 4: err = launch_fast<4>(a, stream); break;
-            case 5: err = launch_fast<5>(a, stream); break;
-            case 6: err = launch_fast<6>(a, stream); break;
-            case 7: err = launch_fast<7>(a, stream); break;
-            case 8: err = launch_fast<8>(a, stream); break;
+            case 1: err = launch_fast<1>(a, smem, stream); break;
+            case 2: err = launch_fast<2>(a, smem, stream); break;
+            case 3: err = launch_fast<3>(a, smem, stream); break;
+            case 4: err = launch_fast<4>(a, smem, stream); break;
+            case 5: err = launch_fast<5>(a, smem, stream); break;
+            case 6: err = launch_fast<6>(a, smem, stream); break;
+            case 7: err = launch_fast<7>(a, smem, stream); break;
+            case 8: err = launch_fast<8>(a, smem, stream); break;
             default: break;
         }
         if (err != cudaSuccess) return err;
@@ -601,32 +691,12 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, cudaStream_t stream, int* 
     return cudaGetLastError();
 }
 
-cudaError_t launch_full_pairs(const FullPairArgs& a0, cudaStream_t stream, int* launches) {
-    if (a0.n_items <= 0) return cudaSuccess;
-    FullPairArgs a = a0;
-    const size_t ksmem = sizeof(double) * (size_t)a.np * a.np;
-    a.kfull_in_smem = ksmem <= 200 * 1024 ? 1 : 0;
-    const size_t smem = a.kfull_in_smem ? ksmem : 0;
-    cudaError_t err;
+cudaError_t launch_full_pairs(const FullPairArgs& a, cudaStream_t stream, int* launches) {
+    if (a.n_items <= 0) return cudaSuccess;
+    long long blocks = (a.n_items + 255) / 256;
+    if (blocks > kSms * 16) blocks = kSms * 16;
+    full_pairs_kernel<<<(unsigned)blocks, 256, 0, stream>>>(a);
     ++*launches;
-    if (a.ka > 0 && a.kb >= 1 && a.kb <= 8 && a.ka <= 16) {
-        switch (a.kb) {
-            case 1: return launch_full<1>(a, smem, stream);
-            case 2: return launch_full<2>(a, smem, stream);
-            case 3: return launch_full<3>(a, smem, stream);
-            case 4: return launch_full<4>(a, smem, stream);
-            case 5: return launch_full<5>(a, smem, stream);
-            case 6: return launch_full<6>(a, smem, stream);
-            case 7: return launch_full<7>(a, smem, stream);
-            case 8: return launch_full<8>(a, smem, stream);
-            default: break;
-        }
-    }
-    err = cudaFuncSetAttribute(full_pairs_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    long long blocks = (a.n_items + 127) / 128;
-    if (blocks > kSms * 32) blocks = kSms * 32;
-    full_pairs_generic<<<(unsigned)blocks, 128, smem, stream>>>(a);
     return cudaGetLastError();
 }
 

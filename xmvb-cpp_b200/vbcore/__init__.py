@@ -209,7 +209,16 @@ class Context:
         return self._h
 
     def set_stream(self, stream_handle: int | None):
-        _check(load_library().vb_context_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)), self._h)
+        """Run this context's work on a caller stream (a cudaStream_t handle as an int).  None
+        restores the context's own stream; 0 (torch's default stream) means the legacy default
+        stream (cudaStreamLegacy)."""
+        if stream_handle is None:
+            handle = None
+        elif stream_handle == 0:
+            handle = 1  # cudaStreamLegacy
+        else:
+            handle = stream_handle
+        _check(load_library().vb_context_set_stream(self._h, ctypes.c_void_p(handle)), self._h)
 
     def synchronize(self):
         _check(load_library().vb_context_synchronize(self._h), self._h)
