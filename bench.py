@@ -38,7 +38,7 @@ sys.path.insert(0, os.path.join(ROOT, "xmvb-cpp_b200"))
 
 N_ACTIVE = 14
 N_ELECTRONS = 14
-N_AUX = 42
+N_AUX = 42  # 3 n_active auxiliary functions
 SEED = 20261203
 KEYWORD = "COV"
 
@@ -61,10 +61,12 @@ def dist_env():
 
 
 def config_dict(n_det, n_str, world):
+    k = N_ELECTRONS // 2
     return {
-        "workload": "determinant-pair microbenchmark: n_active=14, 7a+7b electrons, 3432 covalent determinants, "
-                    "429 covalent Rumer structures, 11,778,624 ordered determinant pairs per H/S evaluation",
-        "n_active": N_ACTIVE, "n_alpha": 7, "n_beta": 7, "n_determinants": n_det, "n_structures": n_str,
+        "workload": f"determinant-pair microbenchmark: n_active={N_ACTIVE}, {k}a+{k}b electrons, {n_det} covalent "
+                    f"determinants, {n_str} covalent Rumer structures, {n_det * n_det:,} ordered determinant pairs "
+                    "per H/S evaluation",
+        "n_active": N_ACTIVE, "n_alpha": k, "n_beta": k, "n_determinants": n_det, "n_structures": n_str,
         "n_aux": N_AUX, "seed": SEED, "structure_class": KEYWORD,
         "l2": "256 MiB device write between timed steps (plus a >2 GB per-step working set)",
         "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
@@ -378,7 +380,15 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vbcore", choices=["vbcore", "reference"])
+    ap.add_argument("--n-active", type=int, default=14,
+                    help="active orbitals (even; 14 is the benchmark workload, smaller cases are for profiling)")
     args = ap.parse_args()
+    global N_ACTIVE, N_ELECTRONS, N_AUX
+    if args.n_active != N_ACTIVE:
+        if args.n_active % 2 or not 2 <= args.n_active <= 16:
+            ap.error("--n-active must be even, 2..16")
+        N_ACTIVE = N_ELECTRONS = args.n_active
+        N_AUX = 3 * args.n_active
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -50,23 +50,31 @@ __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(Band
         }
         const int first = __shfl_sync(0xffffffffu, d_l, 0);
         if (first >= row_end) break;
-#pragma unroll 8
-        for (int q = 0; q < 32; ++q) {
-            const int d = __shfl_sync(0xffffffffu, d_l, q);
-            const int I = __shfl_sync(0xffffffffu, I_l, q);
-            const double c = __shfl_sync(0xffffffffu, c_l, q);
-            if (d >= row_end) break;
-            double hv = 0.0, sv = 0.0;
-            if (valid && d <= e) {
-                hv = __ldg(a.Hb + (long long)d * a.width + j);
-                sv = __ldg(a.Sb + (long long)d * a.width + j);
-                if (d == e) {
-                    hv *= 0.5;
-                    sv *= 0.5;
-                }
+        // eight independent band loads in flight per batch
+#pragma unroll
+        for (int q0 = 0; q0 < 32; q0 += 8) {
+            int d[8], I[8];
+            double c[8], hv[8], sv[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                d[i] = __shfl_sync(0xffffffffu, d_l, q0 + i);
+                I[i] = __shfl_sync(0xffffffffu, I_l, q0 + i);
+                c[i] = __shfl_sync(0xffffffffu, c_l, q0 + i);
             }
-            zh[I * kPad + lane] = fma(c, hv, zh[I * kPad + lane]);
-            zs[I * kPad + lane] = fma(c, sv, zs[I * kPad + lane]);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const bool use = valid && d[i] <= e && d[i] < row_end;
+                const long long o = use ? (long long)d[i] * a.width + j : 0;
+                hv[i] = use ? __ldg(a.Hb + o) : 0.0;
+                sv[i] = use ? __ldg(a.Sb + o) : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (d[i] >= row_end) continue;  // padding triples and rows past this column block
+                const double w = (d[i] == e) ? 0.5 * c[i] : c[i];
+                zh[I[i] * kPad + lane] = fma(w, hv[i], zh[I[i] * kPad + lane]);
+                zs[I[i] * kPad + lane] = fma(w, sv[i], zs[I[i] * kPad + lane]);
+            }
         }
     }
     __syncthreads();

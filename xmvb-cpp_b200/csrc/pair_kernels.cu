@@ -206,50 +206,56 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a) {
     double* sL = sG + (K >= 2 ? CP * gd : 0);  // [(c n + i) Rs + m] = lf(pair(i, L_c), m)
     const long long N = a.n_strings;
     const int nch = (a.R + CH - 1) / CH;
-    for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+    // contiguous item range per CTA: consecutive items mostly share the left string, whose
+    // tables are reloaded only when it changes
+    const int per = (a.n_items + gridDim.x - 1) / gridDim.x;
+    const int item_begin = blockIdx.x * per;
+    const int item_end = min(a.n_items, item_begin + per);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    long long loaded_u = -1;
+    for (int item = item_begin; item < item_end; ++item) {
         const int2 it = a.items[item];
         const long long u = it.x;
-        __syncthreads();
         const uint64_t wl = __ldg(a.occ + 2 * u);
         int L[K];
 #pragma unroll
         for (int c = 0; c < K; ++c) L[c] = (int)((wl >> (8 * c)) & 0xFFu);
-        for (int idx = threadIdx.x; idx < K * n; idx += blockDim.x) {
-            const int c = idx / n, i = idx % n;
-            int lc = 0;
+        if (u != loaded_u) {
+            __syncthreads();
+            // rows of the left string's tables: one warp per row, lanes along the row
+            for (int row = warp; row < K * n; row += nwarps) {
+                const int c = row / n, i = row % n;
+                int lc = 0;
 #pragma unroll
-            for (int cc = 0; cc < K; ++cc)
-                if (cc == c) lc = L[cc];
-            sS[idx] = __ldg(a.S + lc * n + i);
-            sh[idx] = __ldg(a.h + lc * n + i);
-        }
-        if (K >= 2) {
-            for (int idx = threadIdx.x; idx < CP * gd; idx += blockDim.x) {
-                const int cp = idx / gd, rp = idx % gd;
-                // cp enumerates (c1 < c2) in the order c2 (c2 - 1) / 2 + c1
-                int c2 = (int)floorf((1.0f + sqrtf(1.0f + 8.0f * cp)) * 0.5f);
-                while (c2 * (c2 - 1) / 2 > cp) --c2;
-                while ((c2 + 1) * c2 / 2 <= cp) ++c2;
-                const int c1 = cp - c2 * (c2 - 1) / 2;
-                int l1 = 0, l2 = 0;
-#pragma unroll
-                for (int cc = 0; cc < K; ++cc) {
-                    if (cc == c1) l1 = L[cc];
-                    if (cc == c2) l2 = L[cc];
+                for (int cc = 0; cc < K; ++cc)
+                    if (cc == c) lc = L[cc];
+                if (lane == 0) {
+                    sS[row] = __ldg(a.S + lc * n + i);
+                    sh[row] = __ldg(a.h + lc * n + i);
                 }
-                sG[idx] = __ldg(a.gamma + (long long)rp * gd + dev::anti_index(l1, l2));
+                const double* src = a.lf + (long long)dev::pair_index(i, lc) * a.ld;
+                double* dst = sL + (long long)row * Rs;
+                for (int m = lane; m < Rs; m += 32) dst[m] = m < a.R ? __ldg(src + m) : 0.0;
             }
-        }
-        for (int idx = threadIdx.x; idx < K * n * Rs; idx += blockDim.x) {
-            const int m = idx % Rs, row = idx / Rs;
-            const int c = row / n, i = row % n;
-            int lc = 0;
+            if (K >= 2) {
+                // gamma is symmetric: column pair(L_c1, L_c2) read as a contiguous row
+                for (int cp = warp; cp < CP; cp += nwarps) {
+                    int c2 = 1;
+                    while ((c2 + 1) * c2 / 2 <= cp) ++c2;
+                    const int c1 = cp - c2 * (c2 - 1) / 2;
+                    int l1 = 0, l2 = 0;
 #pragma unroll
-            for (int cc = 0; cc < K; ++cc)
-                if (cc == c) lc = L[cc];
-            sL[idx] = m < a.R ? __ldg(a.lf + (long long)dev::pair_index(i, lc) * a.ld + m) : 0.0;
+                    for (int cc = 0; cc < K; ++cc) {
+                        if (cc == c1) l1 = L[cc];
+                        if (cc == c2) l2 = L[cc];
+                    }
+                    const double* src = a.gamma + (long long)dev::anti_index(l1, l2) * gd;
+                    for (int rp = lane; rp < gd; rp += 32) sG[cp * gd + rp] = __ldg(src + rp);
+                }
+            }
+            loaded_u = u;
+            __syncthreads();
         }
-        __syncthreads();
         const long long v = (long long)it.y + threadIdx.x;
         if (v >= N) continue;
         const long long t = record_index(u, v, N);
@@ -630,8 +636,11 @@ template <int K>
 cudaError_t launch_fast(const SpinTableArgs& a, size_t smem, cudaStream_t stream) {
     cudaError_t err = cudaFuncSetAttribute(spin_pairs_fast<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    int blocks = a.n_items;
-    if (blocks > kSms * 24) blocks = kSms * 24;
+    int per_sm = 1;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_pairs_fast<K>, kSpinBlock, smem);
+    if (err != cudaSuccess) return err;
+    int blocks = kSms * (per_sm > 0 ? per_sm : 1);
+    if (blocks > a.n_items) blocks = a.n_items;
     if (blocks < 1) blocks = 1;
     spin_pairs_fast<K><<<blocks, kSpinBlock, smem, stream>>>(a);
     return cudaGetLastError();
