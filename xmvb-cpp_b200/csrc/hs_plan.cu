@@ -33,7 +33,7 @@ struct vb_hs_plan {
     int Na = 0, Nb = 0;
     bool shared_tables = false;
     DeviceBuffer occ_a, occ_b, det_alpha, det_beta;
-    DeviceBuffer rec_a, rec_b;
+    DeviceBuffer rec_a, rec_b, tables_a, tables_b;
     int stride_a = 0, stride_b = 0;
     long long npairs_a = 0, npairs_b = 0;
     DeviceBuffer counters, list_a, list_b, items_a, items_b;
@@ -229,6 +229,13 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
             return fail(st);
     }
     if ((st = p->counters.allocate(ctx, 4 * sizeof(unsigned long long))) != VB_OK) return fail(st);
+    // per-left-string decomposition tables, sized for the largest factor rank
+    if (p->ka > 0 &&
+        (st = p->tables_a.allocate(ctx, sizeof(double) * left_table_doubles(n, p->ka, p->np) * p->Na)) != VB_OK)
+        return fail(st);
+    if (p->kb > 0 && !p->shared_tables &&
+        (st = p->tables_b.allocate(ctx, sizeof(double) * left_table_doubles(n, p->kb, p->np) * p->Nb)) != VB_OK)
+        return fail(st);
 
     // inputs and derived integral tables
     if ((st = p->S_in.allocate(ctx, sizeof(double) * n * n)) != VB_OK) return fail(st);
@@ -338,8 +345,6 @@ SpinTableArgs table_args(vb_hs_plan* p, bool beta, const double* S, const double
     a.lf = p->lf.as<double>();
     a.ld = p->np;
     a.R = p->R;
-    const int chunks = (p->R + kFactorChunk - 1) / kFactorChunk;
-    a.Rs = std::max(1, chunks * kFactorChunk) | 1;
     a.records = beta ? p->rec_b.as<double>() : p->rec_a.as<double>();
     a.rec_stride = record_stride(p->R);
     a.careful_count = p->counters.as<unsigned long long>() + (beta ? 1 : 0);
@@ -408,11 +413,11 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
     err = cudaMemsetAsync(p->counters.ptr, 0, 4 * sizeof(unsigned long long), s);
     if (err != cudaSuccess) return cuda_error(ctx, err, "cudaMemsetAsync");
     if (p->ka > 0) {
-        err = launch_spin_pairs(table_args(p, false, *dS, *dh, *deri), s, launches);
+        err = launch_spin_pairs(table_args(p, false, *dS, *dh, *deri), p->tables_a.as<double>(), s, launches);
         if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs (alpha)");
     }
     if (p->kb > 0 && !p->shared_tables) {
-        err = launch_spin_pairs(table_args(p, true, *dS, *dh, *deri), s, launches);
+        err = launch_spin_pairs(table_args(p, true, *dS, *dh, *deri), p->tables_b.as<double>(), s, launches);
         if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs (beta)");
     }
     return VB_OK;
@@ -531,11 +536,7 @@ vb_status vb_hs_plan_stats(const vb_hs_plan* p, vb_hs_stats* stats) {
         cudaError_t err = cudaMemcpyAsync(c, p->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, p->ctx->stream);
         if (err == cudaSuccess) err = cudaStreamSynchronize(p->ctx->stream);
         if (err != cudaSuccess) return cuda_error(p->ctx, err, "stats download");
-        auto all_exact = [&](int k) {
-            const int chunks = (p->R + kFactorChunk - 1) / kFactorChunk;
-            const int Rs = std::max(1, chunks * kFactorChunk) | 1;
-            return k > vbcore::kMaxFastElectrons || factored_spin_smem_bytes(p->n, k, Rs) > 227 * 1024;
-        };
+        auto all_exact = [&](int k) { return !fast_spin_supported(p->n, k, p->R); };
         const bool all_a = p->ka > 0 && all_exact(p->ka);
         const bool all_b = p->kb > 0 && !p->shared_tables && all_exact(p->kb);
         s.careful_spin_pairs = (long long)(all_a ? p->npairs_a : c[0]) + (long long)(all_b ? p->npairs_b : c[1]);

@@ -31,7 +31,6 @@ struct SpinTableArgs {
     const double* lf;     // pair-kernel factor, lf[q * ld + m]
     int ld;               // leading dimension of lf (>= R)
     int R;                // number of factor columns
-    int Rs;               // shared-memory row stride (odd, >= chunks * 21)
     double* records;
     int rec_stride;
     unsigned long long* careful_count;
@@ -86,14 +85,15 @@ struct StructureReduceArgs {
 
 constexpr int kBandReduceWarps = 8;
 constexpr int kBandReduceColumns = 32;
-constexpr int kFactorChunk = 21;   // u-vector entries accumulated per pass
 constexpr int kSpinBlock = 128;    // right strings per fast-kernel item (threads per CTA)
 
 cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, double* kfull, cudaStream_t stream);
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs,
                                       double* lf, int ld, int* meta, cudaStream_t stream);
-size_t factored_spin_smem_bytes(int n, int k, int Rs);
-cudaError_t launch_spin_pairs(const SpinTableArgs& a, cudaStream_t stream, int* launches);
+size_t left_table_doubles(int n, int k, int R);
+size_t factored_spin_smem_bytes(int n, int k, int R);
+bool fast_spin_supported(int n, int k, int R);
+cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches);
 cudaError_t launch_full_pairs(const FullPairArgs& a, cudaStream_t stream, int* launches);
 cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches);
 cudaError_t launch_structure_reduce(const StructureReduceArgs& a, double* H, double* S, cudaStream_t stream,

@@ -28,7 +28,7 @@ namespace vbcore {
 namespace {
 
 constexpr double kThreshold = 1.0e-12;
-constexpr double kCertificate2 = 1.0e18;  // (1e9)^2 on ||X||_F^2 ||X^-1||_F^2
+constexpr double kCertificate2 = 1.0e12;  // (1e6)^2 on ||X||_F^2 ||X^-1||_F^2
 constexpr double kFactorTolerance = 1.0e-15;  // relative pivot cut of the pair-kernel factorization
 constexpr int kSms = 148;
 
@@ -189,56 +189,174 @@ __device__ __forceinline__ long long record_index(long long u, long long v, long
     return u * N - u * (u - 1) / 2 + (v - u);
 }
 
-// One CTA per work item (left string u, right strings v0 .. v0 + 127): the tables restricted to
-// the left string's columns live in shared memory, so every per-lane gather stays inside one
-// row of at most n doubles (conflict-free) and every column index is warp-uniform.
+// Table geometry of the left-string decomposition (shared by host and device code).
+__host__ __device__ constexpr int nb_max(int k) { return k <= 4 ? k + 4 : k; }
+__host__ __device__ constexpr int even_up(int x) { return (x + 1) / 2 * 2; }
+__host__ __device__ constexpr int table_block(int k) { return even_up(nb_max(k) * k); }
+__host__ __device__ constexpr int table_head(int R) { return even_up(R + 1); }
+__host__ __device__ constexpr int table_stride_of(int k, int R) { return table_head(R) + (R + 1) * table_block(k); }
+
+// Complement decomposition per left string L (K orbitals; Lbar = the other NB = n - K orbitals).
+// For a right string R with X = S[R, L], any n x K block W gives
+//   tr(X^{-1} W[R, :]) = tr(T) + <V, Y^T>,   W = S[:, L] T + I[:, Lbar] V,
+// with T = S[L,L]^{-1} W[L,:], V = W[Lbar,:] - S[Lbar,L] T, and Y = X^{-1} I[R, Lbar], a column
+// selection of X^{-1}.  With W = B_m[:, L] (B_m[i][j] = lf(pair(i, j), m)) this is
+// u[m] / det, and with W = h[:, L] it is H_1e / det (Jacobi's formula: both are first-order
+// terms sum_{r,c} A(r,c) W(R_r, L_c) of det(X + eps W[R, :])).  T and V depend on L only, so the
+// per-pair work is K NB fused multiply-adds per column against warp-uniform table entries.
+//
+// Table of left string L, (R + 1) blocks (m < R factor columns, m = R one-electron h):
+//   [m] trace T_m (head of table_head(R) doubles), then block m at table_head(R) + m * vb:
+//   V_m[b][c] (b < nb_max(K) rows, c fastest, zero rows for b >= NB, zero padding to vb).
 template <int K>
-__global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a) {
+__global__ void __launch_bounds__(128) left_string_tables(SpinTableArgs a, double* __restrict__ tables) {
+    constexpr int vb = table_block(K);
+    const int table_stride = table_stride_of(K, a.R);
+    __shared__ double sInv[K * K];
+    __shared__ int sL[K], sLb[32];
+    const int n = a.n;
+    const int nb = n - K;
+    const long long u = blockIdx.x;
+    if (u >= a.n_strings) return;
+    if (threadIdx.x == 0) {
+        const uint64_t w0 = a.occ[2 * u];
+        int L[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) L[c] = (int)((w0 >> (8 * c)) & 0xFFu);
+        uint64_t mask = 0;
+#pragma unroll
+        for (int c = 0; c < K; ++c) mask |= 1ull << L[c];
+        int q = 0;
+        for (int i = 0; i < n; ++i)
+            if (!((mask >> i) & 1)) sLb[q++] = i;
+        // S[L, L]^{-1}: Gauss-Jordan with partial pivoting (S[L, L] is a principal block of an SPD matrix)
+        double m[K][2 * K];
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+            for (int c = 0; c < 2 * K; ++c) m[r][c] = c < K ? a.S[L[r] * n + L[c]] : (c - K == r ? 1.0 : 0.0);
+#pragma unroll
+        for (int s = 0; s < K; ++s) {
+            const double ip = 1.0 / m[s][s];
+#pragma unroll
+            for (int c = 0; c < 2 * K; ++c) m[s][c] *= ip;
+#pragma unroll
+            for (int r = 0; r < K; ++r) {
+                if (r == s) continue;
+                const double f = m[r][s];
+#pragma unroll
+                for (int c = 0; c < 2 * K; ++c) m[r][c] = fma(-f, m[s][c], m[r][c]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            sL[r] = L[r];
+#pragma unroll
+            for (int c = 0; c < K; ++c) sInv[r * K + c] = m[r][K + c];
+        }
+    }
+    __syncthreads();
+    double* tab = tables + u * (long long)table_stride;
+    const int blocks = a.R + 1;
+    const int head = table_head(a.R);
+    // one thread per (block m, column c): T[:, c] then V[:, c]
+    for (int idx = threadIdx.x; idx < blocks * K; idx += blockDim.x) {
+        const int mm = idx / K, c = idx % K;
+        const int lc = sL[c];
+        double wl[K];
+#pragma unroll
+        for (int ap = 0; ap < K; ++ap)
+            wl[ap] = mm < a.R ? a.lf[(long long)dev::pair_index(sL[ap], lc) * a.ld + mm] : a.h[sL[ap] * n + lc];
+        double tc[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            double acc = 0.0;
+#pragma unroll
+            for (int ap = 0; ap < K; ++ap) acc = fma(sInv[r * K + ap], wl[ap], acc);
+            tc[r] = acc;
+        }
+        double* vblk = tab + head + (long long)mm * vb;
+        for (int b = 0; b < nb_max(K); ++b) {
+            if (b >= nb) {
+                vblk[b * K + c] = 0.0;
+                continue;
+            }
+            const int ib = sLb[b];
+            double acc = mm < a.R ? a.lf[(long long)dev::pair_index(ib, lc) * a.ld + mm] : a.h[ib * n + lc];
+#pragma unroll
+            for (int r = 0; r < K; ++r) acc = fma(-a.S[ib * n + sL[r]], tc[r], acc);
+            vblk[b * K + c] = acc;
+        }
+        if (c == 0) {
+            // the diagonal of T needs every column: recompute it (K^2 fused multiply-adds)
+            double tr = 0.0;
+            for (int cc = 0; cc < K; ++cc) {
+                const int l2 = sL[cc];
+                double acc = 0.0;
+#pragma unroll
+                for (int ap = 0; ap < K; ++ap) {
+                    const double w = mm < a.R ? a.lf[(long long)dev::pair_index(sL[ap], l2) * a.ld + mm]
+                                              : a.h[sL[ap] * n + l2];
+                    acc = fma(sInv[cc * K + ap], w, acc);
+                }
+                tr += acc;
+            }
+            tab[mm] = tr;
+        }
+        for (int pad = nb_max(K) * K; pad < vb; ++pad)
+            if (c == 0) vblk[pad] = 0.0;
+    }
+    for (int pad = blocks + threadIdx.x; pad < head; pad += blockDim.x) tab[pad] = 0.0;
+}
+
+// One CTA per contiguous range of work items (left string u, right strings v0 .. v0 + 127);
+// the left string's tables live in shared memory and are reloaded only when u changes.
+template <int K>
+__global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a, const double* __restrict__ tables) {
     extern __shared__ double smem[];
     constexpr int CP = K * (K - 1) / 2;
-    constexpr int CH = kFactorChunk;
+    constexpr int NBMAX = nb_max(K);
+    constexpr int vb = table_block(K);
     const int n = a.n;
+    const int nb = n - K;
     const int gd = a.gamma_dim;
-    const int Rs = a.Rs;
-    double* sS = smem;                      // [c][i] = S(i, L_c)
-    double* sh = sS + K * n;                // [c][i] = h(i, L_c)
-    double* sG = sh + K * n;                // [cp][rp] = gamma(rp, pair(L_c1, L_c2))
-    double* sL = sG + (K >= 2 ? CP * gd : 0);  // [(c n + i) Rs + m] = lf(pair(i, L_c), m)
+    const int table_stride = table_stride_of(K, a.R);
+    const int head = table_head(a.R);
+    double* sT = smem;                                // left-string table (t, V blocks), 16-byte aligned
+    double* sS = sT + table_stride;                   // [c][i] = S(i, L_c)
+    double* sG = sS + even_up(K * n);                 // [cp][rp] = gamma(rp, pair(L_c1, L_c2))
+    __shared__ int sLb[NBMAX];
     const long long N = a.n_strings;
-    const int nch = (a.R + CH - 1) / CH;
-    // contiguous item range per CTA: consecutive items mostly share the left string, whose
-    // tables are reloaded only when it changes
     const int per = (a.n_items + gridDim.x - 1) / gridDim.x;
     const int item_begin = blockIdx.x * per;
     const int item_end = min(a.n_items, item_begin + per);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     long long loaded_u = -1;
+    int L[K];
     for (int item = item_begin; item < item_end; ++item) {
         const int2 it = a.items[item];
         const long long u = it.x;
-        const uint64_t wl = __ldg(a.occ + 2 * u);
-        int L[K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) L[c] = (int)((wl >> (8 * c)) & 0xFFu);
         if (u != loaded_u) {
             __syncthreads();
-            // rows of the left string's tables: one warp per row, lanes along the row
-            for (int row = warp; row < K * n; row += nwarps) {
-                const int c = row / n, i = row % n;
+            const uint64_t wl = __ldg(a.occ + 2 * u);
+#pragma unroll
+            for (int c = 0; c < K; ++c) L[c] = (int)((wl >> (8 * c)) & 0xFFu);
+            if (threadIdx.x == 0) {
+                uint64_t mask = 0;
+#pragma unroll
+                for (int c = 0; c < K; ++c) mask |= 1ull << L[c];
+                int q = 0;
+                for (int i = 0; i < n && q < NBMAX; ++i)
+                    if (!((mask >> i) & 1)) sLb[q++] = i;
+            }
+            for (int row = warp; row < K; row += nwarps) {
                 int lc = 0;
 #pragma unroll
                 for (int cc = 0; cc < K; ++cc)
-                    if (cc == c) lc = L[cc];
-                if (lane == 0) {
-                    sS[row] = __ldg(a.S + lc * n + i);
-                    sh[row] = __ldg(a.h + lc * n + i);
-                }
-                const double* src = a.lf + (long long)dev::pair_index(i, lc) * a.ld;
-                double* dst = sL + (long long)row * Rs;
-                for (int m = lane; m < Rs; m += 32) dst[m] = m < a.R ? __ldg(src + m) : 0.0;
+                    if (cc == row) lc = L[cc];
+                for (int i = lane; i < n; i += 32) sS[row * n + i] = __ldg(a.S + lc * n + i);
             }
             if (K >= 2) {
-                // gamma is symmetric: column pair(L_c1, L_c2) read as a contiguous row
                 for (int cp = warp; cp < CP; cp += nwarps) {
                     int c2 = 1;
                     while ((c2 + 1) * c2 / 2 <= cp) ++c2;
@@ -253,6 +371,8 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a) {
                     for (int rp = lane; rp < gd; rp += 32) sG[cp * gd + rp] = __ldg(src + rp);
                 }
             }
+            const double* tsrc = tables + u * (long long)table_stride;
+            for (int i = threadIdx.x; i < table_stride; i += blockDim.x) sT[i] = __ldg(tsrc + i);
             loaded_u = u;
             __syncthreads();
         }
@@ -337,74 +457,28 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a) {
             continue;
         }
         double* rec = a.records + t * (long long)a.rec_stride;
-        double h1 = 0.0, h2 = 0.0;
-        // A(row, c): value and right orbital, in the order the u-vector loop visits them
+        // x holds C = (P X)^{-1}: X^{-1}[c][lab[j]] = C[c][j]; row lab[j] carries orbital Rp[j]
         int Rp[K];
-        if (K <= 3) {
 #pragma unroll
-            for (int j = 0; j < K; ++j) Rp[j] = R[j];
-            double cof[K0][K0];
+        for (int j = 0; j < K; ++j) Rp[j] = (int)((wr >> (8 * lab[j])) & 0xFFu);
+        double h2 = 0.0;
+        if (K == 2) {
+            h2 = sG[dev::anti_index(R[0], R[1])];
+        } else if (K == 3) {
 #pragma unroll
-            for (int i = 0; i < K0; ++i)
+            for (int r1 = 0; r1 < K0; ++r1)
 #pragma unroll
-                for (int j = 0; j < K0; ++j) {
-                    double value = 1.0;
-                    if (K == 2) {
-                        value = x0[1 - i][1 - j];
-                    } else if (K == 3) {
-                        const int rr = i == 0 ? 1 : 0, ss = i == 2 ? 1 : 2;
-                        const int cc = j == 0 ? 1 : 0, dd = j == 2 ? 1 : 2;
-                        const double product = x0[rr][dd] * x0[ss][cc];
-                        value = fma(x0[rr][cc], x0[ss][dd], -product) - fma(x0[rr][dd], x0[ss][cc], -product);
-                    }
-                    cof[i][j] = ((i + j) & 1) ? -value : value;
-                    h1 = fma(sh[j * n + R[i]], cof[i][j], h1);
-                }
-            if (K == 2) {
-                h2 = sG[dev::anti_index(R[0], R[1])];
-            } else if (K == 3) {
+                for (int r2 = r1 + 1; r2 < K0; ++r2)
 #pragma unroll
-                for (int r1 = 0; r1 < K0; ++r1)
+                    for (int c1 = 0; c1 < K0; ++c1)
 #pragma unroll
-                    for (int r2 = r1 + 1; r2 < K0; ++r2)
-#pragma unroll
-                        for (int c1 = 0; c1 < K0; ++c1)
-#pragma unroll
-                            for (int c2 = c1 + 1; c2 < K0; ++c2) {
-                                const double sign = ((r1 + r2 + c1 + c2) & 1) ? -1.0 : 1.0;
-                                const int cp = c2 * (c2 - 1) / 2 + c1;
-                                h2 = fma(sG[cp * gd + dev::anti_index(R[r1], R[r2])],
-                                         sign * x0[3 - r1 - r2][3 - c1 - c2], h2);
-                            }
-            }
-            // u-vector: u[m] = sum_{r,c} cof(r, c) lf(pair(R_r, L_c), m)
-            for (int ch = 0; ch < nch; ++ch) {
-                double acc[CH];
-#pragma unroll
-                for (int q = 0; q < CH; ++q) acc[q] = 0.0;
-#pragma unroll
-                for (int c = 0; c < K0; ++c)
-#pragma unroll
-                    for (int r = 0; r < K0; ++r) {
-                        const double av = cof[r][c];
-                        const double* row = sL + (c * n + R[r]) * Rs + ch * CH;
-#pragma unroll
-                        for (int q = 0; q < CH; ++q) acc[q] = fma(av, row[q], acc[q]);
-                    }
-#pragma unroll
-                for (int q = 0; q < CH; ++q)
-                    if (ch * CH + q < a.R) rec[ch * CH + q] = acc[q];
-            }
-        } else {
-            // x holds C = (P X)^{-1}: X^{-1}[c][lab[j]] = C[c][j], A(lab[j], c) = det C[c][j]
-#pragma unroll
-            for (int j = 0; j < K; ++j) Rp[j] = (int)((wr >> (8 * lab[j])) & 0xFFu);
-            double acc1 = 0.0;
-#pragma unroll
-            for (int j = 0; j < K; ++j)
-#pragma unroll
-                for (int c = 0; c < K; ++c) acc1 = fma(sh[c * n + Rp[j]], x[c][j], acc1);
-            h1 = det * acc1;
+                        for (int c2 = c1 + 1; c2 < K0; ++c2) {
+                            const double sign = ((r1 + r2 + c1 + c2) & 1) ? -1.0 : 1.0;
+                            const int cp = c2 * (c2 - 1) / 2 + c1;
+                            h2 = fma(sG[cp * gd + dev::anti_index(R[r1], R[r2])], sign * x0[3 - r1 - r2][3 - c1 - c2],
+                                     h2);
+                        }
+        } else if (K >= 4) {
             double acc2 = 0.0;
 #pragma unroll
             for (int j1 = 0; j1 < K; ++j1)
@@ -424,23 +498,46 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a) {
                     acc2 += ordered ? part : -part;
                 }
             h2 = det * acc2;
-            for (int ch = 0; ch < nch; ++ch) {
-                double acc[CH];
+        }
+        // Y[b * K + c] = X^{-1}[c][r] for the row r carrying orbital Lbar_b (zero when Lbar_b is not in R)
+        double Y[vb];
 #pragma unroll
-                for (int q = 0; q < CH; ++q) acc[q] = 0.0;
+        for (int b = 0; b < NBMAX; ++b) {
+            const int ib = b < nb ? sLb[b] : -1;
 #pragma unroll
-                for (int c = 0; c < K; ++c)
+            for (int c = 0; c < K; ++c) {
+                double y = 0.0;
 #pragma unroll
-                    for (int j = 0; j < K; ++j) {
-                        const double av = x[c][j];
-                        const double* row = sL + (c * n + Rp[j]) * Rs + ch * CH;
-#pragma unroll
-                        for (int q = 0; q < CH; ++q) acc[q] = fma(av, row[q], acc[q]);
-                    }
-#pragma unroll
-                for (int q = 0; q < CH; ++q)
-                    if (ch * CH + q < a.R) rec[ch * CH + q] = det * acc[q];
+                for (int j = 0; j < K; ++j) y = (Rp[j] == ib) ? x[c][j] : y;
+                Y[b * K + c] = y;
             }
+        }
+#pragma unroll
+        for (int f = NBMAX * K; f < vb; ++f) Y[f] = 0.0;
+        // one-electron energy and the u-vector: det (tr T_m + sum_f Y[f] V_m[f]), V_m read as
+        // warp-uniform 16-byte shared-memory loads
+        double h1;
+        {
+            const double2* vblk = reinterpret_cast<const double2*>(sT + head + a.R * vb);
+            double acc = sT[a.R];
+#pragma unroll
+            for (int f = 0; f < vb; f += 2) {
+                const double2 w = vblk[f >> 1];
+                acc = fma(Y[f], w.x, acc);
+                acc = fma(Y[f + 1], w.y, acc);
+            }
+            h1 = det * acc;
+        }
+        for (int m = 0; m < a.R; ++m) {
+            const double2* vblk = reinterpret_cast<const double2*>(sT + head + m * vb);
+            double acc0 = sT[m], acc1 = 0.0;
+#pragma unroll
+            for (int f = 0; f < vb; f += 2) {
+                const double2 w = vblk[f >> 1];
+                acc0 = fma(Y[f], w.x, acc0);
+                acc1 = fma(Y[f + 1], w.y, acc1);
+            }
+            rec[m] = det * (acc0 + acc1);
         }
         rec[a.R + 0] = det;
         rec[a.R + 1] = h1 + h2;
@@ -633,8 +730,11 @@ __global__ void same_spin_list_kernel(int n, int k, long long batch, const int* 
 }
 
 template <int K>
-cudaError_t launch_fast(const SpinTableArgs& a, size_t smem, cudaStream_t stream) {
-    cudaError_t err = cudaFuncSetAttribute(spin_pairs_fast<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t launch_fast(const SpinTableArgs& a, size_t smem, double* tables, cudaStream_t stream) {
+    left_string_tables<K><<<a.n_strings, 128, 0, stream>>>(a, tables);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    err = cudaFuncSetAttribute(spin_pairs_fast<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     int per_sm = 1;
     err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_pairs_fast<K>, kSpinBlock, smem);
@@ -642,16 +742,25 @@ cudaError_t launch_fast(const SpinTableArgs& a, size_t smem, cudaStream_t stream
     int blocks = kSms * (per_sm > 0 ? per_sm : 1);
     if (blocks > a.n_items) blocks = a.n_items;
     if (blocks < 1) blocks = 1;
-    spin_pairs_fast<K><<<blocks, kSpinBlock, smem, stream>>>(a);
+    spin_pairs_fast<K><<<blocks, kSpinBlock, smem, stream>>>(a, tables);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t factored_spin_smem_bytes(int n, int k, int Rs) {
+size_t left_table_doubles(int n, int k, int R) {
+    (void)n;
+    return (size_t)table_stride_of(k, R);
+}
+
+size_t factored_spin_smem_bytes(int n, int k, int R) {
     const size_t gd = (size_t)n * (n - 1) / 2;
     const size_t cp = (size_t)k * (k - 1) / 2;
-    return sizeof(double) * (2 * (size_t)k * n + (k >= 2 ? cp * gd : 0) + (size_t)k * n * Rs);
+    return sizeof(double) * (left_table_doubles(n, k, R) + (size_t)even_up(k * n) + (k >= 2 ? cp * gd : 0));
+}
+
+bool fast_spin_supported(int n, int k, int R) {
+    return k >= 1 && k <= 8 && n - k >= 0 && n - k <= nb_max(k) && factored_spin_smem_bytes(n, k, R) <= 200 * 1024;
 }
 
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs, double* lf,
@@ -673,25 +782,25 @@ cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, doubl
     return cudaGetLastError();
 }
 
-cudaError_t launch_spin_pairs(const SpinTableArgs& a, cudaStream_t stream, int* launches) {
+cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches) {
     if (a.n_pairs <= 0 || a.k <= 0) return cudaSuccess;
     cudaError_t err = cudaSuccess;
-    const size_t smem = factored_spin_smem_bytes(a.n, a.k, a.Rs);
-    const bool fast_ok = !a.all_careful && a.k <= 8 && smem <= 227 * 1024;
+    const size_t smem = factored_spin_smem_bytes(a.n, a.k, a.R);
+    const bool fast_ok = !a.all_careful && fast_spin_supported(a.n, a.k, a.R);
     if (fast_ok) {
         switch (a.k) {
-            case 1: err = launch_fast<1>(a, smem, stream); break;
-            case 2: err = launch_fast<2>(a, smem, stream); break;
-            case 3: err = launch_fast<3>(a, smem, stream); break;
-            case 4: err = launch_fast<4>(a, smem, stream); break;
-            case 5: err = launch_fast<5>(a, smem, stream); break;
-            case 6: err = launch_fast<6>(a, smem, stream); break;
-            case 7: err = launch_fast<7>(a, smem, stream); break;
-            case 8: err = launch_fast<8>(a, smem, stream); break;
+            case 1: err = launch_fast<1>(a, smem, tables, stream); break;
+            case 2: err = launch_fast<2>(a, smem, tables, stream); break;
+            case 3: err = launch_fast<3>(a, smem, tables, stream); break;
+            case 4: err = launch_fast<4>(a, smem, tables, stream); break;
+            case 5: err = launch_fast<5>(a, smem, tables, stream); break;
+            case 6: err = launch_fast<6>(a, smem, tables, stream); break;
+            case 7: err = launch_fast<7>(a, smem, tables, stream); break;
+            case 8: err = launch_fast<8>(a, smem, tables, stream); break;
             default: break;
         }
         if (err != cudaSuccess) return err;
-        ++*launches;
+        *launches += 2;
     }
     SpinTableArgs b = a;
     b.all_careful = fast_ok ? 0 : 1;
