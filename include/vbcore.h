@@ -174,6 +174,29 @@ vb_status vb_hs_plan_determinant_pairs(vb_hs_plan* plan, const double* ovlp_act,
                                        const double* eri_packed, int64_t n_pairs, const int64_t* pairs,
                                        int mem_space, double* h_out, double* s_out);
 
+/* ---- allocation-free spin-pair evaluation ------------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot allocate device memory where
+ * they need the numbers (a serving loop that reserves all HBM up front and forbids allocation
+ * on the request path, or an application whose own allocator owns the device budget): every
+ * unordered pair (u <= v) of one spin-string table is evaluated with the structure plan's
+ * kernels, but all scratch comes from a file-scope 32 MiB device array instead of cudaMalloc
+ * (each GPU that loads the library holds that array until exit).  Tables needing more scratch
+ * than that are rejected with VB_ERR_BUDGET (about 250 strings of 5 electrons in 10 orbitals
+ * fit; use the plan API above for larger ones).
+ *
+ * All pointers are device pointers: strings = n_strings occupation masks (k bits set, orbitals
+ * < n_orbitals), S_act and h (n x n), packed (ij|kl); out_scalars receives, for pair index
+ * t = u N - u (u - 1) / 2 + (v - u), {det, one-electron H, total same-spin H, nullity} at
+ * out_scalars[4 t .. 4 t + 3].  The work is enqueued on `cuda_stream` (the output is complete
+ * when the stream reaches it); the call synchronizes the stream once, midway, to read back
+ * the pair-kernel rank.  The first call on a device looks up the scratch array's address
+ * (cudaGetSymbolAddress) with that device current: make it before any stream capture.  Calls
+ * share the array and keep its last contents; calls that overlap on the GPU race on it. */
+vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, int k, int n_strings, const uint64_t* strings,
+                                const double* ovlp_act, const double* h1e_act, const double* eri_packed,
+                                double* out_scalars);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,7 @@ EXPORTED_SYMBOLS = (
     "vb_context_memory", "vb_generate_structures", "vb_expand_structures", "vb_hs_plan_create",
     "vb_hs_plan_destroy", "vb_hs_plan_execute", "vb_hs_plan_stats", "vb_resolve_overlaps", "vb_same_spin_pairs",
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
+    "vb_spin_pairs_noalloc",
 )
 
 PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
@@ -100,6 +101,7 @@ def load_library(path: str = LIB_PATH):
     lib.vb_hs_plan_enable_phase_timing.argtypes = [P, c.c_int]
     lib.vb_hs_plan_phase_times.argtypes = [P, P, c.c_int]
     lib.vb_resolve_overlaps.argtypes = [P, c.c_int, c.c_int64, P, c.c_int, P, P, P]
+    lib.vb_spin_pairs_noalloc.argtypes = [P, c.c_int, c.c_int, c.c_int, P, P, P, P, P]
     lib.vb_same_spin_pairs.argtypes = [P, c.c_int, c.c_int, c.c_int64, P, P, P, P, P, c.c_int, P, P]
     for name in EXPORTED_SYMBOLS:
         fn = getattr(lib, name)
@@ -267,6 +269,16 @@ class Context:
                                                  _ptr(Sf), _ptr(hf), _ptr(ef), VB_MEM_HOST, _ptr(sc), _ptr(cof)),
                self._h)
         return sc, np.transpose(cof, (0, 2, 1)).copy()
+
+
+def spin_pairs_noalloc(stream_handle: int, n_orbitals: int, k: int, n_strings: int, strings_ptr: int, S_ptr: int,
+                       h_ptr: int, eri_ptr: int, out_ptr: int):
+    """Allocation-free evaluation of every unordered pair of one spin-string table (device
+    pointers; see vb_spin_pairs_noalloc in include/vbcore.h).  Raises VbError on failure."""
+    _check(load_library().vb_spin_pairs_noalloc(ctypes.c_void_p(stream_handle), n_orbitals, k, n_strings,
+                                                ctypes.c_void_p(strings_ptr), ctypes.c_void_p(S_ptr),
+                                                ctypes.c_void_p(h_ptr), ctypes.c_void_p(eri_ptr),
+                                                ctypes.c_void_p(out_ptr)))
 
 
 class HsPlan:
