@@ -128,7 +128,8 @@ vb_status vb_hs_plan_execute(vb_hs_plan* plan, const double* ovlp_act, const dou
                              double* overlap_out);
 
 /* Diagnostics of the last execute: spin pairs evaluated, pairs routed to the exact
- * full-pivot/SVD path, determinant pairs evaluated. */
+ * full-pivot/SVD path, unordered determinant pairs evaluated (with alpha/beta-exchange
+ * symmetry one pair per orbit {(d, e), (flip d, flip e)}), kernel launches. */
 typedef struct {
     int64_t spin_pairs;
     int64_t careful_spin_pairs;

@@ -55,6 +55,23 @@ def test_structure_matrices_match_oracle(ctx, kw, n, seed):
     assert np.array_equal(H, H.T) and np.array_equal(So, So.T)
     st = plan.stats()
     assert st["spin_pairs"] > 0 and st["kernel_launches"] >= 5
+    if n <= 8:
+        # one evaluation per orbit {(d, e), (flip d, flip e)} of unordered pairs (brute force)
+        n_det = ex.n_determinants
+        index = {(int(a), int(b)): d for d, (a, b) in enumerate(zip(ex.det_alpha, ex.det_beta))}
+        flip = [index.get((int(b), int(a))) for a, b in zip(ex.det_alpha, ex.det_beta)]
+        orbits = set()
+        for d in range(n_det):
+            for e in range(d, n_det):
+                if None in (flip[d], flip[e]):
+                    orbits.add((d, e))
+                    continue
+                f = tuple(sorted((flip[d], flip[e])))
+                orbits.add(min((d, e), f))
+        if None in flip:
+            assert st["determinant_pairs"] == n_det * (n_det + 1) // 2
+        else:
+            assert st["determinant_pairs"] == len(orbits)
 
 
 def test_open_shell_tables(ctx):

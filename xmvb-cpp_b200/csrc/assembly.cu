@@ -2,8 +2,9 @@
 //
 // The reference accumulates H_IJ = sum_{d in I, e in J} c_dI c_eJ H_de for left <= right
 // structure pairs and mirrors the upper triangle (hamiltonian_overlap.cpp:437-450, 890-1022).
-// Here the determinant matrix is symmetric and only its upper triangle U (d <= e) is produced,
-// in bands of columns.  With U' = U with halved diagonal, H_d = U' + U'^T, so
+// Here the determinant matrix is symmetric and only its upper triangle is produced, in bands
+// of columns, already weighted by the determinant-pair kernel (U' = upper triangle with halved
+// diagonal, folded over the spin-flip symmetry when present), so that H_d = U' + U'^T and
 //   Z  = T^T U'          (n_str x n_det; one streaming pass over every band, band_reduce)
 //   W  = Z T             (n_str x n_str; structure_reduce)
 //   H  = W + W^T         (symmetrize)
@@ -71,9 +72,8 @@ __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(Band
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 if (d[i] >= row_end) continue;  // padding triples and rows past this column block
-                const double w = (d[i] == e) ? 0.5 * c[i] : c[i];
-                zh[I[i] * kPad + lane] = fma(w, hv[i], zh[I[i] * kPad + lane]);
-                zs[I[i] * kPad + lane] = fma(w, sv[i], zs[I[i] * kPad + lane]);
+                zh[I[i] * kPad + lane] = fma(c[i], hv[i], zh[I[i] * kPad + lane]);
+                zs[I[i] * kPad + lane] = fma(c[i], sv[i], zs[I[i] * kPad + lane]);
             }
         }
     }

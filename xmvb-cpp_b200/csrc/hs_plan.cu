@@ -48,6 +48,10 @@ struct vb_hs_plan {
     DeviceBuffer Zh, Zs, Wh, Ws, Hout, Sout;
     DeviceBuffer str_off, str_det, str_coef;
     std::vector<StructureChunk> chunks;
+    // spin-flip map of the determinant list (folds the determinant-pair work in half)
+    DeviceBuffer flip;
+    bool has_flip = false;
+    long long det_pair_evaluations = 0;  // unordered determinant pairs evaluated (orbit representatives)
     vb_hs_stats stats{};
     bool evaluated = false;
     // phase timing: per phase a pool of (start, stop) event pairs, `used` pairs this execute
@@ -249,6 +253,53 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     if ((st = p->fmeta.allocate(ctx, sizeof(int) * 2)) != VB_OK) return fail(st);
     if (cudaMallocHost(&p->meta_host, sizeof(int) * 2) != cudaSuccess) return fail(set_error(ctx, VB_ERR_CUDA, "cudaMallocHost"));
 
+    // spin-flip map: determinant with the alpha and beta strings exchanged; usable when every
+    // determinant's image exists and carries the same structure coefficients
+    std::vector<int> flipmap;
+    if (p->shared_tables) {
+        std::vector<long long> key(p->n_det);
+        for (long long d = 0; d < p->n_det; ++d) key[d] = (long long)ex->det_alpha[d] * p->Na + ex->det_beta[d];
+        std::vector<long long> order(p->n_det);
+        for (long long d = 0; d < p->n_det; ++d) order[d] = d;
+        std::sort(order.begin(), order.end(), [&](long long x, long long y) { return key[x] < key[y]; });
+        flipmap.assign(p->n_det, -1);
+        bool ok = true;
+        for (long long d = 0; d < p->n_det && ok; ++d) {
+            const long long want = (long long)ex->det_beta[d] * p->Na + ex->det_alpha[d];
+            auto it = std::lower_bound(order.begin(), order.end(), want,
+                                       [&](long long idx, long long v) { return key[idx] < v; });
+            if (it == order.end() || key[*it] != want) {
+                ok = false;
+                break;
+            }
+            const long long f = *it;
+            flipmap[d] = (int)f;
+            const long long n1 = ex->term_offsets[d + 1] - ex->term_offsets[d];
+            const long long n2 = ex->term_offsets[f + 1] - ex->term_offsets[f];
+            if (n1 != n2) {
+                ok = false;
+                break;
+            }
+            for (long long q = 0; q < n1; ++q)
+                if (ex->term_structure[ex->term_offsets[d] + q] != ex->term_structure[ex->term_offsets[f] + q] ||
+                    ex->term_coefficient[ex->term_offsets[d] + q] != ex->term_coefficient[ex->term_offsets[f] + q]) {
+                    ok = false;
+                    break;
+                }
+        }
+        if (ok) {
+            p->has_flip = true;
+            // orbits of unordered pairs {d, e} under the flip (Burnside): (P + fixed pairs) / 2
+            long long fixed_dets = 0;
+            for (long long d = 0; d < p->n_det; ++d) fixed_dets += flipmap[d] == d;
+            const long long P = p->n_det * (p->n_det + 1) / 2;
+            p->det_pair_evaluations = (P + fixed_dets * (fixed_dets + 1) / 2 + (p->n_det - fixed_dets) / 2) / 2;
+            if ((st = upload(ctx, p->flip, flipmap.data(), sizeof(int) * p->n_det)) != VB_OK) return fail(st);
+        }
+    }
+
+    if (!p->has_flip) p->det_pair_evaluations = p->n_det * (p->n_det + 1) / 2;
+
     // band of determinant columns: keep the two band buffers within ~4 GB and 1/4 of the budget
     const size_t band_cap = std::min<size_t>((size_t)4 << 30, ctx->budget / 4);
     long long width = (long long)(band_cap / (16 * (size_t)p->n_det));
@@ -440,6 +491,7 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
     vb_status st = prepare_spin_records(p, S, h, eri, mem, &dS, &dh, &deri, &launches);
     if (st != VB_OK) return st;
     FullPairArgs fa = full_args(p);
+    fa.flip = p->has_flip ? p->flip.as<int>() : nullptr;
     for (long long e0 = 0; e0 < p->n_det; e0 += p->band_width) {
         const long long e1 = std::min(p->n_det, e0 + p->band_width);
         const long long B = e1 - e0;
@@ -497,7 +549,7 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
         if (err != cudaSuccess) return cuda_error(ctx, err, "result download");
     }
     p->stats.spin_pairs = p->npairs_a + p->npairs_b;
-    p->stats.determinant_pairs = p->n_det * (p->n_det + 1) / 2;
+    p->stats.determinant_pairs = p->det_pair_evaluations;
     p->stats.kernel_launches = launches;
     p->evaluated = true;
     return VB_OK;

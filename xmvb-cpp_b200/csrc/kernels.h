@@ -54,6 +54,7 @@ struct FullPairArgs {
     long long n_items;    // determinant pairs (d <= e) in the band
     double* Hb;           // band, row-major: Hb[d * (e1 - e0) + (e - e0)], valid for d <= e
     double* Sb;
+    const int* flip;      // spin-flip permutation of determinants (nullptr: no folding)
 };
 
 struct BandReduceArgs {

@@ -23,6 +23,7 @@
 
 #include "device_algebra.cuh"
 #include "kernels.h"
+#include "pair_value.cuh"
 
 namespace vbcore {
 namespace {
@@ -70,29 +71,32 @@ __global__ void prepare_tables_kernel(int n, const double* __restrict__ eri, dou
 // Stops when the largest remaining |diagonal| falls to rel_tol times the largest initial one;
 // the dropped remainder then perturbs any opposite-spin energy by at most
 // rel_tol * max|K_pp| * ||p_a||_1 ||p_b||_1.  Columns are emitted positive-sign first.
+// The working matrix lives in shared memory when it fits (in_smem), else in `work`.
 __global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* __restrict__ kfull,
-                                                          double* __restrict__ work, double* __restrict__ cols,
+                                                          double* __restrict__ work_g, double* __restrict__ cols,
                                                           int* __restrict__ signs, double* __restrict__ lf, int ld,
-                                                          int* __restrict__ meta, double rel_tol) {
-    extern __shared__ unsigned char fsm[];
-    int* used = reinterpret_cast<int*>(fsm);
+                                                          int* __restrict__ meta, double rel_tol, int in_smem) {
+    extern __shared__ double fsm[];
+    double* work = in_smem ? fsm : work_g;
+    int* used = reinterpret_cast<int*>(in_smem ? fsm + (size_t)np * np : fsm);
+    int* slot_col = used + np;  // emission map: output slot -> column
     __shared__ double red_v[32];
     __shared__ int red_i[32];
     __shared__ double s_piv;
     __shared__ int s_p;
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nwarps = nt >> 5;
     const long long n2 = (long long)np * np;
     for (long long i = tid; i < n2; i += nt) work[i] = kfull[i];
     for (int i = tid; i < np; i += nt) used[i] = 0;
     __syncthreads();
-    // largest initial |diagonal|
     double local = 0.0;
     for (int i = tid; i < np; i += nt) local = fmax(local, fabs(work[(long long)i * np + i]));
     for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(0xffffffffu, local, o));
-    if ((tid & 31) == 0) red_v[tid >> 5] = local;
+    if (lane == 0) red_v[warp] = local;
     __syncthreads();
     if (tid < 32) {
-        double v = tid < (nt >> 5) ? red_v[tid] : 0.0;
+        double v = tid < nwarps ? red_v[tid] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
         if (tid == 0) s_piv = v;
     }
@@ -118,14 +122,14 @@ __global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* 
                 bi = oi;
             }
         }
-        if ((tid & 31) == 0) {
-            red_v[tid >> 5] = best;
-            red_i[tid >> 5] = bi;
+        if (lane == 0) {
+            red_v[warp] = best;
+            red_i[warp] = bi;
         }
         __syncthreads();
         if (tid < 32) {
-            double v = tid < (nt >> 5) ? red_v[tid] : -1.0;
-            int vi = tid < (nt >> 5) ? red_i[tid] : -1;
+            double v = tid < nwarps ? red_v[tid] : -1.0;
+            int vi = tid < nwarps ? red_i[tid] : -1;
             for (int o = 16; o > 0; o >>= 1) {
                 const double ov = __shfl_xor_sync(0xffffffffu, v, o);
                 const int oi = __shfl_xor_sync(0xffffffffu, vi, o);
@@ -145,56 +149,55 @@ __global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* 
         if (p < 0 || !(fabs(piv) > cut) || fabs(piv) == 0.0) break;
         const double inv = 1.0 / sqrt(fabs(piv));
         const int sgn = piv > 0.0 ? 1 : -1;
-        for (int i = tid; i < np; i += nt) cols[(long long)m * np + i] = used[i] ? 0.0 : work[(long long)i * np + p] * inv;
+        double* l = cols + (long long)m * np;
+        for (int i = tid; i < np; i += nt) l[i] = used[i] ? 0.0 : work[(long long)i * np + p] * inv;
         if (tid == 0) signs[m] = sgn;
         __syncthreads();
         if (tid == 0) used[p] = 1;
         __syncthreads();
-        const double* l = cols + (long long)m * np;
-        for (long long idx = tid; idx < n2; idx += nt) {
-            const int i = (int)(idx / np), j = (int)(idx % np);
-            if (!used[i] && !used[j]) work[idx] -= (double)sgn * l[i] * l[j];
+        // rank-1 update of the remaining block, one warp per row
+        for (int i = warp; i < np; i += nwarps) {
+            if (used[i]) continue;
+            const double li = (double)sgn * l[i];
+            double* row = work + (long long)i * np;
+            for (int j = lane; j < np; j += 32)
+                if (!used[j]) row[j] = fma(-li, l[j], row[j]);
         }
         __syncthreads();
     }
-    // emit: positive-sign columns first, then negative, zero padding up to ld
-    int pos = 0;
-    for (int c = 0; c < m; ++c) pos += signs[c] > 0 ? 1 : 0;
-    for (long long idx = tid; idx < (long long)np * ld; idx += nt) {
-        const int q = (int)(idx / ld), slot = (int)(idx % ld);
-        double v = 0.0;
-        if (slot < m) {
-            // find the column that lands in `slot`
-            int c = -1, seen_pos = 0, seen_neg = 0;
-            for (int t = 0; t < m; ++t) {
-                if (signs[t] > 0) {
-                    if (seen_pos == slot) { c = t; break; }
-                    ++seen_pos;
-                } else {
-                    if (pos + seen_neg == slot) { c = t; break; }
-                    ++seen_neg;
-                }
-            }
-            if (c >= 0) v = cols[(long long)c * np + q];
-        }
-        lf[idx] = v;
-    }
     if (tid == 0) {
+        int pos = 0;
+        for (int c = 0; c < m; ++c) pos += signs[c] > 0 ? 1 : 0;
+        int ip = 0, in = pos;
+        for (int c = 0; c < m; ++c) slot_col[signs[c] > 0 ? ip++ : in++] = c;
         meta[0] = pos;
         meta[1] = m - pos;
     }
-}
-
-__device__ __forceinline__ long long record_index(long long u, long long v, long long N) {
-    return u * N - u * (u - 1) / 2 + (v - u);
+    __syncthreads();
+    for (int q = warp; q < np; q += nwarps)
+        for (int slot = lane; slot < ld; slot += 32)
+            lf[(long long)q * ld + slot] = slot < m ? cols[(long long)slot_col[slot] * np + q] : 0.0;
 }
 
 // Table geometry of the left-string decomposition (shared by host and device code).
+//   nb_max(K)   complement orbitals held per left string (n - K <= nb_max)
+//   kf(K)       GEMM depth: nb_max K entries of V, one trace slot, padded to 4
+//   kfs(K)      shared-memory row stride >= kf with stride % 16 in {4, 12} (conflict-free
+//               m8n8k4 fragment loads: the four rows of a half-warp land on disjoint banks)
+//   nt_of(R)    8-row tiles covering the R + 1 table rows (factor columns and h)
 __host__ __device__ constexpr int nb_max(int k) { return k <= 4 ? k + 4 : k; }
-__host__ __device__ constexpr int even_up(int x) { return (x + 1) / 2 * 2; }
-__host__ __device__ constexpr int table_block(int k) { return even_up(nb_max(k) * k); }
-__host__ __device__ constexpr int table_head(int R) { return even_up(R + 1); }
-__host__ __device__ constexpr int table_stride_of(int k, int R) { return table_head(R) + (R + 1) * table_block(k); }
+__host__ __device__ constexpr int kf(int k) { return (nb_max(k) * k + 1 + 3) / 4 * 4; }
+__host__ __device__ constexpr int kfs(int k) {
+    return (kf(k) % 16 == 4 || kf(k) % 16 == 12) ? kf(k) : kf(k) + 4;
+}
+__host__ __device__ constexpr int nt_of(int R) { return (R + 1 + 7) / 8; }
+__host__ __device__ constexpr int table_stride_of(int k, int R) { return nt_of(R) * 8 * kfs(k); }
+
+__device__ __forceinline__ void mma_f64(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
 
 // Complement decomposition per left string L (K orbitals; Lbar = the other NB = n - K orbitals).
 // For a right string R with X = S[R, L], any n x K block W gives
@@ -202,22 +205,24 @@ __host__ __device__ constexpr int table_stride_of(int k, int R) { return table_h
 // with T = S[L,L]^{-1} W[L,:], V = W[Lbar,:] - S[Lbar,L] T, and Y = X^{-1} I[R, Lbar], a column
 // selection of X^{-1}.  With W = B_m[:, L] (B_m[i][j] = lf(pair(i, j), m)) this is
 // u[m] / det, and with W = h[:, L] it is H_1e / det (Jacobi's formula: both are first-order
-// terms sum_{r,c} A(r,c) W(R_r, L_c) of det(X + eps W[R, :])).  T and V depend on L only, so the
-// per-pair work is K NB fused multiply-adds per column against warp-uniform table entries.
+// terms sum_{r,c} A(r,c) W(R_r, L_c) of det(X + eps W[R, :])).  T and V depend on L only.
 //
-// Table of left string L, (R + 1) blocks (m < R factor columns, m = R one-electron h):
-//   [m] trace T_m (head of table_head(R) doubles), then block m at table_head(R) + m * vb:
-//   V_m[b][c] (b < nb_max(K) rows, c fastest, zero rows for b >= NB, zero padding to vb).
+// Table of left string L: row m (m < R factor columns, m = R one-electron h) of kfs(K) doubles
+// holds V_m[b][c] at b K + c (b < nb_max(K), zero rows for b >= NB), tr T_m at nb_max(K) K,
+// zeros elsewhere; rows R + 1 .. 8 nt_of(R) - 1 are zero.
 template <int K>
 __global__ void __launch_bounds__(128) left_string_tables(SpinTableArgs a, double* __restrict__ tables) {
-    constexpr int vb = table_block(K);
+    constexpr int NBMAX = nb_max(K);
+    constexpr int KFS = kfs(K);
     const int table_stride = table_stride_of(K, a.R);
     __shared__ double sInv[K * K];
-    __shared__ int sL[K], sLb[32];
+    __shared__ int sL[K], sLb[NBMAX];
     const int n = a.n;
     const int nb = n - K;
     const long long u = blockIdx.x;
     if (u >= a.n_strings) return;
+    double* tab = tables + u * (long long)table_stride;
+    for (int i = threadIdx.x; i < table_stride; i += blockDim.x) tab[i] = 0.0;
     if (threadIdx.x == 0) {
         const uint64_t w0 = a.occ[2 * u];
         int L[K];
@@ -227,9 +232,9 @@ __global__ void __launch_bounds__(128) left_string_tables(SpinTableArgs a, doubl
 #pragma unroll
         for (int c = 0; c < K; ++c) mask |= 1ull << L[c];
         int q = 0;
-        for (int i = 0; i < n; ++i)
+        for (int i = 0; i < n && q < NBMAX; ++i)
             if (!((mask >> i) & 1)) sLb[q++] = i;
-        // S[L, L]^{-1}: Gauss-Jordan with partial pivoting (S[L, L] is a principal block of an SPD matrix)
+        // S[L, L]^{-1} by Gauss-Jordan (S[L, L] is a principal block of an SPD matrix)
         double m[K][2 * K];
 #pragma unroll
         for (int r = 0; r < K; ++r)
@@ -256,17 +261,17 @@ __global__ void __launch_bounds__(128) left_string_tables(SpinTableArgs a, doubl
         }
     }
     __syncthreads();
-    double* tab = tables + u * (long long)table_stride;
     const int blocks = a.R + 1;
-    const int head = table_head(a.R);
-    // one thread per (block m, column c): T[:, c] then V[:, c]
+    // one thread per (row m, column c): T[:, c] then V[:, c]; the c == 0 thread adds tr T_m
     for (int idx = threadIdx.x; idx < blocks * K; idx += blockDim.x) {
         const int mm = idx / K, c = idx % K;
+        auto wval = [&](int i, int j) {
+            return mm < a.R ? __ldg(a.lf + (long long)dev::pair_index(i, j) * a.ld + mm) : __ldg(a.h + i * n + j);
+        };
         const int lc = sL[c];
         double wl[K];
 #pragma unroll
-        for (int ap = 0; ap < K; ++ap)
-            wl[ap] = mm < a.R ? a.lf[(long long)dev::pair_index(sL[ap], lc) * a.ld + mm] : a.h[sL[ap] * n + lc];
+        for (int ap = 0; ap < K; ++ap) wl[ap] = wval(sL[ap], lc);
         double tc[K];
 #pragma unroll
         for (int r = 0; r < K; ++r) {
@@ -275,56 +280,51 @@ __global__ void __launch_bounds__(128) left_string_tables(SpinTableArgs a, doubl
             for (int ap = 0; ap < K; ++ap) acc = fma(sInv[r * K + ap], wl[ap], acc);
             tc[r] = acc;
         }
-        double* vblk = tab + head + (long long)mm * vb;
-        for (int b = 0; b < nb_max(K); ++b) {
-            if (b >= nb) {
-                vblk[b * K + c] = 0.0;
-                continue;
-            }
+        double* row = tab + (long long)mm * KFS;
+        for (int b = 0; b < nb && b < NBMAX; ++b) {
             const int ib = sLb[b];
-            double acc = mm < a.R ? a.lf[(long long)dev::pair_index(ib, lc) * a.ld + mm] : a.h[ib * n + lc];
+            double acc = wval(ib, lc);
 #pragma unroll
-            for (int r = 0; r < K; ++r) acc = fma(-a.S[ib * n + sL[r]], tc[r], acc);
-            vblk[b * K + c] = acc;
+            for (int r = 0; r < K; ++r) acc = fma(-__ldg(a.S + ib * n + sL[r]), tc[r], acc);
+            row[b * K + c] = acc;
         }
         if (c == 0) {
-            // the diagonal of T needs every column: recompute it (K^2 fused multiply-adds)
             double tr = 0.0;
             for (int cc = 0; cc < K; ++cc) {
                 const int l2 = sL[cc];
                 double acc = 0.0;
 #pragma unroll
-                for (int ap = 0; ap < K; ++ap) {
-                    const double w = mm < a.R ? a.lf[(long long)dev::pair_index(sL[ap], l2) * a.ld + mm]
-                                              : a.h[sL[ap] * n + l2];
-                    acc = fma(sInv[cc * K + ap], w, acc);
-                }
+                for (int ap = 0; ap < K; ++ap) acc = fma(sInv[cc * K + ap], wval(sL[ap], l2), acc);
                 tr += acc;
             }
-            tab[mm] = tr;
+            row[NBMAX * K] = tr;
         }
-        for (int pad = nb_max(K) * K; pad < vb; ++pad)
-            if (c == 0) vblk[pad] = 0.0;
     }
-    for (int pad = blocks + threadIdx.x; pad < head; pad += blockDim.x) tab[pad] = 0.0;
 }
 
 // One CTA per contiguous range of work items (left string u, right strings v0 .. v0 + 127);
 // the left string's tables live in shared memory and are reloaded only when u changes.
+// Phase A (a thread per spin pair): overlap block, Gauss-Jordan inverse, certificate, the
+// same-spin two-electron term, and the row Y of the pair (with 1 in the trace slot) to shared
+// memory.  Phase B (a warp per 32 pairs): [u | H_1e] / det = Y V^T on the FP64 tensor cores
+// (mma.sync m8n8k4), then the records.
 template <int K>
 __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a, const double* __restrict__ tables) {
     extern __shared__ double smem[];
     constexpr int CP = K * (K - 1) / 2;
     constexpr int NBMAX = nb_max(K);
-    constexpr int vb = table_block(K);
+    constexpr int KF = kf(K);
+    constexpr int KFS = kfs(K);
     const int n = a.n;
     const int nb = n - K;
     const int gd = a.gamma_dim;
-    const int table_stride = table_stride_of(K, a.R);
-    const int head = table_head(a.R);
-    double* sT = smem;                                // left-string table (t, V blocks), 16-byte aligned
-    double* sS = sT + table_stride;                   // [c][i] = S(i, L_c)
-    double* sG = sS + even_up(K * n);                 // [cp][rp] = gamma(rp, pair(L_c1, L_c2))
+    const int R = a.R;
+    const int NT = nt_of(R);
+    const int table_stride = table_stride_of(K, R);
+    double* sT = smem;                                // left-string table, row m = block m
+    double* sY = sT + table_stride;                   // [pair][f] rows of Y
+    double* sS = sY + kSpinBlock * KFS;               // [c][i] = S(i, L_c)
+    double* sG = sS + ((K * n + 1) / 2 * 2);          // [cp][rp] = gamma(rp, pair(L_c1, L_c2))
     __shared__ int sLb[NBMAX];
     const long long N = a.n_strings;
     const int per = (a.n_items + gridDim.x - 1) / gridDim.x;
@@ -376,195 +376,236 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a, c
             loaded_u = u;
             __syncthreads();
         }
+        // ---------------- phase A ----------------
         const long long v = (long long)it.y + threadIdx.x;
-        if (v >= N) continue;
-        const long long t = record_index(u, v, N);
-        const uint64_t wr = __ldg(a.occ + 2 * v);
-        int R[K];
+        bool ok = false;
+        double det = 0.0, h2 = 0.0;
+        long long t = 0;
+        double* yrow = sY + threadIdx.x * KFS;
+        if (v < N) {
+            t = record_index(u, v, N);
+            const uint64_t wr = __ldg(a.occ + 2 * v);
+            int Rr[K];
 #pragma unroll
-        for (int c = 0; c < K; ++c) R[c] = (int)((wr >> (8 * c)) & 0xFFu);
-        double x[K][K];
-        double nx2 = 0.0;
+            for (int c = 0; c < K; ++c) Rr[c] = (int)((wr >> (8 * c)) & 0xFFu);
+            double x[K][K];
+            double nx2 = 0.0;
 #pragma unroll
-        for (int r = 0; r < K; ++r)
+            for (int r = 0; r < K; ++r)
 #pragma unroll
-            for (int c = 0; c < K; ++c) {
-                x[r][c] = sS[c * n + R[r]];
-                nx2 = fma(x[r][c], x[r][c], nx2);
+                for (int c = 0; c < K; ++c) {
+                    x[r][c] = sS[c * n + Rr[r]];
+                    nx2 = fma(x[r][c], x[r][c], nx2);
+                }
+            constexpr int K0 = K <= 3 ? K : 1;
+            double x0[K0][K0];
+            if (K <= 3) {
+#pragma unroll
+                for (int r = 0; r < K0; ++r)
+#pragma unroll
+                    for (int c = 0; c < K0; ++c) x0[r][c] = x[r][c];
             }
-        constexpr int K0 = K <= 3 ? K : 1;
-        double x0[K0][K0];
-        if (K <= 3) {
+            int lab[K];
 #pragma unroll
-            for (int r = 0; r < K0; ++r)
+            for (int r = 0; r < K; ++r) lab[r] = r;
+            det = 1.0;
 #pragma unroll
-                for (int c = 0; c < K0; ++c) x0[r][c] = x[r][c];
-        }
-        int lab[K];
+            for (int s = 0; s < K; ++s) {
+                int p = s;
+                double best = fabs(x[s][s]);
 #pragma unroll
-        for (int r = 0; r < K; ++r) lab[r] = r;
-        double det = 1.0;
+                for (int i = s + 1; i < K; ++i) {
+                    const double av = fabs(x[i][s]);
+                    if (av > best) {
+                        best = av;
+                        p = i;
+                    }
+                }
 #pragma unroll
-        for (int s = 0; s < K; ++s) {
-            int p = s;
-            double best = fabs(x[s][s]);
+                for (int i = s + 1; i < K; ++i) {
+                    const bool sw = (p == i);
 #pragma unroll
-            for (int i = s + 1; i < K; ++i) {
-                const double av = fabs(x[i][s]);
-                if (av > best) {
-                    best = av;
-                    p = i;
+                    for (int j = 0; j < K; ++j) {
+                        const double a0 = x[s][j], a1 = x[i][j];
+                        x[s][j] = sw ? a1 : a0;
+                        x[i][j] = sw ? a0 : a1;
+                    }
+                    const int l0 = lab[s], l1 = lab[i];
+                    lab[s] = sw ? l1 : l0;
+                    lab[i] = sw ? l0 : l1;
+                }
+                if (p != s) det = -det;
+                const double piv = x[s][s];
+                det *= piv;
+                const double ip = 1.0 / piv;
+                x[s][s] = 1.0;
+#pragma unroll
+                for (int j = 0; j < K; ++j) x[s][j] *= ip;
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    if (i == s) continue;
+                    const double f = x[i][s];
+                    x[i][s] = 0.0;
+#pragma unroll
+                    for (int j = 0; j < K; ++j) x[i][j] = fma(-f, x[s][j], x[i][j]);
                 }
             }
+            double ni2 = 0.0;
 #pragma unroll
-            for (int i = s + 1; i < K; ++i) {
-                const bool sw = (p == i);
+            for (int r = 0; r < K; ++r)
 #pragma unroll
-                for (int j = 0; j < K; ++j) {
-                    const double a0 = x[s][j], a1 = x[i][j];
-                    x[s][j] = sw ? a1 : a0;
-                    x[i][j] = sw ? a0 : a1;
-                }
-                const int l0 = lab[s], l1 = lab[i];
-                lab[s] = sw ? l1 : l0;
-                lab[i] = sw ? l0 : l1;
-            }
-            if (p != s) det = -det;
-            const double piv = x[s][s];
-            det *= piv;
-            const double ip = 1.0 / piv;
-            x[s][s] = 1.0;
+                for (int c = 0; c < K; ++c) ni2 = fma(x[r][c], x[r][c], ni2);
+            ok = isfinite(det) && det != 0.0 && (nx2 * ni2 < kCertificate2);
+            if (!ok) {
+                const unsigned long long slot = atomicAdd(a.careful_count, 1ull);
+                a.careful_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
 #pragma unroll
-            for (int j = 0; j < K; ++j) x[s][j] *= ip;
+                for (int f = 0; f < KFS; ++f) yrow[f] = 0.0;
+            } else {
+                // x holds C = (P X)^{-1}: X^{-1}[c][lab[j]] = C[c][j]; row lab[j] carries orbital Rp[j]
+                int Rp[K];
 #pragma unroll
-            for (int i = 0; i < K; ++i) {
-                if (i == s) continue;
-                const double f = x[i][s];
-                x[i][s] = 0.0;
+                for (int j = 0; j < K; ++j) Rp[j] = (int)((wr >> (8 * lab[j])) & 0xFFu);
+                if (K == 2) {
+                    h2 = sG[dev::anti_index(Rr[0], Rr[1])];
+                } else if (K == 3) {
 #pragma unroll
-                for (int j = 0; j < K; ++j) x[i][j] = fma(-f, x[s][j], x[i][j]);
-            }
-        }
-        double ni2 = 0.0;
+                    for (int r1 = 0; r1 < K0; ++r1)
 #pragma unroll
-        for (int r = 0; r < K; ++r)
+                        for (int r2 = r1 + 1; r2 < K0; ++r2)
 #pragma unroll
-            for (int c = 0; c < K; ++c) ni2 = fma(x[r][c], x[r][c], ni2);
-        const bool accepted = isfinite(det) && det != 0.0 && (nx2 * ni2 < kCertificate2);
-        if (!accepted) {
-            const unsigned long long slot = atomicAdd(a.careful_count, 1ull);
-            a.careful_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
-            continue;
-        }
-        double* rec = a.records + t * (long long)a.rec_stride;
-        // x holds C = (P X)^{-1}: X^{-1}[c][lab[j]] = C[c][j]; row lab[j] carries orbital Rp[j]
-        int Rp[K];
+                            for (int c1 = 0; c1 < K0; ++c1)
 #pragma unroll
-        for (int j = 0; j < K; ++j) Rp[j] = (int)((wr >> (8 * lab[j])) & 0xFFu);
-        double h2 = 0.0;
-        if (K == 2) {
-            h2 = sG[dev::anti_index(R[0], R[1])];
-        } else if (K == 3) {
+                                for (int c2 = c1 + 1; c2 < K0; ++c2) {
+                                    const double sign = ((r1 + r2 + c1 + c2) & 1) ? -1.0 : 1.0;
+                                    const int cp = c2 * (c2 - 1) / 2 + c1;
+                                    h2 = fma(sG[cp * gd + dev::anti_index(Rr[r1], Rr[r2])],
+                                             sign * x0[3 - r1 - r2][3 - c1 - c2], h2);
+                                }
+                } else if (K >= 4) {
+                    double acc2 = 0.0;
 #pragma unroll
-            for (int r1 = 0; r1 < K0; ++r1)
+                    for (int j1 = 0; j1 < K; ++j1)
 #pragma unroll
-                for (int r2 = r1 + 1; r2 < K0; ++r2)
+                        for (int j2 = j1 + 1; j2 < K; ++j2) {
+                            const int ra = Rp[j1], rb = Rp[j2];
+                            const bool ordered = ra < rb;
+                            const int rp = dev::anti_index(ordered ? ra : rb, ordered ? rb : ra);
+                            double part = 0.0;
 #pragma unroll
-                    for (int c1 = 0; c1 < K0; ++c1)
+                            for (int c1 = 0; c1 < K; ++c1)
 #pragma unroll
-                        for (int c2 = c1 + 1; c2 < K0; ++c2) {
-                            const double sign = ((r1 + r2 + c1 + c2) & 1) ? -1.0 : 1.0;
-                            const int cp = c2 * (c2 - 1) / 2 + c1;
-                            h2 = fma(sG[cp * gd + dev::anti_index(R[r1], R[r2])], sign * x0[3 - r1 - r2][3 - c1 - c2],
-                                     h2);
+                                for (int c2 = c1 + 1; c2 < K; ++c2) {
+                                    const double m2 = fma(x[c1][j1], x[c2][j2], -x[c2][j1] * x[c1][j2]);
+                                    part = fma(sG[(c2 * (c2 - 1) / 2 + c1) * gd + rp], m2, part);
+                                }
+                            acc2 += ordered ? part : -part;
                         }
-        } else if (K >= 4) {
-            double acc2 = 0.0;
-#pragma unroll
-            for (int j1 = 0; j1 < K; ++j1)
-#pragma unroll
-                for (int j2 = j1 + 1; j2 < K; ++j2) {
-                    const int ra = Rp[j1], rb = Rp[j2];
-                    const bool ordered = ra < rb;
-                    const int rp = dev::anti_index(ordered ? ra : rb, ordered ? rb : ra);
-                    double part = 0.0;
-#pragma unroll
-                    for (int c1 = 0; c1 < K; ++c1)
-#pragma unroll
-                        for (int c2 = c1 + 1; c2 < K; ++c2) {
-                            const double m2 = fma(x[c1][j1], x[c2][j2], -x[c2][j1] * x[c1][j2]);
-                            part = fma(sG[(c2 * (c2 - 1) / 2 + c1) * gd + rp], m2, part);
-                        }
-                    acc2 += ordered ? part : -part;
+                    h2 = det * acc2;
                 }
-            h2 = det * acc2;
+                // Y[b K + c] = X^{-1}[c][r] for the row r carrying orbital Lbar_b (0 if Lbar_b not in R)
+#pragma unroll
+                for (int b = 0; b < NBMAX; ++b) {
+                    const int ib = b < nb ? sLb[b] : -1;
+#pragma unroll
+                    for (int c = 0; c < K; ++c) {
+                        double y = 0.0;
+#pragma unroll
+                        for (int j = 0; j < K; ++j) y = (Rp[j] == ib) ? x[c][j] : y;
+                        yrow[b * K + c] = y;
+                    }
+                }
+                yrow[NBMAX * K] = 1.0;
+#pragma unroll
+                for (int f = NBMAX * K + 1; f < KFS; ++f) yrow[f] = 0.0;
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < KFS; ++f) yrow[f] = 0.0;
         }
-        // Y[b * K + c] = X^{-1}[c][r] for the row r carrying orbital Lbar_b (zero when Lbar_b is not in R)
-        double Y[vb];
+        __syncwarp();
+        // ---------------- phase B ----------------
+        const double* Yw = sY + (warp * 32) * KFS;
+        const int g = lane >> 2, tq = lane & 3;
+        double det_m[4], h2_m[4];
+        long long t_m[4];
+        bool ok_m[4];
 #pragma unroll
-        for (int b = 0; b < NBMAX; ++b) {
-            const int ib = b < nb ? sLb[b] : -1;
+        for (int mt = 0; mt < 4; ++mt) {
+            det_m[mt] = __shfl_sync(0xffffffffu, det, 8 * mt + g);
+            h2_m[mt] = __shfl_sync(0xffffffffu, h2, 8 * mt + g);
+            t_m[mt] = __shfl_sync(0xffffffffu, t, 8 * mt + g);
+            ok_m[mt] = __shfl_sync(0xffffffffu, (int)ok, 8 * mt + g) != 0;
+        }
+        for (int nt0 = 0; nt0 < NT; nt0 += 6) {
+            double acc[4][6][2];
 #pragma unroll
-            for (int c = 0; c < K; ++c) {
-                double y = 0.0;
+            for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-                for (int j = 0; j < K; ++j) y = (Rp[j] == ib) ? x[c][j] : y;
-                Y[b * K + c] = y;
+                for (int j = 0; j < 6; ++j) acc[mt][j][0] = acc[mt][j][1] = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < KF / 4; ++ks) {
+                double af[4], bf[6];
+#pragma unroll
+                for (int mt = 0; mt < 4; ++mt) af[mt] = Yw[(8 * mt + g) * KFS + 4 * ks + tq];
+#pragma unroll
+                for (int j = 0; j < 6; ++j)
+                    bf[j] = (nt0 + j < NT) ? sT[(8 * (nt0 + j) + g) * KFS + 4 * ks + tq] : 0.0;
+#pragma unroll
+                for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) mma_f64(acc[mt][j], af[mt], bf[j]);
+            }
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) {
+                if (!ok_m[mt]) continue;
+                double* rec = a.records + t_m[mt] * (long long)a.rec_stride;
+#pragma unroll
+                for (int j = 0; j < 6; ++j)
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const int col = 8 * (nt0 + j) + 2 * tq + i;
+                        const double val = det_m[mt] * acc[mt][j][i];
+                        if (col < R) {
+                            rec[col] = val;
+                        } else if (col == R) {
+                            rec[R + 0] = det_m[mt];
+                            rec[R + 1] = val + h2_m[mt];
+                            rec[R + 2] = val;
+                            rec[R + 3] = 0.0;
+                        }
+                    }
             }
         }
-#pragma unroll
-        for (int f = NBMAX * K; f < vb; ++f) Y[f] = 0.0;
-        // one-electron energy and the u-vector: det (tr T_m + sum_f Y[f] V_m[f]), V_m read as
-        // warp-uniform 16-byte shared-memory loads
-        double h1;
-        {
-            const double2* vblk = reinterpret_cast<const double2*>(sT + head + a.R * vb);
-            double acc = sT[a.R];
-#pragma unroll
-            for (int f = 0; f < vb; f += 2) {
-                const double2 w = vblk[f >> 1];
-                acc = fma(Y[f], w.x, acc);
-                acc = fma(Y[f + 1], w.y, acc);
-            }
-            h1 = det * acc;
-        }
-        for (int m = 0; m < a.R; ++m) {
-            const double2* vblk = reinterpret_cast<const double2*>(sT + head + m * vb);
-            double acc0 = sT[m], acc1 = 0.0;
-#pragma unroll
-            for (int f = 0; f < vb; f += 2) {
-                const double2 w = vblk[f >> 1];
-                acc0 = fma(Y[f], w.x, acc0);
-                acc1 = fma(Y[f + 1], w.y, acc1);
-            }
-            rec[m] = det * (acc0 + acc1);
-        }
-        rec[a.R + 0] = det;
-        rec[a.R + 1] = h1 + h2;
-        rec[a.R + 2] = h1;
-        rec[a.R + 3] = 0.0;
+        __syncwarp();
     }
 }
 
+__device__ __forceinline__ void unanti(int p, int* a, int* b) {
+    int hi = 1;
+    while ((hi + 1) * hi / 2 <= p) ++hi;
+    *b = hi;
+    *a = p - hi * (hi - 1) / 2;
+}
+
+// One warp per listed pair: every lane resolves the block (same result), then the lanes split
+// the one- and two-electron terms and the u-vector entries; sums are reduced across the warp.
 __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
     const long long count = a.all_careful ? a.n_pairs : (long long)(*a.careful_count);
-    const long long stride = (long long)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const int k = a.k;
     const long long N = a.n_strings;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < count; idx += stride) {
+    for (long long idx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < count; idx += nwarps) {
         long long u, v;
         if (a.all_careful) {
-            // idx enumerates pairs row by row: decode the row-major upper packing
             long long uu = 0;
-            {
-                // offset(u) = u N - u (u - 1) / 2; solve offset(u) <= idx < offset(u + 1)
-                const double b = 2.0 * (double)N + 1.0;
-                uu = (long long)floor((b - sqrt(fmax(b * b - 8.0 * (double)idx, 0.0))) * 0.5);
-                if (uu < 0) uu = 0;
-                if (uu > N - 1) uu = N - 1;
-                while (uu > 0 && uu * N - uu * (uu - 1) / 2 > idx) --uu;
-                while (uu + 1 < N && (uu + 1) * N - (uu + 1) * uu / 2 <= idx) ++uu;
-            }
+            const double b = 2.0 * (double)N + 1.0;
+            uu = (long long)floor((b - sqrt(fmax(b * b - 8.0 * (double)idx, 0.0))) * 0.5);
+            if (uu < 0) uu = 0;
+            if (uu > N - 1) uu = N - 1;
+            while (uu > 0 && uu * N - uu * (uu - 1) / 2 > idx) --uu;
+            while (uu + 1 < N && (uu + 1) * N - (uu + 1) * uu / 2 <= idx) ++uu;
             u = uu;
             v = u + (idx - (u * N - u * (u - 1) / 2));
         } else {
@@ -585,10 +626,32 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
         dev::resolve_exact(k, x, kThreshold, &res);
         double cof[dev::KMAX * dev::KMAX];
         dev::first_cofactor(res, cof);
-        double h1 = 0.0, htot = 0.0;
-        if (res.nullity < 3) htot = dev::same_spin_exact(a.n, k, L, R, res, cof, a.h, a.eri, &h1);
+        double h1 = 0.0, h2 = 0.0;
+        if (res.nullity < 3) {
+            if (res.nullity <= 1)
+                for (int q = lane; q < k * k; q += 32) {
+                    const int c = q / k, r = q % k;
+                    h1 += __ldg(a.h + L[c] * a.n + R[r]) * cof[c * k + r];
+                }
+            const int cp_count = k * (k - 1) / 2;
+            const bool regular = res.nullity == 0 && k > 3;
+            for (int q = lane; q < cp_count * cp_count; q += 32) {
+                int c1, c2, r1, r2;
+                unanti(q / cp_count, &c1, &c2);
+                unanti(q % cp_count, &r1, &r2);
+                const double g = dev::eri_packed(a.eri, R[r1], L[c1], R[r2], L[c2]) -
+                                 dev::eri_packed(a.eri, R[r1], L[c2], R[r2], L[c1]);
+                const double m2 = regular ? (cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2]) / res.det
+                                          : dev::second_cofactor(res, r1, r2, c1, c2);
+                h2 += g * m2;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            h1 += __shfl_xor_sync(0xffffffffu, h1, o);
+            h2 += __shfl_xor_sync(0xffffffffu, h2, o);
+        }
         double* rec = a.records + t * (long long)a.rec_stride;
-        for (int m = 0; m < a.R; ++m) {
+        for (int m = lane; m < a.R; m += 32) {
             double acc = 0.0;
             if (res.nullity <= 1)
                 for (int c = 0; c < k; ++c)
@@ -596,10 +659,12 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
                         acc = fma(cof[c * k + r], __ldg(a.lf + (long long)dev::pair_index(R[r], L[c]) * a.ld + m), acc);
             rec[m] = acc;
         }
-        rec[a.R + 0] = res.det;
-        rec[a.R + 1] = htot;
-        rec[a.R + 2] = h1;
-        rec[a.R + 3] = (double)res.nullity;
+        if (lane == 0) {
+            rec[a.R + 0] = res.det;
+            rec[a.R + 1] = res.nullity < 3 ? h1 + h2 : 0.0;
+            rec[a.R + 2] = res.nullity < 3 ? h1 : 0.0;
+            rec[a.R + 3] = (double)res.nullity;
+        }
     }
 }
 
@@ -622,41 +687,18 @@ __device__ __forceinline__ void band_decode(long long t, long long e0, long long
     *e = *d + (tp - (i * B - i * (i - 1) / 2));
 }
 
-// S_de = S_a S_b, H_de = H_a S_b + H_b S_a + sum_m sigma_m u_a[m] u_b[m] for one determinant pair.
-__device__ __forceinline__ void pair_value(const FullPairArgs& a, long long d, long long e, double* H, double* S) {
-    double sa = 1.0, hsa = 0.0, sb = 1.0, hsb = 0.0, dot = 0.0;
-    const double* ra = nullptr;
-    const double* rb = nullptr;
-    const int R = a.R;
-    if (a.ka > 0) {
-        const int ia = __ldg(a.det_alpha + d), ja = __ldg(a.det_alpha + e);
-        const long long lo = min(ia, ja), hi = max(ia, ja);
-        ra = a.rec_a + record_index(lo, hi, a.Na) * a.stride_a;
-        sa = ra[R];
-        hsa = ra[R + 1];
-    }
-    if (a.kb > 0) {
-        const int ib = __ldg(a.det_beta + d), jb = __ldg(a.det_beta + e);
-        const long long lo = min(ib, jb), hi = max(ib, jb);
-        rb = a.rec_b + record_index(lo, hi, a.Nb) * a.stride_b;
-        sb = rb[R];
-        hsb = rb[R + 1];
-    }
-    if (ra && rb) {
-        double pos = 0.0, neg = 0.0;
-        int m = 0;
-        for (; m + 1 < a.r_pos; m += 2) {
-            const double2 x = *reinterpret_cast<const double2*>(ra + m);
-            const double2 y = *reinterpret_cast<const double2*>(rb + m);
-            pos = fma(x.x, y.x, pos);
-            pos = fma(x.y, y.y, pos);
-        }
-        for (; m < a.r_pos; ++m) pos = fma(ra[m], rb[m], pos);
-        for (; m < R; ++m) neg = fma(ra[m], rb[m], neg);
-        dot = pos - neg;
-    }
-    *H = fma(hsa, sb, fma(hsb, sa, dot));
-    *S = sa * sb;
+// Weight of the upper-triangle pair (d <= e) in H_d = U' + U'^T: 1/2 on the diagonal, and,
+// with a spin-flip permutation, the unordered pairs {d, e} and {flip d, flip e} (same H_de and,
+// for structures whose coefficients are flip-invariant, the same coefficient products) fold
+// onto one representative with twice the weight; the other member gets weight 0.
+__device__ __forceinline__ double pair_weight(const int* flip, long long d, long long e) {
+    const double w = (d == e) ? 0.5 : 1.0;
+    if (!flip) return w;
+    const long long fd = __ldg(flip + d), fe = __ldg(flip + e);
+    const long long d2 = fd < fe ? fd : fe, e2 = fd < fe ? fe : fd;
+    if (d < d2 || (d == d2 && e < e2)) return 2.0 * w;
+    if (d == d2 && e == e2) return w;
+    return 0.0;
 }
 
 __global__ void __launch_bounds__(256) full_pairs_kernel(FullPairArgs a) {
@@ -665,8 +707,13 @@ __global__ void __launch_bounds__(256) full_pairs_kernel(FullPairArgs a) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < a.n_items; t += stride) {
         long long d, e;
         band_decode(t, a.e0, a.e1, &d, &e);
-        double H, S;
-        pair_value(a, d, e, &H, &S);
+        const double w = pair_weight(a.flip, d, e);
+        double H = 0.0, S = 0.0;
+        if (w != 0.0) {
+            pair_value(a, d, e, &H, &S);
+            H *= w;
+            S *= w;
+        }
         const long long o = d * B + (e - a.e0);
         a.Hb[o] = H;
         a.Sb[o] = S;
@@ -756,7 +803,8 @@ size_t left_table_doubles(int n, int k, int R) {
 size_t factored_spin_smem_bytes(int n, int k, int R) {
     const size_t gd = (size_t)n * (n - 1) / 2;
     const size_t cp = (size_t)k * (k - 1) / 2;
-    return sizeof(double) * (left_table_doubles(n, k, R) + (size_t)even_up(k * n) + (k >= 2 ? cp * gd : 0));
+    return sizeof(double) * (left_table_doubles(n, k, R) + (size_t)kSpinBlock * kfs(k) + (size_t)((k * n + 1) / 2 * 2) +
+                             (k >= 2 ? cp * gd : 0));
 }
 
 bool fast_spin_supported(int n, int k, int R) {
@@ -765,10 +813,12 @@ bool fast_spin_supported(int n, int k, int R) {
 
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs, double* lf,
                                       int ld, int* meta, cudaStream_t stream) {
-    const size_t smem = sizeof(int) * (size_t)np;
+    const size_t in_smem_bytes = sizeof(double) * (size_t)np * np + sizeof(int) * 2 * (size_t)np;
+    const int in_smem = in_smem_bytes <= 200 * 1024 ? 1 : 0;
+    const size_t smem = in_smem ? in_smem_bytes : sizeof(int) * 2 * (size_t)np;
     cudaError_t err = cudaFuncSetAttribute(factor_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    factor_pair_kernel<<<1, 512, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, kFactorTolerance);
+    factor_pair_kernel<<<1, 512, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, kFactorTolerance, in_smem);
     return cudaGetLastError();
 }
 
