@@ -245,7 +245,9 @@ def run_vbcore(args):
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
 
-    ctx = vbcore.Context(local)
+    # --profile: a reduced HBM budget (smaller determinant-pair bands) and no side measurements,
+    # so that one kernel of the full-size evaluation can be captured under a profiler
+    ctx = vbcore.Context(local, (4 << 30) if args.profile else 0)
     rows = vbcore.generate_structures(KEYWORD, N_ACTIVE, N_ELECTRONS)
     ex = vbcore.expand_structures(rows, N_ELECTRONS)
     plan = vbcore.HsPlan(ctx, ex, N_ACTIVE)
@@ -263,7 +265,7 @@ def run_vbcore(args):
     dSo = torch.empty((n_str, n_str), dtype=torch.float64, device=device)
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=device)
 
-    peak = measured_fp64_peak_tflops(torch, device)
+    peak = None if args.profile else measured_fp64_peak_tflops(torch, device)
     plan.enable_phase_timing(True)
 
     def step():
@@ -306,10 +308,10 @@ def run_vbcore(args):
     pe = torch.tensor(eri).pin_memory()
     pH = torch.empty((n_str, n_str), dtype=torch.float64).pin_memory()
     pSo = torch.empty((n_str, n_str), dtype=torch.float64).pin_memory()
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(0 if args.profile else max(1, args.warmup // 2)):
         plan.execute_host_pointers(pS.data_ptr(), ph.data_ptr(), pe.data_ptr(), pH.data_ptr(), pSo.data_ptr())
     e2e_ms = 0.0
-    for _ in range(args.steps):
+    for _ in range(0 if args.profile else args.steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -321,7 +323,7 @@ def run_vbcore(args):
         t = torch.tensor([e2e_ms], device=device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = ordered * args.steps * world / (e2e_ms * 1e-3)
+    e2e_value = ordered * args.steps * world / (e2e_ms * 1e-3) if e2e_ms > 0 else None
     h2d = (2 * N_ACTIVE * N_ACTIVE + len(eri)) * 8
     d2h = 2 * n_str * n_str * 8
 
@@ -340,12 +342,17 @@ def run_vbcore(args):
     achieved = flops / (mean_phase[dominant] * 1e-3) / 1e12
     traffic = read_profile_traffic(kname)
     per_kernel = {name: {"ms": mean_phase[name], "tflops": f / (mean_phase[name] * 1e-3) / 1e12,
-                         "frac": f / (mean_phase[name] * 1e-3) / 1e12 / peak, "units": u}
+                         "frac": f / (mean_phase[name] * 1e-3) / 1e12 / peak if peak else None, "units": u}
                   for name, (_, f, u) in kernels.items()}
+    # whole evaluation under the same pair-flop model (ordered spin pairs and determinant pairs)
+    model_flops = ordered * (flops_spin_pair(k) + flops_full_pair(k, k))
+    evaluation = {"flops_model": model_flops, "ms": total_ms / args.steps,
+                  "tflops": model_flops / (total_ms / args.steps * 1e-3) / 1e12}
+    evaluation["frac"] = evaluation["tflops"] / peak if peak else None
 
     if rank == 0:
         base = None
-        if world == 1:
+        if world == 1 and not args.profile:
             O = _oracle()
             ex_o = O.expand(O.generate_structures(KEYWORD, N_ACTIVE, N_ELECTRONS), N_ELECTRONS)
             base = cpu_baseline(ex_o, S, h, eri, ordered)
@@ -355,10 +362,10 @@ def run_vbcore(args):
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded)", "config": config_dict(n_det, n_str, world),
             "roofline": {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured)",
                          "flops_per_launch": flops, "units_per_launch": units},
-            "phases_ms": mean_phase, "kernels": per_kernel,
+            "phases_ms": mean_phase, "kernels": per_kernel, "evaluation": evaluation,
             "cpu_baseline": base,
             "e2e": {"value": e2e_value, "unit": "ordered determinant pairs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -380,6 +387,8 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vbcore", choices=["vbcore", "reference"])
+    ap.add_argument("--profile", action="store_true",
+                    help="for profiler captures: 4 GiB HBM budget, no DGEMM peak, CPU baseline or end-to-end leg")
     ap.add_argument("--n-active", type=int, default=14,
                     help="active orbitals (even; 14 is the benchmark workload, smaller cases are for profiling)")
     args = ap.parse_args()

@@ -38,6 +38,7 @@ struct vb_hs_plan {
     long long npairs_a = 0, npairs_b = 0;
     DeviceBuffer counters, list_a, list_b, items_a, items_b;
     int n_items_a = 0, n_items_b = 0;
+    int rec_stride_alloc = 0;  // record stride the spin-pair records are allocated for
     DeviceBuffer S_in, h_in, eri_in, gamma, kfull;
     // pair-kernel factorization: lf[q * np + m], scratch, signs, meta = {r_pos, r_neg} (+ host copy)
     DeviceBuffer lf, fwork, fcols, fsigns, fmeta;
@@ -210,11 +211,9 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     if ((st = upload(ctx, p->det_alpha, ex->det_alpha, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
     if ((st = upload(ctx, p->det_beta, ex->det_beta, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
 
-    // spin-pair records, sized for the largest factor rank (np columns)
-    const int max_stride = record_stride(p->np);
+    // spin-pair records are allocated by the first execute, once the factor rank is known
     p->npairs_a = (long long)p->Na * (p->Na + 1) / 2;
     p->npairs_b = p->shared_tables ? 0 : (long long)p->Nb * (p->Nb + 1) / 2;
-    if ((st = p->rec_a.allocate(ctx, sizeof(double) * max_stride * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
     if ((st = p->list_a.allocate(ctx, sizeof(unsigned long long) * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
     {
         std::vector<int2> it = spin_items(p->Na);
@@ -223,8 +222,6 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
             return fail(st);
     }
     if (!p->shared_tables) {
-        if ((st = p->rec_b.allocate(ctx, sizeof(double) * max_stride * std::max(1LL, p->npairs_b))) != VB_OK)
-            return fail(st);
         if ((st = p->list_b.allocate(ctx, sizeof(unsigned long long) * std::max(1LL, p->npairs_b))) != VB_OK)
             return fail(st);
         std::vector<int2> it = spin_items(p->Nb);
@@ -460,6 +457,20 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
     p->r_pos = p->meta_host[0];
     p->R = p->meta_host[0] + p->meta_host[1];
     tables.close();
+    if (record_stride(p->R) > p->rec_stride_alloc) {
+        // (re)size the records for this rank; a later execute with a lower rank reuses them
+        const int stride = record_stride(p->R);
+        vb_status st = p->rec_a.allocate(ctx, sizeof(double) * stride * std::max(1LL, p->npairs_a));
+        if (st == VB_OK && !p->shared_tables && p->kb > 0)
+            st = p->rec_b.allocate(ctx, sizeof(double) * stride * std::max(1LL, p->npairs_b));
+        if (st != VB_OK) {
+            p->rec_a.release();
+            p->rec_b.release();
+            p->rec_stride_alloc = 0;
+            return st;
+        }
+        p->rec_stride_alloc = stride;
+    }
     PhaseMark spin(p, VB_PHASE_SPIN_PAIRS);
     err = cudaMemsetAsync(p->counters.ptr, 0, 4 * sizeof(unsigned long long), s);
     if (err != cudaSuccess) return cuda_error(ctx, err, "cudaMemsetAsync");
