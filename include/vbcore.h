@@ -175,6 +175,32 @@ vb_status vb_hs_plan_determinant_pairs(vb_hs_plan* plan, const double* ovlp_act,
                                        const double* eri_packed, int64_t n_pairs, const int64_t* pairs,
                                        int mem_space, double* h_out, double* s_out);
 
+/* ---- metric Cholesky and the structure eigenproblem ------------------------------------------- */
+
+/* Upper Cholesky factor S = U^T U of a symmetric positive-definite metric
+ * (overlap_upper, src/vbscf/orbitals/preparation/cholesky.hpp:10-15, Eigen::LLT; also the
+ * first stage of dsygvd).  Only the upper triangle of S is read; upper_out (n x n,
+ * column-major) receives U with zeros below the diagonal and may alias S.  A non-positive (or
+ * non-finite) pivot returns VB_ERR_NUMERIC with *info = order of that leading minor. */
+vb_status vb_metric_cholesky(vb_context* ctx, const double* S, int n, int mem_space, double* upper_out, int* info);
+
+/* H C = S C E, LAPACK dsygvd(itype 1, 'V', 'U') semantics as called by
+ * GeneralizedEigensolver::solve_dense (src/linalg/eigensolver.cpp:365-388): upper triangles of
+ * H and S read, eigenvalues ascending, eigenvectors column-major with C^T S C = I.  S not
+ * positive definite: VB_ERR_NUMERIC with *info = n + i (i = order of the failing leading
+ * minor), the reference's "overlap_matrix is not positive definite" (eigensolver.cpp:39-49).
+ * Synchronizes the context stream. */
+vb_status vb_generalized_eigh(vb_context* ctx, const double* H, const double* S, int n, int mem_space,
+                              double* eigenvalues, double* eigenvectors, int* info);
+
+/* `count` independent problems in device memory (one CTA each): problem b has dimension
+ * dims[b], H, S and eigenvectors at element offset offsets[b], eigenvalues at
+ * value_offsets[b]; info[b] (host) = 0, n + i (S not positive definite) or -1 (no
+ * convergence).  Returns the first failure as VB_ERR_NUMERIC. */
+vb_status vb_generalized_eigh_batched(vb_context* ctx, int count, const int* dims, const int64_t* offsets,
+                                      const double* H, const double* S, int mem_space, double* eigenvalues,
+                                      const int64_t* value_offsets, double* eigenvectors, int* info);
+
 /* ---- allocation-free spin-pair evaluation ------------------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot allocate device memory where

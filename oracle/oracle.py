@@ -197,6 +197,40 @@ def ri_transform(B_packed: np.ndarray, C: np.ndarray, threads: int = 0):
 
 
 # ----------------------------------------------------------------------------------------------
+# metric Cholesky and the dense structure eigenproblem
+
+
+def metric_cholesky(S):
+    """Upper Cholesky factor U with S = U^T U (overlap_upper,
+    src/vbscf/orbitals/preparation/cholesky.hpp:10-15, an Eigen::LLT): LAPACK dpotrf on the
+    upper triangle through SciPy."""
+    import scipy.linalg
+
+    return scipy.linalg.cholesky(np.asarray(S, dtype=np.float64), lower=False)
+
+
+def generalized_eigh(H, S):
+    """H C = S C E by LAPACK dsygvd(itype 1, 'V', 'U') -- the routine
+    GeneralizedEigensolver::solve_dense calls (src/linalg/eigensolver.cpp:365-388) -- through
+    SciPy's LAPACK binding: upper triangles read, eigenvalues ascending, C^T S C = I."""
+    import scipy.linalg
+
+    return scipy.linalg.eigh(np.asarray(H, dtype=np.float64), np.asarray(S, dtype=np.float64), lower=False,
+                             driver="gvd")
+
+
+def conditioned_metric(n: int, cond: float, seed: int) -> np.ndarray:
+    """Seeded symmetric positive-definite metric with condition number `cond`:
+    S = Q diag(logspace(0, -log10 cond, n)) Q^T, Q from the QR factor of a Gaussian matrix."""
+    rng = np.random.default_rng(seed)
+    q, r = np.linalg.qr(rng.standard_normal((n, n)))
+    q = q * np.sign(np.diag(r))
+    d = np.logspace(0.0, -math.log10(cond), n) if n > 1 else np.ones(1)
+    S = (q * d) @ q.T
+    return 0.5 * (S + S.T)
+
+
+# ----------------------------------------------------------------------------------------------
 # structure-class generation (src/input/loading/generated_structures.cpp)
 
 

@@ -91,3 +91,21 @@ def test_full_pivot_lu_rank_threshold():
     assert rank == 2 and inv is None
     rank, det, inv = O.full_pivot_lu(np.diag([1.0, 1e-6, 1e-11]))
     assert rank == 3 and abs(det - 1e-17) < 1e-30
+
+
+def test_linalg_oracle_is_dsygvd():
+    # the oracle's dense eigenproblem is LAPACK dsygvd; cross-check it against an explicit
+    # Cholesky reduction to a standard symmetric problem
+    n = 30
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((n, n))
+    H = 0.5 * (a + a.T)
+    S = O.conditioned_metric(n, 1e5, seed=5)
+    assert abs(np.linalg.cond(S) / 1e5 - 1) < 1e-6
+    U = O.metric_cholesky(S)
+    assert np.abs(U.T @ U - S).max() < 1e-14
+    w, C = O.generalized_eigh(H, S)
+    Ui = np.linalg.inv(U)
+    wr = np.linalg.eigvalsh(Ui.T @ H @ Ui)
+    assert np.abs(w - wr).max() < 1e-12 * np.abs(w).max()
+    assert np.abs(C.T @ S @ C - np.eye(n)).max() < 1e-10

@@ -1,0 +1,763 @@
+// Dense FP64 metric linear algebra on the device.
+//
+//  * vb_metric_cholesky: upper Cholesky factor S = U^T U of a symmetric positive-definite
+//    metric (overlap_upper, src/vbscf/orbitals/preparation/cholesky.hpp:10-15, Eigen::LLT).
+//  * vb_generalized_eigh: H C = S C E with LAPACK dsygvd(itype 1, 'V', 'U') semantics
+//    (GeneralizedEigensolver::solve_dense, src/linalg/eigensolver.cpp:365-388): only the upper
+//    triangles of H and S are read, eigenvalues ascending, C^T S C = I, and info = n + i when
+//    the leading minor of order i of S is not positive definite
+//    (check_generalized_eigensolver_info, eigensolver.cpp:39-49).
+//  * vb_generalized_eigh_batched: many independent problems, one CTA each.
+//
+// Method (one kernel): blocked right-looking Cholesky (32-column panels), blocked inverse of
+// the triangular factor, A = U^-T H U^-1 and C = U^-1 Q as tiled GEMMs, and the symmetric
+// eigenproblem of A by cyclic Jacobi in round-robin (tournament) order: every round rotates
+// m/2 disjoint pivot pairs at once, so one round is a single pass over A (two-sided 2 x 2 block
+// updates, ping-pong buffers) and over the eigenvector matrix.  Jacobi needs no
+// tridiagonalization, is embarrassingly parallel within a round and attains eigenvalues to
+// working accuracy (quadratic convergence, typically 8-10 sweeps).
+//
+// A single problem runs as a cooperative launch (one CTA per SM) whose phases are separated
+// by a grid barrier with a bounded spin; a batch runs one problem per CTA with __syncthreads.
+// Data written inside the kernel is read with __ldcg (L2), never through the incoherent L1
+// or read-only paths.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace vbcore {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTile = 32;
+constexpr long long kBarrierSpinLimit = 1ll << 26;  // ~ seconds with 64 ns sleeps
+constexpr int kMaxSweeps = 60;
+constexpr int kSmallProblem = 96;  // single-problem calls at or below this size use one CTA
+
+struct Control {
+    unsigned bar_count;
+    unsigned bar_gen;
+    int err;       // 1: a grid barrier gave up waiting
+    int info;      // Cholesky failure: order of the first non-positive leading minor
+    unsigned rotations[3];
+    int sweeps;
+    double fro2;   // squared Frobenius norm of the reduced matrix
+};
+
+struct EighArgs {
+    int n;
+    int mode;            // 0: Cholesky only, 1: full generalized eigenproblem
+    const double* H;     // n x n, column-major (upper triangle read)
+    const double* S;     // n x n, column-major (upper triangle read)
+    double* U;           // Cholesky factor (output for mode 0)
+    double* Ui;          // U^-1 (zero-initialised)
+    double* T;           // scratch n x n
+    double* A0;          // ping-pong n x n
+    double* A1;
+    double* V;           // Jacobi rotations (zero-initialised)
+    int* rank;           // n
+    double* evals;       // n
+    double* evecs;       // n x n
+    Control* ctl;        // zero-initialised
+};
+
+struct BlockSync {
+    __device__ __forceinline__ bool operator()() const {
+        __syncthreads();
+        return true;
+    }
+};
+
+struct GridSync {
+    Control* ctl;
+    unsigned nblocks;
+    __device__ bool operator()() const {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile unsigned* gen = &ctl->bar_gen;
+            const unsigned g = *gen;
+            __threadfence();
+            if (atomicAdd(&ctl->bar_count, 1u) == nblocks - 1) {
+                atomicExch(&ctl->bar_count, 0u);
+                __threadfence();
+                atomicAdd(&ctl->bar_gen, 1u);
+            } else {
+                long long spins = 0;
+                while (*gen == g) {
+                    if (++spins > kBarrierSpinLimit) {
+                        atomicExch(&ctl->err, 1);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        return *(volatile int*)&ctl->err == 0;
+    }
+};
+
+__device__ __forceinline__ double ld(const double* p) { return __ldcg(p); }
+
+// Element (r, c) of the symmetric matrix whose upper triangle is stored column-major in M.
+__device__ __forceinline__ double upper_elem(const double* M, int n, int r, int c) {
+    return r <= c ? ld(M + r + (long long)c * n) : ld(M + c + (long long)r * n);
+}
+
+struct Shared {
+    double a[kTile][kTile + 1];
+    double b[kTile][kTile + 1];
+    double d[kTile][kTile + 1];
+    int flag;
+};
+
+// ---------------------------------------------------------------------------------------
+// Cholesky, S = U^T U (upper), right-looking with 32-column panels.
+template <class Sync>
+__device__ bool cholesky(const EighArgs& a, const Sync& sync, Shared& sh, int cta, int ncta) {
+    const int n = a.n;
+    const int tid = threadIdx.x;
+    const long long gtid = (long long)cta * blockDim.x + tid, gstride = (long long)ncta * blockDim.x;
+    double* U = a.U;
+    for (long long e = gtid; e < (long long)n * n; e += gstride) {
+        const int r = (int)(e % n), c = (int)(e / n);
+        U[e] = r <= c ? ld(a.S + e) : 0.0;
+    }
+    if (!sync()) return false;
+    for (int j0 = 0; j0 < n; j0 += kTile) {
+        const int jb = min(kTile, n - j0);
+        const int j1 = j0 + jb;
+        // (1) factor the diagonal block
+        if (cta == 0) {
+            for (int e = tid; e < jb * jb; e += blockDim.x) {
+                const int r = e % jb, c = e / jb;
+                sh.d[r][c] = r <= c ? ld(U + (j0 + r) + (long long)(j0 + c) * n) : 0.0;
+            }
+            if (tid == 0) sh.flag = 0;
+            __syncthreads();
+            for (int k = 0; k < jb; ++k) {
+                if (tid == 0) {
+                    const double dk = sh.d[k][k];
+                    if (!(dk > 0.0) || !isfinite(dk))
+                        sh.flag = j0 + k + 1;
+                    else
+                        sh.d[k][k] = sqrt(dk);
+                }
+                __syncthreads();
+                if (sh.flag) break;
+                const double piv = sh.d[k][k];
+                for (int c = k + 1 + tid; c < jb; c += blockDim.x) sh.d[k][c] /= piv;
+                __syncthreads();
+                const int w = jb - k - 1;
+                for (int e = tid; e < w * w; e += blockDim.x) {
+                    const int r = k + 1 + e % w, c = k + 1 + e / w;
+                    if (r <= c) sh.d[r][c] = fma(-sh.d[k][r], sh.d[k][c], sh.d[r][c]);
+                }
+                __syncthreads();
+            }
+            if (sh.flag) {
+                if (tid == 0) atomicExch(&a.ctl->info, sh.flag);
+            } else {
+                for (int e = tid; e < jb * jb; e += blockDim.x) {
+                    const int r = e % jb, c = e / jb;
+                    if (r <= c) U[(j0 + r) + (long long)(j0 + c) * n] = sh.d[r][c];
+                }
+            }
+        }
+        if (!sync()) return false;
+        if (*(volatile int*)&a.ctl->info) return false;
+        if (j1 >= n) break;
+        // (2) panel row: U12 = U11^-T A12, one column per thread
+        for (int e = tid; e < jb * jb; e += blockDim.x) {
+            const int r = e % jb, c = e / jb;
+            sh.d[r][c] = r <= c ? ld(U + (j0 + r) + (long long)(j0 + c) * n) : 0.0;
+        }
+        __syncthreads();
+        for (long long c = j1 + gtid; c < n; c += gstride) {
+            double x[kTile];
+#pragma unroll
+            for (int r = 0; r < kTile; ++r) x[r] = r < jb ? ld(U + (j0 + r) + c * n) : 0.0;
+#pragma unroll
+            for (int r = 0; r < kTile; ++r) {
+                if (r < jb) {
+                    double s = x[r];
+#pragma unroll
+                    for (int k = 0; k < r; ++k) s = fma(-sh.d[k][r], x[k], s);
+                    x[r] = s / sh.d[r][r];
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kTile; ++r)
+                if (r < jb) U[(j0 + r) + c * n] = x[r];
+        }
+        if (!sync()) return false;
+        // (3) trailing update of the upper part: A22 -= U12^T U12, 32 x 32 tiles (ti <= tj)
+        const int m = n - j1;
+        const int nt = (m + kTile - 1) / kTile;
+        const int ntiles = nt * (nt + 1) / 2;
+        for (int t = cta; t < ntiles; t += ncta) {
+            int tj = 0;
+            while ((tj + 1) * (tj + 2) / 2 <= t) ++tj;
+            const int ti = t - tj * (tj + 1) / 2;
+            for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                const int k = e % kTile, i = e / kTile;
+                const int ri = j1 + ti * kTile + i, cj = j1 + tj * kTile + i;
+                sh.a[k][i] = (k < jb && ri < n) ? ld(U + (j0 + k) + (long long)ri * n) : 0.0;
+                sh.b[k][i] = (k < jb && cj < n) ? ld(U + (j0 + k) + (long long)cj * n) : 0.0;
+            }
+            __syncthreads();
+            const int i = tid & 31, jq = tid >> 5;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int k = 0; k < jb; ++k) {
+                const double av = sh.a[k][i];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = fma(av, sh.b[k][jq + 8 * q], acc[q]);
+            }
+            const int r = j1 + ti * kTile + i;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int c = j1 + tj * kTile + jq + 8 * q;
+                if (r < n && c < n && r <= c) U[r + (long long)c * n] -= acc[q];
+            }
+            __syncthreads();
+        }
+        if (!sync()) return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------
+// Ui = U^-1 (upper), by 32 x 32 blocks: diagonal blocks first, then block diagonals
+// Ui[I][J] = -Ui[I][I] sum_{K=I+1..J} U[I][K] Ui[K][J].
+template <class Sync>
+__device__ bool triangular_inverse(const EighArgs& a, const Sync& sync, Shared& sh, int cta, int ncta) {
+    const int n = a.n;
+    const int tid = threadIdx.x;
+    const int nb = (n + kTile - 1) / kTile;
+    const double* U = a.U;
+    double* Ui = a.Ui;
+    for (int I = cta; I < nb; I += ncta) {
+        const int r0 = I * kTile, bi = min(kTile, n - r0);
+        for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+            const int r = e % kTile, c = e / kTile;
+            sh.d[r][c] = (r < bi && c < bi && r <= c) ? ld(U + (r0 + r) + (long long)(r0 + c) * n) : 0.0;
+            sh.a[r][c] = 0.0;
+        }
+        __syncthreads();
+        if (tid < bi) {
+            const int j = tid;
+            sh.a[j][j] = 1.0 / sh.d[j][j];
+            for (int i = j - 1; i >= 0; --i) {
+                double s = 0.0;
+                for (int k = i + 1; k <= j; ++k) s = fma(sh.d[i][k], sh.a[k][j], s);
+                sh.a[i][j] = -s / sh.d[i][i];
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < bi * bi; e += blockDim.x) {
+            const int r = e % bi, c = e / bi;
+            if (r <= c) Ui[(r0 + r) + (long long)(r0 + c) * n] = sh.a[r][c];
+        }
+        __syncthreads();
+    }
+    if (!sync()) return false;
+    for (int dgl = 1; dgl < nb; ++dgl) {
+        for (int I = cta; I + dgl < nb; I += ncta) {
+            const int J = I + dgl;
+            const int r0 = I * kTile, c0 = J * kTile;
+            const int i = tid & 31, jq = tid >> 5;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int K = I + 1; K <= J; ++K) {
+                const int k0 = K * kTile;
+                for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                    const int r = e % kTile, c = e / kTile;
+                    sh.a[r][c] = (r0 + r < n && k0 + c < n) ? ld(U + (r0 + r) + (long long)(k0 + c) * n) : 0.0;
+                    sh.b[r][c] = (k0 + r < n && c0 + c < n) ? ld(Ui + (k0 + r) + (long long)(c0 + c) * n) : 0.0;
+                }
+                __syncthreads();
+#pragma unroll 8
+                for (int k = 0; k < kTile; ++k) {
+                    const double av = sh.a[i][k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] = fma(av, sh.b[k][jq + 8 * q], acc[q]);
+                }
+                __syncthreads();
+            }
+            // Ui[I][J] = -Ui[I][I] P
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sh.b[i][jq + 8 * q] = acc[q];
+            for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                const int r = e % kTile, c = e / kTile;
+                sh.a[r][c] = (r0 + r < n && r0 + c < n) ? ld(Ui + (r0 + r) + (long long)(r0 + c) * n) : 0.0;
+            }
+            __syncthreads();
+            double out[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int k = 0; k < kTile; ++k) {
+                const double av = sh.a[i][k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) out[q] = fma(av, sh.b[k][jq + 8 * q], out[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = r0 + i, c = c0 + jq + 8 * q;
+                if (r < n && c < n) Ui[r + (long long)c * n] = -out[q];
+            }
+            __syncthreads();
+        }
+        if (!sync()) return false;
+    }
+    return true;
+}
+
+// C (n x n) = op_A * op_B with 32 x 32 output tiles; la(r, k), lb(k, c) return the operands.
+template <class LA, class LB>
+__device__ void gemm_tiles(int n, LA la, LB lb, double* C, Shared& sh, int cta, int ncta) {
+    const int tid = threadIdx.x;
+    const int tm = (n + kTile - 1) / kTile;
+    for (int t = cta; t < tm * tm; t += ncta) {
+        const int ti = t % tm, tj = t / tm;
+        const int i = tid & 31, jq = tid >> 5;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int k0 = 0; k0 < n; k0 += kTile) {
+            for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                const int r = e % kTile, c = e / kTile;
+                const int gr = ti * kTile + r, gk = k0 + c;
+                sh.a[r][c] = (gr < n && gk < n) ? la(gr, gk) : 0.0;
+                const int gk2 = k0 + r, gc = tj * kTile + c;
+                sh.b[r][c] = (gk2 < n && gc < n) ? lb(gk2, gc) : 0.0;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int k = 0; k < kTile; ++k) {
+                const double av = sh.a[i][k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = fma(av, sh.b[k][jq + 8 * q], acc[q]);
+            }
+            __syncthreads();
+        }
+        const int r = ti * kTile + i;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = tj * kTile + jq + 8 * q;
+            if (r < n && c < n) C[r + (long long)c * n] = acc[q];
+        }
+    }
+}
+
+// Round-robin pairing: round r of m - 1 (m even), pair i of m / 2 -> (p, q), p < q.
+__device__ __forceinline__ void round_pair(int m, int r, int i, int* p, int* q) {
+    auto pos = [&](int k) { return k == 0 ? 0 : 1 + (k - 1 + r) % (m - 1); };
+    int a = pos(i), b = pos(m - 1 - i);
+    *p = min(a, b);
+    *q = max(a, b);
+}
+
+// Jacobi rotation J = [[c, s], [-s, c]] annihilating a_pq in J^T A J (Golub & Van Loan,
+// Algorithm 8.4.1); rotations below the threshold are skipped (c = 1, s = 0).
+__device__ __forceinline__ bool jacobi_rotation(const double* A, int n, int p, int q, double skip_abs, double* c,
+                                                double* s, double* t) {
+    *c = 1.0;
+    *s = 0.0;
+    *t = 0.0;
+    if (q >= n) return false;  // padding index of odd n
+    const double app = ld(A + p + (long long)p * n), aqq = ld(A + q + (long long)q * n);
+    const double apq = ld(A + p + (long long)q * n);
+    const double aapq = fabs(apq);
+    if (aapq <= skip_abs || aapq <= 1.0e-15 * sqrt(fabs(app) * fabs(aqq))) return false;
+    const double tau = (aqq - app) / (2.0 * apq);
+    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
+    const double cc = 1.0 / sqrt(1.0 + tt * tt);
+    *c = cc;
+    *s = tt * cc;
+    *t = tt;
+    return true;
+}
+
+template <class Sync>
+__device__ bool jacobi(const EighArgs& a, const Sync& sync, Shared& sh, int cta, int ncta, double** A_final) {
+    const int n = a.n;
+    const int m = n + (n & 1);
+    const int half = m / 2;
+    const int tid = threadIdx.x;
+    const long long gtid = (long long)cta * blockDim.x + tid, gstride = (long long)ncta * blockDim.x;
+    const double skip_abs = 1.0e-18 * sqrt(ld(&a.ctl->fro2)) + 1.0e-300;
+    double* Ain = a.A0;
+    double* Aout = a.A1;
+    for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
+        if (cta == 0 && tid == 0) a.ctl->rotations[(sweep + 1) % 3] = 0u;
+        for (int r = 0; r < m - 1; ++r) {
+            unsigned applied = 0;
+            for (long long b = gtid; b < (long long)half * half; b += gstride) {
+                const int i = (int)(b % half), j = (int)(b / half);
+                int pi, qi, pj, qj;
+                round_pair(m, r, i, &pi, &qi);
+                round_pair(m, r, j, &pj, &qj);
+                double ci, si, ti, cj, sj, tj;
+                const bool roti = jacobi_rotation(Ain, n, pi, qi, skip_abs, &ci, &si, &ti);
+                if (i == j) {
+                    // diagonal block: exact annihilation
+                    const double app = ld(Ain + pi + (long long)pi * n);
+                    if (qi < n) {
+                        const double aqq = ld(Ain + qi + (long long)qi * n);
+                        const double apq = ld(Ain + pi + (long long)qi * n);
+                        Aout[pi + (long long)pi * n] = roti ? app - ti * apq : app;
+                        Aout[qi + (long long)qi * n] = roti ? aqq + ti * apq : aqq;
+                        Aout[pi + (long long)qi * n] = roti ? 0.0 : apq;
+                        Aout[qi + (long long)pi * n] = roti ? 0.0 : apq;
+                        applied += roti ? 1u : 0u;
+                    } else {
+                        Aout[pi + (long long)pi * n] = app;
+                    }
+                    continue;
+                }
+                jacobi_rotation(Ain, n, pj, qj, skip_abs, &cj, &sj, &tj);
+                // B' = J_i^T B J_j with B = [[A(pi,pj), A(pi,qj)], [A(qi,pj), A(qi,qj)]]
+                const double b00 = ld(Ain + pi + (long long)pj * n);
+                const double b01 = qj < n ? ld(Ain + pi + (long long)qj * n) : 0.0;
+                const double b10 = qi < n ? ld(Ain + qi + (long long)pj * n) : 0.0;
+                const double b11 = (qi < n && qj < n) ? ld(Ain + qi + (long long)qj * n) : 0.0;
+                const double x00 = cj * b00 - sj * b01, x01 = sj * b00 + cj * b01;
+                const double x10 = cj * b10 - sj * b11, x11 = sj * b10 + cj * b11;
+                Aout[pi + (long long)pj * n] = ci * x00 - si * x10;
+                if (qj < n) Aout[pi + (long long)qj * n] = ci * x01 - si * x11;
+                if (qi < n) Aout[qi + (long long)pj * n] = si * x00 + ci * x10;
+                if (qi < n && qj < n) Aout[qi + (long long)qj * n] = si * x01 + ci * x11;
+            }
+            // eigenvector columns: V <- V J
+            for (long long u = gtid; u < (long long)n * half; u += gstride) {
+                const int k = (int)(u % n), i = (int)(u / n);
+                int p, q;
+                round_pair(m, r, i, &p, &q);
+                double c, s, t;
+                if (!jacobi_rotation(Ain, n, p, q, skip_abs, &c, &s, &t)) continue;
+                const double vp = ld(a.V + k + (long long)p * n), vq = ld(a.V + k + (long long)q * n);
+                a.V[k + (long long)p * n] = c * vp - s * vq;
+                a.V[k + (long long)q * n] = s * vp + c * vq;
+            }
+            // rotation count of this round (warp reduction, one atomic per warp)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) applied += __shfl_xor_sync(0xffffffffu, applied, o);
+            if ((tid & 31) == 0 && applied) atomicAdd(&a.ctl->rotations[sweep % 3], applied);
+            double* tmp = Ain;
+            Ain = Aout;
+            Aout = tmp;
+            if (!sync()) return false;
+        }
+        const unsigned count = *(volatile unsigned*)&a.ctl->rotations[sweep % 3];
+        if (cta == 0 && tid == 0) a.ctl->sweeps = sweep + 1;
+        if (count == 0u) break;
+    }
+    *A_final = Ain;
+    return true;
+}
+
+template <class Sync>
+__device__ void eigh_body(const EighArgs& a, const Sync& sync, Shared& sh, int cta, int ncta) {
+    const int n = a.n;
+    const int tid = threadIdx.x;
+    const long long gtid = (long long)cta * blockDim.x + tid, gstride = (long long)ncta * blockDim.x;
+    if (!cholesky(a, sync, sh, cta, ncta)) return;
+    if (a.mode == 0) return;
+    if (!triangular_inverse(a, sync, sh, cta, ncta)) return;
+    // T = H Ui (H symmetric from its upper triangle; Ui upper)
+    const double* H = a.H;
+    const double* Ui = a.Ui;
+    gemm_tiles(
+        n, [&](int r, int k) { return upper_elem(H, n, r, k); },
+        [&](int k, int c) { return k <= c ? ld(Ui + k + (long long)c * n) : 0.0; }, a.T, sh, cta, ncta);
+    if (!sync()) return;
+    // A1 = Ui^T T
+    const double* T = a.T;
+    gemm_tiles(
+        n, [&](int r, int k) { return k <= r ? ld(Ui + k + (long long)r * n) : 0.0; },
+        [&](int k, int c) { return ld(T + k + (long long)c * n); }, a.A1, sh, cta, ncta);
+    if (!sync()) return;
+    // A0 = (A1 + A1^T) / 2, V = I, Frobenius norm
+    double part = 0.0;
+    for (long long e = gtid; e < (long long)n * n; e += gstride) {
+        const int r = (int)(e % n), c = (int)(e / n);
+        const double v = 0.5 * (ld(a.A1 + e) + ld(a.A1 + c + (long long)r * n));
+        a.A0[e] = v;
+        part = fma(v, v, part);
+        if (r == c) a.V[e] = 1.0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if ((tid & 31) == 0) atomicAdd(&a.ctl->fro2, part);
+    if (!sync()) return;
+    double* A = nullptr;
+    if (!jacobi(a, sync, sh, cta, ncta, &A)) return;
+    // C = Ui V
+    const double* V = a.V;
+    gemm_tiles(
+        n, [&](int r, int k) { return r <= k ? ld(Ui + r + (long long)k * n) : 0.0; },
+        [&](int k, int c) { return ld(V + k + (long long)c * n); }, a.T, sh, cta, ncta);
+    // ascending order (stable for ties)
+    for (long long i = gtid; i < n; i += gstride) {
+        const double li = ld(A + i + i * (long long)n);
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+            const double lj = ld(A + j + (long long)j * n);
+            rank += (lj < li || (lj == li && j < i)) ? 1 : 0;
+        }
+        a.rank[i] = rank;
+        a.evals[rank] = li;
+    }
+    if (!sync()) return;
+    for (long long e = gtid; e < (long long)n * n; e += gstride) {
+        const int r = (int)(e % n), c = (int)(e / n);
+        a.evecs[r + (long long)__ldcg(a.rank + c) * n] = ld(a.T + e);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) eigh_grid_kernel(EighArgs a) {
+    __shared__ Shared sh;
+    GridSync sync{a.ctl, gridDim.x};
+    eigh_body(a, sync, sh, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(kThreads) eigh_block_kernel(const EighArgs* __restrict__ args, int count) {
+    __shared__ Shared sh;
+    const int b = blockIdx.x;
+    if (b >= count) return;
+    const EighArgs a = args[b];
+    BlockSync sync;
+    eigh_body(a, sync, sh, 0, 1);
+}
+
+// Workspace of one problem (doubles / ints), all offsets 256-byte aligned.
+struct Layout {
+    size_t U, Ui, T, A0, A1, V, evals, evecs, H, S, rank, ctl, total;
+};
+
+size_t align_up(size_t x) { return (x + 255) / 256 * 256; }
+
+Layout layout_for(int n, int mode, bool own_inputs, bool own_outputs) {
+    Layout L{};
+    const size_t m2 = sizeof(double) * (size_t)n * n;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = off;
+        off = align_up(off + bytes);
+        return at;
+    };
+    L.U = take(m2);
+    if (mode == 1) {
+        L.Ui = take(m2);
+        L.T = take(m2);
+        L.A0 = take(m2);
+        L.A1 = take(m2);
+        L.V = take(m2);
+        L.rank = take(sizeof(int) * n);
+        if (own_outputs) {
+            L.evals = take(sizeof(double) * n);
+            L.evecs = take(m2);
+        }
+        if (own_inputs) L.H = take(m2);
+    }
+    if (own_inputs) L.S = take(m2);
+    L.ctl = take(sizeof(Control));
+    L.total = off;
+    return L;
+}
+
+// Bytes that must start at zero: Ui and V (mode 1) and the control block.
+cudaError_t clear_workspace(unsigned char* base, const Layout& L, int n, int mode, cudaStream_t s) {
+    const size_t m2 = sizeof(double) * (size_t)n * n;
+    cudaError_t err = cudaMemsetAsync(base + L.ctl, 0, sizeof(Control), s);
+    if (err == cudaSuccess && mode == 1) err = cudaMemsetAsync(base + L.Ui, 0, m2, s);
+    if (err == cudaSuccess && mode == 1) err = cudaMemsetAsync(base + L.V, 0, m2, s);
+    return err;
+}
+
+EighArgs args_for(unsigned char* base, const Layout& L, int n, int mode, const double* H, const double* S,
+                  double* evals, double* evecs, double* U_out) {
+    EighArgs a{};
+    a.n = n;
+    a.mode = mode;
+    a.H = H;
+    a.S = S;
+    a.U = U_out ? U_out : reinterpret_cast<double*>(base + L.U);
+    if (mode == 1) {
+        a.Ui = reinterpret_cast<double*>(base + L.Ui);
+        a.T = reinterpret_cast<double*>(base + L.T);
+        a.A0 = reinterpret_cast<double*>(base + L.A0);
+        a.A1 = reinterpret_cast<double*>(base + L.A1);
+        a.V = reinterpret_cast<double*>(base + L.V);
+        a.rank = reinterpret_cast<int*>(base + L.rank);
+        a.evals = evals;
+        a.evecs = evecs;
+    }
+    a.ctl = reinterpret_cast<Control*>(base + L.ctl);
+    return a;
+}
+
+cudaError_t launch_single(const EighArgs& a, cudaStream_t s, int* grid_out) {
+    if (a.n <= kSmallProblem) {
+        // one CTA: the grid barrier of a one-block launch never waits
+        void* params[] = {const_cast<EighArgs*>(&a)};
+        *grid_out = 1;
+        return cudaLaunchCooperativeKernel((const void*)eigh_grid_kernel, dim3(1), dim3(kThreads), params, 0, s);
+    }
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_grid_kernel, kThreads, 0);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int grid = sms;  // one CTA per SM
+    *grid_out = grid;
+    void* params[] = {const_cast<EighArgs*>(&a)};
+    return cudaLaunchCooperativeKernel((const void*)eigh_grid_kernel, dim3(grid), dim3(kThreads), params, 0, s);
+}
+
+}  // namespace
+}  // namespace vbcore
+
+using namespace vbcore;
+
+namespace {
+
+vb_status run_single(vb_context* ctx, int mode, const double* H, const double* S, int n, int mem, double* evals,
+                     double* evecs, double* U_out, int* info, const char* name) {
+    if (!ctx) return VB_ERR_INVALID;
+    if (info) *info = 0;
+    if (n < 1 || !S || (mode == 1 && (!H || !evals || !evecs)) || (mode == 0 && !U_out))
+        return set_error(ctx, VB_ERR_INVALID, std::string(name) + ": dimension must be positive and pointers non-null");
+    if (mem != VB_MEM_HOST && mem != VB_MEM_DEVICE) return set_error(ctx, VB_ERR_INVALID, "bad memory space");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const bool host = mem == VB_MEM_HOST;
+    const Layout L = layout_for(n, mode, host, host);
+    DeviceBuffer ws;
+    vb_status st = ws.allocate(ctx, L.total);
+    if (st != VB_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ws.ptr);
+    const size_t m2 = sizeof(double) * (size_t)n * n;
+    cudaError_t err = cudaSuccess;
+    const double* dS = S;
+    const double* dH = H;
+    double* dvals = evals;
+    double* dvecs = evecs;
+    double* dU = U_out;
+    if (host) {
+        err = cudaMemcpyAsync(base + L.S, S, m2, cudaMemcpyHostToDevice, s);
+        dS = reinterpret_cast<double*>(base + L.S);
+        if (mode == 1) {
+            if (err == cudaSuccess) err = cudaMemcpyAsync(base + L.H, H, m2, cudaMemcpyHostToDevice, s);
+            dH = reinterpret_cast<double*>(base + L.H);
+            dvals = reinterpret_cast<double*>(base + L.evals);
+            dvecs = reinterpret_cast<double*>(base + L.evecs);
+        }
+        dU = nullptr;
+    }
+    if (err == cudaSuccess) err = clear_workspace(base, L, n, mode, s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, name);
+    EighArgs a = args_for(base, L, n, mode, dH, dS, dvals, dvecs, mode == 0 ? dU : nullptr);
+    int grid = 0;
+    err = launch_single(a, s, &grid);
+    if (err != cudaSuccess) return cuda_error(ctx, err, name);
+    Control c{};
+    err = cudaMemcpyAsync(&c, base + L.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess && host) {
+        if (mode == 0)
+            err = cudaMemcpyAsync(U_out, base + L.U, m2, cudaMemcpyDeviceToHost, s);
+        else {
+            err = cudaMemcpyAsync(evals, dvals, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+            if (err == cudaSuccess) err = cudaMemcpyAsync(evecs, dvecs, m2, cudaMemcpyDeviceToHost, s);
+        }
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, name);
+    if (c.err) return set_error(ctx, VB_ERR_TIMEOUT, std::string(name) + ": grid barrier timed out");
+    if (c.info) {
+        if (info) *info = mode == 1 ? n + c.info : c.info;
+        return set_error(ctx, VB_ERR_NUMERIC,
+                         mode == 1 ? std::string(name) + ": overlap_matrix is not positive definite (info=" +
+                                         std::to_string(n + c.info) + ")"
+                                   : std::string(name) + ": matrix is not positive definite (leading minor " +
+                                         std::to_string(c.info) + ")");
+    }
+    if (mode == 1 && c.sweeps >= kMaxSweeps)
+        return set_error(ctx, VB_ERR_NUMERIC, std::string(name) + ": Jacobi iteration did not converge");
+    return VB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vb_status vb_metric_cholesky(vb_context* ctx, const double* S, int n, int mem_space, double* upper_out, int* info) {
+    return run_single(ctx, 0, nullptr, S, n, mem_space, nullptr, nullptr, upper_out, info, "vb_metric_cholesky");
+}
+
+vb_status vb_generalized_eigh(vb_context* ctx, const double* H, const double* S, int n, int mem_space,
+                              double* eigenvalues, double* eigenvectors, int* info) {
+    return run_single(ctx, 1, H, S, n, mem_space, eigenvalues, eigenvectors, nullptr, info, "vb_generalized_eigh");
+}
+
+vb_status vb_generalized_eigh_batched(vb_context* ctx, int count, const int* dims, const int64_t* offsets,
+                                      const double* H, const double* S, int mem_space, double* eigenvalues,
+                                      const int64_t* value_offsets, double* eigenvectors, int* info) {
+    if (!ctx) return VB_ERR_INVALID;
+    if (count < 0 || (count > 0 && (!dims || !offsets || !H || !S || !eigenvalues || !value_offsets ||
+                                    !eigenvectors || !info)))
+        return set_error(ctx, VB_ERR_INVALID, "vb_generalized_eigh_batched: bad arguments");
+    if (mem_space != VB_MEM_DEVICE)
+        return set_error(ctx, VB_ERR_INVALID, "vb_generalized_eigh_batched: device pointers only");
+    if (count == 0) return VB_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    std::vector<Layout> layouts(count);
+    std::vector<size_t> base_off(count);
+    size_t total = 0;
+    for (int b = 0; b < count; ++b) {
+        if (dims[b] < 1) return set_error(ctx, VB_ERR_INVALID, "vb_generalized_eigh_batched: dimension must be positive");
+        layouts[b] = layout_for(dims[b], 1, false, false);
+        base_off[b] = total;
+        total += layouts[b].total;
+    }
+    const size_t args_off = total;
+    total = align_up(total + sizeof(EighArgs) * count);
+    DeviceBuffer ws;
+    vb_status st = ws.allocate(ctx, total);
+    if (st != VB_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ws.ptr);
+    std::vector<EighArgs> args(count);
+    cudaError_t err = cudaSuccess;
+    for (int b = 0; b < count && err == cudaSuccess; ++b) {
+        unsigned char* pb = base + base_off[b];
+        err = clear_workspace(pb, layouts[b], dims[b], 1, s);
+        args[b] = args_for(pb, layouts[b], dims[b], 1, H + offsets[b], S + offsets[b], eigenvalues + value_offsets[b],
+                           eigenvectors + offsets[b], nullptr);
+    }
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(base + args_off, args.data(), sizeof(EighArgs) * count, cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess) {
+        eigh_block_kernel<<<count, kThreads, 0, s>>>(reinterpret_cast<const EighArgs*>(base + args_off), count);
+        err = cudaGetLastError();
+    }
+    std::vector<Control> ctl(count);
+    for (int b = 0; b < count && err == cudaSuccess; ++b)
+        err = cudaMemcpyAsync(&ctl[b], base + base_off[b] + layouts[b].ctl, sizeof(Control), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "vb_generalized_eigh_batched");
+    vb_status result = VB_OK;
+    for (int b = 0; b < count; ++b) {
+        info[b] = ctl[b].info ? dims[b] + ctl[b].info : (ctl[b].sweeps >= kMaxSweeps ? -1 : 0);
+        if (info[b] != 0 && result == VB_OK)
+            result = set_error(ctx, VB_ERR_NUMERIC,
+                               "vb_generalized_eigh_batched: problem " + std::to_string(b) +
+                                   (ctl[b].info ? " has an overlap matrix that is not positive definite"
+                                                : " did not converge"));
+    }
+    return result;
+}
+
+}  // extern "C"

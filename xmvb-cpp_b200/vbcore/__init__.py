@@ -32,9 +32,10 @@ _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "HBM budget excee
 
 
 class VbError(RuntimeError):
-    def __init__(self, status: int, message: str):
+    def __init__(self, status: int, message: str, info: int = 0):
         super().__init__(f"vbcore {_STATUS.get(status, status)}: {message}")
         self.status = status
+        self.info = info
 
 
 class _ExpansionSizes(ctypes.Structure):
@@ -65,7 +66,7 @@ EXPORTED_SYMBOLS = (
     "vb_context_memory", "vb_generate_structures", "vb_expand_structures", "vb_hs_plan_create",
     "vb_hs_plan_destroy", "vb_hs_plan_execute", "vb_hs_plan_stats", "vb_resolve_overlaps", "vb_same_spin_pairs",
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
-    "vb_spin_pairs_noalloc",
+    "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
 )
 
 PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
@@ -102,6 +103,9 @@ def load_library(path: str = LIB_PATH):
     lib.vb_hs_plan_phase_times.argtypes = [P, P, c.c_int]
     lib.vb_resolve_overlaps.argtypes = [P, c.c_int, c.c_int64, P, c.c_int, P, P, P]
     lib.vb_spin_pairs_noalloc.argtypes = [P, c.c_int, c.c_int, c.c_int, P, P, P, P, P]
+    lib.vb_metric_cholesky.argtypes = [P, P, c.c_int, c.c_int, P, c.POINTER(c.c_int)]
+    lib.vb_generalized_eigh.argtypes = [P, P, P, c.c_int, c.c_int, P, P, c.POINTER(c.c_int)]
+    lib.vb_generalized_eigh_batched.argtypes = [P, c.c_int, P, P, P, P, c.c_int, P, P, P, P]
     lib.vb_same_spin_pairs.argtypes = [P, c.c_int, c.c_int, c.c_int64, P, P, P, P, P, c.c_int, P, P]
     for name in EXPORTED_SYMBOLS:
         fn = getattr(lib, name)
@@ -111,10 +115,10 @@ def load_library(path: str = LIB_PATH):
     return lib
 
 
-def _check(status: int, ctx_handle=None):
+def _check(status: int, ctx_handle=None, info: int = 0):
     if status != 0:
         msg = load_library().vb_last_error(ctx_handle)
-        raise VbError(status, msg.decode() if msg else "")
+        raise VbError(status, msg.decode() if msg else "", info)
 
 
 def _ptr(a: np.ndarray):
@@ -279,6 +283,67 @@ def spin_pairs_noalloc(stream_handle: int, n_orbitals: int, k: int, n_strings: i
                                                 ctypes.c_void_p(strings_ptr), ctypes.c_void_p(S_ptr),
                                                 ctypes.c_void_p(h_ptr), ctypes.c_void_p(eri_ptr),
                                                 ctypes.c_void_p(out_ptr)))
+
+
+def metric_cholesky(ctx: "Context", S) -> np.ndarray:
+    """Upper Cholesky factor U of a symmetric positive-definite metric, S = U^T U (host
+    arrays; overlap_upper of the reference).  Raises VbError (info = failing minor order)."""
+    S = np.asarray(S, dtype=np.float64)
+    n = S.shape[0]
+    Sf = _c(S.T, np.float64)
+    U = np.empty(n * n, dtype=np.float64)
+    info = ctypes.c_int(0)
+    st = load_library().vb_metric_cholesky(ctx.handle, _ptr(Sf), n, VB_MEM_HOST, _ptr(U), ctypes.byref(info))
+    _check(st, ctx.handle, info.value)
+    return U.reshape(n, n).T.copy()
+
+
+def generalized_eigh(ctx: "Context", H, S):
+    """(eigenvalues ascending, eigenvectors as columns) of H C = S C E with dsygvd semantics
+    (GeneralizedEigensolver::solve_dense of the reference); host arrays."""
+    H = np.asarray(H, dtype=np.float64)
+    S = np.asarray(S, dtype=np.float64)
+    n = H.shape[0]
+    Hf = _c(H.T, np.float64)
+    Sf = _c(S.T, np.float64)
+    w = np.empty(n, dtype=np.float64)
+    C = np.empty(n * n, dtype=np.float64)
+    info = ctypes.c_int(0)
+    st = load_library().vb_generalized_eigh(ctx.handle, _ptr(Hf), _ptr(Sf), n, VB_MEM_HOST, _ptr(w), _ptr(C),
+                                            ctypes.byref(info))
+    _check(st, ctx.handle, info.value)
+    return w, C.reshape(n, n).T.copy()
+
+
+def generalized_eigh_batched(ctx: "Context", problems, device=None):
+    """Batched dense eigenproblems [(H, S), ...] (host arrays in, host results out), solved
+    on the device one CTA per problem; returns [(eigenvalues, eigenvectors), ...]."""
+    import torch
+
+    dev = torch.device("cuda", ctx.device) if device is None else device
+    dims = np.array([np.asarray(H).shape[0] for H, _ in problems], dtype=np.int32)
+    sizes = dims.astype(np.int64) ** 2
+    offsets = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    voff = np.concatenate([[0], np.cumsum(dims.astype(np.int64))[:-1]]).astype(np.int64)
+    Hcat = np.concatenate([np.asarray(H, dtype=np.float64).T.ravel() for H, _ in problems])
+    Scat = np.concatenate([np.asarray(S, dtype=np.float64).T.ravel() for _, S in problems])
+    dH = torch.tensor(Hcat, device=dev)
+    dS = torch.tensor(Scat, device=dev)
+    dw = torch.empty(int(dims.sum()), dtype=torch.float64, device=dev)
+    dC = torch.empty(int(sizes.sum()), dtype=torch.float64, device=dev)
+    info = np.zeros(len(problems), dtype=np.int32)
+    torch.cuda.synchronize(dev)
+    st = load_library().vb_generalized_eigh_batched(ctx.handle, len(problems), _ptr(dims), _ptr(offsets),
+                                                    ctypes.c_void_p(dH.data_ptr()), ctypes.c_void_p(dS.data_ptr()),
+                                                    VB_MEM_DEVICE, ctypes.c_void_p(dw.data_ptr()), _ptr(voff),
+                                                    ctypes.c_void_p(dC.data_ptr()), _ptr(info))
+    _check(st, ctx.handle, int(info[info != 0][0]) if np.any(info != 0) else 0)
+    w = dw.cpu().numpy()
+    C = dC.cpu().numpy()
+    out = []
+    for b, n in enumerate(dims):
+        out.append((w[voff[b]:voff[b] + n].copy(), C[offsets[b]:offsets[b] + n * n].reshape(n, n).T.copy()))
+    return out
 
 
 class HsPlan:
