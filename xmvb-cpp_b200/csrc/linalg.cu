@@ -11,11 +11,11 @@
 //
 // Method (one kernel): blocked right-looking Cholesky (32-column panels), blocked inverse of
 // the triangular factor, A = U^-T H U^-1 and C = U^-1 Q as tiled GEMMs, and the symmetric
-// eigenproblem of A by cyclic Jacobi in round-robin (tournament) order: every round rotates
-// m/2 disjoint pivot pairs at once, so one round is a single pass over A (two-sided 2 x 2 block
-// updates, ping-pong buffers) and over the eigenvector matrix.  Jacobi needs no
-// tridiagonalization, is embarrassingly parallel within a round and attains eigenvalues to
-// working accuracy (quadratic convergence, typically 8-10 sweeps).
+// eigenproblem of A by block Jacobi in round-robin (tournament) order over 16-index blocks:
+// each round diagonalizes the 32 x 32 subproblems of m_b / 2 disjoint block pairs in shared
+// memory and applies the resulting orthogonal 32 x 32 factors to A and the eigenvectors as
+// small GEMMs.  Jacobi needs no tridiagonalization, is parallel within a round and converges
+// quadratically.
 //
 // A single problem runs as a cooperative launch (one CTA per SM) whose phases are separated
 // by a grid barrier with a bounded spin; a batch runs one problem per CTA with __syncthreads.
@@ -60,6 +60,7 @@ struct EighArgs {
     double* A0;          // ping-pong n x n
     double* A1;
     double* V;           // Jacobi rotations (zero-initialised)
+    double* W;           // per block pair 32 x 32 subproblem rotations
     int* rank;           // n
     double* evals;       // n
     double* evecs;       // n x n
@@ -358,92 +359,212 @@ __device__ __forceinline__ void round_pair(int m, int r, int i, int* p, int* q) 
     *q = max(a, b);
 }
 
-// Jacobi rotation J = [[c, s], [-s, c]] annihilating a_pq in J^T A J (Golub & Van Loan,
-// Algorithm 8.4.1); rotations below the threshold are skipped (c = 1, s = 0).
-__device__ __forceinline__ bool jacobi_rotation(const double* A, int n, int p, int q, double skip_abs, double* c,
-                                                double* s, double* t) {
-    *c = 1.0;
-    *s = 0.0;
-    *t = 0.0;
-    if (q >= n) return false;  // padding index of odd n
-    const double app = ld(A + p + (long long)p * n), aqq = ld(A + q + (long long)q * n);
-    const double apq = ld(A + p + (long long)q * n);
-    const double aapq = fabs(apq);
-    if (aapq <= skip_abs || aapq <= 1.0e-15 * sqrt(fabs(app) * fabs(aqq))) return false;
-    const double tau = (aqq - app) / (2.0 * apq);
-    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
-    const double cc = 1.0 / sqrt(1.0 + tt * tt);
-    *c = cc;
-    *s = tt * cc;
-    *t = tt;
-    return true;
+// Block Jacobi.  Indices are grouped in blocks of kHalf = 16; block pairs (P, Q) meet in
+// round-robin order, m_b - 1 rounds per sweep.  A round (1) diagonalizes every 32 x 32
+// subproblem [[A_PP, A_PQ], [A_QP, A_QQ]] by one cyclic Jacobi sweep in shared memory, giving an
+// orthogonal W per pair, and (2) applies them: A'[I_i, I_j] = W_i^T A[I_i, I_j] W_j for all pair
+// combinations (ping-pong buffers) and V[:, I_i] <- V[:, I_i] W_i.  Rotations of the inner sweep
+// use J = [[c, s], [-s, c]] annihilating g_pq in J^T G J (Golub & Van Loan, Algorithm 8.4.1) and
+// are skipped when |g_pq| <= 1e-15 sqrt(|g_pp g_qq|) or <= 1e-14 ||A||_F (the rounding level of
+// the blocked update); a sweep without an applied rotation ends the iteration.
+constexpr int kHalf = 16;
+
+__device__ __forceinline__ int sub_index(int P, int Q, int l, int n) {
+    const int g = l < kHalf ? P * kHalf + l : Q * kHalf + (l - kHalf);
+    return g < n ? g : -1;
 }
 
 template <class Sync>
 __device__ bool jacobi(const EighArgs& a, const Sync& sync, Shared& sh, int cta, int ncta, double** A_final) {
     const int n = a.n;
-    const int m = n + (n & 1);
-    const int half = m / 2;
+    const int nbk = (n + kHalf - 1) / kHalf;
+    const int mb = nbk + (nbk & 1);
+    const int pairs = mb / 2;
     const int tid = threadIdx.x;
-    const long long gtid = (long long)cta * blockDim.x + tid, gstride = (long long)ncta * blockDim.x;
-    const double skip_abs = 1.0e-18 * sqrt(ld(&a.ctl->fro2)) + 1.0e-300;
+    const double fro = sqrt(ld(&a.ctl->fro2));
+    const double skip_abs = 1.0e-14 * fro + 1.0e-300;
     double* Ain = a.A0;
     double* Aout = a.A1;
+    double* Wg = a.W;
+    __shared__ double rc[kHalf], rs[kHalf], rt[kHalf];
+    __shared__ int rapplied, roff;
+    __shared__ unsigned char inner_p[kTile - 1][kHalf], inner_q[kTile - 1][kHalf];
+    for (int e = tid; e < (kTile - 1) * kHalf; e += blockDim.x) {
+        int p, q;
+        round_pair(kTile, e / kHalf, e % kHalf, &p, &q);
+        inner_p[e / kHalf][e % kHalf] = (unsigned char)p;
+        inner_q[e / kHalf][e % kHalf] = (unsigned char)q;
+    }
+    __syncthreads();
     for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
         if (cta == 0 && tid == 0) a.ctl->rotations[(sweep + 1) % 3] = 0u;
-        for (int r = 0; r < m - 1; ++r) {
-            unsigned applied = 0;
-            for (long long b = gtid; b < (long long)half * half; b += gstride) {
-                const int i = (int)(b % half), j = (int)(b / half);
-                int pi, qi, pj, qj;
-                round_pair(m, r, i, &pi, &qi);
-                round_pair(m, r, j, &pj, &qj);
-                double ci, si, ti, cj, sj, tj;
-                const bool roti = jacobi_rotation(Ain, n, pi, qi, skip_abs, &ci, &si, &ti);
-                if (i == j) {
-                    // diagonal block: exact annihilation
-                    const double app = ld(Ain + pi + (long long)pi * n);
-                    if (qi < n) {
-                        const double aqq = ld(Ain + qi + (long long)qi * n);
-                        const double apq = ld(Ain + pi + (long long)qi * n);
-                        Aout[pi + (long long)pi * n] = roti ? app - ti * apq : app;
-                        Aout[qi + (long long)qi * n] = roti ? aqq + ti * apq : aqq;
-                        Aout[pi + (long long)qi * n] = roti ? 0.0 : apq;
-                        Aout[qi + (long long)pi * n] = roti ? 0.0 : apq;
-                        applied += roti ? 1u : 0u;
-                    } else {
-                        Aout[pi + (long long)pi * n] = app;
-                    }
-                    continue;
+        for (int r = 0; r < mb - 1; ++r) {
+            // (1) one Jacobi sweep on each 32 x 32 subproblem
+            for (int i = cta; i < pairs; i += ncta) {
+                int P, Q;
+                round_pair(mb, r, i, &P, &Q);
+                for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                    const int l = e % kTile, c = e / kTile;
+                    const int gl = sub_index(P, Q, l, n), gc = sub_index(P, Q, c, n);
+                    sh.a[l][c] = (gl >= 0 && gc >= 0) ? ld(Ain + gl + (long long)gc * n) : 0.0;
+                    sh.b[l][c] = l == c ? 1.0 : 0.0;
                 }
-                jacobi_rotation(Ain, n, pj, qj, skip_abs, &cj, &sj, &tj);
-                // B' = J_i^T B J_j with B = [[A(pi,pj), A(pi,qj)], [A(qi,pj), A(qi,qj)]]
-                const double b00 = ld(Ain + pi + (long long)pj * n);
-                const double b01 = qj < n ? ld(Ain + pi + (long long)qj * n) : 0.0;
-                const double b10 = qi < n ? ld(Ain + qi + (long long)pj * n) : 0.0;
-                const double b11 = (qi < n && qj < n) ? ld(Ain + qi + (long long)qj * n) : 0.0;
-                const double x00 = cj * b00 - sj * b01, x01 = sj * b00 + cj * b01;
-                const double x10 = cj * b10 - sj * b11, x11 = sj * b10 + cj * b11;
-                Aout[pi + (long long)pj * n] = ci * x00 - si * x10;
-                if (qj < n) Aout[pi + (long long)qj * n] = ci * x01 - si * x11;
-                if (qi < n) Aout[qi + (long long)pj * n] = si * x00 + ci * x10;
-                if (qi < n && qj < n) Aout[qi + (long long)qj * n] = si * x01 + ci * x11;
+                if (tid == 0) {
+                    rapplied = 0;
+                    roff = 0;
+                }
+                __syncthreads();
+                // a subproblem that is already diagonal to the thresholds keeps W = I
+                for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                    const int l = e % kTile, c = e / kTile;
+                    if (l < c) {
+                        const double v = fabs(sh.a[l][c]);
+                        if (v > skip_abs && v > 1.0e-15 * sqrt(fabs(sh.a[l][l]) * fabs(sh.a[c][c]))) roff = 1;
+                    }
+                }
+                __syncthreads();
+                for (int ir = 0; ir < kTile - 1 && roff; ++ir) {
+                    if (tid < kHalf) {
+                        const int p = inner_p[ir][tid], q = inner_q[ir][tid];
+                        double c = 1.0, sn = 0.0, t = 0.0;
+                        if (sub_index(P, Q, p, n) >= 0 && sub_index(P, Q, q, n) >= 0) {
+                            const double app = sh.a[p][p], aqq = sh.a[q][q], apq = sh.a[p][q];
+                            const double aapq = fabs(apq);
+                            if (aapq > skip_abs && aapq > 1.0e-15 * sqrt(fabs(app) * fabs(aqq))) {
+                                // t = tan of the rotation angle, |t| <= 1 (the smaller root)
+                                const double d = aqq - app;
+                                const double two = 2.0 * apq;
+                                const double den = fabs(d) + sqrt(fma(d, d, two * two));
+                                t = (d >= 0.0 ? two : -two) / den;
+                                c = rsqrt(fma(t, t, 1.0));
+                                sn = t * c;
+                                atomicAdd(&rapplied, 1);
+                            }
+                        }
+                        rc[tid] = c;
+                        rs[tid] = sn;
+                        rt[tid] = t;
+                    }
+                    __syncthreads();
+                    {
+                        // 2 x 2 block (bi, bj) of the subproblem, one per thread
+                        const int bi = tid % kHalf, bj = tid / kHalf;
+                        const int pi = inner_p[ir][bi], qi = inner_q[ir][bi];
+                        const int pj = inner_p[ir][bj], qj = inner_q[ir][bj];
+                        const double ci = rc[bi], si = rs[bi], cj = rc[bj], sj = rs[bj];
+                        if (bi == bj) {
+                            if (si != 0.0) {
+                                const double apq = sh.a[pi][qi], ti = rt[bi];
+                                sh.a[pi][pi] -= ti * apq;
+                                sh.a[qi][qi] += ti * apq;
+                                sh.a[pi][qi] = 0.0;
+                                sh.a[qi][pi] = 0.0;
+                            }
+                        } else if (si != 0.0 || sj != 0.0) {
+                            const double b00 = sh.a[pi][pj], b01 = sh.a[pi][qj];
+                            const double b10 = sh.a[qi][pj], b11 = sh.a[qi][qj];
+                            const double x00 = cj * b00 - sj * b01, x01 = sj * b00 + cj * b01;
+                            const double x10 = cj * b10 - sj * b11, x11 = sj * b10 + cj * b11;
+                            sh.a[pi][pj] = ci * x00 - si * x10;
+                            sh.a[pi][qj] = ci * x01 - si * x11;
+                            sh.a[qi][pj] = si * x00 + ci * x10;
+                            sh.a[qi][qj] = si * x01 + ci * x11;
+                        }
+                        // W <- W J: rows x, pair k (two per thread)
+                        for (int u = tid; u < kTile * kHalf; u += blockDim.x) {
+                            const int x = u % kTile, k = u / kTile;
+                            const double sk = rs[k];
+                            if (sk == 0.0) continue;
+                            const int p = inner_p[ir][k], q = inner_q[ir][k];
+                            const double ck = rc[k];
+                            const double wp = sh.b[x][p], wq = sh.b[x][q];
+                            sh.b[x][p] = ck * wp - sk * wq;
+                            sh.b[x][q] = sk * wp + ck * wq;
+                        }
+                    }
+                    __syncthreads();
+                }
+                for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                    const int l = e % kTile, c = e / kTile;
+                    Wg[(long long)i * kTile * kTile + l + c * kTile] = sh.b[l][c];
+                }
+                if (tid == 0 && rapplied) atomicAdd(&a.ctl->rotations[sweep % 3], (unsigned)rapplied);
+                __syncthreads();
             }
-            // eigenvector columns: V <- V J
-            for (long long u = gtid; u < (long long)n * half; u += gstride) {
-                const int k = (int)(u % n), i = (int)(u / n);
-                int p, q;
-                round_pair(m, r, i, &p, &q);
-                double c, s, t;
-                if (!jacobi_rotation(Ain, n, p, q, skip_abs, &c, &s, &t)) continue;
-                const double vp = ld(a.V + k + (long long)p * n), vq = ld(a.V + k + (long long)q * n);
-                a.V[k + (long long)p * n] = c * vp - s * vq;
-                a.V[k + (long long)q * n] = s * vp + c * vq;
-            }
-            // rotation count of this round (warp reduction, one atomic per warp)
+            if (!sync()) return false;
+            // (2) apply: A' = W_i^T A W_j per pair combination, V <- V W
+            const int chunks = (n + kTile - 1) / kTile;
+            const int a_tasks = pairs * pairs;
+            for (int task = cta; task < a_tasks + chunks * pairs; task += ncta) {
+                const int l = tid & 31, cq = tid >> 5;
+                if (task < a_tasks) {
+                    const int i = task % pairs, j = task / pairs;
+                    int Pi, Qi, Pj, Qj;
+                    round_pair(mb, r, i, &Pi, &Qi);
+                    round_pair(mb, r, j, &Pj, &Qj);
+                    for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                        const int x = e % kTile, c = e / kTile;
+                        const int gx = sub_index(Pi, Qi, x, n), gc = sub_index(Pj, Qj, c, n);
+                        sh.a[x][c] = (gx >= 0 && gc >= 0) ? ld(Ain + gx + (long long)gc * n) : 0.0;
+                        sh.b[x][c] = ld(Wg + (long long)i * kTile * kTile + x + c * kTile);
+                    }
+                    __syncthreads();
+                    double y[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+                    for (int k = 0; k < kTile; ++k) {
+                        const double w = sh.b[k][l];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) applied += __shfl_xor_sync(0xffffffffu, applied, o);
-            if ((tid & 31) == 0 && applied) atomicAdd(&a.ctl->rotations[sweep % 3], applied);
+                        for (int q = 0; q < 4; ++q) y[q] = fma(w, sh.a[k][cq + 8 * q], y[q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) sh.d[l][cq + 8 * q] = y[q];
+                    __syncthreads();
+                    for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                        const int x = e % kTile, c = e / kTile;
+                        sh.a[x][c] = ld(Wg + (long long)j * kTile * kTile + x + c * kTile);
+                    }
+                    __syncthreads();
+                    double z[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+                    for (int k = 0; k < kTile; ++k) {
+                        const double yv = sh.d[l][k];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) z[q] = fma(yv, sh.a[k][cq + 8 * q], z[q]);
+                    }
+                    const int gl = sub_index(Pi, Qi, l, n);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int gc = sub_index(Pj, Qj, cq + 8 * q, n);
+                        if (gl >= 0 && gc >= 0) Aout[gl + (long long)gc * n] = z[q];
+                    }
+                } else {
+                    const int v = task - a_tasks;
+                    const int chunk = v % chunks, j = v / chunks;
+                    int Pj, Qj;
+                    round_pair(mb, r, j, &Pj, &Qj);
+                    for (int e = tid; e < kTile * kTile; e += blockDim.x) {
+                        const int x = e % kTile, c = e / kTile;
+                        const int gx = chunk * kTile + x, gc = sub_index(Pj, Qj, c, n);
+                        sh.a[x][c] = (gx < n && gc >= 0) ? ld(a.V + gx + (long long)gc * n) : 0.0;
+                        sh.b[x][c] = ld(Wg + (long long)j * kTile * kTile + x + c * kTile);
+                    }
+                    __syncthreads();
+                    double z[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+                    for (int k = 0; k < kTile; ++k) {
+                        const double xv = sh.a[l][k];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) z[q] = fma(xv, sh.b[k][cq + 8 * q], z[q]);
+                    }
+                    const int gx = chunk * kTile + l;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int gc = sub_index(Pj, Qj, cq + 8 * q, n);
+                        if (gx < n && gc >= 0) a.V[gx + (long long)gc * n] = z[q];
+                    }
+                }
+                __syncthreads();
+            }
             double* tmp = Ain;
             Ain = Aout;
             Aout = tmp;
@@ -533,7 +654,7 @@ __global__ void __launch_bounds__(kThreads) eigh_block_kernel(const EighArgs* __
 
 // Workspace of one problem (doubles / ints), all offsets 256-byte aligned.
 struct Layout {
-    size_t U, Ui, T, A0, A1, V, evals, evecs, H, S, rank, ctl, total;
+    size_t U, Ui, T, A0, A1, V, W, evals, evecs, H, S, rank, ctl, total;
 };
 
 size_t align_up(size_t x) { return (x + 255) / 256 * 256; }
@@ -554,6 +675,8 @@ Layout layout_for(int n, int mode, bool own_inputs, bool own_outputs) {
         L.A0 = take(m2);
         L.A1 = take(m2);
         L.V = take(m2);
+        const int nbk = (n + 15) / 16;
+        L.W = take(sizeof(double) * 1024 * (size_t)((nbk + (nbk & 1)) / 2));
         L.rank = take(sizeof(int) * n);
         if (own_outputs) {
             L.evals = take(sizeof(double) * n);
@@ -590,6 +713,7 @@ EighArgs args_for(unsigned char* base, const Layout& L, int n, int mode, const d
         a.A0 = reinterpret_cast<double*>(base + L.A0);
         a.A1 = reinterpret_cast<double*>(base + L.A1);
         a.V = reinterpret_cast<double*>(base + L.V);
+        a.W = reinterpret_cast<double*>(base + L.W);
         a.rank = reinterpret_cast<int*>(base + L.rank);
         a.evals = evals;
         a.evecs = evecs;
