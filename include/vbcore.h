@@ -201,6 +201,26 @@ vb_status vb_generalized_eigh_batched(vb_context* ctx, int count, const int* dim
                                       const double* H, const double* S, int mem_space, double* eigenvalues,
                                       const int64_t* value_offsets, double* eigenvectors, int* info);
 
+/* ---- RI AO -> active-space transform ----------------------------------------------------------- */
+
+/* transform_ri_active_integrals (src/integrals/active/ri.cpp:33-96) in FP64.  B_packed:
+ * metric-whitened AO-pair factors [n_aux x n_bf(n_bf+1)/2], column-major (row = auxiliary
+ * function, column = AO pair hi(hi+1)/2+lo; RiAoFactorization::metric_whitened_ao_pair_factors);
+ * C: active coefficients [n_bf x n_act], column-major, n_act <= 16.  Outputs:
+ *   one_index [(n_act n_aux) x n_bf], row a*n_aux + P (ri_one_index_factors; may be NULL),
+ *   L [n_aux x n_act(n_act+1)/2] (ri_active_pair_factors),
+ *   K_packed [P(P+1)/2] (pack_ri_active_integrals, ri.cpp:13-31; may be NULL).
+ * VB_MEM_HOST: synchronous.  VB_MEM_DEVICE: stream-ordered on the context stream. */
+vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_aux, int n_bf, const double* C,
+                                 int n_act, int mem_space, double* one_index, double* L, double* K_packed);
+
+/* Adjoint of the transform: given dE/dL [n_aux x n_act(n_act+1)/2] and the one-index factors
+ * of the forward call, dE/dC [n_bf x n_act] (column-major), the orbital pull-back of RI pair
+ * factors that the reference's gradients take from ri_one_index_factors
+ * (src/integrals/response/ri.cpp:370). */
+vb_status vb_active_transform_ri_adjoint(vb_context* ctx, const double* one_index, const double* dL, int n_aux,
+                                         int n_bf, int n_act, int mem_space, double* dC);
+
 /* ---- allocation-free spin-pair evaluation ------------------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot allocate device memory where

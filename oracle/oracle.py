@@ -196,6 +196,33 @@ def ri_transform(B_packed: np.ndarray, C: np.ndarray, threads: int = 0):
     return L.T.copy(), K
 
 
+def ri_one_index(B_packed: np.ndarray, C: np.ndarray) -> np.ndarray:
+    """One-index RI factors T [(n_act n_aux), n_bf], row a*n_aux + P:
+    T[(a, P), mu] = sum_nu B_P(mu, nu) C(nu, a) (transform_ri_one_index,
+    src/integrals/ao/ri_transform.cpp:10-37, stored as ri_one_index_factors in
+    src/integrals/active/ri.cpp:80-90)."""
+    n_aux = B_packed.shape[0]
+    n_bf, n_act = C.shape
+    idx = np.array([[pair_index(m, v) for v in range(n_bf)] for m in range(n_bf)])
+    Bfull = B_packed[:, idx]  # [n_aux, mu, nu]
+    T = np.einsum("Pmn,na->aPm", Bfull, C)
+    return T.reshape(n_act * n_aux, n_bf)
+
+
+def ri_adjoint(T: np.ndarray, G: np.ndarray, n_act: int) -> np.ndarray:
+    """dE/dC from dE/dL for L[P, pair(a,b)] = sum_{mu,nu} C(mu,a) B_P(mu,nu) C(nu,b) (the
+    derivative of transform_ri_active_integrals, src/integrals/active/ri.cpp:33-96):
+    dE/dC(kappa, c) = sum_{P,b} G[P, pair(c,b)] (1 + delta_cb) T[(b, P), kappa]."""
+    n_aux = G.shape[0]
+    n_bf = T.shape[1]
+    Gs = np.zeros((n_aux, n_act, n_act))
+    for c in range(n_act):
+        for b in range(n_act):
+            Gs[:, c, b] = G[:, pair_index(c, b)] * (2.0 if c == b else 1.0)
+    T3 = T.reshape(n_act, n_aux, n_bf)
+    return np.einsum("Pcb,bPk->kc", Gs, T3)
+
+
 # ----------------------------------------------------------------------------------------------
 # metric Cholesky and the dense structure eigenproblem
 

@@ -109,3 +109,35 @@ def test_linalg_oracle_is_dsygvd():
     wr = np.linalg.eigvalsh(Ui.T @ H @ Ui)
     assert np.abs(w - wr).max() < 1e-12 * np.abs(w).max()
     assert np.abs(C.T @ S @ C - np.eye(n)).max() < 1e-10
+
+
+def _ri_inputs(n_aux, n_bf, n_act, seed):
+    rng = np.random.default_rng(seed)
+    npair = n_bf * (n_bf + 1) // 2
+    B = rng.standard_normal((n_aux, npair))
+    C = rng.standard_normal((n_bf, n_act)) / np.sqrt(n_bf)
+    return B, C
+
+
+def test_ri_oracle_restatements_agree():
+    # the numpy one-index factors reproduce the C++ restatement's L, and the adjoint matches
+    # central differences of a linear functional of L (exact up to rounding: L is quadratic in C)
+    n_aux, n_bf, n_act = 9, 7, 3
+    B, C = _ri_inputs(n_aux, n_bf, n_act, 1)
+    L, K = O.ri_transform(B, C)
+    T = O.ri_one_index(B, C)
+    L2 = np.zeros_like(L)
+    T3 = T.reshape(n_act, n_aux, n_bf)
+    for a in range(n_act):
+        for b in range(a + 1):
+            L2[:, O.pair_index(a, b)] = T3[a] @ C[:, b]
+    assert np.abs(L - L2).max() < 1e-13
+    assert np.abs(K - np.array([L[:, p] @ L[:, q] for p in range(L.shape[1]) for q in range(p + 1)])).max() < 1e-12
+    rng = np.random.default_rng(2)
+    G = rng.standard_normal(L.shape)
+    dC = O.ri_adjoint(T, G, n_act)
+    D = rng.standard_normal(C.shape)
+    h = 1e-3
+    fp = np.sum(G * O.ri_transform(B, C + h * D)[0])
+    fm = np.sum(G * O.ri_transform(B, C - h * D)[0])
+    assert abs((fp - fm) / (2 * h) - np.sum(dC * D)) < 1e-9

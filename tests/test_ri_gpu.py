@@ -1,0 +1,87 @@
+"""RI AO -> active transform on the device against the oracle (transform_ri_active_integrals,
+src/integrals/active/ri.cpp:33-96), including the one-index factors and the adjoint."""
+
+import numpy as np
+import pytest
+
+import oracle as O
+import vbcore
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = vbcore.Context(0)
+    yield c
+    c.close()
+
+
+def _inputs(n_aux, n_bf, n_act, seed, decay=None):
+    rng = np.random.default_rng(seed)
+    npair = n_bf * (n_bf + 1) // 2
+    B = rng.standard_normal((n_aux, npair))
+    if decay:
+        idx = np.array([(m, v) for m in range(n_bf) for v in range(m + 1)])
+        B *= np.exp(-np.abs(idx[:, 0] - idx[:, 1]) / decay)[None, :]
+    C = rng.standard_normal((n_bf, n_act)) / np.sqrt(n_bf)
+    return B, C
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(1e-300, np.abs(b).max())
+
+
+@pytest.mark.parametrize("n_aux,n_bf,n_act", [(1, 1, 1), (10, 7, 3), (37, 20, 6), (129, 50, 1), (130, 33, 16),
+                                              (300, 64, 16), (257, 300, 8)])
+def test_transform_matches_oracle(ctx, n_aux, n_bf, n_act):
+    B, C = _inputs(n_aux, n_bf, n_act, n_aux + n_bf + n_act)
+    L, K, T = vbcore.active_transform_ri(ctx, B, C, one_index=True)
+    Lr, Kr = O.ri_transform(B, C)
+    assert _rel(L, Lr) < 1e-13
+    assert _rel(K, Kr) < 1e-13
+    if n_aux * n_bf * n_bf <= 300 * 64 * 64:
+        assert _rel(T, O.ri_one_index(B, C)) < 1e-13
+
+
+@pytest.mark.parametrize("n_aux,n_bf,n_act", [(10, 7, 3), (130, 33, 16), (64, 100, 5)])
+def test_adjoint_matches_oracle_and_differences(ctx, n_aux, n_bf, n_act):
+    B, C = _inputs(n_aux, n_bf, n_act, 5)
+    L, _, T = vbcore.active_transform_ri(ctx, B, C, one_index=True)
+    rng = np.random.default_rng(6)
+    G = rng.standard_normal(L.shape)
+    dC = vbcore.active_transform_ri_adjoint(ctx, T, G, n_bf)
+    assert _rel(dC, O.ri_adjoint(T, G, n_act)) < 1e-12
+    D = rng.standard_normal(C.shape)
+    h = 1e-3
+    fp = np.sum(G * vbcore.active_transform_ri(ctx, B, C + h * D)[0])
+    fm = np.sum(G * vbcore.active_transform_ri(ctx, B, C - h * D)[0])
+    assert abs((fp - fm) / (2 * h) - np.sum(dC * D)) < 1e-8 * max(1.0, abs(np.sum(dC * D)))
+
+
+def test_full_size_precision_workload(ctx):
+    # n_bf 400, n_aux 1600, n_act 16 with |mu - nu| decay 20: every output against the oracle
+    # on a slice of auxiliary rows (L and its rows are independent per auxiliary function),
+    # plus size-independent properties of the whole result
+    n_aux, n_bf, n_act = 1600, 400, 16
+    B, C = _inputs(n_aux, n_bf, n_act, 20261203, decay=20.0)
+    L, K, _ = vbcore.active_transform_ri(ctx, B, C)
+    rows = np.arange(0, n_aux, 25)
+    Lr, _ = O.ri_transform(B[rows], C)
+    assert _rel(L[rows], Lr) < 1e-13
+    P = n_act * (n_act + 1) // 2
+    Kfull = np.zeros((P, P))
+    iu = np.tril_indices(P)
+    Kfull[iu] = K
+    Kfull = Kfull + np.tril(Kfull, -1).T
+    assert _rel(Kfull, L.T @ L) < 1e-13
+    # linearity in B
+    L2, _, _ = vbcore.active_transform_ri(ctx, 2.0 * B, C)
+    assert np.array_equal(L2, 2.0 * L)
+
+
+def test_rejects_too_many_active_orbitals(ctx):
+    B, C = _inputs(4, 20, 17, 1)
+    with pytest.raises(vbcore.VbError) as e:
+        vbcore.active_transform_ri(ctx, B, C)
+    assert e.value.status == 5

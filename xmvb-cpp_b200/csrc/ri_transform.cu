@@ -1,0 +1,460 @@
+// RI AO -> active-space transform of the metric-whitened three-index factors, FP64
+// (transform_ri_active_integrals, src/integrals/active/ri.cpp:33-96;
+//  transform_ri_one_index, src/integrals/ao/ri_transform.cpp:10-37;
+//  pack_ri_active_integrals, src/integrals/active/ri.cpp:13-31), and its adjoint.
+//
+// Layouts (column-major, as the reference's Eigen matrices):
+//   B  [n_aux x NP], NP = n_bf (n_bf + 1) / 2, B[P + pair(mu, nu) n_aux]
+//   C  [n_bf x n_act]
+//   T  one-index factors [(n_act n_aux) x n_bf], T[(a n_aux + P) + mu n_act n_aux]
+//        = sum_nu B_P(mu, nu) C(nu, a)                                     (ri_one_index_factors)
+//   L  [n_aux x n_act (n_act + 1) / 2], L[P + pair(a, b) n_aux] = sum_mu T[a, P, mu] C(mu, b)
+//   K  packed, K[pair(p, q)] = sum_P L[P, p] L[P, q]
+//
+// one_index_kernel carries the flops (2 n_aux n_bf^2 n_act): a warp owns one AO index mu and
+// 128 auxiliary rows (4 per lane) and accumulates T[a, P, mu] for all n_act orbitals in
+// registers (64 FP64 accumulators per lane), streaming the AO-pair columns pair(mu, nu) of B
+// (1 KB coalesced per column) against C rows staged in shared memory.  Each packed column is
+// needed by two AO indices (mu and nu); CTAs are ordered AO index fastest so that both uses of
+// an auxiliary tile's slice of B (82 MB for 128 auxiliary functions at n_bf = 400) fall in
+// the same wave and the second read is an L2 hit: B crosses HBM about once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace vbcore {
+namespace {
+
+constexpr int kMaxActive = 16;
+constexpr int kRowsPerLane = 4;
+constexpr int kAuxTile = 32 * kRowsPerLane;  // auxiliary rows per warp
+constexpr int kWarpsPerCta = 4;              // AO indices per CTA
+constexpr int kNuChunk = 256;                // C rows staged per shared-memory chunk
+
+__device__ __forceinline__ long long ao_pair(int a, int b) {
+    const long long hi = a > b ? a : b, lo = a > b ? b : a;
+    return hi * (hi + 1) / 2 + lo;
+}
+
+// T[a, P, mu] = sum_nu B[P, pair(mu, nu)] C(nu, a).  grid.x = AO-index groups (fastest),
+// grid.y = auxiliary tiles.
+__global__ void __launch_bounds__(32 * kWarpsPerCta) one_index_kernel(const double* __restrict__ B, int n_aux, int n_bf,
+                                                                      const double* __restrict__ C, int n_act,
+                                                                      double* __restrict__ T) {
+    __shared__ __align__(16) double sC[kNuChunk][kMaxActive];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mu = blockIdx.x * kWarpsPerCta + warp;
+    const int aux0 = blockIdx.y * kAuxTile;
+    double acc[kRowsPerLane][kMaxActive];
+#pragma unroll
+    for (int i = 0; i < kRowsPerLane; ++i)
+#pragma unroll
+        for (int a = 0; a < kMaxActive; ++a) acc[i][a] = 0.0;
+    bool row_ok[kRowsPerLane];
+#pragma unroll
+    for (int i = 0; i < kRowsPerLane; ++i) row_ok[i] = aux0 + lane + 32 * i < n_aux;
+    for (int nu0 = 0; nu0 < n_bf; nu0 += kNuChunk) {
+        const int cnt = min(kNuChunk, n_bf - nu0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < cnt * kMaxActive; e += blockDim.x) {
+            const int a = e / cnt, nu = e % cnt;
+            sC[nu][a] = a < n_act ? __ldg(C + nu0 + nu + (long long)a * n_bf) : 0.0;
+        }
+        __syncthreads();
+        if (mu < n_bf) {
+            const double* base = B + aux0 + lane;
+#pragma unroll 2
+            for (int nu = 0; nu < cnt; ++nu) {
+                const double* col = base + ao_pair(mu, nu0 + nu) * n_aux;
+                double b[kRowsPerLane];
+#pragma unroll
+                for (int i = 0; i < kRowsPerLane; ++i) b[i] = row_ok[i] ? __ldg(col + 32 * i) : 0.0;
+                const double2* c2 = reinterpret_cast<const double2*>(&sC[nu][0]);
+#pragma unroll
+                for (int h = 0; h < kMaxActive / 2; ++h) {
+                    const double2 c = c2[h];
+#pragma unroll
+                    for (int i = 0; i < kRowsPerLane; ++i) {
+                        acc[i][2 * h] = fma(b[i], c.x, acc[i][2 * h]);
+                        acc[i][2 * h + 1] = fma(b[i], c.y, acc[i][2 * h + 1]);
+                    }
+                }
+            }
+        }
+    }
+    if (mu >= n_bf) return;
+    const long long ld = (long long)n_act * n_aux;
+#pragma unroll
+    for (int i = 0; i < kRowsPerLane; ++i) {
+        const int P = aux0 + lane + 32 * i;
+        if (!row_ok[i]) continue;
+#pragma unroll
+        for (int a = 0; a < kMaxActive; ++a)
+            if (a < n_act) T[(long long)a * n_aux + P + (long long)mu * ld] = acc[i][a];
+    }
+}
+
+// Pipelined variant for even n_aux (16-byte aligned columns): each warp streams its columns
+// of B through a private kStages-deep ring in shared memory with cp.async (no registers held
+// by loads in flight), C rows come from a zero-padded transposed copy Ct [n_bf x 16] through
+// the read-only cache (warp-uniform addresses).
+constexpr int kStages = 4;
+constexpr int kNuStage = 4;
+constexpr size_t kPipelinedSmem = sizeof(double) * kWarpsPerCta * kStages * kNuStage * kAuxTile;
+
+__global__ void transpose_coefficients_kernel(const double* __restrict__ C, int n_bf, int n_act,
+                                              double* __restrict__ Ct) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_bf * kMaxActive) return;
+    const int nu = e / kMaxActive, a = e % kMaxActive;
+    Ct[e] = a < n_act ? C[nu + (long long)a * n_bf] : 0.0;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src, int src_bytes) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(gmem_src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(32 * kWarpsPerCta) one_index_pipelined_kernel(const double* __restrict__ B, int n_aux,
+                                                                                int n_bf, const double* __restrict__ Ct,
+                                                                                int n_act, double* __restrict__ T) {
+    extern __shared__ __align__(16) double sB[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mu = blockIdx.x * kWarpsPerCta + warp;
+    const int aux0 = blockIdx.y * kAuxTile;
+    if (mu >= n_bf) return;  // warp-private pipeline: no CTA-wide barrier below
+    double* ring = sB + (size_t)warp * kStages * kNuStage * kAuxTile;
+    const int n_steps = (n_bf + kNuStage - 1) / kNuStage;
+    auto issue = [&](int step) {
+        if (step < n_steps) {
+            const int stage = step % kStages;
+#pragma unroll
+            for (int v = 0; v < kNuStage; ++v) {
+                const int nu = step * kNuStage + v;
+                const double* col = nu < n_bf ? B + ao_pair(mu, nu) * n_aux + aux0 : B;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int j = lane + 32 * h;  // 16-byte chunk: rows 2j, 2j + 1 of the tile
+                    const bool ok = nu < n_bf && aux0 + 2 * j < n_aux;
+                    cp_async16(ring + (stage * kNuStage + v) * kAuxTile + 2 * j, ok ? col + 2 * j : B, ok ? 16 : 0);
+                }
+            }
+        }
+        cp_async_commit();  // empty groups keep the group count uniform
+    };
+#pragma unroll
+    for (int st = 0; st < kStages - 1; ++st) issue(st);
+    double acc[kRowsPerLane][kMaxActive];
+#pragma unroll
+    for (int i = 0; i < kRowsPerLane; ++i)
+#pragma unroll
+        for (int a = 0; a < kMaxActive; ++a) acc[i][a] = 0.0;
+    for (int step = 0; step < n_steps; ++step) {
+        issue(step + kStages - 1);
+        cp_async_wait<kStages - 1>();
+        __syncwarp();
+        const int stage = step % kStages;
+#pragma unroll
+        for (int v = 0; v < kNuStage; ++v) {
+            const int nu = step * kNuStage + v;
+            if (nu >= n_bf) break;
+            const double* tile = ring + (stage * kNuStage + v) * kAuxTile + lane;
+            double b[kRowsPerLane];
+#pragma unroll
+            for (int i = 0; i < kRowsPerLane; ++i) b[i] = tile[32 * i];
+            const double2* c2 = reinterpret_cast<const double2*>(Ct + (long long)nu * kMaxActive);
+#pragma unroll
+            for (int h = 0; h < kMaxActive / 2; ++h) {
+                const double2 c = __ldg(c2 + h);
+#pragma unroll
+                for (int i = 0; i < kRowsPerLane; ++i) {
+                    acc[i][2 * h] = fma(b[i], c.x, acc[i][2 * h]);
+                    acc[i][2 * h + 1] = fma(b[i], c.y, acc[i][2 * h + 1]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    cp_async_wait<0>();
+    const long long ld = (long long)n_act * n_aux;
+#pragma unroll
+    for (int i = 0; i < kRowsPerLane; ++i) {
+        const int P = aux0 + lane + 32 * i;
+        if (P >= n_aux) continue;
+#pragma unroll
+        for (int a = 0; a < kMaxActive; ++a)
+            if (a < n_act) T[(long long)a * n_aux + P + (long long)mu * ld] = acc[i][a];
+    }
+}
+
+// L[P, pair(a, b)] = sum_mu T[a, P, mu] C(mu, b) for b <= a: one thread per (P, a).
+__global__ void __launch_bounds__(128) second_index_kernel(const double* __restrict__ T, int n_aux, int n_bf,
+                                                           const double* __restrict__ C, int n_act,
+                                                           double* __restrict__ L) {
+    __shared__ __align__(16) double sC[kNuChunk][kMaxActive];
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int P = (int)(idx % n_aux), a = (int)(idx / n_aux);
+    const bool ok = a < n_act;
+    double acc[kMaxActive];
+#pragma unroll
+    for (int b = 0; b < kMaxActive; ++b) acc[b] = 0.0;
+    const long long ld = (long long)n_act * n_aux;
+    for (int mu0 = 0; mu0 < n_bf; mu0 += kNuChunk) {
+        const int cnt = min(kNuChunk, n_bf - mu0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < cnt * kMaxActive; e += blockDim.x) {
+            const int b = e / cnt, m = e % cnt;
+            sC[m][b] = b < n_act ? __ldg(C + mu0 + m + (long long)b * n_bf) : 0.0;
+        }
+        __syncthreads();
+        if (ok) {
+            const double* t = T + (long long)a * n_aux + P + (long long)mu0 * ld;
+            for (int m = 0; m < cnt; ++m) {
+                const double tv = __ldg(t + (long long)m * ld);
+                const double2* c2 = reinterpret_cast<const double2*>(&sC[m][0]);
+#pragma unroll
+                for (int h = 0; h < kMaxActive / 2; ++h) {
+                    const double2 c = c2[h];
+                    acc[2 * h] = fma(tv, c.x, acc[2 * h]);
+                    acc[2 * h + 1] = fma(tv, c.y, acc[2 * h + 1]);
+                }
+            }
+        }
+    }
+    if (!ok) return;
+#pragma unroll
+    for (int b = 0; b < kMaxActive; ++b)
+        if (b <= a) L[P + ao_pair(a, b) * n_aux] = acc[b];
+}
+
+// K[pair(p, q)] = sum_P L[P, p] L[P, q] (q <= p): one warp per packed element.
+__global__ void __launch_bounds__(256) pack_kernel(const double* __restrict__ L, int n_aux, int npair,
+                                                   double* __restrict__ K) {
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long total = (long long)npair * (npair + 1) / 2;
+    if (w >= total) return;
+    int p = (int)((sqrt(8.0 * (double)w + 1.0) - 1.0) / 2.0);
+    while ((long long)p * (p + 1) / 2 > w) --p;
+    while ((long long)(p + 1) * (p + 2) / 2 <= w) ++p;
+    const int q = (int)(w - (long long)p * (p + 1) / 2);
+    const double* lp = L + (long long)p * n_aux;
+    const double* lq = L + (long long)q * n_aux;
+    double acc = 0.0;
+    for (int P = lane; P < n_aux; P += 32) acc = fma(__ldg(lp + P), __ldg(lq + P), acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) K[w] = acc;
+}
+
+// Adjoint.  With G = dE/dL and Gs[P, c, b] = G[P, pair(c, b)] (1 + delta_cb):
+//   dE/dC(kappa, c) = sum_{P, b} Gs[P, c, b] T[b, P, kappa].
+// adjoint_kernel: one CTA per (AO tile of 32, slice of the (b, P) range); partial sums go to
+// a [slices x n_bf x n_act] buffer reduced in a fixed order by adjoint_reduce_kernel.
+constexpr int kAdjSlices = 16;
+
+__global__ void __launch_bounds__(256) adjoint_kernel(const double* __restrict__ T, const double* __restrict__ G,
+                                                      int n_aux, int n_bf, int n_act, double* __restrict__ partial) {
+    __shared__ double sT[32][33];   // [kappa local][k local]
+    __shared__ double sG[32][kMaxActive + 1];  // [k local][c]
+    const int k0_tile = blockIdx.x * 32;
+    const int slice = blockIdx.y;
+    const long long Ktot = (long long)n_act * n_aux;
+    const long long per = (Ktot + kAdjSlices - 1) / kAdjSlices;
+    const long long kb = slice * per, ke = min(Ktot, kb + per);
+    const int tid = threadIdx.x;
+    const int kl = tid & 31, cg = tid >> 5;  // thread: kappa local kl, c in {cg, cg + 8}
+    double acc0 = 0.0, acc1 = 0.0;
+    for (long long k0 = kb; k0 < ke; k0 += 32) {
+        __syncthreads();
+        for (int e = tid; e < 32 * 32; e += blockDim.x) {
+            const int kk = e % 32, r = e / 32;
+            const long long k = k0 + kk;
+            const int kappa = k0_tile + r;
+            sT[r][kk] = (k < ke && kappa < n_bf) ? __ldg(T + k + (long long)kappa * Ktot) : 0.0;
+        }
+        for (int e = tid; e < 32 * kMaxActive; e += blockDim.x) {
+            const int kk = e % 32, c = e / 32;
+            const long long k = k0 + kk;
+            double g = 0.0;
+            if (k < ke && c < n_act) {
+                const int b = (int)(k / n_aux), P = (int)(k % n_aux);
+                g = __ldg(G + P + ao_pair(c, b) * n_aux) * (c == b ? 2.0 : 1.0);
+            }
+            sG[kk][c] = g;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 32; ++kk) {
+            const double t = sT[kl][kk];
+            acc0 = fma(t, sG[kk][cg], acc0);
+            acc1 = fma(t, sG[kk][cg + 8], acc1);
+        }
+    }
+    const int kappa = k0_tile + kl;
+    if (kappa < n_bf) {
+        double* out = partial + (long long)slice * n_bf * kMaxActive;
+        out[(long long)kappa * kMaxActive + cg] = acc0;
+        out[(long long)kappa * kMaxActive + cg + 8] = acc1;
+    }
+}
+
+__global__ void adjoint_reduce_kernel(const double* __restrict__ partial, int n_bf, int n_act, double* __restrict__ dC) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_bf * n_act) return;
+    const int kappa = e % n_bf, c = e / n_bf;
+    double s = 0.0;
+    for (int sl = 0; sl < kAdjSlices; ++sl) s += partial[(long long)sl * n_bf * kMaxActive + (long long)kappa * kMaxActive + c];
+    dC[kappa + (long long)c * n_bf] = s;
+}
+
+size_t align_up(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+}  // namespace vbcore
+
+using namespace vbcore;
+
+extern "C" {
+
+vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_aux, int n_bf, const double* C,
+                                 int n_act, int mem_space, double* one_index, double* L, double* K_packed) {
+    if (!ctx) return VB_ERR_INVALID;
+    if (n_aux < 1 || n_bf < 1 || n_act < 1 || !B_packed || !C || !L)
+        return set_error(ctx, VB_ERR_INVALID, "vb_active_transform_ri: dimensions must be positive, B, C and L non-null");
+    if (n_act > kMaxActive)
+        return set_error(ctx, VB_ERR_UNSUPPORTED, "vb_active_transform_ri: at most 16 active orbitals");
+    if (mem_space != VB_MEM_HOST && mem_space != VB_MEM_DEVICE)
+        return set_error(ctx, VB_ERR_INVALID, "bad memory space");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const bool host = mem_space == VB_MEM_HOST;
+    const long long NP = (long long)n_bf * (n_bf + 1) / 2;
+    const int npair = n_act * (n_act + 1) / 2;
+    const size_t bB = sizeof(double) * (size_t)n_aux * NP, bC = sizeof(double) * (size_t)n_bf * n_act;
+    const size_t bT = sizeof(double) * (size_t)n_act * n_aux * n_bf, bL = sizeof(double) * (size_t)n_aux * npair;
+    const size_t bK = sizeof(double) * (size_t)npair * (npair + 1) / 2;
+    size_t off = 0;
+    auto take = [&](size_t bytes, bool need) {
+        const size_t at = off;
+        if (need) off = align_up(off + bytes);
+        return at;
+    };
+    const size_t oB = take(bB, host), oC = take(bC, host), oT = take(bT, host || !one_index);
+    const size_t oL = take(bL, host), oK = take(bK, host && K_packed);
+    const bool pipelined = n_aux % 2 == 0 && (host || reinterpret_cast<uintptr_t>(B_packed) % 16 == 0);
+    const size_t oCt = take(sizeof(double) * (size_t)n_bf * kMaxActive, pipelined);
+    DeviceBuffer ws;
+    vb_status st = ws.allocate(ctx, off);
+    if (st != VB_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ws.ptr);
+    const double* dB = host ? reinterpret_cast<double*>(base + oB) : B_packed;
+    const double* dC = host ? reinterpret_cast<double*>(base + oC) : C;
+    double* dT = (host || !one_index) ? reinterpret_cast<double*>(base + oT) : one_index;
+    double* dL = host ? reinterpret_cast<double*>(base + oL) : L;
+    double* dK = host ? reinterpret_cast<double*>(base + oK) : K_packed;
+    cudaError_t err = cudaSuccess;
+    if (host) {
+        err = cudaMemcpyAsync(const_cast<double*>(dB), B_packed, bB, cudaMemcpyHostToDevice, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(const_cast<double*>(dC), C, bC, cudaMemcpyHostToDevice, s);
+    }
+    if (err == cudaSuccess) {
+        const dim3 grid((n_bf + kWarpsPerCta - 1) / kWarpsPerCta, (n_aux + kAuxTile - 1) / kAuxTile);
+        if (pipelined) {
+            double* Ct = reinterpret_cast<double*>(base + oCt);
+            transpose_coefficients_kernel<<<(n_bf * kMaxActive + 255) / 256, 256, 0, s>>>(dC, n_bf, n_act, Ct);
+            err = cudaGetLastError();
+            if (err == cudaSuccess)
+                err = cudaFuncSetAttribute(one_index_pipelined_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kPipelinedSmem);
+            if (err == cudaSuccess) {
+                one_index_pipelined_kernel<<<grid, 32 * kWarpsPerCta, kPipelinedSmem, s>>>(dB, n_aux, n_bf, Ct, n_act,
+                                                                                          dT);
+                err = cudaGetLastError();
+            }
+        } else {
+            one_index_kernel<<<grid, 32 * kWarpsPerCta, 0, s>>>(dB, n_aux, n_bf, dC, n_act, dT);
+            err = cudaGetLastError();
+        }
+    }
+    if (err == cudaSuccess) {
+        const long long threads = (long long)n_aux * n_act;
+        second_index_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(dT, n_aux, n_bf, dC, n_act, dL);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess && K_packed) {
+        const long long warps = (long long)npair * (npair + 1) / 2;
+        pack_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(dL, n_aux, npair, dK);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess && host) {
+        err = cudaMemcpyAsync(L, dL, bL, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess && K_packed) err = cudaMemcpyAsync(K_packed, dK, bK, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess && one_index) err = cudaMemcpyAsync(one_index, dT, bT, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    }
+    if (err != cudaSuccess) return cuda_error(ctx, err, "vb_active_transform_ri");
+    return VB_OK;  // device mode: stream-ordered (the workspace is freed in stream order)
+}
+
+vb_status vb_active_transform_ri_adjoint(vb_context* ctx, const double* one_index, const double* dL, int n_aux,
+                                         int n_bf, int n_act, int mem_space, double* dC) {
+    if (!ctx) return VB_ERR_INVALID;
+    if (n_aux < 1 || n_bf < 1 || n_act < 1 || !one_index || !dL || !dC)
+        return set_error(ctx, VB_ERR_INVALID, "vb_active_transform_ri_adjoint: bad arguments");
+    if (n_act > kMaxActive)
+        return set_error(ctx, VB_ERR_UNSUPPORTED, "vb_active_transform_ri_adjoint: at most 16 active orbitals");
+    if (mem_space != VB_MEM_HOST && mem_space != VB_MEM_DEVICE)
+        return set_error(ctx, VB_ERR_INVALID, "bad memory space");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const bool host = mem_space == VB_MEM_HOST;
+    const int npair = n_act * (n_act + 1) / 2;
+    const size_t bT = sizeof(double) * (size_t)n_act * n_aux * n_bf, bG = sizeof(double) * (size_t)n_aux * npair;
+    const size_t bD = sizeof(double) * (size_t)n_bf * n_act;
+    const size_t bP = sizeof(double) * (size_t)kAdjSlices * n_bf * kMaxActive;
+    size_t off = 0;
+    auto take = [&](size_t bytes, bool need) {
+        const size_t at = off;
+        if (need) off = align_up(off + bytes);
+        return at;
+    };
+    const size_t oT = take(bT, host), oG = take(bG, host), oD = take(bD, host), oP = take(bP, true);
+    DeviceBuffer ws;
+    vb_status st = ws.allocate(ctx, off);
+    if (st != VB_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ws.ptr);
+    const double* dT = host ? reinterpret_cast<double*>(base + oT) : one_index;
+    const double* dG = host ? reinterpret_cast<double*>(base + oG) : dL;
+    double* dOut = host ? reinterpret_cast<double*>(base + oD) : dC;
+    double* partial = reinterpret_cast<double*>(base + oP);
+    cudaError_t err = cudaSuccess;
+    if (host) {
+        err = cudaMemcpyAsync(const_cast<double*>(dT), one_index, bT, cudaMemcpyHostToDevice, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(const_cast<double*>(dG), dL, bG, cudaMemcpyHostToDevice, s);
+    }
+    if (err == cudaSuccess) {
+        adjoint_kernel<<<dim3((n_bf + 31) / 32, kAdjSlices), 256, 0, s>>>(dT, dG, n_aux, n_bf, n_act, partial);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) {
+        adjoint_reduce_kernel<<<(n_bf * n_act + 255) / 256, 256, 0, s>>>(partial, n_bf, n_act, dOut);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess && host) err = cudaMemcpyAsync(dC, dOut, bD, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess && host) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "vb_active_transform_ri_adjoint");
+    return VB_OK;
+}
+
+}  // extern "C"

@@ -67,6 +67,7 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_destroy", "vb_hs_plan_execute", "vb_hs_plan_stats", "vb_resolve_overlaps", "vb_same_spin_pairs",
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
     "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
+    "vb_active_transform_ri", "vb_active_transform_ri_adjoint",
 )
 
 PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
@@ -106,6 +107,8 @@ def load_library(path: str = LIB_PATH):
     lib.vb_metric_cholesky.argtypes = [P, P, c.c_int, c.c_int, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh.argtypes = [P, P, P, c.c_int, c.c_int, P, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh_batched.argtypes = [P, c.c_int, P, P, P, P, c.c_int, P, P, P, P]
+    lib.vb_active_transform_ri.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, P, P, P]
+    lib.vb_active_transform_ri_adjoint.argtypes = [P, P, P, c.c_int, c.c_int, c.c_int, c.c_int, P]
     lib.vb_same_spin_pairs.argtypes = [P, c.c_int, c.c_int, c.c_int64, P, P, P, P, P, c.c_int, P, P]
     for name in EXPORTED_SYMBOLS:
         fn = getattr(lib, name)
@@ -344,6 +347,43 @@ def generalized_eigh_batched(ctx: "Context", problems, device=None):
     for b, n in enumerate(dims):
         out.append((w[voff[b]:voff[b] + n].copy(), C[offsets[b]:offsets[b] + n * n].reshape(n, n).T.copy()))
     return out
+
+
+def active_transform_ri(ctx: "Context", B_packed, C, one_index: bool = False):
+    """RI AO -> active transform (transform_ri_active_integrals of the reference), host arrays:
+    B_packed [n_aux, n_bf(n_bf+1)/2], C [n_bf, n_act] -> (L [n_aux, P], K packed, T or None)
+    with T [(n_act n_aux), n_bf] the one-index factors (row a*n_aux + P)."""
+    B = np.asarray(B_packed, dtype=np.float64)
+    C = np.asarray(C, dtype=np.float64)
+    n_aux = B.shape[0]
+    n_bf, n_act = C.shape
+    P = n_act * (n_act + 1) // 2
+    Bf = _c(B.T, np.float64)  # column-major
+    Cf = _c(C.T, np.float64)
+    L = np.empty(n_aux * P, dtype=np.float64)
+    K = np.empty(P * (P + 1) // 2, dtype=np.float64)
+    T = np.empty(n_act * n_aux * n_bf, dtype=np.float64) if one_index else None
+    st = load_library().vb_active_transform_ri(ctx.handle, _ptr(Bf), n_aux, n_bf, _ptr(Cf), n_act, VB_MEM_HOST,
+                                               _ptr(T) if one_index else None, _ptr(L), _ptr(K))
+    _check(st, ctx.handle)
+    Lm = L.reshape(P, n_aux).T.copy()
+    Tm = T.reshape(n_bf, n_act * n_aux).T.copy() if one_index else None
+    return Lm, K, Tm
+
+
+def active_transform_ri_adjoint(ctx: "Context", T, dL, n_bf: int):
+    """dE/dC [n_bf, n_act] from dE/dL [n_aux, P] and the one-index factors T of the forward call."""
+    T = np.asarray(T, dtype=np.float64)
+    dL = np.asarray(dL, dtype=np.float64)
+    n_aux, P = dL.shape
+    n_act = int(round((np.sqrt(8 * P + 1) - 1) / 2))
+    Tf = _c(T.T, np.float64)
+    Gf = _c(dL.T, np.float64)
+    dC = np.empty(n_bf * n_act, dtype=np.float64)
+    st = load_library().vb_active_transform_ri_adjoint(ctx.handle, _ptr(Tf), _ptr(Gf), n_aux, n_bf, n_act,
+                                                       VB_MEM_HOST, _ptr(dC))
+    _check(st, ctx.handle)
+    return dC.reshape(n_act, n_bf).T.copy()
 
 
 class HsPlan:
