@@ -175,6 +175,22 @@ vb_status vb_hs_plan_determinant_pairs(vb_hs_plan* plan, const double* ovlp_act,
                                        const double* eri_packed, int64_t n_pairs, const int64_t* pairs,
                                        int mem_space, double* h_out, double* s_out);
 
+/* Analytic gradient of a structure root (accumulate_active_space_gradient and its same-spin /
+ * opposite-spin backward parts, src/vbscf/derivatives/gradient/active_space/
+ * evaluator.cpp:1046-1133).  With c = structure_coefficients (the S-normalized eigenvector of
+ * `eigenvalue`), the gradient of E = c^T (H - eigenvalue S) c, which equals the root's
+ * derivative, with respect to the plan inputs at (S, h, eri):
+ *   dS_out, dh_out (n x n, symmetric: dE = sum_ij G_ij dS_ij for symmetric perturbations),
+ *   deri_out (packed, derivative per stored element; NULL to skip; needs a full-rank pair
+ *     kernel, else VB_ERR_UNSUPPORTED),
+ *   dri_out (np x n_aux, column-major, np = n(n+1)/2) = dE/dF when the integrals are
+ *     (ij|kl) = sum_c F[pair(i,j)][c] F[pair(k,l)][c] with ri_factors = F (NULL to skip).
+ * Re-evaluates the spin-pair records of (S, h, eri); synchronizes the context stream. */
+vb_status vb_hs_plan_gradient(vb_hs_plan* plan, const double* ovlp_act, const double* h1e_act,
+                              const double* eri_packed, int mem_space, const double* structure_coefficients,
+                              double eigenvalue, double* dS_out, double* dh_out, double* deri_out,
+                              const double* ri_factors, int n_aux, double* dri_out);
+
 /* ---- metric Cholesky and the structure eigenproblem ------------------------------------------- */
 
 /* Upper Cholesky factor S = U^T U of a symmetric positive-definite metric

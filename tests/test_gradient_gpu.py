@@ -1,0 +1,118 @@
+"""Analytic structure-root gradient on the device against central differences of the oracle's
+energy (the reference verifies its gradients the same way: tests/cuda/test_structure_action.cpp
+:267-294).  E(S, h, eri) = lowest root of the oracle structure H/S (dsygvd)."""
+
+import numpy as np
+import pytest
+
+import oracle as O
+import vbcore
+from vbcore import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = vbcore.Context(0)
+    yield c
+    c.close()
+
+
+def _energy(n, ex_o, S, h, eri):
+    Hs, Ss, _ = O.structure_matrices(n, ex_o, S, h, eri)
+    w, _ = O.generalized_eigh(Hs, Ss)
+    return w[0]
+
+
+def _richardson(f, step):
+    d1 = (f(step) - f(-step)) / (2 * step)
+    d2 = (f(step / 2) - f(-step / 2)) / step
+    return (4 * d2 - d1) / 3
+
+
+def _sym(rng, n):
+    a = rng.standard_normal((n, n))
+    return 0.5 * (a + a.T)
+
+
+def _full_rank_eri(n, seed):
+    rng = np.random.default_rng(seed)
+    P = n * (n + 1) // 2
+    M = rng.standard_normal((P, P)) * 0.05
+    K = M @ M.T + 0.01 * np.eye(P)
+    return workloads.pack_pair_kernel(K)
+
+
+def _setup(ctx, kw, n, nel, mult, S, h, eri):
+    rows = vbcore.generate_structures(kw, n, nel, mult)
+    ex = vbcore.expand_structures(rows, nel, mult)
+    plan = vbcore.HsPlan(ctx, ex, n)
+    ex_o = O.expand(O.generate_structures(kw, n, nel, mult), nel, mult)
+    Hs, Ss = plan.execute(S, h, eri)
+    w, C = vbcore.generalized_eigh(ctx, Hs, Ss)
+    return plan, ex_o, w[0], C[:, 0]
+
+
+@pytest.mark.parametrize("kw,n,nel,mult", [("COV", 4, 4, 1), ("COV", 6, 6, 1), ("COV ION(1)", 5, 6, 1),
+                                           ("COV", 5, 5, 2), ("COV", 6, 4, 3), ("COV ION(1)", 6, 6, 1)])
+def test_gradient_matches_differences(ctx, kw, n, nel, mult):
+    S, h, _ = workloads.active_space(n, 3 * n, 50 + n + nel)
+    eri = _full_rank_eri(n, 60 + n)
+    plan, ex_o, lam, c = _setup(ctx, kw, n, nel, mult, S, h, eri)
+    g = plan.gradient(S, h, eri, c, lam)
+    assert np.allclose(g["S"], g["S"].T) and np.allclose(g["h"], g["h"].T)
+    rng = np.random.default_rng(7)
+    dS, dh = _sym(rng, n), _sym(rng, n)
+    de = rng.standard_normal(eri.size)
+    for name, direction, analytic in (
+            ("S", lambda t: _energy(n, ex_o, S + t * dS, h, eri), np.sum(g["S"] * dS)),
+            ("h", lambda t: _energy(n, ex_o, S, h + t * dh, eri), np.sum(g["h"] * dh)),
+            ("eri", lambda t: _energy(n, ex_o, S, h, eri + t * de), np.dot(g["eri"], de))):
+        fd = _richardson(direction, 1e-3)
+        assert abs(fd - analytic) < 1e-7 * max(1.0, abs(fd)), (name, fd, analytic)
+    # single entries, both triangles at once
+    for (i, j) in ((0, 0), (0, n - 1), (1, 2)):
+        E = np.zeros((n, n))
+        E[i, j] = E[j, i] = 1.0
+        fd = _richardson(lambda t: _energy(n, ex_o, S + t * E, h, eri), 1e-3)
+        assert abs(fd - np.sum(g["S"] * E)) < 1e-7 * max(1.0, abs(fd))
+    plan.close()
+
+
+def test_gradient_with_ri_factors(ctx):
+    n, n_aux = 6, 8
+    rng = np.random.default_rng(3)
+    S, h, _ = workloads.active_space(n, 3 * n, 4)
+    P = n * (n + 1) // 2
+    F = 0.2 * rng.standard_normal((P, n_aux))
+    eri = workloads.pack_pair_kernel(F @ F.T)
+    plan, ex_o, lam, c = _setup(ctx, "COV", n, n, 1, S, h, eri)
+    with pytest.raises(vbcore.VbError) as e:
+        plan.gradient(S, h, eri, c, lam)
+    assert e.value.status == 5
+    g = plan.gradient(S, h, eri, c, lam, packed_eri=False, ri_factors=F)
+    dF = rng.standard_normal(F.shape)
+    fd = _richardson(lambda t: _energy(n, ex_o, S, h, workloads.pack_pair_kernel((F + t * dF) @ (F + t * dF).T)),
+                     1e-3)
+    assert abs(fd - np.sum(g["ri"] * dF)) < 1e-7 * max(1.0, abs(fd))
+    plan.close()
+
+
+def test_gradient_exact_path_orthogonal_orbitals(ctx):
+    # S = I: every spin-pair block is a permutation-like 0/1 matrix (nullities 1, 2, ...):
+    # the exact-path backward handles all of them
+    n = 6
+    _, h, _ = workloads.active_space(n, 3 * n, 9)
+    S = np.eye(n)
+    eri = _full_rank_eri(n, 10)
+    plan, ex_o, lam, c = _setup(ctx, "COV", n, n, 1, S, h, eri)
+    g = plan.gradient(S, h, eri, c, lam)
+    # the energy curves sharply away from S = I: small steps, entry by entry
+    for (i, j) in ((0, 0), (1, 1), (0, 1), (0, 2), (2, 5), (4, 5)):
+        E = np.zeros((n, n))
+        E[i, j] = E[j, i] = 1.0
+        fd = _richardson(lambda t: _energy(n, ex_o, S + t * E, h, eri), 1e-4)
+        assert abs(fd - np.sum(g["S"] * E)) < 1e-7 * max(1.0, abs(fd)), (i, j)
+    assert plan.stats()["careful_spin_pairs"] > 0
+    plan.close()

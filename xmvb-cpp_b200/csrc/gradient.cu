@@ -1,0 +1,704 @@
+// Analytic gradient of a structure eigenvalue with respect to the active-space inputs
+// (the device counterpart of accumulate_active_space_gradient and its same-spin /
+// opposite-spin backward contributions, src/vbscf/derivatives/gradient/active_space/
+// evaluator.cpp:1046-1133, src/vbscf/derivatives/hessian/responses/same_spin/backward.cpp,
+// .../opposite_spin/backward.cpp).
+//
+// With c the S-normalized structure eigenvector of eigenvalue lambda, dE = c^T (dH - lambda dS) c
+// (the Rayleigh quotient is stationary in c), i.e. with determinant weights w = T c,
+//   dE = sum_{d,e} w_d w_e (dH_de - lambda dS_de).
+// Reverse mode through the plan's pipeline:
+//   1. det_pair_adjoint_kernel: every determinant pair (d <= e) scatters its weight onto the
+//      two spin-pair records it was built from (H_de = H_a S_b + H_b S_a + sum_m s_m u_a u_b):
+//      adj(det_a) += w (H_b - lambda S_b), adj(H_a) += w S_b, adj(u_a[m]) += w s_m u_b[m], and
+//      the same with a <-> b.
+//   2. spin_backward_kernel<K>: per spin pair, with X = S[R, L], B = X^-1 and d = det X:
+//      det = d, A = d B^T, H_1 = <h[R, L], A>, H_2 = d q(B) (q: the same-spin two-electron form
+//      in B), u[m] = <l_m[pair(R, L)], A>.  The adjoint with respect to X is
+//        d ( s B^T - (B M B)^T ),  s = adj_det + <G_A, B^T> + adj_H q,  M = G_A + adj_H Q^T,
+//      G_A = adj_H h[R, L] + sum_m adj_u[m] l_m[pair(R, L)], Q = dq/dB; the linear inputs get
+//      adj_H A (h), adj_H d B-minors (the antisymmetrized two-electron table) and
+//      adj_u[m] A (factor columns).  Blocks whose conditioning certificate fails are listed.
+//   3. careful_backward_kernel: listed blocks through the exact (reference-semantics) path;
+//      every pair quantity is multilinear in the entries of X, so the X-adjoint is the exact
+//      central difference of the exact evaluation along each entry.
+// The host then maps the two-electron table and factor-column adjoints onto the packed
+// integrals (full-rank pair kernel) or onto caller-supplied RI factors.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "device_algebra.cuh"
+#include "internal.h"
+#include "kernels.h"
+#include "pair_value.cuh"
+#include "plan.h"
+
+namespace vbcore {
+namespace {
+
+constexpr double kThreshold = 1.0e-12;
+constexpr double kCertificate2 = 1.0e12;
+
+__device__ __forceinline__ int occ_byte(const uint64_t* row, int i) {
+    const uint64_t w = row[i >> 3];
+    return (int)((w >> (8 * (i & 7))) & 0xFFu);
+}
+
+// Row-major upper-triangle index t -> (u, v), u <= v, of an N x N table.
+__device__ __forceinline__ void upper_decode(long long t, long long N, long long* u, long long* v) {
+    const double b = 2.0 * (double)N + 1.0;
+    long long uu = (long long)floor((b - sqrt(fmax(b * b - 8.0 * (double)t, 0.0))) * 0.5);
+    if (uu < 0) uu = 0;
+    if (uu > N - 1) uu = N - 1;
+    while (uu > 0 && uu * N - uu * (uu - 1) / 2 > t) --uu;
+    while (uu + 1 < N && (uu + 1) * N - (uu + 1) * uu / 2 <= t) ++uu;
+    *u = uu;
+    *v = uu + (t - (uu * N - uu * (uu - 1) / 2));
+}
+
+__global__ void det_weights_kernel(long long n_det, const int64_t* __restrict__ off, const int* __restrict__ str,
+                                   const double* __restrict__ coef, const double* __restrict__ c, double* __restrict__ w) {
+    for (long long d = blockIdx.x * (long long)blockDim.x + threadIdx.x; d < n_det; d += (long long)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (long long t = off[d]; t < off[d + 1]; ++t) acc = fma(coef[t], c[str[t]], acc);
+        w[d] = acc;
+    }
+}
+
+struct AdjArgs {
+    FullPairArgs f;
+    const double* w;
+    double lambda;
+    double* adj_a;
+    double* adj_b;
+    int adj_stride;  // R + 2: [u adjoint (R)], adj(det), adj(H)
+};
+
+__global__ void __launch_bounds__(256) det_pair_adjoint_kernel(AdjArgs a) {
+    const long long n = a.f.n_det;
+    const long long total = n * (n + 1) / 2;
+    const int R = a.f.R;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        long long d, e;
+        upper_decode(t, n, &d, &e);
+        const double omega = __ldg(a.w + d) * __ldg(a.w + e) * (d == e ? 1.0 : 2.0);
+        if (omega == 0.0) continue;
+        double sa = 1.0, ha = 0.0, sb = 1.0, hb = 0.0;
+        const double* ra = nullptr;
+        const double* rb = nullptr;
+        long long ta = -1, tb = -1;
+        if (a.f.ka > 0) {
+            const int i = __ldg(a.f.det_alpha + d), j = __ldg(a.f.det_alpha + e);
+            ta = record_index(min(i, j), max(i, j), a.f.Na);
+            ra = a.f.rec_a + ta * a.f.stride_a;
+            sa = ra[R];
+            ha = ra[R + 1];
+        }
+        if (a.f.kb > 0) {
+            const int i = __ldg(a.f.det_beta + d), j = __ldg(a.f.det_beta + e);
+            tb = record_index(min(i, j), max(i, j), a.f.Nb);
+            rb = a.f.rec_b + tb * a.f.stride_b;
+            sb = rb[R];
+            hb = rb[R + 1];
+        }
+        if (ra) {
+            double* adj = a.adj_a + ta * a.adj_stride;
+            if (rb)
+                for (int m = 0; m < R; ++m) atomicAdd(adj + m, omega * (m < a.f.r_pos ? rb[m] : -rb[m]));
+            atomicAdd(adj + R, omega * (hb - a.lambda * sb));
+            atomicAdd(adj + R + 1, omega * sb);
+        }
+        if (rb) {
+            double* adj = a.adj_b + tb * a.adj_stride;
+            if (ra)
+                for (int m = 0; m < R; ++m) atomicAdd(adj + m, omega * (m < a.f.r_pos ? ra[m] : -ra[m]));
+            atomicAdd(adj + R, omega * (ha - a.lambda * sa));
+            atomicAdd(adj + R + 1, omega * sa);
+        }
+    }
+}
+
+struct BackArgs {
+    int n, k, N;
+    const uint64_t* occ;
+    const double* S;
+    const double* h;
+    const double* eri;
+    const double* gamma;
+    int gd;
+    const double* lf;
+    int ld;
+    int R;
+    const double* adj;
+    int adj_stride;
+    double* gS;  // n x n (index as read: S[L_c n + R_r])
+    double* gh;  // n x n
+    double* gG;  // gd x gd, [anti(L pair) gd + anti(R pair)]
+    double* gL;  // [pair q * ld + m]
+    unsigned long long* careful_count;
+    unsigned long long* careful_list;
+};
+
+template <int K>
+__global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
+    extern __shared__ double acc_s[];  // gS then gh (n*n each)
+    const int n = a.n;
+    for (int i = threadIdx.x; i < 2 * n * n; i += blockDim.x) acc_s[i] = 0.0;
+    __syncthreads();
+    double* sgS = acc_s;
+    double* sgh = acc_s + n * n;
+    const long long N = a.N;
+    const long long total = N * (N + 1) / 2;
+    const int R = a.R;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const double* adj = a.adj + t * a.adj_stride;
+        const double aS = adj[R], aH = adj[R + 1];
+        bool any = aS != 0.0 || aH != 0.0;
+        for (int m = 0; m < R && !any; ++m) any = adj[m] != 0.0;
+        if (!any) continue;
+        long long u, v;
+        upper_decode(t, N, &u, &v);
+        int L[K], Rr[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+            L[c] = occ_byte(a.occ + 2 * u, c);
+            Rr[c] = occ_byte(a.occ + 2 * v, c);
+        }
+        double x[K][K];
+        double nx2 = 0.0;
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                x[r][c] = __ldg(a.S + L[c] * n + Rr[r]);
+                nx2 = fma(x[r][c], x[r][c], nx2);
+            }
+        // Gauss-Jordan with partial pivoting: x -> (P X)^-1, lab = row permutation
+        int lab[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) lab[r] = r;
+        double det = 1.0;
+#pragma unroll
+        for (int s = 0; s < K; ++s) {
+            int p = s;
+            double best = fabs(x[s][s]);
+#pragma unroll
+            for (int i = s + 1; i < K; ++i) {
+                const double av = fabs(x[i][s]);
+                if (av > best) {
+                    best = av;
+                    p = i;
+                }
+            }
+#pragma unroll
+            for (int i = s + 1; i < K; ++i) {
+                const bool sw = (p == i);
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    const double a0 = x[s][j], a1 = x[i][j];
+                    x[s][j] = sw ? a1 : a0;
+                    x[i][j] = sw ? a0 : a1;
+                }
+                const int l0 = lab[s], l1 = lab[i];
+                lab[s] = sw ? l1 : l0;
+                lab[i] = sw ? l0 : l1;
+            }
+            if (p != s) det = -det;
+            const double piv = x[s][s];
+            det *= piv;
+            const double ip = 1.0 / piv;
+            x[s][s] = 1.0;
+#pragma unroll
+            for (int j = 0; j < K; ++j) x[s][j] *= ip;
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                if (i == s) continue;
+                const double f = x[i][s];
+                x[i][s] = 0.0;
+#pragma unroll
+                for (int j = 0; j < K; ++j) x[i][j] = fma(-f, x[s][j], x[i][j]);
+            }
+        }
+        double ni2 = 0.0;
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+            for (int c = 0; c < K; ++c) ni2 = fma(x[r][c], x[r][c], ni2);
+        if (!(isfinite(det) && det != 0.0 && nx2 * ni2 < kCertificate2)) {
+            const unsigned long long slot = atomicAdd(a.careful_count, 1ull);
+            a.careful_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
+            continue;
+        }
+        // B[c][r] = X^-1[c][r]: X^-1 = C P with C = x, so X^-1[c][lab[j]] = x[c][j]
+        double B[K][K];
+#pragma unroll
+        for (int c = 0; c < K; ++c)
+#pragma unroll
+            for (int r = 0; r < K; ++r) {
+                double val = 0.0;
+#pragma unroll
+                for (int j = 0; j < K; ++j) val = lab[j] == r ? x[c][j] : val;
+                B[c][r] = val;
+            }
+        // G_A[r][c] (in x, reused as storage)
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const int q = dev::pair_index(Rr[r], L[c]);
+                const double* lq = a.lf + (long long)q * a.ld;
+                double g = aH * __ldg(a.h + L[c] * n + Rr[r]);
+                for (int m = 0; m < R; ++m) g = fma(adj[m], __ldg(lq + m), g);
+                x[r][c] = g;
+            }
+        double gsum = 0.0;
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+            for (int c = 0; c < K; ++c) gsum = fma(x[r][c], B[c][r], gsum);
+        // same-spin two-electron form: q(B) and Q = dq/dB (added into M = G_A + aH Q^T)
+        double qv = 0.0;
+        if (K >= 2) {
+#pragma unroll
+            for (int c1 = 0; c1 < K; ++c1)
+#pragma unroll
+                for (int c2 = c1 + 1; c2 < K; ++c2) {
+                    const double* grow = a.gamma + (long long)dev::anti_index(L[c1], L[c2]) * a.gd;
+                    double* gout = a.gG + (long long)dev::anti_index(L[c1], L[c2]) * a.gd;
+#pragma unroll
+                    for (int r1 = 0; r1 < K; ++r1)
+#pragma unroll
+                        for (int r2 = r1 + 1; r2 < K; ++r2) {
+                            const int rp = dev::anti_index(Rr[r1], Rr[r2]);
+                            const double G = __ldg(grow + rp);
+                            const double minor = B[c1][r1] * B[c2][r2] - B[c1][r2] * B[c2][r1];
+                            qv = fma(G, minor, qv);
+                            const double gA = aH * G;
+                            // M[r][c] += aH Q[c][r]
+                            x[r1][c1] = fma(gA, B[c2][r2], x[r1][c1]);
+                            x[r2][c2] = fma(gA, B[c1][r1], x[r2][c2]);
+                            x[r2][c1] = fma(-gA, B[c2][r1], x[r2][c1]);
+                            x[r1][c2] = fma(-gA, B[c1][r2], x[r1][c2]);
+                            if (aH != 0.0) atomicAdd(gout + rp, aH * det * minor);
+                        }
+                }
+        }
+        const double s = aS + gsum + aH * qv;
+        // P = M B  (P[r][i] = sum_c M[r][c] B[c][i]), then (B P)[c][i]
+        double P[K][K];
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                double acc = 0.0;
+#pragma unroll
+                for (int c = 0; c < K; ++c) acc = fma(x[r][c], B[c][i], acc);
+                P[r][i] = acc;
+            }
+#pragma unroll
+        for (int c = 0; c < K; ++c)
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                double bp = 0.0;
+#pragma unroll
+                for (int r = 0; r < K; ++r) bp = fma(B[c][r], P[r][i], bp);
+                // adj_X[i][c] = d (s B[c][i] - (B M B)[c][i]); X[i][c] = S[L_c n + R_i]
+                atomicAdd(sgS + L[c] * n + Rr[i], det * (s * B[c][i] - bp));
+                const double A = det * B[c][i];
+                if (aH != 0.0) atomicAdd(sgh + L[c] * n + Rr[i], aH * A);
+                const int q = dev::pair_index(Rr[i], L[c]);
+                double* gq = a.gL + (long long)q * a.ld;
+                for (int m = 0; m < R; ++m)
+                    if (adj[m] != 0.0) atomicAdd(gq + m, adj[m] * A);
+            }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+        if (sgS[i] != 0.0) atomicAdd(a.gS + i, sgS[i]);
+        if (sgh[i] != 0.0) atomicAdd(a.gh + i, sgh[i]);
+    }
+}
+
+// Exact-semantics pair functional f(X) = aS det + aH H_same(X) + sum_m au[m] u_m(X).
+__device__ double pair_functional(const BackArgs& a, const int* L, const int* Rr, const double* x, const double* au,
+                                  double aS, double aH) {
+    const int k = a.k;
+    dev::Resolution res;
+    dev::resolve_exact(k, x, kThreshold, &res);
+    double cof[dev::KMAX * dev::KMAX];
+    dev::first_cofactor(res, cof);
+    double f = aS * res.det;
+    if (res.nullity < 3 && aH != 0.0) {
+        double h1 = 0.0;
+        f += aH * dev::same_spin_exact(a.n, k, L, Rr, res, cof, a.h, a.eri, &h1);
+    }
+    if (res.nullity <= 1)
+        for (int c = 0; c < k; ++c)
+            for (int r = 0; r < k; ++r) {
+                const double cv = cof[c * k + r];
+                if (cv == 0.0) continue;
+                const double* lq = a.lf + (long long)dev::pair_index(Rr[r], L[c]) * a.ld;
+                double acc = 0.0;
+                for (int m = 0; m < a.R; ++m) acc = fma(au[m], __ldg(lq + m), acc);
+                f = fma(cv, acc, f);
+            }
+    return f;
+}
+
+// Listed (uncertified) pairs: one warp per pair.  Entries of X are split over lanes for the
+// central differences; lane 0 adds the linear-input adjoints from the exact cofactors.
+__global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long long count_all) {
+    const long long count = count_all >= 0 ? count_all : (long long)(*a.careful_count);
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int k = a.k, n = a.n;
+    const long long N = a.N;
+    for (long long idx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < count; idx += nwarps) {
+        long long u, v;
+        if (count_all >= 0) {
+            upper_decode(idx, N, &u, &v);
+        } else {
+            const unsigned long long w = a.careful_list[idx];
+            u = (long long)(w >> 32);
+            v = (long long)(w & 0xffffffffull);
+        }
+        const long long t = record_index(u, v, N);
+        const double* adj = a.adj + t * a.adj_stride;
+        const double aS = adj[a.R], aH = adj[a.R + 1];
+        int L[dev::KMAX], Rr[dev::KMAX];
+        for (int c = 0; c < k; ++c) {
+            L[c] = occ_byte(a.occ + 2 * u, c);
+            Rr[c] = occ_byte(a.occ + 2 * v, c);
+        }
+        double x[dev::KMAX * dev::KMAX];  // x[c k + r] = X[r][c]
+        double xmax = 0.0;
+        for (int c = 0; c < k; ++c)
+            for (int r = 0; r < k; ++r) {
+                x[c * k + r] = __ldg(a.S + L[c] * n + Rr[r]);
+                xmax = fmax(xmax, fabs(x[c * k + r]));
+            }
+        const double eps = 1.0e-2 * (xmax > 0.0 ? xmax : 1.0);
+        for (int e = lane; e < k * k; e += 32) {
+            const int c = e / k, r = e % k;
+            const double x0 = x[c * k + r];
+            x[c * k + r] = x0 + eps;
+            const double fp = pair_functional(a, L, Rr, x, adj, aS, aH);
+            x[c * k + r] = x0 - eps;
+            const double fm = pair_functional(a, L, Rr, x, adj, aS, aH);
+            x[c * k + r] = x0;
+            atomicAdd(a.gS + L[c] * n + Rr[r], (fp - fm) / (2.0 * eps));
+        }
+        if (lane == 0) {
+            dev::Resolution res;
+            dev::resolve_exact(k, x, kThreshold, &res);
+            double cof[dev::KMAX * dev::KMAX];
+            dev::first_cofactor(res, cof);
+            for (int c = 0; c < k; ++c)
+                for (int r = 0; r < k; ++r) {
+                    const double A = cof[c * k + r];
+                    if (A == 0.0) continue;
+                    if (aH != 0.0 && res.nullity < 3) atomicAdd(a.gh + L[c] * n + Rr[r], aH * A);
+                    double* gq = a.gL + (long long)dev::pair_index(Rr[r], L[c]) * a.ld;
+                    for (int m = 0; m < a.R; ++m)
+                        if (adj[m] != 0.0) atomicAdd(gq + m, adj[m] * A);
+                }
+            if (aH != 0.0 && res.nullity < 3 && k >= 2) {
+                const bool regular = res.nullity == 0 && k > 3;
+                for (int c1 = 0; c1 < k; ++c1)
+                    for (int c2 = c1 + 1; c2 < k; ++c2)
+                        for (int r1 = 0; r1 < k; ++r1)
+                            for (int r2 = r1 + 1; r2 < k; ++r2) {
+                                const double m2 =
+                                    regular ? (cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2]) / res.det
+                                            : dev::second_cofactor(res, r1, r2, c1, c2);
+                                if (m2 != 0.0)
+                                    atomicAdd(a.gG + (long long)dev::anti_index(L[c1], L[c2]) * a.gd +
+                                                  dev::anti_index(Rr[r1], Rr[r2]),
+                                              aH * m2);
+                            }
+            }
+        }
+    }
+}
+
+template <int K>
+cudaError_t launch_backward(const BackArgs& b, cudaStream_t s) {
+    const size_t smem = sizeof(double) * 2 * b.n * b.n;
+    spin_backward_kernel<K><<<148 * 4, 128, smem, s>>>(b);
+    return cudaGetLastError();
+}
+
+// ---- host-side small dense algebra ---------------------------------------------------------
+
+// Least squares min ||A X - Y|| for A (m x r, column-major, full column rank) by Householder QR;
+// Y is m x p, X (r x p) returned column-major.
+std::vector<double> least_squares(std::vector<double> A, int m, int r, std::vector<double> Y, int p) {
+    std::vector<double> tau(r, 0.0);
+    for (int j = 0; j < r; ++j) {
+        double norm = 0.0;
+        for (int i = j; i < m; ++i) norm += A[i + (size_t)j * m] * A[i + (size_t)j * m];
+        norm = std::sqrt(norm);
+        if (norm == 0.0) continue;
+        const double alpha = A[j + (size_t)j * m] > 0 ? -norm : norm;
+        std::vector<double> vh(m, 0.0);
+        vh[j] = A[j + (size_t)j * m] - alpha;
+        for (int i = j + 1; i < m; ++i) vh[i] = A[i + (size_t)j * m];
+        double vv = 0.0;
+        for (int i = j; i < m; ++i) vv += vh[i] * vh[i];
+        if (vv == 0.0) continue;
+        auto reflect = [&](double* col) {
+            double dot = 0.0;
+            for (int i = j; i < m; ++i) dot += vh[i] * col[i];
+            const double f = 2.0 * dot / vv;
+            for (int i = j; i < m; ++i) col[i] -= f * vh[i];
+        };
+        for (int c = j; c < r; ++c) reflect(&A[(size_t)c * m]);
+        for (int c = 0; c < p; ++c) reflect(&Y[(size_t)c * m]);
+    }
+    std::vector<double> X((size_t)r * p, 0.0);
+    for (int c = 0; c < p; ++c)
+        for (int i = r - 1; i >= 0; --i) {
+            double acc = Y[i + (size_t)c * m];
+            for (int k2 = i + 1; k2 < r; ++k2) acc -= A[i + (size_t)k2 * m] * X[k2 + (size_t)c * r];
+            const double d = A[i + (size_t)i * m];
+            X[i + (size_t)c * r] = d != 0.0 ? acc / d : 0.0;
+        }
+    return X;
+}
+
+int host_pair(int a, int b) {
+    const int hi = std::max(a, b), lo = std::min(a, b);
+    return hi * (hi + 1) / 2 + lo;
+}
+
+}  // namespace
+}  // namespace vbcore
+
+using namespace vbcore;
+
+extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const double* h, const double* eri,
+                                         int mem_space, const double* structure_coefficients, double eigenvalue,
+                                         double* dS_out, double* dh_out, double* deri_out, const double* ri_factors,
+                                         int n_aux, double* dri_out) {
+    if (!p) return VB_ERR_INVALID;
+    vb_context* ctx = p->ctx;
+    if (!S || !h || !eri || !structure_coefficients || !dS_out || !dh_out)
+        return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_gradient: null pointer");
+    if (mem_space != VB_MEM_HOST && mem_space != VB_MEM_DEVICE)
+        return set_error(ctx, VB_ERR_INVALID, "bad memory space");
+    if ((ri_factors == nullptr) != (dri_out == nullptr) || (ri_factors && n_aux < 1))
+        return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_gradient: ri_factors and dri_out go together");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int launches = 0;
+    const double *dS = nullptr, *dh = nullptr, *deri = nullptr;
+    vb_status st = prepare_spin_records(p, S, h, eri, mem_space, &dS, &dh, &deri, &launches);
+    if (st != VB_OK) return st;
+    const int n = p->n, np = p->np, gd = p->gd, R = p->R;
+    const int adj_stride = R + 2;
+    // scratch: w, coefficients, adjoint records, gradient accumulators
+    const size_t n_gS = (size_t)n * n, n_gG = (size_t)std::max(gd, 1) * std::max(gd, 1), n_gL = (size_t)np * np;
+    const size_t acc_doubles = 2 * n_gS + n_gG + n_gL;
+    if ((st = p->grad_acc.allocate(ctx, sizeof(double) * (acc_doubles + p->n_det + p->n_str))) != VB_OK) return st;
+    double* gS = p->grad_acc.as<double>();
+    double* gh = gS + n_gS;
+    double* gG = gh + n_gS;
+    double* gL = gG + n_gG;
+    double* w = gL + n_gL;
+    double* cdev = w + p->n_det;
+    const long long adj_a_n = std::max(1LL, p->npairs_a) * adj_stride;
+    const long long adj_b_n = p->shared_tables ? 0 : std::max(1LL, p->npairs_b) * adj_stride;
+    if ((st = p->adj_a.allocate(ctx, sizeof(double) * adj_a_n)) != VB_OK) return st;
+    if (!p->shared_tables && p->kb > 0 && (st = p->adj_b.allocate(ctx, sizeof(double) * adj_b_n)) != VB_OK) return st;
+    cudaError_t err = cudaMemsetAsync(gS, 0, sizeof(double) * acc_doubles, s);
+    if (err == cudaSuccess) err = cudaMemsetAsync(p->adj_a.ptr, 0, sizeof(double) * adj_a_n, s);
+    if (err == cudaSuccess && p->adj_b.ptr) err = cudaMemsetAsync(p->adj_b.ptr, 0, sizeof(double) * adj_b_n, s);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(cdev, structure_coefficients, sizeof(double) * p->n_str,
+                              mem_space == VB_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s);
+    if (err == cudaSuccess) {
+        det_weights_kernel<<<(unsigned)std::min<long long>(4096, (p->n_det + 255) / 256), 256, 0, s>>>(
+            p->n_det, p->det_off.as<int64_t>(), p->det_str.as<int>(), p->det_coef.as<double>(), cdev, w);
+        err = cudaGetLastError();
+    }
+    AdjArgs aa{};
+    aa.f = full_args(p);
+    aa.w = w;
+    aa.lambda = eigenvalue;
+    aa.adj_a = p->adj_a.as<double>();
+    aa.adj_b = p->shared_tables ? p->adj_a.as<double>() : p->adj_b.as<double>();
+    aa.adj_stride = adj_stride;
+    if (err == cudaSuccess) {
+        det_pair_adjoint_kernel<<<148 * 8, 256, 0, s>>>(aa);
+        err = cudaGetLastError();
+    }
+    // backward through each distinct spin table
+    for (int beta = 0; beta < 2 && err == cudaSuccess; ++beta) {
+        const int k = beta ? p->kb : p->ka;
+        if (k <= 0 || (beta && p->shared_tables)) continue;
+        BackArgs b{};
+        b.n = n;
+        b.k = k;
+        b.N = beta ? p->Nb : p->Na;
+        b.occ = beta ? p->occ_b.as<uint64_t>() : p->occ_a.as<uint64_t>();
+        b.S = dS;
+        b.h = dh;
+        b.eri = deri;
+        b.gamma = p->gamma.as<double>();
+        b.gd = gd;
+        b.lf = p->lf.as<double>();
+        b.ld = np;
+        b.R = R;
+        b.adj = beta ? p->adj_b.as<double>() : p->adj_a.as<double>();
+        b.adj_stride = adj_stride;
+        b.gS = gS;
+        b.gh = gh;
+        b.gG = gG;
+        b.gL = gL;
+        b.careful_count = p->counters.as<unsigned long long>() + 2 + beta;
+        b.careful_list = beta ? p->list_b.as<unsigned long long>() : p->list_a.as<unsigned long long>();
+        err = cudaMemsetAsync(b.careful_count, 0, sizeof(unsigned long long), s);
+        if (err != cudaSuccess) break;
+        const bool fast = k <= 8 && fast_spin_supported(n, k, R);
+        if (fast) {
+            switch (k) {
+                case 1: err = launch_backward<1>(b, s); break;
+                case 2: err = launch_backward<2>(b, s); break;
+                case 3: err = launch_backward<3>(b, s); break;
+                case 4: err = launch_backward<4>(b, s); break;
+                case 5: err = launch_backward<5>(b, s); break;
+                case 6: err = launch_backward<6>(b, s); break;
+                case 7: err = launch_backward<7>(b, s); break;
+                case 8: err = launch_backward<8>(b, s); break;
+                default: break;
+            }
+            if (err != cudaSuccess) break;
+            careful_backward_kernel<<<148 * 8, 64, 0, s>>>(b, -1);
+        } else {
+            const long long NN = b.N;
+            careful_backward_kernel<<<148 * 8, 64, 0, s>>>(b, NN * (NN + 1) / 2);
+        }
+        err = cudaGetLastError();
+    }
+    std::vector<double> hS(n_gS), hh(n_gS), hG(n_gG), hL(n_gL), hlf((size_t)np * np);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(hS.data(), gS, sizeof(double) * n_gS, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(hh.data(), gh, sizeof(double) * n_gS, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(hG.data(), gG, sizeof(double) * n_gG, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(hL.data(), gL, sizeof(double) * n_gL, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(hlf.data(), p->lf.ptr, sizeof(double) * (size_t)np * np, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient");
+
+    // symmetric gradients of S and h: dE = sum G_ij dS_ij for symmetric dS
+    std::vector<double> outS(n_gS), outh(n_gS);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            outS[i + (size_t)j * n] = 0.5 * (hS[i + (size_t)j * n] + hS[j + (size_t)i * n]);
+            outh[i + (size_t)j * n] = 0.5 * (hh[i + (size_t)j * n] + hh[j + (size_t)i * n]);
+        }
+    // factor-column adjoint G (np x R, G[q][m] = hL[q * np + m]) = Ksym L_f Sigma with
+    // Ksym = dE/dK symmetrized; X = G Sigma, Ksym L_f = X
+    std::vector<double> Xm((size_t)np * R), Lf((size_t)np * R);
+    for (int q = 0; q < np; ++q)
+        for (int m = 0; m < R; ++m) {
+            Xm[q + (size_t)m * np] = hL[(size_t)q * np + m] * (m < p->r_pos ? 1.0 : -1.0);
+            Lf[q + (size_t)m * np] = hlf[(size_t)q * np + m];
+        }
+    if (deri_out) {
+        if (R != np)
+            return set_error(ctx, VB_ERR_UNSUPPORTED,
+                             "vb_hs_plan_gradient: the pair kernel has rank " + std::to_string(R) + " < " +
+                                 std::to_string(np) +
+                                 "; packed-integral gradients need a full-rank kernel (pass RI factors instead)");
+        // Ksym = X L_f^-1  <=>  L_f^T Ksym^T = X^T
+        std::vector<double> LfT((size_t)np * np), XT((size_t)np * np);
+        for (int i = 0; i < np; ++i)
+            for (int j = 0; j < np; ++j) {
+                LfT[i + (size_t)j * np] = Lf[j + (size_t)i * np];
+                XT[i + (size_t)j * np] = Xm[j + (size_t)i * np];
+            }
+        std::vector<double> KsT = least_squares(LfT, np, np, XT, np);  // = Ksym^T
+        const long long ne = (long long)np * (np + 1) / 2;
+        std::vector<double> outE(ne, 0.0);
+        for (int a2 = 0; a2 < np; ++a2)
+            for (int b2 = 0; b2 <= a2; ++b2) {
+                const double ks = 0.5 * (KsT[a2 + (size_t)b2 * np] + KsT[b2 + (size_t)a2 * np]);
+                outE[(size_t)a2 * (a2 + 1) / 2 + b2] += a2 == b2 ? 0.5 * ks : ks;
+            }
+        // same-spin table: Gamma[(i<k)][(j<l)] = (ij|kl) - (il|kj)
+        for (int row = 0; row < gd; ++row) {
+            int kk = 1;
+            while ((kk + 1) * kk / 2 <= row) ++kk;
+            const int i = row - kk * (kk - 1) / 2;
+            for (int col = 0; col < gd; ++col) {
+                const double g = hG[(size_t)row * gd + col];
+                if (g == 0.0) continue;
+                int l = 1;
+                while ((l + 1) * l / 2 <= col) ++l;
+                const int j = col - l * (l - 1) / 2;
+                outE[host_pair(host_pair(i, j), host_pair(kk, l))] += g;
+                outE[host_pair(host_pair(i, l), host_pair(kk, j))] -= g;
+            }
+        }
+        if (mem_space == VB_MEM_HOST)
+            std::copy(outE.begin(), outE.end(), deri_out);
+        else if ((err = cudaMemcpyAsync(deri_out, outE.data(), sizeof(double) * ne, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return cuda_error(ctx, err, "vb_hs_plan_gradient");
+    }
+    if (ri_factors) {
+        // dE/dF for K = F F^T with F (np x n_aux) spanning the factor space: Ksym F = X M, F = L_f M
+        std::vector<double> F((size_t)np * n_aux);
+        if (mem_space == VB_MEM_HOST)
+            std::copy(ri_factors, ri_factors + F.size(), F.begin());
+        else if ((err = cudaMemcpy(F.data(), ri_factors, sizeof(double) * F.size(), cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return cuda_error(ctx, err, "vb_hs_plan_gradient");
+        std::vector<double> M = least_squares(Lf, np, R, F, n_aux);  // R x n_aux
+        std::vector<double> D((size_t)np * n_aux, 0.0);
+        for (int q = 0; q < np; ++q)
+            for (int c = 0; c < n_aux; ++c) {
+                double acc = 0.0;
+                for (int m = 0; m < R; ++m) acc += Xm[q + (size_t)m * np] * M[m + (size_t)c * R];
+                D[q + (size_t)c * np] = acc;
+            }
+        // same-spin table through K: Gamma = K-entries difference; its adjoint maps onto the
+        // packed integrals, which are F F^T entries: d(ij|kl) = dF_p F_q^T + F_p dF_q^T
+        for (int row = 0; row < gd; ++row) {
+            int kk = 1;
+            while ((kk + 1) * kk / 2 <= row) ++kk;
+            const int i = row - kk * (kk - 1) / 2;
+            for (int col = 0; col < gd; ++col) {
+                const double g = hG[(size_t)row * gd + col];
+                if (g == 0.0) continue;
+                int l = 1;
+                while ((l + 1) * l / 2 <= col) ++l;
+                const int j = col - l * (l - 1) / 2;
+                const int p1 = host_pair(i, j), q1 = host_pair(kk, l), p2 = host_pair(i, l), q2 = host_pair(kk, j);
+                for (int c = 0; c < n_aux; ++c) {
+                    D[p1 + (size_t)c * np] += g * F[q1 + (size_t)c * np];
+                    D[q1 + (size_t)c * np] += g * F[p1 + (size_t)c * np];
+                    D[p2 + (size_t)c * np] -= g * F[q2 + (size_t)c * np];
+                    D[q2 + (size_t)c * np] -= g * F[p2 + (size_t)c * np];
+                }
+            }
+        }
+        if (mem_space == VB_MEM_HOST)
+            std::copy(D.begin(), D.end(), dri_out);
+        else if ((err = cudaMemcpyAsync(dri_out, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return cuda_error(ctx, err, "vb_hs_plan_gradient");
+    }
+    if (mem_space == VB_MEM_HOST) {
+        std::copy(outS.begin(), outS.end(), dS_out);
+        std::copy(outh.begin(), outh.end(), dh_out);
+    } else {
+        err = cudaMemcpyAsync(dS_out, outS.data(), sizeof(double) * n_gS, cudaMemcpyHostToDevice, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(dh_out, outh.data(), sizeof(double) * n_gS, cudaMemcpyHostToDevice, s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient");
+    }
+    return VB_OK;
+}

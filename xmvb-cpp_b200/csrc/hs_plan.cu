@@ -17,59 +17,11 @@
 #include "device_algebra.cuh"
 #include "internal.h"
 #include "kernels.h"
+#include "plan.h"
 
 using namespace vbcore;
 
-struct StructureChunk {
-    int begin = 0, count = 0;
-    DeviceBuffer wbegin, wdet, wstruct, wcoef;
-};
-
-struct vb_hs_plan {
-    vb_context* ctx = nullptr;
-    int n = 0, ka = 0, kb = 0, np = 0, gd = 0;
-    int n_str = 0;
-    long long n_det = 0;
-    int Na = 0, Nb = 0;
-    bool shared_tables = false;
-    DeviceBuffer occ_a, occ_b, det_alpha, det_beta;
-    DeviceBuffer rec_a, rec_b, tables_a, tables_b;
-    int stride_a = 0, stride_b = 0;
-    long long npairs_a = 0, npairs_b = 0;
-    DeviceBuffer counters, list_a, list_b, items_a, items_b;
-    int n_items_a = 0, n_items_b = 0;
-    int rec_stride_alloc = 0;  // record stride the spin-pair records are allocated for
-    DeviceBuffer S_in, h_in, eri_in, gamma, kfull;
-    // pair-kernel factorization: lf[q * np + m], scratch, signs, meta = {r_pos, r_neg} (+ host copy)
-    DeviceBuffer lf, fwork, fcols, fsigns, fmeta;
-    int* meta_host = nullptr;
-    int R = 0, r_pos = 0;
-    DeviceBuffer band_h, band_s;
-    long long band_width = 0;
-    DeviceBuffer Zh, Zs, Wh, Ws, Hout, Sout;
-    DeviceBuffer str_off, str_det, str_coef;
-    std::vector<StructureChunk> chunks;
-    // spin-flip map of the determinant list (folds the determinant-pair work in half)
-    DeviceBuffer flip;
-    bool has_flip = false;
-    long long det_pair_evaluations = 0;  // unordered determinant pairs evaluated (orbit representatives)
-    vb_hs_stats stats{};
-    bool evaluated = false;
-    // phase timing: per phase a pool of (start, stop) event pairs, `used` pairs this execute
-    bool timing = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[VB_PHASE_COUNT];
-    int used[VB_PHASE_COUNT] = {0, 0, 0, 0, 0};
-    ~vb_hs_plan() {
-        if (meta_host) cudaFreeHost(meta_host);
-        for (auto& v : events)
-            for (auto& e : v) {
-                cudaEventDestroy(e.first);
-                cudaEventDestroy(e.second);
-            }
-    }
-};
-
-namespace {
+namespace vbcore {
 
 vb_status upload(vb_context* ctx, DeviceBuffer& buf, const void* src, size_t bytes) {
     vb_status st = buf.allocate(ctx, bytes);
@@ -79,6 +31,10 @@ vb_status upload(vb_context* ctx, DeviceBuffer& buf, const void* src, size_t byt
     if (err != cudaSuccess) return cuda_error(ctx, err, "cudaMemcpyAsync (plan upload)");
     return VB_OK;
 }
+
+}  // namespace vbcore
+
+namespace {
 
 std::vector<uint64_t> occupation_rows(const uint64_t* masks, int count, int k, int n, std::string* error) {
     std::vector<uint64_t> rows(2 * (size_t)count, ~uint64_t{0});
@@ -128,12 +84,20 @@ struct PhaseMark {
     ~PhaseMark() { close(); }
 };
 
+}  // namespace
+
+namespace vbcore {
+
 int record_stride(int R) {
     const int s = R + 4;
     return (s + 1) / 2 * 2;
 }
 
 // Work items of the fast spin-pair kernel: (left string u, first right string v0), v0 >= u.
+}  // namespace vbcore
+
+namespace {
+
 std::vector<int2> spin_items(int N) {
     std::vector<int2> items;
     for (int u = 0; u < N; ++u)
@@ -209,6 +173,12 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     if ((st = upload(ctx, p->occ_a, occa.data(), occa.size() * 8)) != VB_OK) return fail(st);
     if ((st = upload(ctx, p->occ_b, occb.data(), occb.size() * 8)) != VB_OK) return fail(st);
     if ((st = upload(ctx, p->det_alpha, ex->det_alpha, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
+    {
+        const long long n_terms = ex->term_offsets[p->n_det];
+        if ((st = upload(ctx, p->det_off, ex->term_offsets, sizeof(int64_t) * (p->n_det + 1))) != VB_OK) return fail(st);
+        if ((st = upload(ctx, p->det_str, ex->term_structure, sizeof(int32_t) * n_terms)) != VB_OK) return fail(st);
+        if ((st = upload(ctx, p->det_coef, ex->term_coefficient, sizeof(double) * n_terms)) != VB_OK) return fail(st);
+    }
     if ((st = upload(ctx, p->det_beta, ex->det_beta, sizeof(int32_t) * p->n_det)) != VB_OK) return fail(st);
 
     // spin-pair records are allocated by the first execute, once the factor rank is known
@@ -376,7 +346,7 @@ vb_status vb_hs_plan_destroy(vb_hs_plan* plan) {
 
 }  // extern "C"
 
-namespace {
+namespace vbcore {
 
 SpinTableArgs table_args(vb_hs_plan* p, bool beta, const double* S, const double* h, const double* eri) {
     SpinTableArgs a{};
@@ -485,7 +455,7 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
     return VB_OK;
 }
 
-}  // namespace
+}  // namespace vbcore
 
 extern "C" {
 

@@ -67,7 +67,7 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_destroy", "vb_hs_plan_execute", "vb_hs_plan_stats", "vb_resolve_overlaps", "vb_same_spin_pairs",
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
     "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
-    "vb_active_transform_ri", "vb_active_transform_ri_adjoint",
+    "vb_active_transform_ri", "vb_active_transform_ri_adjoint", "vb_hs_plan_gradient",
 )
 
 PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
@@ -107,6 +107,7 @@ def load_library(path: str = LIB_PATH):
     lib.vb_metric_cholesky.argtypes = [P, P, c.c_int, c.c_int, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh.argtypes = [P, P, P, c.c_int, c.c_int, P, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh_batched.argtypes = [P, c.c_int, P, P, P, P, c.c_int, P, P, P, P]
+    lib.vb_hs_plan_gradient.argtypes = [P, P, P, P, c.c_int, P, c.c_double, P, P, P, P, c.c_int, P]
     lib.vb_active_transform_ri.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, P, P, P]
     lib.vb_active_transform_ri_adjoint.argtypes = [P, P, P, c.c_int, c.c_int, c.c_int, c.c_int, P]
     lib.vb_same_spin_pairs.argtypes = [P, c.c_int, c.c_int, c.c_int64, P, P, P, P, P, c.c_int, P, P]
@@ -237,7 +238,17 @@ class Context:
         _check(load_library().vb_context_memory(self._h, ctypes.byref(cur), ctypes.byref(peak)), self._h)
         return cur.value, peak.value
 
+    def _adopt(self, child):
+        """Track an object whose native handle depends on this context (closed first)."""
+        import weakref
+
+        if not hasattr(self, "_children"):
+            self._children = weakref.WeakSet()
+        self._children.add(child)
+
     def close(self):
+        for child in list(getattr(self, "_children", ())):
+            child.close()
         if getattr(self, "_h", None) is not None and self._h.value:
             load_library().vb_context_destroy(self._h)
             self._h = ctypes.c_void_p()
@@ -404,6 +415,7 @@ class HsPlan:
         h = ctypes.c_void_p()
         _check(load_library().vb_hs_plan_create(ctx.handle, ctypes.byref(desc), ctypes.byref(h)), ctx.handle)
         self._h = h
+        ctx._adopt(self)
         self.n_structures = e.n_structures
 
     def execute(self, S, h, eri):
@@ -436,6 +448,34 @@ class HsPlan:
         _check(load_library().vb_hs_plan_execute(self._h, ctypes.c_void_p(S_ptr), ctypes.c_void_p(h_ptr),
                                                  ctypes.c_void_p(eri_ptr), VB_MEM_HOST, ctypes.c_void_p(H_ptr),
                                                  ctypes.c_void_p(S_out_ptr)), self.ctx.handle)
+
+    def gradient(self, S, h, eri, coefficients, eigenvalue, packed_eri: bool = True, ri_factors=None):
+        """Gradient of the structure root (eigenvalue, S-normalized coefficients) with respect to
+        S, h (symmetric n x n) and the packed integrals (if packed_eri) or RI factors
+        F [n(n+1)/2, n_aux] with (ij|kl) = F[pair(i,j)] . F[pair(k,l)] (if given).
+        Returns a dict with keys S, h and eri / ri."""
+        n = self.n_orbitals
+        Sf = _c(np.asarray(S).T, np.float64)
+        hf = _c(np.asarray(h).T, np.float64)
+        ef = _c(eri, np.float64)
+        cf = _c(coefficients, np.float64)
+        gS = np.empty(n * n)
+        gh = np.empty(n * n)
+        ge = np.empty(ef.size) if packed_eri else None
+        F = None if ri_factors is None else _c(np.asarray(ri_factors).T, np.float64)
+        n_aux = 0 if ri_factors is None else np.asarray(ri_factors).shape[1]
+        gF = None if ri_factors is None else np.empty(F.size)
+        st = load_library().vb_hs_plan_gradient(self._h, _ptr(Sf), _ptr(hf), _ptr(ef), VB_MEM_HOST, _ptr(cf),
+                                                float(eigenvalue), _ptr(gS), _ptr(gh),
+                                                _ptr(ge) if packed_eri else None, _ptr(F) if F is not None else None,
+                                                n_aux, _ptr(gF) if gF is not None else None)
+        _check(st, self.ctx.handle)
+        out = {"S": gS.reshape(n, n).T.copy(), "h": gh.reshape(n, n).T.copy()}
+        if packed_eri:
+            out["eri"] = ge
+        if gF is not None:
+            out["ri"] = gF.reshape(n_aux, -1).T.copy()
+        return out
 
     def determinant_pairs(self, S, h, eri, pairs):
         """<d|H|e>, <d|e> for an (m, 2) array of determinant index pairs."""
