@@ -217,6 +217,66 @@ vb_status vb_generalized_eigh_batched(vb_context* ctx, int count, const int* dim
                                       const double* H, const double* S, int mem_space, double* eigenvalues,
                                       const int64_t* value_offsets, double* eigenvectors, int* info);
 
+/* ---- VBSCF energy, gradient and orbital optimization ------------------------------------------ */
+
+/* A molecule with s-type contracted Gaussian shells (hydrogen 6-31G and the like), active
+ * orbitals restricted to listed basis functions (the deck's fragment/HAO pattern), and a
+ * structure class.  Replaces the host side of run_cuvbscf -> xmvb::cuda::solve_scf
+ * (src/cli/cuvbscf.cpp:31, src/cuda/vb/scf.hpp:41-46) for this basis family. */
+typedef struct vb_scf_problem vb_scf_problem;
+typedef struct {
+    int32_t n_atoms;
+    const double* charges;            /* n_atoms */
+    const double* coords;             /* n_atoms x 3, bohr */
+    int32_t n_shells;                 /* one basis function per s shell */
+    const int32_t* shell_atom;
+    const int32_t* shell_nprim;
+    const double* shell_exponents;    /* concatenated primitives */
+    const double* shell_coefficients; /* for normalized primitives (basis-file convention) */
+    int32_t n_active;
+    const int32_t* orbital_offsets;   /* CSR: basis functions orbital a may use */
+    const int32_t* orbital_functions;
+    int32_t n_electrons;
+    int32_t multiplicity;
+    const char* structures;           /* STR= keyword, e.g. "COV" */
+} vb_scf_input;
+
+typedef struct {
+    int32_t max_iterations;
+    double gradient_tolerance;  /* on the infinity norm of the coefficient gradient */
+    int32_t history_size;       /* secant pairs kept */
+    double armijo;              /* sufficient-decrease constant */
+} vb_scf_options;
+
+typedef struct {
+    double energy;
+    double gradient_inf;
+    int32_t iterations;
+    int32_t evaluations;
+    int32_t converged;
+} vb_scf_result;
+
+/* Host only (no device needed): the AO integrals of the input's shells and the nuclear
+ * repulsion; S_ao, h_ao n_bf x n_bf, eri_ao n_bf^4 (any may be NULL). */
+vb_status vb_ao_integrals_s(const vb_scf_input* input, double* S_ao, double* h_ao, double* eri_ao,
+                            double* nuclear_repulsion);
+vb_status vb_scf_problem_create(vb_context* ctx, const vb_scf_input* input, vb_scf_problem** problem);
+vb_status vb_scf_problem_destroy(vb_scf_problem* problem);
+vb_status vb_scf_problem_sizes(const vb_scf_problem* problem, int* n_basis, int* n_active, int* n_structures,
+                               double* nuclear_repulsion);
+/* AO overlap, core Hamiltonian (n_bf x n_bf) and full (mu nu|la si) (n_bf^4), host buffers. */
+vb_status vb_scf_ao_integrals(const vb_scf_problem* problem, double* S_ao, double* h_ao, double* eri_ao);
+/* Total energy at coefficients C (n_bf x n_act, column-major, entries outside each orbital's
+ * basis functions ignored), and optionally dE/dC (same shape, zero outside the pattern) and
+ * the structure H/S (n_str^2 each). */
+vb_status vb_scf_energy_gradient(vb_scf_problem* problem, const double* coefficients, double* energy,
+                                 double* gradient, double* hamiltonian_out, double* overlap_out);
+/* Limited-memory quasi-Newton (two-loop recursion, scaled identity initial inverse, Armijo
+ * backtracking) over the allowed coefficients, the P-LBFGS backend's scheme
+ * (run_plbfgs_backend, src/vbscf/optimization/backends/plbfgs.cpp:19-228). */
+vb_status vb_solve_scf(vb_scf_problem* problem, const double* initial_coefficients, const vb_scf_options* options,
+                       vb_scf_result* result, double* coefficients_out);
+
 /* ---- RI AO -> active-space transform ----------------------------------------------------------- */
 
 /* transform_ri_active_integrals (src/integrals/active/ri.cpp:33-96) in FP64.  B_packed:

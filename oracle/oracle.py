@@ -614,3 +614,146 @@ def rumer_pairings(first: int, past_last: int):
             for right in rumer_pairings(mate + 1, past_last):
                 result.append([(first, mate)] + left + right)
     return result
+
+
+# ----------------------------------------------------------------------------------------------
+# VBSCF on s-type Gaussian molecules (configuration "plain VBSCF": H chains in 6-31G)
+
+
+def _boys0(t: float) -> float:
+    if t < 1e-8:
+        return 1.0 - t / 3.0 + t * t / 10.0
+    return 0.5 * math.sqrt(math.pi / t) * math.erf(math.sqrt(t))
+
+
+def s_shell_integrals(charges, coords, shells):
+    """Overlap, core Hamiltonian (kinetic + nuclear attraction), (mu nu|la si) and the nuclear
+    repulsion for contracted s shells [(atom, exponents, coefficients for normalized
+    primitives)], each renormalized to unit self-overlap.  Closed-form s-type Gaussian
+    integrals (the Boys function F0); the reference obtains them from libcint."""
+    n = len(shells)
+    prims = []
+    for atom, exps, coefs in shells:
+        e = np.asarray(exps, float)
+        c = np.asarray(coefs, float) * (2.0 * e / math.pi) ** 0.75
+        norm = sum(c[i] * c[j] * (math.pi / (e[i] + e[j])) ** 1.5 for i in range(len(e)) for j in range(len(e)))
+        prims.append((np.asarray(coords[atom], float), e, c / math.sqrt(norm)))
+    S = np.zeros((n, n))
+    H = np.zeros((n, n))
+    for m in range(n):
+        for v in range(n):
+            A, ea, ca = prims[m]
+            B, eb, cb = prims[v]
+            ab2 = float(np.sum((A - B) ** 2))
+            for a, x in zip(ea, ca):
+                for b, y in zip(eb, cb):
+                    p, mu = a + b, a * b / (a + b)
+                    sij = (math.pi / p) ** 1.5 * math.exp(-mu * ab2)
+                    S[m, v] += x * y * sij
+                    H[m, v] += x * y * mu * (3.0 - 2.0 * mu * ab2) * sij
+                    P = (a * A + b * B) / p
+                    for Z, Cn in zip(charges, coords):
+                        H[m, v] -= x * y * Z * 2.0 * math.pi / p * math.exp(-mu * ab2) * _boys0(
+                            p * float(np.sum((P - np.asarray(Cn)) ** 2)))
+    eri = np.zeros((n, n, n, n))
+    for m in range(n):
+        for v in range(m + 1):
+            for l in range(n):
+                for s in range(l + 1):
+                    if m * (m + 1) // 2 + v < l * (l + 1) // 2 + s:
+                        continue
+                    A, ea, ca = prims[m]
+                    B, eb, cb = prims[v]
+                    C, ec, cc = prims[l]
+                    D, ed, cd = prims[s]
+                    val = 0.0
+                    for a, xa in zip(ea, ca):
+                        for b, xb in zip(eb, cb):
+                            p = a + b
+                            P = (a * A + b * B) / p
+                            kab = xa * xb * math.exp(-a * b / p * float(np.sum((A - B) ** 2)))
+                            for c, xc in zip(ec, cc):
+                                for d, xd in zip(ed, cd):
+                                    q = c + d
+                                    Q = (c * C + d * D) / q
+                                    kcd = xc * xd * math.exp(-c * d / q * float(np.sum((C - D) ** 2)))
+                                    val += kab * kcd * 2.0 * math.pi ** 2.5 / (p * q * math.sqrt(p + q)) * _boys0(
+                                        p * q / (p + q) * float(np.sum((P - Q) ** 2)))
+                    for t in ((m, v, l, s), (v, m, l, s), (m, v, s, l), (v, m, s, l), (l, s, m, v), (s, l, m, v),
+                              (l, s, v, m), (s, l, v, m)):
+                        eri[t] = val
+    enuc = 0.0
+    for i in range(len(charges)):
+        for j in range(i + 1, len(charges)):
+            enuc += charges[i] * charges[j] / float(np.linalg.norm(np.asarray(coords[i]) - np.asarray(coords[j])))
+    return S, H, eri, enuc
+
+
+def active_integrals(S_ao, h_ao, eri_ao, C):
+    """S_act = C^T S C, h_act = C^T h C, packed (pq|rs) (transform_exact_active_integrals,
+    src/integrals/active/exact.cpp:347-557, as a dense four-index transform)."""
+    S = C.T @ S_ao @ C
+    h = C.T @ h_ao @ C
+    full = np.einsum("mnls,mp,nq,lr,st->pqrt", eri_ao, C, C, C, C, optimize=True)
+    n = C.shape[1]
+    P = n * (n + 1) // 2
+    pairs = [(a, b) for a in range(n) for b in range(a + 1)]
+    packed = np.zeros(P * (P + 1) // 2)
+    for x, (a, b) in enumerate(pairs):
+        for y, (c, d) in enumerate(pairs[:x + 1]):
+            packed[x * (x + 1) // 2 + y] = full[a, b, c, d]
+    return S, h, packed
+
+
+class VbscfOracle:
+    """Energy (lowest structure root + nuclear repulsion, src/vbscf/workflow/evaluator.cpp:
+    103-108), its gradient by Richardson-extrapolated central differences over the allowed
+    coefficients, and a quasi-Newton solve, all on the CPU restatement above."""
+
+    def __init__(self, charges, coords, shells, pattern, n_electrons, multiplicity=1, keyword="COV"):
+        self.S_ao, self.h_ao, self.eri_ao, self.enuc = s_shell_integrals(charges, coords, shells)
+        self.pattern = pattern
+        self.n = len(pattern)
+        self.expansion = expand(generate_structures(keyword, self.n, n_electrons, multiplicity), n_electrons,
+                                multiplicity)
+        self.where = [(m, a) for a, funcs in enumerate(pattern) for m in funcs]
+
+    def matrices(self, C):
+        S, h, eri = active_integrals(self.S_ao, self.h_ao, self.eri_ao, C)
+        return structure_matrices(self.n, self.expansion, S, h, eri)[:2]
+
+    def energy(self, C):
+        Hs, Ss = self.matrices(C)
+        return generalized_eigh(Hs, Ss)[0][0] + self.enuc
+
+    def gradient(self, C, step=1e-4):
+        g = np.zeros_like(C)
+        for (m, a) in self.where:
+            def f(t):
+                Ct = C.copy()
+                Ct[m, a] += t
+                return self.energy(Ct)
+            d1 = (f(step) - f(-step)) / (2 * step)
+            d2 = (f(step / 2) - f(-step / 2)) / step
+            g[m, a] = (4 * d2 - d1) / 3
+        return g
+
+    def solve(self, C0, gtol=1e-7, maxiter=500):
+        import scipy.optimize
+
+        x0 = np.array([C0[m, a] for (m, a) in self.where])
+
+        def unpack(x):
+            C = np.zeros_like(C0)
+            for v, (m, a) in zip(x, self.where):
+                C[m, a] = v
+            return C
+
+        def fun(x):
+            C = unpack(x)
+            g = self.gradient(C)
+            return self.energy(C), np.array([g[m, a] for (m, a) in self.where])
+
+        res = scipy.optimize.minimize(fun, x0, jac=True, method="L-BFGS-B",
+                                      options={"maxcor": 100, "gtol": gtol, "ftol": 1e-15, "maxiter": maxiter})
+        return res.fun, unpack(res.x), res

@@ -1,0 +1,548 @@
+// VBSCF energy, orbital gradient and the quasi-Newton orbital optimization (host driver).
+//
+// The counterpart of xmvb::cuda::solve_scf (src/cuda/vb/scf.hpp:41-46) with the P-LBFGS
+// backend (run_plbfgs_backend, src/vbscf/optimization/backends/plbfgs.cpp:19-228) instead of
+// CIAH.  Per energy+gradient evaluation (every optimizer trial point):
+//   host:   S_act = C^T S_ao C, h_act = C^T h_ao C, (pq|rs) = C^4 (mu nu|la si)
+//           (transform_exact_active_integrals, src/integrals/active/exact.cpp:347-557, dense)
+//   device: structure H/S (vb_hs_plan_execute), lowest root (vb_generalized_eigh),
+//           gradient with respect to S_act, h_act, (pq|rs) (vb_hs_plan_gradient)
+//   host:   chain rule to the active coefficients, restricted to each orbital's allowed basis
+//           functions (the HAO fragment pattern of the deck).
+// Energy = lowest root + nuclear repulsion (src/vbscf/workflow/evaluator.cpp:103-108; no
+// inactive orbitals, so the one-electron reference energy is zero).
+//
+// AO integrals are closed-form s-type contracted Gaussians (overlap, kinetic, nuclear
+// attraction and repulsion through the Boys function F0), which covers hydrogen 6-31G; the
+// reference takes them from libcint.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace vbcore {
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+double boys0(double t) {
+    if (t < 1.0e-8) return 1.0 - t / 3.0 + t * t / 10.0;
+    const double s = std::sqrt(t);
+    return 0.5 * std::sqrt(kPi / t) * std::erf(s);
+}
+
+struct Basis {
+    int n_bf = 0;
+    std::vector<int> atom;                      // per basis function
+    std::vector<std::vector<double>> exps, cs;  // normalized contraction coefficients
+};
+
+double dist2(const double* a, const double* b) {
+    const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    return dx * dx + dy * dy + dz * dz;
+}
+
+Basis make_basis(int n_shells, const int32_t* shell_atom, const int32_t* shell_nprim, const double* exps, const double* coefs) {
+    Basis b;
+    b.n_bf = n_shells;
+    int off = 0;
+    for (int s = 0; s < n_shells; ++s) {
+        std::vector<double> e(exps + off, exps + off + shell_nprim[s]);
+        std::vector<double> c(coefs + off, coefs + off + shell_nprim[s]);
+        off += shell_nprim[s];
+        // primitive normalization (2a/pi)^(3/4), then unit self-overlap of the contraction
+        for (size_t i = 0; i < e.size(); ++i) c[i] *= std::pow(2.0 * e[i] / kPi, 0.75);
+        double norm = 0.0;
+        for (size_t i = 0; i < e.size(); ++i)
+            for (size_t j = 0; j < e.size(); ++j) norm += c[i] * c[j] * std::pow(kPi / (e[i] + e[j]), 1.5);
+        for (double& v : c) v /= std::sqrt(norm);
+        b.atom.push_back(shell_atom[s]);
+        b.exps.push_back(e);
+        b.cs.push_back(c);
+    }
+    return b;
+}
+
+struct AoIntegrals {
+    std::vector<double> S, H;  // n x n column-major
+    std::vector<double> eri;   // full n^4, (mu nu|la si) at mu + n (nu + n (la + n si))
+    double enuc = 0.0;
+};
+
+AoIntegrals ao_integrals(const Basis& b, int n_atoms, const double* Z, const double* xyz) {
+    const int n = b.n_bf;
+    AoIntegrals ao;
+    ao.S.assign((size_t)n * n, 0.0);
+    ao.H.assign((size_t)n * n, 0.0);
+    ao.eri.assign((size_t)n * n * n * n, 0.0);
+    for (int i = 0; i < n_atoms; ++i)
+        for (int j = i + 1; j < n_atoms; ++j) ao.enuc += Z[i] * Z[j] / std::sqrt(dist2(xyz + 3 * i, xyz + 3 * j));
+    for (int m = 0; m < n; ++m)
+        for (int v = 0; v <= m; ++v) {
+            const double* A = xyz + 3 * b.atom[m];
+            const double* B = xyz + 3 * b.atom[v];
+            const double ab2 = dist2(A, B);
+            double s = 0.0, t = 0.0, pot = 0.0;
+            for (size_t i = 0; i < b.exps[m].size(); ++i)
+                for (size_t j = 0; j < b.exps[v].size(); ++j) {
+                    const double a = b.exps[m][i], bb = b.exps[v][j], p = a + bb, mu = a * bb / p;
+                    const double cc = b.cs[m][i] * b.cs[v][j];
+                    const double sij = std::pow(kPi / p, 1.5) * std::exp(-mu * ab2);
+                    s += cc * sij;
+                    t += cc * mu * (3.0 - 2.0 * mu * ab2) * sij;
+                    double P[3];
+                    for (int k = 0; k < 3; ++k) P[k] = (a * A[k] + bb * B[k]) / p;
+                    for (int c = 0; c < n_atoms; ++c)
+                        pot -= cc * Z[c] * 2.0 * kPi / p * std::exp(-mu * ab2) * boys0(p * dist2(P, xyz + 3 * c));
+                }
+            ao.S[m + (size_t)v * n] = ao.S[v + (size_t)m * n] = s;
+            ao.H[m + (size_t)v * n] = ao.H[v + (size_t)m * n] = t + pot;
+        }
+    auto idx = [n](int a, int bq, int c, int d) { return (size_t)a + (size_t)n * (bq + (size_t)n * (c + (size_t)n * d)); };
+    for (int m = 0; m < n; ++m)
+        for (int v = 0; v <= m; ++v)
+            for (int l = 0; l < n; ++l)
+                for (int sg = 0; sg <= l; ++sg) {
+                    if (m * (m + 1) / 2 + v < l * (l + 1) / 2 + sg) continue;
+                    const double* A = xyz + 3 * b.atom[m];
+                    const double* B = xyz + 3 * b.atom[v];
+                    const double* C = xyz + 3 * b.atom[l];
+                    const double* D = xyz + 3 * b.atom[sg];
+                    double val = 0.0;
+                    for (size_t i = 0; i < b.exps[m].size(); ++i)
+                        for (size_t j = 0; j < b.exps[v].size(); ++j) {
+                            const double a = b.exps[m][i], bb = b.exps[v][j], p = a + bb;
+                            const double cab = b.cs[m][i] * b.cs[v][j] * std::exp(-a * bb / p * dist2(A, B));
+                            double P[3];
+                            for (int k = 0; k < 3; ++k) P[k] = (a * A[k] + bb * B[k]) / p;
+                            for (size_t k2 = 0; k2 < b.exps[l].size(); ++k2)
+                                for (size_t l2 = 0; l2 < b.exps[sg].size(); ++l2) {
+                                    const double c = b.exps[l][k2], d = b.exps[sg][l2], q = c + d;
+                                    const double ccd = b.cs[l][k2] * b.cs[sg][l2] * std::exp(-c * d / q * dist2(C, D));
+                                    double Q[3];
+                                    for (int k = 0; k < 3; ++k) Q[k] = (c * C[k] + d * D[k]) / q;
+                                    const double pre = 2.0 * std::pow(kPi, 2.5) / (p * q * std::sqrt(p + q));
+                                    val += cab * ccd * pre * boys0(p * q / (p + q) * dist2(P, Q));
+                                }
+                        }
+                    const int I[8][4] = {{m, v, l, sg}, {v, m, l, sg}, {m, v, sg, l}, {v, m, sg, l},
+                                         {l, sg, m, v}, {sg, l, m, v}, {l, sg, v, m}, {sg, l, v, m}};
+                    for (auto& t4 : I) ao.eri[idx(t4[0], t4[1], t4[2], t4[3])] = val;
+                }
+    return ao;
+}
+
+int pidx(int a, int b) { return a > b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; }
+
+struct Active {
+    std::vector<double> S, h, eri;  // eri packed
+    std::vector<double> T3;         // (kappa x|y z): kappa + nbf (x + na (y + na z))
+};
+
+Active transform(const AoIntegrals& ao, int nbf, int na, const std::vector<double>& C) {
+    Active r;
+    std::vector<double> SC((size_t)nbf * na, 0.0), HC((size_t)nbf * na, 0.0);
+    for (int a = 0; a < na; ++a)
+        for (int m = 0; m < nbf; ++m) {
+            double s = 0.0, hh = 0.0;
+            for (int v = 0; v < nbf; ++v) {
+                s += ao.S[m + (size_t)v * nbf] * C[v + (size_t)a * nbf];
+                hh += ao.H[m + (size_t)v * nbf] * C[v + (size_t)a * nbf];
+            }
+            SC[m + (size_t)a * nbf] = s;
+            HC[m + (size_t)a * nbf] = hh;
+        }
+    r.S.assign((size_t)na * na, 0.0);
+    r.h.assign((size_t)na * na, 0.0);
+    for (int a = 0; a < na; ++a)
+        for (int b = 0; b < na; ++b) {
+            double s = 0.0, hh = 0.0;
+            for (int m = 0; m < nbf; ++m) {
+                s += C[m + (size_t)a * nbf] * SC[m + (size_t)b * nbf];
+                hh += C[m + (size_t)a * nbf] * HC[m + (size_t)b * nbf];
+            }
+            r.S[a + (size_t)b * na] = s;
+            r.h[a + (size_t)b * na] = hh;
+        }
+    // quarter transforms: (mu nu|la si) -> (mu nu|la d) -> (mu nu|c d) -> (mu b|c d) = T3 -> (a b|c d)
+    const size_t n3 = (size_t)nbf * nbf * nbf;
+    std::vector<double> t1(n3 * na, 0.0);  // mu + n(nu + n(la + n d))
+    for (int d = 0; d < na; ++d)
+        for (int s = 0; s < nbf; ++s) {
+            const double c = C[s + (size_t)d * nbf];
+            if (c == 0.0) continue;
+            for (size_t e = 0; e < n3; ++e) t1[e + n3 * d] += c * ao.eri[e + n3 * s];
+        }
+    const size_t n2 = (size_t)nbf * nbf;
+    std::vector<double> t2(n2 * na * na, 0.0);  // mu + n(nu + n(c + na d))
+    for (int d = 0; d < na; ++d)
+        for (int c = 0; c < na; ++c)
+            for (int l = 0; l < nbf; ++l) {
+                const double cc = C[l + (size_t)c * nbf];
+                if (cc == 0.0) continue;
+                for (size_t e = 0; e < n2; ++e) t2[e + n2 * (c + (size_t)na * d)] += cc * t1[e + n2 * (l + (size_t)nbf * d)];
+            }
+    r.T3.assign((size_t)nbf * na * na * na, 0.0);  // kappa + n(b + na(c + na d))
+    for (int cd = 0; cd < na * na; ++cd)
+        for (int b = 0; b < na; ++b)
+            for (int v = 0; v < nbf; ++v) {
+                const double cv = C[v + (size_t)b * nbf];
+                if (cv == 0.0) continue;
+                for (int m = 0; m < nbf; ++m)
+                    r.T3[m + (size_t)nbf * (b + (size_t)na * cd)] += cv * t2[m + (size_t)nbf * (v + (size_t)nbf * cd)];
+            }
+    const int P = na * (na + 1) / 2;
+    r.eri.assign((size_t)P * (P + 1) / 2, 0.0);
+    for (int a = 0; a < na; ++a)
+        for (int b = 0; b <= a; ++b)
+            for (int c = 0; c < na; ++c)
+                for (int d = 0; d <= c; ++d) {
+                    const int pq = pidx(a, b), rs = pidx(c, d);
+                    if (pq < rs) continue;
+                    double v = 0.0;
+                    for (int m = 0; m < nbf; ++m)
+                        v += C[m + (size_t)a * nbf] * r.T3[m + (size_t)nbf * (b + (size_t)na * (c + (size_t)na * d))];
+                    r.eri[(size_t)pq * (pq + 1) / 2 + rs] = v;
+                }
+    return r;
+}
+
+}  // namespace
+}  // namespace vbcore
+
+using namespace vbcore;
+
+struct vb_scf_problem {
+    vb_context* ctx = nullptr;
+    Basis basis;
+    AoIntegrals ao;
+    int n_act = 0;
+    std::vector<std::vector<int>> pattern;
+    std::vector<int32_t> rows;
+    std::vector<uint64_t> alpha, beta;
+    std::vector<int32_t> det_a, det_b, term_str;
+    std::vector<int64_t> term_off;
+    std::vector<double> term_coef;
+    vb_hs_plan* plan = nullptr;
+    int n_str = 0;
+    ~vb_scf_problem() {
+        if (plan) vb_hs_plan_destroy(plan);
+    }
+};
+
+namespace {
+
+// One energy + gradient evaluation at coefficients C (n_bf x n_act, column-major).
+vb_status evaluate(vb_scf_problem* pr, const std::vector<double>& C, double* energy, std::vector<double>* grad,
+                   std::vector<double>* Hs_out, std::vector<double>* Ss_out) {
+    const int nbf = pr->basis.n_bf, na = pr->n_act;
+    Active act = transform(pr->ao, nbf, na, C);
+    const int ns = pr->n_str;
+    std::vector<double> Hs((size_t)ns * ns), Ss((size_t)ns * ns);
+    vb_status st = vb_hs_plan_execute(pr->plan, act.S.data(), act.h.data(), act.eri.data(), VB_MEM_HOST, Hs.data(), Ss.data());
+    if (st != VB_OK) return st;
+    std::vector<double> w(ns), V((size_t)ns * ns);
+    int info = 0;
+    st = vb_generalized_eigh(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, w.data(), V.data(), &info);
+    if (st != VB_OK) return st;
+    *energy = w[0] + pr->ao.enuc;
+    if (Hs_out) *Hs_out = Hs;
+    if (Ss_out) *Ss_out = Ss;
+    if (!grad) return VB_OK;
+    std::vector<double> gS((size_t)na * na), gh((size_t)na * na), ge(act.eri.size());
+    st = vb_hs_plan_gradient(pr->plan, act.S.data(), act.h.data(), act.eri.data(), VB_MEM_HOST, V.data(), w[0],
+                             gS.data(), gh.data(), ge.data(), nullptr, 0, nullptr);
+    if (st != VB_OK) return st;
+    // chain rule: dE/dC = 2 S_ao C G_S + 2 h_ao C G_h + sum over the packed integrals
+    std::vector<double>& g = *grad;
+    g.assign((size_t)nbf * na, 0.0);
+    for (int a = 0; a < na; ++a)
+        for (int m = 0; m < nbf; ++m) {
+            double acc = 0.0;
+            for (int b = 0; b < na; ++b) {
+                double sc = 0.0, hc = 0.0;
+                for (int v = 0; v < nbf; ++v) {
+                    sc += pr->ao.S[m + (size_t)v * nbf] * C[v + (size_t)b * nbf];
+                    hc += pr->ao.H[m + (size_t)v * nbf] * C[v + (size_t)b * nbf];
+                }
+                acc += 2.0 * (sc * gS[b + (size_t)a * na] + hc * gh[b + (size_t)a * na]);
+            }
+            g[m + (size_t)a * nbf] = acc;
+        }
+    auto T3 = [&](int kappa, int b, int c, int d) {
+        return act.T3[kappa + (size_t)nbf * (b + (size_t)na * (c + (size_t)na * d))];
+    };
+    for (int a = 0; a < na; ++a)
+        for (int b = 0; b <= a; ++b)
+            for (int c = 0; c < na; ++c)
+                for (int d = 0; d <= c; ++d) {
+                    const int pq = pidx(a, b), rs = pidx(c, d);
+                    if (pq < rs) continue;
+                    const double G = ge[(size_t)pq * (pq + 1) / 2 + rs];
+                    if (G == 0.0) continue;
+                    for (int k = 0; k < nbf; ++k) {
+                        g[k + (size_t)a * nbf] += G * T3(k, b, c, d);
+                        g[k + (size_t)b * nbf] += G * T3(k, a, c, d);
+                        g[k + (size_t)c * nbf] += G * T3(k, d, a, b);
+                        g[k + (size_t)d * nbf] += G * T3(k, c, a, b);
+                    }
+                }
+    // parameters outside each orbital's allowed basis functions stay fixed
+    for (int a = 0; a < na; ++a) {
+        std::vector<char> allowed(nbf, 0);
+        for (int m : pr->pattern[a]) allowed[m] = 1;
+        for (int m = 0; m < nbf; ++m)
+            if (!allowed[m]) g[m + (size_t)a * nbf] = 0.0;
+    }
+    return VB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vb_status vb_scf_problem_create(vb_context* ctx, const vb_scf_input* in, vb_scf_problem** out) {
+    if (!ctx || !in || !out) return VB_ERR_INVALID;
+    *out = nullptr;
+    if (in->n_atoms < 1 || !in->charges || !in->coords || in->n_shells < 1 || !in->shell_atom || !in->shell_nprim ||
+        !in->shell_exponents || !in->shell_coefficients || in->n_active < 1 || !in->orbital_offsets ||
+        !in->orbital_functions || !in->structures)
+        return set_error(ctx, VB_ERR_INVALID, "vb_scf_problem_create: incomplete input");
+    for (int s = 0; s < in->n_shells; ++s)
+        if (in->shell_atom[s] < 0 || in->shell_atom[s] >= in->n_atoms || in->shell_nprim[s] < 1)
+            return set_error(ctx, VB_ERR_INVALID, "vb_scf_problem_create: bad shell");
+    auto pr = new vb_scf_problem();
+    pr->ctx = ctx;
+    pr->basis = make_basis(in->n_shells, in->shell_atom, in->shell_nprim, in->shell_exponents, in->shell_coefficients);
+    pr->ao = ao_integrals(pr->basis, in->n_atoms, in->charges, in->coords);
+    pr->n_act = in->n_active;
+    for (int a = 0; a < in->n_active; ++a) {
+        std::vector<int> f;
+        for (int t = in->orbital_offsets[a]; t < in->orbital_offsets[a + 1]; ++t) {
+            if (in->orbital_functions[t] < 0 || in->orbital_functions[t] >= pr->basis.n_bf) {
+                delete pr;
+                return set_error(ctx, VB_ERR_INVALID, "vb_scf_problem_create: orbital basis function out of range");
+            }
+            f.push_back(in->orbital_functions[t]);
+        }
+        pr->pattern.push_back(f);
+    }
+    int64_t ns = 0;
+    vb_status st = vb_generate_structures(in->structures, in->n_active, in->n_electrons, in->multiplicity, 0, &ns,
+                                          nullptr, 0);
+    if (st != VB_OK) {
+        delete pr;
+        return set_error(ctx, st, std::string("vb_scf_problem_create: ") + vb_last_error(nullptr));
+    }
+    pr->rows.resize((size_t)ns * in->n_electrons);
+    vb_generate_structures(in->structures, in->n_active, in->n_electrons, in->multiplicity, 0, &ns, pr->rows.data(),
+                           (int64_t)pr->rows.size());
+    vb_expansion_sizes sz{};
+    st = vb_expand_structures(pr->rows.data(), ns, in->n_electrons, in->multiplicity, 0, &sz, nullptr, nullptr, nullptr,
+                              nullptr, nullptr, nullptr, nullptr);
+    if (st != VB_OK) {
+        delete pr;
+        return set_error(ctx, st, "vb_scf_problem_create: expansion failed");
+    }
+    pr->alpha.resize(sz.n_alpha_strings);
+    pr->beta.resize(sz.n_beta_strings);
+    pr->det_a.resize(sz.n_determinants);
+    pr->det_b.resize(sz.n_determinants);
+    pr->term_off.resize(sz.n_determinants + 1);
+    pr->term_str.resize(sz.n_terms);
+    pr->term_coef.resize(sz.n_terms);
+    vb_expand_structures(pr->rows.data(), ns, in->n_electrons, in->multiplicity, 0, &sz, pr->alpha.data(),
+                         pr->beta.data(), pr->det_a.data(), pr->det_b.data(), pr->term_off.data(), pr->term_str.data(),
+                         pr->term_coef.data());
+    vb_expansion e{in->n_active, sz.n_alpha_electrons, sz.n_beta_electrons, sz.n_alpha_strings, sz.n_beta_strings,
+                   pr->alpha.data(), pr->beta.data(), sz.n_determinants, pr->det_a.data(), pr->det_b.data(),
+                   sz.n_structures, pr->term_off.data(), pr->term_str.data(), pr->term_coef.data()};
+    st = vb_hs_plan_create(ctx, &e, &pr->plan);
+    if (st != VB_OK) {
+        delete pr;
+        return st;
+    }
+    pr->n_str = sz.n_structures;
+    *out = pr;
+    return VB_OK;
+}
+
+vb_status vb_ao_integrals_s(const vb_scf_input* in, double* S_ao, double* h_ao, double* eri_ao,
+                            double* nuclear_repulsion) {
+    if (!in || in->n_atoms < 1 || !in->charges || !in->coords || in->n_shells < 1 || !in->shell_atom ||
+        !in->shell_nprim || !in->shell_exponents || !in->shell_coefficients)
+        return set_error(nullptr, VB_ERR_INVALID, "vb_ao_integrals_s: incomplete input");
+    for (int s = 0; s < in->n_shells; ++s)
+        if (in->shell_atom[s] < 0 || in->shell_atom[s] >= in->n_atoms || in->shell_nprim[s] < 1)
+            return set_error(nullptr, VB_ERR_INVALID, "vb_ao_integrals_s: bad shell");
+    const Basis b = make_basis(in->n_shells, in->shell_atom, in->shell_nprim, in->shell_exponents, in->shell_coefficients);
+    const AoIntegrals ao = ao_integrals(b, in->n_atoms, in->charges, in->coords);
+    if (S_ao) std::copy(ao.S.begin(), ao.S.end(), S_ao);
+    if (h_ao) std::copy(ao.H.begin(), ao.H.end(), h_ao);
+    if (eri_ao) std::copy(ao.eri.begin(), ao.eri.end(), eri_ao);
+    if (nuclear_repulsion) *nuclear_repulsion = ao.enuc;
+    return VB_OK;
+}
+
+vb_status vb_scf_problem_destroy(vb_scf_problem* pr) {
+    delete pr;
+    return VB_OK;
+}
+
+vb_status vb_scf_problem_sizes(const vb_scf_problem* pr, int* n_basis, int* n_active, int* n_structures,
+                               double* nuclear_repulsion) {
+    if (!pr) return VB_ERR_INVALID;
+    if (n_basis) *n_basis = pr->basis.n_bf;
+    if (n_active) *n_active = pr->n_act;
+    if (n_structures) *n_structures = pr->n_str;
+    if (nuclear_repulsion) *nuclear_repulsion = pr->ao.enuc;
+    return VB_OK;
+}
+
+vb_status vb_scf_ao_integrals(const vb_scf_problem* pr, double* S_ao, double* h_ao, double* eri_ao) {
+    if (!pr) return VB_ERR_INVALID;
+    if (S_ao) std::copy(pr->ao.S.begin(), pr->ao.S.end(), S_ao);
+    if (h_ao) std::copy(pr->ao.H.begin(), pr->ao.H.end(), h_ao);
+    if (eri_ao) std::copy(pr->ao.eri.begin(), pr->ao.eri.end(), eri_ao);
+    return VB_OK;
+}
+
+vb_status vb_scf_energy_gradient(vb_scf_problem* pr, const double* coefficients, double* energy, double* gradient,
+                                 double* hamiltonian_out, double* overlap_out) {
+    if (!pr || !coefficients || !energy) return VB_ERR_INVALID;
+    const int nbf = pr->basis.n_bf, na = pr->n_act;
+    std::vector<double> C(coefficients, coefficients + (size_t)nbf * na);
+    std::vector<double> g, Hs, Ss;
+    vb_status st = evaluate(pr, C, energy, gradient ? &g : nullptr, hamiltonian_out ? &Hs : nullptr,
+                            overlap_out ? &Ss : nullptr);
+    if (st != VB_OK) return st;
+    if (gradient) std::copy(g.begin(), g.end(), gradient);
+    if (hamiltonian_out) std::copy(Hs.begin(), Hs.end(), hamiltonian_out);
+    if (overlap_out) std::copy(Ss.begin(), Ss.end(), overlap_out);
+    return VB_OK;
+}
+
+vb_status vb_solve_scf(vb_scf_problem* pr, const double* initial_coefficients, const vb_scf_options* opt,
+                       vb_scf_result* res, double* coefficients_out) {
+    if (!pr || !initial_coefficients || !opt || !res) return VB_ERR_INVALID;
+    const int nbf = pr->basis.n_bf, na = pr->n_act;
+    // parameters: the allowed entries of C
+    std::vector<size_t> where;
+    for (int a = 0; a < na; ++a)
+        for (int m : pr->pattern[a]) where.push_back(m + (size_t)a * nbf);
+    const size_t np_ = where.size();
+    std::vector<double> C((size_t)nbf * na, 0.0);
+    for (size_t i : where) C[i] = initial_coefficients[i];
+    auto pack = [&](const std::vector<double>& full) {
+        std::vector<double> x(np_);
+        for (size_t i = 0; i < np_; ++i) x[i] = full[where[i]];
+        return x;
+    };
+    auto unpack = [&](const std::vector<double>& x) {
+        std::vector<double> full((size_t)nbf * na, 0.0);
+        for (size_t i = 0; i < np_; ++i) full[where[i]] = x[i];
+        return full;
+    };
+    auto dot = [](const std::vector<double>& a, const std::vector<double>& b) {
+        double s = 0.0;
+        for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+        return s;
+    };
+    auto inf_norm = [](const std::vector<double>& a) {
+        double s = 0.0;
+        for (double v : a) s = std::max(s, std::fabs(v));
+        return s;
+    };
+    std::vector<double> x = pack(C), gfull;
+    double f = 0.0;
+    vb_status st = evaluate(pr, unpack(x), &f, &gfull, nullptr, nullptr);
+    if (st != VB_OK) return st;
+    std::vector<double> g = pack(gfull);
+    int evaluations = 1;
+    std::vector<std::vector<double>> S_hist, Y_hist;
+    res->converged = 0;
+    res->iterations = 0;
+    const int history = std::max(1, opt->history_size);
+    const double c1 = opt->armijo > 0.0 ? opt->armijo : 1.0e-4;
+    for (int it = 0; it < opt->max_iterations; ++it) {
+        if (inf_norm(g) <= opt->gradient_tolerance) {
+            res->converged = 1;
+            break;
+        }
+        // two-loop recursion with the scaled identity as initial inverse Hessian
+        std::vector<double> q = g;
+        const int k = (int)S_hist.size();
+        std::vector<double> alpha(k);
+        for (int i = k - 1; i >= 0; --i) {
+            const double rho = 1.0 / dot(Y_hist[i], S_hist[i]);
+            alpha[i] = rho * dot(S_hist[i], q);
+            for (size_t j = 0; j < np_; ++j) q[j] -= alpha[i] * Y_hist[i][j];
+        }
+        double gamma = 1.0;
+        if (k > 0) gamma = dot(S_hist[k - 1], Y_hist[k - 1]) / dot(Y_hist[k - 1], Y_hist[k - 1]);
+        for (double& v : q) v *= gamma;
+        for (int i = 0; i < k; ++i) {
+            const double rho = 1.0 / dot(Y_hist[i], S_hist[i]);
+            const double beta = rho * dot(Y_hist[i], q);
+            for (size_t j = 0; j < np_; ++j) q[j] += S_hist[i][j] * (alpha[i] - beta);
+        }
+        std::vector<double> d(np_);
+        for (size_t j = 0; j < np_; ++j) d[j] = -q[j];
+        double slope = dot(g, d);
+        if (!(slope < 0.0)) {
+            S_hist.clear();
+            Y_hist.clear();
+            for (size_t j = 0; j < np_; ++j) d[j] = -g[j];
+            slope = dot(g, d);
+        }
+        // first step without curvature information: bounded length
+        double step = k == 0 ? std::min(1.0, 0.1 / std::max(inf_norm(d), 1e-300)) : 1.0;
+        std::vector<double> xn(np_), gn;
+        double fn = 0.0;
+        bool accepted = false;
+        for (int bt = 0; bt < 40; ++bt) {
+            for (size_t j = 0; j < np_; ++j) xn[j] = x[j] + step * d[j];
+            st = evaluate(pr, unpack(xn), &fn, &gfull, nullptr, nullptr);
+            ++evaluations;
+            if (st != VB_OK) return st;
+            if (std::isfinite(fn) && fn <= f + c1 * step * slope) {
+                accepted = true;
+                break;
+            }
+            step *= 0.5;
+        }
+        res->iterations = it + 1;
+        if (!accepted) break;
+        gn = pack(gfull);
+        std::vector<double> s(np_), y(np_);
+        for (size_t j = 0; j < np_; ++j) {
+            s[j] = xn[j] - x[j];
+            y[j] = gn[j] - g[j];
+        }
+        if (dot(s, y) > 1.0e-16 * std::sqrt(dot(s, s) * dot(y, y))) {
+            S_hist.push_back(s);
+            Y_hist.push_back(y);
+            if ((int)S_hist.size() > history) {
+                S_hist.erase(S_hist.begin());
+                Y_hist.erase(Y_hist.begin());
+            }
+        }
+        x = xn;
+        g = gn;
+        f = fn;
+    }
+    if (!res->converged && inf_norm(g) <= opt->gradient_tolerance) res->converged = 1;
+    res->energy = f;
+    res->gradient_inf = inf_norm(g);
+    res->evaluations = evaluations;
+    if (coefficients_out) {
+        std::vector<double> full = unpack(x);
+        std::copy(full.begin(), full.end(), coefficients_out);
+    }
+    return VB_OK;
+}
+
+}  // extern "C"

@@ -55,6 +55,25 @@ class _Expansion(ctypes.Structure):
                 ("term_coefficient", ctypes.c_void_p)]
 
 
+class _ScfInput(ctypes.Structure):
+    _fields_ = [("n_atoms", ctypes.c_int32), ("charges", ctypes.c_void_p), ("coords", ctypes.c_void_p),
+                ("n_shells", ctypes.c_int32), ("shell_atom", ctypes.c_void_p), ("shell_nprim", ctypes.c_void_p),
+                ("shell_exponents", ctypes.c_void_p), ("shell_coefficients", ctypes.c_void_p),
+                ("n_active", ctypes.c_int32), ("orbital_offsets", ctypes.c_void_p),
+                ("orbital_functions", ctypes.c_void_p), ("n_electrons", ctypes.c_int32),
+                ("multiplicity", ctypes.c_int32), ("structures", ctypes.c_char_p)]
+
+
+class _ScfOptions(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_int32), ("gradient_tolerance", ctypes.c_double),
+                ("history_size", ctypes.c_int32), ("armijo", ctypes.c_double)]
+
+
+class _ScfResult(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("gradient_inf", ctypes.c_double), ("iterations", ctypes.c_int32),
+                ("evaluations", ctypes.c_int32), ("converged", ctypes.c_int32)]
+
+
 class _HsStats(ctypes.Structure):
     _fields_ = [("spin_pairs", ctypes.c_int64), ("careful_spin_pairs", ctypes.c_int64),
                 ("determinant_pairs", ctypes.c_int64), ("kernel_launches", ctypes.c_int64)]
@@ -68,6 +87,8 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
     "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
     "vb_active_transform_ri", "vb_active_transform_ri_adjoint", "vb_hs_plan_gradient",
+    "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
+    "vb_scf_ao_integrals", "vb_scf_energy_gradient", "vb_solve_scf",
 )
 
 PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
@@ -107,6 +128,14 @@ def load_library(path: str = LIB_PATH):
     lib.vb_metric_cholesky.argtypes = [P, P, c.c_int, c.c_int, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh.argtypes = [P, P, P, c.c_int, c.c_int, P, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh_batched.argtypes = [P, c.c_int, P, P, P, P, c.c_int, P, P, P, P]
+    lib.vb_ao_integrals_s.argtypes = [c.POINTER(_ScfInput), P, P, P, c.POINTER(c.c_double)]
+    lib.vb_scf_problem_create.argtypes = [P, c.POINTER(_ScfInput), c.POINTER(P)]
+    lib.vb_scf_problem_destroy.argtypes = [P]
+    lib.vb_scf_problem_sizes.argtypes = [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int),
+                                         c.POINTER(c.c_double)]
+    lib.vb_scf_ao_integrals.argtypes = [P, P, P, P]
+    lib.vb_scf_energy_gradient.argtypes = [P, P, c.POINTER(c.c_double), P, P, P]
+    lib.vb_solve_scf.argtypes = [P, P, c.POINTER(_ScfOptions), c.POINTER(_ScfResult), P]
     lib.vb_hs_plan_gradient.argtypes = [P, P, P, P, c.c_int, P, c.c_double, P, P, P, P, c.c_int, P]
     lib.vb_active_transform_ri.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, P, P, P]
     lib.vb_active_transform_ri_adjoint.argtypes = [P, P, P, c.c_int, c.c_int, c.c_int, c.c_int, P]
@@ -395,6 +424,96 @@ def active_transform_ri_adjoint(ctx: "Context", T, dL, n_bf: int):
                                                        VB_MEM_HOST, _ptr(dC))
     _check(st, ctx.handle)
     return dC.reshape(n_act, n_bf).T.copy()
+
+
+def _scf_input(mol, pattern, n_electrons, multiplicity, structures, keep):
+    arrays = [_c(mol.charges, np.float64), _c(mol.coords, np.float64), _c(mol.shell_atom, np.int32),
+              _c(mol.shell_nprim, np.int32), _c(mol.shell_exponents, np.float64),
+              _c(mol.shell_coefficients, np.float64)]
+    offsets = np.concatenate([[0], np.cumsum([len(p) for p in pattern])]).astype(np.int32)
+    funcs = np.array([m for p in pattern for m in p], dtype=np.int32)
+    arrays += [offsets, funcs]
+    keep.extend(arrays)
+    kw = structures.encode()
+    keep.append(kw)
+    return _ScfInput(len(mol.charges), _ptr(arrays[0]).value, _ptr(arrays[1]).value, len(mol.shell_atom),
+                     _ptr(arrays[2]).value, _ptr(arrays[3]).value, _ptr(arrays[4]).value, _ptr(arrays[5]).value,
+                     len(pattern), _ptr(offsets).value, _ptr(funcs).value if funcs.size else None, n_electrons,
+                     multiplicity, kw)
+
+
+def ao_integrals_s(mol):
+    """(S_ao, h_ao, eri_ao [n,n,n,n], nuclear repulsion) of an s-shell molecule (host only)."""
+    keep = []
+    inp = _scf_input(mol, [], 0, 1, "COV", keep)
+    n = mol.n_basis
+    S = np.empty(n * n)
+    h = np.empty(n * n)
+    eri = np.empty(n ** 4)
+    enuc = ctypes.c_double(0.0)
+    _check(load_library().vb_ao_integrals_s(ctypes.byref(inp), _ptr(S), _ptr(h), _ptr(eri), ctypes.byref(enuc)))
+    return (S.reshape(n, n).T.copy(), h.reshape(n, n).T.copy(), eri.reshape(n, n, n, n).transpose(3, 2, 1, 0).copy(),
+            enuc.value)
+
+
+class ScfProblem:
+    """A VBSCF problem (molecule, HAO pattern, structure class) with its plan on the device."""
+
+    def __init__(self, ctx: "Context", mol, pattern, n_electrons: int, multiplicity: int = 1,
+                 structures: str = "COV"):
+        self.ctx = ctx
+        self.mol = mol
+        self.pattern = pattern
+        self._keep = []
+        inp = _scf_input(mol, pattern, n_electrons, multiplicity, structures, self._keep)
+        h = ctypes.c_void_p()
+        _check(load_library().vb_scf_problem_create(ctx.handle, ctypes.byref(inp), ctypes.byref(h)), ctx.handle)
+        self._h = h
+        ctx._adopt(self)
+        nb, na, ns, en = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        load_library().vb_scf_problem_sizes(h, ctypes.byref(nb), ctypes.byref(na), ctypes.byref(ns), ctypes.byref(en))
+        self.n_basis, self.n_active, self.n_structures, self.nuclear_repulsion = nb.value, na.value, ns.value, en.value
+
+    def energy_gradient(self, C, with_matrices: bool = False):
+        """Total energy, dE/dC [n_basis, n_active] (zero outside the pattern) and, optionally,
+        the structure H and S at coefficients C."""
+        Cf = _c(np.asarray(C).T, np.float64)
+        e = ctypes.c_double()
+        g = np.empty(self.n_basis * self.n_active)
+        ns = self.n_structures
+        H = np.empty(ns * ns) if with_matrices else None
+        S = np.empty(ns * ns) if with_matrices else None
+        _check(load_library().vb_scf_energy_gradient(self._h, _ptr(Cf), ctypes.byref(e), _ptr(g),
+                                                     _ptr(H) if with_matrices else None,
+                                                     _ptr(S) if with_matrices else None), self.ctx.handle)
+        out = (e.value, g.reshape(self.n_active, self.n_basis).T.copy())
+        if with_matrices:
+            out += (H.reshape(ns, ns).T.copy(), S.reshape(ns, ns).T.copy())
+        return out
+
+    def solve(self, C0, max_iterations: int = 200, gradient_tolerance: float = 1e-6, history_size: int = 100,
+              armijo: float = 1e-4):
+        """Quasi-Newton orbital optimization from C0; returns (result dict, final C)."""
+        Cf = _c(np.asarray(C0).T, np.float64)
+        out = np.empty(self.n_basis * self.n_active)
+        opt = _ScfOptions(max_iterations, gradient_tolerance, history_size, armijo)
+        res = _ScfResult()
+        _check(load_library().vb_solve_scf(self._h, _ptr(Cf), ctypes.byref(opt), ctypes.byref(res), _ptr(out)),
+               self.ctx.handle)
+        return ({"energy": res.energy, "gradient_inf": res.gradient_inf, "iterations": res.iterations,
+                 "evaluations": res.evaluations, "converged": bool(res.converged)},
+                out.reshape(self.n_active, self.n_basis).T.copy())
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().vb_scf_problem_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class HsPlan:
