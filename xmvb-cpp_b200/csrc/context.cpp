@@ -36,7 +36,8 @@ void* device_alloc(vb_context* ctx, size_t bytes, vb_status* status) {
         return nullptr;
     }
     void* p = nullptr;
-    cudaError_t err = cudaMallocAsync(&p, bytes, ctx->stream);
+    cudaError_t err = ctx->pool ? cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream)
+                                : cudaMallocAsync(&p, bytes, ctx->stream);
     if (err != cudaSuccess) {
         *status = cuda_error(ctx, err, "cudaMallocAsync");
         return nullptr;
@@ -85,6 +86,20 @@ vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** ou
         return set_error(nullptr, VB_ERR_CUDA, "cudaStreamCreate failed");
     }
     ctx->stream = ctx->own_stream;
+    // a private pool whose freed blocks stay mapped between calls (a release threshold of 0,
+    // the default pool's, would unmap them at every synchronization and re-map on the next call)
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&ctx->pool, &props) == cudaSuccess) {
+        uint64_t keep = ~uint64_t{0};
+        cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        ctx->pool = nullptr;
+        cudaGetLastError();
+    }
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     ctx->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.9 * (double)free_b);
@@ -98,6 +113,10 @@ vb_status vb_context_destroy(vb_context* ctx) {
     if (ctx->own_stream) {
         cudaStreamSynchronize(ctx->own_stream);
         cudaStreamDestroy(ctx->own_stream);
+    }
+    if (ctx->pool) {
+        cudaDeviceSynchronize();
+        cudaMemPoolDestroy(ctx->pool);
     }
     delete ctx;
     return VB_OK;

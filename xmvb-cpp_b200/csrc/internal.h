@@ -13,6 +13,7 @@ struct vb_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    cudaMemPool_t pool = nullptr;  // the context's own stream-ordered pool (keeps freed memory)
     size_t budget = 0;
     size_t current = 0;
     size_t peak = 0;

@@ -11,13 +11,10 @@
 //   L  [n_aux x n_act (n_act + 1) / 2], L[P + pair(a, b) n_aux] = sum_mu T[a, P, mu] C(mu, b)
 //   K  packed, K[pair(p, q)] = sum_P L[P, p] L[P, q]
 //
-// one_index_kernel carries the flops (2 n_aux n_bf^2 n_act): a warp owns one AO index mu and
-// 128 auxiliary rows (4 per lane) and accumulates T[a, P, mu] for all n_act orbitals in
-// registers (64 FP64 accumulators per lane), streaming the AO-pair columns pair(mu, nu) of B
-// (1 KB coalesced per column) against C rows staged in shared memory.  Each packed column is
-// needed by two AO indices (mu and nu); CTAs are ordered AO index fastest so that both uses of
-// an auxiliary tile's slice of B (82 MB for 128 auxiliary functions at n_bf = 400) fall in
-// the same wave and the second read is an L2 hit: B crosses HBM about once.
+// The one-index step carries the flops (2 n_aux n_bf^2 n_act): lanes own 4 auxiliary rows each
+// (128 per warp) and accumulate T[a, P, mu] for all n_act orbitals in registers (64 FP64
+// accumulators per lane), streaming the AO-pair columns pair(mu, nu) of B (1 KB coalesced per
+// column) against rows of C.  Each packed column is needed by two AO indices (mu and nu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -99,13 +96,19 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) one_index_kernel(const doub
     }
 }
 
-// Pipelined variant for even n_aux (16-byte aligned columns): each warp streams its columns
-// of B through a private kStages-deep ring in shared memory with cp.async (no registers held
-// by loads in flight), C rows come from a zero-padded transposed copy Ct [n_bf x 16] through
-// the read-only cache (warp-uniform addresses).
-constexpr int kStages = 4;
-constexpr int kNuStage = 4;
-constexpr size_t kPipelinedSmem = sizeof(double) * kWarpsPerCta * kStages * kNuStage * kAuxTile;
+// Pipelined variant for even n_aux (16-byte aligned columns) and n_bf <= kPipelinedMaxBf: a
+// warp per AO index mu (six per CTA), each streaming its columns pair(mu, nu) of B through a
+// private 3-stage cp.async ring in shared memory (no registers held by loads in flight), the
+// rows of C staged once per CTA in shared memory (warp-uniform broadcast reads).  Two CTAs
+// (12 warps) per SM: the 64 FP64 accumulators per lane cap residency at 12 warps anyway.
+constexpr int kStages = 3;
+constexpr int kNuStage = 2;
+constexpr int kPipeWarps = 6;
+constexpr int kPipelinedMaxBf = 1024;
+
+size_t pipelined_smem_bytes(int n_bf) {
+    return sizeof(double) * ((size_t)n_bf * kMaxActive + (size_t)kPipeWarps * kStages * kNuStage * kAuxTile);
+}
 
 __global__ void transpose_coefficients_kernel(const double* __restrict__ C, int n_bf, int n_act,
                                               double* __restrict__ Ct) {
@@ -125,16 +128,22 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-__global__ void __launch_bounds__(32 * kWarpsPerCta) one_index_pipelined_kernel(const double* __restrict__ B, int n_aux,
-                                                                                int n_bf, const double* __restrict__ Ct,
-                                                                                int n_act, double* __restrict__ T) {
-    extern __shared__ __align__(16) double sB[];
+__global__ void __launch_bounds__(32 * kPipeWarps, 2) one_index_pipelined_kernel(const double* __restrict__ B,
+                                                                                 int n_aux, int n_bf,
+                                                                                 const double* __restrict__ Ct,
+                                                                                 int n_act, double* __restrict__ T) {
+    extern __shared__ __align__(16) double smem[];
+    double* sCt = smem;                                    // [n_bf][16]
+    double* ring_all = smem + (size_t)n_bf * kMaxActive;   // [warp][stage][nu][128]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int mu = blockIdx.x * kWarpsPerCta + warp;
+    const int mu = blockIdx.x * kPipeWarps + warp;
     const int aux0 = blockIdx.y * kAuxTile;
-    if (mu >= n_bf) return;  // warp-private pipeline: no CTA-wide barrier below
-    double* ring = sB + (size_t)warp * kStages * kNuStage * kAuxTile;
+    for (int e = threadIdx.x; e < n_bf * kMaxActive / 2; e += blockDim.x)
+        reinterpret_cast<double2*>(sCt)[e] = __ldg(reinterpret_cast<const double2*>(Ct) + e);
+    __syncthreads();
+    if (mu >= n_bf) return;  // warp-private pipeline below: no CTA-wide barrier after this point
     const int n_steps = (n_bf + kNuStage - 1) / kNuStage;
+    double* ring = ring_all + (size_t)warp * kStages * kNuStage * kAuxTile;
     auto issue = [&](int step) {
         if (step < n_steps) {
             const int stage = step % kStages;
@@ -172,10 +181,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) one_index_pipelined_kernel(
             double b[kRowsPerLane];
 #pragma unroll
             for (int i = 0; i < kRowsPerLane; ++i) b[i] = tile[32 * i];
-            const double2* c2 = reinterpret_cast<const double2*>(Ct + (long long)nu * kMaxActive);
+            const double2* c2 = reinterpret_cast<const double2*>(sCt + (size_t)nu * kMaxActive);
 #pragma unroll
             for (int h = 0; h < kMaxActive / 2; ++h) {
-                const double2 c = __ldg(c2 + h);
+                const double2 c = c2[h];
 #pragma unroll
                 for (int i = 0; i < kRowsPerLane; ++i) {
                     acc[i][2 * h] = fma(b[i], c.x, acc[i][2 * h]);
@@ -197,44 +206,41 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) one_index_pipelined_kernel(
     }
 }
 
-// L[P, pair(a, b)] = sum_mu T[a, P, mu] C(mu, b) for b <= a: one thread per (P, a).
+// L[P, pair(a, b)] = sum_mu T[a, P, mu] C(mu, b) for b <= a.  CTA = (32 auxiliary rows, one
+// orbital a); its four warps split the mu range (lane = auxiliary row, 16 accumulators for b)
+// and reduce through shared memory.
 __global__ void __launch_bounds__(128) second_index_kernel(const double* __restrict__ T, int n_aux, int n_bf,
                                                            const double* __restrict__ C, int n_act,
                                                            double* __restrict__ L) {
-    __shared__ __align__(16) double sC[kNuChunk][kMaxActive];
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int P = (int)(idx % n_aux), a = (int)(idx / n_aux);
-    const bool ok = a < n_act;
+    __shared__ double red[4][kMaxActive][33];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int P = blockIdx.x * 32 + lane;
+    const int a = blockIdx.y;
+    const long long ld = (long long)n_act * n_aux;
     double acc[kMaxActive];
 #pragma unroll
     for (int b = 0; b < kMaxActive; ++b) acc[b] = 0.0;
-    const long long ld = (long long)n_act * n_aux;
-    for (int mu0 = 0; mu0 < n_bf; mu0 += kNuChunk) {
-        const int cnt = min(kNuChunk, n_bf - mu0);
-        __syncthreads();
-        for (int e = threadIdx.x; e < cnt * kMaxActive; e += blockDim.x) {
-            const int b = e / cnt, m = e % cnt;
-            sC[m][b] = b < n_act ? __ldg(C + mu0 + m + (long long)b * n_bf) : 0.0;
-        }
-        __syncthreads();
-        if (ok) {
-            const double* t = T + (long long)a * n_aux + P + (long long)mu0 * ld;
-            for (int m = 0; m < cnt; ++m) {
-                const double tv = __ldg(t + (long long)m * ld);
-                const double2* c2 = reinterpret_cast<const double2*>(&sC[m][0]);
+    const int chunk = (n_bf + 3) / 4;
+    const int m0 = warp * chunk, m1 = min(n_bf, m0 + chunk);
+    if (P < n_aux) {
+        const double* t = T + (long long)a * n_aux + P;
+#pragma unroll 4
+        for (int m = m0; m < m1; ++m) {
+            const double tv = __ldg(t + (long long)m * ld);
 #pragma unroll
-                for (int h = 0; h < kMaxActive / 2; ++h) {
-                    const double2 c = c2[h];
-                    acc[2 * h] = fma(tv, c.x, acc[2 * h]);
-                    acc[2 * h + 1] = fma(tv, c.y, acc[2 * h + 1]);
-                }
-            }
+            for (int b = 0; b < kMaxActive; ++b)
+                if (b <= a) acc[b] = fma(tv, __ldg(C + m + (long long)b * n_bf), acc[b]);
         }
     }
-    if (!ok) return;
 #pragma unroll
-    for (int b = 0; b < kMaxActive; ++b)
-        if (b <= a) L[P + ao_pair(a, b) * n_aux] = acc[b];
+    for (int b = 0; b < kMaxActive; ++b) red[warp][b][lane] = acc[b];
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * kMaxActive; e += blockDim.x) {
+        const int l = e % 32, b = e / 32;
+        const int PP = blockIdx.x * 32 + l;
+        if (b > a || PP >= n_aux) continue;
+        L[PP + ao_pair(a, b) * n_aux] = red[0][b][l] + red[1][b][l] + red[2][b][l] + red[3][b][l];
+    }
 }
 
 // K[pair(p, q)] = sum_P L[P, p] L[P, q] (q <= p): one warp per packed element.
@@ -352,7 +358,8 @@ vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_
     };
     const size_t oB = take(bB, host), oC = take(bC, host), oT = take(bT, host || !one_index);
     const size_t oL = take(bL, host), oK = take(bK, host && K_packed);
-    const bool pipelined = n_aux % 2 == 0 && (host || reinterpret_cast<uintptr_t>(B_packed) % 16 == 0);
+    const bool pipelined = n_aux % 2 == 0 && n_bf <= kPipelinedMaxBf &&
+                           (host || reinterpret_cast<uintptr_t>(B_packed) % 16 == 0);
     const size_t oCt = take(sizeof(double) * (size_t)n_bf * kMaxActive, pipelined);
     DeviceBuffer ws;
     vb_status st = ws.allocate(ctx, off);
@@ -374,12 +381,13 @@ vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_
             double* Ct = reinterpret_cast<double*>(base + oCt);
             transpose_coefficients_kernel<<<(n_bf * kMaxActive + 255) / 256, 256, 0, s>>>(dC, n_bf, n_act, Ct);
             err = cudaGetLastError();
+            const size_t smem = pipelined_smem_bytes(n_bf);
             if (err == cudaSuccess)
                 err = cudaFuncSetAttribute(one_index_pipelined_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kPipelinedSmem);
+                                           (int)smem);
             if (err == cudaSuccess) {
-                one_index_pipelined_kernel<<<grid, 32 * kWarpsPerCta, kPipelinedSmem, s>>>(dB, n_aux, n_bf, Ct, n_act,
-                                                                                          dT);
+                const dim3 pgrid((n_bf + kPipeWarps - 1) / kPipeWarps, (n_aux + kAuxTile - 1) / kAuxTile);
+                one_index_pipelined_kernel<<<pgrid, 32 * kPipeWarps, smem, s>>>(dB, n_aux, n_bf, Ct, n_act, dT);
                 err = cudaGetLastError();
             }
         } else {
@@ -388,8 +396,7 @@ vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_
         }
     }
     if (err == cudaSuccess) {
-        const long long threads = (long long)n_aux * n_act;
-        second_index_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(dT, n_aux, n_bf, dC, n_act, dL);
+        second_index_kernel<<<dim3((n_aux + 31) / 32, n_act), 128, 0, s>>>(dT, n_aux, n_bf, dC, n_act, dL);
         err = cudaGetLastError();
     }
     if (err == cudaSuccess && K_packed) {
