@@ -209,6 +209,16 @@ vb_status vb_metric_cholesky(vb_context* ctx, const double* S, int n, int mem_sp
 vb_status vb_generalized_eigh(vb_context* ctx, const double* H, const double* S, int n, int mem_space,
                               double* eigenvalues, double* eigenvectors, int* info);
 
+/* Lowest root only, by a generalized Davidson iteration on the device (the selected-root
+ * structure solve of solve_structure_problem, src/vbscf/derivatives/gradient/active_space/
+ * evaluator.cpp:466-560; GeneralizedEigensolver::solve_davidson, src/linalg/eigensolver.hpp:
+ * 194-198) for structure spaces too large for the dense solver.  Converged when
+ * ||H c - E S c||_2 <= tolerance (||H c|| + |E| ||S c||); eigenvector S-normalized (sign
+ * arbitrary).
+ * VB_ERR_NUMERIC when max_iterations pass without convergence. */
+vb_status vb_lowest_root(vb_context* ctx, const double* H, const double* S, int n, int mem_space, double tolerance,
+                         int max_iterations, double* eigenvalue, double* eigenvector, int* iterations);
+
 /* `count` independent problems in device memory (one CTA each): problem b has dimension
  * dims[b], H, S and eigenvectors at element offset offsets[b], eigenvalues at
  * value_offsets[b]; info[b] (host) = 0, n + i (S not positive definite) or -1 (no

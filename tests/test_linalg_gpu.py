@@ -131,3 +131,27 @@ def test_batched_matches_single(ctx):
         wr, _ = O.generalized_eigh(H, S)
         assert np.abs(w - wr).max() < 1e-11 * np.abs(wr).max()
         assert np.abs(C.T @ S @ C - np.eye(len(w))).max() < 1e-10
+
+
+@pytest.mark.parametrize("kw,n", [("COV", 8), ("COV ION(1)", 8), ("COV ION(1)", 10)])
+def test_lowest_root_matches_dsygvd_on_structure_problems(ctx, kw, n):
+    S, h, eri = workloads.active_space(n, 3 * n, 300 + n)
+    rows = vbcore.generate_structures(kw, n, n)
+    ex = vbcore.expand_structures(rows, n)
+    plan = vbcore.HsPlan(ctx, ex, n)
+    Hs, Ss = plan.execute(S, h, eri)
+    E, c, its = vbcore.lowest_root(ctx, Hs, Ss, tolerance=1e-11)
+    wr, Cr = O.generalized_eigh(Hs, Ss)
+    assert abs(E - wr[0]) < 1e-9 * max(1.0, abs(wr[0]))
+    assert abs(c @ Ss @ c - 1.0) < 1e-10
+    r0 = Cr[:, 0]
+    assert min(np.abs(c - r0).max(), np.abs(c + r0).max()) < 1e-6 * np.abs(r0).max()
+    plan.close()
+
+
+def test_lowest_root_random(ctx):
+    n = 700
+    H = _random_symmetric(n, 12)
+    S = O.conditioned_metric(n, 1e3, seed=13)
+    E, c, its = vbcore.lowest_root(ctx, H, S, tolerance=1e-11, max_iterations=3000)
+    assert abs(E - O.generalized_eigh(H, S)[0][0]) < 1e-9 * max(1.0, abs(E))

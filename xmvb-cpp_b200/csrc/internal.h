@@ -36,6 +36,10 @@ constexpr int kMaxOrbitals = 64;
 vb_status set_error(vb_context* ctx, vb_status code, const std::string& message);
 vb_status cuda_error(vb_context* ctx, cudaError_t err, const char* what);
 
+// U^-1 of the Cholesky factor S = U^T U of a device matrix (linalg.cu); *info > 0 when the
+// leading minor of that order is not positive definite.  Synchronizes the context stream.
+vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double* Ui_out, int* info);
+
 // Budgeted device allocation; returns nullptr (and records VB_ERR_BUDGET / VB_ERR_CUDA) on failure.
 void* device_alloc(vb_context* ctx, size_t bytes, vb_status* status);
 void device_free(vb_context* ctx, void* ptr, size_t bytes);

@@ -51,7 +51,7 @@ struct Control {
 
 struct EighArgs {
     int n;
-    int mode;            // 0: Cholesky only, 1: full generalized eigenproblem
+    int mode;            // 0: Cholesky only, 1: full generalized eigenproblem, 2: Cholesky + U^-1
     const double* H;     // n x n, column-major (upper triangle read)
     const double* S;     // n x n, column-major (upper triangle read)
     double* U;           // Cholesky factor (output for mode 0)
@@ -586,6 +586,7 @@ __device__ void eigh_body(const EighArgs& a, const Sync& sync, Shared& sh, int c
     if (!cholesky(a, sync, sh, cta, ncta)) return;
     if (a.mode == 0) return;
     if (!triangular_inverse(a, sync, sh, cta, ncta)) return;
+    if (a.mode == 2) return;
     // T = H Ui (H symmetric from its upper triangle; Ui upper)
     const double* H = a.H;
     const double* Ui = a.Ui;
@@ -669,6 +670,7 @@ Layout layout_for(int n, int mode, bool own_inputs, bool own_outputs) {
         return at;
     };
     L.U = take(m2);
+    if (mode == 2) L.Ui = take(m2);
     if (mode == 1) {
         L.Ui = take(m2);
         L.T = take(m2);
@@ -694,7 +696,7 @@ Layout layout_for(int n, int mode, bool own_inputs, bool own_outputs) {
 cudaError_t clear_workspace(unsigned char* base, const Layout& L, int n, int mode, cudaStream_t s) {
     const size_t m2 = sizeof(double) * (size_t)n * n;
     cudaError_t err = cudaMemsetAsync(base + L.ctl, 0, sizeof(Control), s);
-    if (err == cudaSuccess && mode == 1) err = cudaMemsetAsync(base + L.Ui, 0, m2, s);
+    if (err == cudaSuccess && mode >= 1) err = cudaMemsetAsync(base + L.Ui, 0, m2, s);
     if (err == cudaSuccess && mode == 1) err = cudaMemsetAsync(base + L.V, 0, m2, s);
     return err;
 }
@@ -707,6 +709,7 @@ EighArgs args_for(unsigned char* base, const Layout& L, int n, int mode, const d
     a.H = H;
     a.S = S;
     a.U = U_out ? U_out : reinterpret_cast<double*>(base + L.U);
+    if (mode == 2) a.Ui = reinterpret_cast<double*>(base + L.Ui);
     if (mode == 1) {
         a.Ui = reinterpret_cast<double*>(base + L.Ui);
         a.T = reinterpret_cast<double*>(base + L.T);
@@ -814,6 +817,36 @@ vb_status run_single(vb_context* ctx, int mode, const double* H, const double* S
 }
 
 }  // namespace
+
+namespace vbcore {
+
+// U^-1 of the Cholesky factor of a device matrix (upper triangles read); *info = order of the
+// first non-positive leading minor (0 on success).  Synchronizes the context stream.
+vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double* Ui_out, int* info) {
+    *info = 0;
+    cudaStream_t s = ctx->stream;
+    const Layout L = layout_for(n, 2, false, false);
+    DeviceBuffer ws;
+    vb_status st = ws.allocate(ctx, L.total);
+    if (st != VB_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ws.ptr);
+    cudaError_t err = clear_workspace(base, L, n, 2, s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "factor_inverse_device");
+    EighArgs a = args_for(base, L, n, 2, nullptr, M, nullptr, nullptr, nullptr);
+    int grid = 0;
+    err = launch_single(a, s, &grid);
+    Control c{};
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&c, base + L.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(Ui_out, base + L.Ui, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(ctx, err, "factor_inverse_device");
+    if (c.err) return set_error(ctx, VB_ERR_TIMEOUT, "factor_inverse_device: grid barrier timed out");
+    *info = c.info;
+    return VB_OK;
+}
+
+}  // namespace vbcore
 
 extern "C" {
 

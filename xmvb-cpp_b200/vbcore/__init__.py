@@ -87,7 +87,7 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
     "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
     "vb_active_transform_ri", "vb_active_transform_ri_adjoint", "vb_hs_plan_gradient",
-    "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
+    "vb_lowest_root", "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
     "vb_scf_ao_integrals", "vb_scf_energy_gradient", "vb_solve_scf",
 )
 
@@ -128,6 +128,8 @@ def load_library(path: str = LIB_PATH):
     lib.vb_metric_cholesky.argtypes = [P, P, c.c_int, c.c_int, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh.argtypes = [P, P, P, c.c_int, c.c_int, P, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh_batched.argtypes = [P, c.c_int, P, P, P, P, c.c_int, P, P, P, P]
+    lib.vb_lowest_root.argtypes = [P, P, P, c.c_int, c.c_int, c.c_double, c.c_int, c.POINTER(c.c_double), P,
+                                   c.POINTER(c.c_int)]
     lib.vb_ao_integrals_s.argtypes = [c.POINTER(_ScfInput), P, P, P, c.POINTER(c.c_double)]
     lib.vb_scf_problem_create.argtypes = [P, c.POINTER(_ScfInput), c.POINTER(P)]
     lib.vb_scf_problem_destroy.argtypes = [P]
@@ -356,6 +358,21 @@ def generalized_eigh(ctx: "Context", H, S):
                                             ctypes.byref(info))
     _check(st, ctx.handle, info.value)
     return w, C.reshape(n, n).T.copy()
+
+
+def lowest_root(ctx: "Context", H, S, tolerance: float = 1e-10, max_iterations: int = 1000):
+    """(E, c, iterations): lowest root of H c = E S c by the device Davidson iteration."""
+    H = np.asarray(H, dtype=np.float64)
+    S = np.asarray(S, dtype=np.float64)
+    n = H.shape[0]
+    Hf = _c(H.T, np.float64)
+    Sf = _c(S.T, np.float64)
+    c = np.empty(n)
+    e = ctypes.c_double()
+    its = ctypes.c_int()
+    _check(load_library().vb_lowest_root(ctx.handle, _ptr(Hf), _ptr(Sf), n, VB_MEM_HOST, tolerance, max_iterations,
+                                         ctypes.byref(e), _ptr(c), ctypes.byref(its)), ctx.handle)
+    return e.value, c, its.value
 
 
 def generalized_eigh_batched(ctx: "Context", problems, device=None):
