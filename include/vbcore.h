@@ -287,6 +287,39 @@ vb_status vb_scf_energy_gradient(vb_scf_problem* problem, const double* coeffici
 vb_status vb_solve_scf(vb_scf_problem* problem, const double* initial_coefficients, const vb_scf_options* options,
                        vb_scf_result* result, double* coefficients_out);
 
+/* ---- batched and served work ------------------------------------------------------------------ */
+
+/* An engine: n_workers host workers, each with its own context (stream, memory pool), sharing
+ * one GPU.  No counterpart in the reference (one instance per process); requests mirror its
+ * solve entry point (xmvb::cuda::solve_scf, src/cuda/vb/scf.hpp:41-46). */
+typedef struct vb_engine vb_engine;
+vb_status vb_engine_create(int device, size_t hbm_budget_bytes, int n_workers, vb_engine** engine);
+vb_status vb_engine_destroy(vb_engine* engine);
+const char* vb_engine_last_error(const vb_engine* engine);
+
+/* Batched form: register an active-space instance (its plan stays on the device, assigned to
+ * the least-loaded worker); not concurrent with evaluate. */
+vb_status vb_engine_add_instance(vb_engine* engine, const vb_expansion* expansion, int64_t* instance_id);
+/* Energy (lowest structure root, no nuclear term) and, when dS/dh are given, its gradient with
+ * respect to S, h and the RI factors (ri_factors[i]: n(n+1)/2 x n_aux[i], column-major; NULL
+ * entries skip) for every listed instance; host buffers; returns when all are done. */
+vb_status vb_engine_evaluate_instances(vb_engine* engine, int count, const int64_t* ids, const double* const* S,
+                                       const double* const* h, const double* const* eri,
+                                       const double* const* ri_factors, const int* n_aux, double* energies,
+                                       double* const* dS, double* const* dh, double* const* dri);
+
+/* Serving: queue a VBSCF solve (copied); admitted first-in first-out when the HBM budget holds
+ * its estimated footprint (or when nothing else runs). */
+vb_status vb_engine_submit_scf(vb_engine* engine, const vb_scf_input* input, const double* initial_coefficients,
+                               const vb_scf_options* options, int64_t tag);
+/* Up to `capacity` completed solves (wait != 0: block until one completes or all are done):
+ * tag, total energy, gradient infinity norm, iterations, converged, status, seconds queued and
+ * seconds from submission to completion. */
+vb_status vb_engine_poll(vb_engine* engine, int capacity, int wait, int64_t* tags, double* energies,
+                         double* gradient_inf, int32_t* iterations, int32_t* converged, int32_t* status,
+                         double* wait_s, double* latency_s, int* n_out);
+vb_status vb_engine_pending(vb_engine* engine, int* queued, int* running, size_t* bytes_in_use);
+
 /* ---- RI AO -> active-space transform ----------------------------------------------------------- */
 
 /* transform_ri_active_integrals (src/integrals/active/ri.cpp:33-96) in FP64.  B_packed:

@@ -496,8 +496,14 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
     cudaStream_t s = ctx->stream;
     int launches = 0;
     const double *dS = nullptr, *dh = nullptr, *deri = nullptr;
-    vb_status st = prepare_spin_records(p, S, h, eri, mem_space, &dS, &dh, &deri, &launches);
-    if (st != VB_OK) return st;
+    vb_status st = VB_OK;
+    if (records_match(p, S, h, eri, mem_space)) {
+        dS = p->S_in.as<double>();
+        dh = p->h_in.as<double>();
+        deri = p->eri_in.as<double>();
+    } else if ((st = prepare_spin_records(p, S, h, eri, mem_space, &dS, &dh, &deri, &launches)) != VB_OK) {
+        return st;
+    }
     const int n = p->n, np = p->np, gd = p->gd, R = p->R;
     const int adj_stride = R + 2;
     // scratch: w, coefficients, adjoint records, gradient accumulators

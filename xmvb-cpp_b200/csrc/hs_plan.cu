@@ -392,12 +392,29 @@ FullPairArgs full_args(vb_hs_plan* p) {
 }
 
 // Stage inputs and evaluate the spin-pair records of every distinct table.
+bool records_match(const vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem) {
+    if (mem != VB_MEM_HOST || !p->records_current) return false;
+    const size_t n2 = (size_t)p->n * p->n, ne = (size_t)p->np * (p->np + 1) / 2;
+    if (p->last_inputs.size() != 2 * n2 + ne) return false;
+    return std::memcmp(p->last_inputs.data(), S, sizeof(double) * n2) == 0 &&
+           std::memcmp(p->last_inputs.data() + n2, h, sizeof(double) * n2) == 0 &&
+           std::memcmp(p->last_inputs.data() + 2 * n2, eri, sizeof(double) * ne) == 0;
+}
+
 vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem,
                                const double** dS, const double** dh, const double** deri, int* launches) {
     vb_context* ctx = p->ctx;
     cudaStream_t s = ctx->stream;
     const size_t n2 = sizeof(double) * p->n * p->n;
     const size_t ne = sizeof(double) * (size_t)p->np * (p->np + 1) / 2;
+    p->records_current = false;
+    if (mem == VB_MEM_HOST) {
+        const size_t a = (size_t)p->n * p->n, b = (size_t)p->np * (p->np + 1) / 2;
+        p->last_inputs.resize(2 * a + b);
+        std::memcpy(p->last_inputs.data(), S, n2);
+        std::memcpy(p->last_inputs.data() + a, h, n2);
+        std::memcpy(p->last_inputs.data() + 2 * a, eri, ne);
+    }
     if (mem == VB_MEM_HOST) {
         cudaError_t err = cudaMemcpyAsync(p->S_in.ptr, S, n2, cudaMemcpyHostToDevice, s);
         if (err == cudaSuccess) err = cudaMemcpyAsync(p->h_in.ptr, h, n2, cudaMemcpyHostToDevice, s);
@@ -452,6 +469,7 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
         err = launch_spin_pairs(table_args(p, true, *dS, *dh, *deri), p->tables_b.as<double>(), s, launches);
         if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs (beta)");
     }
+    p->records_current = mem == VB_MEM_HOST;
     return VB_OK;
 }
 

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -725,6 +726,11 @@ EighArgs args_for(unsigned char* base, const Layout& L, int n, int mode, const d
     return a;
 }
 
+// Multi-CTA cooperative launches are serialized across the process (they are held from launch
+// to completion by the callers below): the grid barrier needs every CTA resident, and two
+// grid-wide solves from different host threads must not compete for residency.
+std::mutex g_cooperative;
+
 cudaError_t launch_single(const EighArgs& a, cudaStream_t s, int* grid_out) {
     if (a.n <= kSmallProblem) {
         // one CTA: the grid barrier of a one-block launch never waits
@@ -788,6 +794,8 @@ vb_status run_single(vb_context* ctx, int mode, const double* H, const double* S
     if (err != cudaSuccess) return cuda_error(ctx, err, name);
     EighArgs a = args_for(base, L, n, mode, dH, dS, dvals, dvecs, mode == 0 ? dU : nullptr);
     int grid = 0;
+    std::unique_lock<std::mutex> coop(g_cooperative, std::defer_lock);
+    if (n > kSmallProblem) coop.lock();
     err = launch_single(a, s, &grid);
     if (err != cudaSuccess) return cuda_error(ctx, err, name);
     Control c{};
@@ -834,6 +842,8 @@ vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double*
     if (err != cudaSuccess) return cuda_error(ctx, err, "factor_inverse_device");
     EighArgs a = args_for(base, L, n, 2, nullptr, M, nullptr, nullptr, nullptr);
     int grid = 0;
+    std::unique_lock<std::mutex> coop(g_cooperative, std::defer_lock);
+    if (n > kSmallProblem) coop.lock();
     err = launch_single(a, s, &grid);
     Control c{};
     if (err == cudaSuccess) err = cudaMemcpyAsync(&c, base + L.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s);

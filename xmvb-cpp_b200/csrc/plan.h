@@ -42,6 +42,9 @@ struct vb_hs_plan {
     // structure incidence by determinant (CSR) and the gradient's adjoint scratch
     DeviceBuffer det_off, det_str, det_coef;
     DeviceBuffer adj_a, adj_b, grad_acc;
+    // host inputs of the last host-pointer evaluation whose records are still resident
+    std::vector<double> last_inputs;
+    bool records_current = false;
     std::vector<StructureChunk> chunks;
     // spin-flip map of the determinant list (folds the determinant-pair work in half)
     DeviceBuffer flip;
@@ -73,6 +76,8 @@ FullPairArgs full_args(vb_hs_plan* p);
 // Uploads host inputs (mem == VB_MEM_HOST), builds the integral tables and the pair-kernel
 // factorization, and evaluates every spin-pair record; *dS, *dh, *deri receive the device
 // copies of the inputs.
+// True when the resident spin-pair records were evaluated from exactly these host inputs.
+bool records_match(const vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem);
 vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem,
                                const double** dS, const double** dh, const double** deri, int* launches);
 

@@ -137,6 +137,10 @@ AoIntegrals ao_integrals(const Basis& b, int n_atoms, const double* Z, const dou
 
 int pidx(int a, int b) { return a > b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; }
 
+// structure spaces up to this size take the dense all-root solver, larger ones the
+// lowest-root Davidson iteration
+constexpr int kDenseStructureLimit = 200;
+
 struct Active {
     std::vector<double> S, h, eri;  // eri packed
     std::vector<double> T3;         // (kappa x|y z): kappa + nbf (x + na (y + na z))
@@ -246,7 +250,12 @@ vb_status evaluate(vb_scf_problem* pr, const std::vector<double>& C, double* ene
     if (st != VB_OK) return st;
     std::vector<double> w(ns), V((size_t)ns * ns);
     int info = 0;
-    st = vb_generalized_eigh(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, w.data(), V.data(), &info);
+    if (ns <= kDenseStructureLimit) {
+        st = vb_generalized_eigh(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, w.data(), V.data(), &info);
+    } else {
+        int its = 0;
+        st = vb_lowest_root(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, 1.0e-11, 2000, w.data(), V.data(), &its);
+    }
     if (st != VB_OK) return st;
     *energy = w[0] + pr->ao.enuc;
     if (Hs_out) *Hs_out = Hs;

@@ -87,7 +87,9 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
     "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
     "vb_active_transform_ri", "vb_active_transform_ri_adjoint", "vb_hs_plan_gradient",
-    "vb_lowest_root", "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
+    "vb_lowest_root", "vb_engine_create", "vb_engine_destroy", "vb_engine_last_error", "vb_engine_add_instance",
+    "vb_engine_evaluate_instances", "vb_engine_submit_scf", "vb_engine_poll", "vb_engine_pending",
+    "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
     "vb_scf_ao_integrals", "vb_scf_energy_gradient", "vb_solve_scf",
 )
 
@@ -128,6 +130,15 @@ def load_library(path: str = LIB_PATH):
     lib.vb_metric_cholesky.argtypes = [P, P, c.c_int, c.c_int, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh.argtypes = [P, P, P, c.c_int, c.c_int, P, P, c.POINTER(c.c_int)]
     lib.vb_generalized_eigh_batched.argtypes = [P, c.c_int, P, P, P, P, c.c_int, P, P, P, P]
+    lib.vb_engine_create.argtypes = [c.c_int, c.c_size_t, c.c_int, c.POINTER(P)]
+    lib.vb_engine_destroy.argtypes = [P]
+    lib.vb_engine_last_error.argtypes = [P]
+    lib.vb_engine_last_error.restype = c.c_char_p
+    lib.vb_engine_add_instance.argtypes = [P, c.POINTER(_Expansion), c.POINTER(c.c_int64)]
+    lib.vb_engine_evaluate_instances.argtypes = [P, c.c_int, P, P, P, P, P, P, P, P, P, P]
+    lib.vb_engine_submit_scf.argtypes = [P, c.POINTER(_ScfInput), P, c.POINTER(_ScfOptions), c.c_int64]
+    lib.vb_engine_poll.argtypes = [P, c.c_int, c.c_int, P, P, P, P, P, P, P, P, c.POINTER(c.c_int)]
+    lib.vb_engine_pending.argtypes = [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_size_t)]
     lib.vb_lowest_root.argtypes = [P, P, P, c.c_int, c.c_int, c.c_double, c.c_int, c.POINTER(c.c_double), P,
                                    c.POINTER(c.c_int)]
     lib.vb_ao_integrals_s.argtypes = [c.POINTER(_ScfInput), P, P, P, c.POINTER(c.c_double)]
@@ -524,6 +535,120 @@ class ScfProblem:
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             load_library().vb_scf_problem_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine:
+    """Batched and served work on one GPU: `workers` host workers with their own contexts."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, workers: int = 8):
+        h = ctypes.c_void_p()
+        lib = load_library()
+        _check(lib.vb_engine_create(device, hbm_budget_bytes, workers, ctypes.byref(h)))
+        self._h = h
+        self.workers = workers
+        self._keep = []
+        self._n = {}
+
+    def _err(self, status):
+        if status != 0:
+            raise VbError(status, load_library().vb_engine_last_error(self._h).decode())
+
+    def add_instance(self, expansion: "Expansion", n_orbitals: int) -> int:
+        e = expansion
+        keep = [_c(e.alpha_strings, np.uint64), _c(e.beta_strings, np.uint64), _c(e.det_alpha, np.int32),
+                _c(e.det_beta, np.int32), _c(e.term_offsets, np.int64), _c(e.term_structure, np.int32),
+                _c(e.term_coefficient, np.float64)]
+        a, b, da, db, off, ts, tc = keep
+        desc = _Expansion(n_orbitals, e.n_alpha_electrons, e.n_beta_electrons, len(a), len(b), _ptr(a).value,
+                          _ptr(b).value, len(da), _ptr(da).value, _ptr(db).value, e.n_structures, _ptr(off).value,
+                          _ptr(ts).value, _ptr(tc).value)
+        iid = ctypes.c_int64()
+        self._err(load_library().vb_engine_add_instance(self._h, ctypes.byref(desc), ctypes.byref(iid)))
+        self._n[iid.value] = n_orbitals
+        return iid.value
+
+    def evaluate(self, ids, S_list, h_list, eri_list, F_list=None, gradient: bool = True):
+        """Energies (lowest roots) and, if `gradient`, per-instance dicts {S, h, ri} of the gradient."""
+        count = len(ids)
+        P = ctypes.c_void_p
+        keep = []
+
+        def ptrs(arrays):
+            arr = (P * count)()
+            for i, x in enumerate(arrays):
+                if x is None:
+                    arr[i] = None
+                else:
+                    keep.append(x)
+                    arr[i] = _ptr(x).value
+            return arr
+
+        Sf = [_c(np.asarray(S).T, np.float64) for S in S_list]
+        hf = [_c(np.asarray(h).T, np.float64) for h in h_list]
+        ef = [_c(e, np.float64) for e in eri_list]
+        Ff = [None if (F_list is None or F is None) else _c(np.asarray(F).T, np.float64)
+              for F in (F_list or [None] * count)]
+        naux = np.array([0 if F is None else np.asarray(F_list[i]).shape[1] for i, F in enumerate(Ff)], np.int32)
+        energies = np.empty(count)
+        gS = [np.empty(self._n[i] ** 2) for i in ids] if gradient else None
+        gh = [np.empty(self._n[i] ** 2) for i in ids] if gradient else None
+        gF = [None if F is None else np.empty(F.size) for F in Ff] if gradient else None
+        idarr = np.asarray(ids, np.int64)
+        st = load_library().vb_engine_evaluate_instances(
+            self._h, count, _ptr(idarr), ptrs(Sf), ptrs(hf), ptrs(ef), ptrs(Ff), _ptr(naux), _ptr(energies),
+            ptrs(gS) if gradient else None, ptrs(gh) if gradient else None, ptrs(gF) if gradient else None)
+        self._err(st)
+        if not gradient:
+            return energies, None
+        grads = []
+        for i, iid in enumerate(ids):
+            n = self._n[iid]
+            g = {"S": gS[i].reshape(n, n).T.copy(), "h": gh[i].reshape(n, n).T.copy()}
+            if gF[i] is not None:
+                g["ri"] = gF[i].reshape(naux[i], -1).T.copy()
+            grads.append(g)
+        return energies, grads
+
+    def submit_scf(self, mol, pattern, n_electrons, C0, multiplicity: int = 1, structures: str = "COV",
+                   max_iterations: int = 200, gradient_tolerance: float = 1e-6, history_size: int = 100,
+                   tag: int = 0):
+        keep = []
+        inp = _scf_input(mol, pattern, n_electrons, multiplicity, structures, keep)
+        Cf = _c(np.asarray(C0).T, np.float64)
+        opt = _ScfOptions(max_iterations, gradient_tolerance, history_size, 1e-4)
+        self._err(load_library().vb_engine_submit_scf(self._h, ctypes.byref(inp), _ptr(Cf), ctypes.byref(opt), tag))
+
+    def poll(self, wait: bool = True, capacity: int = 256):
+        tags = np.empty(capacity, np.int64)
+        e = np.empty(capacity)
+        g = np.empty(capacity)
+        it = np.empty(capacity, np.int32)
+        cv = np.empty(capacity, np.int32)
+        st = np.empty(capacity, np.int32)
+        ws = np.empty(capacity)
+        lat = np.empty(capacity)
+        n = ctypes.c_int()
+        self._err(load_library().vb_engine_poll(self._h, capacity, 1 if wait else 0, _ptr(tags), _ptr(e), _ptr(g),
+                                                _ptr(it), _ptr(cv), _ptr(st), _ptr(ws), _ptr(lat), ctypes.byref(n)))
+        return [{"tag": int(tags[i]), "energy": float(e[i]), "gradient_inf": float(g[i]), "iterations": int(it[i]),
+                 "converged": bool(cv[i]), "status": int(st[i]), "wait_s": float(ws[i]), "latency_s": float(lat[i])}
+                for i in range(n.value)]
+
+    def pending(self):
+        q, r, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+        self._err(load_library().vb_engine_pending(self._h, ctypes.byref(q), ctypes.byref(r), ctypes.byref(b)))
+        return q.value, r.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().vb_engine_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
