@@ -55,6 +55,18 @@ struct ScfRequest {
     std::vector<int32_t> shell_atom, shell_nprim, orb_off, orb_fun;
     std::string structures;
     Clock::time_point submitted;
+    // point the input block at this object's own copies (after every move)
+    void bind() {
+        in.charges = charges.data();
+        in.coords = coords.data();
+        in.shell_atom = shell_atom.data();
+        in.shell_nprim = shell_nprim.data();
+        in.shell_exponents = exps.data();
+        in.shell_coefficients = coefs.data();
+        in.orbital_offsets = orb_off.data();
+        in.orbital_functions = orb_fun.data();
+        in.structures = structures.c_str();
+    }
 };
 
 struct ScfDone {
@@ -135,6 +147,7 @@ struct vb_engine {
             const auto t_admit = Clock::now();
             d.wait_s = std::chrono::duration<double>(t_admit - req.submitted).count();
             vb_scf_problem* prob = nullptr;
+            req.bind();
             d.status = vb_scf_problem_create(ctx[w], &req.in, &prob);
             if (d.status == VB_OK) {
                 vb_scf_result res{};
@@ -315,15 +328,6 @@ vb_status vb_engine_submit_scf(vb_engine* e, const vb_scf_input* in, const doubl
     r.structures = in->structures;
     r.c0.assign(initial_coefficients, initial_coefficients + (size_t)in->n_shells * in->n_active);
     r.in = *in;
-    r.in.charges = r.charges.data();
-    r.in.coords = r.coords.data();
-    r.in.shell_atom = r.shell_atom.data();
-    r.in.shell_nprim = r.shell_nprim.data();
-    r.in.shell_exponents = r.exps.data();
-    r.in.shell_coefficients = r.coefs.data();
-    r.in.orbital_offsets = r.orb_off.data();
-    r.in.orbital_functions = r.orb_fun.data();
-    r.in.structures = r.structures.c_str();
     r.bytes = scf_bytes(in->n_active, in->n_electrons, in->multiplicity);
     {
         std::lock_guard<std::mutex> lock(e->mu);

@@ -3,12 +3,14 @@
 // The counterpart of xmvb::cuda::solve_scf (src/cuda/vb/scf.hpp:41-46) with the P-LBFGS
 // backend (run_plbfgs_backend, src/vbscf/optimization/backends/plbfgs.cpp:19-228) instead of
 // CIAH.  Per energy+gradient evaluation (every optimizer trial point):
-//   host:   S_act = C^T S_ao C, h_act = C^T h_ao C, (pq|rs) = C^4 (mu nu|la si)
-//           (transform_exact_active_integrals, src/integrals/active/exact.cpp:347-557, dense)
-//   device: structure H/S (vb_hs_plan_execute), lowest root (vb_generalized_eigh),
-//           gradient with respect to S_act, h_act, (pq|rs) (vb_hs_plan_gradient)
-//   host:   chain rule to the active coefficients, restricted to each orbital's allowed basis
-//           functions (the HAO fragment pattern of the deck).
+//   host:   S_act = C^T S_ao C, h_act = C^T h_ao C
+//   device: (pq|rs) through the RI transform of the AO pair Cholesky vectors (an exact
+//           factorization of (mu nu|la si) to 1e-15 of its largest diagonal, computed once per
+//           problem), structure H/S (vb_hs_plan_execute), lowest root (dense solver or Davidson),
+//           gradient with respect to S_act, h_act and the pair factors (vb_hs_plan_gradient),
+//           and the transform adjoint to the coefficients (vb_active_transform_ri_adjoint)
+//   host:   the one-electron chain rule, restricted to each orbital's allowed basis functions
+//           (the HAO fragment pattern of the deck).
 // Energy = lowest root + nuclear repulsion (src/vbscf/workflow/evaluator.cpp:103-108; no
 // inactive orbitals, so the one-electron reference energy is zero).
 //
@@ -214,6 +216,54 @@ Active transform(const AoIntegrals& ao, int nbf, int na, const std::vector<doubl
     return r;
 }
 
+// Pivoted Cholesky of the AO pair Coulomb matrix V[(mu nu), (la si)] = (mu nu|la si) over
+// packed pairs: V = B^T B with B [rank x n_pairs] (row = Cholesky vector, column = AO pair
+// hi(hi+1)/2+lo), stopping when the largest remaining diagonal falls to tol times the largest
+// initial one.  The packed factor has the layout of metric-whitened RI factors, so the active
+// transform, the pair-kernel factorization and the gradient run through the RI path.
+std::vector<double> ao_pair_cholesky(const AoIntegrals& ao, int n, double tol, int* rank) {
+    const int P = n * (n + 1) / 2;
+    std::vector<int> pm(P), pn(P);
+    for (int m = 0, t = 0; m < n; ++m)
+        for (int v = 0; v <= m; ++v, ++t) {
+            pm[t] = m;
+            pn[t] = v;
+        }
+    auto V = [&](int p, int q) {
+        return ao.eri[(size_t)pm[p] + (size_t)n * (pn[p] + (size_t)n * (pm[q] + (size_t)n * pn[q]))];
+    };
+    std::vector<double> diag(P);
+    double dmax = 0.0;
+    for (int p = 0; p < P; ++p) dmax = std::max(dmax, diag[p] = V(p, p));
+    std::vector<std::vector<double>> rows;
+    std::vector<char> used(P, 0);
+    while ((int)rows.size() < P) {
+        int piv = -1;
+        double best = tol * dmax;
+        for (int p = 0; p < P; ++p)
+            if (!used[p] && diag[p] > best) {
+                best = diag[p];
+                piv = p;
+            }
+        if (piv < 0) break;
+        std::vector<double> row(P);
+        const double sq = std::sqrt(diag[piv]);
+        for (int q = 0; q < P; ++q) {
+            double v = V(piv, q);
+            for (const auto& r : rows) v -= r[piv] * r[q];
+            row[q] = v / sq;
+        }
+        for (int q = 0; q < P; ++q) diag[q] -= row[q] * row[q];
+        used[piv] = 1;
+        rows.push_back(std::move(row));
+    }
+    *rank = (int)rows.size();
+    std::vector<double> B((size_t)rows.size() * P);  // column-major [rank x P]
+    for (size_t c = 0; c < rows.size(); ++c)
+        for (int q = 0; q < P; ++q) B[c + rows.size() * (size_t)q] = rows[c][q];
+    return B;
+}
+
 }  // namespace
 }  // namespace vbcore
 
@@ -223,6 +273,8 @@ struct vb_scf_problem {
     vb_context* ctx = nullptr;
     Basis basis;
     AoIntegrals ao;
+    std::vector<double> chol;  // AO pair Cholesky vectors, [n_chol x n_bf(n_bf+1)/2]
+    int n_chol = 0;
     int n_act = 0;
     std::vector<std::vector<int>> pattern;
     std::vector<int32_t> rows;
@@ -242,11 +294,39 @@ namespace {
 // One energy + gradient evaluation at coefficients C (n_bf x n_act, column-major).
 vb_status evaluate(vb_scf_problem* pr, const std::vector<double>& C, double* energy, std::vector<double>* grad,
                    std::vector<double>* Hs_out, std::vector<double>* Ss_out) {
-    const int nbf = pr->basis.n_bf, na = pr->n_act;
-    Active act = transform(pr->ao, nbf, na, C);
+    const int nbf = pr->basis.n_bf, na = pr->n_act, nc = pr->n_chol;
+    const int P = na * (na + 1) / 2;
+    // one-electron parts on the host (n_bf x n_act), two-electron parts through the device RI
+    // transform of the AO Cholesky vectors: (pq|rs) = sum_c L[c, pq] L[c, rs]
+    std::vector<double> SC((size_t)nbf * na, 0.0), HC((size_t)nbf * na, 0.0);
+    for (int a = 0; a < na; ++a)
+        for (int m = 0; m < nbf; ++m) {
+            double sacc = 0.0, hacc = 0.0;
+            for (int v = 0; v < nbf; ++v) {
+                sacc += pr->ao.S[m + (size_t)v * nbf] * C[v + (size_t)a * nbf];
+                hacc += pr->ao.H[m + (size_t)v * nbf] * C[v + (size_t)a * nbf];
+            }
+            SC[m + (size_t)a * nbf] = sacc;
+            HC[m + (size_t)a * nbf] = hacc;
+        }
+    std::vector<double> Sact((size_t)na * na), hact((size_t)na * na);
+    for (int a = 0; a < na; ++a)
+        for (int b = 0; b < na; ++b) {
+            double sacc = 0.0, hacc = 0.0;
+            for (int m = 0; m < nbf; ++m) {
+                sacc += C[m + (size_t)a * nbf] * SC[m + (size_t)b * nbf];
+                hacc += C[m + (size_t)a * nbf] * HC[m + (size_t)b * nbf];
+            }
+            Sact[a + (size_t)b * na] = sacc;
+            hact[a + (size_t)b * na] = hacc;
+        }
+    std::vector<double> L((size_t)nc * P), K((size_t)P * (P + 1) / 2), T((size_t)na * nc * nbf);
+    vb_status st = vb_active_transform_ri(pr->ctx, pr->chol.data(), nc, nbf, C.data(), na, VB_MEM_HOST,
+                                          grad ? T.data() : nullptr, L.data(), K.data());
+    if (st != VB_OK) return st;
     const int ns = pr->n_str;
     std::vector<double> Hs((size_t)ns * ns), Ss((size_t)ns * ns);
-    vb_status st = vb_hs_plan_execute(pr->plan, act.S.data(), act.h.data(), act.eri.data(), VB_MEM_HOST, Hs.data(), Ss.data());
+    st = vb_hs_plan_execute(pr->plan, Sact.data(), hact.data(), K.data(), VB_MEM_HOST, Hs.data(), Ss.data());
     if (st != VB_OK) return st;
     std::vector<double> w(ns), V((size_t)ns * ns);
     int info = 0;
@@ -261,44 +341,29 @@ vb_status evaluate(vb_scf_problem* pr, const std::vector<double>& C, double* ene
     if (Hs_out) *Hs_out = Hs;
     if (Ss_out) *Ss_out = Ss;
     if (!grad) return VB_OK;
-    std::vector<double> gS((size_t)na * na), gh((size_t)na * na), ge(act.eri.size());
-    st = vb_hs_plan_gradient(pr->plan, act.S.data(), act.h.data(), act.eri.data(), VB_MEM_HOST, V.data(), w[0],
-                             gS.data(), gh.data(), ge.data(), nullptr, 0, nullptr);
+    // gradient with respect to S_act, h_act and the pair factors F = L^T (P x n_chol)
+    std::vector<double> F((size_t)P * nc);
+    for (int c = 0; c < nc; ++c)
+        for (int q = 0; q < P; ++q) F[q + (size_t)c * P] = L[c + (size_t)nc * q];
+    std::vector<double> gS((size_t)na * na), gh((size_t)na * na), gF((size_t)P * nc);
+    st = vb_hs_plan_gradient(pr->plan, Sact.data(), hact.data(), K.data(), VB_MEM_HOST, V.data(), w[0], gS.data(),
+                             gh.data(), nullptr, F.data(), nc, gF.data());
     if (st != VB_OK) return st;
-    // chain rule: dE/dC = 2 S_ao C G_S + 2 h_ao C G_h + sum over the packed integrals
+    // dE/dC = 2 S_ao C G_S + 2 h_ao C G_h + RI adjoint of dE/dL
+    std::vector<double> gL((size_t)nc * P), gC((size_t)nbf * na);
+    for (int c = 0; c < nc; ++c)
+        for (int q = 0; q < P; ++q) gL[c + (size_t)nc * q] = gF[q + (size_t)c * P];
+    st = vb_active_transform_ri_adjoint(pr->ctx, T.data(), gL.data(), nc, nbf, na, VB_MEM_HOST, gC.data());
+    if (st != VB_OK) return st;
     std::vector<double>& g = *grad;
     g.assign((size_t)nbf * na, 0.0);
     for (int a = 0; a < na; ++a)
         for (int m = 0; m < nbf; ++m) {
-            double acc = 0.0;
-            for (int b = 0; b < na; ++b) {
-                double sc = 0.0, hc = 0.0;
-                for (int v = 0; v < nbf; ++v) {
-                    sc += pr->ao.S[m + (size_t)v * nbf] * C[v + (size_t)b * nbf];
-                    hc += pr->ao.H[m + (size_t)v * nbf] * C[v + (size_t)b * nbf];
-                }
-                acc += 2.0 * (sc * gS[b + (size_t)a * na] + hc * gh[b + (size_t)a * na]);
-            }
+            double acc = gC[m + (size_t)a * nbf];
+            for (int b = 0; b < na; ++b)
+                acc += 2.0 * (SC[m + (size_t)b * nbf] * gS[b + (size_t)a * na] + HC[m + (size_t)b * nbf] * gh[b + (size_t)a * na]);
             g[m + (size_t)a * nbf] = acc;
         }
-    auto T3 = [&](int kappa, int b, int c, int d) {
-        return act.T3[kappa + (size_t)nbf * (b + (size_t)na * (c + (size_t)na * d))];
-    };
-    for (int a = 0; a < na; ++a)
-        for (int b = 0; b <= a; ++b)
-            for (int c = 0; c < na; ++c)
-                for (int d = 0; d <= c; ++d) {
-                    const int pq = pidx(a, b), rs = pidx(c, d);
-                    if (pq < rs) continue;
-                    const double G = ge[(size_t)pq * (pq + 1) / 2 + rs];
-                    if (G == 0.0) continue;
-                    for (int k = 0; k < nbf; ++k) {
-                        g[k + (size_t)a * nbf] += G * T3(k, b, c, d);
-                        g[k + (size_t)b * nbf] += G * T3(k, a, c, d);
-                        g[k + (size_t)c * nbf] += G * T3(k, d, a, b);
-                        g[k + (size_t)d * nbf] += G * T3(k, c, a, b);
-                    }
-                }
     // parameters outside each orbital's allowed basis functions stay fixed
     for (int a = 0; a < na; ++a) {
         std::vector<char> allowed(nbf, 0);
@@ -327,6 +392,7 @@ vb_status vb_scf_problem_create(vb_context* ctx, const vb_scf_input* in, vb_scf_
     pr->ctx = ctx;
     pr->basis = make_basis(in->n_shells, in->shell_atom, in->shell_nprim, in->shell_exponents, in->shell_coefficients);
     pr->ao = ao_integrals(pr->basis, in->n_atoms, in->charges, in->coords);
+    pr->chol = ao_pair_cholesky(pr->ao, pr->basis.n_bf, 1.0e-15, &pr->n_chol);
     pr->n_act = in->n_active;
     for (int a = 0; a < in->n_active; ++a) {
         std::vector<int> f;
