@@ -591,13 +591,175 @@ def run_ri(args):
     return 0
 
 
+def _batch_instance(n: int, seed: int):
+    """A synthetic active-space instance: S, h as the microbenchmark, (ij|kl) = sum_P B_ij^P B_kl^P
+    with B ~ N(0, 0.1) of shape [3n, n, n] symmetrized; also the pair factors F [n(n+1)/2, 3n]."""
+    import numpy as np
+    from vbcore import workloads
+
+    S, h, _ = workloads.active_space(n, 3 * n, seed)
+    rng = np.random.default_rng(seed + 7919)
+    B = 0.1 * rng.standard_normal((3 * n, n, n))
+    B = 0.5 * (B + B.transpose(0, 2, 1))
+    rows, cols = np.tril_indices(n)
+    F = np.ascontiguousarray(B[:, rows, cols].T)
+    return S, h, workloads.pack_pair_kernel(F @ F.T), F
+
+
+def run_batch(args):
+    """Batched form: `--instances` synthetic instances, n drawn from `--batch-sizes` (seeded),
+    covalent + singly ionic structures; one step = energy + gradient (S, h, pair factors) of every
+    instance through the engine; compared with the same instances one at a time on one context."""
+    import numpy as np
+    import torch
+    import vbcore
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(SEED)
+    sizes = [int(x) for x in rng.choice(args.batch_sizes, size=args.instances)]
+    data = [_batch_instance(n, SEED + i) for i, n in enumerate(sizes)]
+    exps = {n: vbcore.expand_structures(vbcore.generate_structures("COV ION(1)", n, n), n) for n in set(sizes)}
+    eng = vbcore.Engine(local, 0, workers=args.workers)
+    ids = [eng.add_instance(exps[n], n) for n in sizes]
+    Sl, hl, el, Fl = zip(*data)
+    for _ in range(args.warmup):
+        eng.evaluate(ids, Sl, hl, el, Fl)
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        E, _ = eng.evaluate(ids, Sl, hl, el, Fl)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    eng.close()
+    ctx = vbcore.Context(local)
+    plans = {n: vbcore.HsPlan(ctx, exps[n], n) for n in set(sizes)}
+
+    def plain_pass():
+        energies = []
+        for i, n in enumerate(sizes):
+            S, h, eri, F = data[i]
+            Hs, Ss = plans[n].execute(S, h, eri)
+            if Hs.shape[0] <= 200:
+                w, C = vbcore.generalized_eigh(ctx, Hs, Ss)
+                lam, c = w[0], C[:, 0]
+            else:
+                lam, c, _ = vbcore.lowest_root(ctx, Hs, Ss, tolerance=1e-11, max_iterations=2000)
+            plans[n].gradient(S, h, eri, c, lam, packed_eri=False, ri_factors=F)
+            energies.append(lam)
+        return energies
+
+    plain_pass()  # warm-up
+    t0 = time.perf_counter()
+    E_plain = plain_pass()
+    t_plain = time.perf_counter() - t0
+    for p in plans.values():
+        p.close()
+    ctx.close()
+    batched = args.instances * args.steps / sum(times)
+    plain = args.instances / t_plain
+    line = {
+        "metric": "VBSCF energy+gradient evaluations/s (batched instances)", "value": batched,
+        "unit": "instance evaluations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * statistics.mean(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.instances} instances, n_active from {list(args.batch_sizes)} (seeded), "
+                               "electrons = n_active, singlet, covalent Rumer + singly ionic structures, low-rank "
+                               "(ij|kl) from B [3n, n, n]; energy + gradient w.r.t. S, h and the pair factors",
+                   "instances_by_n": {str(k): sizes.count(k) for k in sorted(set(sizes))},
+                   "workers": args.workers},
+        "plain_one_at_a_time": {"value": plain, "seconds": t_plain},
+        "speedup_vs_plain": batched / plain,
+        "max_abs_energy_diff_batched_vs_plain": float(np.max(np.abs(np.array(E) - np.array(E_plain)))),
+        "roofline": None, "cpu_baseline": None,
+        "e2e": {"value": batched, "unit": "instance evaluations/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """Serving form: Poisson arrivals of VBSCF solves of linear H_n chains (n from
+    {4, 6, 8, 10, 12, 14}, spacing U(0.7, 3.0) A with +-0.05 A jitter, 6-31G, all covalent
+    structures), through the engine (`--workers` concurrent solves, HBM admission) and through a
+    one-worker engine (sequential plain solves) on the same arrival sequence."""
+    import numpy as np
+    import torch
+    import vbcore
+    from vbcore import molecules
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    results = {}
+    for rate in args.rates:
+        rng = np.random.default_rng(SEED + int(rate))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=args.requests))
+        reqs = []
+        for _ in range(args.requests):
+            n = int(rng.choice([4, 6, 8, 10, 12, 14]))
+            mol = molecules.h_chain(n, float(rng.uniform(0.7, 3.0)), 0.05, seed=int(rng.integers(1 << 30)))
+            pat = molecules.hao_pattern(mol, n)
+            reqs.append((mol, pat, n, molecules.hao_guess(mol, pat)))
+        per = {}
+        for label, workers in (("served", args.workers), ("sequential_plain", 1)):
+            eng = vbcore.Engine(local, 0, workers=workers)
+            t0 = time.perf_counter()
+            done, i = [], 0
+            while len(done) < len(reqs):
+                now = time.perf_counter() - t0
+                while i < len(reqs) and arrivals[i] <= now:
+                    mol, pat, n, C0 = reqs[i]
+                    eng.submit_scf(mol, pat, n, C0, gradient_tolerance=1e-5, max_iterations=200, tag=i)
+                    i += 1
+                got = eng.poll(wait=False)
+                done.extend(got)
+                if not got:
+                    time.sleep(0.0005)
+            makespan = time.perf_counter() - t0
+            eng.close()
+            lat = np.array([d["latency_s"] for d in done])
+            per[label] = {"solves_per_s": len(done) / makespan, "p50_latency_s": float(np.percentile(lat, 50)),
+                          "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": makespan,
+                          "converged": int(sum(d["converged"] for d in done)),
+                          "failed": int(sum(d["status"] != 0 for d in done))}
+        per["speedup_solves_per_s"] = per["served"]["solves_per_s"] / per["sequential_plain"]["solves_per_s"]
+        results[str(rate)] = per
+    head = results[str(args.rates[0])]
+    line = {
+        "metric": "VBSCF solves/s under Poisson arrivals (served)", "value": head["served"]["solves_per_s"],
+        "unit": "solves/s", "n_gpus": world, "steps": len(args.rates), "warmup": 0, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded geometries and arrivals)",
+        "config": {"workload": f"{args.requests} requests per rate, H_n chains n in {{4..14}} even, 6-31G, COV, "
+                               "spacing U(0.7, 3.0) A +- 0.05 A, energy+gradient solves to |g|_inf <= 1e-5",
+                   "rates_per_s": list(args.rates), "workers": args.workers},
+        "per_rate": results, "roofline": None, "cpu_baseline": None,
+        "e2e": {"value": head["served"]["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vbcore", choices=["vbcore", "reference"])
-    ap.add_argument("--workload", default="hs", choices=["hs", "scf", "ri"],
+    ap.add_argument("--instances", type=int, default=256, help="batch: number of instances")
+    ap.add_argument("--batch-sizes", type=int, nargs="+", default=[4, 6, 8, 10, 12],
+                    help="batch: active-space sizes drawn per instance")
+    ap.add_argument("--workers", type=int, default=8, help="batch/serve: concurrent workers")
+    ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
+    ap.add_argument("--rates", type=float, nargs="+", default=[50.0, 200.0, 800.0], help="serve: arrival rates")
+    ap.add_argument("--workload", default="hs", choices=["hs", "scf", "ri", "batch", "serve"],
                     help="hs: determinant-pair H/S evaluation (default); scf: plain VBSCF on H6; "
                          "ri: RI AO->active transform and metric Cholesky sweep")
     ap.add_argument("--profile", action="store_true",
@@ -619,6 +781,10 @@ def main():
         return run_scf(args)
     if args.workload == "ri":
         return run_ri(args)
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_vbcore(args)
 
 
