@@ -1,11 +1,15 @@
 // Context, error reporting and budgeted device memory (the role of xmvb::cuda::Context,
 // src/cuda/memory/context.hpp:66-405 in the reference: one device, one stream, a byte budget
 // of 90 % of free HBM by default, allocation counters).
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <new>
 
+#include <cublas_v2.h>
+
 #include "internal.h"
+#include "kernels.h"
 
 namespace {
 std::mutex g_error_mutex;
@@ -100,6 +104,18 @@ vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** ou
         ctx->pool = nullptr;
         cudaGetLastError();
     }
+    // Reserve the stack the exact-path kernels need once, up front: otherwise the runtime grows
+    // the device's local-memory reservation at their first launch, which can fail while other
+    // host threads (other contexts) have work in flight.
+    {
+        static std::mutex stack_mutex;
+        std::lock_guard<std::mutex> lock(stack_mutex);
+        const size_t need = std::max(vbcore::exact_stack_bytes(), vbcore::gradient_stack_bytes()) + 1024;
+        size_t have = 0;
+        if (cudaDeviceGetLimit(&have, cudaLimitStackSize) == cudaSuccess && have < need)
+            cudaDeviceSetLimit(cudaLimitStackSize, need);
+        cudaGetLastError();
+    }
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     ctx->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.9 * (double)free_b);
@@ -114,6 +130,7 @@ vb_status vb_context_destroy(vb_context* ctx) {
         cudaStreamSynchronize(ctx->own_stream);
         cudaStreamDestroy(ctx->own_stream);
     }
+    if (ctx->blas) cublasDestroy(static_cast<cublasHandle_t>(ctx->blas));
     if (ctx->pool) {
         cudaDeviceSynchronize();
         cudaMemPoolDestroy(ctx->pool);

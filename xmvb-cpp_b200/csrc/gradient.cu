@@ -19,11 +19,17 @@
 //      G_A = adj_H h[R, L] + sum_m adj_u[m] l_m[pair(R, L)], Q = dq/dB; the linear inputs get
 //      adj_H A (h), adj_H d B-minors (the antisymmetrized two-electron table) and
 //      adj_u[m] A (factor columns).  Blocks whose conditioning certificate fails are listed.
-//   3. careful_backward_kernel: listed blocks through the exact (reference-semantics) path;
-//      every pair quantity is multilinear in the entries of X, so the X-adjoint is the exact
-//      central difference of the exact evaluation along each entry.
-// The host then maps the two-electron table and factor-column adjoints onto the packed
-// integrals (full-rank pair kernel) or onto caller-supplied RI factors.
+//   3. careful_backward_kernel: listed blocks through the exact (reference-semantics) path:
+//      full-rank blocks take the same analytic adjoint with the exact path's inverse; for
+//      rank-deficient blocks, every pair quantity is multilinear in the entries of X, so the
+//      X-adjoint is the exact central difference of the exact evaluation along each entry.
+// The two contractions over the R factor columns (adj_u . l_m at each packed pair, and the
+// factor-column adjoint sum_t adj_u (x) A-scatter) run as FP64 GEMMs (cuBLAS) over chunks of
+// records around the backward kernel, which walks left-string work items like the forward
+// kernel and accumulates the two-electron table per left string in shared memory.  The host
+// then maps the two-electron table and factor-column adjoints onto the packed integrals
+// (full-rank pair kernel) or onto caller-supplied RI factors.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,7 +47,6 @@ namespace vbcore {
 namespace {
 
 constexpr double kThreshold = 1.0e-12;
-constexpr double kCertificate2 = 1.0e12;
 
 __device__ __forceinline__ int occ_byte(const uint64_t* row, int i) {
     const uint64_t w = row[i >> 3];
@@ -141,32 +146,73 @@ struct BackArgs {
     double* gL;  // [pair q * ld + m]
     unsigned long long* careful_count;
     unsigned long long* careful_list;
+    // chunked fast path: items [item_begin, item_end) own records [record_base, ...)
+    const int2* items;
+    int item_begin, item_end;
+    long long record_base;
+    const double* Q;  // [record - record_base][np]: adj_u . l_m at each packed pair
+    double* Pout;     // [record - record_base][np]: A scattered onto packed pairs (zeroed)
 };
 
 template <int K>
 __global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
-    extern __shared__ double acc_s[];  // gS then gh (n*n each)
-    const int n = a.n;
-    for (int i = threadIdx.x; i < 2 * n * n; i += blockDim.x) acc_s[i] = 0.0;
-    __syncthreads();
+    // shared accumulators: gS, gh (n x n) and the two-electron table rows of the current left
+    // string's orbital pairs (CP x gd); flushed to global memory when the left string changes
+    extern __shared__ double acc_s[];
+    constexpr int CP = K * (K - 1) / 2;
+    const int n = a.n, gd = a.gd, np = a.ld;
     double* sgS = acc_s;
     double* sgh = acc_s + n * n;
+    double* sgG = acc_s + 2 * n * n;
+    __shared__ int sCp[CP > 0 ? CP : 1];
+    for (int i = threadIdx.x; i < 2 * n * n + CP * gd; i += blockDim.x) acc_s[i] = 0.0;
     const long long N = a.N;
-    const long long total = N * (N + 1) / 2;
-    const int R = a.R;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-        const double* adj = a.adj + t * a.adj_stride;
-        const double aS = adj[R], aH = adj[R + 1];
-        bool any = aS != 0.0 || aH != 0.0;
-        for (int m = 0; m < R && !any; ++m) any = adj[m] != 0.0;
-        if (!any) continue;
-        long long u, v;
-        upper_decode(t, N, &u, &v);
-        int L[K], Rr[K];
+    const int per = (a.item_end - a.item_begin + gridDim.x - 1) / gridDim.x;
+    const int ib = a.item_begin + blockIdx.x * per;
+    const int ie = min(a.item_end, ib + per);
+    long long cur_u = -1;
+    auto flush_gamma = [&]() {
+        __syncthreads();
+        if (cur_u >= 0)
+            for (int i = threadIdx.x; i < CP * gd; i += blockDim.x) {
+                const double v = sgG[i];
+                if (v != 0.0) atomicAdd(a.gG + (long long)sCp[i / gd] * gd + (i % gd), v);
+                sgG[i] = 0.0;
+            }
+        __syncthreads();
+    };
+    for (int item = ib; item < ie; ++item) {
+        const int2 it = a.items[item];
+        const long long u = it.x;
+        int L[K];
+        {
+            const uint64_t wl = __ldg(a.occ + 2 * u);
 #pragma unroll
-        for (int c = 0; c < K; ++c) {
-            L[c] = occ_byte(a.occ + 2 * u, c);
-            Rr[c] = occ_byte(a.occ + 2 * v, c);
+            for (int c = 0; c < K; ++c) L[c] = (int)((wl >> (8 * c)) & 0xFFu);
+        }
+        if (u != cur_u) {
+            flush_gamma();
+            if (threadIdx.x == 0) {
+                int q = 0;
+#pragma unroll
+                for (int c2 = 1; c2 < K; ++c2)
+#pragma unroll
+                    for (int c1 = 0; c1 < c2; ++c1) sCp[c2 * (c2 - 1) / 2 + c1] = dev::anti_index(L[c1], L[c2]), ++q;
+            }
+            cur_u = u;
+            __syncthreads();
+        }
+        const long long v = (long long)it.y + threadIdx.x;
+        if (v >= N) continue;
+        const long long t = record_index(u, v, N);
+        const long long tl = t - a.record_base;
+        const double* adj = a.adj + t * a.adj_stride;
+        const double aS = adj[a.R], aH = adj[a.R + 1];
+        int Rr[K];
+        {
+            const uint64_t wr = __ldg(a.occ + 2 * v);
+#pragma unroll
+            for (int c = 0; c < K; ++c) Rr[c] = (int)((wr >> (8 * c)) & 0xFFu);
         }
         double x[K][K];
         double nx2 = 0.0;
@@ -244,16 +290,15 @@ __global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
                 for (int j = 0; j < K; ++j) val = lab[j] == r ? x[c][j] : val;
                 B[c][r] = val;
             }
-        // G_A[r][c] (in x, reused as storage)
+        // G_A[r][c] = aH h(R_r, L_c) + sum_m adj_u[m] l_m[pair(R_r, L_c)], the sum read from the
+        // chunk's Q = adj_U L_f^T (in x, reused as storage)
+        const double* qrow = a.Q + tl * np;
 #pragma unroll
         for (int r = 0; r < K; ++r)
 #pragma unroll
             for (int c = 0; c < K; ++c) {
                 const int q = dev::pair_index(Rr[r], L[c]);
-                const double* lq = a.lf + (long long)q * a.ld;
-                double g = aH * __ldg(a.h + L[c] * n + Rr[r]);
-                for (int m = 0; m < R; ++m) g = fma(adj[m], __ldg(lq + m), g);
-                x[r][c] = g;
+                x[r][c] = fma(aH, __ldg(a.h + L[c] * n + Rr[r]), qrow[q]);
             }
         double gsum = 0.0;
 #pragma unroll
@@ -264,11 +309,11 @@ __global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
         double qv = 0.0;
         if (K >= 2) {
 #pragma unroll
-            for (int c1 = 0; c1 < K; ++c1)
+            for (int c2 = 1; c2 < K; ++c2)
 #pragma unroll
-                for (int c2 = c1 + 1; c2 < K; ++c2) {
-                    const double* grow = a.gamma + (long long)dev::anti_index(L[c1], L[c2]) * a.gd;
-                    double* gout = a.gG + (long long)dev::anti_index(L[c1], L[c2]) * a.gd;
+                for (int c1 = 0; c1 < c2; ++c1) {
+                    const int cpl = c2 * (c2 - 1) / 2 + c1;
+                    const double* grow = a.gamma + (long long)dev::anti_index(L[c1], L[c2]) * gd;
 #pragma unroll
                     for (int r1 = 0; r1 < K; ++r1)
 #pragma unroll
@@ -278,17 +323,15 @@ __global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
                             const double minor = B[c1][r1] * B[c2][r2] - B[c1][r2] * B[c2][r1];
                             qv = fma(G, minor, qv);
                             const double gA = aH * G;
-                            // M[r][c] += aH Q[c][r]
                             x[r1][c1] = fma(gA, B[c2][r2], x[r1][c1]);
                             x[r2][c2] = fma(gA, B[c1][r1], x[r2][c2]);
                             x[r2][c1] = fma(-gA, B[c2][r1], x[r2][c1]);
                             x[r1][c2] = fma(-gA, B[c1][r2], x[r1][c2]);
-                            if (aH != 0.0) atomicAdd(gout + rp, aH * det * minor);
+                            if (aH != 0.0) atomicAdd(sgG + cpl * gd + rp, aH * det * minor);
                         }
                 }
         }
         const double s = aS + gsum + aH * qv;
-        // P = M B  (P[r][i] = sum_c M[r][c] B[c][i]), then (B P)[c][i]
         double P[K][K];
 #pragma unroll
         for (int r = 0; r < K; ++r)
@@ -299,6 +342,7 @@ __global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
                 for (int c = 0; c < K; ++c) acc = fma(x[r][c], B[c][i], acc);
                 P[r][i] = acc;
             }
+        double* prow = a.Pout + tl * np;
 #pragma unroll
         for (int c = 0; c < K; ++c)
 #pragma unroll
@@ -310,13 +354,12 @@ __global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
                 atomicAdd(sgS + L[c] * n + Rr[i], det * (s * B[c][i] - bp));
                 const double A = det * B[c][i];
                 if (aH != 0.0) atomicAdd(sgh + L[c] * n + Rr[i], aH * A);
-                const int q = dev::pair_index(Rr[i], L[c]);
-                double* gq = a.gL + (long long)q * a.ld;
-                for (int m = 0; m < R; ++m)
-                    if (adj[m] != 0.0) atomicAdd(gq + m, adj[m] * A);
+                // A scattered onto the packed pairs: the chunk's P row (gL += adj_U^T P after);
+                // two (i, c) can share a pair when both orbitals occur in both strings
+                prow[dev::pair_index(Rr[i], L[c])] += A;
             }
     }
-    __syncthreads();
+    flush_gamma();
     for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
         if (sgS[i] != 0.0) atomicAdd(a.gS + i, sgS[i]);
         if (sgh[i] != 0.0) atomicAdd(a.gh + i, sgh[i]);
@@ -349,24 +392,58 @@ __device__ double pair_functional(const BackArgs& a, const int* L, const int* Rr
     return f;
 }
 
-// Listed (uncertified) pairs: one warp per pair.  Entries of X are split over lanes for the
-// central differences; lane 0 adds the linear-input adjoints from the exact cofactors.
-__global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long long count_all) {
-    const long long count = count_all >= 0 ? count_all : (long long)(*a.careful_count);
-    const int lane = threadIdx.x & 31;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int k = a.k, n = a.n;
-    const long long N = a.N;
-    for (long long idx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < count; idx += nwarps) {
+// Listed (uncertified) pairs [idx_begin, idx_end) of the careful list (or of all pairs): one
+// warp per pair, lane 0 resolving the block by the exact path.  Full-rank blocks take the
+// analytic adjoint with the exact inverse, rank-deficient ones central differences of the exact
+// evaluation (entries split over lanes); lane 0 adds the linear-input adjoints and writes the
+// cofactors scattered onto packed pairs into the chunk's P row (row i = idx - idx_begin; the
+// factor-column adjoint is the GEMM adj_U P^T after the kernel), reading adj_u . l_m from Q.
+__device__ __forceinline__ void careful_pair(const BackArgs& a, long long idx, int all_pairs, long long* u,
+                                             long long* v) {
+    if (all_pairs) {
+        upper_decode(idx, a.N, u, v);
+    } else {
+        const unsigned long long w = a.careful_list[idx];
+        *u = (long long)(w >> 32);
+        *v = (long long)(w & 0xffffffffull);
+    }
+}
+
+__global__ void gather_adjoint_kernel(BackArgs a, long long idx_begin, long long idx_end, int all_pairs,
+                                      double* __restrict__ Ac) {
+    const long long cnt = idx_end - idx_begin;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < cnt * a.R;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long i = e / a.R;
+        const int m = (int)(e % a.R);
         long long u, v;
-        if (count_all >= 0) {
-            upper_decode(idx, N, &u, &v);
-        } else {
-            const unsigned long long w = a.careful_list[idx];
-            u = (long long)(w >> 32);
-            v = (long long)(w & 0xffffffffull);
-        }
+        careful_pair(a, idx_begin + i, all_pairs, &u, &v);
+        Ac[e] = a.adj[record_index(u, v, a.N) * a.adj_stride + m];
+    }
+}
+
+// One thread per listed pair: the exact resolution, the analytic adjoint of full-rank blocks,
+// the linear-input adjoints (one-electron, cofactor scatter into the P row, two-electron table
+// accumulated per CTA in shared memory when it fits), and rank-deficient blocks (nullity 1..3)
+// queued for the central-difference kernel.
+__global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long long idx_begin, long long idx_end,
+                                                              int all_pairs, int gamma_in_smem,
+                                                              unsigned long long* fd_count,
+                                                              unsigned long long* fd_list) {
+    extern __shared__ double sgG[];  // gd x gd when gamma_in_smem
+    const int k = a.k, n = a.n, np = a.ld, gd = a.gd;
+    const long long N = a.N;
+    if (gamma_in_smem) {
+        for (int i = threadIdx.x; i < gd * gd; i += blockDim.x) sgG[i] = 0.0;
+        __syncthreads();
+    }
+    double* gG = gamma_in_smem ? sgG : a.gG;
+    for (long long idx = idx_begin + blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < idx_end;
+         idx += (long long)gridDim.x * blockDim.x) {
+        long long u, v;
+        careful_pair(a, idx, all_pairs, &u, &v);
         const long long t = record_index(u, v, N);
+        const long long row = idx - idx_begin;
         const double* adj = a.adj + t * a.adj_stride;
         const double aS = adj[a.R], aH = adj[a.R + 1];
         int L[dev::KMAX], Rr[dev::KMAX];
@@ -375,6 +452,120 @@ __global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long l
             Rr[c] = occ_byte(a.occ + 2 * v, c);
         }
         double x[dev::KMAX * dev::KMAX];  // x[c k + r] = X[r][c]
+        for (int c = 0; c < k; ++c)
+            for (int r = 0; r < k; ++r) x[c * k + r] = __ldg(a.S + L[c] * n + Rr[r]);
+        dev::Resolution res;
+        dev::resolve_exact(k, x, kThreshold, &res);
+        if (res.nullity == 0 && res.det != 0.0) {
+            // full rank under the reference semantics: the analytic adjoint with the exact
+            // path's inverse (B[c][r] = inv[r k + c])
+            const double d = res.det;
+            const double* qrow = a.Q + row * np;
+            double GA[dev::KMAX * dev::KMAX];  // GA[r k + c], then M = GA + aH Q^T
+            for (int r = 0; r < k; ++r)
+                for (int c = 0; c < k; ++c)
+                    GA[r * k + c] = fma(aH, __ldg(a.h + L[c] * n + Rr[r]), qrow[dev::pair_index(Rr[r], L[c])]);
+            auto Bm = [&](int c, int r) { return res.inv[r * k + c]; };
+            double gsum = 0.0;
+            for (int r = 0; r < k; ++r)
+                for (int c = 0; c < k; ++c) gsum = fma(GA[r * k + c], Bm(c, r), gsum);
+            double qv = 0.0;
+            for (int c1 = 0; c1 < k; ++c1)
+                for (int c2 = c1 + 1; c2 < k; ++c2) {
+                    const int cp = dev::anti_index(L[c1], L[c2]);
+                    const double* grow = a.gamma + (long long)cp * gd;
+                    for (int r1 = 0; r1 < k; ++r1)
+                        for (int r2 = r1 + 1; r2 < k; ++r2) {
+                            const int rp = dev::anti_index(Rr[r1], Rr[r2]);
+                            const double G = __ldg(grow + rp);
+                            const double minor = Bm(c1, r1) * Bm(c2, r2) - Bm(c1, r2) * Bm(c2, r1);
+                            qv = fma(G, minor, qv);
+                            const double gA = aH * G;
+                            GA[r1 * k + c1] = fma(gA, Bm(c2, r2), GA[r1 * k + c1]);
+                            GA[r2 * k + c2] = fma(gA, Bm(c1, r1), GA[r2 * k + c2]);
+                            GA[r2 * k + c1] = fma(-gA, Bm(c2, r1), GA[r2 * k + c1]);
+                            GA[r1 * k + c2] = fma(-gA, Bm(c1, r2), GA[r1 * k + c2]);
+                            // the second cofactor is det * minor for a nonsingular block
+                            if (aH != 0.0) atomicAdd(gG + (long long)cp * gd + rp, aH * d * minor);
+                        }
+                }
+            const double sc = aS + gsum + aH * qv;
+            double P[dev::KMAX * dev::KMAX];  // P[r k + i] = sum_c M[r][c] B[c][i]
+            for (int r = 0; r < k; ++r)
+                for (int i = 0; i < k; ++i) {
+                    double acc = 0.0;
+                    for (int c = 0; c < k; ++c) acc = fma(GA[r * k + c], Bm(c, i), acc);
+                    P[r * k + i] = acc;
+                }
+            double* prow = a.Pout + row * np;
+            for (int c = 0; c < k; ++c)
+                for (int i = 0; i < k; ++i) {
+                    double bp = 0.0;
+                    for (int r = 0; r < k; ++r) bp = fma(Bm(c, r), P[r * k + i], bp);
+                    atomicAdd(a.gS + L[c] * n + Rr[i], d * (sc * Bm(c, i) - bp));
+                    const double A = d * Bm(c, i);
+                    if (aH != 0.0) atomicAdd(a.gh + L[c] * n + Rr[i], aH * A);
+                    prow[dev::pair_index(Rr[i], L[c])] += A;
+                }
+            continue;
+        }
+        // rank-deficient: overlap adjoint by differences (nullity <= 3; >= 4 contributes zero:
+        // every first derivative is then a minor of order >= k - 3, and one perturbed entry leaves
+        // nullity >= 3, where the reference semantics set all pair quantities to zero)
+        if (res.nullity <= 3) {
+            const unsigned long long slot = atomicAdd(fd_count, 1ull);
+            fd_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
+        }
+        if (res.nullity < 3) {
+            double cof[dev::KMAX * dev::KMAX];
+            dev::first_cofactor(res, cof);
+            double* prow = a.Pout + row * np;
+            for (int c = 0; c < k; ++c)
+                for (int r = 0; r < k; ++r) {
+                    const double A = cof[c * k + r];
+                    if (A == 0.0) continue;
+                    if (aH != 0.0) atomicAdd(a.gh + L[c] * n + Rr[r], aH * A);
+                    prow[dev::pair_index(Rr[r], L[c])] += A;
+                }
+            if (aH != 0.0 && k >= 2)
+                for (int c1 = 0; c1 < k; ++c1)
+                    for (int c2 = c1 + 1; c2 < k; ++c2)
+                        for (int r1 = 0; r1 < k; ++r1)
+                            for (int r2 = r1 + 1; r2 < k; ++r2) {
+                                const double m2 = dev::second_cofactor(res, r1, r2, c1, c2);
+                                if (m2 != 0.0)
+                                    atomicAdd(gG + (long long)dev::anti_index(L[c1], L[c2]) * gd +
+                                                  dev::anti_index(Rr[r1], Rr[r2]),
+                                              aH * m2);
+                            }
+        }
+    }
+    if (gamma_in_smem) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < gd * gd; i += blockDim.x)
+            if (sgG[i] != 0.0) atomicAdd(a.gG + i, sgG[i]);
+    }
+}
+
+// Rank-deficient listed blocks: one warp per block, entries of X split over lanes, the overlap
+// adjoint as exact central differences of the exact (multilinear) pair functional.
+__global__ void __launch_bounds__(64) difference_backward_kernel(BackArgs a, const unsigned long long* fd_count,
+                                                                 const unsigned long long* fd_list) {
+    const long long count = (long long)*fd_count;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int k = a.k, n = a.n;
+    for (long long idx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < count; idx += nwarps) {
+        const unsigned long long w = fd_list[idx];
+        const long long u = (long long)(w >> 32), v = (long long)(w & 0xffffffffull);
+        const double* adj = a.adj + record_index(u, v, a.N) * a.adj_stride;
+        const double aS = adj[a.R], aH = adj[a.R + 1];
+        int L[dev::KMAX], Rr[dev::KMAX];
+        for (int c = 0; c < k; ++c) {
+            L[c] = occ_byte(a.occ + 2 * u, c);
+            Rr[c] = occ_byte(a.occ + 2 * v, c);
+        }
+        double x[dev::KMAX * dev::KMAX];
         double xmax = 0.0;
         for (int c = 0; c < k; ++c)
             for (int r = 0; r < k; ++r) {
@@ -392,45 +583,112 @@ __global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long l
             x[c * k + r] = x0;
             atomicAdd(a.gS + L[c] * n + Rr[r], (fp - fm) / (2.0 * eps));
         }
-        if (lane == 0) {
-            dev::Resolution res;
-            dev::resolve_exact(k, x, kThreshold, &res);
-            double cof[dev::KMAX * dev::KMAX];
-            dev::first_cofactor(res, cof);
-            for (int c = 0; c < k; ++c)
-                for (int r = 0; r < k; ++r) {
-                    const double A = cof[c * k + r];
-                    if (A == 0.0) continue;
-                    if (aH != 0.0 && res.nullity < 3) atomicAdd(a.gh + L[c] * n + Rr[r], aH * A);
-                    double* gq = a.gL + (long long)dev::pair_index(Rr[r], L[c]) * a.ld;
-                    for (int m = 0; m < a.R; ++m)
-                        if (adj[m] != 0.0) atomicAdd(gq + m, adj[m] * A);
-                }
-            if (aH != 0.0 && res.nullity < 3 && k >= 2) {
-                const bool regular = res.nullity == 0 && k > 3;
-                for (int c1 = 0; c1 < k; ++c1)
-                    for (int c2 = c1 + 1; c2 < k; ++c2)
-                        for (int r1 = 0; r1 < k; ++r1)
-                            for (int r2 = r1 + 1; r2 < k; ++r2) {
-                                const double m2 =
-                                    regular ? (cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2]) / res.det
-                                            : dev::second_cofactor(res, r1, r2, c1, c2);
-                                if (m2 != 0.0)
-                                    atomicAdd(a.gG + (long long)dev::anti_index(L[c1], L[c2]) * a.gd +
-                                                  dev::anti_index(Rr[r1], Rr[r2]),
-                                              aH * m2);
-                            }
-            }
-        }
     }
 }
 
 template <int K>
 cudaError_t launch_backward(const BackArgs& b, cudaStream_t s) {
-    const size_t smem = sizeof(double) * 2 * b.n * b.n;
-    spin_backward_kernel<K><<<148 * 4, 128, smem, s>>>(b);
+    const size_t smem = sizeof(double) * (2 * b.n * b.n + (size_t)(K * (K - 1) / 2) * b.gd);
+    if (smem > 48 * 1024) {
+        cudaError_t err = cudaFuncSetAttribute(spin_backward_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+        if (err != cudaSuccess) return err;
+    }
+    const int items = b.item_end - b.item_begin;
+    const int grid = std::max(1, std::min(148 * 4, items));
+    spin_backward_kernel<K><<<grid, 128, smem, s>>>(b);
     return cudaGetLastError();
 }
+
+// The context's cuBLAS handle (created on first use, bound to the context stream).
+vb_status blas_handle(vb_context* ctx, cublasHandle_t* out) {
+    if (!ctx->blas) {
+        cublasHandle_t h = nullptr;
+        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS)
+            return set_error(ctx, VB_ERR_CUDA, "cublasCreate failed");
+        ctx->blas = h;
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->blas);
+    cublasSetStream(h, ctx->stream);
+    *out = h;
+    return VB_OK;
+}
+
+// The listed (or all) pairs in chunks: gather their u-adjoint rows Ac, Q = L_f^T Ac, the careful
+// kernel (P rows), gL += Ac P^T.
+vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_pairs, cublasHandle_t blas) {
+    if (count <= 0) return VB_OK;
+    cudaStream_t s = ctx->stream;
+    // rank-deficient blocks found by the chunks, handled by the difference kernel at the end
+    DeviceBuffer fdb;
+    vb_status st0 = fdb.allocate(ctx, sizeof(unsigned long long) * (size_t)(count + 1));
+    if (st0 != VB_OK) return st0;
+    unsigned long long* fd_count = fdb.as<unsigned long long>();
+    unsigned long long* fd_list = fd_count + 1;
+    if (cudaMemsetAsync(fd_count, 0, sizeof(unsigned long long), s) != cudaSuccess)
+        return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: memset failed");
+    const int np = b.ld, R = b.R;
+    const long long chunk = std::min<long long>(count, std::max<long long>(1024, ((long long)192 << 20) /
+                                                                                   (8LL * (2 * np + R + 1))));
+    DeviceBuffer acb, qb, pb;
+    vb_status st;
+    if ((st = acb.allocate(ctx, sizeof(double) * (size_t)chunk * std::max(R, 1))) != VB_OK) return st;
+    if ((st = qb.allocate(ctx, sizeof(double) * (size_t)chunk * np)) != VB_OK) return st;
+    if ((st = pb.allocate(ctx, sizeof(double) * (size_t)chunk * np)) != VB_OK) return st;
+    b.Q = qb.as<double>();
+    b.Pout = pb.as<double>();
+    const double one = 1.0, zero = 0.0;
+    for (long long i0 = 0; i0 < count; i0 += chunk) {
+        const long long i1 = std::min(count, i0 + chunk), cnt = i1 - i0;
+        cudaError_t err = cudaMemsetAsync(pb.ptr, 0, sizeof(double) * (size_t)cnt * np, s);
+        if (err == cudaSuccess && R > 0) {
+            gather_adjoint_kernel<<<(unsigned)std::min<long long>(4096, (cnt * R + 255) / 256), 256, 0, s>>>(
+                b, i0, i1, all_pairs, acb.as<double>());
+            err = cudaGetLastError();
+            if (err == cudaSuccess &&
+                cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, np, (int)cnt, R, &one, b.lf, np, acb.as<double>(), R,
+                            &zero, qb.as<double>(), np) != CUBLAS_STATUS_SUCCESS)
+                return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+        } else if (err == cudaSuccess) {
+            err = cudaMemsetAsync(qb.ptr, 0, sizeof(double) * (size_t)cnt * np, s);
+        }
+        if (err == cudaSuccess) {
+            const size_t smem = sizeof(double) * (size_t)b.gd * b.gd;
+            const int in_smem = smem <= 96 * 1024 ? 1 : 0;
+            if (in_smem && smem > 48 * 1024)
+                err = cudaFuncSetAttribute(careful_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+            if (err == cudaSuccess) {
+                const long long blocks = std::min<long long>(148 * 4, (cnt + 63) / 64);
+                careful_backward_kernel<<<(unsigned)blocks, 64, in_smem ? smem : 0, s>>>(
+                    b, i0, i1, all_pairs, in_smem, fd_count, fd_list);
+                err = cudaGetLastError();
+            }
+        }
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (exact path)");
+        if (R > 0 && cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, R, np, (int)cnt, &one, acb.as<double>(), R,
+                                 pb.as<double>(), np, &one, b.gL, np) != CUBLAS_STATUS_SUCCESS)
+            return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+    }
+    difference_backward_kernel<<<148 * 8, 64, 0, s>>>(b, fd_count, fd_list);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);  // fdb is released at return
+    if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (differences)");
+    return VB_OK;
+}
+
+}  // namespace
+
+// Largest per-thread stack frame among the exact-path gradient kernels (see the context).
+size_t gradient_stack_bytes() {
+    size_t m = 0;
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, careful_backward_kernel) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, difference_backward_kernel) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    return m;
+}
+
+namespace {
 
 // ---- host-side small dense algebra ---------------------------------------------------------
 
@@ -571,22 +829,80 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
         if (err != cudaSuccess) break;
         const bool fast = k <= 8 && fast_spin_supported(n, k, R);
         if (fast) {
-            switch (k) {
-                case 1: err = launch_backward<1>(b, s); break;
-                case 2: err = launch_backward<2>(b, s); break;
-                case 3: err = launch_backward<3>(b, s); break;
-                case 4: err = launch_backward<4>(b, s); break;
-                case 5: err = launch_backward<5>(b, s); break;
-                case 6: err = launch_backward<6>(b, s); break;
-                case 7: err = launch_backward<7>(b, s); break;
-                case 8: err = launch_backward<8>(b, s); break;
-                default: break;
+            // chunks of whole work items (left string u, right strings v0 .. v0 + 127): per chunk
+            // Q = L_f^T adj_U (the u-adjoint contracted with every factor column at every packed
+            // pair), the backward kernel (writes P = A scattered onto packed pairs), then
+            // gL += adj_U P^T -- the two contractions over the R factor columns as FP64 GEMMs
+            const long long NN = b.N;
+            std::vector<int2> items;
+            std::vector<long long> rec_off;  // first record of each item, then the total
+            long long tot = 0;
+            for (long long u = 0; u < NN; ++u)
+                for (long long v0 = u; v0 < NN; v0 += kSpinBlock) {
+                    items.push_back(make_int2((int)u, (int)v0));
+                    rec_off.push_back(tot);
+                    tot += std::min<long long>(kSpinBlock, NN - v0);
+                }
+            rec_off.push_back(tot);
+            const long long cap = std::max<long long>(kSpinBlock, ((long long)256 << 20) / (8LL * np));
+            DeviceBuffer ditems, qbuf, pbuf;
+            if ((st = upload(ctx, ditems, items.data(), sizeof(int2) * items.size())) != VB_OK) return st;
+            const long long rows_max = std::min<long long>(cap + kSpinBlock, tot);
+            if ((st = qbuf.allocate(ctx, sizeof(double) * (size_t)np * rows_max)) != VB_OK) return st;
+            if ((st = pbuf.allocate(ctx, sizeof(double) * (size_t)np * rows_max)) != VB_OK) return st;
+            cublasHandle_t blas = nullptr;
+            if ((st = blas_handle(ctx, &blas)) != VB_OK) return st;
+            const double one = 1.0, zero = 0.0;
+            b.items = ditems.as<int2>();
+            b.Q = qbuf.as<double>();
+            b.Pout = pbuf.as<double>();
+            for (size_t i0 = 0; i0 < items.size() && err == cudaSuccess;) {
+                size_t i1 = i0;
+                while (i1 < items.size() && rec_off[i1 + 1] - rec_off[i0] <= cap) ++i1;
+                if (i1 == i0) ++i1;
+                const long long tb = rec_off[i0], rows = rec_off[i1] - tb;
+                const double* A = b.adj + tb * adj_stride;
+                cublasStatus_t cs = CUBLAS_STATUS_SUCCESS;
+                if (R > 0)
+                    cs = cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, np, (int)rows, R, &one, b.lf, np, A, adj_stride,
+                                     &zero, qbuf.as<double>(), np);
+                else
+                    err = cudaMemsetAsync(qbuf.ptr, 0, sizeof(double) * (size_t)np * rows, s);
+                if (cs != CUBLAS_STATUS_SUCCESS)
+                    return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+                if (err == cudaSuccess) err = cudaMemsetAsync(pbuf.ptr, 0, sizeof(double) * (size_t)np * rows, s);
+                if (err != cudaSuccess) break;
+                b.item_begin = (int)i0;
+                b.item_end = (int)i1;
+                b.record_base = tb;
+                switch (k) {
+                    case 1: err = launch_backward<1>(b, s); break;
+                    case 2: err = launch_backward<2>(b, s); break;
+                    case 3: err = launch_backward<3>(b, s); break;
+                    case 4: err = launch_backward<4>(b, s); break;
+                    case 5: err = launch_backward<5>(b, s); break;
+                    case 6: err = launch_backward<6>(b, s); break;
+                    case 7: err = launch_backward<7>(b, s); break;
+                    case 8: err = launch_backward<8>(b, s); break;
+                    default: break;
+                }
+                if (err != cudaSuccess) break;
+                if (R > 0 && cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, R, np, (int)rows, &one, A, adj_stride,
+                                         pbuf.as<double>(), np, &one, gL, np) != CUBLAS_STATUS_SUCCESS)
+                    return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+                i0 = i1;
             }
             if (err != cudaSuccess) break;
-            careful_backward_kernel<<<148 * 8, 64, 0, s>>>(b, -1);
+            unsigned long long listed = 0;
+            err = cudaMemcpyAsync(&listed, b.careful_count, sizeof(listed), cudaMemcpyDeviceToHost, s);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+            if (err != cudaSuccess) break;
+            if ((st = careful_chunks(ctx, b, (long long)listed, 0, blas)) != VB_OK) return st;
         } else {
             const long long NN = b.N;
-            careful_backward_kernel<<<148 * 8, 64, 0, s>>>(b, NN * (NN + 1) / 2);
+            cublasHandle_t blas = nullptr;
+            if ((st = blas_handle(ctx, &blas)) != VB_OK) return st;
+            if ((st = careful_chunks(ctx, b, NN * (NN + 1) / 2, 1, blas)) != VB_OK) return st;
         }
         err = cudaGetLastError();
     }

@@ -14,6 +14,7 @@ struct vb_context {
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     cudaMemPool_t pool = nullptr;  // the context's own stream-ordered pool (keeps freed memory)
+    void* blas = nullptr;          // cuBLAS handle, created on first use (plain FP64 GEMMs)
     size_t budget = 0;
     size_t current = 0;
     size_t peak = 0;

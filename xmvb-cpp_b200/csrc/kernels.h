@@ -84,9 +84,21 @@ struct StructureReduceArgs {
     double* Ws;
 };
 
+// Conditioning certificate of the register-resident spin-pair paths: a block is evaluated there
+// only if ||X||_F^2 ||X^-1||_F^2 < kCertificate2, i.e. kappa_F < 1e8.  The last pivot of any LU
+// of X is 1 / (an entry of the permuted X^-1) >= 1 / ||X^-1||_F and the first complete-pivoting
+// pivot is max|x_ij| <= ||X||_F, so the smallest pivot ratio of the reference's complete-pivoting
+// LU stays >= ~1 / (c_k kappa_F) with c_k modest for k <= 16: far above its 1e-12 rank threshold,
+// so these blocks are full rank under the reference semantics.  Others take the exact path.
+constexpr double kCertificate2 = 1.0e16;
+
 constexpr int kBandReduceWarps = 8;
 constexpr int kBandReduceColumns = 32;
 constexpr int kSpinBlock = 128;    // right strings per fast-kernel item (threads per CTA)
+
+// Per-thread stack frames of the exact-path kernels (local arrays of the k <= 16 algebra).
+size_t exact_stack_bytes();
+size_t gradient_stack_bytes();
 
 cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, double* kfull, cudaStream_t stream);
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs,

@@ -29,7 +29,6 @@ namespace vbcore {
 namespace {
 
 constexpr double kThreshold = 1.0e-12;
-constexpr double kCertificate2 = 1.0e12;  // (1e6)^2 on ||X||_F^2 ||X^-1||_F^2
 constexpr double kFactorTolerance = 1.0e-15;  // relative pivot cut of the pair-kernel factorization
 constexpr int kSms = 148;
 
@@ -830,6 +829,11 @@ cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, doubl
     if (blocks < 1) blocks = 1;
     prepare_tables_kernel<<<(unsigned)blocks, 256, 0, stream>>>(n, eri, gamma, kfull);
     return cudaGetLastError();
+}
+
+size_t exact_stack_bytes() {
+    cudaFuncAttributes fa{};
+    return cudaFuncGetAttributes(&fa, spin_pairs_exact) == cudaSuccess ? fa.localSizeBytes : 0;
 }
 
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches) {
