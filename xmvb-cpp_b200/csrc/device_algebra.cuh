@@ -1,4 +1,5 @@
-// Exact-semantics determinant-pair algebra for the device (runtime k <= 16, local arrays).
+// Exact-semantics determinant-pair algebra for the device (runtime k <= KM, local arrays sized by
+// the compile-time bound KM: 16 by default, 8 for kernels instantiated for k <= 8).
 //
 // This is the path every block takes when the register-resident fast path cannot certify
 // that the reference's rank decision would be "full rank": it follows
@@ -38,9 +39,10 @@ __device__ __forceinline__ double eri_packed(const double* eri, int p, int q, in
 }
 
 // Complete-pivoting LU; returns the rank, writes det and (if rank == k and inv != nullptr) the inverse.
+template <int KM = KMAX>
 __device__ inline int full_pivot_lu(int k, const double* x, double threshold, double* det, double* inv) {
-    double lu[KMAX * KMAX];
-    int rowt[KMAX], colt[KMAX];
+    double lu[KM * KM];
+    int rowt[KM], colt[KM];
     for (int i = 0; i < k * k; ++i) lu[i] = x[i];
     int ntrans = 0, nonzero = k;
     double maxpivot = 0.0;
@@ -93,7 +95,7 @@ __device__ inline int full_pivot_lu(int k, const double* x, double threshold, do
     for (int i = 0; i < k; ++i) d *= lu[i * k + i];
     *det = d;
     if (inv != nullptr && rank == k) {
-        double c[KMAX];
+        double c[KM];
         for (int col = 0; col < k; ++col) {
             for (int i = 0; i < k; ++i) c[i] = (i == col) ? 1.0 : 0.0;
             for (int s = 0; s < k; ++s) {
@@ -119,8 +121,9 @@ __device__ inline int full_pivot_lu(int k, const double* x, double threshold, do
 }
 
 // Two-sided cyclic Jacobi SVD: x = u diag(sv) v^T, sv descending.
+template <int KM = KMAX>
 __device__ inline void jacobi_svd(int k, const double* x, double* sv, double* u, double* v) {
-    double a[KMAX * KMAX];
+    double a[KM * KM];
     double scale = 0.0;
     for (int i = 0; i < k * k; ++i) scale = fmax(scale, fabs(x[i]));
     if (scale == 0.0) scale = 1.0;
@@ -210,27 +213,32 @@ __device__ inline void jacobi_svd(int k, const double* x, double* sv, double* u,
     }
 }
 
+template <int KM = KMAX>
 __device__ inline double orthogonal_det_sign(int k, const double* q) {
     double det = 0.0;
-    full_pivot_lu(k, q, 1e-300, &det, nullptr);
+    full_pivot_lu<KM>(k, q, 1e-300, &det, nullptr);
     return det >= 0.0 ? 1.0 : -1.0;
 }
 
 // Resolution of one overlap block with the reference's semantics.
-struct Resolution {
+template <int KM>
+struct ResolutionT {
     int k;
     double det;
     int nullity;
     double parity;
     bool have_svd;
-    double x[KMAX * KMAX];
-    double inv[KMAX * KMAX];
-    double sv[KMAX];
-    double u[KMAX * KMAX];
-    double v[KMAX * KMAX];
+    double x[KM * KM];
+    double inv[KM * KM];
+    double sv[KM];
+    double u[KM * KM];
+    double v[KM * KM];
 };
 
-__device__ inline void resolve_exact(int k, const double* x, double threshold, Resolution* r) {
+using Resolution = ResolutionT<KMAX>;
+
+template <int KM>
+__device__ inline void resolve_exact(int k, const double* x, double threshold, ResolutionT<KM>* r) {
     r->k = k;
     r->parity = 1.0;
     r->have_svd = false;
@@ -241,19 +249,19 @@ __device__ inline void resolve_exact(int k, const double* x, double threshold, R
         return;
     }
     double det = 0.0;
-    const int rank = full_pivot_lu(k, x, threshold, &det, r->inv);
+    const int rank = full_pivot_lu<KM>(k, x, threshold, &det, r->inv);
     if (rank == k) {
         r->nullity = 0;
         r->det = det;
         return;
     }
-    jacobi_svd(k, x, r->sv, r->u, r->v);
+    jacobi_svd<KM>(k, x, r->sv, r->u, r->v);
     r->have_svd = true;
     int nullity = 0;
     for (int i = 0; i < k; ++i)
         if (r->sv[i] < threshold) ++nullity;
     r->nullity = nullity;
-    r->parity = orthogonal_det_sign(k, r->u) * orthogonal_det_sign(k, r->v);
+    r->parity = orthogonal_det_sign<KM>(k, r->u) * orthogonal_det_sign<KM>(k, r->v);
     if (nullity == 0) {
         double prod = 1.0;
         for (int i = 0; i < k; ++i) prod *= r->sv[i];
@@ -269,14 +277,16 @@ __device__ inline void resolve_exact(int k, const double* x, double threshold, R
     }
 }
 
-__device__ inline double leading_product(const Resolution& r, int count) {
+template <int KM>
+__device__ inline double leading_product(const ResolutionT<KM>& r, int count) {
     double p = 1.0;
     for (int i = 0; i < count; ++i) p *= r.sv[i];
     return p;
 }
 
 // First-order cofactor matrix (column-major, rows = right); zero for nullity >= 2.
-__device__ inline void first_cofactor(const Resolution& r, double* cof) {
+template <int KM>
+__device__ inline void first_cofactor(const ResolutionT<KM>& r, double* cof) {
     const int k = r.k;
     for (int i = 0; i < k * k; ++i) cof[i] = 0.0;
     if (k == 0) return;
@@ -334,7 +344,8 @@ __device__ inline double minor_det(int m, double* a) {
     return det;
 }
 
-__device__ inline double second_cofactor(const Resolution& r, int r1, int r2, int c1, int c2) {
+template <int KM>
+__device__ inline double second_cofactor(const ResolutionT<KM>& r, int r1, int r2, int c1, int c2) {
     const int k = r.k;
     if (r1 == r2 || c1 == c2 || k < 2) return 0.0;
     const double sign = ((r1 + r2 + c1 + c2) & 1) ? -1.0 : 1.0;
@@ -342,7 +353,7 @@ __device__ inline double second_cofactor(const Resolution& r, int r1, int r2, in
     if (k == 3) return sign * r.x[(3 - c1 - c2) * k + (3 - r1 - r2)];
     if (r.nullity == 0 && r.det != 0.0) {
         const int m = k - 2;
-        double minor[KMAX * KMAX];
+        double minor[KM * KM];
         int mc = 0;
         for (int c = 0; c < k; ++c) {
             if (c == c1 || c == c2) continue;
@@ -382,7 +393,8 @@ __device__ inline double second_cofactor(const Resolution& r, int r1, int r2, in
 
 // Same-spin Hamiltonian with the reference's branch structure; h is n x n (symmetric),
 // eri is packed.  Returns total and writes the one-electron part.
-__device__ inline double same_spin_exact(int n, int k, const int* occL, const int* occR, const Resolution& r,
+template <int KM>
+__device__ inline double same_spin_exact(int n, int k, const int* occL, const int* occR, const ResolutionT<KM>& r,
                                          const double* cof, const double* h, const double* eri, double* h1_out) {
     *h1_out = 0.0;
     if (r.nullity >= 3) return 0.0;

@@ -19,10 +19,10 @@
 //      G_A = adj_H h[R, L] + sum_m adj_u[m] l_m[pair(R, L)], Q = dq/dB; the linear inputs get
 //      adj_H A (h), adj_H d B-minors (the antisymmetrized two-electron table) and
 //      adj_u[m] A (factor columns).  Blocks whose conditioning certificate fails are listed.
-//   3. careful_backward_kernel: listed blocks through the exact (reference-semantics) path:
-//      full-rank blocks take the same analytic adjoint with the exact path's inverse; for
-//      rank-deficient blocks, every pair quantity is multilinear in the entries of X, so the
-//      X-adjoint is the exact central difference of the exact evaluation along each entry.
+//   3. careful_backward_kernel: listed blocks (uncertified: ill-conditioned or rank deficient)
+//      take the derivative of the exact cofactor polynomial, evaluated in the frame of the
+//      block's singular value decomposition (products of singular values only, no inverse;
+//      see svd_frame_adjoint).
 // The two contractions over the R factor columns (adj_u . l_m at each packed pair, and the
 // factor-column adjoint sum_t adj_u (x) A-scatter) run as FP64 GEMMs (cuBLAS) over chunks of
 // records around the backward kernel, which walks left-string work items like the forward
@@ -46,7 +46,6 @@
 namespace vbcore {
 namespace {
 
-constexpr double kThreshold = 1.0e-12;
 
 __device__ __forceinline__ int occ_byte(const uint64_t* row, int i) {
     const uint64_t w = row[i >> 3];
@@ -366,38 +365,7 @@ __global__ void __launch_bounds__(128) spin_backward_kernel(BackArgs a) {
     }
 }
 
-// Exact-semantics pair functional f(X) = aS det + aH H_same(X) + sum_m au[m] u_m(X).
-__device__ double pair_functional(const BackArgs& a, const int* L, const int* Rr, const double* x, const double* au,
-                                  double aS, double aH) {
-    const int k = a.k;
-    dev::Resolution res;
-    dev::resolve_exact(k, x, kThreshold, &res);
-    double cof[dev::KMAX * dev::KMAX];
-    dev::first_cofactor(res, cof);
-    double f = aS * res.det;
-    if (res.nullity < 3 && aH != 0.0) {
-        double h1 = 0.0;
-        f += aH * dev::same_spin_exact(a.n, k, L, Rr, res, cof, a.h, a.eri, &h1);
-    }
-    if (res.nullity <= 1)
-        for (int c = 0; c < k; ++c)
-            for (int r = 0; r < k; ++r) {
-                const double cv = cof[c * k + r];
-                if (cv == 0.0) continue;
-                const double* lq = a.lf + (long long)dev::pair_index(Rr[r], L[c]) * a.ld;
-                double acc = 0.0;
-                for (int m = 0; m < a.R; ++m) acc = fma(au[m], __ldg(lq + m), acc);
-                f = fma(cv, acc, f);
-            }
-    return f;
-}
-
-// Listed (uncertified) pairs [idx_begin, idx_end) of the careful list (or of all pairs): one
-// warp per pair, lane 0 resolving the block by the exact path.  Full-rank blocks take the
-// analytic adjoint with the exact inverse, rank-deficient ones central differences of the exact
-// evaluation (entries split over lanes); lane 0 adds the linear-input adjoints and writes the
-// cofactors scattered onto packed pairs into the chunk's P row (row i = idx - idx_begin; the
-// factor-column adjoint is the GEMM adj_U P^T after the kernel), reading adj_u . l_m from Q.
+// Listed (uncertified) pairs [idx_begin, idx_end) of the careful list, or of all pairs.
 __device__ __forceinline__ void careful_pair(const BackArgs& a, long long idx, int all_pairs, long long* u,
                                              long long* v) {
     if (all_pairs) {
@@ -422,15 +390,138 @@ __global__ void gather_adjoint_kernel(BackArgs a, long long idx_begin, long long
     }
 }
 
-// One thread per listed pair: the exact resolution, the analytic adjoint of full-rank blocks,
-// the linear-input adjoints (one-electron, cofactor scatter into the P row, two-electron table
-// accumulated per CTA in shared memory when it fits), and rank-deficient blocks (nullity 1..3)
-// queued for the central-difference kernel.
+// Product of the singular values outside the index set `skip` (bit mask).
+template <int KM>
+__device__ __forceinline__ double sv_product_except(int k, const double* sv, unsigned skip) {
+    double p = 1.0;
+    for (int l = 0; l < k; ++l)
+        if (!((skip >> l) & 1u)) p *= sv[l];
+    return p;
+}
+
+// Overlap adjoint of the exact cofactor polynomial of one block,
+//   f(X) = aS det X + sum_{r,c} Aw[r][c] C_{r,c}(X) + sum_{r1<r2, c1<c2} Gw(r1 r2; c1 c2) C_{r1 r2; c1 c2}(X)
+// (C: first- and second-order cofactors), at a block given by its singular value decomposition
+// X = U diag(sv) V^T.  Cofactors are covariant under orthogonal changes of basis, so with
+// X' = U^T X V, f(X) = det(U) det(V) F(X') where F carries the rotated weights A' = U^T Aw V and
+// G' = C2(U)^T Gw C2(V) (C2: the matrix of 2 x 2 minors).  Every cofactor of a diagonal matrix,
+// and every derivative of one, is a product of singular values, which gives
+//   df/dX = det(U) det(V) U D' V^T,
+//   D'(a,a) = aS D1_a + sum_{r != a} A'(r,r) D2_{ar} + sum_{p not containing a} G'(p,p) D3_{p+a},
+//   D'(a,b) = -A'(b,a) D2_{ab} + sum_{m != a,b} (-1)^(1+[m>a]+[m>b]) G'({b,m},{a,m}) D3_{abm},
+// with D_j the product of the singular values outside the j listed indices.  Nothing is divided
+// by a singular value, so the result is the exact derivative at any nullity.
+// Aw[r k + c]; gamma_row(c1, c2) returns the two-electron table row of the left pair (already
+// scaled by the Hamiltonian adjoint through `scale`); gX[r k + c] receives df/dX[r][c].
+template <int KM>
+__device__ void svd_frame_adjoint(int k, const double* U, const double* V, const double* sv, double parity,
+                                  double aS, const double* Aw, double scale, const double* gamma, int gd,
+                                  const int* L, const int* Rr, double* gX) {
+    // U[r][s] = U[s k + r], V[c][s] = V[s k + c]
+    double Ap[KM * KM], Dp[KM * KM], W[KM * KM];
+    for (int r = 0; r < k; ++r)
+        for (int t = 0; t < k; ++t) {
+            double acc = 0.0;
+            for (int c = 0; c < k; ++c) acc = fma(Aw[r * k + c], V[t * k + c], acc);
+            W[r * k + t] = acc;
+        }
+    for (int s2 = 0; s2 < k; ++s2)
+        for (int t = 0; t < k; ++t) {
+            double acc = 0.0;
+            for (int r = 0; r < k; ++r) acc = fma(U[s2 * k + r], W[r * k + t], acc);
+            Ap[s2 * k + t] = acc;
+        }
+    for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) {
+            if (a == b) {
+                double d = aS * sv_product_except<KM>(k, sv, 1u << a);
+                for (int r = 0; r < k; ++r)
+                    if (r != a) d = fma(Ap[r * k + r], sv_product_except<KM>(k, sv, (1u << a) | (1u << r)), d);
+                Dp[a * k + a] = d;
+            } else {
+                Dp[a * k + b] = -Ap[b * k + a] * sv_product_except<KM>(k, sv, (1u << a) | (1u << b));
+            }
+        }
+    if (k >= 3 && scale != 0.0) {
+        constexpr int KP = KM * (KM - 1) / 2;
+        const int kp = k * (k - 1) / 2;
+        int pi[KP], pj[KP];  // local pair t = j (j - 1) / 2 + i, i < j
+        for (int j = 1, t = 0; j < k; ++j)
+            for (int i = 0; i < j; ++i, ++t) {
+                pi[t] = i;
+                pj[t] = j;
+            }
+        int rowp[KP];  // table column of each right (row) pair
+        for (int t = 0; t < kp; ++t) rowp[t] = dev::anti_index(Rr[pi[t]], Rr[pj[t]]);
+        double Vq[KP], Tq[KP];
+        for (int q = 0; q < kp; ++q) {
+            const int q1 = pi[q], q2 = pj[q];
+            for (int t = 0; t < kp; ++t) {
+                const int c1 = pi[t], c2 = pj[t];
+                Vq[t] = V[q1 * k + c1] * V[q2 * k + c2] - V[q2 * k + c1] * V[q1 * k + c2];
+            }
+            for (int t = 0; t < kp; ++t) Tq[t] = 0.0;
+            for (int t = 0; t < kp; ++t) {
+                const double vc = Vq[t];
+                const double* grow = gamma + (long long)dev::anti_index(L[pi[t]], L[pj[t]]) * gd;
+                for (int rp = 0; rp < kp; ++rp) Tq[rp] = fma(__ldg(grow + rowp[rp]), vc, Tq[rp]);
+            }
+            // G'(p, q) for a row pair p = (p1 < p2)
+            auto gprime = [&](int p1, int p2) {
+                double acc = 0.0;
+                for (int rp = 0; rp < kp; ++rp) {
+                    const int r1 = pi[rp], r2 = pj[rp];
+                    acc = fma(U[p1 * k + r1] * U[p2 * k + r2] - U[p2 * k + r1] * U[p1 * k + r2], Tq[rp], acc);
+                }
+                return scale * acc;
+            };
+            const double gqq = gprime(q1, q2);
+            for (int a = 0; a < k; ++a)
+                if (a != q1 && a != q2)
+                    Dp[a * k + a] = fma(gqq, sv_product_except<KM>(k, sv, (1u << q1) | (1u << q2) | (1u << a)),
+                                        Dp[a * k + a]);
+            for (int side = 0; side < 2; ++side) {
+                const int a = side ? q2 : q1, m = side ? q1 : q2;
+                for (int b = 0; b < k; ++b) {
+                    if (b == a || b == m) continue;
+                    const double g = b < m ? gprime(b, m) : gprime(m, b);
+                    const int parity = 1 + (m > a) + (m > b);
+                    const double d3 = sv_product_except<KM>(k, sv, (1u << a) | (1u << b) | (1u << m));
+                    Dp[a * k + b] = fma((parity & 1) ? -g : g, d3, Dp[a * k + b]);
+                }
+            }
+        }
+    }
+    // gX = parity U D' V^T
+    for (int a = 0; a < k; ++a)
+        for (int c = 0; c < k; ++c) {
+            double acc = 0.0;
+            for (int b = 0; b < k; ++b) acc = fma(Dp[a * k + b], V[b * k + c], acc);
+            W[a * k + c] = acc;
+        }
+    for (int r = 0; r < k; ++r)
+        for (int c = 0; c < k; ++c) {
+            double acc = 0.0;
+            for (int a = 0; a < k; ++a) acc = fma(U[a * k + r], W[a * k + c], acc);
+            gX[r * k + c] = parity * acc;
+        }
+}
+
+// One thread per listed (uncertified) pair.  The adjoints are those of the exact cofactor
+// polynomial, evaluated in the frame of the block's singular value decomposition with the
+// singular values as computed (no rank truncation): the overlap adjoint by svd_frame_adjoint, the
+// first cofactors C = det(U) det(V) U diag(D1) V^T for the one-electron adjoint and the P row
+// (row i = idx - idx_begin, for the factor-column GEMM adj_U P^T after the kernel), and the
+// second cofactors det(U) det(V) C2(U) diag(D2) C2(V)^T for the two-electron table (accumulated
+// per CTA in shared memory when it fits).  For a full-rank block this is the same derivative as
+// the inverse-based one, without its loss of accuracy (relative kappa * eps) on ill-conditioned
+// blocks; where the reference truncates singular values below 1e-12 the two functions differ by
+// terms of that order.  adj_u . l_m at each packed pair is read from Q.
+template <int KM>
 __global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long long idx_begin, long long idx_end,
-                                                              int all_pairs, int gamma_in_smem,
-                                                              unsigned long long* fd_count,
-                                                              unsigned long long* fd_list) {
+                                                              int all_pairs, int gamma_in_smem) {
     extern __shared__ double sgG[];  // gd x gd when gamma_in_smem
+    constexpr int KP = KM * (KM - 1) / 2;
     const int k = a.k, n = a.n, np = a.ld, gd = a.gd;
     const long long N = a.N;
     if (gamma_in_smem) {
@@ -440,149 +531,81 @@ __global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long l
     double* gG = gamma_in_smem ? sgG : a.gG;
     for (long long idx = idx_begin + blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < idx_end;
          idx += (long long)gridDim.x * blockDim.x) {
+        if (k == 0) break;
         long long u, v;
         careful_pair(a, idx, all_pairs, &u, &v);
         const long long t = record_index(u, v, N);
         const long long row = idx - idx_begin;
         const double* adj = a.adj + t * a.adj_stride;
         const double aS = adj[a.R], aH = adj[a.R + 1];
-        int L[dev::KMAX], Rr[dev::KMAX];
+        int L[KM], Rr[KM];
         for (int c = 0; c < k; ++c) {
             L[c] = occ_byte(a.occ + 2 * u, c);
             Rr[c] = occ_byte(a.occ + 2 * v, c);
         }
-        double x[dev::KMAX * dev::KMAX];  // x[c k + r] = X[r][c]
+        double x[KM * KM];  // x[c k + r] = X[r][c]
         for (int c = 0; c < k; ++c)
             for (int r = 0; r < k; ++r) x[c * k + r] = __ldg(a.S + L[c] * n + Rr[r]);
-        dev::Resolution res;
-        dev::resolve_exact(k, x, kThreshold, &res);
-        if (res.nullity == 0 && res.det != 0.0) {
-            // full rank under the reference semantics: the analytic adjoint with the exact
-            // path's inverse (B[c][r] = inv[r k + c])
-            const double d = res.det;
-            const double* qrow = a.Q + row * np;
-            double GA[dev::KMAX * dev::KMAX];  // GA[r k + c], then M = GA + aH Q^T
+        double U[KM * KM], V[KM * KM], sv[KM];
+        dev::jacobi_svd<KM>(k, x, sv, U, V);
+        const double parity = dev::orthogonal_det_sign<KM>(k, U) * dev::orthogonal_det_sign<KM>(k, V);
+        const double* qrow = a.Q + row * np;
+        double GA[KM * KM];  // GA[r k + c] = aH h[L_c][R_r] + adj_u . l_m at pair(R_r, L_c)
+        for (int r = 0; r < k; ++r)
+            for (int c = 0; c < k; ++c)
+                GA[r * k + c] = fma(aH, __ldg(a.h + L[c] * n + Rr[r]), qrow[dev::pair_index(Rr[r], L[c])]);
+        {
+            double gX[KM * KM];
+            svd_frame_adjoint<KM>(k, U, V, sv, parity, aS, GA, aH, a.gamma, gd, L, Rr, gX);
             for (int r = 0; r < k; ++r)
-                for (int c = 0; c < k; ++c)
-                    GA[r * k + c] = fma(aH, __ldg(a.h + L[c] * n + Rr[r]), qrow[dev::pair_index(Rr[r], L[c])]);
-            auto Bm = [&](int c, int r) { return res.inv[r * k + c]; };
-            double gsum = 0.0;
-            for (int r = 0; r < k; ++r)
-                for (int c = 0; c < k; ++c) gsum = fma(GA[r * k + c], Bm(c, r), gsum);
-            double qv = 0.0;
-            for (int c1 = 0; c1 < k; ++c1)
-                for (int c2 = c1 + 1; c2 < k; ++c2) {
-                    const int cp = dev::anti_index(L[c1], L[c2]);
-                    const double* grow = a.gamma + (long long)cp * gd;
-                    for (int r1 = 0; r1 < k; ++r1)
-                        for (int r2 = r1 + 1; r2 < k; ++r2) {
-                            const int rp = dev::anti_index(Rr[r1], Rr[r2]);
-                            const double G = __ldg(grow + rp);
-                            const double minor = Bm(c1, r1) * Bm(c2, r2) - Bm(c1, r2) * Bm(c2, r1);
-                            qv = fma(G, minor, qv);
-                            const double gA = aH * G;
-                            GA[r1 * k + c1] = fma(gA, Bm(c2, r2), GA[r1 * k + c1]);
-                            GA[r2 * k + c2] = fma(gA, Bm(c1, r1), GA[r2 * k + c2]);
-                            GA[r2 * k + c1] = fma(-gA, Bm(c2, r1), GA[r2 * k + c1]);
-                            GA[r1 * k + c2] = fma(-gA, Bm(c1, r2), GA[r1 * k + c2]);
-                            // the second cofactor is det * minor for a nonsingular block
-                            if (aH != 0.0) atomicAdd(gG + (long long)cp * gd + rp, aH * d * minor);
-                        }
+                for (int c = 0; c < k; ++c) atomicAdd(a.gS + L[c] * n + Rr[r], gX[r * k + c]);
+        }
+        // first cofactors
+        double d1[KM];
+        for (int s2 = 0; s2 < k; ++s2) d1[s2] = parity * sv_product_except<KM>(k, sv, 1u << s2);
+        double* prow = a.Pout + row * np;
+        for (int r = 0; r < k; ++r)
+            for (int c = 0; c < k; ++c) {
+                double A = 0.0;
+                for (int s2 = 0; s2 < k; ++s2) A = fma(U[s2 * k + r] * d1[s2], V[s2 * k + c], A);
+                if (aH != 0.0) atomicAdd(a.gh + L[c] * n + Rr[r], aH * A);
+                prow[dev::pair_index(Rr[r], L[c])] += A;
+            }
+        // second cofactors into the two-electron table
+        if (aH != 0.0 && k >= 2) {
+            const int kp = k * (k - 1) / 2;
+            int pi[KP], pj[KP];
+            for (int j = 1, q = 0; j < k; ++j)
+                for (int i = 0; i < j; ++i, ++q) {
+                    pi[q] = i;
+                    pj[q] = j;
                 }
-            const double sc = aS + gsum + aH * qv;
-            double P[dev::KMAX * dev::KMAX];  // P[r k + i] = sum_c M[r][c] B[c][i]
-            for (int r = 0; r < k; ++r)
-                for (int i = 0; i < k; ++i) {
+            double d2[KP];
+            for (int q = 0; q < kp; ++q) d2[q] = aH * parity * sv_product_except<KM>(k, sv, (1u << pi[q]) | (1u << pj[q]));
+            for (int rp = 0; rp < kp; ++rp) {
+                const int r1 = pi[rp], r2 = pj[rp];
+                double w[KP];
+                for (int q = 0; q < kp; ++q) {
+                    const int p1 = pi[q], p2 = pj[q];
+                    w[q] = d2[q] * (U[p1 * k + r1] * U[p2 * k + r2] - U[p2 * k + r1] * U[p1 * k + r2]);
+                }
+                const int rcol = dev::anti_index(Rr[r1], Rr[r2]);
+                for (int cp = 0; cp < kp; ++cp) {
+                    const int c1 = pi[cp], c2 = pj[cp];
                     double acc = 0.0;
-                    for (int c = 0; c < k; ++c) acc = fma(GA[r * k + c], Bm(c, i), acc);
-                    P[r * k + i] = acc;
+                    for (int q = 0; q < kp; ++q) {
+                        const int p1 = pi[q], p2 = pj[q];
+                        acc = fma(w[q], V[p1 * k + c1] * V[p2 * k + c2] - V[p2 * k + c1] * V[p1 * k + c2], acc);
+                    }
+                    if (acc != 0.0) atomicAdd(gG + (long long)dev::anti_index(L[c1], L[c2]) * gd + rcol, acc);
                 }
-            double* prow = a.Pout + row * np;
-            for (int c = 0; c < k; ++c)
-                for (int i = 0; i < k; ++i) {
-                    double bp = 0.0;
-                    for (int r = 0; r < k; ++r) bp = fma(Bm(c, r), P[r * k + i], bp);
-                    atomicAdd(a.gS + L[c] * n + Rr[i], d * (sc * Bm(c, i) - bp));
-                    const double A = d * Bm(c, i);
-                    if (aH != 0.0) atomicAdd(a.gh + L[c] * n + Rr[i], aH * A);
-                    prow[dev::pair_index(Rr[i], L[c])] += A;
-                }
-            continue;
-        }
-        // rank-deficient: overlap adjoint by differences (nullity <= 3; >= 4 contributes zero:
-        // every first derivative is then a minor of order >= k - 3, and one perturbed entry leaves
-        // nullity >= 3, where the reference semantics set all pair quantities to zero)
-        if (res.nullity <= 3) {
-            const unsigned long long slot = atomicAdd(fd_count, 1ull);
-            fd_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
-        }
-        if (res.nullity < 3) {
-            double cof[dev::KMAX * dev::KMAX];
-            dev::first_cofactor(res, cof);
-            double* prow = a.Pout + row * np;
-            for (int c = 0; c < k; ++c)
-                for (int r = 0; r < k; ++r) {
-                    const double A = cof[c * k + r];
-                    if (A == 0.0) continue;
-                    if (aH != 0.0) atomicAdd(a.gh + L[c] * n + Rr[r], aH * A);
-                    prow[dev::pair_index(Rr[r], L[c])] += A;
-                }
-            if (aH != 0.0 && k >= 2)
-                for (int c1 = 0; c1 < k; ++c1)
-                    for (int c2 = c1 + 1; c2 < k; ++c2)
-                        for (int r1 = 0; r1 < k; ++r1)
-                            for (int r2 = r1 + 1; r2 < k; ++r2) {
-                                const double m2 = dev::second_cofactor(res, r1, r2, c1, c2);
-                                if (m2 != 0.0)
-                                    atomicAdd(gG + (long long)dev::anti_index(L[c1], L[c2]) * gd +
-                                                  dev::anti_index(Rr[r1], Rr[r2]),
-                                              aH * m2);
-                            }
+            }
         }
     }
     if (gamma_in_smem) {
         __syncthreads();
         for (int i = threadIdx.x; i < gd * gd; i += blockDim.x)
             if (sgG[i] != 0.0) atomicAdd(a.gG + i, sgG[i]);
-    }
-}
-
-// Rank-deficient listed blocks: one warp per block, entries of X split over lanes, the overlap
-// adjoint as exact central differences of the exact (multilinear) pair functional.
-__global__ void __launch_bounds__(64) difference_backward_kernel(BackArgs a, const unsigned long long* fd_count,
-                                                                 const unsigned long long* fd_list) {
-    const long long count = (long long)*fd_count;
-    const int lane = threadIdx.x & 31;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int k = a.k, n = a.n;
-    for (long long idx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < count; idx += nwarps) {
-        const unsigned long long w = fd_list[idx];
-        const long long u = (long long)(w >> 32), v = (long long)(w & 0xffffffffull);
-        const double* adj = a.adj + record_index(u, v, a.N) * a.adj_stride;
-        const double aS = adj[a.R], aH = adj[a.R + 1];
-        int L[dev::KMAX], Rr[dev::KMAX];
-        for (int c = 0; c < k; ++c) {
-            L[c] = occ_byte(a.occ + 2 * u, c);
-            Rr[c] = occ_byte(a.occ + 2 * v, c);
-        }
-        double x[dev::KMAX * dev::KMAX];
-        double xmax = 0.0;
-        for (int c = 0; c < k; ++c)
-            for (int r = 0; r < k; ++r) {
-                x[c * k + r] = __ldg(a.S + L[c] * n + Rr[r]);
-                xmax = fmax(xmax, fabs(x[c * k + r]));
-            }
-        const double eps = 1.0e-2 * (xmax > 0.0 ? xmax : 1.0);
-        for (int e = lane; e < k * k; e += 32) {
-            const int c = e / k, r = e % k;
-            const double x0 = x[c * k + r];
-            x[c * k + r] = x0 + eps;
-            const double fp = pair_functional(a, L, Rr, x, adj, aS, aH);
-            x[c * k + r] = x0 - eps;
-            const double fm = pair_functional(a, L, Rr, x, adj, aS, aH);
-            x[c * k + r] = x0;
-            atomicAdd(a.gS + L[c] * n + Rr[r], (fp - fm) / (2.0 * eps));
-        }
     }
 }
 
@@ -619,14 +642,6 @@ vb_status blas_handle(vb_context* ctx, cublasHandle_t* out) {
 vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_pairs, cublasHandle_t blas) {
     if (count <= 0) return VB_OK;
     cudaStream_t s = ctx->stream;
-    // rank-deficient blocks found by the chunks, handled by the difference kernel at the end
-    DeviceBuffer fdb;
-    vb_status st0 = fdb.allocate(ctx, sizeof(unsigned long long) * (size_t)(count + 1));
-    if (st0 != VB_OK) return st0;
-    unsigned long long* fd_count = fdb.as<unsigned long long>();
-    unsigned long long* fd_list = fd_count + 1;
-    if (cudaMemsetAsync(fd_count, 0, sizeof(unsigned long long), s) != cudaSuccess)
-        return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: memset failed");
     const int np = b.ld, R = b.R;
     const long long chunk = std::min<long long>(count, std::max<long long>(1024, ((long long)192 << 20) /
                                                                                    (8LL * (2 * np + R + 1))));
@@ -655,13 +670,12 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
         if (err == cudaSuccess) {
             const size_t smem = sizeof(double) * (size_t)b.gd * b.gd;
             const int in_smem = smem <= 96 * 1024 ? 1 : 0;
+            auto kernel = b.k <= 8 ? careful_backward_kernel<8> : careful_backward_kernel<dev::KMAX>;
             if (in_smem && smem > 48 * 1024)
-                err = cudaFuncSetAttribute(careful_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
+                err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (err == cudaSuccess) {
                 const long long blocks = std::min<long long>(148 * 4, (cnt + 63) / 64);
-                careful_backward_kernel<<<(unsigned)blocks, 64, in_smem ? smem : 0, s>>>(
-                    b, i0, i1, all_pairs, in_smem, fd_count, fd_list);
+                kernel<<<(unsigned)blocks, 64, in_smem ? smem : 0, s>>>(b, i0, i1, all_pairs, in_smem);
                 err = cudaGetLastError();
             }
         }
@@ -670,10 +684,6 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
                                  pb.as<double>(), np, &one, b.gL, np) != CUBLAS_STATUS_SUCCESS)
             return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
     }
-    difference_backward_kernel<<<148 * 8, 64, 0, s>>>(b, fd_count, fd_list);
-    cudaError_t err = cudaGetLastError();
-    if (err == cudaSuccess) err = cudaStreamSynchronize(s);  // fdb is released at return
-    if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (differences)");
     return VB_OK;
 }
 
@@ -683,8 +693,9 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
 size_t gradient_stack_bytes() {
     size_t m = 0;
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, careful_backward_kernel) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
-    if (cudaFuncGetAttributes(&fa, difference_backward_kernel) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, careful_backward_kernel<8>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, careful_backward_kernel<dev::KMAX>) == cudaSuccess)
+        m = std::max(m, fa.localSizeBytes);
     return m;
 }
 

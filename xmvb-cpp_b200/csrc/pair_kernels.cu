@@ -7,18 +7,20 @@
 //    registers, Gauss-Jordan inversion with partial pivoting (row interchanges tracked as a
 //    label permutation, no dynamic register indexing), determinant, first cofactors
 //    A = det X^{-T}, one-electron and same-spin two-electron energies from shared-memory
-//    tables.  A block is accepted only when ||X||_F ||X^{-1}||_F < 1e9: then every pivot of a
-//    complete-pivoting LU exceeds sigma_min / k >= 1e-12 * (growth bound) * max pivot for
-//    k <= 16, i.e. the reference's FullPivLU would also find full rank
-//    (overlap.cpp:60-71).  Every other block is appended to a list for the exact kernel.
-//  * spin_pairs_exact: complete-pivoting LU / Jacobi SVD with the reference semantics
-//    (device_algebra.cuh) for listed blocks.
+//    tables.  A block is accepted only when ||X||_F ||X^{-1}||_F < 1e8 (kCertificate2): then the
+//    last pivot of a complete-pivoting LU is at least 1 / ||X^{-1}||_F and the first at most
+//    ||X||_F, so their ratio stays far above 1e-12 and the reference's FullPivLU would also find
+//    full rank (overlap.cpp:60-71).  Every other block is appended to a list for the exact kernel.
+//  * spin_pairs_exact<KM>: complete-pivoting LU / Jacobi SVD with the reference semantics
+//    (device_algebra.cuh) for listed blocks, one thread per block, local arrays bounded by KM.
 //  * full_pairs<KB>: one thread per determinant pair (d <= e) of a band of columns:
 //    S = S_a S_b, H = H_a S_b + H_b S_a + sum A_a(r,c) A_b(r',c') (r c | r' c')
 //    (evaluator.cpp:95-148, 354-384), the opposite-spin sum as k_a^2 k_b^2 gathers of the
 //    shared-memory pair kernel against the beta cofactors held in registers.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "device_algebra.cuh"
@@ -580,90 +582,109 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a, c
     }
 }
 
-__device__ __forceinline__ void unanti(int p, int* a, int* b) {
-    int hi = 1;
-    while ((hi + 1) * hi / 2 <= p) ++hi;
-    *b = hi;
-    *a = p - hi * (hi - 1) / 2;
-}
 
-// One warp per listed pair: every lane resolves the block (same result), then the lanes split
-// the one- and two-electron terms and the u-vector entries; sums are reduced across the warp.
+// Listed blocks (or all blocks): one thread per block resolves it by the exact path and sums its
+// one- and two-electron terms; its first cofactors go to the warp's shared-memory slot, from
+// which the warp writes the u-vectors of its 32 records with the factor columns split over lanes.
+// Dynamic shared memory: 32 k^2 doubles per warp.
+template <int KM>
 __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
+    extern __shared__ double slots[];
     const long long count = a.all_careful ? a.n_pairs : (long long)(*a.careful_count);
     const int lane = threadIdx.x & 31;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int k = a.k;
+    const int k = a.k, kk = a.k * a.k, gd = a.gamma_dim;
+    double* wslot = slots + (size_t)(threadIdx.x >> 5) * 32 * kk;
+    double* cof = wslot + (size_t)lane * kk;
     const long long N = a.n_strings;
-    for (long long idx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < count; idx += nwarps) {
-        long long u, v;
-        if (a.all_careful) {
-            long long uu = 0;
-            const double b = 2.0 * (double)N + 1.0;
-            uu = (long long)floor((b - sqrt(fmax(b * b - 8.0 * (double)idx, 0.0))) * 0.5);
-            if (uu < 0) uu = 0;
-            if (uu > N - 1) uu = N - 1;
-            while (uu > 0 && uu * N - uu * (uu - 1) / 2 > idx) --uu;
-            while (uu + 1 < N && (uu + 1) * N - (uu + 1) * uu / 2 <= idx) ++uu;
-            u = uu;
-            v = u + (idx - (u * N - u * (u - 1) / 2));
-        } else {
-            const unsigned long long w = a.careful_list[idx];
-            u = (long long)(w >> 32);
-            v = (long long)(w & 0xffffffffull);
-        }
-        const long long t = record_index(u, v, N);
-        int L[dev::KMAX], R[dev::KMAX];
-        for (int c = 0; c < k; ++c) {
-            L[c] = occ_byte(a.occ + 2 * u, c);
-            R[c] = occ_byte(a.occ + 2 * v, c);
-        }
-        double x[dev::KMAX * dev::KMAX];
-        for (int c = 0; c < k; ++c)
-            for (int r = 0; r < k; ++r) x[c * k + r] = __ldg(a.S + R[r] * a.n + L[c]);
-        dev::Resolution res;
-        dev::resolve_exact(k, x, kThreshold, &res);
-        double cof[dev::KMAX * dev::KMAX];
-        dev::first_cofactor(res, cof);
-        double h1 = 0.0, h2 = 0.0;
-        if (res.nullity < 3) {
-            if (res.nullity <= 1)
-                for (int q = lane; q < k * k; q += 32) {
-                    const int c = q / k, r = q % k;
-                    h1 += __ldg(a.h + L[c] * a.n + R[r]) * cof[c * k + r];
-                }
-            const int cp_count = k * (k - 1) / 2;
-            const bool regular = res.nullity == 0 && k > 3;
-            for (int q = lane; q < cp_count * cp_count; q += 32) {
-                int c1, c2, r1, r2;
-                unanti(q / cp_count, &c1, &c2);
-                unanti(q % cp_count, &r1, &r2);
-                const double g = dev::eri_packed(a.eri, R[r1], L[c1], R[r2], L[c2]) -
-                                 dev::eri_packed(a.eri, R[r1], L[c2], R[r2], L[c1]);
-                const double m2 = regular ? (cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2]) / res.det
-                                          : dev::second_cofactor(res, r1, r2, c1, c2);
-                h2 += g * m2;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * 32; base < count; base += nwarps * 32) {
+        const long long idx = base + lane;
+        long long u = 0, v = 0;
+        const bool valid = idx < count;
+        if (valid) {
+            if (a.all_careful) {
+                const double b = 2.0 * (double)N + 1.0;
+                long long uu = (long long)floor((b - sqrt(fmax(b * b - 8.0 * (double)idx, 0.0))) * 0.5);
+                if (uu < 0) uu = 0;
+                if (uu > N - 1) uu = N - 1;
+                while (uu > 0 && uu * N - uu * (uu - 1) / 2 > idx) --uu;
+                while (uu + 1 < N && (uu + 1) * N - (uu + 1) * uu / 2 <= idx) ++uu;
+                u = uu;
+                v = u + (idx - (u * N - u * (u - 1) / 2));
+            } else {
+                const unsigned long long w = a.careful_list[idx];
+                u = (long long)(w >> 32);
+                v = (long long)(w & 0xffffffffull);
             }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            h1 += __shfl_xor_sync(0xffffffffu, h1, o);
-            h2 += __shfl_xor_sync(0xffffffffu, h2, o);
-        }
-        double* rec = a.records + t * (long long)a.rec_stride;
-        for (int m = lane; m < a.R; m += 32) {
-            double acc = 0.0;
-            if (res.nullity <= 1)
-                for (int c = 0; c < k; ++c)
-                    for (int r = 0; r < k; ++r)
-                        acc = fma(cof[c * k + r], __ldg(a.lf + (long long)dev::pair_index(R[r], L[c]) * a.ld + m), acc);
-            rec[m] = acc;
-        }
-        if (lane == 0) {
+            int L[KM], R[KM];
+            for (int c = 0; c < k; ++c) {
+                L[c] = occ_byte(a.occ + 2 * u, c);
+                R[c] = occ_byte(a.occ + 2 * v, c);
+            }
+            double x[KM * KM];
+            for (int c = 0; c < k; ++c)
+                for (int r = 0; r < k; ++r) x[c * k + r] = __ldg(a.S + R[r] * a.n + L[c]);
+            dev::ResolutionT<KM> res;
+            dev::resolve_exact<KM>(k, x, kThreshold, &res);
+            dev::first_cofactor<KM>(res, cof);
+            double h1 = 0.0, h2 = 0.0;
+            if (res.nullity < 3) {
+                if (res.nullity <= 1)
+                    for (int c = 0; c < k; ++c)
+                        for (int r = 0; r < k; ++r) h1 = fma(__ldg(a.h + L[c] * a.n + R[r]), cof[c * k + r], h1);
+                // two-electron sum over r1 < r2, c1 < c2: gamma[(R r1, R r2)][(L c1, L c2)] is
+                // (r1 c1 | r2 c2) - (r1 c2 | r2 c1) (hamiltonian.cpp:83-162)
+                const bool regular = res.nullity == 0 && k > 3;
+                for (int r2 = 1; r2 < k; ++r2)
+                    for (int r1 = 0; r1 < r2; ++r1) {
+                        const double* grow = a.gamma + (long long)dev::anti_index(R[r1], R[r2]) * gd;
+                        double part = 0.0;
+                        for (int c2 = 1; c2 < k; ++c2)
+                            for (int c1 = 0; c1 < c2; ++c1) {
+                                const double g = __ldg(grow + dev::anti_index(L[c1], L[c2]));
+                                const double m2 =
+                                    regular ? cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2]
+                                            : dev::second_cofactor<KM>(res, r1, r2, c1, c2);
+                                part = fma(g, m2, part);
+                            }
+                        h2 += part;
+                    }
+                if (regular) h2 /= res.det;
+            } else {
+                for (int i = 0; i < kk; ++i) cof[i] = 0.0;
+            }
+            if (res.nullity > 1)
+                for (int i = 0; i < kk; ++i) cof[i] = 0.0;
+            double* rec = a.records + record_index(u, v, N) * (long long)a.rec_stride;
             rec[a.R + 0] = res.det;
             rec[a.R + 1] = res.nullity < 3 ? h1 + h2 : 0.0;
             rec[a.R + 2] = res.nullity < 3 ? h1 : 0.0;
             rec[a.R + 3] = (double)res.nullity;
         }
+        __syncwarp();
+        // u-vectors of the warp's records: u_m = sum_{c,r} A(r,c) l_m[pair(R_r, L_c)]
+        for (int j = 0; j < 32; ++j) {
+            const long long jdx = base + j;
+            if (jdx >= count) break;
+            const long long uj = __shfl_sync(0xffffffffu, u, j), vj = __shfl_sync(0xffffffffu, v, j);
+            const double* cj = wslot + (size_t)j * kk;
+            double* rec = a.records + record_index(uj, vj, N) * (long long)a.rec_stride;
+            for (int m = lane; m < a.R; m += 32) {
+                double acc = 0.0;
+                for (int c = 0; c < k; ++c) {
+                    const int lc = occ_byte(a.occ + 2 * uj, c);
+                    for (int r = 0; r < k; ++r) {
+                        const double cv = cj[c * k + r];
+                        if (cv != 0.0)
+                            acc = fma(cv, __ldg(a.lf + (long long)dev::pair_index(occ_byte(a.occ + 2 * vj, r), lc) * a.ld + m),
+                                      acc);
+                    }
+                }
+                rec[m] = acc;
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -832,8 +853,11 @@ cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, doubl
 }
 
 size_t exact_stack_bytes() {
+    size_t m = 0;
     cudaFuncAttributes fa{};
-    return cudaFuncGetAttributes(&fa, spin_pairs_exact) == cudaSuccess ? fa.localSizeBytes : 0;
+    if (cudaFuncGetAttributes(&fa, spin_pairs_exact<8>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, spin_pairs_exact<dev::KMAX>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    return m;
 }
 
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches) {
@@ -858,7 +882,13 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream
     }
     SpinTableArgs b = a;
     b.all_careful = fast_ok ? 0 : 1;
-    spin_pairs_exact<<<kSms * 8, 64, 0, stream>>>(b);
+    auto exact = a.k <= 8 ? spin_pairs_exact<8> : spin_pairs_exact<dev::KMAX>;
+    const size_t slot_bytes = sizeof(double) * 64 * (size_t)a.k * a.k;  // two warps
+    if (slot_bytes > 48 * 1024) {
+        err = cudaFuncSetAttribute(exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slot_bytes);
+        if (err != cudaSuccess) return err;
+    }
+    exact<<<kSms * 8, 64, slot_bytes, stream>>>(b);
     ++*launches;
     return cudaGetLastError();
 }
