@@ -518,9 +518,9 @@ __device__ void svd_frame_adjoint(int k, const double* U, const double* V, const
 // blocks; where the reference truncates singular values below 1e-12 the two functions differ by
 // terms of that order.  adj_u . l_m at each packed pair is read from Q.
 template <int KM>
-__global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long long idx_begin, long long idx_end,
-                                                              int all_pairs, int gamma_in_smem) {
-    extern __shared__ double sgG[];  // gd x gd when gamma_in_smem
+__global__ void __launch_bounds__(128) careful_backward_kernel(BackArgs a, long long idx_begin, long long idx_end,
+                                                               int all_pairs, int gamma_in_smem, double* gpart) {
+    extern __shared__ double sgG[];  // gd x gd when gamma_in_smem; flushed into this block's gpart slot
     constexpr int KP = KM * (KM - 1) / 2;
     const int k = a.k, n = a.n, np = a.ld, gd = a.gd;
     const long long N = a.N;
@@ -604,8 +604,17 @@ __global__ void __launch_bounds__(64) careful_backward_kernel(BackArgs a, long l
     }
     if (gamma_in_smem) {
         __syncthreads();
-        for (int i = threadIdx.x; i < gd * gd; i += blockDim.x)
-            if (sgG[i] != 0.0) atomicAdd(a.gG + i, sgG[i]);
+        double* slot = gpart + (size_t)blockIdx.x * gd * gd;  // owned by this block index
+        for (int i = threadIdx.x; i < gd * gd; i += blockDim.x) slot[i] += sgG[i];
+    }
+}
+
+// gG += sum over block slots.
+__global__ void reduce_slots_kernel(const double* __restrict__ gpart, int slots, int count, double* __restrict__ gG) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < slots; ++b) acc += gpart[(size_t)b * count + i];
+        gG[i] += acc;
     }
 }
 
@@ -643,10 +652,23 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
     if (count <= 0) return VB_OK;
     cudaStream_t s = ctx->stream;
     const int np = b.ld, R = b.R;
-    const long long chunk = std::min<long long>(count, std::max<long long>(1024, ((long long)192 << 20) /
-                                                                                   (8LL * (2 * np + R + 1))));
-    DeviceBuffer acb, qb, pb;
+    // chunk buffers: up to 768 MB, at most half of what the context budget has left
+    const size_t left = ctx->budget > ctx->current ? ctx->budget - ctx->current : 0;
+    const size_t target = std::max<size_t>((size_t)16 << 20, std::min<size_t>((size_t)768 << 20, left / 2));
+    const long long chunk = std::min<long long>(
+        count, std::max<long long>(1024, (long long)(target / (8ULL * (2 * np + R + 1)))));
+    // two-electron table per block in shared memory when it fits (three blocks per SM), each
+    // block adding into its own slot; the slots are summed once after the last chunk
+    const size_t gbytes = sizeof(double) * (size_t)b.gd * b.gd;
+    const int in_smem = gbytes <= 72 * 1024 ? 1 : 0;
+    const int grid = in_smem ? 148 * 3 : 148 * 8;
+    DeviceBuffer acb, qb, pb, slots;
     vb_status st;
+    if (in_smem) {
+        if ((st = slots.allocate(ctx, gbytes * grid)) != VB_OK) return st;
+        if (cudaMemsetAsync(slots.ptr, 0, gbytes * grid, s) != cudaSuccess)
+            return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: memset failed");
+    }
     if ((st = acb.allocate(ctx, sizeof(double) * (size_t)chunk * std::max(R, 1))) != VB_OK) return st;
     if ((st = qb.allocate(ctx, sizeof(double) * (size_t)chunk * np)) != VB_OK) return st;
     if ((st = pb.allocate(ctx, sizeof(double) * (size_t)chunk * np)) != VB_OK) return st;
@@ -668,14 +690,11 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
             err = cudaMemsetAsync(qb.ptr, 0, sizeof(double) * (size_t)cnt * np, s);
         }
         if (err == cudaSuccess) {
-            const size_t smem = sizeof(double) * (size_t)b.gd * b.gd;
-            const int in_smem = smem <= 96 * 1024 ? 1 : 0;
             auto kernel = b.k <= 8 ? careful_backward_kernel<8> : careful_backward_kernel<dev::KMAX>;
-            if (in_smem && smem > 48 * 1024)
-                err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (in_smem && gbytes > 48 * 1024)
+                err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gbytes);
             if (err == cudaSuccess) {
-                const long long blocks = std::min<long long>(148 * 4, (cnt + 63) / 64);
-                kernel<<<(unsigned)blocks, 64, in_smem ? smem : 0, s>>>(b, i0, i1, all_pairs, in_smem);
+                kernel<<<grid, 128, in_smem ? gbytes : 0, s>>>(b, i0, i1, all_pairs, in_smem, slots.as<double>());
                 err = cudaGetLastError();
             }
         }
@@ -683,6 +702,13 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
         if (R > 0 && cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, R, np, (int)cnt, &one, acb.as<double>(), R,
                                  pb.as<double>(), np, &one, b.gL, np) != CUBLAS_STATUS_SUCCESS)
             return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+    }
+    if (in_smem) {
+        const int cnt = b.gd * b.gd;
+        reduce_slots_kernel<<<std::max(1, std::min(148 * 4, (cnt + 127) / 128)), 128, 0, s>>>(slots.as<double>(), grid,
+                                                                                            cnt, b.gG);
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (table slots)");
     }
     return VB_OK;
 }
@@ -694,8 +720,6 @@ size_t gradient_stack_bytes() {
     size_t m = 0;
     cudaFuncAttributes fa{};
     if (cudaFuncGetAttributes(&fa, careful_backward_kernel<8>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
-    if (cudaFuncGetAttributes(&fa, careful_backward_kernel<dev::KMAX>) == cudaSuccess)
-        m = std::max(m, fa.localSizeBytes);
     return m;
 }
 

@@ -96,7 +96,9 @@ constexpr int kBandReduceWarps = 8;
 constexpr int kBandReduceColumns = 32;
 constexpr int kSpinBlock = 128;    // right strings per fast-kernel item (threads per CTA)
 
-// Per-thread stack frames of the exact-path kernels (local arrays of the k <= 16 algebra).
+// Per-thread stack frames of the exact-path kernels instantiated for k <= 8 (reserved when a
+// context is created; the k <= 16 instantiations, about four times larger, grow the reservation
+// at their first launch).
 size_t exact_stack_bytes();
 size_t gradient_stack_bytes();
 

@@ -636,6 +636,31 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
                 // two-electron sum over r1 < r2, c1 < c2: gamma[(R r1, R r2)][(L c1, L c2)] is
                 // (r1 c1 | r2 c2) - (r1 c2 | r2 c1) (hamiltonian.cpp:83-162)
                 const bool regular = res.nullity == 0 && k > 3;
+                // nullity 1 (k > 3): the second cofactor parity * prod_{i<k-1} sv_i *
+                // sum_{s<k-1} (u_s ^ u_n)(v_s ^ v_n) / sv_s (contractions.cpp:937-963) expands to
+                // Y(r1,c1) zu(r2) zv(c2) - Y(r1,c2) zu(r2) zv(c1) - Y(r2,c1) zu(r1) zv(c2) + Y(r2,c2) zu(r1) zv(c1)
+                // with Y = parity sum_{s<k-1} u_s v_s^T prod_{l<k-1, l != s} sv_l and (zu, zv) the null pair
+                const bool rank1 = res.nullity == 1 && k > 3;
+                double Y[KM * KM], zu[KM], zv[KM];
+                if (rank1) {
+                    const int ni = k - 1;
+                    double w[KM];
+                    for (int s2 = 0; s2 < ni; ++s2) {
+                        double p = res.parity;
+                        for (int l = 0; l < ni; ++l)
+                            if (l != s2) p *= res.sv[l];
+                        w[s2] = p;
+                    }
+                    for (int r = 0; r < k; ++r) {
+                        zu[r] = res.u[ni * k + r];
+                        zv[r] = res.v[ni * k + r];
+                        for (int c = 0; c < k; ++c) {
+                            double acc = 0.0;
+                            for (int s2 = 0; s2 < ni; ++s2) acc = fma(res.u[s2 * k + r] * w[s2], res.v[s2 * k + c], acc);
+                            Y[r * k + c] = acc;
+                        }
+                    }
+                }
                 for (int r2 = 1; r2 < k; ++r2)
                     for (int r1 = 0; r1 < r2; ++r1) {
                         const double* grow = a.gamma + (long long)dev::anti_index(R[r1], R[r2]) * gd;
@@ -643,9 +668,14 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
                         for (int c2 = 1; c2 < k; ++c2)
                             for (int c1 = 0; c1 < c2; ++c1) {
                                 const double g = __ldg(grow + dev::anti_index(L[c1], L[c2]));
-                                const double m2 =
-                                    regular ? cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2]
-                                            : dev::second_cofactor<KM>(res, r1, r2, c1, c2);
+                                double m2;
+                                if (regular)
+                                    m2 = cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2];
+                                else if (rank1)
+                                    m2 = Y[r1 * k + c1] * zu[r2] * zv[c2] - Y[r1 * k + c2] * zu[r2] * zv[c1] -
+                                         Y[r2 * k + c1] * zu[r1] * zv[c2] + Y[r2 * k + c2] * zu[r1] * zv[c1];
+                                else
+                                    m2 = dev::second_cofactor<KM>(res, r1, r2, c1, c2);
                                 part = fma(g, m2, part);
                             }
                         h2 += part;
@@ -856,7 +886,6 @@ size_t exact_stack_bytes() {
     size_t m = 0;
     cudaFuncAttributes fa{};
     if (cudaFuncGetAttributes(&fa, spin_pairs_exact<8>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
-    if (cudaFuncGetAttributes(&fa, spin_pairs_exact<dev::KMAX>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
     return m;
 }
 
