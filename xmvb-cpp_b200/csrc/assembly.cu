@@ -11,6 +11,7 @@
 // Every sum runs in a fixed order (no atomics), so results are bitwise reproducible.
 #include <cuda_runtime.h>
 
+#include "internal.h"
 #include "kernels.h"
 
 namespace vbcore {
@@ -124,7 +125,7 @@ int band_reduce_max_structures() { return (int)((227 * 1024) / (sizeof(double) *
 
 cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches) {
     const size_t smem = band_reduce_smem_bytes(a.struct_count);
-    cudaError_t err = cudaFuncSetAttribute(band_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t err = allow_dynamic_smem((const void*)band_reduce_kernel, (int)smem);
     if (err != cudaSuccess) return err;
     const long long blocks = (a.width + kBandReduceColumns - 1) / kBandReduceColumns;
     band_reduce_kernel<<<(unsigned)blocks, kBandReduceWarps * 32, smem, stream>>>(a);

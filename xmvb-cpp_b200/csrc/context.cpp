@@ -3,6 +3,7 @@
 // of 90 % of free HBM by default, allocation counters).
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 
@@ -56,6 +57,43 @@ void device_free(vb_context* ctx, void* ptr, size_t bytes) {
     if (!ptr) return;
     cudaFreeAsync(ptr, ctx->stream);
     ctx->current -= bytes;
+}
+
+cudaError_t allow_dynamic_smem(const void* kernel, size_t bytes) {
+    static std::mutex mutex;
+    static std::map<std::pair<const void*, int>, size_t> raised;
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    std::lock_guard<std::mutex> lock(mutex);
+    const auto key = std::make_pair(kernel, dev);
+    const auto it = raised.find(key);
+    if (it != raised.end() && it->second >= bytes) return cudaSuccess;
+    int optin = 0;
+    if ((err = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return err;
+    cudaFuncAttributes fa{};
+    if ((err = cudaFuncGetAttributes(&fa, kernel)) != cudaSuccess) return err;
+    const size_t limit = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+    if (bytes > limit) return cudaErrorInvalidValue;
+    if ((err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit)) != cudaSuccess)
+        return err;
+    raised[key] = limit;
+    return cudaSuccess;
+}
+
+void* context_scratch(vb_context* ctx, int slot, size_t bytes, vb_status* status) {
+    *status = VB_OK;
+    if (bytes == 0) bytes = 16;
+    if (ctx->scratch_bytes[slot] >= bytes) return ctx->scratch[slot];
+    device_free(ctx, ctx->scratch[slot], ctx->scratch_bytes[slot]);
+    ctx->scratch[slot] = nullptr;
+    ctx->scratch_bytes[slot] = 0;
+    void* p = device_alloc(ctx, bytes, status);
+    if (p) {
+        ctx->scratch[slot] = p;
+        ctx->scratch_bytes[slot] = bytes;
+    }
+    return p;
 }
 
 }  // namespace vbcore
@@ -126,6 +164,7 @@ vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** ou
 vb_status vb_context_destroy(vb_context* ctx) {
     if (!ctx) return VB_OK;
     cudaSetDevice(ctx->device);
+    for (int i = 0; i < 6; ++i) device_free(ctx, ctx->scratch[i], ctx->scratch_bytes[i]);
     if (ctx->own_stream) {
         cudaStreamSynchronize(ctx->own_stream);
         cudaStreamDestroy(ctx->own_stream);

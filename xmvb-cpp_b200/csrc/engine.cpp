@@ -91,7 +91,7 @@ size_t scf_bytes(int n_act, int n_el, int mult) {
     const size_t np = (size_t)n_act * (n_act + 1) / 2;
     const size_t rec = (Na * (Na + 1) / 2 + (ka == kb ? 0 : Nb * (Nb + 1) / 2)) * (np + 6) * 8;
     const size_t ndet = std::min(Na * Nb, (size_t)4000000);
-    const size_t band = std::min<size_t>((size_t)4 << 30, ndet * ndet * 16);
+    const size_t band = std::min<size_t>((size_t)1 << 30, ndet * ndet * 16);
     const size_t nstr = std::max<size_t>(1, ndet / 4);
     return rec + band + 8 * nstr * nstr * 8 + ((size_t)64 << 20);
 }

@@ -622,8 +622,7 @@ template <int K>
 cudaError_t launch_backward(const BackArgs& b, cudaStream_t s) {
     const size_t smem = sizeof(double) * (2 * b.n * b.n + (size_t)(K * (K - 1) / 2) * b.gd);
     if (smem > 48 * 1024) {
-        cudaError_t err = cudaFuncSetAttribute(spin_backward_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem);
+        cudaError_t err = allow_dynamic_smem((const void*)spin_backward_kernel<K>, (int)smem);
         if (err != cudaSuccess) return err;
     }
     const int items = b.item_end - b.item_begin;
@@ -692,7 +691,7 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
         if (err == cudaSuccess) {
             auto kernel = b.k <= 8 ? careful_backward_kernel<8> : careful_backward_kernel<dev::KMAX>;
             if (in_smem && gbytes > 48 * 1024)
-                err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gbytes);
+                err = allow_dynamic_smem((const void*)kernel, (int)gbytes);
             if (err == cudaSuccess) {
                 kernel<<<grid, 128, in_smem ? gbytes : 0, s>>>(b, i0, i1, all_pairs, in_smem, slots.as<double>());
                 err = cudaGetLastError();

@@ -267,18 +267,14 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
 
     if (!p->has_flip) p->det_pair_evaluations = p->n_det * (p->n_det + 1) / 2;
 
-    // band of determinant columns: keep the two band buffers within ~4 GB and 1/4 of the budget
-    const size_t band_cap = std::min<size_t>((size_t)4 << 30, ctx->budget / 4);
+    // band of determinant columns: keep the two band buffers within ~1 GB and 1/8 of the budget
+    const size_t band_cap = std::min<size_t>((size_t)1 << 30, ctx->budget / 8);
     long long width = (long long)(band_cap / (16 * (size_t)p->n_det));
     width = std::max(32LL, std::min(width, p->n_det));
     p->band_width = width;
-    if ((st = p->band_h.allocate(ctx, sizeof(double) * p->n_det * width)) != VB_OK) return fail(st);
-    if ((st = p->band_s.allocate(ctx, sizeof(double) * p->n_det * width)) != VB_OK) return fail(st);
-    const size_t zbytes = sizeof(double) * (size_t)p->n_str * p->n_det;
-    if ((st = p->Zh.allocate(ctx, zbytes)) != VB_OK) return fail(st);
-    if ((st = p->Zs.allocate(ctx, zbytes)) != VB_OK) return fail(st);
+    // the bands and the structure-reduce buffers (Z, W) are the context's execute scratch
     const size_t wbytes = sizeof(double) * (size_t)p->n_str * p->n_str;
-    for (DeviceBuffer* b : {&p->Wh, &p->Ws, &p->Hout, &p->Sout})
+    for (DeviceBuffer* b : {&p->Hout, &p->Sout})
         if ((st = b->allocate(ctx, wbytes)) != VB_OK) return fail(st);
 
     // structure-major incidence (CSC of T)
@@ -489,6 +485,18 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
     const double *dS, *dh, *deri;
     vb_status st = prepare_spin_records(p, S, h, eri, mem, &dS, &dh, &deri, &launches);
     if (st != VB_OK) return st;
+    // execute scratch of the context: bands [n_det x width] and Z [n_det x n_str] (H, S), W [n_str^2] (H, S)
+    double* scr[6];
+    {
+        const size_t band = sizeof(double) * (size_t)p->n_det * p->band_width;
+        const size_t zb = sizeof(double) * (size_t)p->n_str * p->n_det;
+        const size_t wb = sizeof(double) * (size_t)p->n_str * p->n_str;
+        const size_t sizes[6] = {band, band, zb, zb, wb, wb};
+        for (int i = 0; i < 6; ++i) {
+            scr[i] = static_cast<double*>(context_scratch(ctx, i, sizes[i], &st));
+            if (!scr[i]) return st;
+        }
+    }
     FullPairArgs fa = full_args(p);
     fa.flip = p->has_flip ? p->flip.as<int>() : nullptr;
     for (long long e0 = 0; e0 < p->n_det; e0 += p->band_width) {
@@ -497,8 +505,8 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
         fa.e0 = e0;
         fa.e1 = e1;
         fa.n_items = e0 * B + B * (B + 1) / 2;
-        fa.Hb = p->band_h.as<double>();
-        fa.Sb = p->band_s.as<double>();
+        fa.Hb = scr[0];
+        fa.Sb = scr[1];
         PhaseMark pairs(p, VB_PHASE_DETERMINANT_PAIRS);
         cudaError_t err = launch_full_pairs(fa, s, &launches);
         if (err != cudaSuccess) return cuda_error(ctx, err, "full_pairs");
@@ -518,8 +526,8 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
             ba.wcoef = ch.wcoef.as<double>();
             ba.struct_begin = ch.begin;
             ba.struct_count = ch.count;
-            ba.Zh = p->Zh.as<double>();
-            ba.Zs = p->Zs.as<double>();
+            ba.Zh = scr[2];
+            ba.Zs = scr[3];
             err = launch_band_reduce(ba, s, &launches);
             if (err != cudaSuccess) return cuda_error(ctx, err, "band_reduce");
         }
@@ -530,10 +538,10 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
     ra.str_off = p->str_off.as<long long>();
     ra.str_det = p->str_det.as<long long>();
     ra.str_coef = p->str_coef.as<double>();
-    ra.Zh = p->Zh.as<double>();
-    ra.Zs = p->Zs.as<double>();
-    ra.Wh = p->Wh.as<double>();
-    ra.Ws = p->Ws.as<double>();
+    ra.Zh = scr[2];
+    ra.Zs = scr[3];
+    ra.Wh = scr[4];
+    ra.Ws = scr[5];
     double* Hdst = mem == VB_MEM_DEVICE ? H_out : p->Hout.as<double>();
     double* Sdst = mem == VB_MEM_DEVICE ? S_out : p->Sout.as<double>();
     PhaseMark sreduce(p, VB_PHASE_STRUCTURE_REDUCE);

@@ -15,6 +15,10 @@ struct vb_context {
     cudaStream_t own_stream = nullptr;
     cudaMemPool_t pool = nullptr;  // the context's own stream-ordered pool (keeps freed memory)
     void* blas = nullptr;          // cuBLAS handle, created on first use (plain FP64 GEMMs)
+    // grow-only execute scratch shared by every plan of this context (plans of one context run
+    // in order on its stream): the determinant-pair bands and the structure-reduce buffers
+    void* scratch[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t scratch_bytes[6] = {0, 0, 0, 0, 0, 0};
     size_t budget = 0;
     size_t current = 0;
     size_t peak = 0;
@@ -40,6 +44,16 @@ vb_status cuda_error(vb_context* ctx, cudaError_t err, const char* what);
 // U^-1 of the Cholesky factor S = U^T U of a device matrix (linalg.cu); *info > 0 when the
 // leading minor of that order is not positive definite.  Synchronizes the context stream.
 vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double* Ui_out, int* info);
+
+// Lets `kernel` launch with up to `bytes` of dynamic shared memory on the current device.  The
+// limit is a process-wide function attribute, so it is raised once per kernel and device to the
+// opt-in maximum (never lowered) under a lock: threads launching the same kernel with different
+// sizes cannot undo each other's setting.
+cudaError_t allow_dynamic_smem(const void* kernel, size_t bytes);
+
+// Slot `slot` (< 6) of the context's execute scratch, grown to at least `bytes` (contents are
+// not kept across growth); nullptr with *status set on failure.
+void* context_scratch(vb_context* ctx, int slot, size_t bytes, vb_status* status);
 
 // Budgeted device allocation; returns nullptr (and records VB_ERR_BUDGET / VB_ERR_CUDA) on failure.
 void* device_alloc(vb_context* ctx, size_t bytes, vb_status* status);

@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include "device_algebra.cuh"
+#include "internal.h"
 #include "kernels.h"
 #include "pair_value.cuh"
 
@@ -831,7 +832,7 @@ cudaError_t launch_fast(const SpinTableArgs& a, size_t smem, double* tables, cud
     left_string_tables<K><<<a.n_strings, 128, 0, stream>>>(a, tables);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(spin_pairs_fast<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    err = allow_dynamic_smem((const void*)spin_pairs_fast<K>, (int)smem);
     if (err != cudaSuccess) return err;
     int per_sm = 1;
     err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_pairs_fast<K>, kSpinBlock, smem);
@@ -866,7 +867,7 @@ cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work,
     const size_t in_smem_bytes = sizeof(double) * (size_t)np * np + sizeof(int) * 2 * (size_t)np;
     const int in_smem = in_smem_bytes <= 200 * 1024 ? 1 : 0;
     const size_t smem = in_smem ? in_smem_bytes : sizeof(int) * 2 * (size_t)np;
-    cudaError_t err = cudaFuncSetAttribute(factor_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t err = allow_dynamic_smem((const void*)factor_pair_kernel, (int)smem);
     if (err != cudaSuccess) return err;
     factor_pair_kernel<<<1, 512, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, kFactorTolerance, in_smem);
     return cudaGetLastError();
@@ -914,7 +915,7 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream
     auto exact = a.k <= 8 ? spin_pairs_exact<8> : spin_pairs_exact<dev::KMAX>;
     const size_t slot_bytes = sizeof(double) * 64 * (size_t)a.k * a.k;  // two warps
     if (slot_bytes > 48 * 1024) {
-        err = cudaFuncSetAttribute(exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slot_bytes);
+        err = allow_dynamic_smem((const void*)exact, (int)slot_bytes);
         if (err != cudaSuccess) return err;
     }
     exact<<<kSms * 8, 64, slot_bytes, stream>>>(b);

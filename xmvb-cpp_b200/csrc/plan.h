@@ -35,9 +35,8 @@ struct vb_hs_plan {
     DeviceBuffer lf, fwork, fcols, fsigns, fmeta;
     int* meta_host = nullptr;
     int R = 0, r_pos = 0;
-    DeviceBuffer band_h, band_s;
-    long long band_width = 0;
-    DeviceBuffer Zh, Zs, Wh, Ws, Hout, Sout;
+    long long band_width = 0;  // determinant columns per band (bands live in the context scratch)
+    DeviceBuffer Hout, Sout;
     DeviceBuffer str_off, str_det, str_coef;
     // structure incidence by determinant (CSR) and the gradient's adjoint scratch
     DeviceBuffer det_off, det_str, det_coef;

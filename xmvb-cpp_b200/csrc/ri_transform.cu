@@ -383,8 +383,7 @@ vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_
             err = cudaGetLastError();
             const size_t smem = pipelined_smem_bytes(n_bf);
             if (err == cudaSuccess)
-                err = cudaFuncSetAttribute(one_index_pipelined_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
+                err = allow_dynamic_smem((const void*)one_index_pipelined_kernel, (int)smem);
             if (err == cudaSuccess) {
                 const dim3 pgrid((n_bf + kPipeWarps - 1) / kPipeWarps, (n_aux + kAuxTile - 1) / kAuxTile);
                 one_index_pipelined_kernel<<<pgrid, 32 * kPipeWarps, smem, s>>>(dB, n_aux, n_bf, Ct, n_act, dT);
