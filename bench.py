@@ -538,6 +538,50 @@ def run_ri(args):
                                         ctypes.c_void_p(Lp.data_ptr()), ctypes.c_void_p(Kp.data_ptr()))
         if i > 0:
             e2e.append(time.perf_counter() - t0)
+    # split precision (BF16 x 3 on the tensor cores for the one-index step): same inputs, timed the
+    # same way; errors of every output against this run's FP64 result and the oracle rows
+    T64, L64, K64 = T.clone(), L.clone(), K.clone()
+
+    def split_step():
+        st = lib.vb_active_transform_ri_precision(ctx.handle, ctypes.c_void_p(B.data_ptr()), n_aux, n_bf,
+                                                  ctypes.c_void_p(C.data_ptr()), n_act, 1, 1,
+                                                  ctypes.c_void_p(T.data_ptr()), ctypes.c_void_p(L.data_ptr()),
+                                                  ctypes.c_void_p(K.data_ptr()))
+        if st != 0:
+            raise RuntimeError(lib.vb_last_error(ctx.handle))
+
+    for _ in range(args.warmup):
+        split_step()
+    torch.cuda.synchronize()
+    split_times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        split_step()
+        e1.record(stream)
+        e1.synchronize()
+        split_times.append(e0.elapsed_time(e1))
+    split_ms = statistics.mean(split_times)
+
+    def _err(x, ref):
+        a = float((x - ref).abs().max())
+        return {"max_abs": a, "rel": a / float(ref.abs().max())}
+
+    Ls = L.view(P, n_aux).T.cpu().numpy()
+    split = {
+        "scheme": "one-index step: operands rounded to FP32 and split into three BF16 parts, the six products of "
+                  "order <= 2 as mma.sync m16n8k16 BF16 tiles with FP32 accumulation (leading order flushed to FP64 "
+                  "every 4 K steps), FP64 recombination; second index and packing FP64",
+        "ms": split_ms, "speedup_vs_fp64": ms / split_ms,
+        "b_read_gbs": bytes_b / (split_ms * 1e-3) / 1e9,
+        "errors_vs_fp64": {"one_index": _err(T, T64), "L": _err(L, L64), "K": _err(K, K64)},
+        "errors_vs_oracle_L_rows": {"max_abs": float(np.abs(Ls[rows] - Lr).max()),
+                                    "rel": float(np.abs(Ls[rows] - Lr).max() / np.abs(Lr).max())},
+    }
+    T.copy_(T64)
+    L.copy_(L64)
+    K.copy_(K64)
     # metric Cholesky sweep (429 x 429)
     chol = []
     nS = 429
@@ -574,7 +618,7 @@ def run_ri(args):
                      "hbm_gbs": bytes_b / (ms * 1e-3) / 1e9,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured)"},
         "errors_vs_fp64_oracle": {"max_abs": err_abs, "rel": err_rel, "rows_checked": int(len(rows))},
-        "split_precision": None,
+        "split_precision": split,
         "cholesky_429": chol,
         "cpu_baseline": {"value": flops * len(rows) / n_aux / dt_cpu / 1e9, "unit": "GFLOP/s",
                          "cores": os.cpu_count() or 1, "kind": "port",

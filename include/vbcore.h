@@ -333,6 +333,19 @@ vb_status vb_engine_pending(vb_engine* engine, int* queued, int* running, size_t
 vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_aux, int n_bf, const double* C,
                                  int n_act, int mem_space, double* one_index, double* L, double* K_packed);
 
+/* Precision of the one-index step (the flop-carrying GEMM) of the RI transform. */
+enum { VB_PRECISION_FP64 = 0, VB_PRECISION_BF16X3 = 1 };
+
+/* vb_active_transform_ri with a selectable precision for the one-index step (same arguments and
+ * outputs).  VB_PRECISION_BF16X3: each FP64 operand is rounded to FP32 and split into three BF16
+ * parts, the products of order <= 2 run on the tensor cores with FP32 accumulation and an FP64
+ * recombination (relative error of order 1e-7 against FP64; n_bf <= 1536); the second index and
+ * the packing stay FP64.  The reference computes this step in FP64 only
+ * (transform_ri_one_index, src/integrals/ao/ri_transform.cpp:10-37). */
+vb_status vb_active_transform_ri_precision(vb_context* ctx, const double* B_packed, int n_aux, int n_bf,
+                                           const double* C, int n_act, int precision, int mem_space,
+                                           double* one_index, double* L, double* K_packed);
+
 /* Adjoint of the transform: given dE/dL [n_aux x n_act(n_act+1)/2] and the one-index factors
  * of the forward call, dE/dC [n_bf x n_act] (column-major), the orbital pull-back of RI pair
  * factors that the reference's gradients take from ri_one_index_factors

@@ -80,6 +80,37 @@ def test_full_size_precision_workload(ctx):
     assert np.array_equal(L2, 2.0 * L)
 
 
+# Split precision: the one-index step as three-way BF16 splits on the tensor cores with FP32
+# accumulation and FP64 recombination.  Bar: 1e-6 relative to the largest element for the
+# one-index factors and L, 2e-6 for K = L^T L (FP32-level: each operand keeps about 24 bits).
+SPLIT_REL = 1e-6
+
+
+@pytest.mark.parametrize("n_aux,n_bf,n_act", [(1, 1, 1), (10, 7, 3), (37, 20, 6), (129, 50, 1), (130, 33, 16),
+                                              (300, 64, 16), (257, 300, 8)])
+def test_split_precision_transform(ctx, n_aux, n_bf, n_act):
+    B, C = _inputs(n_aux, n_bf, n_act, 3 * n_aux + n_bf + n_act)
+    L, K, T = vbcore.active_transform_ri(ctx, B, C, one_index=True, precision="bf16x3")
+    Lr, Kr = O.ri_transform(B, C)
+    assert _rel(L, Lr) < SPLIT_REL
+    assert _rel(K, Kr) < 2 * SPLIT_REL
+    if n_aux * n_bf * n_bf <= 300 * 64 * 64:
+        assert _rel(T, O.ri_one_index(B, C)) < SPLIT_REL
+    # and agrees with the FP64 path to the same bar
+    L64, _, _ = vbcore.active_transform_ri(ctx, B, C)
+    assert _rel(L, L64) < SPLIT_REL
+
+
+def test_split_precision_full_size(ctx):
+    n_aux, n_bf, n_act = 1600, 400, 16
+    B, C = _inputs(n_aux, n_bf, n_act, 20261203, decay=20.0)
+    L64, K64, T64 = vbcore.active_transform_ri(ctx, B, C, one_index=True)
+    L, K, T = vbcore.active_transform_ri(ctx, B, C, one_index=True, precision="bf16x3")
+    assert _rel(T, T64) < SPLIT_REL
+    assert _rel(L, L64) < SPLIT_REL
+    assert _rel(K, K64) < 2 * SPLIT_REL
+
+
 def test_rejects_too_many_active_orbitals(ctx):
     B, C = _inputs(4, 20, 17, 1)
     with pytest.raises(vbcore.VbError) as e:

@@ -15,6 +15,20 @@
 // (128 per warp) and accumulate T[a, P, mu] for all n_act orbitals in registers (64 FP64
 // accumulators per lane), streaming the AO-pair columns pair(mu, nu) of B (1 KB coalesced per
 // column) against rows of C.  Each packed column is needed by two AO indices (mu and nu).
+//
+// Split precision (VB_PRECISION_BF16X3): the one-index step on the tensor cores.  Every operand
+// x (FP64, rounded to FP32) is split into three BF16 parts x = x0 + x1 + x2 (about 24 mantissa
+// bits); the products of order <= 2 (a0 c0; a0 c1 + a1 c0; a0 c2 + a1 c1 + a2 c0) run as BF16
+// mma.sync m16n8k16 tiles with FP32 accumulation, the leading order in its own accumulator that
+// is flushed into FP64 every few K steps, the recombination in FP64 (compensated).  A warp owns
+// 16 auxiliary rows of one AO index mu (one M tile; the two N tiles cover 16 active orbitals)
+// and streams K = nu in steps of 16 straight from the packed columns (each column read is one
+// aligned 128-byte line of 16 rows), one step prefetched in registers; the coefficient
+// fragments (three splits, fragment order) are built once and staged in shared memory.  The
+// kernel reads B once per (mu, nu) use like the FP64 kernel; with mu fastest in the grid, the
+// second use of a packed column is normally an L2 hit.  The second index and the packing stay
+// FP64.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -206,6 +220,259 @@ __global__ void __launch_bounds__(32 * kPipeWarps, 2) one_index_pipelined_kernel
     }
 }
 
+constexpr int kSplitWarps = 8;   // AO indices per CTA
+constexpr int kSplitRows = 16;   // auxiliary rows per warp (one M tile)
+constexpr int kSplitFlush = 4;   // K steps between flushes of the leading-order FP32 accumulator
+constexpr int kSplitMaxSteps = 96;  // shared-memory coefficient fragments: n_bf <= 1536
+
+__device__ __forceinline__ uint32_t bf16x2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
+
+// Two FP32 values (x0: lower column / K index) as three BF16x2 words, x = w0 + w1 + w2.
+__device__ __forceinline__ void split3(float x0, float x1, uint32_t& w0, uint32_t& w1, uint32_t& w2) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    const float r0 = x0 - __low2float(h), r1 = x1 - __high2float(h);
+    const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+    const float s0 = r0 - __low2float(m), s1 = r1 - __high2float(m);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(s0, s1);
+    w0 = bf16x2_bits(h);
+    w1 = bf16x2_bits(m);
+    w2 = bf16x2_bits(l);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Coefficient fragments for the m16n8k16 B operand: entry (step s, lane) holds, per split z,
+// uint4 {b0 (N tile 0), b1 (N tile 0), b0 (N tile 1), b1 (N tile 1)} with
+// b0 = C(16 s + 2 q + {0, 1}, a), b1 = C(16 s + 2 q + 8 + {0, 1}, a), a = 8 j + g (g = lane / 4,
+// q = lane % 4); zero beyond n_bf and n_act.
+__global__ void split_coefficients_kernel(const double* __restrict__ C, int n_bf, int n_act, int n_steps,
+                                          uint4* __restrict__ Cf) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_steps * 32) return;
+    const int st = e >> 5, lane = e & 31, g = lane >> 2, q = lane & 3;
+    uint32_t w[3][2][2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int a = 8 * j + g;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int nu = 16 * st + 2 * q + 8 * r;
+            const float c0 = (a < n_act && nu < n_bf) ? (float)C[nu + (long long)a * n_bf] : 0.0f;
+            const float c1 = (a < n_act && nu + 1 < n_bf) ? (float)C[nu + 1 + (long long)a * n_bf] : 0.0f;
+            split3(c0, c1, w[0][j][r], w[1][j][r], w[2][j][r]);
+        }
+    }
+#pragma unroll
+    for (int z = 0; z < 3; ++z) Cf[(size_t)e * 3 + z] = make_uint4(w[z][0][0], w[z][0][1], w[z][1][0], w[z][1][1]);
+}
+
+// T[a, P, mu] = sum_nu B[P, pair(mu, nu)] C(nu, a) by split-BF16 tensor-core tiles.
+// grid.x = groups of kSplitWarps AO indices (fastest), grid.y = tiles of 16 auxiliary rows.
+__global__ void __launch_bounds__(32 * kSplitWarps, 2) one_index_split_kernel(const double* __restrict__ B, int n_aux,
+                                                                              int n_bf, int n_steps,
+                                                                              const uint4* __restrict__ Cf, int n_act,
+                                                                              double* __restrict__ T) {
+    extern __shared__ uint4 sCf[];  // [n_steps][32][3]
+    for (int e = threadIdx.x; e < n_steps * 32 * 3; e += blockDim.x) sCf[e] = __ldg(Cf + e);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mu = blockIdx.x * kSplitWarps + warp;
+    if (mu >= n_bf) return;  // no CTA barrier below
+    const int g = lane >> 2, q = lane & 3;
+    const int P0 = blockIdx.y * kSplitRows;
+    const int row0 = P0 + g, row1 = P0 + g + 8;
+    const bool ok0 = row0 < n_aux, ok1 = row1 < n_aux;
+    // x[2 ci + h]: column ci of {2q, 2q + 1, 2q + 8, 2q + 9}, row h of {g, g + 8}
+    auto load = [&](int st, double(&x)[8]) {
+#pragma unroll
+        for (int ci = 0; ci < 4; ++ci) {
+            const int nu = 16 * st + 2 * q + (ci & 1) + 8 * (ci >> 1);
+            const bool nok = nu < n_bf;
+            const double* col = B + ao_pair(mu, nok ? nu : 0) * n_aux;
+            x[2 * ci] = (nok && ok0) ? __ldg(col + row0) : 0.0;
+            x[2 * ci + 1] = (nok && ok1) ? __ldg(col + row1) : 0.0;
+        }
+    };
+    float acc0[2][4], acc12[2][4];
+    double accd[2][4];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            acc0[j][i] = 0.0f;
+            acc12[j][i] = 0.0f;
+            accd[j][i] = 0.0;
+        }
+    auto step = [&](int st, const double(&x)[8]) {
+        // A fragments: reg0 (g, 2q..2q+1), reg1 (g+8, 2q..), reg2 (g, 2q+8..), reg3 (g+8, 2q+8..)
+        uint32_t A0[4], A1[4], A2[4];
+        split3((float)x[0], (float)x[2], A0[0], A1[0], A2[0]);
+        split3((float)x[1], (float)x[3], A0[1], A1[1], A2[1]);
+        split3((float)x[4], (float)x[6], A0[2], A1[2], A2[2]);
+        split3((float)x[5], (float)x[7], A0[3], A1[3], A2[3]);
+        const uint4* cf = sCf + ((size_t)st * 32 + lane) * 3;
+        const uint4 c0 = cf[0], c1 = cf[1], c2 = cf[2];
+        mma_bf16(acc0[0], A0, c0.x, c0.y);
+        mma_bf16(acc0[1], A0, c0.z, c0.w);
+        mma_bf16(acc12[0], A0, c1.x, c1.y);
+        mma_bf16(acc12[1], A0, c1.z, c1.w);
+        mma_bf16(acc12[0], A1, c0.x, c0.y);
+        mma_bf16(acc12[1], A1, c0.z, c0.w);
+        mma_bf16(acc12[0], A0, c2.x, c2.y);
+        mma_bf16(acc12[1], A0, c2.z, c2.w);
+        mma_bf16(acc12[0], A1, c1.x, c1.y);
+        mma_bf16(acc12[1], A1, c1.z, c1.w);
+        mma_bf16(acc12[0], A2, c0.x, c0.y);
+        mma_bf16(acc12[1], A2, c0.z, c0.w);
+        if ((st + 1) % kSplitFlush == 0) {
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    accd[j][i] += (double)acc0[j][i];
+                    acc0[j][i] = 0.0f;
+                }
+        }
+    };
+    double xa[8], xb[8];
+    load(0, xa);
+    for (int st = 0; st < n_steps; st += 2) {
+        if (st + 1 < n_steps) load(st + 1, xb);
+        step(st, xa);
+        if (st + 2 < n_steps) load(st + 2, xa);
+        if (st + 1 < n_steps) step(st + 1, xb);
+    }
+    const long long ld = (long long)n_act * n_aux;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int P = (i < 2) ? row0 : row1;
+            const int a = 8 * j + 2 * q + (i & 1);
+            if (P < n_aux && a < n_act)
+                T[(long long)a * n_aux + P + (long long)mu * ld] = accd[j][i] + (double)acc0[j][i] + (double)acc12[j][i];
+        }
+}
+
+// Pipelined split kernel (even n_aux, 16-byte aligned B): each warp streams its 16 x 16 tiles
+// of B through a private kSplitStages-deep cp.async ring in shared memory.  A tile is stored
+// column by column (16 rows = eight 16-byte chunks); chunk j of column c sits at chunk
+// position j ^ (c & 7), so the 8-byte fragment reads of a quarter warp hit distinct banks.
+constexpr int kSplitStages = 4;
+
+size_t split_pipelined_smem_bytes(int n_steps) {
+    return sizeof(uint4) * (size_t)n_steps * 32 * 3 + sizeof(double) * (size_t)kSplitWarps * kSplitStages * 256;
+}
+
+__global__ void __launch_bounds__(32 * kSplitWarps, 2) one_index_split_pipelined_kernel(
+    const double* __restrict__ B, int n_aux, int n_bf, int n_steps, const uint4* __restrict__ Cf, int n_act,
+    double* __restrict__ T) {
+    extern __shared__ uint4 sCf[];  // [n_steps][32][3], then the rings
+    for (int e = threadIdx.x; e < n_steps * 32 * 3; e += blockDim.x) sCf[e] = __ldg(Cf + e);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mu = blockIdx.x * kSplitWarps + warp;
+    if (mu >= n_bf) return;  // warp-private pipeline below: no CTA-wide barrier after this point
+    double* ring = reinterpret_cast<double*>(sCf + (size_t)n_steps * 32 * 3) + (size_t)warp * kSplitStages * 256;
+    const int g = lane >> 2, q = lane & 3;
+    const int P0 = blockIdx.y * kSplitRows;
+    // copy side: this lane moves chunk jc (rows 2 jc, 2 jc + 1) of columns cc + 4 t
+    const int jc = lane & 7, cc = lane >> 3;
+    const bool row_ok = P0 + 2 * jc < n_aux;
+    const double* bsrc = B + P0 + 2 * jc;
+    const int mu_tri = mu * (mu + 1) / 2;
+    auto issue = [&](int st) {
+        if (st < n_steps) {
+            double* tile = ring + (st % kSplitStages) * 256;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int c = cc + 4 * t;
+                const int nu = 16 * st + c;
+                const bool ok = row_ok && nu < n_bf;
+                const int pair = nu <= mu ? mu_tri + nu : nu * (nu + 1) / 2 + mu;
+                const double* src = ok ? bsrc + (long long)pair * n_aux : B;
+                cp_async16(tile + c * 16 + 2 * (jc ^ (c & 7)), src, ok ? 16 : 0);
+            }
+        }
+        cp_async_commit();  // empty groups keep the group count uniform
+    };
+    // read side: fragment rows g and g + 8 are auxiliary rows 2g and 2g + 1 (one 16-byte chunk,
+    // chunk g of a column); fragment columns 2q, 2q + 1, 2q + 8, 2q + 9 are nu offsets
+    int roff[4];
+#pragma unroll
+    for (int ci = 0; ci < 4; ++ci) {
+        const int c = 2 * q + (ci & 1) + 8 * (ci >> 1);
+        roff[ci] = c * 16 + 2 * (g ^ (c & 7));
+    }
+#pragma unroll
+    for (int st = 0; st < kSplitStages - 1; ++st) issue(st);
+    float acc0[2][4], acc12[2][4];
+    double accd[2][4];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            acc0[j][i] = 0.0f;
+            acc12[j][i] = 0.0f;
+            accd[j][i] = 0.0;
+        }
+    for (int st = 0; st < n_steps; ++st) {
+        issue(st + kSplitStages - 1);
+        cp_async_wait<kSplitStages - 1>();
+        __syncwarp();
+        const double* tile = ring + (st % kSplitStages) * 256;
+        double2 v[4];  // v[ci] = (aux row 2g, aux row 2g + 1) of fragment column ci
+#pragma unroll
+        for (int ci = 0; ci < 4; ++ci) v[ci] = *reinterpret_cast<const double2*>(tile + roff[ci]);
+        __syncwarp();  // the stage may be refilled by the next issue
+        uint32_t A0[4], A1[4], A2[4];
+        split3((float)v[0].x, (float)v[1].x, A0[0], A1[0], A2[0]);
+        split3((float)v[0].y, (float)v[1].y, A0[1], A1[1], A2[1]);
+        split3((float)v[2].x, (float)v[3].x, A0[2], A1[2], A2[2]);
+        split3((float)v[2].y, (float)v[3].y, A0[3], A1[3], A2[3]);
+        const uint4* cf = sCf + ((size_t)st * 32 + lane) * 3;
+        const uint4 c0 = cf[0], c1 = cf[1], c2 = cf[2];
+        mma_bf16(acc0[0], A0, c0.x, c0.y);
+        mma_bf16(acc0[1], A0, c0.z, c0.w);
+        mma_bf16(acc12[0], A0, c1.x, c1.y);
+        mma_bf16(acc12[1], A0, c1.z, c1.w);
+        mma_bf16(acc12[0], A1, c0.x, c0.y);
+        mma_bf16(acc12[1], A1, c0.z, c0.w);
+        mma_bf16(acc12[0], A0, c2.x, c2.y);
+        mma_bf16(acc12[1], A0, c2.z, c2.w);
+        mma_bf16(acc12[0], A1, c1.x, c1.y);
+        mma_bf16(acc12[1], A1, c1.z, c1.w);
+        mma_bf16(acc12[0], A2, c0.x, c0.y);
+        mma_bf16(acc12[1], A2, c0.z, c0.w);
+        if ((st + 1) % kSplitFlush == 0) {
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    accd[j][i] += (double)acc0[j][i];
+                    acc0[j][i] = 0.0f;
+                }
+        }
+    }
+    cp_async_wait<0>();
+    const long long ld = (long long)n_act * n_aux;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int P = P0 + 2 * g + ((i < 2) ? 0 : 1);
+            const int a = 8 * j + 2 * q + (i & 1);
+            if (P < n_aux && a < n_act)
+                T[(long long)a * n_aux + P + (long long)mu * ld] = accd[j][i] + (double)acc0[j][i] + (double)acc12[j][i];
+        }
+}
+
 // L[P, pair(a, b)] = sum_mu T[a, P, mu] C(mu, b) for b <= a.  CTA = (32 auxiliary rows, one
 // orbital a); its four warps split the mu range (lane = auxiliary row, 16 accumulators for b)
 // and reduce through shared memory.
@@ -335,7 +602,20 @@ extern "C" {
 
 vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_aux, int n_bf, const double* C,
                                  int n_act, int mem_space, double* one_index, double* L, double* K_packed) {
+    return vb_active_transform_ri_precision(ctx, B_packed, n_aux, n_bf, C, n_act, VB_PRECISION_FP64, mem_space,
+                                            one_index, L, K_packed);
+}
+
+vb_status vb_active_transform_ri_precision(vb_context* ctx, const double* B_packed, int n_aux, int n_bf,
+                                           const double* C, int n_act, int precision, int mem_space,
+                                           double* one_index, double* L, double* K_packed) {
     if (!ctx) return VB_ERR_INVALID;
+    if (precision != VB_PRECISION_FP64 && precision != VB_PRECISION_BF16X3)
+        return set_error(ctx, VB_ERR_INVALID, "vb_active_transform_ri: unknown precision");
+    const bool split = precision == VB_PRECISION_BF16X3;
+    const int split_steps = (n_bf + 15) / 16;
+    if (split && split_steps > kSplitMaxSteps)
+        return set_error(ctx, VB_ERR_UNSUPPORTED, "vb_active_transform_ri: split precision supports n_bf <= 1536");
     if (n_aux < 1 || n_bf < 1 || n_act < 1 || !B_packed || !C || !L)
         return set_error(ctx, VB_ERR_INVALID, "vb_active_transform_ri: dimensions must be positive, B, C and L non-null");
     if (n_act > kMaxActive)
@@ -358,9 +638,10 @@ vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_
     };
     const size_t oB = take(bB, host), oC = take(bC, host), oT = take(bT, host || !one_index);
     const size_t oL = take(bL, host), oK = take(bK, host && K_packed);
-    const bool pipelined = n_aux % 2 == 0 && n_bf <= kPipelinedMaxBf &&
+    const bool pipelined = !split && n_aux % 2 == 0 && n_bf <= kPipelinedMaxBf &&
                            (host || reinterpret_cast<uintptr_t>(B_packed) % 16 == 0);
     const size_t oCt = take(sizeof(double) * (size_t)n_bf * kMaxActive, pipelined);
+    const size_t oCf = take(sizeof(uint4) * (size_t)split_steps * 32 * 3, split);
     DeviceBuffer ws;
     vb_status st = ws.allocate(ctx, off);
     if (st != VB_OK) return st;
@@ -377,7 +658,30 @@ vb_status vb_active_transform_ri(vb_context* ctx, const double* B_packed, int n_
     }
     if (err == cudaSuccess) {
         const dim3 grid((n_bf + kWarpsPerCta - 1) / kWarpsPerCta, (n_aux + kAuxTile - 1) / kAuxTile);
-        if (pipelined) {
+        if (split) {
+            uint4* Cf = reinterpret_cast<uint4*>(base + oCf);
+            split_coefficients_kernel<<<(split_steps * 32 + 127) / 128, 128, 0, s>>>(dC, n_bf, n_act, split_steps, Cf);
+            err = cudaGetLastError();
+            const dim3 sgrid((n_bf + kSplitWarps - 1) / kSplitWarps, (n_aux + kSplitRows - 1) / kSplitRows);
+            const bool ring = n_aux % 2 == 0 && (host || reinterpret_cast<uintptr_t>(B_packed) % 16 == 0);
+            if (ring) {
+                const size_t smem = split_pipelined_smem_bytes(split_steps);
+                if (err == cudaSuccess) err = allow_dynamic_smem((const void*)one_index_split_pipelined_kernel, smem);
+                if (err == cudaSuccess) {
+                    one_index_split_pipelined_kernel<<<sgrid, 32 * kSplitWarps, smem, s>>>(dB, n_aux, n_bf, split_steps,
+                                                                                          Cf, n_act, dT);
+                    err = cudaGetLastError();
+                }
+            } else {
+                const size_t smem = sizeof(uint4) * (size_t)split_steps * 32 * 3;
+                if (err == cudaSuccess) err = allow_dynamic_smem((const void*)one_index_split_kernel, smem);
+                if (err == cudaSuccess) {
+                    one_index_split_kernel<<<sgrid, 32 * kSplitWarps, smem, s>>>(dB, n_aux, n_bf, split_steps, Cf,
+                                                                                n_act, dT);
+                    err = cudaGetLastError();
+                }
+            }
+        } else if (pipelined) {
             double* Ct = reinterpret_cast<double*>(base + oCt);
             transpose_coefficients_kernel<<<(n_bf * kMaxActive + 255) / 256, 256, 0, s>>>(dC, n_bf, n_act, Ct);
             err = cudaGetLastError();

@@ -86,7 +86,8 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_destroy", "vb_hs_plan_execute", "vb_hs_plan_stats", "vb_resolve_overlaps", "vb_same_spin_pairs",
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
     "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
-    "vb_active_transform_ri", "vb_active_transform_ri_adjoint", "vb_hs_plan_gradient",
+    "vb_active_transform_ri", "vb_active_transform_ri_precision", "vb_active_transform_ri_adjoint",
+    "vb_hs_plan_gradient",
     "vb_lowest_root", "vb_engine_create", "vb_engine_destroy", "vb_engine_last_error", "vb_engine_add_instance",
     "vb_engine_evaluate_instances", "vb_engine_submit_scf", "vb_engine_poll", "vb_engine_pending",
     "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
@@ -151,6 +152,7 @@ def load_library(path: str = LIB_PATH):
     lib.vb_solve_scf.argtypes = [P, P, c.POINTER(_ScfOptions), c.POINTER(_ScfResult), P]
     lib.vb_hs_plan_gradient.argtypes = [P, P, P, P, c.c_int, P, c.c_double, P, P, P, P, c.c_int, P]
     lib.vb_active_transform_ri.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, P, P, P]
+    lib.vb_active_transform_ri_precision.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, c.c_int, P, P, P]
     lib.vb_active_transform_ri_adjoint.argtypes = [P, P, P, c.c_int, c.c_int, c.c_int, c.c_int, P]
     lib.vb_same_spin_pairs.argtypes = [P, c.c_int, c.c_int, c.c_int64, P, P, P, P, P, c.c_int, P, P]
     for name in EXPORTED_SYMBOLS:
@@ -417,10 +419,14 @@ def generalized_eigh_batched(ctx: "Context", problems, device=None):
     return out
 
 
-def active_transform_ri(ctx: "Context", B_packed, C, one_index: bool = False):
+PRECISIONS = {"fp64": 0, "bf16x3": 1}
+
+
+def active_transform_ri(ctx: "Context", B_packed, C, one_index: bool = False, precision: str = "fp64"):
     """RI AO -> active transform (transform_ri_active_integrals of the reference), host arrays:
     B_packed [n_aux, n_bf(n_bf+1)/2], C [n_bf, n_act] -> (L [n_aux, P], K packed, T or None)
-    with T [(n_act n_aux), n_bf] the one-index factors (row a*n_aux + P)."""
+    with T [(n_act n_aux), n_bf] the one-index factors (row a*n_aux + P).  precision "bf16x3"
+    runs the one-index step as split-BF16 tensor-core products (about 1e-7 relative)."""
     B = np.asarray(B_packed, dtype=np.float64)
     C = np.asarray(C, dtype=np.float64)
     n_aux = B.shape[0]
@@ -431,8 +437,9 @@ def active_transform_ri(ctx: "Context", B_packed, C, one_index: bool = False):
     L = np.empty(n_aux * P, dtype=np.float64)
     K = np.empty(P * (P + 1) // 2, dtype=np.float64)
     T = np.empty(n_act * n_aux * n_bf, dtype=np.float64) if one_index else None
-    st = load_library().vb_active_transform_ri(ctx.handle, _ptr(Bf), n_aux, n_bf, _ptr(Cf), n_act, VB_MEM_HOST,
-                                               _ptr(T) if one_index else None, _ptr(L), _ptr(K))
+    st = load_library().vb_active_transform_ri_precision(ctx.handle, _ptr(Bf), n_aux, n_bf, _ptr(Cf), n_act,
+                                                         PRECISIONS[precision], VB_MEM_HOST,
+                                                         _ptr(T) if one_index else None, _ptr(L), _ptr(K))
     _check(st, ctx.handle)
     Lm = L.reshape(P, n_aux).T.copy()
     Tm = T.reshape(n_bf, n_act * n_aux).T.copy() if one_index else None
