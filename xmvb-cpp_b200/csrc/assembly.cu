@@ -19,17 +19,21 @@ namespace {
 
 constexpr int kPad = kBandReduceColumns + 1;
 
-// One CTA per 32 band columns; every row of the band streams through once.  Warp w owns the
-// structures bucketed to it (local structure index = w mod warps), so each shared-memory
-// accumulator has exactly one writer and the sum order is fixed.  A warp walks its
-// (determinant, structure, coefficient) triples, sorted by determinant, 32 at a time: lane j
-// fetches triple j, then the warp broadcasts them one by one; the band loads of consecutive
-// triples are independent, which keeps many loads in flight.
+// One CTA per (32 band columns, structure chunk of at most 64 structures): every chunk's
+// triples stream the band rows they need, and the small per-chunk accumulators let several
+// CTAs share an SM.  Warp w owns the chunk's structures bucketed to it (local structure index
+// = w mod warps), so each shared-memory accumulator has exactly one writer and the sum order is
+// fixed.  A warp walks its (determinant, structure, coefficient) triples, sorted by
+// determinant, 32 at a time: lane j fetches triple j, then the warp broadcasts them one by one;
+// the band loads of consecutive triples are independent, which keeps many loads in flight.
 __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(BandReduceArgs a) {
     extern __shared__ double zsm[];
+    const int chunk = blockIdx.y;
+    const int struct_begin = __ldg(a.chunk_begin + chunk), struct_count = __ldg(a.chunk_count + chunk);
+    const long long* wbegin = a.wbegin + (size_t)chunk * (kBandReduceWarps + 1);
     double* zh = zsm;
-    double* zs = zsm + (size_t)a.struct_count * kPad;
-    for (int i = threadIdx.x; i < a.struct_count * kPad; i += blockDim.x) {
+    double* zs = zsm + (size_t)struct_count * kPad;
+    for (int i = threadIdx.x; i < struct_count * kPad; i += blockDim.x) {
         zh[i] = 0.0;
         zs[i] = 0.0;
     }
@@ -40,7 +44,7 @@ __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(Band
     const long long e = a.e0 + j;
     long long row_end = a.e0 + (long long)blockIdx.x * kBandReduceColumns + kBandReduceColumns;
     if (row_end > a.e0 + a.width) row_end = a.e0 + a.width;
-    const long long t_begin = a.wbegin[warp], t_end = a.wbegin[warp + 1];
+    const long long t_begin = wbegin[warp], t_end = wbegin[warp + 1];
     for (long long base = t_begin; base < t_end; base += 32) {
         const long long mine = base + lane;
         int d_l = 0x7fffffff, I_l = 0;
@@ -80,12 +84,12 @@ __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(Band
     }
     __syncthreads();
     const long long col0 = a.e0 + (long long)blockIdx.x * kBandReduceColumns;
-    for (int i = threadIdx.x; i < a.struct_count * kBandReduceColumns; i += blockDim.x) {
-        const int I = i % a.struct_count, l = i / a.struct_count;
+    for (int i = threadIdx.x; i < struct_count * kBandReduceColumns; i += blockDim.x) {
+        const int I = i % struct_count, l = i / struct_count;
         if ((long long)blockIdx.x * kBandReduceColumns + l >= a.width) continue;
         const long long col = col0 + l;
-        a.Zh[col * a.n_str + a.struct_begin + I] = zh[I * kPad + l];
-        a.Zs[col * a.n_str + a.struct_begin + I] = zs[I * kPad + l];
+        a.Zh[col * a.n_str + struct_begin + I] = zh[I * kPad + l];
+        a.Zs[col * a.n_str + struct_begin + I] = zs[I * kPad + l];
     }
 }
 
@@ -121,14 +125,15 @@ __global__ void symmetrize_kernel(int n, const double* __restrict__ Wh, const do
 
 size_t band_reduce_smem_bytes(int struct_count) { return sizeof(double) * 2 * (size_t)struct_count * kPad; }
 
-int band_reduce_max_structures() { return (int)((227 * 1024) / (sizeof(double) * 2 * kPad)) / 8 * 8; }
+// 64 structures per chunk: 33.8 KB of accumulators, six CTAs per SM.
+int band_reduce_max_structures() { return 64; }
 
 cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches) {
-    const size_t smem = band_reduce_smem_bytes(a.struct_count);
+    const size_t smem = band_reduce_smem_bytes(a.max_count);
     cudaError_t err = allow_dynamic_smem((const void*)band_reduce_kernel, (int)smem);
     if (err != cudaSuccess) return err;
     const long long blocks = (a.width + kBandReduceColumns - 1) / kBandReduceColumns;
-    band_reduce_kernel<<<(unsigned)blocks, kBandReduceWarps * 32, smem, stream>>>(a);
+    band_reduce_kernel<<<dim3((unsigned)blocks, (unsigned)a.n_chunks), kBandReduceWarps * 32, smem, stream>>>(a);
     ++*launches;
     return cudaGetLastError();
 }

@@ -296,36 +296,46 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
         return fail(st);
 
     // per structure chunk and warp bucket ((structure - begin) mod warps): triples
-    // (determinant, local structure, coefficient) sorted by determinant
-    const int max_chunk = band_reduce_max_structures();
-    for (int begin = 0; begin < p->n_str; begin += max_chunk) {
-        StructureChunk ch;
-        ch.begin = begin;
-        ch.count = std::min(max_chunk, p->n_str - begin);
-        std::vector<long long> wbegin(kBandReduceWarps + 1, 0);
+    // (determinant, local structure, coefficient) sorted by determinant, concatenated over chunks
+    {
+        const int max_chunk = band_reduce_max_structures();
+        std::vector<int> cbegin, ccount;
+        std::vector<long long> wbegin;
         std::vector<int> wdet, wstruct;
         std::vector<double> wcoef;
-        for (int w = 0; w < kBandReduceWarps; ++w) {
-            wbegin[w] = (long long)wdet.size();
-            for (long long d = 0; d < p->n_det; ++d)
-                for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t) {
-                    const int I = ex->term_structure[t];
-                    if (I >= begin && I < begin + ch.count && (I - begin) % kBandReduceWarps == w) {
-                        wdet.push_back((int)d);
-                        wstruct.push_back(I - begin);
-                        wcoef.push_back(ex->term_coefficient[t]);
+        for (int begin = 0; begin < p->n_str; begin += max_chunk) {
+            const int count = std::min(max_chunk, p->n_str - begin);
+            cbegin.push_back(begin);
+            ccount.push_back(count);
+            for (int w = 0; w < kBandReduceWarps; ++w) {
+                wbegin.push_back((long long)wdet.size());
+                for (long long d = 0; d < p->n_det; ++d)
+                    for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t) {
+                        const int I = ex->term_structure[t];
+                        if (I >= begin && I < begin + count && (I - begin) % kBandReduceWarps == w) {
+                            wdet.push_back((int)d);
+                            wstruct.push_back(I - begin);
+                            wcoef.push_back(ex->term_coefficient[t]);
+                        }
                     }
-                }
+            }
+            wbegin.push_back((long long)wdet.size());
+            p->chunks.max_count = std::max(p->chunks.max_count, count);
         }
-        wbegin[kBandReduceWarps] = (long long)wdet.size();
-        if ((st = upload(ctx, ch.wbegin, wbegin.data(), sizeof(long long) * wbegin.size())) != VB_OK) return fail(st);
-        if ((st = upload(ctx, ch.wdet, wdet.data(), sizeof(int) * std::max<size_t>(1, wdet.size()))) != VB_OK)
+        p->chunks.n = (int)cbegin.size();
+        StructureChunks& c = p->chunks;
+        if ((st = upload(ctx, c.begin, cbegin.data(), sizeof(int) * std::max<size_t>(1, cbegin.size()))) != VB_OK)
             return fail(st);
-        if ((st = upload(ctx, ch.wstruct, wstruct.data(), sizeof(int) * std::max<size_t>(1, wstruct.size()))) != VB_OK)
+        if ((st = upload(ctx, c.count, ccount.data(), sizeof(int) * std::max<size_t>(1, ccount.size()))) != VB_OK)
             return fail(st);
-        if ((st = upload(ctx, ch.wcoef, wcoef.data(), sizeof(double) * std::max<size_t>(1, wcoef.size()))) != VB_OK)
+        if ((st = upload(ctx, c.wbegin, wbegin.data(), sizeof(long long) * std::max<size_t>(1, wbegin.size()))) != VB_OK)
             return fail(st);
-        p->chunks.push_back(std::move(ch));
+        if ((st = upload(ctx, c.wdet, wdet.data(), sizeof(int) * std::max<size_t>(1, wdet.size()))) != VB_OK)
+            return fail(st);
+        if ((st = upload(ctx, c.wstruct, wstruct.data(), sizeof(int) * std::max<size_t>(1, wstruct.size()))) != VB_OK)
+            return fail(st);
+        if ((st = upload(ctx, c.wcoef, wcoef.data(), sizeof(double) * std::max<size_t>(1, wcoef.size()))) != VB_OK)
+            return fail(st);
     }
     cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
     if (e2 != cudaSuccess) return fail(cuda_error(ctx, e2, "plan upload"));
@@ -512,7 +522,7 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
         if (err != cudaSuccess) return cuda_error(ctx, err, "full_pairs");
         pairs.close();
         PhaseMark reduce(p, VB_PHASE_BAND_REDUCE);
-        for (const StructureChunk& ch : p->chunks) {
+        {
             BandReduceArgs ba{};
             ba.n_det = p->n_det;
             ba.n_str = p->n_str;
@@ -520,12 +530,14 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
             ba.width = B;
             ba.Hb = fa.Hb;
             ba.Sb = fa.Sb;
-            ba.wbegin = ch.wbegin.as<long long>();
-            ba.wdet = ch.wdet.as<int>();
-            ba.wstruct = ch.wstruct.as<int>();
-            ba.wcoef = ch.wcoef.as<double>();
-            ba.struct_begin = ch.begin;
-            ba.struct_count = ch.count;
+            ba.n_chunks = p->chunks.n;
+            ba.max_count = p->chunks.max_count;
+            ba.chunk_begin = p->chunks.begin.as<int>();
+            ba.chunk_count = p->chunks.count.as<int>();
+            ba.wbegin = p->chunks.wbegin.as<long long>();
+            ba.wdet = p->chunks.wdet.as<int>();
+            ba.wstruct = p->chunks.wstruct.as<int>();
+            ba.wcoef = p->chunks.wcoef.as<double>();
             ba.Zh = scr[2];
             ba.Zs = scr[3];
             err = launch_band_reduce(ba, s, &launches);

@@ -63,11 +63,16 @@ struct BandReduceArgs {
     long long e0, width;      // band columns
     const double* Hb;
     const double* Sb;
-    const long long* wbegin;  // per warp bucket: triple range [wbegin[w], wbegin[w + 1])
-    const int* wdet;          // triples sorted by determinant: (determinant, local structure, coef)
+    // structure chunks (grid.y): chunk c covers structures [chunk_begin[c], + chunk_count[c]);
+    // its warp w owns the triples [wbegin[c (W + 1) + w], wbegin[c (W + 1) + w + 1]) of the
+    // concatenated lists, sorted by determinant: (determinant, local structure, coefficient)
+    int n_chunks, max_count;
+    const int* chunk_begin;
+    const int* chunk_count;
+    const long long* wbegin;
+    const int* wdet;
     const int* wstruct;
     const double* wcoef;
-    int struct_begin, struct_count;
     double* Zh;  // n_str x n_det column-major: Z[e * n_str + I]
     double* Zs;
 };

@@ -11,9 +11,10 @@
 
 using namespace vbcore;
 
-struct StructureChunk {
-    int begin = 0, count = 0;
-    DeviceBuffer wbegin, wdet, wstruct, wcoef;
+// Structure chunks of the band reduction, all in one launch (see BandReduceArgs).
+struct StructureChunks {
+    int n = 0, max_count = 0;
+    DeviceBuffer begin, count, wbegin, wdet, wstruct, wcoef;
 };
 
 struct vb_hs_plan {
@@ -44,7 +45,7 @@ struct vb_hs_plan {
     // host inputs of the last host-pointer evaluation whose records are still resident
     std::vector<double> last_inputs;
     bool records_current = false;
-    std::vector<StructureChunk> chunks;
+    StructureChunks chunks;
     // spin-flip map of the determinant list (folds the determinant-pair work in half)
     DeviceBuffer flip;
     bool has_flip = false;
