@@ -682,16 +682,11 @@ def run_batch(args):
     plans = {n: vbcore.HsPlan(ctx, exps[n], n) for n in set(sizes)}
 
     def plain_pass():
+        # the same per-instance work as an engine worker (H and S device-resident, root, gradient)
         energies = []
         for i, n in enumerate(sizes):
             S, h, eri, F = data[i]
-            Hs, Ss = plans[n].execute(S, h, eri)
-            if Hs.shape[0] <= 200:
-                w, C = vbcore.generalized_eigh(ctx, Hs, Ss)
-                lam, c = w[0], C[:, 0]
-            else:
-                lam, c, _ = vbcore.lowest_root(ctx, Hs, Ss, tolerance=1e-11, max_iterations=2000)
-            plans[n].gradient(S, h, eri, c, lam, packed_eri=False, ri_factors=F)
+            lam, _, _ = plans[n].root_gradient(S, h, eri, ri_factors=F)
             energies.append(lam)
         return energies
 

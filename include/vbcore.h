@@ -191,6 +191,19 @@ vb_status vb_hs_plan_gradient(vb_hs_plan* plan, const double* ovlp_act, const do
                               double eigenvalue, double* dS_out, double* dh_out, double* deri_out,
                               const double* ri_factors, int n_aux, double* dri_out);
 
+/* One structure-space evaluation with H and S kept on the device: the plan at host inputs
+ * (S, h, eri as for vb_hs_plan_execute), its lowest root (dense solver up to 200 structures,
+ * else the Davidson iteration of vb_lowest_root with `tolerance`) and, when dS_out and dh_out
+ * are given, the root's gradient as vb_hs_plan_gradient (reusing the spin-pair records).
+ * energy: the root (no nuclear term); coefficients (n_str, may be NULL): its S-normalized
+ * eigenvector.  The selected-root solve and gradient accumulation of one trial point
+ * (solve_structure_problem, src/vbscf/derivatives/gradient/active_space/evaluator.cpp:466-560,
+ * and accumulate_active_space_gradient, :1046-1133).  Host buffers; synchronizes. */
+vb_status vb_hs_plan_root_gradient(vb_hs_plan* plan, const double* ovlp_act, const double* h1e_act,
+                                   const double* eri_packed, double tolerance, double* energy,
+                                   double* coefficients, double* dS_out, double* dh_out, const double* ri_factors,
+                                   int n_aux, double* dri_out);
+
 /* ---- metric Cholesky and the structure eigenproblem ------------------------------------------- */
 
 /* Upper Cholesky factor S = U^T U of a symmetric positive-definite metric

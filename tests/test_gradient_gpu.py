@@ -138,3 +138,29 @@ def test_gradient_exact_path_graded_overlaps(ctx):
         assert abs(fd - np.sum(g["S"] * E)) < 1e-7 * max(1.0, abs(fd)), (i, j, fd, np.sum(g["S"] * E))
     assert plan.stats()["careful_spin_pairs"] > plan.stats()["spin_pairs"] // 4
     plan.close()
+
+
+@pytest.mark.parametrize("kw,n,seed", [("COV", 6, 21), ("COV ION(1)", 8, 22)])
+def test_root_gradient_matches_separate_steps(ctx, kw, n, seed):
+    # one call with H and S device-resident (dense solver for 5 structures, Davidson for 294)
+    # against execute -> eigensolver -> gradient through host buffers
+    _, h, _ = workloads.active_space(n, 3 * n, seed)
+    S, _, _ = workloads.active_space(n, 3 * n, seed + 1)
+    rng = np.random.default_rng(seed)
+    F = 0.1 * rng.standard_normal((n * (n + 1) // 2, 3 * n))
+    eri = workloads.pack_pair_kernel(F @ F.T)
+    ex = vbcore.expand_structures(vbcore.generate_structures(kw, n, n), n)
+    plan = vbcore.HsPlan(ctx, ex, n)
+    E, c, g = plan.root_gradient(S, h, eri, ri_factors=F)
+    Hs, Ss = plan.execute(S, h, eri)
+    if Hs.shape[0] <= 200:
+        w, C = vbcore.generalized_eigh(ctx, Hs, Ss)
+        lam, cr = w[0], C[:, 0]
+    else:
+        lam, cr, _ = vbcore.lowest_root(ctx, Hs, Ss, tolerance=1e-11, max_iterations=2000)
+    gr = plan.gradient(S, h, eri, cr, lam, packed_eri=False, ri_factors=F)
+    assert abs(E - lam) < 1e-10 * max(1.0, abs(lam))
+    assert abs(abs(c @ Ss @ cr) - 1.0) < 1e-8
+    for key in ("S", "h", "ri"):
+        assert np.abs(g[key] - gr[key]).max() < 1e-8 * max(1.0, np.abs(gr[key]).max()), key
+    plan.close()

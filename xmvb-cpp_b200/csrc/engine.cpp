@@ -266,25 +266,13 @@ vb_status vb_engine_evaluate_instances(vb_engine* e, int count, const int64_t* i
             Instance* inst = &e->instances[ids[i]];
             per[inst->worker].push_back([=, &status, &msg] {
                 vb_context* c = e->ctx[inst->worker];
-                const int ns = inst->n_str, n = inst->n;
-                std::vector<double> Hs((size_t)ns * ns), Ss((size_t)ns * ns), w(ns), V((size_t)ns * ns);
-                vb_status st = vb_hs_plan_execute(inst->plan, S[i], h[i], eri[i], VB_MEM_HOST, Hs.data(), Ss.data());
-                if (st == VB_OK) {
-                    int info = 0, its = 0;
-                    st = ns <= 200 ? vb_generalized_eigh(c, Hs.data(), Ss.data(), ns, VB_MEM_HOST, w.data(), V.data(), &info)
-                                   : vb_lowest_root(c, Hs.data(), Ss.data(), ns, VB_MEM_HOST, 1.0e-11, 2000, w.data(),
-                                                    V.data(), &its);
-                }
-                if (st == VB_OK) {
-                    energies[i] = w[0];
-                    if (dS && dh && dS[i] && dh[i]) {
-                        std::vector<double> gs((size_t)n * n), gh((size_t)n * n);
-                        const bool ri = ri_factors && ri_factors[i] && dri && dri[i];
-                        st = vb_hs_plan_gradient(inst->plan, S[i], h[i], eri[i], VB_MEM_HOST, V.data(), w[0], dS[i],
-                                                 dh[i], nullptr, ri ? ri_factors[i] : nullptr, ri ? n_aux[i] : 0,
-                                                 ri ? dri[i] : nullptr);
-                    }
-                }
+                // structure H/S stay on the device (the plan's buffers); only the root returns
+                const bool grad = dS && dh && dS[i] && dh[i];
+                const bool ri = grad && ri_factors && ri_factors[i] && dri && dri[i];
+                vb_status st = vb_hs_plan_root_gradient(inst->plan, S[i], h[i], eri[i], 1.0e-11, &energies[i], nullptr,
+                                                        grad ? dS[i] : nullptr, grad ? dh[i] : nullptr,
+                                                        ri ? ri_factors[i] : nullptr, ri ? n_aux[i] : 0,
+                                                        ri ? dri[i] : nullptr);
                 status[i] = st;
                 if (st != VB_OK) msg[i] = vb_last_error(c);
             });

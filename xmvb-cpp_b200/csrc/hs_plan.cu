@@ -483,12 +483,13 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
 
 extern "C" {
 
-vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem,
-                             double* H_out, double* S_out) {
-    if (!p) return VB_ERR_INVALID;
+namespace {
+
+// Inputs in `mem`; outputs: H_out/S_out in `mem`, or (H_out == nullptr) left in the plan's
+// device buffers Hout/Sout.
+vb_status execute_impl(vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem, double* H_out,
+                       double* S_out) {
     vb_context* ctx = p->ctx;
-    if (!S || !h || !eri || !H_out || !S_out) return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_execute: null pointer");
-    if (mem != VB_MEM_HOST && mem != VB_MEM_DEVICE) return set_error(ctx, VB_ERR_INVALID, "bad memory space");
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     int launches = 0;
@@ -554,13 +555,14 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
     ra.Zs = scr[3];
     ra.Wh = scr[4];
     ra.Ws = scr[5];
-    double* Hdst = mem == VB_MEM_DEVICE ? H_out : p->Hout.as<double>();
-    double* Sdst = mem == VB_MEM_DEVICE ? S_out : p->Sout.as<double>();
+    const bool to_plan = H_out == nullptr;
+    double* Hdst = (mem == VB_MEM_DEVICE && !to_plan) ? H_out : p->Hout.as<double>();
+    double* Sdst = (mem == VB_MEM_DEVICE && !to_plan) ? S_out : p->Sout.as<double>();
     PhaseMark sreduce(p, VB_PHASE_STRUCTURE_REDUCE);
     cudaError_t err = launch_structure_reduce(ra, Hdst, Sdst, s, &launches);
     if (err != cudaSuccess) return cuda_error(ctx, err, "structure_reduce");
     sreduce.close();
-    if (mem == VB_MEM_HOST) {
+    if (mem == VB_MEM_HOST && !to_plan) {
         const size_t wbytes = sizeof(double) * (size_t)p->n_str * p->n_str;
         err = cudaMemcpyAsync(H_out, Hdst, wbytes, cudaMemcpyDeviceToHost, s);
         if (err == cudaSuccess) err = cudaMemcpyAsync(S_out, Sdst, wbytes, cudaMemcpyDeviceToHost, s);
@@ -572,6 +574,60 @@ vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, co
     p->stats.kernel_launches = launches;
     p->evaluated = true;
     return VB_OK;
+}
+
+}  // namespace
+
+vb_status vb_hs_plan_execute(vb_hs_plan* p, const double* S, const double* h, const double* eri, int mem,
+                             double* H_out, double* S_out) {
+    if (!p) return VB_ERR_INVALID;
+    vb_context* ctx = p->ctx;
+    if (!S || !h || !eri || !H_out || !S_out) return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_execute: null pointer");
+    if (mem != VB_MEM_HOST && mem != VB_MEM_DEVICE) return set_error(ctx, VB_ERR_INVALID, "bad memory space");
+    return execute_impl(p, S, h, eri, mem, H_out, S_out);
+}
+
+vb_status vb_hs_plan_root_gradient(vb_hs_plan* p, const double* S, const double* h, const double* eri,
+                                   double tolerance, double* energy, double* coefficients, double* dS_out,
+                                   double* dh_out, const double* ri_factors, int n_aux, double* dri_out) {
+    if (!p) return VB_ERR_INVALID;
+    vb_context* ctx = p->ctx;
+    if (!S || !h || !eri || !energy)
+        return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_root_gradient: null pointer");
+    vb_status st = execute_impl(p, S, h, eri, VB_MEM_HOST, nullptr, nullptr);
+    if (st != VB_OK) return st;
+    const int ns = p->n_str;
+    std::vector<double> c(ns);
+    double E = 0.0;
+    if (ns <= 200) {
+        DeviceBuffer w, V;
+        if ((st = w.allocate(ctx, sizeof(double) * ns)) != VB_OK) return st;
+        if ((st = V.allocate(ctx, sizeof(double) * (size_t)ns * ns)) != VB_OK) return st;
+        int info = 0;
+        st = vb_generalized_eigh(ctx, p->Hout.as<double>(), p->Sout.as<double>(), ns, VB_MEM_DEVICE, w.as<double>(),
+                                 V.as<double>(), &info);
+        if (st != VB_OK) return st;
+        cudaError_t err = cudaMemcpyAsync(&E, w.ptr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(c.data(), V.ptr, sizeof(double) * ns, cudaMemcpyDeviceToHost, ctx->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_root_gradient");
+    } else {
+        DeviceBuffer x;
+        if ((st = x.allocate(ctx, sizeof(double) * ns)) != VB_OK) return st;
+        int its = 0;
+        st = vb_lowest_root(ctx, p->Hout.as<double>(), p->Sout.as<double>(), ns, VB_MEM_DEVICE, tolerance, 2000, &E,
+                            x.as<double>(), &its);
+        if (st != VB_OK) return st;
+        cudaError_t err = cudaMemcpyAsync(c.data(), x.ptr, sizeof(double) * ns, cudaMemcpyDeviceToHost, ctx->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_root_gradient");
+    }
+    *energy = E;
+    if (coefficients) std::copy(c.begin(), c.end(), coefficients);
+    if (!dS_out || !dh_out) return VB_OK;
+    return vb_hs_plan_gradient(p, S, h, eri, VB_MEM_HOST, c.data(), E, dS_out, dh_out, nullptr, ri_factors, n_aux,
+                               dri_out);
 }
 
 vb_status vb_hs_plan_enable_phase_timing(vb_hs_plan* p, int enable) {

@@ -87,7 +87,7 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
     "vb_spin_pairs_noalloc", "vb_metric_cholesky", "vb_generalized_eigh", "vb_generalized_eigh_batched",
     "vb_active_transform_ri", "vb_active_transform_ri_precision", "vb_active_transform_ri_adjoint",
-    "vb_hs_plan_gradient",
+    "vb_hs_plan_gradient", "vb_hs_plan_root_gradient",
     "vb_lowest_root", "vb_engine_create", "vb_engine_destroy", "vb_engine_last_error", "vb_engine_add_instance",
     "vb_engine_evaluate_instances", "vb_engine_submit_scf", "vb_engine_poll", "vb_engine_pending",
     "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
@@ -154,6 +154,7 @@ def load_library(path: str = LIB_PATH):
     lib.vb_active_transform_ri.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, P, P, P]
     lib.vb_active_transform_ri_precision.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, c.c_int, P, P, P]
     lib.vb_active_transform_ri_adjoint.argtypes = [P, P, P, c.c_int, c.c_int, c.c_int, c.c_int, P]
+    lib.vb_hs_plan_root_gradient.argtypes = [P, P, P, P, c.c_double, P, P, P, P, P, c.c_int, P]
     lib.vb_same_spin_pairs.argtypes = [P, c.c_int, c.c_int, c.c_int64, P, P, P, P, P, c.c_int, P, P]
     for name in EXPORTED_SYMBOLS:
         fn = getattr(lib, name)
@@ -716,6 +717,35 @@ class HsPlan:
         _check(load_library().vb_hs_plan_execute(self._h, ctypes.c_void_p(S_ptr), ctypes.c_void_p(h_ptr),
                                                  ctypes.c_void_p(eri_ptr), VB_MEM_HOST, ctypes.c_void_p(H_ptr),
                                                  ctypes.c_void_p(S_out_ptr)), self.ctx.handle)
+
+    def root_gradient(self, S, h, eri, ri_factors=None, tolerance: float = 1e-11, gradient: bool = True):
+        """Lowest root of the structure problem at host inputs with H and S kept on the device,
+        and (gradient=True) its gradient: (E, c, {"S": dS, "h": dh, "ri": dF or None})."""
+        n = self.n_orbitals
+        Sf = _c(np.asarray(S).T, np.float64)
+        hf = _c(np.asarray(h).T, np.float64)
+        ef = _c(eri, np.float64)
+        ns = self.n_structures
+        E = ctypes.c_double()
+        c = np.empty(ns)
+        gS = np.empty(n * n) if gradient else None
+        gh = np.empty(n * n) if gradient else None
+        Ff = dF = None
+        n_aux = 0
+        if gradient and ri_factors is not None:
+            F = np.asarray(ri_factors, dtype=np.float64)
+            n_aux = F.shape[1]
+            Ff = _c(F.T, np.float64)
+            dF = np.empty(F.size)
+        _check(load_library().vb_hs_plan_root_gradient(
+            self._h, _ptr(Sf), _ptr(hf), _ptr(ef), tolerance, ctypes.byref(E), _ptr(c),
+            _ptr(gS) if gradient else None, _ptr(gh) if gradient else None, _ptr(Ff) if Ff is not None else None,
+            n_aux, _ptr(dF) if dF is not None else None), self.ctx.handle)
+        g = None
+        if gradient:
+            g = {"S": gS.reshape(n, n).T.copy(), "h": gh.reshape(n, n).T.copy(),
+                 "ri": dF.reshape(n_aux, -1).T.copy() if dF is not None else None}
+        return E.value, c, g
 
     def gradient(self, S, h, eri, coefficients, eigenvalue, packed_eri: bool = True, ri_factors=None):
         """Gradient of the structure root (eigenvalue, S-normalized coefficients) with respect to
