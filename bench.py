@@ -635,6 +635,56 @@ def run_ri(args):
     return 0
 
 
+def run_chain(args):
+    """Exact-path workload: one VBSCF energy + orbital gradient evaluation per step of a
+    stretched linear H14 chain (3.0 A spacing, seeded +-0.05 A jitter), 6-31G, 14e/14o singlet,
+    all 429 covalent Rumer structures; at this spacing most spin-pair overlap blocks are
+    ill-conditioned or rank deficient (the reference's SVD paths), the regime that dominates the
+    served H_n requests at large spacing."""
+    import numpy as np
+    import torch
+    import vbcore
+    from vbcore import molecules
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    ctx = vbcore.Context(local)
+    n = 14
+    mol = molecules.h_chain(n, 3.0, 0.05, seed=SEED)
+    pattern = molecules.hao_pattern(mol, n)
+    prob = vbcore.ScfProblem(ctx, mol, pattern, n)
+    C0 = molecules.hao_guess(mol, pattern)
+    for _ in range(args.warmup):
+        prob.energy_gradient(C0)
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        E, G = prob.energy_gradient(C0)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    ms = 1e3 * statistics.mean(times)
+    line = {
+        "metric": "VBSCF energy+gradient evaluations/s (stretched H14 chain)", "value": 1e3 / ms,
+        "unit": "evaluations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded geometry)",
+        "config": {"workload": "H14 chain 3.0 A + U(-0.05, 0.05) A jitter, 6-31G (n_bf 28), 14e/14o singlet, 429 "
+                               "covalent Rumer structures, HAO guess orbitals; energy + orbital gradient through "
+                               "the public API (host coefficients in, energy and gradient out)",
+                   "seed": SEED, "energy_Eh": E, "gradient_inf": float(np.abs(G).max())},
+        "roofline": None, "cpu_baseline": None,
+        "e2e": {"value": 1e3 / ms, "unit": "evaluations/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    prob.close()
+    ctx.close()
+    return 0
+
+
 def _batch_instance(n: int, seed: int):
     """A synthetic active-space instance: S, h as the microbenchmark, (ij|kl) = sum_P B_ij^P B_kl^P
     with B ~ N(0, 0.1) of shape [3n, n, n] symmetrized; also the pair factors F [n(n+1)/2, 3n]."""
@@ -798,7 +848,7 @@ def main():
     ap.add_argument("--workers", type=int, default=8, help="batch/serve: concurrent workers")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
     ap.add_argument("--rates", type=float, nargs="+", default=[50.0, 200.0, 800.0], help="serve: arrival rates")
-    ap.add_argument("--workload", default="hs", choices=["hs", "scf", "ri", "batch", "serve"],
+    ap.add_argument("--workload", default="hs", choices=["hs", "scf", "ri", "batch", "serve", "chain"],
                     help="hs: determinant-pair H/S evaluation (default); scf: plain VBSCF on H6; "
                          "ri: RI AO->active transform and metric Cholesky sweep")
     ap.add_argument("--profile", action="store_true",
@@ -822,6 +872,8 @@ def main():
         return run_ri(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "chain":
+        return run_chain(args)
     if args.workload == "serve":
         return run_serve(args)
     return run_vbcore(args)

@@ -584,16 +584,24 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a, c
 }
 
 
-// Listed blocks (or all blocks): one thread per block resolves it by the exact path and sums its
-// one- and two-electron terms; its first cofactors go to the warp's shared-memory slot, from
-// which the warp writes the u-vectors of its 32 records with the factor columns split over lanes.
-// Dynamic shared memory: 32 k^2 doubles per warp.
+// Listed blocks (or all blocks): one thread per block resolves it by the exact path; its first
+// cofactors A go to the lane's shared slot (k^2 doubles).  The warp then treats its 32 blocks one
+// at a time: the u-vectors of the records with the factor columns split over lanes, and, for
+// full-rank blocks with k > 3, the regular two-electron sum (A11 A22 - A12 A21) / det
+// (hamiltonian.cpp:83-123) with its C(k,2)^2 terms split over lanes, which keeps a block's
+// latency short when only a few blocks are listed.  Rank-deficient blocks and k <= 3 are summed
+// by their own thread: nullity 1 in the expanded form of the wedge second cofactors
+//   parity prod sv * sum_{s<k-1} (u_s ^ u_n)(v_s ^ v_n) / sv_s            (contractions.cpp:937-963)
+//   = Y(r1,c1) zu(r2) zv(c2) - Y(r1,c2) zu(r2) zv(c1) - Y(r2,c1) zu(r1) zv(c2) + Y(r2,c2) zu(r1) zv(c1),
+// Y = parity sum_{s<k-1} u_s v_s^T prod_{l<k-1, l != s} sv_l; nullity 2 and k <= 3 by
+// second_cofactor; nullity >= 3 is zero.  Dynamic shared memory: 32 k^2 doubles per warp.
 template <int KM>
 __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
     extern __shared__ double slots[];
     const long long count = a.all_careful ? a.n_pairs : (long long)(*a.careful_count);
     const int lane = threadIdx.x & 31;
     const int k = a.k, kk = a.k * a.k, gd = a.gamma_dim;
+    const int cp = k * (k - 1) / 2;
     double* wslot = slots + (size_t)(threadIdx.x >> 5) * 32 * kk;
     double* cof = wslot + (size_t)lane * kk;
     const long long N = a.n_strings;
@@ -603,6 +611,9 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
         const long long idx = base + lane;
         long long u = 0, v = 0;
         const bool valid = idx < count;
+        double det = 0.0, h1 = 0.0, h2 = 0.0;
+        int nullity = 3;
+        bool regular = false;  // two-electron sum done by the warp
         if (valid) {
             if (a.all_careful) {
                 const double b = 2.0 * (double)N + 1.0;
@@ -629,91 +640,102 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
             dev::ResolutionT<KM> res;
             dev::resolve_exact<KM>(k, x, kThreshold, &res);
             dev::first_cofactor<KM>(res, cof);
-            double h1 = 0.0, h2 = 0.0;
+            det = res.det;
+            nullity = res.nullity;
+            regular = res.nullity == 0 && k > 3;
             if (res.nullity < 3) {
                 if (res.nullity <= 1)
                     for (int c = 0; c < k; ++c)
                         for (int r = 0; r < k; ++r) h1 = fma(__ldg(a.h + L[c] * a.n + R[r]), cof[c * k + r], h1);
-                // two-electron sum over r1 < r2, c1 < c2: gamma[(R r1, R r2)][(L c1, L c2)] is
-                // (r1 c1 | r2 c2) - (r1 c2 | r2 c1) (hamiltonian.cpp:83-162)
-                const bool regular = res.nullity == 0 && k > 3;
-                // nullity 1 (k > 3): the second cofactor parity * prod_{i<k-1} sv_i *
-                // sum_{s<k-1} (u_s ^ u_n)(v_s ^ v_n) / sv_s (contractions.cpp:937-963) expands to
-                // Y(r1,c1) zu(r2) zv(c2) - Y(r1,c2) zu(r2) zv(c1) - Y(r2,c1) zu(r1) zv(c2) + Y(r2,c2) zu(r1) zv(c1)
-                // with Y = parity sum_{s<k-1} u_s v_s^T prod_{l<k-1, l != s} sv_l and (zu, zv) the null pair
-                const bool rank1 = res.nullity == 1 && k > 3;
-                double Y[KM * KM], zu[KM], zv[KM];
-                if (rank1) {
-                    const int ni = k - 1;
-                    double w[KM];
-                    for (int s2 = 0; s2 < ni; ++s2) {
-                        double p = res.parity;
-                        for (int l = 0; l < ni; ++l)
-                            if (l != s2) p *= res.sv[l];
-                        w[s2] = p;
-                    }
-                    for (int r = 0; r < k; ++r) {
-                        zu[r] = res.u[ni * k + r];
-                        zv[r] = res.v[ni * k + r];
-                        for (int c = 0; c < k; ++c) {
-                            double acc = 0.0;
-                            for (int s2 = 0; s2 < ni; ++s2) acc = fma(res.u[s2 * k + r] * w[s2], res.v[s2 * k + c], acc);
-                            Y[r * k + c] = acc;
+                if (!regular) {
+                    const bool rank1 = res.nullity == 1 && k > 3;
+                    double Y[KM * KM], zu[KM], zv[KM];
+                    if (rank1) {
+                        const int ni = k - 1;
+                        double w[KM];
+                        for (int s2 = 0; s2 < ni; ++s2) {
+                            double p = res.parity;
+                            for (int l = 0; l < ni; ++l)
+                                if (l != s2) p *= res.sv[l];
+                            w[s2] = p;
+                        }
+                        for (int r = 0; r < k; ++r) {
+                            zu[r] = res.u[ni * k + r];
+                            zv[r] = res.v[ni * k + r];
+                            for (int c = 0; c < k; ++c) {
+                                double acc = 0.0;
+                                for (int s2 = 0; s2 < ni; ++s2) acc = fma(res.u[s2 * k + r] * w[s2], res.v[s2 * k + c], acc);
+                                Y[r * k + c] = acc;
+                            }
                         }
                     }
+                    for (int r2 = 1; r2 < k; ++r2)
+                        for (int r1 = 0; r1 < r2; ++r1) {
+                            const double* grow = a.gamma + (long long)dev::anti_index(R[r1], R[r2]) * gd;
+                            double part = 0.0;
+                            for (int c2 = 1; c2 < k; ++c2)
+                                for (int c1 = 0; c1 < c2; ++c1) {
+                                    const double g = __ldg(grow + dev::anti_index(L[c1], L[c2]));
+                                    const double m2 = rank1 ? Y[r1 * k + c1] * zu[r2] * zv[c2] - Y[r1 * k + c2] * zu[r2] * zv[c1] -
+                                                                  Y[r2 * k + c1] * zu[r1] * zv[c2] + Y[r2 * k + c2] * zu[r1] * zv[c1]
+                                                            : dev::second_cofactor<KM>(res, r1, r2, c1, c2);
+                                    part = fma(g, m2, part);
+                                }
+                            h2 += part;
+                        }
                 }
-                for (int r2 = 1; r2 < k; ++r2)
-                    for (int r1 = 0; r1 < r2; ++r1) {
-                        const double* grow = a.gamma + (long long)dev::anti_index(R[r1], R[r2]) * gd;
-                        double part = 0.0;
-                        for (int c2 = 1; c2 < k; ++c2)
-                            for (int c1 = 0; c1 < c2; ++c1) {
-                                const double g = __ldg(grow + dev::anti_index(L[c1], L[c2]));
-                                double m2;
-                                if (regular)
-                                    m2 = cof[c1 * k + r1] * cof[c2 * k + r2] - cof[c2 * k + r1] * cof[c1 * k + r2];
-                                else if (rank1)
-                                    m2 = Y[r1 * k + c1] * zu[r2] * zv[c2] - Y[r1 * k + c2] * zu[r2] * zv[c1] -
-                                         Y[r2 * k + c1] * zu[r1] * zv[c2] + Y[r2 * k + c2] * zu[r1] * zv[c1];
-                                else
-                                    m2 = dev::second_cofactor<KM>(res, r1, r2, c1, c2);
-                                part = fma(g, m2, part);
-                            }
-                        h2 += part;
-                    }
-                if (regular) h2 /= res.det;
-            } else {
-                for (int i = 0; i < kk; ++i) cof[i] = 0.0;
             }
             if (res.nullity > 1)
                 for (int i = 0; i < kk; ++i) cof[i] = 0.0;
-            double* rec = a.records + record_index(u, v, N) * (long long)a.rec_stride;
-            rec[a.R + 0] = res.det;
-            rec[a.R + 1] = res.nullity < 3 ? h1 + h2 : 0.0;
-            rec[a.R + 2] = res.nullity < 3 ? h1 : 0.0;
-            rec[a.R + 3] = (double)res.nullity;
         }
         __syncwarp();
-        // u-vectors of the warp's records: u_m = sum_{c,r} A(r,c) l_m[pair(R_r, L_c)]
         for (int j = 0; j < 32; ++j) {
             const long long jdx = base + j;
             if (jdx >= count) break;
             const long long uj = __shfl_sync(0xffffffffu, u, j), vj = __shfl_sync(0xffffffffu, v, j);
+            const uint64_t* ol = a.occ + 2 * uj;
+            const uint64_t* orr = a.occ + 2 * vj;
             const double* cj = wslot + (size_t)j * kk;
+            // regular two-electron sum of block j, terms split over lanes: gamma[(R r1, R r2)][(L c1, L c2)]
+            // is (r1 c1 | r2 c2) - (r1 c2 | r2 c1)
+            if (__shfl_sync(0xffffffffu, (int)regular, j)) {
+                double part = 0.0;
+                for (int q = lane; q < cp * cp; q += 32) {
+                    const int rp = q / cp, cq = q % cp;
+                    int r2 = 1;
+                    while ((r2 + 1) * r2 / 2 <= rp) ++r2;
+                    const int r1 = rp - r2 * (r2 - 1) / 2;
+                    int c2 = 1;
+                    while ((c2 + 1) * c2 / 2 <= cq) ++c2;
+                    const int c1 = cq - c2 * (c2 - 1) / 2;
+                    const double g = __ldg(a.gamma + (long long)dev::anti_index(occ_byte(orr, r1), occ_byte(orr, r2)) * gd +
+                                           dev::anti_index(occ_byte(ol, c1), occ_byte(ol, c2)));
+                    part = fma(g, cj[c1 * k + r1] * cj[c2 * k + r2] - cj[c2 * k + r1] * cj[c1 * k + r2], part);
+                }
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                if (lane == j) h2 = part / det;
+            }
+            // u-vectors: u_m = sum_{c,r} A(r,c) l_m[pair(R_r, L_c)]
             double* rec = a.records + record_index(uj, vj, N) * (long long)a.rec_stride;
             for (int m = lane; m < a.R; m += 32) {
                 double acc = 0.0;
                 for (int c = 0; c < k; ++c) {
-                    const int lc = occ_byte(a.occ + 2 * uj, c);
+                    const int lc = occ_byte(ol, c);
                     for (int r = 0; r < k; ++r) {
                         const double cv = cj[c * k + r];
                         if (cv != 0.0)
-                            acc = fma(cv, __ldg(a.lf + (long long)dev::pair_index(occ_byte(a.occ + 2 * vj, r), lc) * a.ld + m),
-                                      acc);
+                            acc = fma(cv, __ldg(a.lf + (long long)dev::pair_index(occ_byte(orr, r), lc) * a.ld + m), acc);
                     }
                 }
                 rec[m] = acc;
             }
+        }
+        if (valid) {
+            double* rec = a.records + record_index(u, v, N) * (long long)a.rec_stride;
+            rec[a.R + 0] = det;
+            rec[a.R + 1] = nullity < 3 ? h1 + h2 : 0.0;
+            rec[a.R + 2] = nullity < 3 ? h1 : 0.0;
+            rec[a.R + 3] = (double)nullity;
         }
         __syncwarp();
     }
