@@ -519,16 +519,15 @@ __device__ void svd_frame_adjoint(int k, const double* U, const double* V, const
 // terms of that order.  adj_u . l_m at each packed pair is read from Q.
 template <int KM>
 __global__ void __launch_bounds__(128) careful_backward_kernel(BackArgs a, long long idx_begin, long long idx_end,
-                                                               int all_pairs, int gamma_in_smem, double* gpart) {
-    extern __shared__ double sgG[];  // gd x gd when gamma_in_smem; flushed into this block's gpart slot
+                                                               int all_pairs, double* gpart) {
+    // this block's slot: two-electron table (gd^2), then the S and h adjoints (n^2 each);
+    // only the block's own threads add into it, no shared memory, no barrier
     constexpr int KP = KM * (KM - 1) / 2;
     const int k = a.k, n = a.n, np = a.ld, gd = a.gd;
     const long long N = a.N;
-    if (gamma_in_smem) {
-        for (int i = threadIdx.x; i < gd * gd; i += blockDim.x) sgG[i] = 0.0;
-        __syncthreads();
-    }
-    double* gG = gamma_in_smem ? sgG : a.gG;
+    double* gG = gpart + (size_t)blockIdx.x * ((size_t)gd * gd + 2 * (size_t)n * n);
+    double* gSb = gG + (size_t)gd * gd;
+    double* ghb = gSb + (size_t)n * n;
     for (long long idx = idx_begin + blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < idx_end;
          idx += (long long)gridDim.x * blockDim.x) {
         if (k == 0) break;
@@ -558,7 +557,7 @@ __global__ void __launch_bounds__(128) careful_backward_kernel(BackArgs a, long 
             double gX[KM * KM];
             svd_frame_adjoint<KM>(k, U, V, sv, parity, aS, GA, aH, a.gamma, gd, L, Rr, gX);
             for (int r = 0; r < k; ++r)
-                for (int c = 0; c < k; ++c) atomicAdd(a.gS + L[c] * n + Rr[r], gX[r * k + c]);
+                for (int c = 0; c < k; ++c) atomicAdd(gSb + L[c] * n + Rr[r], gX[r * k + c]);
         }
         // first cofactors
         double d1[KM];
@@ -568,7 +567,7 @@ __global__ void __launch_bounds__(128) careful_backward_kernel(BackArgs a, long 
             for (int c = 0; c < k; ++c) {
                 double A = 0.0;
                 for (int s2 = 0; s2 < k; ++s2) A = fma(U[s2 * k + r] * d1[s2], V[s2 * k + c], A);
-                if (aH != 0.0) atomicAdd(a.gh + L[c] * n + Rr[r], aH * A);
+                if (aH != 0.0) atomicAdd(ghb + L[c] * n + Rr[r], aH * A);
                 prow[dev::pair_index(Rr[r], L[c])] += A;
             }
         // second cofactors into the two-electron table
@@ -602,19 +601,21 @@ __global__ void __launch_bounds__(128) careful_backward_kernel(BackArgs a, long 
             }
         }
     }
-    if (gamma_in_smem) {
-        __syncthreads();
-        double* slot = gpart + (size_t)blockIdx.x * gd * gd;  // owned by this block index
-        for (int i = threadIdx.x; i < gd * gd; i += blockDim.x) slot[i] += sgG[i];
-    }
 }
 
-// gG += sum over block slots.
-__global__ void reduce_slots_kernel(const double* __restrict__ gpart, int slots, int count, double* __restrict__ gG) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+// Sums the block slots [gG (g2) | gS (n2) | gh (n2)] into the outputs.
+__global__ void reduce_slots_kernel(const double* __restrict__ gpart, int slots, int g2, int n2, double* __restrict__ gG,
+                                    double* __restrict__ gS, double* __restrict__ gh) {
+    const int size = g2 + 2 * n2;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x) {
         double acc = 0.0;
-        for (int b = 0; b < slots; ++b) acc += gpart[(size_t)b * count + i];
-        gG[i] += acc;
+        for (int b = 0; b < slots; ++b) acc += gpart[(size_t)b * size + i];
+        if (i < g2)
+            gG[i] += acc;
+        else if (i < g2 + n2)
+            gS[i - g2] += acc;
+        else
+            gh[i - g2 - n2] += acc;
     }
 }
 
@@ -656,18 +657,17 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
     const size_t target = std::max<size_t>((size_t)16 << 20, std::min<size_t>((size_t)768 << 20, left / 2));
     const long long chunk = std::min<long long>(
         count, std::max<long long>(1024, (long long)(target / (8ULL * (2 * np + R + 1)))));
-    // two-electron table per block in shared memory when it fits (three blocks per SM), each
-    // block adding into its own slot; the slots are summed once after the last chunk
-    const size_t gbytes = sizeof(double) * (size_t)b.gd * b.gd;
-    const int in_smem = gbytes <= 72 * 1024 ? 1 : 0;
-    const int grid = in_smem ? 148 * 3 : 148 * 8;
+    // per-block slots (two-electron table, S and h adjoints), summed once after the last chunk
+    const size_t slot_bytes = sizeof(double) * ((size_t)b.gd * b.gd + 2 * (size_t)b.n * b.n);
+    auto kernel = b.k <= 8 ? careful_backward_kernel<8> : careful_backward_kernel<dev::KMAX>;
+    int per_sm = 4;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0) != cudaSuccess || per_sm < 1) per_sm = 4;
+    const int grid = 148 * std::min(per_sm, 8);  // one wave of resident blocks
     DeviceBuffer acb, qb, pb, slots;
     vb_status st;
-    if (in_smem) {
-        if ((st = slots.allocate(ctx, gbytes * grid)) != VB_OK) return st;
-        if (cudaMemsetAsync(slots.ptr, 0, gbytes * grid, s) != cudaSuccess)
-            return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: memset failed");
-    }
+    if ((st = slots.allocate(ctx, slot_bytes * grid)) != VB_OK) return st;
+    if (cudaMemsetAsync(slots.ptr, 0, slot_bytes * grid, s) != cudaSuccess)
+        return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: memset failed");
     if ((st = acb.allocate(ctx, sizeof(double) * (size_t)chunk * std::max(R, 1))) != VB_OK) return st;
     if ((st = qb.allocate(ctx, sizeof(double) * (size_t)chunk * np)) != VB_OK) return st;
     if ((st = pb.allocate(ctx, sizeof(double) * (size_t)chunk * np)) != VB_OK) return st;
@@ -689,25 +689,20 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
             err = cudaMemsetAsync(qb.ptr, 0, sizeof(double) * (size_t)cnt * np, s);
         }
         if (err == cudaSuccess) {
-            auto kernel = b.k <= 8 ? careful_backward_kernel<8> : careful_backward_kernel<dev::KMAX>;
-            if (in_smem && gbytes > 48 * 1024)
-                err = allow_dynamic_smem((const void*)kernel, (int)gbytes);
-            if (err == cudaSuccess) {
-                kernel<<<grid, 128, in_smem ? gbytes : 0, s>>>(b, i0, i1, all_pairs, in_smem, slots.as<double>());
-                err = cudaGetLastError();
-            }
+            kernel<<<grid, 128, 0, s>>>(b, i0, i1, all_pairs, slots.as<double>());
+            err = cudaGetLastError();
         }
         if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (exact path)");
         if (R > 0 && cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, R, np, (int)cnt, &one, acb.as<double>(), R,
                                  pb.as<double>(), np, &one, b.gL, np) != CUBLAS_STATUS_SUCCESS)
             return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
     }
-    if (in_smem) {
-        const int cnt = b.gd * b.gd;
-        reduce_slots_kernel<<<std::max(1, std::min(148 * 4, (cnt + 127) / 128)), 128, 0, s>>>(slots.as<double>(), grid,
-                                                                                            cnt, b.gG);
+    {
+        const int g2 = b.gd * b.gd, n2 = b.n * b.n;
+        reduce_slots_kernel<<<std::max(1, std::min(148 * 4, (g2 + 2 * n2 + 127) / 128)), 128, 0, s>>>(
+            slots.as<double>(), grid, g2, n2, b.gG, b.gS, b.gh);
         cudaError_t err = cudaGetLastError();
-        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (table slots)");
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (block slots)");
     }
     return VB_OK;
 }
