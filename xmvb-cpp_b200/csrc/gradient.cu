@@ -82,6 +82,62 @@ struct AdjArgs {
     int adj_stride;  // R + 2: [u adjoint (R)], adj(det), adj(H)
 };
 
+// With shared alpha/beta string tables and a spin-flip symmetric determinant list (the flipped
+// determinant carries the same structure terms, so w(flip d) = w(d)), the beta-side scatter of a
+// pair {d, e} equals the alpha-side scatter of {flip d, flip e} into the same record, so the
+// record adjoint is twice the alpha-side sum.  That sum is grouped by alpha record (i <= j): over
+// d in D_i, e in D_j (D_i: determinants with alpha string i), weight 2 w_d w_e for i < j and all
+// ordered pairs with weight w_d w_e for i = j.  One warp per record, lanes over the factor
+// columns (m = lane + 32 q, q < 4: R <= 128), one write per record, no atomics.
+__global__ void __launch_bounds__(256) det_pair_adjoint_flip_kernel(AdjArgs a, const int* __restrict__ aoff,
+                                                                    const int* __restrict__ adets) {
+    const int R = a.f.R;
+    const long long Na = a.f.Na;
+    const long long n_rec = Na * (Na + 1) / 2;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n_rec; t += nwarps) {
+        long long i, j;
+        upper_decode(t, Na, &i, &j);
+        const int i0 = __ldg(aoff + i), i1 = __ldg(aoff + i + 1);
+        const int j0 = __ldg(aoff + j), j1 = __ldg(aoff + j + 1);
+        const double pair_w = i == j ? 1.0 : 2.0;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double acc_det = 0.0, acc_h = 0.0;
+        for (int p = i0; p < i1; ++p) {
+            const int d = __ldg(adets + p);
+            const double wd = __ldg(a.w + d) * pair_w;
+            if (wd == 0.0) continue;
+            const int bd = __ldg(a.f.det_beta + d);
+            for (int q = j0; q < j1; ++q) {
+                const int e = __ldg(adets + q);
+                const double omega = wd * __ldg(a.w + e);
+                if (omega == 0.0) continue;
+                const int be = __ldg(a.f.det_beta + e);
+                const double* rb = a.f.rec_b + record_index(min(bd, be), max(bd, be), a.f.Nb) * a.f.stride_b;
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq) {
+                    const int m = lane + 32 * qq;
+                    if (m < R) acc[qq] = fma(omega, m < a.f.r_pos ? __ldg(rb + m) : -__ldg(rb + m), acc[qq]);
+                }
+                const double sb = __ldg(rb + R), hb = __ldg(rb + R + 1);
+                acc_det = fma(omega, hb - a.lambda * sb, acc_det);
+                acc_h = fma(omega, sb, acc_h);
+            }
+        }
+        double* adj = a.adj_a + t * a.adj_stride;
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+            const int m = lane + 32 * qq;
+            if (m < R) adj[m] += 2.0 * acc[qq];
+        }
+        if (lane == 0) {
+            adj[R] += 2.0 * acc_det;
+            adj[R + 1] += 2.0 * acc_h;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) det_pair_adjoint_kernel(AdjArgs a) {
     const long long n = a.f.n_det;
     const long long total = n * (n + 1) / 2;
@@ -826,7 +882,10 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
     aa.adj_b = p->shared_tables ? p->adj_a.as<double>() : p->adj_b.as<double>();
     aa.adj_stride = adj_stride;
     if (err == cudaSuccess) {
-        det_pair_adjoint_kernel<<<148 * 8, 256, 0, s>>>(aa);
+        if (p->has_flip && p->shared_tables && p->ka > 0 && p->R <= 128)
+            det_pair_adjoint_flip_kernel<<<148 * 8, 256, 0, s>>>(aa, p->alpha_off.as<int>(), p->alpha_dets.as<int>());
+        else
+            det_pair_adjoint_kernel<<<148 * 8, 256, 0, s>>>(aa);
         err = cudaGetLastError();
     }
     // backward through each distinct spin table

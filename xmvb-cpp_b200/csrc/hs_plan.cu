@@ -256,6 +256,15 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
         }
         if (ok) {
             p->has_flip = true;
+            // determinants grouped by alpha string, for the gradient's per-record adjoint sums
+            std::vector<int> aoff(p->Na + 1, 0), adets(p->n_det);
+            for (long long d = 0; d < p->n_det; ++d) ++aoff[ex->det_alpha[d] + 1];
+            for (int i = 0; i < p->Na; ++i) aoff[i + 1] += aoff[i];
+            std::vector<int> next(aoff.begin(), aoff.end() - 1);
+            for (long long d = 0; d < p->n_det; ++d) adets[next[ex->det_alpha[d]]++] = (int)d;
+            if ((st = upload(ctx, p->alpha_off, aoff.data(), sizeof(int) * aoff.size())) != VB_OK) return fail(st);
+            if ((st = upload(ctx, p->alpha_dets, adets.data(), sizeof(int) * std::max<size_t>(1, adets.size()))) != VB_OK)
+                return fail(st);
             // orbits of unordered pairs {d, e} under the flip (Burnside): (P + fixed pairs) / 2
             long long fixed_dets = 0;
             for (long long d = 0; d < p->n_det; ++d) fixed_dets += flipmap[d] == d;

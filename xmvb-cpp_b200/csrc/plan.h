@@ -48,6 +48,8 @@ struct vb_hs_plan {
     StructureChunks chunks;
     // spin-flip map of the determinant list (folds the determinant-pair work in half)
     DeviceBuffer flip;
+    // determinants by alpha string (CSR: alpha_off[i] .. alpha_off[i + 1] index alpha_dets)
+    DeviceBuffer alpha_off, alpha_dets;
     bool has_flip = false;
     long long det_pair_evaluations = 0;  // unordered determinant pairs evaluated (orbit representatives)
     vb_hs_stats stats{};
