@@ -332,9 +332,10 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
     double scale = 1.0;
     int it = 0;
     bool converged = false;
-    // projected matrices are kept with the basis; column k-1 is new
-    auto add_column = [&](int c) -> vb_status {
-        gemv2(V + (size_t)c * n, HV + (size_t)c * n, SV + (size_t)c * n);
+    // projected matrices are kept with the basis; column c is new (its H v and S v are computed
+    // here unless the caller already stored them in HV and SV)
+    auto add_column = [&](int c, bool have_images) -> vb_status {
+        if (!have_images) gemv2(V + (size_t)c * n, HV + (size_t)c * n, SV + (size_t)c * n);
         std::vector<double> hcol, scol;
         dots_of(V, c + 1, HV + (size_t)c * n, &hcol);
         if ((st = check("vb_lowest_root")) != VB_OK) return st;
@@ -346,7 +347,7 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
         }
         return VB_OK;
     };
-    if ((st = add_column(0)) != VB_OK) return st;
+    if ((st = add_column(0, false)) != VB_OK) return st;
     DeviceBuffer mbuf, uibuf;
     double* Ui = nullptr;
     for (it = 0; it < max_iterations; ++it) {
@@ -423,24 +424,28 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
                 }
             k = keep;
         }
-        // S-orthogonalize the correction t against the basis, twice
+        // S-orthogonalize the correction t against the basis, twice: V^T S t = (S V)^T t (S is
+        // symmetric), so the coefficients come from the stored images S V without a pass over S
         for (int pass = 0; pass < 2; ++pass) {
-            gemv2(t, hx, st_vec);  // hx reused as scratch: only S t is needed
             std::vector<double> c;
-            dots_of(V, k, st_vec, &c);
+            dots_of(SV, k, t, &c);
             if ((st = check("vb_lowest_root")) != VB_OK) return st;
             for (double& v : c) v = -v;
             err = cudaMemcpyAsync(coef, c.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s);
             combine_kernel<<<nb, tb, 0, s>>>(V, n, k, coef, 1.0, t);
         }
+        // one pass over H and S: H t and S t give the norm and, scaled, the new column's images
         gemv2(t, hx, st_vec);
         std::vector<double> nrm;
         dots_of(t, 1, st_vec, &nrm);
         if ((st = check("vb_lowest_root")) != VB_OK) return st;
         if (!(nrm[0] > 1e-28)) break;  // no new direction
-        scale_copy_kernel<<<nb, tb, 0, s>>>(n, t, 1.0 / std::sqrt(nrm[0]), V + (size_t)k * n);
+        const double inv = 1.0 / std::sqrt(nrm[0]);
+        scale_copy_kernel<<<nb, tb, 0, s>>>(n, t, inv, V + (size_t)k * n);
+        scale_copy_kernel<<<nb, tb, 0, s>>>(n, hx, inv, HV + (size_t)k * n);
+        scale_copy_kernel<<<nb, tb, 0, s>>>(n, st_vec, inv, SV + (size_t)k * n);
         ++k;
-        if ((st = add_column(k - 1)) != VB_OK) return st;
+        if ((st = add_column(k - 1, true)) != VB_OK) return st;
     }
     if (iterations) *iterations = it;
     *eigenvalue = theta;
