@@ -17,6 +17,11 @@ e2e    = the same through the host-pointer API (pinned host inputs copied in, H 
          back every step);
 roofline = the dominant kernel (by CUDA-event phase time) against the FP64 peak measured here
          with cuBLAS DGEMM, using the pair-flop model per processed unit.
+
+Other workloads (--workload): scf (plain VBSCF solve of H6), ri (RI transform, FP64 and split
+precision, plus the metric Cholesky sweep), batch (256 batched instances, engine vs one at a
+time), serve (Poisson-arrival served solves vs a one-worker engine), chain (stretched H14
+energy + gradient evaluation: the exact path).
 """
 
 from __future__ import annotations
@@ -850,7 +855,9 @@ def main():
     ap.add_argument("--rates", type=float, nargs="+", default=[50.0, 200.0, 800.0], help="serve: arrival rates")
     ap.add_argument("--workload", default="hs", choices=["hs", "scf", "ri", "batch", "serve", "chain"],
                     help="hs: determinant-pair H/S evaluation (default); scf: plain VBSCF on H6; "
-                         "ri: RI AO->active transform and metric Cholesky sweep")
+                         "ri: RI AO->active transform (FP64 and split precision) and metric Cholesky sweep; "
+                         "batch: batched instances through the engine vs one at a time; serve: Poisson-arrival "
+                         "served solves vs a one-worker engine; chain: stretched H14 energy+gradient evaluation")
     ap.add_argument("--profile", action="store_true",
                     help="for profiler captures: 4 GiB HBM budget, no DGEMM peak, CPU baseline or end-to-end leg")
     ap.add_argument("--n-active", type=int, default=14,
