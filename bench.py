@@ -65,6 +65,25 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(ms: float, device) -> float:
+    """The job's time: the largest of the ranks' device-timed milliseconds (all-reduce MAX over
+    the process group; the value itself when there is no group or a single rank)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_step: float, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job rate of independent replicas: every rank processes `units_per_step` per step,
+    and the job takes the slowest rank's time."""
+    return units_per_step * steps * world / (max_ms * 1e-3)
+
+
 def config_dict(n_det, n_str, world):
     k = N_ELECTRONS // 2
     return {
@@ -298,14 +317,11 @@ def run_vbcore(args):
         phases.append(plan.phase_times())
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    total_ms = sum(step_ms)
+    total_ms = max_over_ranks(sum(step_ms), device)
     if world > 1:
-        t = torch.tensor([total_ms], device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
         torch.distributed.barrier()
     stats = plan.stats()
-    value = ordered * args.steps * world / (total_ms * 1e-3)
+    value = job_throughput(ordered, args.steps, world, total_ms)
 
     # end to end through the host-pointer API with pinned buffers
     pS = torch.tensor(np.ascontiguousarray(S.T)).pin_memory()
@@ -324,11 +340,8 @@ def run_vbcore(args):
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = ordered * args.steps * world / (e2e_ms * 1e-3) if e2e_ms > 0 else None
+    e2e_ms = max_over_ranks(e2e_ms, device)
+    e2e_value = job_throughput(ordered, args.steps, world, e2e_ms) if e2e_ms > 0 else None
     h2d = (2 * N_ACTIVE * N_ACTIVE + len(eri)) * 8
     d2h = 2 * n_str * n_str * 8
 
