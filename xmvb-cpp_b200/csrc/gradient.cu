@@ -470,7 +470,7 @@ __device__ __forceinline__ double sv_product_except(int k, const double* sv, uns
 // Aw[r k + c]; gamma_row(c1, c2) returns the two-electron table row of the left pair (already
 // scaled by the Hamiltonian adjoint through `scale`); gX[r k + c] receives df/dX[r][c].
 template <int KM>
-__device__ void svd_frame_adjoint(int k, const double* U, const double* V, const double* sv, double parity,
+__device__ __forceinline__ void svd_frame_adjoint(int k, const double* U, const double* V, const double* sv, double parity,
                                   double aS, const double* Aw, double scale, const double* gamma, int gd,
                                   const int* L, const int* Rr, double* gX) {
     // U[r][s] = U[s k + r], V[c][s] = V[s k + c]
@@ -573,13 +573,13 @@ __device__ void svd_frame_adjoint(int k, const double* U, const double* V, const
 // the inverse-based one, without its loss of accuracy (relative kappa * eps) on ill-conditioned
 // blocks; where the reference truncates singular values below 1e-12 the two functions differ by
 // terms of that order.  adj_u . l_m at each packed pair is read from Q.
-template <int KM>
+template <int KM, int KC>  // KC > 0: electrons per string fixed at compile time (== KM)
 __global__ void __launch_bounds__(128) careful_backward_kernel(BackArgs a, long long idx_begin, long long idx_end,
                                                                int all_pairs, double* gpart) {
     // this block's slot: two-electron table (gd^2), then the S and h adjoints (n^2 each);
     // only the block's own threads add into it, no shared memory, no barrier
     constexpr int KP = KM * (KM - 1) / 2;
-    const int k = a.k, n = a.n, np = a.ld, gd = a.gd;
+    const int k = KC > 0 ? KC : a.k, n = a.n, np = a.ld, gd = a.gd;
     const long long N = a.N;
     double* gG = gpart + (size_t)blockIdx.x * ((size_t)gd * gd + 2 * (size_t)n * n);
     double* gSb = gG + (size_t)gd * gd;
@@ -715,7 +715,8 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
         count, std::max<long long>(1024, (long long)(target / (8ULL * (2 * np + R + 1)))));
     // per-block slots (two-electron table, S and h adjoints), summed once after the last chunk
     const size_t slot_bytes = sizeof(double) * ((size_t)b.gd * b.gd + 2 * (size_t)b.n * b.n);
-    auto kernel = b.k <= 8 ? careful_backward_kernel<8> : careful_backward_kernel<dev::KMAX>;
+    auto kernel = b.k == 7 ? careful_backward_kernel<7, 7>
+                           : (b.k <= 8 ? careful_backward_kernel<8, 0> : careful_backward_kernel<dev::KMAX, 0>);
     int per_sm = 4;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0) != cudaSuccess || per_sm < 1) per_sm = 4;
     const int grid = 148 * std::min(per_sm, 8);  // one wave of resident blocks
@@ -769,7 +770,8 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
 size_t gradient_stack_bytes() {
     size_t m = 0;
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, careful_backward_kernel<8>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, careful_backward_kernel<8, 0>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, careful_backward_kernel<7, 7>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
     return m;
 }
 

@@ -595,12 +595,12 @@ __global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a, c
 //   = Y(r1,c1) zu(r2) zv(c2) - Y(r1,c2) zu(r2) zv(c1) - Y(r2,c1) zu(r1) zv(c2) + Y(r2,c2) zu(r1) zv(c1),
 // Y = parity sum_{s<k-1} u_s v_s^T prod_{l<k-1, l != s} sv_l; nullity 2 and k <= 3 by
 // second_cofactor; nullity >= 3 is zero.  Dynamic shared memory: 32 k^2 doubles per warp.
-template <int KM>
+template <int KM, int KC>  // KC > 0: electrons per string fixed at compile time (== KM)
 __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
     extern __shared__ double slots[];
     const long long count = a.all_careful ? a.n_pairs : (long long)(*a.careful_count);
     const int lane = threadIdx.x & 31;
-    const int k = a.k, kk = a.k * a.k, gd = a.gamma_dim;
+    const int k = KC > 0 ? KC : a.k, kk = k * k, gd = a.gamma_dim;
     const int cp = k * (k - 1) / 2;
     double* wslot = slots + (size_t)(threadIdx.x >> 5) * 32 * kk;
     double* cof = wslot + (size_t)lane * kk;
@@ -908,7 +908,8 @@ cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, doubl
 size_t exact_stack_bytes() {
     size_t m = 0;
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, spin_pairs_exact<8>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, spin_pairs_exact<8, 0>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
+    if (cudaFuncGetAttributes(&fa, spin_pairs_exact<7, 7>) == cudaSuccess) m = std::max(m, fa.localSizeBytes);
     return m;
 }
 
@@ -934,7 +935,7 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream
     }
     SpinTableArgs b = a;
     b.all_careful = fast_ok ? 0 : 1;
-    auto exact = a.k <= 8 ? spin_pairs_exact<8> : spin_pairs_exact<dev::KMAX>;
+    auto exact = a.k == 7 ? spin_pairs_exact<7, 7> : (a.k <= 8 ? spin_pairs_exact<8, 0> : spin_pairs_exact<dev::KMAX, 0>);
     const size_t slot_bytes = sizeof(double) * 64 * (size_t)a.k * a.k;  // two warps
     if (slot_bytes > 48 * 1024) {
         err = allow_dynamic_smem((const void*)exact, (int)slot_bytes);
