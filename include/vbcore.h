@@ -50,7 +50,9 @@ typedef struct vb_hs_plan vb_hs_plan;
  * context.hpp:68-104).  The context owns one non-blocking stream unless one is attached. */
 vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** out);
 vb_status vb_context_destroy(vb_context* ctx);
-/* Use the caller's cudaStream_t for all work of this context (NULL restores its own). */
+/* Use the caller's cudaStream_t for all work of this context (NULL restores its own).  Waits
+ * for the work already queued on the previous stream (the context's scratch memory is reused in
+ * stream order). */
 vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream);
 vb_status vb_context_synchronize(vb_context* ctx);
 /* Last error message of this context (or of the last failed create when ctx is NULL). */

@@ -180,7 +180,15 @@ vb_status vb_context_destroy(vb_context* ctx) {
 
 vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream) {
     if (!ctx) return VB_ERR_INVALID;
-    ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+    cudaStream_t next = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+    if (next != ctx->stream && ctx->stream) {
+        // the context's scratch and pool memory are reused in stream order: let the work queued
+        // on the previous stream finish before anything is queued on the new one
+        cudaSetDevice(ctx->device);
+        cudaError_t err = cudaStreamSynchronize(ctx->stream);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_context_set_stream");
+    }
+    ctx->stream = next;
     return VB_OK;
 }
 
