@@ -379,14 +379,21 @@ vb_status vb_active_transform_ri_adjoint(vb_context* ctx, const double* one_inde
  * than that are rejected with VB_ERR_BUDGET (about 250 strings of 5 electrons in 10 orbitals
  * fit; use the plan API above for larger ones).
  *
+ * At most 8 electrons per string (k > 8 returns VB_ERR_UNSUPPORTED: the stack reserved by the
+ * set-up call covers the exact-path kernels for k <= 8 only).
+ *
  * All pointers are device pointers: strings = n_strings occupation masks (k bits set, orbitals
  * < n_orbitals), S_act and h (n x n), packed (ij|kl); out_scalars receives, for pair index
  * t = u N - u (u - 1) / 2 + (v - u), {det, one-electron H, total same-spin H, nullity} at
  * out_scalars[4 t .. 4 t + 3].  The work is enqueued on `cuda_stream` (the output is complete
- * when the stream reaches it); the call synchronizes the stream once, midway, to read back
- * the pair-kernel rank.  The first call on a device looks up the scratch array's address
- * (cudaGetSymbolAddress) with that device current: make it before any stream capture.  Calls
- * share the array and keep its last contents; calls that overlap on the GPU race on it. */
+ * when the stream reaches it); every call synchronizes the stream once, midway, to read back
+ * the pair-kernel rank.  The first call made with a device current is that device's set-up
+ * call: it raises the device's stack limit to what the exact-path kernels need (later calls
+ * then never make the runtime grow the local-memory reservation), loads every kernel a call may
+ * launch (lazy module loading then places no code in device memory during a later call) and
+ * looks up the scratch array's address (cudaGetSymbolAddress).  Make that first call before
+ * any stream capture.  Calls share the array and keep its last contents;
+ * calls that overlap on the GPU race on it. */
 vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, int k, int n_strings, const uint64_t* strings,
                                 const double* ovlp_act, const double* h1e_act, const double* eri_packed,
                                 double* out_scalars);

@@ -81,6 +81,17 @@ cudaError_t allow_dynamic_smem(const void* kernel, size_t bytes) {
     return cudaSuccess;
 }
 
+cudaError_t reserve_kernel_stack() {
+    static std::mutex stack_mutex;
+    std::lock_guard<std::mutex> lock(stack_mutex);
+    const size_t need = std::max(exact_stack_bytes(), gradient_stack_bytes()) + 1024;
+    size_t have = 0;
+    cudaError_t err = cudaDeviceGetLimit(&have, cudaLimitStackSize);
+    if (err != cudaSuccess) return err;
+    if (have < need) err = cudaDeviceSetLimit(cudaLimitStackSize, need);
+    return err;
+}
+
 void* context_scratch(vb_context* ctx, int slot, size_t bytes, vb_status* status) {
     *status = VB_OK;
     if (bytes == 0) bytes = 16;
@@ -142,18 +153,9 @@ vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** ou
         ctx->pool = nullptr;
         cudaGetLastError();
     }
-    // Reserve the stack the exact-path kernels need once, up front: otherwise the runtime grows
-    // the device's local-memory reservation at their first launch, which can fail while other
-    // host threads (other contexts) have work in flight.
-    {
-        static std::mutex stack_mutex;
-        std::lock_guard<std::mutex> lock(stack_mutex);
-        const size_t need = std::max(vbcore::exact_stack_bytes(), vbcore::gradient_stack_bytes()) + 1024;
-        size_t have = 0;
-        if (cudaDeviceGetLimit(&have, cudaLimitStackSize) == cudaSuccess && have < need)
-            cudaDeviceSetLimit(cudaLimitStackSize, need);
-        cudaGetLastError();
-    }
+    // Reserve the stack the exact-path kernels need once, up front (reserve_kernel_stack).
+    reserve_kernel_stack();
+    cudaGetLastError();
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     ctx->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.9 * (double)free_b);
@@ -163,7 +165,7 @@ vb_status vb_context_create(int device, size_t hbm_budget_bytes, vb_context** ou
 
 vb_status vb_context_destroy(vb_context* ctx) {
     if (!ctx) return VB_OK;
-    cudaSetDevice(ctx->device);
+    DeviceGuard guard(ctx->device);
     for (int i = 0; i < 6; ++i) device_free(ctx, ctx->scratch[i], ctx->scratch_bytes[i]);
     if (ctx->own_stream) {
         cudaStreamSynchronize(ctx->own_stream);
@@ -183,8 +185,9 @@ vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream) {
     cudaStream_t next = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
     if (next != ctx->stream && ctx->stream) {
         // the context's scratch and pool memory are reused in stream order: let the work queued
-        // on the previous stream finish before anything is queued on the new one
-        cudaSetDevice(ctx->device);
+        // on the previous stream finish before anything is queued on the new one (the caller's
+        // current device is restored afterwards)
+        DeviceGuard guard(ctx->device);
         cudaError_t err = cudaStreamSynchronize(ctx->stream);
         if (err != cudaSuccess) return cuda_error(ctx, err, "vb_context_set_stream");
     }

@@ -41,6 +41,27 @@ constexpr int kMaxOrbitals = 64;
 vb_status set_error(vb_context* ctx, vb_status code, const std::string& message);
 vb_status cuda_error(vb_context* ctx, cudaError_t err, const char* what);
 
+// Makes `device` current for the lifetime of the guard and restores the caller's device after.
+struct DeviceGuard {
+    int previous = -1;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+        if (previous != device) cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (previous >= 0 && cudaGetDevice(&now) == cudaSuccess && now != previous) cudaSetDevice(previous);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
+// Raises the current device's per-thread stack limit (never lowers it) to what the exact-path
+// forward and gradient kernels need, under a process-wide lock.  Without it the runtime grows
+// the device's local-memory reservation at the first launch of those kernels, which can fail
+// while other host threads have work in flight.
+cudaError_t reserve_kernel_stack();
+
 // U^-1 of the Cholesky factor S = U^T U of a device matrix (linalg.cu); *info > 0 when the
 // leading minor of that order is not positive definite.  Synchronizes the context stream.
 vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double* Ui_out, int* info);

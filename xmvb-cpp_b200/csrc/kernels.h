@@ -114,6 +114,9 @@ size_t left_table_doubles(int n, int k, int R);
 size_t factored_spin_smem_bytes(int n, int k, int R);
 bool fast_spin_supported(int n, int k, int R);
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches);
+// Loads every kernel launch_spin_pairs and its table steps may use (under lazy module loading a
+// kernel is otherwise loaded, and its code placed in device memory, at its first launch).
+cudaError_t preload_spin_pair_kernels();
 cudaError_t launch_full_pairs(const FullPairArgs& a, cudaStream_t stream, int* launches);
 cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches);
 cudaError_t launch_structure_reduce(const StructureReduceArgs& a, double* H, double* S, cudaStream_t stream,

@@ -9,8 +9,12 @@
 // decomposition tables, register-resident spin-pair kernel, exact path) and takes all of its
 // scratch from one file-scope device array instead of cudaMalloc.
 //
-// The array's address is obtained once per device with cudaGetSymbolAddress, on the first
-// call made with that device current; make that first call before any stream capture.
+// The first call made with a device current is that device's set-up call: it raises the
+// device's stack limit to what the exact-path kernels need (so that later calls never make the
+// runtime grow the local-memory reservation), loads every kernel a call may launch (so that lazy
+// module loading places no code in device memory during a later call) and obtains the array's
+// address with cudaGetSymbolAddress; make that first call before any stream capture.  Every call reads the pair-kernel rank back to the host midway and
+// waits for the stream to reach that point.
 // Every call on a device shares the array, which keeps the last call's contents: the kernels
 // clear what must start at zero (the exact-path counter), and calls that overlap on the GPU
 // (different streams, or different host threads) race on the array.
@@ -89,6 +93,18 @@ __global__ void extract_scalars_kernel(const double* __restrict__ records, int s
 
 int record_stride_for(int R) { return (R + 4 + 1) / 2 * 2; }
 
+// Loads every kernel a call may launch, so that no later call loads code into device memory.
+cudaError_t preload_kernels() {
+    const void* own[] = {(const void*)occupation_rows_kernel, (const void*)spin_items_kernel,
+                         (const void*)extract_scalars_kernel};
+    for (const void* f : own) {
+        cudaFuncAttributes fa{};
+        const cudaError_t err = cudaFuncGetAttributes(&fa, f);
+        if (err != cudaSuccess) return err;
+    }
+    return preload_spin_pair_kernels();
+}
+
 }  // namespace
 }  // namespace vbcore
 
@@ -101,6 +117,11 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
     if (n < 1 || n > kMaxOrbitals || k < 1 || k > kMaxElectrons || k > n || n_strings < 1 || !strings || !ovlp_act ||
         !h1e_act || !eri_packed || !out_scalars)
         return set_error(nullptr, VB_ERR_INVALID, "vb_spin_pairs_noalloc: bad arguments");
+    // the exact-path stack reserved by the set-up call covers the instantiations for k <= 8; a
+    // larger k would make the runtime grow the local-memory reservation during the call
+    if (k > kMaxFastElectrons)
+        return set_error(nullptr, VB_ERR_UNSUPPORTED,
+                         "vb_spin_pairs_noalloc: at most 8 electrons per string (use the plan API for more)");
     const long long N = n_strings;
     const long long n_pairs = N * (N + 1) / 2;
     const int np = n * (n + 1) / 2, gd = n * (n - 1) / 2;
@@ -141,6 +162,12 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
     {
         std::lock_guard<std::mutex> lock(g_scratch_mutex);
         if (!g_scratch_address[device]) {
+            // set-up, once per device: the exact-path kernels' stack (so that no later call makes
+            // the runtime grow the device's local-memory reservation), then the array's address
+            err = reserve_kernel_stack();
+            if (err != cudaSuccess) return cuda_error(nullptr, err, "cudaDeviceSetLimit (kernel stack)");
+            err = preload_kernels();
+            if (err != cudaSuccess) return cuda_error(nullptr, err, "cudaFuncGetAttributes (kernel preload)");
             void* ptr = nullptr;
             err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (err != cudaSuccess) return cuda_error(nullptr, err, "cudaGetSymbolAddress (static scratch)");

@@ -913,6 +913,27 @@ size_t exact_stack_bytes() {
     return m;
 }
 
+cudaError_t preload_spin_pair_kernels() {
+    // cudaFuncGetAttributes loads a function that lazy module loading has not loaded yet
+    const void* fns[] = {(const void*)prepare_tables_kernel, (const void*)factor_pair_kernel,
+                         (const void*)left_string_tables<1>, (const void*)left_string_tables<2>,
+                         (const void*)left_string_tables<3>, (const void*)left_string_tables<4>,
+                         (const void*)left_string_tables<5>, (const void*)left_string_tables<6>,
+                         (const void*)left_string_tables<7>, (const void*)left_string_tables<8>,
+                         (const void*)spin_pairs_fast<1>, (const void*)spin_pairs_fast<2>,
+                         (const void*)spin_pairs_fast<3>, (const void*)spin_pairs_fast<4>,
+                         (const void*)spin_pairs_fast<5>, (const void*)spin_pairs_fast<6>,
+                         (const void*)spin_pairs_fast<7>, (const void*)spin_pairs_fast<8>,
+                         (const void*)spin_pairs_exact<7, 7>, (const void*)spin_pairs_exact<8, 0>,
+                         (const void*)spin_pairs_exact<dev::KMAX, 0>};
+    for (const void* f : fns) {
+        cudaFuncAttributes fa{};
+        const cudaError_t err = cudaFuncGetAttributes(&fa, f);
+        if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches) {
     if (a.n_pairs <= 0 || a.k <= 0) return cudaSuccess;
     cudaError_t err = cudaSuccess;
