@@ -55,6 +55,12 @@ vb_status vb_context_destroy(vb_context* ctx);
  * stream order). */
 vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream);
 vb_status vb_context_synchronize(vb_context* ctx);
+/* Polls a grid-barrier wait of the cooperative eigensolver kernels (vb_metric_cholesky,
+ * vb_generalized_eigh, the Davidson shift-invert factor) makes before it gives up: the kernel
+ * then ends and the call returns VB_ERR_TIMEOUT, with the context still usable.  0 restores the
+ * built-in default (2^26 polls, seconds).  No reference counterpart: the reference's solvers are
+ * library calls (dsygvd) without a device-side wait. */
+vb_status vb_context_set_barrier_spin_limit(vb_context* ctx, long long polls);
 /* Last error message of this context (or of the last failed create when ctx is NULL). */
 const char* vb_last_error(const vb_context* ctx);
 /* Bytes currently allocated by the context and the peak (reference: gpu_peak_device_bytes,

@@ -60,6 +60,8 @@ def lib():
         _lib.oracle_structure_matrices.argtypes = [i, i, i, p, i, p, p, p, p, i, p, p, p, d, i, ll, p, p]
         _lib.oracle_structure_matrices.restype = ll
         _lib.oracle_ri_transform.argtypes = [i, i, i, p, p, i, p, p]
+        _lib.oracle_cached_structure_matrices.argtypes = [i, i, i, p, i, i, p, i, i, p, p, p, p, p, i, p, p, p, d,
+                                                          i, i, p, p, p]
     return _lib
 
 
@@ -180,6 +182,33 @@ def structure_matrices(n, expansion: "Expansion", S, h, eri, threads: int = 0, p
                                              _ptr(Sf), _ptr(hf), _ptr(ef), threshold, threads, int(pair_limit),
                                              _ptr(Hs), _ptr(Ss))
     return Hs.T.copy(), Ss.T.copy(), int(npairs)
+
+
+def cached_structure_matrices(n, expansion: "Expansion", S, h, eri, threads: int = 0, det_rows: int = 0,
+                              threshold: float = THRESHOLD):
+    """Structure H and S by the reference's cached CPU algorithm (ordered spin-pair cache with
+    projected images, then a sparse dot per ordered determinant pair).  det_rows > 0 evaluates only
+    the determinant rows d < det_rows (partial result, for timing).  Returns (H, S, timings) with
+    timings = dict(cache_s, cache_entries, pairs_s, pairs)."""
+    a_occ = _i32(np.array([_occ(m) for m in expansion.alpha_strings], dtype=np.int32).reshape(
+        len(expansion.alpha_strings), expansion.n_alpha))
+    b_occ = _i32(np.array([_occ(m) for m in expansion.beta_strings], dtype=np.int32).reshape(
+        len(expansion.beta_strings), expansion.n_beta))
+    shared = int(expansion.n_alpha == expansion.n_beta and list(expansion.alpha_strings) == list(expansion.beta_strings))
+    da, db = _i32(expansion.det_alpha), _i32(expansion.det_beta)
+    off = np.ascontiguousarray(expansion.offsets, dtype=np.int64)
+    ts = _i32(expansion.term_structure)
+    tc = _f64(expansion.term_coefficient)
+    Sf, hf, ef = _f64(np.asarray(S).T.reshape(-1)), _f64(np.asarray(h).T.reshape(-1)), _f64(eri)
+    ns = expansion.n_structures
+    Hs = np.zeros((ns, ns))
+    Ss = np.zeros((ns, ns))
+    tm = np.zeros(4)
+    lib().oracle_cached_structure_matrices(n, expansion.n_alpha, a_occ.shape[0], _ptr(a_occ), expansion.n_beta,
+                                           b_occ.shape[0], _ptr(b_occ), shared, len(da), _ptr(da), _ptr(db),
+                                           _ptr(off), _ptr(ts), _ptr(tc), ns, _ptr(Sf), _ptr(hf), _ptr(ef),
+                                           threshold, threads, int(det_rows), _ptr(Hs), _ptr(Ss), _ptr(tm))
+    return Hs.T.copy(), Ss.T.copy(), dict(cache_s=tm[0], cache_entries=int(tm[1]), pairs_s=tm[2], pairs=int(tm[3]))
 
 
 def ri_transform(B_packed: np.ndarray, C: np.ndarray, threads: int = 0):

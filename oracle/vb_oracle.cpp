@@ -20,6 +20,12 @@
 //   * full pair: src/vbscf/determinants/pairs/evaluator.cpp:354-384, 421-466
 //   * structure H/S: src/vbscf/structures/assembly/hamiltonian_overlap.cpp:890-1022
 //     (H_IJ = sum_{d in I, e in J} c_d c_e H_de; any deterministic FP64 order)
+//   * cached evaluation (the reference's CPU hot-loop shape, the timed CPU baseline):
+//     build_same_spin_pair_cache, src/vbscf/determinants/pairs/same_spin_cache.cpp:430-477
+//     (every ordered spin pair of a string table, OpenMP dynamic,1 over left strings), with the
+//     sparse packed-pair projection and its dense image over the pair kernel
+//     (same_spin_cache.cpp:166-182, 186-284), and per determinant pair the sparse dot
+//     contract_sparse_projection_with_dense_image, contractions.cpp:136-147
 //   * packed indices: src/core/pair_index.cpp:10-44
 //   * RI transform: src/integrals/ao/ri_transform.cpp:10-37,
 //     src/integrals/active/ri.cpp:13-96
@@ -29,6 +35,7 @@
 // (src/vbscf/determinants/contracts/types.hpp:13-15, 62-66).
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -494,6 +501,67 @@ PairResult full_pair(int n, int ka, const int* aL, const int* aR, int kb, const 
     return out;
 }
 
+// The ordered spin-pair cache (same_spin_cache.cpp:430-477) in flat arrays: per entry the
+// resolved overlap's determinant, the same-spin energy, and the opposite-spin payload: the sparse
+// projection p_q = sum_{pair(R_r, L_c) = q} A(r, c) of the first cofactors onto packed pairs, in
+// first-touch order (left column outer, right row inner) without exact zeros, and its dense image
+// K p over the packed pair kernel (same_spin_cache.cpp:186-284).
+struct SpinCache {
+    int kk = 0, np = 0;
+    std::vector<double> det, htot, val, image;
+    std::vector<int> nnz, idx;
+    void resize(size_t entries, int k, int n_pairs) {
+        kk = std::max(1, k * k);
+        np = n_pairs;
+        det.assign(entries, 0.0);
+        htot.assign(entries, 0.0);
+        nnz.assign(entries, 0);
+        idx.assign(entries * kk, 0);
+        val.assign(entries * kk, 0.0);
+        image.assign(entries * (size_t)np, 0.0);
+    }
+};
+
+void build_cache_entry(int n, int k, const int* occL, const int* occR, const double* S, const double* h,
+                       const double* eri, const double* kdense, double thr, SpinCache* cache, size_t e,
+                       std::vector<double>& dense, std::vector<char>& touched, std::vector<int>& order) {
+    const int np = cache->np;
+    SpinPair sp = prepare_spin_pair(n, k, occL, occR, S, thr);
+    if (k > 0 && sp.res.nullity < 3) same_spin_h(n, k, occL, occR, h, eri, &sp);
+    cache->det[e] = k > 0 ? sp.res.det : 1.0;
+    cache->htot[e] = sp.htot;
+    cache->nnz[e] = 0;
+    if (k == 0 || sp.res.nullity >= 2) return;
+    order.clear();
+    for (int c = 0; c < k; ++c)
+        for (int r = 0; r < k; ++r) {
+            const int q = (int)pair_index(occR[r], occL[c]);
+            if (!touched[q]) {
+                touched[q] = 1;
+                dense[q] = 0.0;
+                order.push_back(q);
+            }
+            dense[q] += sp.cof[c * k + r];
+        }
+    int* ix = &cache->idx[e * cache->kk];
+    double* vx = &cache->val[e * cache->kk];
+    int m = 0;
+    for (int q : order) {
+        touched[q] = 0;
+        if (dense[q] != 0.0) {
+            ix[m] = q;
+            vx[m++] = dense[q];
+        }
+    }
+    cache->nnz[e] = m;
+    double* img = &cache->image[e * (size_t)np];
+    for (int t = 0; t < m; ++t) {
+        const double* col = kdense + (size_t)ix[t] * np;
+        const double v = vx[t];
+        for (int row = 0; row < np; ++row) img[row] += col[row] * v;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -637,6 +705,130 @@ long long oracle_structure_matrices(int n, int n_det, int ka, const int* alpha_o
             Ss[i] += accS[t][i];
         }
     return total;
+}
+
+// Cached structure H/S in the shape of the reference's CPU hot loop: first the ordered spin-pair
+// cache (one entry per (left, right) string pair, OpenMP dynamic,1 over left strings), then every
+// ordered determinant pair (d, e) as S = S_a S_b, H = H_a S_b + H_b S_a + p_a . (K p_b) over the
+// cached entries, accumulated into the structure matrices.  String tables: a_occ (Na x ka),
+// b_occ (Nb x kb); shared != 0 when both spins use the same table (one cache serves both).
+// Determinants: det_a/det_b string ids.  n_det_rows > 0 restricts the work to the determinant rows
+// d < n_det_rows (and the cache to the left strings those rows use): a bounded sample for timing,
+// with a partial result.  timings[0..3] = {cache seconds, cache entries, pair seconds, ordered
+// determinant pairs}.
+void oracle_cached_structure_matrices(int n, int ka, int Na, const int* a_occ, int kb, int Nb, const int* b_occ,
+                                      int shared, int n_det, const int* det_a, const int* det_b,
+                                      const long long* off, const int* term_struct, const double* term_coef,
+                                      int n_str, const double* S, const double* h, const double* eri,
+                                      double threshold, int n_threads, int n_det_rows, double* Hs, double* Ss,
+                                      double* timings) {
+    const int np = n * (n + 1) / 2;
+    std::vector<double> kdense((size_t)np * np);
+    for (int col = 0; col < np; ++col)
+        for (int row = 0; row < np; ++row) kdense[(size_t)col * np + row] = eri[pair_index(row, col)];
+    const int rows = (n_det_rows > 0 && n_det_rows < n_det) ? n_det_rows : n_det;
+    // left strings whose cache rows the sampled determinant rows need
+    std::vector<int> slot_a(Na, -1), slot_b(Nb, -1), left_a, left_b;
+    for (int d = 0; d < rows; ++d) {
+        if (slot_a[det_a[d]] < 0) {
+            slot_a[det_a[d]] = (int)left_a.size();
+            left_a.push_back(det_a[d]);
+        }
+        if (shared) {
+            if (slot_a[det_b[d]] < 0) {
+                slot_a[det_b[d]] = (int)left_a.size();
+                left_a.push_back(det_b[d]);
+            }
+        } else if (slot_b[det_b[d]] < 0) {
+            slot_b[det_b[d]] = (int)left_b.size();
+            left_b.push_back(det_b[d]);
+        }
+    }
+    if (n_threads > 0) {
+#ifdef _OPENMP
+        omp_set_num_threads(n_threads);
+#endif
+    }
+    SpinCache cache_a, cache_b;
+    cache_a.resize(left_a.size() * (size_t)Na, ka, np);
+    cache_b.resize(left_b.size() * (size_t)Nb, kb, np);
+    const auto t0 = std::chrono::steady_clock::now();
+    auto fill = [&](const std::vector<int>& left, int N, int k, const int* occ, SpinCache& cache) {
+#ifdef _OPENMP
+#pragma omp parallel
+#endif
+        {
+            std::vector<double> dense(np, 0.0);
+            std::vector<char> touched(np, 0);
+            std::vector<int> order;
+            order.reserve(std::max(1, k * k));
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+            for (long long li = 0; li < (long long)left.size(); ++li)
+                for (int v = 0; v < N; ++v)
+                    build_cache_entry(n, k, occ + (size_t)left[li] * k, occ + (size_t)v * k, S, h, eri, kdense.data(),
+                                      threshold, &cache, (size_t)li * N + v, dense, touched, order);
+        }
+    };
+    fill(left_a, Na, ka, a_occ, cache_a);
+    if (!shared) fill(left_b, Nb, kb, b_occ, cache_b);
+    const auto t1 = std::chrono::steady_clock::now();
+    const size_t ns2 = (size_t)n_str * n_str;
+    int nt = 1;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    std::vector<std::vector<double>> accH(nt, std::vector<double>(ns2, 0.0)), accS(nt, std::vector<double>(ns2, 0.0));
+    const std::vector<int>& sb = shared ? slot_a : slot_b;
+    const SpinCache& cb = shared ? cache_a : cache_b;
+    const int Nbb = shared ? Na : Nb;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int d = 0; d < rows; ++d) {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double* aH = accH[tid].data();
+        double* aS = accS[tid].data();
+        const size_t rowa = (size_t)slot_a[det_a[d]] * Na;
+        const size_t rowb = (size_t)sb[det_b[d]] * Nbb;
+        for (int e = 0; e < n_det; ++e) {
+            const size_t ea = rowa + det_a[e], eb = rowb + det_b[e];
+            const double s_de = cache_a.det[ea] * cb.det[eb];
+            double h_de = cache_a.htot[ea] * cb.det[eb] + cb.htot[eb] * cache_a.det[ea];
+            const int m = cache_a.nnz[ea];
+            if (m > 0 && cb.nnz[eb] > 0) {
+                const int* ix = &cache_a.idx[ea * cache_a.kk];
+                const double* vx = &cache_a.val[ea * cache_a.kk];
+                const double* img = &cb.image[eb * (size_t)cb.np];
+                double opp = 0.0;
+                for (int t = 0; t < m; ++t) opp += vx[t] * img[ix[t]];
+                h_de += opp;
+            }
+            for (long long td = off[d]; td < off[d + 1]; ++td)
+                for (long long te = off[e]; te < off[e + 1]; ++te) {
+                    const size_t I = term_struct[td], J = term_struct[te];
+                    const double w = term_coef[td] * term_coef[te];
+                    aH[J * n_str + I] += w * h_de;
+                    aS[J * n_str + I] += w * s_de;
+                }
+        }
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    std::fill(Hs, Hs + ns2, 0.0);
+    std::fill(Ss, Ss + ns2, 0.0);
+    for (int t = 0; t < nt; ++t)
+        for (size_t i = 0; i < ns2; ++i) {
+            Hs[i] += accH[t][i];
+            Ss[i] += accS[t][i];
+        }
+    timings[0] = std::chrono::duration<double>(t1 - t0).count();
+    timings[1] = (double)(cache_a.det.size() + cache_b.det.size());
+    timings[2] = std::chrono::duration<double>(t2 - t1).count();
+    timings[3] = (double)rows * n_det;
 }
 
 // RI transform: B packed [n_aux x n_bf(n_bf+1)/2] column-major (row = aux function, column = AO

@@ -155,3 +155,29 @@ def test_lowest_root_random(ctx):
     S = O.conditioned_metric(n, 1e3, seed=13)
     E, c, its = vbcore.lowest_root(ctx, H, S, tolerance=1e-11, max_iterations=3000)
     assert abs(E - O.generalized_eigh(H, S)[0][0]) < 1e-9 * max(1.0, abs(E))
+
+
+def test_grid_barrier_timeout_is_reported_and_the_context_stays_usable():
+    """The cooperative solver's grid barrier gives up after a bounded number of polls: with a
+    one-poll limit the waits run out, the kernel ends and the call returns VB_ERR_TIMEOUT (no
+    trap, no hang); after the default limit is restored the same context solves the problem."""
+    c = vbcore.Context(0)
+    try:
+        n = 200  # above the one-CTA size: a grid-wide cooperative launch with a grid barrier
+        H = _random_symmetric(n, 7)
+        S = O.conditioned_metric(n, 1e3, seed=8)
+        c.set_barrier_spin_limit(1)
+        with pytest.raises(vbcore.VbError) as e:
+            vbcore.generalized_eigh(c, H, S)
+        assert e.value.status == 6 and "grid barrier timed out" in str(e.value)
+        with pytest.raises(vbcore.VbError) as e:
+            vbcore.metric_cholesky(c, S)
+        assert e.value.status == 6
+        c.set_barrier_spin_limit(0)
+        w, _ = vbcore.generalized_eigh(c, H, S)
+        wr, _ = O.generalized_eigh(H, S)
+        assert np.abs(w - wr).max() < 1e-11 * np.abs(wr).max()
+        with pytest.raises(vbcore.VbError):
+            c.set_barrier_spin_limit(-1)
+    finally:
+        c.close()

@@ -164,35 +164,25 @@ def test_reproducible_and_device_path(ctx):
     assert np.array_equal(tH.cpu().numpy().T, H1) and np.array_equal(tSo.cpu().numpy().T, S1)
 
 
-def _structure_elements_oracle(ex, n, S, h, eri, pairs_IJ):
-    """H_IJ, S_IJ for selected structure pairs from the oracle on the determinants involved."""
-    T = ex.coefficient_matrix()
-    out = []
-    for I, J in pairs_IJ:
-        dets = np.nonzero((T[:, I] != 0) | (T[:, J] != 0))[0]
-        Hd, Sd = O.determinant_matrices(n, ex.det_alpha_occ[dets], ex.det_beta_occ[dets], S, h, eri)
-        cI, cJ = T[dets, I], T[dets, J]
-        out.append((cI @ Hd @ cJ, cI @ Sd @ cJ))
-    return np.array(out)
-
-
 def test_full_size_microbenchmark_properties(ctx):
-    """n_active = 14, 3432 determinants, 429 structures (the microbenchmark shape): sampled
-    elements against the oracle, plus size-independent properties (symmetry, positive metric,
-    linearity of H in (h, (ij|kl)))."""
+    """n_active = 14, 3432 determinants, 429 structures (the microbenchmark shape): every one of
+    the 429 x 429 H and S elements against the oracle (all 5,891,028 unordered determinant pairs,
+    all host threads), plus size-independent properties (symmetry, positive metric, linearity of H
+    in (h, (ij|kl)))."""
+    import os
+
     n = 14
     S, h, eri = workloads.active_space(n, 42, 2026)
     plan, ex = _plan(ctx, "COV", n, n)
     H, So = plan.execute(S, h, eri)
     assert H.shape == (429, 429)
-    rng = np.random.default_rng(1)
-    sample = [(0, 0), (428, 428), (0, 428)] + [tuple(rng.integers(0, 429, 2)) for _ in range(5)]
-    ref = _structure_elements_oracle(ex, n, S, h, eri, sample)
-    scale_h = max(1.0, np.abs(H).max())
-    scale_s = max(1.0, np.abs(So).max())
-    for (I, J), (hr, sr) in zip(sample, ref):
-        assert abs(H[I, J] - hr) <= REL * scale_h
-        assert abs(So[I, J] - sr) <= REL * scale_s
+    ex_o = O.expand(O.generate_structures("COV", n, n), n)
+    Hr, Sr, done = O.structure_matrices(n, ex_o, S, h, eri, threads=os.cpu_count() or 1)
+    assert done == 3432 * 3433 // 2
+    scale_h = max(1.0, np.abs(Hr).max())
+    scale_s = max(1.0, np.abs(Sr).max())
+    assert np.abs(H - Hr).max() <= REL * scale_h
+    assert np.abs(So - Sr).max() <= REL * scale_s
     assert np.array_equal(H, H.T)
     assert np.linalg.eigvalsh(So).min() > 0
     H1, S1 = plan.execute(S, h, np.zeros_like(eri))

@@ -195,6 +195,12 @@ vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream) {
     return VB_OK;
 }
 
+vb_status vb_context_set_barrier_spin_limit(vb_context* ctx, long long polls) {
+    if (!ctx || polls < 0) return set_error(ctx, VB_ERR_INVALID, "vb_context_set_barrier_spin_limit: bad arguments");
+    ctx->barrier_spin_limit = polls;
+    return VB_OK;
+}
+
 vb_status vb_context_synchronize(vb_context* ctx) {
     if (!ctx) return VB_ERR_INVALID;
     cudaError_t err = cudaStreamSynchronize(ctx->stream);

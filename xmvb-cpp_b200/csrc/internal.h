@@ -20,6 +20,7 @@ struct vb_context {
     void* scratch[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     size_t scratch_bytes[6] = {0, 0, 0, 0, 0, 0};
     size_t budget = 0;
+    long long barrier_spin_limit = 0;  // grid-barrier polls before a timeout (0: the built-in default)
     size_t current = 0;
     size_t peak = 0;
     std::string last_error;

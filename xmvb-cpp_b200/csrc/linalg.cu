@@ -36,7 +36,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kTile = 32;
-constexpr long long kBarrierSpinLimit = 1ll << 26;  // ~ seconds with 64 ns sleeps
+constexpr long long kBarrierSpinLimit = 1ll << 26;  // default: ~ seconds with 64 ns sleeps
 constexpr int kMaxSweeps = 60;
 constexpr int kSmallProblem = 96;  // single-problem calls at or below this size use one CTA
 
@@ -66,6 +66,7 @@ struct EighArgs {
     double* evals;       // n
     double* evecs;       // n x n
     Control* ctl;        // zero-initialised
+    long long spin_limit;  // polls a grid-barrier wait makes before it gives up (ctl->err = 1)
 };
 
 struct BlockSync {
@@ -75,9 +76,13 @@ struct BlockSync {
     }
 };
 
+// Grid barrier whose waits are bounded: a CTA that polls `spin_limit` times without the barrier
+// opening sets ctl->err and leaves; every other waiting CTA leaves as soon as it sees err, so the
+// kernel always ends and the host reads VB_ERR_TIMEOUT.
 struct GridSync {
     Control* ctl;
     unsigned nblocks;
+    long long spin_limit;
     __device__ bool operator()() const {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -91,10 +96,11 @@ struct GridSync {
             } else {
                 long long spins = 0;
                 while (*gen == g) {
-                    if (++spins > kBarrierSpinLimit) {
+                    if (++spins > spin_limit) {
                         atomicExch(&ctl->err, 1);
                         break;
                     }
+                    if (*(volatile int*)&ctl->err) break;
                     __nanosleep(64);
                 }
             }
@@ -641,7 +647,7 @@ __device__ void eigh_body(const EighArgs& a, const Sync& sync, Shared& sh, int c
 
 __global__ void __launch_bounds__(kThreads) eigh_grid_kernel(EighArgs a) {
     __shared__ Shared sh;
-    GridSync sync{a.ctl, gridDim.x};
+    GridSync sync{a.ctl, gridDim.x, a.spin_limit};
     eigh_body(a, sync, sh, blockIdx.x, gridDim.x);
 }
 
@@ -723,6 +729,7 @@ EighArgs args_for(unsigned char* base, const Layout& L, int n, int mode, const d
         a.evecs = evecs;
     }
     a.ctl = reinterpret_cast<Control*>(base + L.ctl);
+    a.spin_limit = kBarrierSpinLimit;
     return a;
 }
 
@@ -793,6 +800,7 @@ vb_status run_single(vb_context* ctx, int mode, const double* H, const double* S
     if (err == cudaSuccess) err = clear_workspace(base, L, n, mode, s);
     if (err != cudaSuccess) return cuda_error(ctx, err, name);
     EighArgs a = args_for(base, L, n, mode, dH, dS, dvals, dvecs, mode == 0 ? dU : nullptr);
+    if (ctx->barrier_spin_limit > 0) a.spin_limit = ctx->barrier_spin_limit;
     int grid = 0;
     std::unique_lock<std::mutex> coop(g_cooperative, std::defer_lock);
     if (n > kSmallProblem) coop.lock();
@@ -841,6 +849,7 @@ vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double*
     cudaError_t err = clear_workspace(base, L, n, 2, s);
     if (err != cudaSuccess) return cuda_error(ctx, err, "factor_inverse_device");
     EighArgs a = args_for(base, L, n, 2, nullptr, M, nullptr, nullptr, nullptr);
+    if (ctx->barrier_spin_limit > 0) a.spin_limit = ctx->barrier_spin_limit;
     int grid = 0;
     std::unique_lock<std::mutex> coop(g_cooperative, std::defer_lock);
     if (n > kSmallProblem) coop.lock();

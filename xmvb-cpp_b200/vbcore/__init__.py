@@ -81,7 +81,8 @@ class _HsStats(ctypes.Structure):
 
 # every symbol include/vbcore.h declares
 EXPORTED_SYMBOLS = (
-    "vb_context_create", "vb_context_destroy", "vb_context_set_stream", "vb_context_synchronize", "vb_last_error",
+    "vb_context_create", "vb_context_destroy", "vb_context_set_stream", "vb_context_synchronize",
+    "vb_context_set_barrier_spin_limit", "vb_last_error",
     "vb_context_memory", "vb_generate_structures", "vb_expand_structures", "vb_hs_plan_create",
     "vb_hs_plan_destroy", "vb_hs_plan_execute", "vb_hs_plan_stats", "vb_resolve_overlaps", "vb_same_spin_pairs",
     "vb_hs_plan_determinant_pairs", "vb_hs_plan_enable_phase_timing", "vb_hs_plan_phase_times",
@@ -113,6 +114,7 @@ def load_library(path: str = LIB_PATH):
     lib.vb_context_destroy.argtypes = [P]
     lib.vb_context_set_stream.argtypes = [P, P]
     lib.vb_context_synchronize.argtypes = [P]
+    lib.vb_context_set_barrier_spin_limit.argtypes = [P, c.c_longlong]
     lib.vb_last_error.argtypes = [P]
     lib.vb_last_error.restype = c.c_char_p
     lib.vb_context_memory.argtypes = [P, c.POINTER(c.c_size_t), c.POINTER(c.c_size_t)]
@@ -277,6 +279,11 @@ class Context:
 
     def synchronize(self):
         _check(load_library().vb_context_synchronize(self._h), self._h)
+
+    def set_barrier_spin_limit(self, polls: int):
+        """Polls a grid-barrier wait of the cooperative eigensolver kernels makes before the call
+        gives up with VB_ERR_TIMEOUT (0: the built-in default)."""
+        _check(load_library().vb_context_set_barrier_spin_limit(self._h, int(polls)), self._h)
 
     def memory(self):
         cur, peak = ctypes.c_size_t(), ctypes.c_size_t()
