@@ -388,7 +388,7 @@ def run_vbcore(args):
     spin_units = n_strings * (n_strings + 1) // 2
     det_units = stats["determinant_pairs"]  # orbit representatives under the alpha/beta exchange
     kernels = {
-        "spin_pairs": ("spin_pairs_fast", spin_units * flops_spin_pair(k), spin_units),
+        "spin_pairs": ("spin_pairs_frame", spin_units * flops_spin_pair(k), spin_units),
         "determinant_pairs": ("full_pairs_kernel", det_units * flops_full_pair(k, k), det_units),
     }
     dominant = max(kernels, key=lambda name: mean_phase[name])

@@ -292,10 +292,41 @@ typedef struct {
 vb_status vb_ao_integrals_s(const vb_scf_input* input, double* S_ao, double* h_ao, double* eri_ao,
                             double* nuclear_repulsion);
 vb_status vb_scf_problem_create(vb_context* ctx, const vb_scf_input* input, vb_scf_problem** problem);
+/* The same problem from AO integrals the caller already has (the reference computes them with
+ * libcint and hands them to xmvb::cuda::solve_scf(Context&, const VbScfInput&, AoPairGraph&&,
+ * double nuclear_repulsion, const VbScfOptimizerOptions&, observe), src/cuda/vb/scf.hpp:41-46):
+ * any basis (s, p, d ...), the AO overlap and core Hamiltonian, and the two-electron integrals as
+ * the AoPairGraph's unique-integral stream (src/integrals/ao/input.hpp:36-60): AO pairs
+ * (pair_first[p], pair_second[p]) and entries (integral_rows[t], integral_columns[t],
+ * integral_values[t]) = (pair row | pair column), each unordered pair of pairs once; absent
+ * entries are zero.  The pair matrix is factored once by pivoted Cholesky (to 1e-15 of its
+ * largest diagonal), so every evaluation runs the device RI path.  Host buffers, copied. */
+typedef struct {
+    int32_t n_basis;
+    const double* S_ao;  /* n_bf x n_bf, column-major */
+    const double* h_ao;  /* core Hamiltonian, n_bf x n_bf */
+    int64_t n_pairs;
+    const int32_t* pair_first;
+    const int32_t* pair_second;
+    int64_t n_integrals;
+    const int64_t* integral_rows;
+    const int64_t* integral_columns;
+    const double* integral_values;
+    double nuclear_repulsion;
+    int32_t n_active;
+    const int32_t* orbital_offsets; /* CSR: basis functions orbital a may use */
+    const int32_t* orbital_functions;
+    int32_t n_electrons;
+    int32_t multiplicity;
+    const char* structures;         /* STR= keyword, e.g. "COV" */
+} vb_scf_integral_input;
+vb_status vb_scf_problem_create_from_integrals(vb_context* ctx, const vb_scf_integral_input* input,
+                                               vb_scf_problem** problem);
 vb_status vb_scf_problem_destroy(vb_scf_problem* problem);
 vb_status vb_scf_problem_sizes(const vb_scf_problem* problem, int* n_basis, int* n_active, int* n_structures,
                                double* nuclear_repulsion);
-/* AO overlap, core Hamiltonian (n_bf x n_bf) and full (mu nu|la si) (n_bf^4), host buffers. */
+/* AO overlap, core Hamiltonian (n_bf x n_bf) and full (mu nu|la si) (n_bf^4), host buffers
+ * (for a problem built from AO integrals, the two-electron integrals of its pair factors). */
 vb_status vb_scf_ao_integrals(const vb_scf_problem* problem, double* S_ao, double* h_ao, double* eri_ao);
 /* Total energy at coefficients C (n_bf x n_act, column-major, entries outside each orbital's
  * basis functions ignored), and optionally dE/dC (same shape, zero outside the pattern) and
@@ -373,6 +404,17 @@ vb_status vb_active_transform_ri_precision(vb_context* ctx, const double* B_pack
  * (src/integrals/response/ri.cpp:370). */
 vb_status vb_active_transform_ri_adjoint(vb_context* ctx, const double* one_index, const double* dL, int n_aux,
                                          int n_bf, int n_act, int mem_space, double* dC);
+
+/* ---- launch-schedule autotuner ---------------------------------------------------------------- */
+
+/* No counterpart in the reference.  The first evaluation of a shape (electrons per string, active
+ * orbitals, factor rank) on a device times the launch variants of the spin-pair kernel (warps per
+ * CTA x CTAs per SM) and of the determinant-pair kernel (block size x blocks per SM) with CUDA
+ * events and keeps the fastest for the process; the environment variable VBCORE_AUTOTUNE=0 keeps
+ * the default schedules.  The report lists one line per tuned key ("key -> variant (ms: ...)");
+ * `needed` receives its length + 1. */
+vb_status vb_autotune_report(char* buffer, size_t capacity, size_t* needed);
+vb_status vb_autotune_clear(void);
 
 /* ---- allocation-free spin-pair evaluation ------------------------------------------------- */
 

@@ -189,3 +189,54 @@ def test_full_size_microbenchmark_properties(ctx):
     H2, S2 = plan.execute(S, np.zeros_like(h), eri)
     assert np.array_equal(S1, So) and np.array_equal(S2, So)
     assert np.abs(H1 + H2 - H).max() <= 1e-12 * scale_h
+
+
+@pytest.mark.parametrize("kw,n,nel", [("COV", 8, 6), ("COV", 10, 8), ("COV ION(1)", 6, 2), ("COV", 5, 2),
+                                      ("FULL", 5, 4), ("COV ION(1)", 7, 6)])
+def test_more_orbitals_than_electrons(ctx, kw, n, nel):
+    """Active spaces with n > 2k (complements larger than the strings): every excitation level
+    from 0 to min(k, n - k) occurs in the frame kernel."""
+    S, h, eri = workloads.active_space(n, 3 * n, 40 + n + nel)
+    plan, ex = _plan(ctx, kw, n, nel)
+    H, So = plan.execute(S, h, eri)
+    Hr, Sr, _ = O.structure_matrices(n, ex, S, h, eri)
+    assert _rel(H, Hr) < REL and _rel(So, Sr) < REL
+
+
+@pytest.mark.parametrize("n,k", [(3, 1), (6, 2), (7, 3), (8, 4), (9, 5), (10, 6), (10, 7), (11, 8), (9, 8)])
+def test_spin_pair_records_every_electron_count(n, k):
+    """Every spin pair of a complete string table (det, one-electron and total same-spin energy,
+    nullity) against the oracle for k = 1 .. 8, through the allocation-free entry point (which
+    returns the record scalars of the same kernels); one random and one stretched overlap."""
+    import itertools
+
+    import torch
+
+    masks = sorted(sum(1 << o for o in occ) for occ in itertools.combinations(range(n), k))
+    N = len(masks)
+    n_pairs = N * (N + 1) // 2
+    occ = [[o for o in range(n) if (m >> o) & 1] for m in masks]
+    S0, h, eri = workloads.active_space(n, 2 * n, 90 + 10 * n + k)
+    idx = np.arange(n)
+    S1 = np.exp(-0.8 * np.abs(idx[:, None] - idx[None, :]))  # overlaps decaying along a chain
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(n * 100 + k)
+    sample = rng.choice(n_pairs, size=min(n_pairs, 3000), replace=False)
+    for S in (S0, S1):
+        d_masks = torch.tensor(np.array(masks, dtype=np.uint64).view(np.int64), device=dev)
+        dS = torch.tensor(np.ascontiguousarray(S.T), device=dev)
+        dh = torch.tensor(np.ascontiguousarray(h.T), device=dev)
+        de = torch.tensor(eri, device=dev)
+        out = torch.full((4 * n_pairs,), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        vbcore.spin_pairs_noalloc(torch.cuda.current_stream(dev).cuda_stream, n, k, N, d_masks.data_ptr(),
+                                  dS.data_ptr(), dh.data_ptr(), de.data_ptr(), out.data_ptr())
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().reshape(n_pairs, 4)
+        uu = np.repeat(np.arange(N), np.arange(N, 0, -1))
+        vv = np.concatenate([np.arange(u, N) for u in range(N)])
+        for t in sample:
+            ref = O.spin_pair(n, occ[uu[t]], occ[vv[t]], S, h, eri)
+            assert int(got[t, 3]) == ref["nullity"]
+            for col, key in ((0, "det"), (1, "h1"), (2, "htot")):
+                assert abs(got[t, col] - ref[key]) <= REL * max(1.0, abs(ref[key])), (n, k, t, key)

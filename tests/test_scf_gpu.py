@@ -70,3 +70,36 @@ def test_solve_converges_to_the_oracle_minimum(ctx, h6):
     assert np.abs(G - oracle.gradient(C)).max() < 1e-7
     assert np.abs(G).max() < 1e-6
     prob.close()
+
+
+@pytest.mark.parametrize("threshold", [0.0, 1e-12])
+def test_integral_input_matches_shell_input(ctx, h6, threshold):
+    """The problem built from AO integrals the caller already has (an AO pair graph's unique
+    integral stream, the reference solve_scf's input) evaluates the same energy and gradient as
+    the problem that computes its own integrals, and converges to the same minimum."""
+    mol, pattern, oracle = h6
+    a = vbcore.ScfProblem(ctx, mol, pattern, 6)
+    S, h, eri, enuc = vbcore.ao_integrals_s(mol)
+    ints = dict(S_ao=S, h_ao=h, nuclear_repulsion=enuc, **vbcore.ao_pair_graph(eri, threshold))
+    b = vbcore.ScfProblem(ctx, None, pattern, 6, integrals=ints)
+    assert (b.n_basis, b.n_active, b.n_structures) == (a.n_basis, a.n_active, a.n_structures)
+    assert b.nuclear_repulsion == a.nuclear_repulsion
+    tol = 1e-12 if threshold == 0.0 else 1e-10
+    C = molecules.hao_guess(mol, pattern)
+    rng = np.random.default_rng(5)
+    mask = np.zeros_like(C)
+    for o, funcs in enumerate(pattern):
+        mask[funcs, o] = 1.0
+    for _ in range(2):
+        Ea, Ga = a.energy_gradient(C)
+        Eb, Gb = b.energy_gradient(C)
+        assert abs(Ea - Eb) < tol
+        assert np.abs(Ga - Gb).max() < 100 * tol
+        C = C + 0.05 * rng.standard_normal(C.shape) * mask
+    C0 = molecules.hao_guess(mol, pattern)
+    ra, _ = a.solve(C0, gradient_tolerance=1e-7)
+    rb, _ = b.solve(C0, gradient_tolerance=1e-7)
+    assert ra["converged"] and rb["converged"]
+    assert abs(ra["energy"] - rb["energy"]) < 1e-9
+    a.close()
+    b.close()

@@ -7,8 +7,6 @@
 #include <mutex>
 #include <new>
 
-#include <cublas_v2.h>
-
 #include "internal.h"
 #include "kernels.h"
 
@@ -171,7 +169,6 @@ vb_status vb_context_destroy(vb_context* ctx) {
         cudaStreamSynchronize(ctx->own_stream);
         cudaStreamDestroy(ctx->own_stream);
     }
-    if (ctx->blas) cublasDestroy(static_cast<cublasHandle_t>(ctx->blas));
     if (ctx->pool) {
         cudaDeviceSynchronize();
         cudaMemPoolDestroy(ctx->pool);

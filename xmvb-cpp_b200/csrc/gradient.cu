@@ -29,7 +29,6 @@
 // kernel and accumulates the two-electron table per left string in shared memory.  The host
 // then maps the two-electron table and factor-column adjoints onto the packed integrals
 // (full-rank pair kernel) or onto caller-supplied RI factors.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -688,23 +687,9 @@ cudaError_t launch_backward(const BackArgs& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// The context's cuBLAS handle (created on first use, bound to the context stream).
-vb_status blas_handle(vb_context* ctx, cublasHandle_t* out) {
-    if (!ctx->blas) {
-        cublasHandle_t h = nullptr;
-        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS)
-            return set_error(ctx, VB_ERR_CUDA, "cublasCreate failed");
-        ctx->blas = h;
-    }
-    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->blas);
-    cublasSetStream(h, ctx->stream);
-    *out = h;
-    return VB_OK;
-}
-
 // The listed (or all) pairs in chunks: gather their u-adjoint rows Ac, Q = L_f^T Ac, the careful
 // kernel (P rows), gL += Ac P^T.
-vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_pairs, cublasHandle_t blas) {
+vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_pairs, double* partial) {
     if (count <= 0) return VB_OK;
     cudaStream_t s = ctx->stream;
     const int np = b.ld, R = b.R;
@@ -730,7 +715,6 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
     if ((st = pb.allocate(ctx, sizeof(double) * (size_t)chunk * np)) != VB_OK) return st;
     b.Q = qb.as<double>();
     b.Pout = pb.as<double>();
-    const double one = 1.0, zero = 0.0;
     for (long long i0 = 0; i0 < count; i0 += chunk) {
         const long long i1 = std::min(count, i0 + chunk), cnt = i1 - i0;
         cudaError_t err = cudaMemsetAsync(pb.ptr, 0, sizeof(double) * (size_t)cnt * np, s);
@@ -738,10 +722,8 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
             gather_adjoint_kernel<<<(unsigned)std::min<long long>(4096, (cnt * R + 255) / 256), 256, 0, s>>>(
                 b, i0, i1, all_pairs, acb.as<double>());
             err = cudaGetLastError();
-            if (err == cudaSuccess &&
-                cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, np, (int)cnt, R, &one, b.lf, np, acb.as<double>(), R,
-                            &zero, qb.as<double>(), np) != CUBLAS_STATUS_SUCCESS)
-                return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+            if (err == cudaSuccess)
+                err = launch_factor_project(np, R, b.lf, np, acb.as<double>(), R, cnt, qb.as<double>(), np, s);
         } else if (err == cudaSuccess) {
             err = cudaMemsetAsync(qb.ptr, 0, sizeof(double) * (size_t)cnt * np, s);
         }
@@ -749,10 +731,9 @@ vb_status careful_chunks(vb_context* ctx, BackArgs b, long long count, int all_p
             kernel<<<grid, 128, 0, s>>>(b, i0, i1, all_pairs, slots.as<double>());
             err = cudaGetLastError();
         }
+        if (err == cudaSuccess)
+            err = launch_factor_outer(np, R, acb.as<double>(), R, pb.as<double>(), np, cnt, b.gL, np, partial, s);
         if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_gradient (exact path)");
-        if (R > 0 && cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, R, np, (int)cnt, &one, acb.as<double>(), R,
-                                 pb.as<double>(), np, &one, b.gL, np) != CUBLAS_STATUS_SUCCESS)
-            return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
     }
     {
         const int g2 = b.gd * b.gd, n2 = b.n * b.n;
@@ -890,6 +871,10 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
             det_pair_adjoint_kernel<<<148 * 8, 256, 0, s>>>(aa);
         err = cudaGetLastError();
     }
+    // split-K partials of the factor-column adjoint (one R x np block per CTA of factor_outer)
+    DeviceBuffer partial;
+    if (err == cudaSuccess && (st = partial.allocate(ctx, sizeof(double) * 148 * (size_t)std::max(1, R) * np)) != VB_OK)
+        return st;
     // backward through each distinct spin table
     for (int beta = 0; beta < 2 && err == cudaSuccess; ++beta) {
         const int k = beta ? p->kb : p->ka;
@@ -940,9 +925,6 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
             const long long rows_max = std::min<long long>(cap + kSpinBlock, tot);
             if ((st = qbuf.allocate(ctx, sizeof(double) * (size_t)np * rows_max)) != VB_OK) return st;
             if ((st = pbuf.allocate(ctx, sizeof(double) * (size_t)np * rows_max)) != VB_OK) return st;
-            cublasHandle_t blas = nullptr;
-            if ((st = blas_handle(ctx, &blas)) != VB_OK) return st;
-            const double one = 1.0, zero = 0.0;
             b.items = ditems.as<int2>();
             b.Q = qbuf.as<double>();
             b.Pout = pbuf.as<double>();
@@ -952,14 +934,7 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
                 if (i1 == i0) ++i1;
                 const long long tb = rec_off[i0], rows = rec_off[i1] - tb;
                 const double* A = b.adj + tb * adj_stride;
-                cublasStatus_t cs = CUBLAS_STATUS_SUCCESS;
-                if (R > 0)
-                    cs = cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, np, (int)rows, R, &one, b.lf, np, A, adj_stride,
-                                     &zero, qbuf.as<double>(), np);
-                else
-                    err = cudaMemsetAsync(qbuf.ptr, 0, sizeof(double) * (size_t)np * rows, s);
-                if (cs != CUBLAS_STATUS_SUCCESS)
-                    return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+                err = launch_factor_project(np, R, b.lf, np, A, adj_stride, rows, qbuf.as<double>(), np, s);
                 if (err == cudaSuccess) err = cudaMemsetAsync(pbuf.ptr, 0, sizeof(double) * (size_t)np * rows, s);
                 if (err != cudaSuccess) break;
                 b.item_begin = (int)i0;
@@ -977,9 +952,9 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
                     default: break;
                 }
                 if (err != cudaSuccess) break;
-                if (R > 0 && cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, R, np, (int)rows, &one, A, adj_stride,
-                                         pbuf.as<double>(), np, &one, gL, np) != CUBLAS_STATUS_SUCCESS)
-                    return set_error(ctx, VB_ERR_CUDA, "vb_hs_plan_gradient: cublasDgemm failed");
+                err = launch_factor_outer(np, R, A, adj_stride, pbuf.as<double>(), np, rows, gL, np,
+                                          partial.as<double>(), s);
+                if (err != cudaSuccess) break;
                 i0 = i1;
             }
             if (err != cudaSuccess) break;
@@ -987,12 +962,10 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
             err = cudaMemcpyAsync(&listed, b.careful_count, sizeof(listed), cudaMemcpyDeviceToHost, s);
             if (err == cudaSuccess) err = cudaStreamSynchronize(s);
             if (err != cudaSuccess) break;
-            if ((st = careful_chunks(ctx, b, (long long)listed, 0, blas)) != VB_OK) return st;
+            if ((st = careful_chunks(ctx, b, (long long)listed, 0, partial.as<double>())) != VB_OK) return st;
         } else {
             const long long NN = b.N;
-            cublasHandle_t blas = nullptr;
-            if ((st = blas_handle(ctx, &blas)) != VB_OK) return st;
-            if ((st = careful_chunks(ctx, b, NN * (NN + 1) / 2, 1, blas)) != VB_OK) return st;
+            if ((st = careful_chunks(ctx, b, NN * (NN + 1) / 2, 1, partial.as<double>())) != VB_OK) return st;
         }
         err = cudaGetLastError();
     }

@@ -93,19 +93,7 @@ int record_stride(int R) {
     return (s + 1) / 2 * 2;
 }
 
-// Work items of the fast spin-pair kernel: (left string u, first right string v0), v0 >= u.
 }  // namespace vbcore
-
-namespace {
-
-std::vector<int2> spin_items(int N) {
-    std::vector<int2> items;
-    for (int u = 0; u < N; ++u)
-        for (int v0 = u; v0 < N; v0 += kSpinBlock) items.push_back(make_int2(u, v0));
-    return items;
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -185,28 +173,28 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     p->npairs_a = (long long)p->Na * (p->Na + 1) / 2;
     p->npairs_b = p->shared_tables ? 0 : (long long)p->Nb * (p->Nb + 1) / 2;
     if ((st = p->list_a.allocate(ctx, sizeof(unsigned long long) * std::max(1LL, p->npairs_a))) != VB_OK) return fail(st);
-    {
-        std::vector<int2> it = spin_items(p->Na);
-        p->n_items_a = (int)it.size();
-        if ((st = upload(ctx, p->items_a, it.data(), sizeof(int2) * std::max<size_t>(1, it.size()))) != VB_OK)
-            return fail(st);
-    }
-    if (!p->shared_tables) {
-        if ((st = p->list_b.allocate(ctx, sizeof(unsigned long long) * std::max(1LL, p->npairs_b))) != VB_OK)
-            return fail(st);
-        std::vector<int2> it = spin_items(p->Nb);
-        p->n_items_b = (int)it.size();
-        if ((st = upload(ctx, p->items_b, it.data(), sizeof(int2) * std::max<size_t>(1, it.size()))) != VB_OK)
-            return fail(st);
-    }
-    if ((st = p->counters.allocate(ctx, 4 * sizeof(unsigned long long))) != VB_OK) return fail(st);
-    // per-left-string decomposition tables, sized for the largest factor rank
-    if (p->ka > 0 &&
-        (st = p->tables_a.allocate(ctx, sizeof(double) * left_table_doubles(n, p->ka, p->np) * p->Na)) != VB_OK)
+    if (!p->shared_tables &&
+        (st = p->list_b.allocate(ctx, sizeof(unsigned long long) * std::max(1LL, p->npairs_b))) != VB_OK)
         return fail(st);
-    if (p->kb > 0 && !p->shared_tables &&
-        (st = p->tables_b.allocate(ctx, sizeof(double) * left_table_doubles(n, p->kb, p->np) * p->Nb)) != VB_OK)
-        return fail(st);
+    if ((st = p->counters.allocate(ctx, 8 * sizeof(unsigned long long))) != VB_OK) return fail(st);
+    // right strings of every left string bucketed by hole set (depends on the strings only), and
+    // the per-left-string frame tables, sized for the largest factor rank
+    for (int beta = 0; beta < 2; ++beta) {
+        const int k = beta ? p->kb : p->ka;
+        if (k <= 0 || (beta && p->shared_tables) || !frame_spin_supported(n, k, 0)) continue;
+        const long long N = beta ? p->Nb : p->Na;
+        DeviceBuffer& rl = beta ? p->rlist_b : p->rlist_a;
+        DeviceBuffer& rd = beta ? p->rdesc_b : p->rdesc_a;
+        DeviceBuffer& eb = beta ? p->ebound_b : p->ebound_a;
+        DeviceBuffer& tb = beta ? p->tables_b : p->tables_a;
+        if ((st = rl.allocate(ctx, sizeof(int) * (size_t)std::max(1LL, N * (N + 1) / 2))) != VB_OK) return fail(st);
+        if ((st = rd.allocate(ctx, sizeof(unsigned) * (size_t)std::max(1LL, N * (N + 1) / 2))) != VB_OK) return fail(st);
+        if ((st = eb.allocate(ctx, sizeof(int) * (size_t)N * (k + 2))) != VB_OK) return fail(st);
+        if ((st = tb.allocate(ctx, sizeof(double) * frame_table_doubles(n, k, p->np) * N)) != VB_OK) return fail(st);
+        const cudaError_t err = launch_sort_right_strings(k, (int)N, (beta ? p->occ_b : p->occ_a).as<uint64_t>(),
+                                                         rl.as<int>(), rd.as<unsigned>(), eb.as<int>(), ctx->stream);
+        if (err != cudaSuccess) return fail(cuda_error(ctx, err, "sort_right_strings"));
+    }
 
     // inputs and derived integral tables
     if ((st = p->S_in.allocate(ctx, sizeof(double) * n * n)) != VB_OK) return fail(st);
@@ -382,9 +370,14 @@ SpinTableArgs table_args(vb_hs_plan* p, bool beta, const double* S, const double
     a.rec_stride = record_stride(p->R);
     a.careful_count = p->counters.as<unsigned long long>() + (beta ? 1 : 0);
     a.careful_list = beta ? p->list_b.as<unsigned long long>() : p->list_a.as<unsigned long long>();
-    a.items = beta ? p->items_b.as<int2>() : p->items_a.as<int2>();
-    a.n_items = beta ? p->n_items_b : p->n_items_a;
+    a.items = nullptr;
+    a.n_items = 0;
     a.all_careful = 0;
+    a.r_pos = p->r_pos;
+    a.rlist = beta ? p->rlist_b.as<int>() : p->rlist_a.as<int>();
+    a.rdesc = beta ? p->rdesc_b.as<unsigned>() : p->rdesc_a.as<unsigned>();
+    a.ebound = beta ? p->ebound_b.as<int>() : p->ebound_a.as<int>();
+    a.task_counter = p->counters.as<unsigned long long>() + 4 + (beta ? 1 : 0);
     return a;
 }
 
@@ -473,8 +466,20 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
         }
         p->rec_stride_alloc = stride;
     }
+    {
+        // per-left-string frame tables (they depend on S, h and the factor columns)
+        PhaseMark frame(p, VB_PHASE_TABLES);
+        if (p->ka > 0) {
+            err = launch_spin_tables(table_args(p, false, *dS, *dh, *deri), p->tables_a.as<double>(), s, launches);
+            if (err != cudaSuccess) return cuda_error(ctx, err, "frame tables (alpha)");
+        }
+        if (p->kb > 0 && !p->shared_tables) {
+            err = launch_spin_tables(table_args(p, true, *dS, *dh, *deri), p->tables_b.as<double>(), s, launches);
+            if (err != cudaSuccess) return cuda_error(ctx, err, "frame tables (beta)");
+        }
+    }
     PhaseMark spin(p, VB_PHASE_SPIN_PAIRS);
-    err = cudaMemsetAsync(p->counters.ptr, 0, 4 * sizeof(unsigned long long), s);
+    err = cudaMemsetAsync(p->counters.ptr, 0, 8 * sizeof(unsigned long long), s);
     if (err != cudaSuccess) return cuda_error(ctx, err, "cudaMemsetAsync");
     if (p->ka > 0) {
         err = launch_spin_pairs(table_args(p, false, *dS, *dh, *deri), p->tables_a.as<double>(), s, launches);
@@ -672,7 +677,7 @@ vb_status vb_hs_plan_stats(const vb_hs_plan* p, vb_hs_stats* stats) {
         cudaError_t err = cudaMemcpyAsync(c, p->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, p->ctx->stream);
         if (err == cudaSuccess) err = cudaStreamSynchronize(p->ctx->stream);
         if (err != cudaSuccess) return cuda_error(p->ctx, err, "stats download");
-        auto all_exact = [&](int k) { return !fast_spin_supported(p->n, k, p->R); };
+        auto all_exact = [&](int k) { return !frame_spin_supported(p->n, k, p->R); };
         const bool all_a = p->ka > 0 && all_exact(p->ka);
         const bool all_b = p->kb > 0 && !p->shared_tables && all_exact(p->kb);
         s.careful_spin_pairs = (long long)(all_a ? p->npairs_a : c[0]) + (long long)(all_b ? p->npairs_b : c[1]);

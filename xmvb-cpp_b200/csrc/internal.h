@@ -14,7 +14,6 @@ struct vb_context {
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     cudaMemPool_t pool = nullptr;  // the context's own stream-ordered pool (keeps freed memory)
-    void* blas = nullptr;          // cuBLAS handle, created on first use (plain FP64 GEMMs)
     // grow-only execute scratch shared by every plan of this context (plans of one context run
     // in order on its stream): the determinant-pair bands and the structure-reduce buffers
     void* scratch[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

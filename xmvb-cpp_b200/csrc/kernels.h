@@ -1,4 +1,4 @@
-// Kernel argument blocks and launchers (pair_kernels.cu, assembly.cu).
+// Kernel argument blocks and launchers (pair_kernels.cu, spin_frame.cu, assembly.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -38,6 +38,13 @@ struct SpinTableArgs {
     const int2* items;                 // fast-kernel work items: (left string u, first right string v0)
     int n_items;
     int all_careful;  // 1: every pair takes the exact path
+    int r_pos;        // factor columns with sign +1 (the first r_pos of R)
+    // frame kernel: right strings v >= u of each left string u at rlist[record_index(u, u)], bucketed
+    // by hole set (excitation level first); ebound[u (k + 2) + e] = first position of level e
+    const int* rlist;
+    const unsigned* rdesc;  // per rlist entry: hole mask | particle mask << 8 | sign parity << 16
+    const int* ebound;
+    unsigned long long* task_counter;  // zero before the launch: left strings handed out so far
 };
 
 struct FullPairArgs {
@@ -113,7 +120,21 @@ cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work,
 size_t left_table_doubles(int n, int k, int R);
 size_t factored_spin_smem_bytes(int n, int k, int R);
 bool fast_spin_supported(int n, int k, int R);
+// Spin-pair records of one string table: the per-left-string frame tables first
+// (launch_spin_tables, nothing when the register path does not apply), then launch_spin_pairs
+// (the frame kernel and the exact path for the blocks it lists, or the exact path for all).
+cudaError_t launch_spin_tables(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches);
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches);
+// Frame kernels (spin_frame.cu): per-left-string block size, the envelope of the register path,
+// the once-per-table bucketing of right strings, and the table and pair launches.
+size_t frame_table_doubles(int n, int k, int R);
+bool frame_spin_supported(int n, int k, int R);
+cudaError_t launch_sort_right_strings(int k, int N, const uint64_t* occ, int* rlist, unsigned* rdesc, int* ebound,
+                                      cudaStream_t stream);
+cudaError_t launch_frame_tables(const SpinTableArgs& a, double* tables, cudaStream_t stream);
+int frame_pair_variants(int n, int k, int R);
+cudaError_t launch_frame_pairs(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int variant);
+cudaError_t preload_frame_kernels();
 // Loads every kernel launch_spin_pairs and its table steps may use (under lazy module loading a
 // kernel is otherwise loaded, and its code placed in device memory, at its first launch).
 cudaError_t preload_spin_pair_kernels();
@@ -128,6 +149,15 @@ cudaError_t launch_resolve_blocks(int k, long long batch, const double* blocks, 
 cudaError_t launch_same_spin_list(int n, int k, long long batch, const int* occ_left, const int* occ_right,
                                   const double* S, const double* h, const double* eri, double* scalars, double* cof,
                                   cudaStream_t stream);
+// FP64 tensor-core contractions over the pair-kernel factor columns (dgemm.cu):
+//   launch_factor_project: C[q + c ldC] = sum_m lf[q ld + m] Y[m + c ldY]     (np x cnt)
+//   launch_factor_outer:   G[m + q ldG] += sum_c Y[m + c ldY] Z[q + c ldZ]    (R x np); `partial`
+//   holds 148 R np doubles of split-K partials, summed in a fixed order.
+bool factor_contractions_supported(int np, int R);
+cudaError_t launch_factor_project(int np, int R, const double* lf, int ld, const double* Y, long long ldY,
+                                  long long cnt, double* C, long long ldC, cudaStream_t stream);
+cudaError_t launch_factor_outer(int np, int R, const double* Y, long long ldY, const double* Z, long long ldZ,
+                                long long cnt, double* G, long long ldG, double* partial, cudaStream_t stream);
 size_t band_reduce_smem_bytes(int struct_count);
 int band_reduce_max_structures();
 

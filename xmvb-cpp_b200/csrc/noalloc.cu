@@ -63,22 +63,6 @@ __global__ void occupation_rows_kernel(const uint64_t* __restrict__ masks, int c
     }
 }
 
-// Sum_{m=1}^{M} ceil(m / B).
-__device__ __forceinline__ long long ceil_sum(long long M, long long B) {
-    const long long q = M / B, r = M % B;
-    return B * q * (q + 1) / 2 + r * (q + 1);
-}
-
-// Work items (u, v0) of the fast spin-pair kernel, v0 = u, u + B, ...: row u starts at
-// item sum_{u' < u} ceil((N - u') / B) = ceil_sum(N) - ceil_sum(N - u).
-__global__ void spin_items_kernel(int N, int B, int2* __restrict__ items) {
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
-        const long long first = ceil_sum(N, B) - ceil_sum(N - u, B);
-        int j = 0;
-        for (int v0 = u; v0 < N; v0 += B, ++j) items[first + j] = make_int2(u, v0);
-    }
-}
-
 __global__ void extract_scalars_kernel(const double* __restrict__ records, int stride, int R, long long n_pairs,
                                        double* __restrict__ out) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n_pairs;
@@ -95,8 +79,7 @@ int record_stride_for(int R) { return (R + 4 + 1) / 2 * 2; }
 
 // Loads every kernel a call may launch, so that no later call loads code into device memory.
 cudaError_t preload_kernels() {
-    const void* own[] = {(const void*)occupation_rows_kernel, (const void*)spin_items_kernel,
-                         (const void*)extract_scalars_kernel};
+    const void* own[] = {(const void*)occupation_rows_kernel, (const void*)extract_scalars_kernel};
     for (const void* f : own) {
         cudaFuncAttributes fa{};
         const cudaError_t err = cudaFuncGetAttributes(&fa, f);
@@ -125,8 +108,6 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
     const long long N = n_strings;
     const long long n_pairs = N * (N + 1) / 2;
     const int np = n * (n + 1) / 2, gd = n * (n - 1) / 2;
-    long long n_items = 0;
-    for (long long u = 0; u < N; ++u) n_items += (N - u + kSpinBlock - 1) / kSpinBlock;
     // layout of the static scratch, sized for the largest factor rank (np columns)
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -135,7 +116,9 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
         return at;
     };
     const size_t o_rows = take(sizeof(uint64_t) * 2 * N);
-    const size_t o_items = take(sizeof(int2) * n_items);
+    const size_t o_rlist = take(sizeof(int) * n_pairs);
+    const size_t o_rdesc = take(sizeof(unsigned) * n_pairs);
+    const size_t o_ebound = take(sizeof(int) * N * (k + 2));
     const size_t o_gamma = take(sizeof(double) * (size_t)(gd > 0 ? gd : 1) * (gd > 0 ? gd : 1));
     const size_t o_kfull = take(sizeof(double) * (size_t)np * np);
     const size_t o_lf = take(sizeof(double) * (size_t)np * np);
@@ -143,8 +126,8 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
     const size_t o_fcols = take(sizeof(double) * (size_t)np * np);
     const size_t o_signs = take(sizeof(int) * np);
     const size_t o_meta = take(sizeof(int) * 4);
-    const size_t o_counters = take(sizeof(unsigned long long) * 4);
-    const size_t o_tables = take(sizeof(double) * left_table_doubles(n, k, np) * N);
+    const size_t o_counters = take(sizeof(unsigned long long) * 8);
+    const size_t o_tables = take(sizeof(double) * frame_table_doubles(n, k, np) * N);
     const size_t o_records = take(sizeof(double) * (size_t)record_stride_for(np) * n_pairs);
     const size_t o_list = take(sizeof(unsigned long long) * n_pairs);
     if (off > kNoAllocScratchBytes)
@@ -178,7 +161,9 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
     unsigned char* b = static_cast<unsigned char*>(base);
     cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
     uint64_t* rows = reinterpret_cast<uint64_t*>(b + o_rows);
-    int2* items = reinterpret_cast<int2*>(b + o_items);
+    int* rlist = reinterpret_cast<int*>(b + o_rlist);
+    unsigned* rdesc = reinterpret_cast<unsigned*>(b + o_rdesc);
+    int* ebound = reinterpret_cast<int*>(b + o_ebound);
     double* gamma = reinterpret_cast<double*>(b + o_gamma);
     double* kfull = reinterpret_cast<double*>(b + o_kfull);
     double* lf = reinterpret_cast<double*>(b + o_lf);
@@ -206,11 +191,12 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
                          "vb_spin_pairs_noalloc: a string mask has the wrong electron count or an orbital >= n");
     const int R = meta[0] + meta[1];
 
-    err = cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 4, s);
+    err = cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 8, s);
     if (err != cudaSuccess) return cuda_error(nullptr, err, "cudaMemsetAsync");
-    spin_items_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(n_strings, kSpinBlock, items);
-    err = cudaGetLastError();
-    if (err != cudaSuccess) return cuda_error(nullptr, err, "spin_items_kernel");
+    if (frame_spin_supported(n, k, 0)) {
+        err = launch_sort_right_strings(k, n_strings, rows, rlist, rdesc, ebound, s);
+        if (err != cudaSuccess) return cuda_error(nullptr, err, "sort_right_strings");
+    }
     SpinTableArgs a{};
     a.n = n;
     a.k = k;
@@ -229,10 +215,17 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
     a.rec_stride = record_stride_for(R);
     a.careful_count = counters;
     a.careful_list = reinterpret_cast<unsigned long long*>(b + o_list);
-    a.items = items;
-    a.n_items = (int)n_items;
+    a.items = nullptr;
+    a.n_items = 0;
     a.all_careful = 0;
+    a.r_pos = meta[0];
+    a.rlist = rlist;
+    a.rdesc = rdesc;
+    a.ebound = ebound;
+    a.task_counter = counters + 4;
     int launches = 0;
+    err = launch_spin_tables(a, reinterpret_cast<double*>(b + o_tables), s, &launches);
+    if (err != cudaSuccess) return cuda_error(nullptr, err, "spin tables");
     err = launch_spin_pairs(a, reinterpret_cast<double*>(b + o_tables), s, &launches);
     if (err != cudaSuccess) return cuda_error(nullptr, err, "spin_pairs");
     long long blocks = (n_pairs + 255) / 256;

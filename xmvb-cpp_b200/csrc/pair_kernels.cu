@@ -23,6 +23,9 @@
 #include <algorithm>
 #include <stdint.h>
 
+#include <string>
+
+#include "autotune.h"
 #include "device_algebra.cuh"
 #include "internal.h"
 #include "kernels.h"
@@ -774,7 +777,7 @@ __device__ __forceinline__ double pair_weight(const int* flip, long long d, long
     return 0.0;
 }
 
-__global__ void __launch_bounds__(256) full_pairs_kernel(FullPairArgs a) {
+__global__ void __launch_bounds__(512) full_pairs_kernel(FullPairArgs a) {
     const long long B = a.e1 - a.e0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < a.n_items; t += stride) {
@@ -931,28 +934,35 @@ cudaError_t preload_spin_pair_kernels() {
         const cudaError_t err = cudaFuncGetAttributes(&fa, f);
         if (err != cudaSuccess) return err;
     }
-    return cudaSuccess;
+    return preload_frame_kernels();
+}
+
+cudaError_t launch_spin_tables(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches) {
+    if (a.n_pairs <= 0 || a.k <= 0 || a.all_careful || !frame_spin_supported(a.n, a.k, a.R)) return cudaSuccess;
+    ++*launches;
+    return launch_frame_tables(a, tables, stream);
 }
 
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches) {
     if (a.n_pairs <= 0 || a.k <= 0) return cudaSuccess;
     cudaError_t err = cudaSuccess;
-    const size_t smem = factored_spin_smem_bytes(a.n, a.k, a.R);
-    const bool fast_ok = !a.all_careful && fast_spin_supported(a.n, a.k, a.R);
+    const bool fast_ok = !a.all_careful && frame_spin_supported(a.n, a.k, a.R);
     if (fast_ok) {
-        switch (a.k) {
-            case 1: err = launch_fast<1>(a, smem, tables, stream); break;
-            case 2: err = launch_fast<2>(a, smem, tables, stream); break;
-            case 3: err = launch_fast<3>(a, smem, tables, stream); break;
-            case 4: err = launch_fast<4>(a, smem, tables, stream); break;
-            case 5: err = launch_fast<5>(a, smem, tables, stream); break;
-            case 6: err = launch_fast<6>(a, smem, tables, stream); break;
-            case 7: err = launch_fast<7>(a, smem, tables, stream); break;
-            case 8: err = launch_fast<8>(a, smem, tables, stream); break;
-            default: break;
-        }
+        // the pair-to-warp schedule (warps per CTA) is chosen by the autotuner per shape; the
+        // listed-pair counter and the task counter are restored before every timed launch
+        const std::string key = "spin_pairs_frame k=" + std::to_string(a.k) + " n=" + std::to_string(a.n) +
+                                " R=" + std::to_string(a.R) + " N=" + std::to_string(a.n_strings);
+        const int tuned = autotune_run(
+            key, frame_pair_variants(a.n, a.k, a.R), stream, [&](int v) { return launch_frame_pairs(a, tables, stream, v); },
+            [&]() {
+                cudaError_t e = cudaMemsetAsync(a.careful_count, 0, sizeof(unsigned long long), stream);
+                if (e == cudaSuccess) e = cudaMemsetAsync(a.task_counter, 0, sizeof(unsigned long long), stream);
+                return e;
+            },
+            &err);
+        (void)tuned;
         if (err != cudaSuccess) return err;
-        *launches += 2;
+        ++*launches;
     }
     SpinTableArgs b = a;
     b.all_careful = fast_ok ? 0 : 1;
@@ -969,11 +979,24 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream
 
 cudaError_t launch_full_pairs(const FullPairArgs& a, cudaStream_t stream, int* launches) {
     if (a.n_items <= 0) return cudaSuccess;
-    long long blocks = (a.n_items + 255) / 256;
-    if (blocks > kSms * 16) blocks = kSms * 16;
-    full_pairs_kernel<<<(unsigned)blocks, 256, 0, stream>>>(a);
+    // launch variants (block size, CTAs per SM), chosen by the autotuner per band shape
+    constexpr int kVariants = 4;
+    constexpr int threads[kVariants] = {256, 128, 256, 512};
+    constexpr int per_sm[kVariants] = {16, 16, 8, 4};
+    const std::string key = "full_pairs_kernel R=" + std::to_string(a.R) + " ndet=" + std::to_string(a.n_det) +
+                            " items=" + std::to_string(a.n_items) + " flip=" + std::to_string(a.flip ? 1 : 0);
+    cudaError_t err = cudaSuccess;
+    autotune_run(
+        key, kVariants, stream,
+        [&](int v) {
+            long long blocks = (a.n_items + threads[v] - 1) / threads[v];
+            if (blocks > (long long)kSms * per_sm[v]) blocks = (long long)kSms * per_sm[v];
+            full_pairs_kernel<<<(unsigned)blocks, threads[v], 0, stream>>>(a);
+            return cudaGetLastError();
+        },
+        {}, &err);
     ++*launches;
-    return cudaGetLastError();
+    return err;
 }
 
 cudaError_t launch_listed_pairs(const FullPairArgs& a, long long n_pairs, const long long* pairs, double* h_out,

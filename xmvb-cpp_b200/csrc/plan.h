@@ -28,8 +28,11 @@ struct vb_hs_plan {
     DeviceBuffer rec_a, rec_b, tables_a, tables_b;
     int stride_a = 0, stride_b = 0;
     long long npairs_a = 0, npairs_b = 0;
-    DeviceBuffer counters, list_a, list_b, items_a, items_b;
-    int n_items_a = 0, n_items_b = 0;
+    // counters: [0, 1] listed (exact-path) spin pairs alpha/beta, [2, 3] the gradient's listed
+    // pairs, [4, 5] the frame kernel's task counters alpha/beta
+    DeviceBuffer counters, list_a, list_b;
+    // right strings of each left string bucketed by hole set (see SpinTableArgs::rlist)
+    DeviceBuffer rlist_a, rlist_b, rdesc_a, rdesc_b, ebound_a, ebound_b;
     int rec_stride_alloc = 0;  // record stride the spin-pair records are allocated for
     DeviceBuffer S_in, h_in, eri_in, gamma, kfull;
     // pair-kernel factorization: lf[q * np + m], scratch, signs, meta = {r_pos, r_neg} (+ host copy)

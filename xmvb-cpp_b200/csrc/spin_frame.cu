@@ -1,0 +1,859 @@
+// Spin-pair records in the left string's biorthogonal frame (sm_100a).
+//
+// For a left string L (K orbitals; Lbar = the other NB = n - K orbitals) let S_LL = S[L, L],
+// Sinv = S_LL^-1 and P = S[:, L] Sinv (so P[L, :] = I).  For a right string R with holes
+// h_1 < ... < h_E (positions of L's orbitals missing from R) and particles p_1 < ... < p_E
+// (R's orbitals outside L, as Lbar indices), the overlap block X = S[R, L] (rows = right string)
+// factors as X = P[R, :] S_LL, and P[R, :] is the identity on the rows R shares with L.  So
+//   det X = sign det S_LL det B,      B(i, j) = P[p_i, h_j]   (E x E),
+// with sign the parity of the row-to-column assignment, and with W = B^-1 every first-order
+// quantity tr(X^-1 Z[R, :]) of an n x K block Z = Z_m[:, L] is
+//   tr(T_m) + sum_{i,j} W(j, i) Vt_m(p_i, h_j),   T_m = Sinv Z[L, :],
+//   Vt_m = (Z[Lbar, :] - S[Lbar, L] T_m) Sinv,
+// (Jacobi's formula in the L frame).  Z_m = B_m[:, L] (factor column m of the pair kernel)
+// gives the u-vector u_m / det X, Z = h[:, L] the one-electron energy / det X.  With the
+// factored pair kernel (ij|kl) = sum_m sigma_m B_m(ij) B_m(kl), the same-spin two-electron
+// energy of hamiltonian.cpp:83-123 (sum over c1<c2, r1<r2 of [(r1c1|r2c2) - (r1c2|r2c1)] times
+// the second cofactor) divided by det X is (1/2) sum_m sigma_m [tr(M_m)^2 - tr(M_m^2)] with
+// M_m = T'_m + Y' Vt_m in the same frame (Y' carries W on the hole x particle block), i.e.
+//   E2c(L) + sum_{i,j} W(j, i) l(p_i, h_j) + sum_{i<i', j<j'} Q(p_i p_i', h_j h_j') minor_W,
+//   E2c = 1/2 sum sigma (tr T^2... ) [constant], l = sum sigma (tr T Vt - V T Sinv) [linear],
+//   Q(b b', c c') = sum sigma [Vt(b,c) Vt(b',c') - Vt(b,c') Vt(b',c)]           [quadratic],
+// and minor_W the 2 x 2 minor of W on holes (j, j') and particles (i, i').  Per pair this leaves
+// an E x E inverse and C(E,2)^2 quadratic terms instead of a K x K inverse and C(K,2)^2 terms.
+//
+// Kernels:
+//  * sort_right_strings<K> (once per string table): for each left string u, the right strings
+//    v >= u bucketed by hole set, buckets in order of excitation level E then hole mask, each with
+//    a descriptor (hole mask, particle mask, sign of the assignment);
+//  * frame_tables<K> (per evaluation, one CTA per left string): Sinv, P, the table rows
+//    [h | 2e linear | factor columns] over the (hole position x particle) grid plus a trace slot,
+//    Q, and the norms of the conditioning certificate;
+//  * spin_pairs_frame<K> (persistent): a CTA takes left strings from a counter, stages the
+//    string's block in shared memory, and its warps take chunks of 32 pairs of one excitation
+//    level E (so every lane runs the same compile-time-E code).  Phase A, a lane per pair: B,
+//    Gauss-Jordan with partial pivoting, sign, certificate, quadratic two-electron term, and the
+//    pair's row Y' (W scattered onto the grid, 1 in the trace slot) to shared memory.  Phase B,
+//    per 8-pair tile: [h | 2e-linear | u] / det X = Y' Table^T on the FP64 tensor cores
+//    (mma.sync m8n8k4), k-steps only over the hole positions present in the tile (pairs are
+//    sorted by hole set, so a tile's union is usually its own hole set).
+// Blocks failing the certificate go to the exact path (spin_pairs_exact) through the list.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "device_algebra.cuh"
+#include "internal.h"
+#include "kernels.h"
+#include "pair_value.cuh"
+
+namespace vbcore {
+namespace {
+
+constexpr int kFrameWarps = 4;  // warps per CTA of the bucketing kernel
+constexpr int kFrameThreads = 32 * kFrameWarps;
+constexpr int kFrameMaxWarps = 8;  // warps per CTA of the pair kernel: a launch variant (2, 4 or 8)
+
+__host__ __device__ constexpr int fr_nbmax(int K) { return K <= 4 ? K + 4 : K; }
+__host__ __device__ constexpr int fr_kfs(int K) { return 8 * K + 4; }  // 8 columns per hole position + trace block
+__host__ __device__ constexpr int fr_cp(int K) { return K * (K - 1) / 2; }
+__host__ __device__ constexpr int fr_bp(int K) { return fr_nbmax(K) * (fr_nbmax(K) - 1) / 2; }
+
+// Layout of one left string's block (doubles; every part starts on a 2-double boundary).
+struct FrameLayout {
+    int rows;    // table rows: 0 = h, 1 = two-electron linear part, 2 + m = factor column m; padded to 8
+    int kfs;     // table row stride
+    int o_q;     // Q[bp * CP + cp]
+    int o_p;     // P[b * K + c]
+    int o_rowsq; // sum_c S(o, L_c)^2 for o = L_0 .. L_{K-1}, then o = Lbar_0 .. Lbar_{NBM-1}
+    int o_prow2; // sum_c P(b, c)^2
+    int o_scal;  // det S_LL, ||Sinv||_F^2, sum_c rowsq(L_c)
+    int total;
+};
+
+__host__ __device__ inline int even_up(int x) { return (x + 1) / 2 * 2; }
+
+__host__ __device__ inline FrameLayout frame_layout(int n, int K, int R) {
+    (void)n;
+    FrameLayout f{};
+    f.rows = (R + 2 + 7) / 8 * 8;
+    f.kfs = fr_kfs(K);
+    int o = f.rows * f.kfs;
+    f.o_q = o;
+    o += even_up(fr_bp(K) * fr_cp(K));
+    f.o_p = o;
+    o += even_up(fr_nbmax(K) * K);
+    f.o_rowsq = o;
+    o += even_up(K + fr_nbmax(K));
+    f.o_prow2 = o;
+    o += even_up(fr_nbmax(K));
+    f.o_scal = o;
+    o += 4;
+    f.total = o;
+    return f;
+}
+
+__device__ __forceinline__ void mma_f64(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ uint64_t occ_mask(uint64_t w, int k) {
+    uint64_t m = 0;
+    for (int c = 0; c < k; ++c) m |= 1ull << ((w >> (8 * c)) & 0xFFu);
+    return m;
+}
+
+// Hole mask of (L, R): bit c set when L's c-th orbital is not in R.
+template <int K>
+__device__ __forceinline__ unsigned hole_mask(uint64_t wL, uint64_t mR) {
+    unsigned hm = 0;
+#pragma unroll
+    for (int c = 0; c < K; ++c) hm |= ((mR >> ((wL >> (8 * c)) & 0xFFu)) & 1ull) ? 0u : (1u << c);
+    return hm;
+}
+
+// One warp per left string u.  Buckets: hole mask x (2^K of them), ordered by (popcount, x);
+// within a bucket, v ascending (the scatter walks v in order and ranks lanes within a warp).
+// Descriptor of the pair (L, R): bits 0-7 hole mask (positions in L), bits 8-15 particle mask
+// (indices in Lbar), bit 16 the parity of the row (R order) -> column (L position) assignment
+// that takes common orbitals to their positions and the i-th particle to the i-th hole.
+template <int K>
+__device__ __forceinline__ unsigned pair_descriptor(uint64_t wL, uint64_t mL, uint64_t mR) {
+    const unsigned hm = hole_mask<K>(wL, mR);
+    unsigned pbar = 0;
+    uint64_t pm = mR & ~mL;
+    while (pm) {
+        const int o = __ffsll((long long)pm) - 1;
+        pm &= pm - 1;
+        pbar |= 1u << __popcll(~mL & ((1ull << o) - 1ull));
+    }
+    int inv = 0;
+    uint64_t rest = mR;
+    unsigned hrest = hm, seen = 0;
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+        const int o = __ffsll((long long)rest) - 1;
+        rest &= rest - 1;
+        int t;
+        if ((mL >> o) & 1ull) {
+            t = __popcll(mL & ((1ull << o) - 1ull));
+        } else {
+            t = __ffs(hrest) - 1;
+            hrest &= hrest - 1;
+        }
+        inv += __popc(seen >> t);
+        seen |= 1u << t;
+    }
+    return hm | (pbar << 8) | ((unsigned)(inv & 1) << 16);
+}
+
+template <int K>
+__global__ void __launch_bounds__(kFrameThreads) sort_right_strings(int N, const uint64_t* __restrict__ occ,
+                                                                   int* __restrict__ rlist, unsigned* __restrict__ rdesc,
+                                                                   int* __restrict__ ebound) {
+    constexpr int NBINS = 1 << K;
+    __shared__ int cursor[kFrameWarps][NBINS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int u = blockIdx.x * kFrameWarps + warp;
+    if (u >= N) return;
+    int* cur = cursor[warp];
+    for (int x = lane; x < NBINS; x += 32) cur[x] = 0;
+    __syncwarp();
+    const uint64_t wL = __ldg(occ + 2 * (long long)u);
+    for (int v0 = u; v0 < N; v0 += 32) {
+        const int v = v0 + lane;
+        const int hm = v < N ? (int)hole_mask<K>(wL, occ_mask(__ldg(occ + 2 * (long long)v), K)) : -1;
+        const unsigned same = __match_any_sync(0xffffffffu, hm);
+        if (hm >= 0 && lane == __ffs(same) - 1) cur[hm] += __popc(same);
+        __syncwarp();
+    }
+    if (lane == 0) {
+        int run = 0;
+        int* eb = ebound + (long long)u * (K + 2);
+        for (int e = 0; e <= K; ++e) {
+            eb[e] = run;
+            for (int x = 0; x < NBINS; ++x)
+                if (__popc(x) == e) {
+                    const int c = cur[x];
+                    cur[x] = run;
+                    run += c;
+                }
+        }
+        eb[K + 1] = run;
+    }
+    __syncwarp();
+    const long long base = record_index(u, u, N);
+    const uint64_t mL = occ_mask(wL, K);
+    for (int v0 = u; v0 < N; v0 += 32) {
+        const int v = v0 + lane;
+        const uint64_t mR = v < N ? occ_mask(__ldg(occ + 2 * (long long)v), K) : 0;
+        const int hm = v < N ? (int)hole_mask<K>(wL, mR) : -1;
+        const unsigned same = __match_any_sync(0xffffffffu, hm);
+        int pos = 0;
+        if (hm >= 0) pos = cur[hm] + __popc(same & ((1u << lane) - 1u));
+        __syncwarp();
+        if (hm >= 0) {
+            rlist[base + pos] = v;
+            rdesc[base + pos] = pair_descriptor<K>(wL, mL, mR);
+            if (lane == __ffs(same) - 1) cur[hm] += __popc(same);
+        }
+        __syncwarp();
+    }
+}
+
+constexpr int kTableThreads = 256;
+constexpr int kTableSources = 48;  // pair-kernel sources (h and factor columns) staged per pass
+
+__host__ __device__ inline int table_sources(int R) { return R + 1 < kTableSources ? R + 1 : kTableSources; }
+
+// Per-left-string tables, one CTA per string u (dynamic shared memory: frame_tables_smem).  With
+// Y_s = Z_s[:, L] Sinv (n x K) for each source s (Z_0 = h, Z_{1+m} = B_m):
+//   Vt_s = Y_s[Lbar, :] - P Y_s[L, :],  tr T_s = tr Y_s[L, :],  tr T_s^2 = tr (Y_s[L, :])^2,
+//   V_s T_s Sinv = Vt_s Y_s[L, :],
+// so every quantity is a small dense product over staged rows, one thread per output element.
+template <int K>
+__global__ void __launch_bounds__(kTableThreads) frame_tables(SpinTableArgs a, double* __restrict__ tables) {
+    constexpr int NBM = fr_nbmax(K);
+    constexpr int CP = fr_cp(K);
+    constexpr int BP = fr_bp(K);
+    constexpr int KFS = fr_kfs(K);
+    constexpr int NQ = BP * CP;            // quadratic entries
+    constexpr int NE = NQ + NBM * K + 1;   // + linear entries + constant
+    constexpr int PER = (NE + kTableThreads - 1) / kTableThreads;
+    extern __shared__ double dsm[];
+    const int n = a.n, R = a.R;
+    const int nb = n - K;
+    const int SC = table_sources(R);
+    const FrameLayout F = frame_layout(n, K, R);
+    const long long u = blockIdx.x;
+    if (u >= a.n_strings) return;
+    double* blk = tables + u * (long long)F.total;
+    __shared__ int sL[K], sLb[NBM];
+    __shared__ double sM[K][2 * K], sF[K], sSinv[K * K], sP[NBM * K], sDet;
+    double* sZ = dsm;                            // [SC][n][K]: Z_s, then Y_s in place
+    double* sVt = sZ + (size_t)SC * n * K;       // [SC][NBM][K]
+    double* sTr = sVt + (size_t)SC * NBM * K;    // [SC][2]: tr T_s, tr T_s^2
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t w0 = a.occ[2 * u];
+    for (int i = tid; i < F.total; i += kTableThreads) blk[i] = 0.0;
+    if (tid == 0) {
+        const uint64_t mask = occ_mask(w0, K);
+        int q = 0;
+        for (int i = 0; i < n && q < NBM; ++i)
+            if (!((mask >> i) & 1)) sLb[q++] = i;
+        for (; q < NBM; ++q) sLb[q] = 0;
+    }
+    if (tid < K) sL[tid] = (int)((w0 >> (8 * tid)) & 0xFFu);
+    __syncthreads();
+    // S_LL^-1 by Gauss-Jordan on [S_LL | I] (S_LL is a principal block of an SPD matrix: the
+    // diagonal pivots are positive), warp 0 over the augmented entries
+    if (warp == 0) {
+        for (int e = lane; e < K * 2 * K; e += 32) {
+            const int r = e / (2 * K), c = e % (2 * K);
+            sM[r][c] = c < K ? __ldg(a.S + sL[r] * n + sL[c]) : (c - K == r ? 1.0 : 0.0);
+        }
+        double det = 1.0;
+        __syncwarp();
+        for (int st = 0; st < K; ++st) {
+            const double piv = sM[st][st];
+            det *= piv;
+            if (lane < K) sF[lane] = sM[lane][st];
+            __syncwarp();
+            for (int c = lane; c < 2 * K; c += 32) sM[st][c] /= piv;
+            __syncwarp();
+            for (int e = lane; e < K * 2 * K; e += 32) {
+                const int r = e / (2 * K), c = e % (2 * K);
+                if (r != st) sM[r][c] = fma(-sF[r], sM[st][c], sM[r][c]);
+            }
+            __syncwarp();
+        }
+        for (int e = lane; e < K * K; e += 32) sSinv[e] = sM[e / K][K + e % K];
+        if (lane == 0) sDet = det;
+    }
+    __syncthreads();
+    // P = S[Lbar, L] Sinv, the squared row norms of S[:, L], certificate scalars
+    for (int e = tid; e < NBM * K; e += kTableThreads) {
+        const int b = e / K, c = e % K;
+        double acc = 0.0;
+        if (b < nb)
+#pragma unroll
+            for (int t = 0; t < K; ++t) acc = fma(__ldg(a.S + sLb[b] * n + sL[t]), sSinv[t * K + c], acc);
+        sP[e] = acc;
+        blk[F.o_p + e] = acc;
+    }
+    for (int e = tid; e < K + NBM; e += kTableThreads) {
+        double acc = 0.0;
+        if (e < K || e - K < nb) {
+            const int o = e < K ? sL[e] : sLb[e - K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const double v = __ldg(a.S + o * n + sL[c]);
+                acc = fma(v, v, acc);
+            }
+        }
+        blk[F.o_rowsq + e] = acc;
+    }
+    if (tid == kTableThreads - 1) {
+        double s2 = 0.0, x2 = 0.0;
+        for (int e = 0; e < K * K; ++e) s2 = fma(sSinv[e], sSinv[e], s2);
+        for (int c = 0; c < K; ++c)
+            for (int t = 0; t < K; ++t) {
+                const double v = __ldg(a.S + sL[c] * n + sL[t]);
+                x2 = fma(v, v, x2);
+            }
+        blk[F.o_scal + 0] = sDet;
+        blk[F.o_scal + 1] = s2;
+        blk[F.o_scal + 2] = x2;
+    }
+    __syncthreads();
+    if (tid < NBM) {
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc = fma(sP[tid * K + c], sP[tid * K + c], acc);
+        blk[F.o_prow2 + tid] = acc;
+    }
+    double acc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) acc[q] = 0.0;
+    for (int s0 = 0; s0 < R + 1; s0 += SC) {
+        const int sc = min(SC, R + 1 - s0);
+        // stage Z_s(i, L_c) for every orbital i; source fastest, so factor columns read coalesced
+        for (int e = tid; e < sc * n * K; e += kTableThreads) {
+            const int sl = e % sc, ic = e / sc, i = ic / K, c = ic % K, s = s0 + sl;
+            const double v = s == 0 ? __ldg(a.h + i * n + sL[c])
+                                    : __ldg(a.lf + (long long)dev::pair_index(i, sL[c]) * a.ld + (s - 1));
+            sZ[((size_t)sl * n + i) * K + c] = v;
+        }
+        __syncthreads();
+        // Y_s = Z_s Sinv, one row per thread, in place
+        for (int e = tid; e < sc * n; e += kTableThreads) {
+            double* row = sZ + (size_t)e * K;
+            double z[K];
+#pragma unroll
+            for (int t = 0; t < K; ++t) z[t] = row[t];
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                double x = 0.0;
+#pragma unroll
+                for (int t = 0; t < K; ++t) x = fma(z[t], sSinv[t * K + c], x);
+                row[c] = x;
+            }
+        }
+        __syncthreads();
+        // Vt_s and the traces; table rows (row 0 = h, row 1 + s = factor column s - 1)
+        for (int e = tid; e < sc * NBM * K; e += kTableThreads) {
+            const int sl = e / (NBM * K), bc = e % (NBM * K), b = bc / K, c = bc % K;
+            const double* Y = sZ + (size_t)sl * n * K;
+            double x = 0.0;
+            if (b < nb) {
+                x = Y[sLb[b] * K + c];
+#pragma unroll
+                for (int t = 0; t < K; ++t) x = fma(-sP[b * K + t], Y[sL[t] * K + c], x);
+                const int s = s0 + sl;
+                blk[(long long)(s == 0 ? 0 : s + 1) * KFS + c * 8 + b] = x;
+            }
+            sVt[e] = x;
+        }
+        for (int sl = tid; sl < sc; sl += kTableThreads) {
+            const double* Y = sZ + (size_t)sl * n * K;
+            double tr = 0.0, tr2 = 0.0;
+            for (int r = 0; r < K; ++r) {
+                tr += Y[sL[r] * K + r];
+                for (int t = 0; t < K; ++t) tr2 = fma(Y[sL[r] * K + t], Y[sL[t] * K + r], tr2);
+            }
+            sTr[2 * sl] = tr;
+            sTr[2 * sl + 1] = tr2;
+            const int s = s0 + sl;
+            blk[(long long)(s == 0 ? 0 : s + 1) * KFS + 8 * K] = tr;
+        }
+        __syncthreads();
+        // two-electron constant, linear and quadratic tables over the factor sources
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int e = tid + kTableThreads * q;
+            if (e >= NE) continue;
+            double x = acc[q];
+            if (e < NQ) {
+                constexpr int CPD = CP > 0 ? CP : 1;
+                const int bp = e / CPD, cp = e % CPD;
+                int b2 = 1;
+                while ((b2 + 1) * b2 / 2 <= bp) ++b2;
+                const int b1 = bp - b2 * (b2 - 1) / 2;
+                int c2 = 1;
+                while ((c2 + 1) * c2 / 2 <= cp) ++c2;
+                const int c1 = cp - c2 * (c2 - 1) / 2;
+                for (int sl = (s0 == 0 ? 1 : 0); sl < sc; ++sl) {
+                    const double* V = sVt + (size_t)sl * NBM * K;
+                    const double sg = (s0 + sl - 1) < a.r_pos ? 1.0 : -1.0;
+                    x = fma(sg, V[b1 * K + c1] * V[b2 * K + c2] - V[b1 * K + c2] * V[b2 * K + c1], x);
+                }
+            } else if (e < NE - 1) {
+                const int bc = e - NQ, b = bc / K, c = bc % K;
+                for (int sl = (s0 == 0 ? 1 : 0); sl < sc; ++sl) {
+                    const double* V = sVt + (size_t)sl * NBM * K;
+                    const double* Y = sZ + (size_t)sl * n * K;
+                    const double sg = (s0 + sl - 1) < a.r_pos ? 1.0 : -1.0;
+                    double vts = 0.0;
+#pragma unroll
+                    for (int t = 0; t < K; ++t) vts = fma(V[b * K + t], Y[sL[t] * K + c], vts);
+                    x = fma(sg, sTr[2 * sl] * V[bc] - vts, x);
+                }
+            } else {
+                for (int sl = (s0 == 0 ? 1 : 0); sl < sc; ++sl) {
+                    const double sg = (s0 + sl - 1) < a.r_pos ? 1.0 : -1.0;
+                    x = fma(sg, sTr[2 * sl] * sTr[2 * sl] - sTr[2 * sl + 1], x);
+                }
+            }
+            acc[q] = x;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int e = tid + kTableThreads * q;
+        if (e >= NE) continue;
+        if (e < NQ) {
+            blk[F.o_q + e] = acc[q];
+        } else if (e < NE - 1) {
+            const int bc = e - NQ, b = bc / K, c = bc % K;
+            if (b < nb) blk[1 * KFS + c * 8 + b] = acc[q];
+        } else {
+            blk[1 * KFS + 8 * K] = 0.5 * acc[q];
+        }
+    }
+}
+
+template <int K>
+size_t frame_tables_smem(int n, int R) {
+    return sizeof(double) * (size_t)table_sources(R) * ((size_t)n * K + (size_t)fr_nbmax(K) * K + 2);
+}
+
+// Phase A of one pair at excitation level E (compile time).  Writes the pair's Y' row and
+// returns the certificate, det X, the quadratic two-electron term / det X and the hole mask.
+template <int K, int E>
+__device__ __forceinline__ void frame_pair(const double* __restrict__ blk, const FrameLayout& F, unsigned desc,
+                                           double* __restrict__ yrow, bool* ok_out, double* det_out,
+                                           double* quad_out, unsigned* hm_out) {
+    constexpr int CP = fr_cp(K);
+    const unsigned hm = desc & 0xFFu;
+    // holes (positions in L, ascending) and particles (Lbar indices, ascending)
+    int hc[E > 0 ? E : 1], pb[E > 0 ? E : 1];
+    {
+        unsigned h = hm, pm = (desc >> 8) & 0xFFu;
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            hc[j] = __ffs(h) - 1;
+            h &= h - 1;
+            pb[j] = __ffs(pm) - 1;
+            pm &= pm - 1;
+        }
+    }
+    const double* P = blk + F.o_p;
+    double x[E > 0 ? E : 1][E > 0 ? E : 1];
+#pragma unroll
+    for (int i = 0; i < E; ++i)
+#pragma unroll
+        for (int j = 0; j < E; ++j) x[i][j] = P[pb[i] * K + hc[j]];
+    int lab[E > 0 ? E : 1];
+#pragma unroll
+    for (int i = 0; i < E; ++i) lab[i] = i;
+    double detb = 1.0;
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+        int p = s;
+        double best = fabs(x[s][s]);
+#pragma unroll
+        for (int i = s + 1; i < E; ++i) {
+            const double av = fabs(x[i][s]);
+            if (av > best) {
+                best = av;
+                p = i;
+            }
+        }
+#pragma unroll
+        for (int i = s + 1; i < E; ++i) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const double a0 = x[s][j], a1 = x[i][j];
+                x[s][j] = sw ? a1 : a0;
+                x[i][j] = sw ? a0 : a1;
+            }
+            const int l0 = lab[s], l1 = lab[i];
+            lab[s] = sw ? l1 : l0;
+            lab[i] = sw ? l0 : l1;
+        }
+        if (p != s) detb = -detb;
+        const double piv = x[s][s];
+        detb *= piv;
+        const double ip = 1.0 / piv;
+        x[s][s] = 1.0;
+#pragma unroll
+        for (int j = 0; j < E; ++j) x[s][j] *= ip;
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            if (i == s) continue;
+            const double f = x[i][s];
+            x[i][s] = 0.0;
+#pragma unroll
+            for (int j = 0; j < E; ++j) x[i][j] = fma(-f, x[s][j], x[i][j]);
+        }
+    }
+    // x[j][jj] = W(j, lab[jj]): hole slot j, particle slot lab[jj]
+    const double* scal = blk + F.o_scal;
+    const double det = ((desc >> 16) & 1u ? -1.0 : 1.0) * scal[0] * detb;
+    double nw2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < E; ++i)
+#pragma unroll
+        for (int j = 0; j < E; ++j) nw2 = fma(x[i][j], x[i][j], nw2);
+    const double* rowsq = blk + F.o_rowsq;
+    const double* prow2 = blk + F.o_prow2;
+    double nx2 = scal[2], pr = 0.0;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        nx2 += rowsq[K + pb[j]] - rowsq[hc[j]];
+        pr += prow2[pb[j]];
+    }
+    const double bnd = scal[1] * ((double)(K - E) + nw2 * (1.0 + pr));
+    const bool ok = isfinite(det) && det != 0.0 && (nx2 * bnd < kCertificate2);
+    // packed particle Lbar indices by slot, to read the particle of a permuted column
+    uint64_t bword = 0;
+#pragma unroll
+    for (int i = 0; i < E; ++i) bword |= (uint64_t)pb[i] << (8 * i);
+    int bj[E > 0 ? E : 1];
+#pragma unroll
+    for (int jj = 0; jj < E; ++jj) bj[jj] = (int)((bword >> (8 * lab[jj])) & 0xFFu);
+    double quad = 0.0;
+    if (E >= 2) {
+        const double* Q = blk + F.o_q;
+#pragma unroll
+        for (int j1 = 0; j1 < E; ++j1)
+#pragma unroll
+            for (int j2 = j1 + 1; j2 < E; ++j2) {
+                const int cp = hc[j2] * (hc[j2] - 1) / 2 + hc[j1];
+                double part = 0.0;
+#pragma unroll
+                for (int jj1 = 0; jj1 < E; ++jj1)
+#pragma unroll
+                    for (int jj2 = jj1 + 1; jj2 < E; ++jj2) {
+                        const int ba = bj[jj1], bb = bj[jj2];
+                        const bool ordered = ba < bb;
+                        const int lo = ordered ? ba : bb, hi = ordered ? bb : ba;
+                        const double m2 = fma(x[j1][jj1], x[j2][jj2], -x[j1][jj2] * x[j2][jj1]);
+                        const double qv = Q[(hi * (hi - 1) / 2 + lo) * CP + cp];
+                        part = fma(ordered ? qv : -qv, m2, part);
+                    }
+                quad += part;
+            }
+    }
+    // the pair's row (zeroed by the warp beforehand): W on the (hole position, particle) grid,
+    // 1 in the trace slot
+    if (ok) {
+#pragma unroll
+        for (int j = 0; j < E; ++j)
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) yrow[hc[j] * 8 + bj[jj]] = x[j][jj];
+        yrow[8 * K] = 1.0;
+    }
+    *ok_out = ok;
+    *det_out = det;
+    *quad_out = quad;
+    *hm_out = hm;
+}
+
+template <int K>
+__device__ __forceinline__ void frame_pair_dispatch(int e, const double* blk, const FrameLayout& F, unsigned desc,
+                                                    double* yrow, bool* ok, double* det, double* quad, unsigned* hm) {
+    switch (e) {
+        case 0: frame_pair<K, 0>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 1: if constexpr (K >= 1) frame_pair<K, 1>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 2: if constexpr (K >= 2) frame_pair<K, 2>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 3: if constexpr (K >= 3) frame_pair<K, 3>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 4: if constexpr (K >= 4) frame_pair<K, 4>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 5: if constexpr (K >= 5) frame_pair<K, 5>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 6: if constexpr (K >= 6) frame_pair<K, 6>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 7: if constexpr (K >= 7) frame_pair<K, 7>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        case 8: if constexpr (K >= 8) frame_pair<K, 8>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        default: break;
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(32 * kFrameMaxWarps) spin_pairs_frame(SpinTableArgs a,
+                                                                       const double* __restrict__ tables) {
+    extern __shared__ double smem[];
+    constexpr int KFS = fr_kfs(K);
+    const int R = a.R;
+    const FrameLayout F = frame_layout(a.n, K, R);
+    const int NT = F.rows / 8;
+    double* sBlk = smem;
+    double* sY = smem + F.total;
+    __shared__ int s_task, s_chunk;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    const long long N = a.n_strings;
+    double* yw = sY + (size_t)warp * 32 * KFS;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_task = (int)atomicAdd(a.task_counter, 1ull);
+            s_chunk = 0;
+        }
+        __syncthreads();
+        const int u = s_task;
+        if (u >= N) break;
+        {
+            const double2* src = reinterpret_cast<const double2*>(tables + (long long)u * F.total);
+            double2* dst = reinterpret_cast<double2*>(sBlk);
+            for (int i = threadIdx.x; i < F.total / 2; i += blockDim.x) dst[i] = __ldg(src + i);
+        }
+        const int* eb = a.ebound + (long long)u * (K + 2);
+        int bound[K + 2];
+#pragma unroll
+        for (int e = 0; e < K + 2; ++e) bound[e] = __ldg(eb + e);
+        int nchunks = 0;
+#pragma unroll
+        for (int e = 0; e <= K; ++e) nchunks += (bound[e + 1] - bound[e] + 31) >> 5;
+        const long long base = record_index(u, u, N);
+        __syncthreads();
+        // warps take 32-pair chunks dynamically, highest excitation level (the costliest) first
+        for (;;) {
+            int ch = 0;
+            if (lane == 0) ch = atomicAdd(&s_chunk, 1);
+            ch = __shfl_sync(0xffffffffu, ch, 0);
+            if (ch >= nchunks) break;
+            int e = 0, start = 0, cnt = 0, left = ch;
+#pragma unroll
+            for (int ee = K; ee >= 0; --ee) {
+                const int c = (bound[ee + 1] - bound[ee] + 31) >> 5;
+                if (left >= 0 && left < c) {
+                    e = ee;
+                    start = bound[ee] + 32 * left;
+                    cnt = min(32, bound[ee + 1] - start);
+                }
+                left -= c;
+            }
+            // zero the warp's 32 rows, consecutive lanes on consecutive 16-byte words
+            {
+                double2* z = reinterpret_cast<double2*>(yw);
+#pragma unroll
+                for (int f = lane; f < 16 * KFS; f += 32) z[f] = make_double2(0.0, 0.0);
+            }
+            __syncwarp();
+            const bool valid = lane < cnt;
+            const int v = valid ? __ldg(a.rlist + base + start + lane) : u;
+            double* yrow = yw + lane * KFS;
+            bool ok = false;
+            double det = 0.0, quad = 0.0;
+            unsigned hm = 0;
+            if (valid) {
+                frame_pair_dispatch<K>(e, sBlk, F, __ldg(a.rdesc + base + start + lane), yrow, &ok, &det, &quad, &hm);
+                if (!ok) {
+                    const unsigned long long slot = atomicAdd(a.careful_count, 1ull);
+                    a.careful_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
+                }
+            }
+            const long long t = record_index(u, v, N);
+            const unsigned okbits = __ballot_sync(0xffffffffu, ok);
+            __syncwarp();
+            // phase B, one 8-pair tile at a time
+#pragma unroll 1
+            for (int mt = 0; mt < 4; ++mt) {
+                const unsigned uh = __reduce_or_sync(0xffffffffu, ((lane >> 3) == mt && ok) ? hm : 0u);
+                if (((okbits >> (8 * mt)) & 0xFFu) == 0) continue;
+                const int owner = 8 * mt + g;
+                const double det_g = __shfl_sync(0xffffffffu, det, owner);
+                const double quad_g = __shfl_sync(0xffffffffu, quad, owner);
+                const long long t_g = __shfl_sync(0xffffffffu, t, owner);
+                const bool ok_g = (okbits >> owner) & 1u;
+                const double* yr = yw + owner * KFS;
+                double* rec = a.records + t_g * (long long)a.rec_stride;
+#pragma unroll 1
+                for (int nt0 = 0; nt0 < NT; nt0 += 6) {
+                    double acc[6][2];
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) acc[j][0] = acc[j][1] = 0.0;
+                    {
+                        const double af = yr[8 * K + tq];
+#pragma unroll
+                        for (int j = 0; j < 6; ++j) {
+                            const double bf = (nt0 + j < NT) ? sBlk[(8 * (nt0 + j) + g) * KFS + 8 * K + tq] : 0.0;
+                            mma_f64(acc[j], af, bf);
+                        }
+                    }
+                    unsigned rest = uh;
+                    while (rest) {
+                        const int c = __ffs(rest) - 1;
+                        rest &= rest - 1;
+#pragma unroll
+                        for (int ks = 0; ks < 2; ++ks) {
+                            const int col = 8 * c + 4 * ks + tq;
+                            const double af = yr[col];
+#pragma unroll
+                            for (int j = 0; j < 6; ++j) {
+                                const double bf = (nt0 + j < NT) ? sBlk[(8 * (nt0 + j) + g) * KFS + col] : 0.0;
+                                mma_f64(acc[j], af, bf);
+                            }
+                        }
+                    }
+                    if (ok_g) {
+#pragma unroll
+                        for (int j = 0; j < 6; ++j)
+#pragma unroll
+                            for (int i = 0; i < 2; ++i) {
+                                const int row = 8 * (nt0 + j) + 2 * tq + i;
+                                if (row >= 2 && row < R + 2) rec[row - 2] = det_g * acc[j][i];
+                            }
+                        if (nt0 == 0 && tq == 0) {
+                            const double h1 = acc[0][0], e2 = acc[0][1];
+                            rec[R + 0] = det_g;
+                            rec[R + 1] = det_g * (h1 + e2 + quad_g);
+                            rec[R + 2] = det_g * h1;
+                            rec[R + 3] = 0.0;
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
+template <int K>
+size_t frame_spin_smem(int n, int R, int warps = 4) {
+    return sizeof(double) * ((size_t)frame_layout(n, K, R).total + (size_t)warps * 32 * fr_kfs(K));
+}
+
+size_t frame_spin_smem_rt(int n, int k, int R) {
+    switch (k) {
+        case 1: return frame_spin_smem<1>(n, R);
+        case 2: return frame_spin_smem<2>(n, R);
+        case 3: return frame_spin_smem<3>(n, R);
+        case 4: return frame_spin_smem<4>(n, R);
+        case 5: return frame_spin_smem<5>(n, R);
+        case 6: return frame_spin_smem<6>(n, R);
+        case 7: return frame_spin_smem<7>(n, R);
+        case 8: return frame_spin_smem<8>(n, R);
+        default: return ~size_t{0};
+    }
+}
+
+template <int K>
+cudaError_t launch_tables(const SpinTableArgs& a, double* tables, cudaStream_t stream) {
+    const size_t tsmem = frame_tables_smem<K>(a.n, a.R);
+    cudaError_t err = allow_dynamic_smem((const void*)frame_tables<K>, tsmem);
+    if (err != cudaSuccess) return err;
+    frame_tables<K><<<a.n_strings, kTableThreads, tsmem, stream>>>(a, tables);
+    return cudaGetLastError();
+}
+
+// Launch variants (the autotuner's choices): 0 = 4 warps per CTA, 1 = 2 warps, 2 = 8 warps; every
+// variant fills each SM with as many resident CTAs as fit.
+constexpr int kFrameVariants = 3;
+constexpr int kFrameVariantWarps[kFrameVariants] = {4, 2, 8};
+
+template <int K>
+cudaError_t launch_frame(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int variant) {
+    const int warps = kFrameVariantWarps[variant];
+    const size_t smem = frame_spin_smem<K>(a.n, a.R, warps);
+    cudaError_t err = allow_dynamic_smem((const void*)spin_pairs_frame<K>, smem);
+    if (err != cudaSuccess) return err;
+    int per_sm = 1, dev = 0, sms = 148;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_pairs_frame<K>, 32 * warps, smem);
+    if (err != cudaSuccess) return err;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    if (blocks > a.n_strings) blocks = a.n_strings;
+    if (blocks < 1) blocks = 1;
+    spin_pairs_frame<K><<<(unsigned)blocks, 32 * warps, smem, stream>>>(a, tables);
+    return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_sort(int N, const uint64_t* occ, int* rlist, unsigned* rdesc, int* ebound, cudaStream_t stream) {
+    sort_right_strings<K><<<(N + kFrameWarps - 1) / kFrameWarps, kFrameThreads, 0, stream>>>(N, occ, rlist, rdesc,
+                                                                                            ebound);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t frame_table_doubles(int n, int k, int R) { return (size_t)frame_layout(n, k, R).total; }
+
+bool frame_spin_supported(int n, int k, int R) {
+    return k >= 1 && k <= 8 && n - k >= 0 && n - k <= fr_nbmax(k) && frame_spin_smem_rt(n, k, R) <= 200 * 1024;
+}
+
+cudaError_t launch_sort_right_strings(int k, int N, const uint64_t* occ, int* rlist, unsigned* rdesc, int* ebound,
+                                      cudaStream_t stream) {
+    if (N <= 0) return cudaSuccess;
+    switch (k) {
+        case 1: return launch_sort<1>(N, occ, rlist, rdesc, ebound, stream);
+        case 2: return launch_sort<2>(N, occ, rlist, rdesc, ebound, stream);
+        case 3: return launch_sort<3>(N, occ, rlist, rdesc, ebound, stream);
+        case 4: return launch_sort<4>(N, occ, rlist, rdesc, ebound, stream);
+        case 5: return launch_sort<5>(N, occ, rlist, rdesc, ebound, stream);
+        case 6: return launch_sort<6>(N, occ, rlist, rdesc, ebound, stream);
+        case 7: return launch_sort<7>(N, occ, rlist, rdesc, ebound, stream);
+        case 8: return launch_sort<8>(N, occ, rlist, rdesc, ebound, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_frame_tables(const SpinTableArgs& a, double* tables, cudaStream_t stream) {
+    switch (a.k) {
+        case 1: return launch_tables<1>(a, tables, stream);
+        case 2: return launch_tables<2>(a, tables, stream);
+        case 3: return launch_tables<3>(a, tables, stream);
+        case 4: return launch_tables<4>(a, tables, stream);
+        case 5: return launch_tables<5>(a, tables, stream);
+        case 6: return launch_tables<6>(a, tables, stream);
+        case 7: return launch_tables<7>(a, tables, stream);
+        case 8: return launch_tables<8>(a, tables, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int frame_pair_variants(int n, int k, int R) {
+    // the 8-warp variant only where its rows fit next to the table
+    const bool eight = frame_spin_smem_rt(n, k, R) + sizeof(double) * 4 * 32 * fr_kfs(k) <= 200 * 1024;
+    return eight ? kFrameVariants : kFrameVariants - 1;
+}
+
+cudaError_t launch_frame_pairs(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int variant) {
+    if (variant < 0 || variant >= kFrameVariants) variant = 0;
+    switch (a.k) {
+        case 1: return launch_frame<1>(a, tables, stream, variant);
+        case 2: return launch_frame<2>(a, tables, stream, variant);
+        case 3: return launch_frame<3>(a, tables, stream, variant);
+        case 4: return launch_frame<4>(a, tables, stream, variant);
+        case 5: return launch_frame<5>(a, tables, stream, variant);
+        case 6: return launch_frame<6>(a, tables, stream, variant);
+        case 7: return launch_frame<7>(a, tables, stream, variant);
+        case 8: return launch_frame<8>(a, tables, stream, variant);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t preload_frame_kernels() {
+    const void* fns[] = {
+        (const void*)sort_right_strings<1>, (const void*)sort_right_strings<2>, (const void*)sort_right_strings<3>,
+        (const void*)sort_right_strings<4>, (const void*)sort_right_strings<5>, (const void*)sort_right_strings<6>,
+        (const void*)sort_right_strings<7>, (const void*)sort_right_strings<8>, (const void*)frame_tables<1>,
+        (const void*)frame_tables<2>,       (const void*)frame_tables<3>,       (const void*)frame_tables<4>,
+        (const void*)frame_tables<5>,       (const void*)frame_tables<6>,       (const void*)frame_tables<7>,
+        (const void*)frame_tables<8>,       (const void*)spin_pairs_frame<1>,   (const void*)spin_pairs_frame<2>,
+        (const void*)spin_pairs_frame<3>,   (const void*)spin_pairs_frame<4>,   (const void*)spin_pairs_frame<5>,
+        (const void*)spin_pairs_frame<6>,   (const void*)spin_pairs_frame<7>,   (const void*)spin_pairs_frame<8>};
+    for (const void* f : fns) {
+        cudaFuncAttributes fa{};
+        const cudaError_t err = cudaFuncGetAttributes(&fa, f);
+        if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace vbcore

@@ -221,17 +221,8 @@ Active transform(const AoIntegrals& ao, int nbf, int na, const std::vector<doubl
 // hi(hi+1)/2+lo), stopping when the largest remaining diagonal falls to tol times the largest
 // initial one.  The packed factor has the layout of metric-whitened RI factors, so the active
 // transform, the pair-kernel factorization and the gradient run through the RI path.
-std::vector<double> ao_pair_cholesky(const AoIntegrals& ao, int n, double tol, int* rank) {
-    const int P = n * (n + 1) / 2;
-    std::vector<int> pm(P), pn(P);
-    for (int m = 0, t = 0; m < n; ++m)
-        for (int v = 0; v <= m; ++v, ++t) {
-            pm[t] = m;
-            pn[t] = v;
-        }
-    auto V = [&](int p, int q) {
-        return ao.eri[(size_t)pm[p] + (size_t)n * (pn[p] + (size_t)n * (pm[q] + (size_t)n * pn[q]))];
-    };
+template <class PairMatrix>
+std::vector<double> pair_cholesky(int P, const PairMatrix& V, double tol, int* rank) {
     std::vector<double> diag(P);
     double dmax = 0.0;
     for (int p = 0; p < P; ++p) dmax = std::max(dmax, diag[p] = V(p, p));
@@ -262,6 +253,20 @@ std::vector<double> ao_pair_cholesky(const AoIntegrals& ao, int n, double tol, i
     for (size_t c = 0; c < rows.size(); ++c)
         for (int q = 0; q < P; ++q) B[c + rows.size() * (size_t)q] = rows[c][q];
     return B;
+}
+
+std::vector<double> ao_pair_cholesky(const AoIntegrals& ao, int n, double tol, int* rank) {
+    const int P = n * (n + 1) / 2;
+    std::vector<int> pm(P), pn(P);
+    for (int m = 0, t = 0; m < n; ++m)
+        for (int v = 0; v <= m; ++v, ++t) {
+            pm[t] = m;
+            pn[t] = v;
+        }
+    auto V = [&](int p, int q) {
+        return ao.eri[(size_t)pm[p] + (size_t)n * (pn[p] + (size_t)n * (pm[q] + (size_t)n * pn[q]))];
+    };
+    return pair_cholesky(P, V, tol, rank);
 }
 
 }  // namespace
@@ -376,6 +381,65 @@ vb_status evaluate(vb_scf_problem* pr, const std::vector<double>& C, double* ene
 
 }  // namespace
 
+namespace {
+
+// Orbital pattern, structures, expansion and the structure H/S plan of a problem (shared by both
+// creation paths).  Deletes `pr` and returns the failure on error.
+vb_status finish_problem(vb_context* ctx, vb_scf_problem* pr, int n_active, const int32_t* orbital_offsets,
+                         const int32_t* orbital_functions, int n_electrons, int multiplicity, const char* structures,
+                         const char* who) {
+    pr->n_act = n_active;
+    for (int a = 0; a < n_active; ++a) {
+        std::vector<int> f;
+        for (int t = orbital_offsets[a]; t < orbital_offsets[a + 1]; ++t) {
+            if (orbital_functions[t] < 0 || orbital_functions[t] >= pr->basis.n_bf) {
+                delete pr;
+                return set_error(ctx, VB_ERR_INVALID, std::string(who) + ": orbital basis function out of range");
+            }
+            f.push_back(orbital_functions[t]);
+        }
+        pr->pattern.push_back(f);
+    }
+    int64_t ns = 0;
+    vb_status st = vb_generate_structures(structures, n_active, n_electrons, multiplicity, 0, &ns, nullptr, 0);
+    if (st != VB_OK) {
+        delete pr;
+        return set_error(ctx, st, std::string(who) + ": " + vb_last_error(nullptr));
+    }
+    pr->rows.resize((size_t)ns * n_electrons);
+    vb_generate_structures(structures, n_active, n_electrons, multiplicity, 0, &ns, pr->rows.data(),
+                           (int64_t)pr->rows.size());
+    vb_expansion_sizes sz{};
+    st = vb_expand_structures(pr->rows.data(), ns, n_electrons, multiplicity, 0, &sz, nullptr, nullptr, nullptr,
+                              nullptr, nullptr, nullptr, nullptr);
+    if (st != VB_OK) {
+        delete pr;
+        return set_error(ctx, st, std::string(who) + ": expansion failed");
+    }
+    pr->alpha.resize(sz.n_alpha_strings);
+    pr->beta.resize(sz.n_beta_strings);
+    pr->det_a.resize(sz.n_determinants);
+    pr->det_b.resize(sz.n_determinants);
+    pr->term_off.resize(sz.n_determinants + 1);
+    pr->term_str.resize(sz.n_terms);
+    pr->term_coef.resize(sz.n_terms);
+    vb_expand_structures(pr->rows.data(), ns, n_electrons, multiplicity, 0, &sz, pr->alpha.data(), pr->beta.data(),
+                         pr->det_a.data(), pr->det_b.data(), pr->term_off.data(), pr->term_str.data(),
+                         pr->term_coef.data());
+    vb_expansion e{n_active, sz.n_alpha_electrons, sz.n_beta_electrons, sz.n_alpha_strings, sz.n_beta_strings,
+                   pr->alpha.data(), pr->beta.data(), sz.n_determinants, pr->det_a.data(), pr->det_b.data(),
+                   sz.n_structures, pr->term_off.data(), pr->term_str.data(), pr->term_coef.data()};
+    st = vb_hs_plan_create(ctx, &e, &pr->plan);
+    if (st != VB_OK) {
+        delete pr;
+        return st;
+    }
+    pr->n_str = sz.n_structures;
+    return VB_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 vb_status vb_scf_problem_create(vb_context* ctx, const vb_scf_input* in, vb_scf_problem** out) {
@@ -393,54 +457,54 @@ vb_status vb_scf_problem_create(vb_context* ctx, const vb_scf_input* in, vb_scf_
     pr->basis = make_basis(in->n_shells, in->shell_atom, in->shell_nprim, in->shell_exponents, in->shell_coefficients);
     pr->ao = ao_integrals(pr->basis, in->n_atoms, in->charges, in->coords);
     pr->chol = ao_pair_cholesky(pr->ao, pr->basis.n_bf, 1.0e-15, &pr->n_chol);
-    pr->n_act = in->n_active;
-    for (int a = 0; a < in->n_active; ++a) {
-        std::vector<int> f;
-        for (int t = in->orbital_offsets[a]; t < in->orbital_offsets[a + 1]; ++t) {
-            if (in->orbital_functions[t] < 0 || in->orbital_functions[t] >= pr->basis.n_bf) {
-                delete pr;
-                return set_error(ctx, VB_ERR_INVALID, "vb_scf_problem_create: orbital basis function out of range");
-            }
-            f.push_back(in->orbital_functions[t]);
-        }
-        pr->pattern.push_back(f);
+    const vb_status st = finish_problem(ctx, pr, in->n_active, in->orbital_offsets, in->orbital_functions,
+                                        in->n_electrons, in->multiplicity, in->structures, "vb_scf_problem_create");
+    if (st != VB_OK) return st;
+    *out = pr;
+    return VB_OK;
+}
+
+vb_status vb_scf_problem_create_from_integrals(vb_context* ctx, const vb_scf_integral_input* in,
+                                               vb_scf_problem** out) {
+    const char* who = "vb_scf_problem_create_from_integrals";
+    if (!ctx || !in || !out) return VB_ERR_INVALID;
+    *out = nullptr;
+    const int n = in->n_basis;
+    if (n < 1 || !in->S_ao || !in->h_ao || in->n_pairs < 0 || in->n_integrals < 0 ||
+        (in->n_pairs > 0 && (!in->pair_first || !in->pair_second)) ||
+        (in->n_integrals > 0 && (!in->integral_rows || !in->integral_columns || !in->integral_values)) ||
+        in->n_active < 1 || !in->orbital_offsets || !in->orbital_functions || !in->structures)
+        return set_error(ctx, VB_ERR_INVALID, std::string(who) + ": incomplete input");
+    const int P = n * (n + 1) / 2;
+    // AO pair graph -> packed pair index of each graph pair
+    std::vector<int> packed((size_t)in->n_pairs);
+    for (int64_t p = 0; p < in->n_pairs; ++p) {
+        const int a = in->pair_first[p], b = in->pair_second[p];
+        if (a < 0 || a >= n || b < 0 || b >= n)
+            return set_error(ctx, VB_ERR_INVALID, std::string(who) + ": AO pair index out of range");
+        const int hi = std::max(a, b), lo = std::min(a, b);
+        packed[p] = hi * (hi + 1) / 2 + lo;
     }
-    int64_t ns = 0;
-    vb_status st = vb_generate_structures(in->structures, in->n_active, in->n_electrons, in->multiplicity, 0, &ns,
-                                          nullptr, 0);
-    if (st != VB_OK) {
-        delete pr;
-        return set_error(ctx, st, std::string("vb_scf_problem_create: ") + vb_last_error(nullptr));
+    // dense pair matrix V over packed AO pairs; each unique (left, right) entry once, mirrored
+    std::vector<double> V((size_t)P * P, 0.0);
+    for (int64_t t = 0; t < in->n_integrals; ++t) {
+        const int64_t r = in->integral_rows[t], c = in->integral_columns[t];
+        if (r < 0 || r >= in->n_pairs || c < 0 || c >= in->n_pairs)
+            return set_error(ctx, VB_ERR_INVALID, std::string(who) + ": integral pair index out of range");
+        const size_t p = packed[r], q = packed[c];
+        V[p + q * P] = in->integral_values[t];
+        V[q + p * P] = in->integral_values[t];
     }
-    pr->rows.resize((size_t)ns * in->n_electrons);
-    vb_generate_structures(in->structures, in->n_active, in->n_electrons, in->multiplicity, 0, &ns, pr->rows.data(),
-                           (int64_t)pr->rows.size());
-    vb_expansion_sizes sz{};
-    st = vb_expand_structures(pr->rows.data(), ns, in->n_electrons, in->multiplicity, 0, &sz, nullptr, nullptr, nullptr,
-                              nullptr, nullptr, nullptr, nullptr);
-    if (st != VB_OK) {
-        delete pr;
-        return set_error(ctx, st, "vb_scf_problem_create: expansion failed");
-    }
-    pr->alpha.resize(sz.n_alpha_strings);
-    pr->beta.resize(sz.n_beta_strings);
-    pr->det_a.resize(sz.n_determinants);
-    pr->det_b.resize(sz.n_determinants);
-    pr->term_off.resize(sz.n_determinants + 1);
-    pr->term_str.resize(sz.n_terms);
-    pr->term_coef.resize(sz.n_terms);
-    vb_expand_structures(pr->rows.data(), ns, in->n_electrons, in->multiplicity, 0, &sz, pr->alpha.data(),
-                         pr->beta.data(), pr->det_a.data(), pr->det_b.data(), pr->term_off.data(), pr->term_str.data(),
-                         pr->term_coef.data());
-    vb_expansion e{in->n_active, sz.n_alpha_electrons, sz.n_beta_electrons, sz.n_alpha_strings, sz.n_beta_strings,
-                   pr->alpha.data(), pr->beta.data(), sz.n_determinants, pr->det_a.data(), pr->det_b.data(),
-                   sz.n_structures, pr->term_off.data(), pr->term_str.data(), pr->term_coef.data()};
-    st = vb_hs_plan_create(ctx, &e, &pr->plan);
-    if (st != VB_OK) {
-        delete pr;
-        return st;
-    }
-    pr->n_str = sz.n_structures;
+    auto pr = new vb_scf_problem();
+    pr->ctx = ctx;
+    pr->basis.n_bf = n;
+    pr->ao.S.assign(in->S_ao, in->S_ao + (size_t)n * n);
+    pr->ao.H.assign(in->h_ao, in->h_ao + (size_t)n * n);
+    pr->ao.enuc = in->nuclear_repulsion;
+    pr->chol = pair_cholesky(P, [&](int p, int q) { return V[(size_t)p + (size_t)q * P]; }, 1.0e-15, &pr->n_chol);
+    const vb_status st = finish_problem(ctx, pr, in->n_active, in->orbital_offsets, in->orbital_functions,
+                                        in->n_electrons, in->multiplicity, in->structures, who);
+    if (st != VB_OK) return st;
     *out = pr;
     return VB_OK;
 }
@@ -481,7 +545,21 @@ vb_status vb_scf_ao_integrals(const vb_scf_problem* pr, double* S_ao, double* h_
     if (!pr) return VB_ERR_INVALID;
     if (S_ao) std::copy(pr->ao.S.begin(), pr->ao.S.end(), S_ao);
     if (h_ao) std::copy(pr->ao.H.begin(), pr->ao.H.end(), h_ao);
-    if (eri_ao) std::copy(pr->ao.eri.begin(), pr->ao.eri.end(), eri_ao);
+    if (eri_ao && !pr->ao.eri.empty()) std::copy(pr->ao.eri.begin(), pr->ao.eri.end(), eri_ao);
+    if (eri_ao && pr->ao.eri.empty()) {
+        // a problem built from AO pair integrals: (mu nu|la si) from its pair Cholesky vectors
+        const int n = pr->basis.n_bf, nc = pr->n_chol;
+        auto pk = [](int a, int b) { return a > b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; };
+        for (int m = 0; m < n; ++m)
+            for (int v = 0; v < n; ++v)
+                for (int l = 0; l < n; ++l)
+                    for (int q = 0; q < n; ++q) {
+                        const size_t p1 = pk(m, v), p2 = pk(l, q);
+                        double acc = 0.0;
+                        for (int c = 0; c < nc; ++c) acc += pr->chol[c + (size_t)nc * p1] * pr->chol[c + (size_t)nc * p2];
+                        eri_ao[(size_t)m + (size_t)n * (v + (size_t)n * (l + (size_t)n * q))] = acc;
+                    }
+    }
     return VB_OK;
 }
 

@@ -64,6 +64,16 @@ class _ScfInput(ctypes.Structure):
                 ("multiplicity", ctypes.c_int32), ("structures", ctypes.c_char_p)]
 
 
+class _ScfIntegralInput(ctypes.Structure):
+    _fields_ = [("n_basis", ctypes.c_int32), ("S_ao", ctypes.c_void_p), ("h_ao", ctypes.c_void_p),
+                ("n_pairs", ctypes.c_int64), ("pair_first", ctypes.c_void_p), ("pair_second", ctypes.c_void_p),
+                ("n_integrals", ctypes.c_int64), ("integral_rows", ctypes.c_void_p),
+                ("integral_columns", ctypes.c_void_p), ("integral_values", ctypes.c_void_p),
+                ("nuclear_repulsion", ctypes.c_double), ("n_active", ctypes.c_int32),
+                ("orbital_offsets", ctypes.c_void_p), ("orbital_functions", ctypes.c_void_p),
+                ("n_electrons", ctypes.c_int32), ("multiplicity", ctypes.c_int32), ("structures", ctypes.c_char_p)]
+
+
 class _ScfOptions(ctypes.Structure):
     _fields_ = [("max_iterations", ctypes.c_int32), ("gradient_tolerance", ctypes.c_double),
                 ("history_size", ctypes.c_int32), ("armijo", ctypes.c_double)]
@@ -91,8 +101,9 @@ EXPORTED_SYMBOLS = (
     "vb_hs_plan_gradient", "vb_hs_plan_root_gradient",
     "vb_lowest_root", "vb_engine_create", "vb_engine_destroy", "vb_engine_last_error", "vb_engine_add_instance",
     "vb_engine_evaluate_instances", "vb_engine_submit_scf", "vb_engine_poll", "vb_engine_pending",
-    "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_destroy", "vb_scf_problem_sizes",
-    "vb_scf_ao_integrals", "vb_scf_energy_gradient", "vb_solve_scf",
+    "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_create_from_integrals", "vb_scf_problem_destroy",
+    "vb_scf_problem_sizes", "vb_scf_ao_integrals", "vb_scf_energy_gradient", "vb_solve_scf",
+    "vb_autotune_report", "vb_autotune_clear",
 )
 
 PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
@@ -115,6 +126,8 @@ def load_library(path: str = LIB_PATH):
     lib.vb_context_set_stream.argtypes = [P, P]
     lib.vb_context_synchronize.argtypes = [P]
     lib.vb_context_set_barrier_spin_limit.argtypes = [P, c.c_longlong]
+    lib.vb_autotune_report.argtypes = [c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
+    lib.vb_autotune_clear.argtypes = []
     lib.vb_last_error.argtypes = [P]
     lib.vb_last_error.restype = c.c_char_p
     lib.vb_context_memory.argtypes = [P, c.POINTER(c.c_size_t), c.POINTER(c.c_size_t)]
@@ -146,6 +159,7 @@ def load_library(path: str = LIB_PATH):
                                    c.POINTER(c.c_int)]
     lib.vb_ao_integrals_s.argtypes = [c.POINTER(_ScfInput), P, P, P, c.POINTER(c.c_double)]
     lib.vb_scf_problem_create.argtypes = [P, c.POINTER(_ScfInput), c.POINTER(P)]
+    lib.vb_scf_problem_create_from_integrals.argtypes = [P, c.POINTER(_ScfIntegralInput), c.POINTER(P)]
     lib.vb_scf_problem_destroy.argtypes = [P]
     lib.vb_scf_problem_sizes.argtypes = [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int),
                                          c.POINTER(c.c_double)]
@@ -485,6 +499,51 @@ def _scf_input(mol, pattern, n_electrons, multiplicity, structures, keep):
                      multiplicity, kw)
 
 
+def _scf_integral_input(ints, pattern, n_electrons, multiplicity, structures, keep):
+    S = _c(np.asarray(ints["S_ao"]).T, np.float64)
+    hh = _c(np.asarray(ints["h_ao"]).T, np.float64)
+    pf = _c(ints["pair_first"], np.int32)
+    ps = _c(ints["pair_second"], np.int32)
+    rows = _c(ints["rows"], np.int64)
+    cols = _c(ints["columns"], np.int64)
+    vals = _c(ints["values"], np.float64)
+    offsets = np.concatenate([[0], np.cumsum([len(p) for p in pattern])]).astype(np.int32)
+    funcs = np.array([m for p in pattern for m in p], dtype=np.int32)
+    kw = structures.encode()
+    keep.extend([S, hh, pf, ps, rows, cols, vals, offsets, funcs, kw])
+    return _ScfIntegralInput(S.shape[0], _ptr(S).value, _ptr(hh).value, pf.size, _ptr(pf).value, _ptr(ps).value,
+                             vals.size, _ptr(rows).value, _ptr(cols).value, _ptr(vals).value,
+                             float(ints["nuclear_repulsion"]), len(pattern), _ptr(offsets).value,
+                             _ptr(funcs).value if funcs.size else None, n_electrons, multiplicity, kw)
+
+
+def autotune_report() -> str:
+    """The autotuner's cached choices, one line per (kernel, shape, device) key."""
+    lib = load_library()
+    need = ctypes.c_size_t(0)
+    lib.vb_autotune_report(None, 0, ctypes.byref(need))
+    buf = ctypes.create_string_buffer(max(1, need.value))
+    lib.vb_autotune_report(buf, need.value, ctypes.byref(need))
+    return buf.value.decode()
+
+
+def autotune_clear():
+    load_library().vb_autotune_clear()
+
+
+def ao_pair_graph(eri, threshold: float = 0.0):
+    """The unique-integral stream of an AO pair graph from a dense (mu nu|la si) [n,n,n,n]: pairs
+    (mu >= nu), and each unordered pair of pairs once with |value| > threshold."""
+    n = eri.shape[0]
+    first, second = np.tril_indices(n)
+    P = first.size
+    V = eri[first[:, None], second[:, None], first[None, :], second[None, :]]
+    r, c = np.tril_indices(P)
+    keep = np.abs(V[r, c]) > threshold
+    return dict(pair_first=first.astype(np.int32), pair_second=second.astype(np.int32),
+                rows=r[keep].astype(np.int64), columns=c[keep].astype(np.int64), values=V[r, c][keep])
+
+
 def ao_integrals_s(mol):
     """(S_ao, h_ao, eri_ao [n,n,n,n], nuclear repulsion) of an s-shell molecule (host only)."""
     keep = []
@@ -503,14 +562,23 @@ class ScfProblem:
     """A VBSCF problem (molecule, HAO pattern, structure class) with its plan on the device."""
 
     def __init__(self, ctx: "Context", mol, pattern, n_electrons: int, multiplicity: int = 1,
-                 structures: str = "COV"):
+                 structures: str = "COV", integrals=None):
+        """mol: an s-shell molecule (its AO integrals are computed by the library), or None with
+        `integrals` = dict(S_ao, h_ao, pair_first, pair_second, rows, columns, values,
+        nuclear_repulsion): AO integrals the caller already has, as an AO pair graph's unique
+        integral stream (vb_scf_problem_create_from_integrals)."""
         self.ctx = ctx
         self.mol = mol
         self.pattern = pattern
         self._keep = []
-        inp = _scf_input(mol, pattern, n_electrons, multiplicity, structures, self._keep)
         h = ctypes.c_void_p()
-        _check(load_library().vb_scf_problem_create(ctx.handle, ctypes.byref(inp), ctypes.byref(h)), ctx.handle)
+        if integrals is None:
+            inp = _scf_input(mol, pattern, n_electrons, multiplicity, structures, self._keep)
+            _check(load_library().vb_scf_problem_create(ctx.handle, ctypes.byref(inp), ctypes.byref(h)), ctx.handle)
+        else:
+            inp = _scf_integral_input(integrals, pattern, n_electrons, multiplicity, structures, self._keep)
+            _check(load_library().vb_scf_problem_create_from_integrals(ctx.handle, ctypes.byref(inp), ctypes.byref(h)),
+                   ctx.handle)
         self._h = h
         ctx._adopt(self)
         nb, na, ns, en = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
