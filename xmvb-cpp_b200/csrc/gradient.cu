@@ -902,7 +902,7 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
         b.careful_list = beta ? p->list_b.as<unsigned long long>() : p->list_a.as<unsigned long long>();
         err = cudaMemsetAsync(b.careful_count, 0, sizeof(unsigned long long), s);
         if (err != cudaSuccess) break;
-        const bool fast = k <= 8 && fast_spin_supported(n, k, R);
+        const bool fast = k <= 8 && frame_spin_supported(n, k, R);
         if (fast) {
             // chunks of whole work items (left string u, right strings v0 .. v0 + 127): per chunk
             // Q = L_f^T adj_U (the u-adjoint contracted with every factor column at every packed

@@ -117,9 +117,6 @@ size_t gradient_stack_bytes();
 cudaError_t launch_prepare_tables(int n, const double* eri, double* gamma, double* kfull, cudaStream_t stream);
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs,
                                       double* lf, int ld, int* meta, cudaStream_t stream);
-size_t left_table_doubles(int n, int k, int R);
-size_t factored_spin_smem_bytes(int n, int k, int R);
-bool fast_spin_supported(int n, int k, int R);
 // Spin-pair records of one string table: the per-left-string frame tables first
 // (launch_spin_tables, nothing when the register path does not apply), then launch_spin_pairs
 // (the frame kernel and the exact path for the blocks it lists, or the exact path for all).

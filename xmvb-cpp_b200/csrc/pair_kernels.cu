@@ -3,20 +3,17 @@
 //  * prepare_tables: the unpacked pair kernel K[p][q] = (p|q) over packed orbital pairs and the
 //    antisymmetrized same-spin table Gamma[(i<k)][(j<l)] = (ij|kl) - (il|kj) used by the
 //    same-spin two-electron sum (hamiltonian.cpp:83-123 sums exactly these differences).
-//  * spin_pairs_fast<K>: one thread per unordered spin-string pair, K x K overlap block in
-//    registers, Gauss-Jordan inversion with partial pivoting (row interchanges tracked as a
-//    label permutation, no dynamic register indexing), determinant, first cofactors
-//    A = det X^{-T}, one-electron and same-spin two-electron energies from shared-memory
-//    tables.  A block is accepted only when ||X||_F ||X^{-1}||_F < 1e8 (kCertificate2): then the
+//  * factor_pair_kernel: pivoted LDL^T of the pair kernel, K = sum_m sigma_m l_m l_m^T.
+//  * the register-resident spin-pair path lives in spin_frame.cu (left-string frame kernels); a
+//    block is accepted there only under the conditioning certificate (kCertificate2): then the
 //    last pivot of a complete-pivoting LU is at least 1 / ||X^{-1}||_F and the first at most
 //    ||X||_F, so their ratio stays far above 1e-12 and the reference's FullPivLU would also find
 //    full rank (overlap.cpp:60-71).  Every other block is appended to a list for the exact kernel.
 //  * spin_pairs_exact<KM>: complete-pivoting LU / Jacobi SVD with the reference semantics
 //    (device_algebra.cuh) for listed blocks, one thread per block, local arrays bounded by KM.
-//  * full_pairs<KB>: one thread per determinant pair (d <= e) of a band of columns:
-//    S = S_a S_b, H = H_a S_b + H_b S_a + sum A_a(r,c) A_b(r',c') (r c | r' c')
-//    (evaluator.cpp:95-148, 354-384), the opposite-spin sum as k_a^2 k_b^2 gathers of the
-//    shared-memory pair kernel against the beta cofactors held in registers.
+//  * full_pairs_kernel: one thread per determinant pair (d <= e) of a band of columns:
+//    S = S_a S_b, H = H_a S_b + H_b S_a + sum_m sigma_m u_a[m] u_b[m] (evaluator.cpp:95-148,
+//    354-384 with the opposite-spin term in factored form), folded over the spin-flip orbit.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -76,43 +73,32 @@ __global__ void prepare_tables_kernel(int n, const double* __restrict__ eri, dou
 // Stops when the largest remaining |diagonal| falls to rel_tol times the largest initial one;
 // the dropped remainder then perturbs any opposite-spin energy by at most
 // rel_tol * max|K_pp| * ||p_a||_1 ||p_b||_1.  Columns are emitted positive-sign first.
-// The working matrix lives in shared memory when it fits (in_smem), else in `work`.
+// The working matrix lives in shared memory when it fits (in_smem), else in `work`; the current
+// column is always in shared memory.  Two barriers per step: the warp that updates a row also
+// reports the row's new diagonal, so the next pivot search is a reduction over per-warp maxima.
 __global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* __restrict__ kfull,
                                                           double* __restrict__ work_g, double* __restrict__ cols,
                                                           int* __restrict__ signs, double* __restrict__ lf, int ld,
                                                           int* __restrict__ meta, double rel_tol, int in_smem) {
     extern __shared__ double fsm[];
     double* work = in_smem ? fsm : work_g;
-    int* used = reinterpret_cast<int*>(in_smem ? fsm + (size_t)np * np : fsm);
+    double* lc = in_smem ? fsm + (size_t)np * np : fsm;  // current column
+    int* used = reinterpret_cast<int*>(lc + np);
     int* slot_col = used + np;  // emission map: output slot -> column
     __shared__ double red_v[32];
     __shared__ int red_i[32];
-    __shared__ double s_piv;
-    __shared__ int s_p;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nwarps = nt >> 5;
     const long long n2 = (long long)np * np;
     for (long long i = tid; i < n2; i += nt) work[i] = kfull[i];
     for (int i = tid; i < np; i += nt) used[i] = 0;
     __syncthreads();
-    double local = 0.0;
-    for (int i = tid; i < np; i += nt) local = fmax(local, fabs(work[(long long)i * np + i]));
-    for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(0xffffffffu, local, o));
-    if (lane == 0) red_v[warp] = local;
-    __syncthreads();
-    if (tid < 32) {
-        double v = tid < nwarps ? red_v[tid] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (tid == 0) s_piv = v;
-    }
-    __syncthreads();
-    const double cut = rel_tol * s_piv;
-    int m = 0;
-    for (; m < np; ++m) {
+    // per-warp (max |diagonal|, row) over the warp's rows i = warp, warp + nwarps, ...
+    auto warp_best = [&](int exclude) {
         double best = -1.0;
         int bi = -1;
-        for (int i = tid; i < np; i += nt)
-            if (!used[i]) {
+        for (int i = warp + nwarps * lane; i < np; i += nwarps * 32)
+            if (!used[i] && i != exclude) {
                 const double v = fabs(work[(long long)i * np + i]);
                 if (v > best || (v == best && i < bi)) {
                     best = v;
@@ -131,43 +117,56 @@ __global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* 
             red_v[warp] = best;
             red_i[warp] = bi;
         }
-        __syncthreads();
-        if (tid < 32) {
-            double v = tid < nwarps ? red_v[tid] : -1.0;
-            int vi = tid < nwarps ? red_i[tid] : -1;
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-                const int oi = __shfl_xor_sync(0xffffffffu, vi, o);
-                if (ov > v || (ov == v && oi >= 0 && (vi < 0 || oi < vi))) {
-                    v = ov;
-                    vi = oi;
-                }
-            }
-            if (tid == 0) {
-                s_p = vi;
-                s_piv = vi >= 0 ? work[(long long)vi * np + vi] : 0.0;
+    };
+    auto block_best = [&](double* v_out, int* i_out) {
+        double v = -1.0;
+        int vi = -1;
+        for (int w = 0; w < nwarps; ++w) {
+            const double ov = red_v[w];
+            const int oi = red_i[w];
+            if (ov > v || (ov == v && oi >= 0 && (vi < 0 || oi < vi))) {
+                v = ov;
+                vi = oi;
             }
         }
-        __syncthreads();
-        const int p = s_p;
-        const double piv = s_piv;
+        *v_out = v;
+        *i_out = vi;
+    };
+    warp_best(-1);
+    __syncthreads();
+    double dmax = 0.0;
+    int p0 = -1;
+    block_best(&dmax, &p0);
+    const double cut = rel_tol * fmax(dmax, 0.0);
+    int m = 0;
+    for (; m < np; ++m) {
+        double best;
+        int p;
+        block_best(&best, &p);
+        const double piv = p >= 0 ? work[(long long)p * np + p] : 0.0;
         if (p < 0 || !(fabs(piv) > cut) || fabs(piv) == 0.0) break;
         const double inv = 1.0 / sqrt(fabs(piv));
         const int sgn = piv > 0.0 ? 1 : -1;
         double* l = cols + (long long)m * np;
-        for (int i = tid; i < np; i += nt) l[i] = used[i] ? 0.0 : work[(long long)i * np + p] * inv;
+        for (int i = tid; i < np; i += nt) {
+            const double v = used[i] ? 0.0 : work[(long long)i * np + p] * inv;
+            lc[i] = v;
+            l[i] = v;
+        }
         if (tid == 0) signs[m] = sgn;
-        __syncthreads();
-        if (tid == 0) used[p] = 1;
-        __syncthreads();
-        // rank-1 update of the remaining block, one warp per row
+        __syncthreads();  // the column is complete; every thread has read red_v / red_i
+        // rank-1 update of the remaining block (pivot row and column excluded), one warp per row;
+        // the updated diagonals feed the next pivot search
         for (int i = warp; i < np; i += nwarps) {
-            if (used[i]) continue;
-            const double li = (double)sgn * l[i];
+            if (used[i] || i == p) continue;
+            const double li = (double)sgn * lc[i];
             double* row = work + (long long)i * np;
             for (int j = lane; j < np; j += 32)
-                if (!used[j]) row[j] = fma(-li, l[j], row[j]);
+                if (!used[j] && j != p) row[j] = fma(-li, lc[j], row[j]);
         }
+        __syncwarp();
+        if (tid == 0) used[p] = 1;
+        warp_best(p);
         __syncthreads();
     }
     if (tid == 0) {
@@ -183,409 +182,6 @@ __global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* 
         for (int slot = lane; slot < ld; slot += 32)
             lf[(long long)q * ld + slot] = slot < m ? cols[(long long)slot_col[slot] * np + q] : 0.0;
 }
-
-// Table geometry of the left-string decomposition (shared by host and device code).
-//   nb_max(K)   complement orbitals held per left string (n - K <= nb_max)
-//   kf(K)       GEMM depth: nb_max K entries of V, one trace slot, padded to 4
-//   kfs(K)      shared-memory row stride >= kf with stride % 16 in {4, 12} (conflict-free
-//               m8n8k4 fragment loads: the four rows of a half-warp land on disjoint banks)
-//   nt_of(R)    8-row tiles covering the R + 1 table rows (factor columns and h)
-__host__ __device__ constexpr int nb_max(int k) { return k <= 4 ? k + 4 : k; }
-__host__ __device__ constexpr int kf(int k) { return (nb_max(k) * k + 1 + 3) / 4 * 4; }
-__host__ __device__ constexpr int kfs(int k) {
-    return (kf(k) % 16 == 4 || kf(k) % 16 == 12) ? kf(k) : kf(k) + 4;
-}
-__host__ __device__ constexpr int nt_of(int R) { return (R + 1 + 7) / 8; }
-__host__ __device__ constexpr int table_stride_of(int k, int R) { return nt_of(R) * 8 * kfs(k); }
-
-__device__ __forceinline__ void mma_f64(double (&c)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                 : "+d"(c[0]), "+d"(c[1])
-                 : "d"(a), "d"(b));
-}
-
-// Complement decomposition per left string L (K orbitals; Lbar = the other NB = n - K orbitals).
-// For a right string R with X = S[R, L], any n x K block W gives
-//   tr(X^{-1} W[R, :]) = tr(T) + <V, Y^T>,   W = S[:, L] T + I[:, Lbar] V,
-// with T = S[L,L]^{-1} W[L,:], V = W[Lbar,:] - S[Lbar,L] T, and Y = X^{-1} I[R, Lbar], a column
-// selection of X^{-1}.  With W = B_m[:, L] (B_m[i][j] = lf(pair(i, j), m)) this is
-// u[m] / det, and with W = h[:, L] it is H_1e / det (Jacobi's formula: both are first-order
-// terms sum_{r,c} A(r,c) W(R_r, L_c) of det(X + eps W[R, :])).  T and V depend on L only.
-//
-// Table of left string L: row m (m < R factor columns, m = R one-electron h) of kfs(K) doubles
-// holds V_m[b][c] at b K + c (b < nb_max(K), zero rows for b >= NB), tr T_m at nb_max(K) K,
-// zeros elsewhere; rows R + 1 .. 8 nt_of(R) - 1 are zero.
-template <int K>
-__global__ void __launch_bounds__(128) left_string_tables(SpinTableArgs a, double* __restrict__ tables) {
-    constexpr int NBMAX = nb_max(K);
-    constexpr int KFS = kfs(K);
-    const int table_stride = table_stride_of(K, a.R);
-    __shared__ double sInv[K * K];
-    __shared__ int sL[K], sLb[NBMAX];
-    const int n = a.n;
-    const int nb = n - K;
-    const long long u = blockIdx.x;
-    if (u >= a.n_strings) return;
-    double* tab = tables + u * (long long)table_stride;
-    for (int i = threadIdx.x; i < table_stride; i += blockDim.x) tab[i] = 0.0;
-    if (threadIdx.x == 0) {
-        const uint64_t w0 = a.occ[2 * u];
-        int L[K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) L[c] = (int)((w0 >> (8 * c)) & 0xFFu);
-        uint64_t mask = 0;
-#pragma unroll
-        for (int c = 0; c < K; ++c) mask |= 1ull << L[c];
-        int q = 0;
-        for (int i = 0; i < n && q < NBMAX; ++i)
-            if (!((mask >> i) & 1)) sLb[q++] = i;
-        // S[L, L]^{-1} by Gauss-Jordan (S[L, L] is a principal block of an SPD matrix)
-        double m[K][2 * K];
-#pragma unroll
-        for (int r = 0; r < K; ++r)
-#pragma unroll
-            for (int c = 0; c < 2 * K; ++c) m[r][c] = c < K ? a.S[L[r] * n + L[c]] : (c - K == r ? 1.0 : 0.0);
-#pragma unroll
-        for (int s = 0; s < K; ++s) {
-            const double ip = 1.0 / m[s][s];
-#pragma unroll
-            for (int c = 0; c < 2 * K; ++c) m[s][c] *= ip;
-#pragma unroll
-            for (int r = 0; r < K; ++r) {
-                if (r == s) continue;
-                const double f = m[r][s];
-#pragma unroll
-                for (int c = 0; c < 2 * K; ++c) m[r][c] = fma(-f, m[s][c], m[r][c]);
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < K; ++r) {
-            sL[r] = L[r];
-#pragma unroll
-            for (int c = 0; c < K; ++c) sInv[r * K + c] = m[r][K + c];
-        }
-    }
-    __syncthreads();
-    const int blocks = a.R + 1;
-    // one thread per (row m, column c): T[:, c] then V[:, c]; the c == 0 thread adds tr T_m
-    for (int idx = threadIdx.x; idx < blocks * K; idx += blockDim.x) {
-        const int mm = idx / K, c = idx % K;
-        auto wval = [&](int i, int j) {
-            return mm < a.R ? __ldg(a.lf + (long long)dev::pair_index(i, j) * a.ld + mm) : __ldg(a.h + i * n + j);
-        };
-        const int lc = sL[c];
-        double wl[K];
-#pragma unroll
-        for (int ap = 0; ap < K; ++ap) wl[ap] = wval(sL[ap], lc);
-        double tc[K];
-#pragma unroll
-        for (int r = 0; r < K; ++r) {
-            double acc = 0.0;
-#pragma unroll
-            for (int ap = 0; ap < K; ++ap) acc = fma(sInv[r * K + ap], wl[ap], acc);
-            tc[r] = acc;
-        }
-        double* row = tab + (long long)mm * KFS;
-        for (int b = 0; b < nb && b < NBMAX; ++b) {
-            const int ib = sLb[b];
-            double acc = wval(ib, lc);
-#pragma unroll
-            for (int r = 0; r < K; ++r) acc = fma(-__ldg(a.S + ib * n + sL[r]), tc[r], acc);
-            row[b * K + c] = acc;
-        }
-        if (c == 0) {
-            double tr = 0.0;
-            for (int cc = 0; cc < K; ++cc) {
-                const int l2 = sL[cc];
-                double acc = 0.0;
-#pragma unroll
-                for (int ap = 0; ap < K; ++ap) acc = fma(sInv[cc * K + ap], wval(sL[ap], l2), acc);
-                tr += acc;
-            }
-            row[NBMAX * K] = tr;
-        }
-    }
-}
-
-// One CTA per contiguous range of work items (left string u, right strings v0 .. v0 + 127);
-// the left string's tables live in shared memory and are reloaded only when u changes.
-// Phase A (a thread per spin pair): overlap block, Gauss-Jordan inverse, certificate, the
-// same-spin two-electron term, and the row Y of the pair (with 1 in the trace slot) to shared
-// memory.  Phase B (a warp per 32 pairs): [u | H_1e] / det = Y V^T on the FP64 tensor cores
-// (mma.sync m8n8k4), then the records.
-template <int K>
-__global__ void __launch_bounds__(kSpinBlock) spin_pairs_fast(SpinTableArgs a, const double* __restrict__ tables) {
-    extern __shared__ double smem[];
-    constexpr int CP = K * (K - 1) / 2;
-    constexpr int NBMAX = nb_max(K);
-    constexpr int KF = kf(K);
-    constexpr int KFS = kfs(K);
-    const int n = a.n;
-    const int nb = n - K;
-    const int gd = a.gamma_dim;
-    const int R = a.R;
-    const int NT = nt_of(R);
-    const int table_stride = table_stride_of(K, R);
-    double* sT = smem;                                // left-string table, row m = block m
-    double* sY = sT + table_stride;                   // [pair][f] rows of Y
-    double* sS = sY + kSpinBlock * KFS;               // [c][i] = S(i, L_c)
-    double* sG = sS + ((K * n + 1) / 2 * 2);          // [cp][rp] = gamma(rp, pair(L_c1, L_c2))
-    __shared__ int sLb[NBMAX];
-    const long long N = a.n_strings;
-    const int per = (a.n_items + gridDim.x - 1) / gridDim.x;
-    const int item_begin = blockIdx.x * per;
-    const int item_end = min(a.n_items, item_begin + per);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    long long loaded_u = -1;
-    int L[K];
-    for (int item = item_begin; item < item_end; ++item) {
-        const int2 it = a.items[item];
-        const long long u = it.x;
-        if (u != loaded_u) {
-            __syncthreads();
-            const uint64_t wl = __ldg(a.occ + 2 * u);
-#pragma unroll
-            for (int c = 0; c < K; ++c) L[c] = (int)((wl >> (8 * c)) & 0xFFu);
-            if (threadIdx.x == 0) {
-                uint64_t mask = 0;
-#pragma unroll
-                for (int c = 0; c < K; ++c) mask |= 1ull << L[c];
-                int q = 0;
-                for (int i = 0; i < n && q < NBMAX; ++i)
-                    if (!((mask >> i) & 1)) sLb[q++] = i;
-            }
-            for (int row = warp; row < K; row += nwarps) {
-                int lc = 0;
-#pragma unroll
-                for (int cc = 0; cc < K; ++cc)
-                    if (cc == row) lc = L[cc];
-                for (int i = lane; i < n; i += 32) sS[row * n + i] = __ldg(a.S + lc * n + i);
-            }
-            if (K >= 2) {
-                for (int cp = warp; cp < CP; cp += nwarps) {
-                    int c2 = 1;
-                    while ((c2 + 1) * c2 / 2 <= cp) ++c2;
-                    const int c1 = cp - c2 * (c2 - 1) / 2;
-                    int l1 = 0, l2 = 0;
-#pragma unroll
-                    for (int cc = 0; cc < K; ++cc) {
-                        if (cc == c1) l1 = L[cc];
-                        if (cc == c2) l2 = L[cc];
-                    }
-                    const double* src = a.gamma + (long long)dev::anti_index(l1, l2) * gd;
-                    for (int rp = lane; rp < gd; rp += 32) sG[cp * gd + rp] = __ldg(src + rp);
-                }
-            }
-            const double* tsrc = tables + u * (long long)table_stride;
-            for (int i = threadIdx.x; i < table_stride; i += blockDim.x) sT[i] = __ldg(tsrc + i);
-            loaded_u = u;
-            __syncthreads();
-        }
-        // ---------------- phase A ----------------
-        const long long v = (long long)it.y + threadIdx.x;
-        bool ok = false;
-        double det = 0.0, h2 = 0.0;
-        long long t = 0;
-        double* yrow = sY + threadIdx.x * KFS;
-        if (v < N) {
-            t = record_index(u, v, N);
-            const uint64_t wr = __ldg(a.occ + 2 * v);
-            int Rr[K];
-#pragma unroll
-            for (int c = 0; c < K; ++c) Rr[c] = (int)((wr >> (8 * c)) & 0xFFu);
-            double x[K][K];
-            double nx2 = 0.0;
-#pragma unroll
-            for (int r = 0; r < K; ++r)
-#pragma unroll
-                for (int c = 0; c < K; ++c) {
-                    x[r][c] = sS[c * n + Rr[r]];
-                    nx2 = fma(x[r][c], x[r][c], nx2);
-                }
-            constexpr int K0 = K <= 3 ? K : 1;
-            double x0[K0][K0];
-            if (K <= 3) {
-#pragma unroll
-                for (int r = 0; r < K0; ++r)
-#pragma unroll
-                    for (int c = 0; c < K0; ++c) x0[r][c] = x[r][c];
-            }
-            int lab[K];
-#pragma unroll
-            for (int r = 0; r < K; ++r) lab[r] = r;
-            det = 1.0;
-#pragma unroll
-            for (int s = 0; s < K; ++s) {
-                int p = s;
-                double best = fabs(x[s][s]);
-#pragma unroll
-                for (int i = s + 1; i < K; ++i) {
-                    const double av = fabs(x[i][s]);
-                    if (av > best) {
-                        best = av;
-                        p = i;
-                    }
-                }
-#pragma unroll
-                for (int i = s + 1; i < K; ++i) {
-                    const bool sw = (p == i);
-#pragma unroll
-                    for (int j = 0; j < K; ++j) {
-                        const double a0 = x[s][j], a1 = x[i][j];
-                        x[s][j] = sw ? a1 : a0;
-                        x[i][j] = sw ? a0 : a1;
-                    }
-                    const int l0 = lab[s], l1 = lab[i];
-                    lab[s] = sw ? l1 : l0;
-                    lab[i] = sw ? l0 : l1;
-                }
-                if (p != s) det = -det;
-                const double piv = x[s][s];
-                det *= piv;
-                const double ip = 1.0 / piv;
-                x[s][s] = 1.0;
-#pragma unroll
-                for (int j = 0; j < K; ++j) x[s][j] *= ip;
-#pragma unroll
-                for (int i = 0; i < K; ++i) {
-                    if (i == s) continue;
-                    const double f = x[i][s];
-                    x[i][s] = 0.0;
-#pragma unroll
-                    for (int j = 0; j < K; ++j) x[i][j] = fma(-f, x[s][j], x[i][j]);
-                }
-            }
-            double ni2 = 0.0;
-#pragma unroll
-            for (int r = 0; r < K; ++r)
-#pragma unroll
-                for (int c = 0; c < K; ++c) ni2 = fma(x[r][c], x[r][c], ni2);
-            ok = isfinite(det) && det != 0.0 && (nx2 * ni2 < kCertificate2);
-            if (!ok) {
-                const unsigned long long slot = atomicAdd(a.careful_count, 1ull);
-                a.careful_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
-#pragma unroll
-                for (int f = 0; f < KFS; ++f) yrow[f] = 0.0;
-            } else {
-                // x holds C = (P X)^{-1}: X^{-1}[c][lab[j]] = C[c][j]; row lab[j] carries orbital Rp[j]
-                int Rp[K];
-#pragma unroll
-                for (int j = 0; j < K; ++j) Rp[j] = (int)((wr >> (8 * lab[j])) & 0xFFu);
-                if (K == 2) {
-                    h2 = sG[dev::anti_index(Rr[0], Rr[1])];
-                } else if (K == 3) {
-#pragma unroll
-                    for (int r1 = 0; r1 < K0; ++r1)
-#pragma unroll
-                        for (int r2 = r1 + 1; r2 < K0; ++r2)
-#pragma unroll
-                            for (int c1 = 0; c1 < K0; ++c1)
-#pragma unroll
-                                for (int c2 = c1 + 1; c2 < K0; ++c2) {
-                                    const double sign = ((r1 + r2 + c1 + c2) & 1) ? -1.0 : 1.0;
-                                    const int cp = c2 * (c2 - 1) / 2 + c1;
-                                    h2 = fma(sG[cp * gd + dev::anti_index(Rr[r1], Rr[r2])],
-                                             sign * x0[3 - r1 - r2][3 - c1 - c2], h2);
-                                }
-                } else if (K >= 4) {
-                    double acc2 = 0.0;
-#pragma unroll
-                    for (int j1 = 0; j1 < K; ++j1)
-#pragma unroll
-                        for (int j2 = j1 + 1; j2 < K; ++j2) {
-                            const int ra = Rp[j1], rb = Rp[j2];
-                            const bool ordered = ra < rb;
-                            const int rp = dev::anti_index(ordered ? ra : rb, ordered ? rb : ra);
-                            double part = 0.0;
-#pragma unroll
-                            for (int c1 = 0; c1 < K; ++c1)
-#pragma unroll
-                                for (int c2 = c1 + 1; c2 < K; ++c2) {
-                                    const double m2 = fma(x[c1][j1], x[c2][j2], -x[c2][j1] * x[c1][j2]);
-                                    part = fma(sG[(c2 * (c2 - 1) / 2 + c1) * gd + rp], m2, part);
-                                }
-                            acc2 += ordered ? part : -part;
-                        }
-                    h2 = det * acc2;
-                }
-                // Y[b K + c] = X^{-1}[c][r] for the row r carrying orbital Lbar_b (0 if Lbar_b not in R)
-#pragma unroll
-                for (int b = 0; b < NBMAX; ++b) {
-                    const int ib = b < nb ? sLb[b] : -1;
-#pragma unroll
-                    for (int c = 0; c < K; ++c) {
-                        double y = 0.0;
-#pragma unroll
-                        for (int j = 0; j < K; ++j) y = (Rp[j] == ib) ? x[c][j] : y;
-                        yrow[b * K + c] = y;
-                    }
-                }
-                yrow[NBMAX * K] = 1.0;
-#pragma unroll
-                for (int f = NBMAX * K + 1; f < KFS; ++f) yrow[f] = 0.0;
-            }
-        } else {
-#pragma unroll
-            for (int f = 0; f < KFS; ++f) yrow[f] = 0.0;
-        }
-        __syncwarp();
-        // ---------------- phase B ----------------
-        const double* Yw = sY + (warp * 32) * KFS;
-        const int g = lane >> 2, tq = lane & 3;
-        double det_m[4], h2_m[4];
-        long long t_m[4];
-        bool ok_m[4];
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-            det_m[mt] = __shfl_sync(0xffffffffu, det, 8 * mt + g);
-            h2_m[mt] = __shfl_sync(0xffffffffu, h2, 8 * mt + g);
-            t_m[mt] = __shfl_sync(0xffffffffu, t, 8 * mt + g);
-            ok_m[mt] = __shfl_sync(0xffffffffu, (int)ok, 8 * mt + g) != 0;
-        }
-        for (int nt0 = 0; nt0 < NT; nt0 += 6) {
-            double acc[4][6][2];
-#pragma unroll
-            for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-                for (int j = 0; j < 6; ++j) acc[mt][j][0] = acc[mt][j][1] = 0.0;
-#pragma unroll
-            for (int ks = 0; ks < KF / 4; ++ks) {
-                double af[4], bf[6];
-#pragma unroll
-                for (int mt = 0; mt < 4; ++mt) af[mt] = Yw[(8 * mt + g) * KFS + 4 * ks + tq];
-#pragma unroll
-                for (int j = 0; j < 6; ++j)
-                    bf[j] = (nt0 + j < NT) ? sT[(8 * (nt0 + j) + g) * KFS + 4 * ks + tq] : 0.0;
-#pragma unroll
-                for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-                    for (int j = 0; j < 6; ++j) mma_f64(acc[mt][j], af[mt], bf[j]);
-            }
-#pragma unroll
-            for (int mt = 0; mt < 4; ++mt) {
-                if (!ok_m[mt]) continue;
-                double* rec = a.records + t_m[mt] * (long long)a.rec_stride;
-#pragma unroll
-                for (int j = 0; j < 6; ++j)
-#pragma unroll
-                    for (int i = 0; i < 2; ++i) {
-                        const int col = 8 * (nt0 + j) + 2 * tq + i;
-                        const double val = det_m[mt] * acc[mt][j][i];
-                        if (col < R) {
-                            rec[col] = val;
-                        } else if (col == R) {
-                            rec[R + 0] = det_m[mt];
-                            rec[R + 1] = val + h2_m[mt];
-                            rec[R + 2] = val;
-                            rec[R + 3] = 0.0;
-                        }
-                    }
-            }
-        }
-        __syncwarp();
-    }
-}
-
 
 // Listed blocks (or all blocks): one thread per block resolves it by the exact path; its first
 // cofactors A go to the lane's shared slot (k^2 doubles).  The warp then treats its 32 blocks one
@@ -852,46 +448,14 @@ __global__ void same_spin_list_kernel(int n, int k, long long batch, const int* 
     }
 }
 
-template <int K>
-cudaError_t launch_fast(const SpinTableArgs& a, size_t smem, double* tables, cudaStream_t stream) {
-    left_string_tables<K><<<a.n_strings, 128, 0, stream>>>(a, tables);
-    cudaError_t err = cudaGetLastError();
-    if (err != cudaSuccess) return err;
-    err = allow_dynamic_smem((const void*)spin_pairs_fast<K>, (int)smem);
-    if (err != cudaSuccess) return err;
-    int per_sm = 1;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_pairs_fast<K>, kSpinBlock, smem);
-    if (err != cudaSuccess) return err;
-    int blocks = kSms * (per_sm > 0 ? per_sm : 1);
-    if (blocks > a.n_items) blocks = a.n_items;
-    if (blocks < 1) blocks = 1;
-    spin_pairs_fast<K><<<blocks, kSpinBlock, smem, stream>>>(a, tables);
-    return cudaGetLastError();
-}
-
 }  // namespace
-
-size_t left_table_doubles(int n, int k, int R) {
-    (void)n;
-    return (size_t)table_stride_of(k, R);
-}
-
-size_t factored_spin_smem_bytes(int n, int k, int R) {
-    const size_t gd = (size_t)n * (n - 1) / 2;
-    const size_t cp = (size_t)k * (k - 1) / 2;
-    return sizeof(double) * (left_table_doubles(n, k, R) + (size_t)kSpinBlock * kfs(k) + (size_t)((k * n + 1) / 2 * 2) +
-                             (k >= 2 ? cp * gd : 0));
-}
-
-bool fast_spin_supported(int n, int k, int R) {
-    return k >= 1 && k <= 8 && n - k >= 0 && n - k <= nb_max(k) && factored_spin_smem_bytes(n, k, R) <= 200 * 1024;
-}
 
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs, double* lf,
                                       int ld, int* meta, cudaStream_t stream) {
-    const size_t in_smem_bytes = sizeof(double) * (size_t)np * np + sizeof(int) * 2 * (size_t)np;
+    const size_t aux_bytes = sizeof(double) * (size_t)np + sizeof(int) * 2 * (size_t)np;
+    const size_t in_smem_bytes = sizeof(double) * (size_t)np * np + aux_bytes;
     const int in_smem = in_smem_bytes <= 200 * 1024 ? 1 : 0;
-    const size_t smem = in_smem ? in_smem_bytes : sizeof(int) * 2 * (size_t)np;
+    const size_t smem = in_smem ? in_smem_bytes : aux_bytes;
     cudaError_t err = allow_dynamic_smem((const void*)factor_pair_kernel, (int)smem);
     if (err != cudaSuccess) return err;
     factor_pair_kernel<<<1, 512, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, kFactorTolerance, in_smem);
@@ -919,14 +483,6 @@ size_t exact_stack_bytes() {
 cudaError_t preload_spin_pair_kernels() {
     // cudaFuncGetAttributes loads a function that lazy module loading has not loaded yet
     const void* fns[] = {(const void*)prepare_tables_kernel, (const void*)factor_pair_kernel,
-                         (const void*)left_string_tables<1>, (const void*)left_string_tables<2>,
-                         (const void*)left_string_tables<3>, (const void*)left_string_tables<4>,
-                         (const void*)left_string_tables<5>, (const void*)left_string_tables<6>,
-                         (const void*)left_string_tables<7>, (const void*)left_string_tables<8>,
-                         (const void*)spin_pairs_fast<1>, (const void*)spin_pairs_fast<2>,
-                         (const void*)spin_pairs_fast<3>, (const void*)spin_pairs_fast<4>,
-                         (const void*)spin_pairs_fast<5>, (const void*)spin_pairs_fast<6>,
-                         (const void*)spin_pairs_fast<7>, (const void*)spin_pairs_fast<8>,
                          (const void*)spin_pairs_exact<7, 7>, (const void*)spin_pairs_exact<8, 0>,
                          (const void*)spin_pairs_exact<dev::KMAX, 0>};
     for (const void* f : fns) {
@@ -955,8 +511,10 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream
         const int tuned = autotune_run(
             key, frame_pair_variants(a.n, a.k, a.R), stream, [&](int v) { return launch_frame_pairs(a, tables, stream, v); },
             [&]() {
+                // the listed-pair counter and both kernels' task counters (compact at +0, dense at +2)
                 cudaError_t e = cudaMemsetAsync(a.careful_count, 0, sizeof(unsigned long long), stream);
                 if (e == cudaSuccess) e = cudaMemsetAsync(a.task_counter, 0, sizeof(unsigned long long), stream);
+                if (e == cudaSuccess) e = cudaMemsetAsync(a.task_counter + 2, 0, sizeof(unsigned long long), stream);
                 return e;
             },
             &err);

@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(kFrameThreads) sort_right_strings(int N, const
     }
 }
 
-constexpr int kTableThreads = 256;
+constexpr int kTableThreads = 128;
 constexpr int kTableSources = 48;  // pair-kernel sources (h and factor columns) staged per pass
 
 __host__ __device__ inline int table_sources(int R) { return R + 1 < kTableSources ? R + 1 : kTableSources; }
@@ -214,7 +214,7 @@ __host__ __device__ inline int table_sources(int R) { return R + 1 < kTableSourc
 //   V_s T_s Sinv = Vt_s Y_s[L, :],
 // so every quantity is a small dense product over staged rows, one thread per output element.
 template <int K>
-__global__ void __launch_bounds__(kTableThreads) frame_tables(SpinTableArgs a, double* __restrict__ tables) {
+__global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a, double* __restrict__ tables) {
     constexpr int NBM = fr_nbmax(K);
     constexpr int CP = fr_cp(K);
     constexpr int BP = fr_bp(K);
@@ -366,7 +366,12 @@ __global__ void __launch_bounds__(kTableThreads) frame_tables(SpinTableArgs a, d
             sTr[2 * sl] = tr;
             sTr[2 * sl + 1] = tr2;
             const int s = s0 + sl;
-            blk[(long long)(s == 0 ? 0 : s + 1) * KFS + 8 * K] = tr;
+            double* row = blk + (long long)(s == 0 ? 0 : s + 1) * KFS;
+            row[8 * K] = tr;
+            // with at most 7 complement orbitals, column 7 of every hole block is free: the trace
+            // there lets a pair with holes pick it up in its first hole block (no trace k-step)
+            if (nb <= 7)
+                for (int c = 0; c < K; ++c) row[c * 8 + 7] = tr;
         }
         __syncthreads();
         // two-electron constant, linear and quadratic tables over the factor sources
@@ -421,6 +426,8 @@ __global__ void __launch_bounds__(kTableThreads) frame_tables(SpinTableArgs a, d
             if (b < nb) blk[1 * KFS + c * 8 + b] = acc[q];
         } else {
             blk[1 * KFS + 8 * K] = 0.5 * acc[q];
+            if (nb <= 7)
+                for (int c = 0; c < K; ++c) blk[1 * KFS + c * 8 + 7] = 0.5 * acc[q];
         }
     }
 }
@@ -432,10 +439,15 @@ size_t frame_tables_smem(int n, int R) {
 
 // Phase A of one pair at excitation level E (compile time).  Writes the pair's Y' row and
 // returns the certificate, det X, the quadratic two-electron term / det X and the hole mask.
-template <int K, int E>
+// COMPACT: W is stored in canonical order (hole slot j, particle slot i) at yrow[j E + i] and the
+// slot maps are returned (*hmap: nibble c = hole slot of position c, *pmap: nibble b = particle
+// slot of complement index b, 0xF elsewhere); otherwise W is scattered on the pair's dense row
+// (zeroed beforehand) with 1 in the trace slot.
+template <int K, int E, bool COMPACT>
 __device__ __forceinline__ void frame_pair(const double* __restrict__ blk, const FrameLayout& F, unsigned desc,
                                            double* __restrict__ yrow, bool* ok_out, double* det_out,
-                                           double* quad_out, unsigned* hm_out) {
+                                           double* quad_out, unsigned* hm_out, unsigned* hmap_out,
+                                           unsigned* pmap_out) {
     constexpr int CP = fr_cp(K);
     const unsigned hm = desc & 0xFFu;
     // holes (positions in L, ascending) and particles (Lbar indices, ascending)
@@ -549,43 +561,76 @@ __device__ __forceinline__ void frame_pair(const double* __restrict__ blk, const
                 quad += part;
             }
     }
-    // the pair's row (zeroed by the warp beforehand): W on the (hole position, particle) grid,
-    // 1 in the trace slot
-    if (ok) {
+    unsigned hmap = 0xFFFFFFFFu, pmap = 0xFFFFFFFFu;
+    if (COMPACT) {
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                hmap &= ~(0xFu << (4 * hc[j]));
+                hmap |= (unsigned)j << (4 * hc[j]);
+                pmap &= ~(0xFu << (4 * pb[j]));
+                pmap |= (unsigned)j << (4 * pb[j]);
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) yrow[j * E + lab[jj]] = x[j][jj];
+            }
+        }
+    } else if (ok) {
+        // the pair's row (zeroed by the warp beforehand): W on the (hole position, particle)
+        // grid, 1 in the trace slot
 #pragma unroll
         for (int j = 0; j < E; ++j)
 #pragma unroll
             for (int jj = 0; jj < E; ++jj) yrow[hc[j] * 8 + bj[jj]] = x[j][jj];
         yrow[8 * K] = 1.0;
     }
+    *hmap_out = hmap;
+    *pmap_out = pmap;
     *ok_out = ok;
     *det_out = det;
     *quad_out = quad;
     *hm_out = hm;
 }
 
-template <int K>
+template <int K, int ELO, int EHI, bool COMPACT>
 __device__ __forceinline__ void frame_pair_dispatch(int e, const double* blk, const FrameLayout& F, unsigned desc,
-                                                    double* yrow, bool* ok, double* det, double* quad, unsigned* hm) {
+                                                    double* yrow, bool* ok, double* det, double* quad, unsigned* hm,
+                                                    unsigned* hmap, unsigned* pmap) {
+#define VB_FRAME_CASE(E_)                                                                             \
+    case E_:                                                                                          \
+        if constexpr (E_ >= ELO && E_ <= EHI && E_ <= K)                                              \
+            frame_pair<K, E_, COMPACT>(blk, F, desc, yrow, ok, det, quad, hm, hmap, pmap);             \
+        break;
     switch (e) {
-        case 0: frame_pair<K, 0>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 1: if constexpr (K >= 1) frame_pair<K, 1>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 2: if constexpr (K >= 2) frame_pair<K, 2>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 3: if constexpr (K >= 3) frame_pair<K, 3>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 4: if constexpr (K >= 4) frame_pair<K, 4>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 5: if constexpr (K >= 5) frame_pair<K, 5>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 6: if constexpr (K >= 6) frame_pair<K, 6>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 7: if constexpr (K >= 7) frame_pair<K, 7>(blk, F, desc, yrow, ok, det, quad, hm); break;
-        case 8: if constexpr (K >= 8) frame_pair<K, 8>(blk, F, desc, yrow, ok, det, quad, hm); break;
+        VB_FRAME_CASE(0)
+        VB_FRAME_CASE(1)
+        VB_FRAME_CASE(2)
+        VB_FRAME_CASE(3)
+        VB_FRAME_CASE(4)
+        VB_FRAME_CASE(5)
+        VB_FRAME_CASE(6)
+        VB_FRAME_CASE(7)
+        VB_FRAME_CASE(8)
         default: break;
     }
+#undef VB_FRAME_CASE
 }
 
-template <int K>
-__global__ void __launch_bounds__(32 * kFrameMaxWarps) spin_pairs_frame(SpinTableArgs a,
-                                                                       const double* __restrict__ tables) {
+// Compact slots: W of an E <= 5 pair (25 doubles; stride 26 spreads a tile's pairs over banks).
+constexpr int kCompactEMax = 5;
+constexpr int kCompactSlot = 26;
+
+__host__ __device__ constexpr int frame_row_doubles(int K, bool compact) { return compact ? kCompactSlot : fr_kfs(K); }
+
+// The pairs of excitation levels ELO .. EHI of every left string.  COMPACT (EHI <= 4): each pair's
+// W is kept as an E x E slot and the tensor-core A fragments are read through the pair's slot
+// maps (a few registers and 4.3 KB of shared memory per warp); otherwise each pair has a dense row
+// on the (hole position x particle) grid.  Task counter: a.task_counter (+2 for the dense kernel).
+template <int K, int ELO, int EHI, bool COMPACT>
+__global__ void __launch_bounds__(32 * kFrameMaxWarps, COMPACT ? 2 : 1)
+    spin_pairs_frame(SpinTableArgs a, const double* __restrict__ tables) {
     extern __shared__ double smem[];
     constexpr int KFS = fr_kfs(K);
+    constexpr int ROW = frame_row_doubles(K, COMPACT);
     const int R = a.R;
     const FrameLayout F = frame_layout(a.n, K, R);
     const int NT = F.rows / 8;
@@ -595,38 +640,44 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps) spin_pairs_frame(SpinTabl
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, tq = lane & 3;
     const long long N = a.n_strings;
-    double* yw = sY + (size_t)warp * 32 * KFS;
+    double* yw = sY + (size_t)warp * 32 * ROW;
+    unsigned long long* task_counter = a.task_counter + (COMPACT ? 0 : 2);
     for (;;) {
         if (threadIdx.x == 0) {
-            s_task = (int)atomicAdd(a.task_counter, 1ull);
+            s_task = (int)atomicAdd(task_counter, 1ull);
             s_chunk = 0;
         }
         __syncthreads();
         const int u = s_task;
         if (u >= N) break;
-        {
-            const double2* src = reinterpret_cast<const double2*>(tables + (long long)u * F.total);
-            double2* dst = reinterpret_cast<double2*>(sBlk);
-            for (int i = threadIdx.x; i < F.total / 2; i += blockDim.x) dst[i] = __ldg(src + i);
-        }
         const int* eb = a.ebound + (long long)u * (K + 2);
         int bound[K + 2];
 #pragma unroll
         for (int e = 0; e < K + 2; ++e) bound[e] = __ldg(eb + e);
         int nchunks = 0;
 #pragma unroll
-        for (int e = 0; e <= K; ++e) nchunks += (bound[e + 1] - bound[e] + 31) >> 5;
+        for (int e = ELO; e <= EHI && e <= K; ++e) nchunks += (bound[e + 1] - bound[e] + 31) >> 5;
+        if (nchunks == 0) {
+            __syncthreads();
+            continue;
+        }
+        {
+            const double2* src = reinterpret_cast<const double2*>(tables + (long long)u * F.total);
+            double2* dst = reinterpret_cast<double2*>(sBlk);
+            for (int i = threadIdx.x; i < F.total / 2; i += blockDim.x) dst[i] = __ldg(src + i);
+        }
         const long long base = record_index(u, u, N);
         __syncthreads();
-        // warps take 32-pair chunks dynamically, highest excitation level (the costliest) first
-        for (;;) {
+        // warps take 32-pair chunks dynamically, highest excitation level (the costliest) first;
+        // the next chunk is claimed and its right strings and descriptors are loaded while the
+        // current one is evaluated
+        auto claim = [&](int* e_out, int* cnt_out, int* v_out, unsigned* d_out) {
             int ch = 0;
             if (lane == 0) ch = atomicAdd(&s_chunk, 1);
             ch = __shfl_sync(0xffffffffu, ch, 0);
-            if (ch >= nchunks) break;
-            int e = 0, start = 0, cnt = 0, left = ch;
+            int e = -1, start = 0, cnt = 0, left = ch;
 #pragma unroll
-            for (int ee = K; ee >= 0; --ee) {
+            for (int ee = (EHI < K ? EHI : K); ee >= ELO; --ee) {
                 const int c = (bound[ee + 1] - bound[ee] + 31) >> 5;
                 if (left >= 0 && left < c) {
                     e = ee;
@@ -635,21 +686,35 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps) spin_pairs_frame(SpinTabl
                 }
                 left -= c;
             }
-            // zero the warp's 32 rows, consecutive lanes on consecutive 16-byte words
-            {
+            const bool valid = e >= 0 && lane < cnt;
+            *v_out = valid ? __ldg(a.rlist + base + start + lane) : u;
+            *d_out = valid ? __ldg(a.rdesc + base + start + lane) : 0u;
+            *e_out = e;
+            *cnt_out = cnt;
+        };
+        int e_next, cnt_next, v_next;
+        unsigned d_next;
+        claim(&e_next, &cnt_next, &v_next, &d_next);
+        for (;;) {
+            const int e = e_next, cnt = cnt_next, v = v_next;
+            const unsigned desc = d_next;
+            if (e < 0) break;
+            claim(&e_next, &cnt_next, &v_next, &d_next);
+            const bool valid = lane < cnt;
+            if (!COMPACT) {
+                // zero the warp's 32 rows, consecutive lanes on consecutive 16-byte words
                 double2* z = reinterpret_cast<double2*>(yw);
 #pragma unroll
                 for (int f = lane; f < 16 * KFS; f += 32) z[f] = make_double2(0.0, 0.0);
+                __syncwarp();
             }
-            __syncwarp();
-            const bool valid = lane < cnt;
-            const int v = valid ? __ldg(a.rlist + base + start + lane) : u;
-            double* yrow = yw + lane * KFS;
+            double* yrow = yw + lane * ROW;
             bool ok = false;
             double det = 0.0, quad = 0.0;
-            unsigned hm = 0;
+            unsigned hm = 0, hmap = 0xFFFFFFFFu, pmap = 0xFFFFFFFFu;
             if (valid) {
-                frame_pair_dispatch<K>(e, sBlk, F, __ldg(a.rdesc + base + start + lane), yrow, &ok, &det, &quad, &hm);
+                frame_pair_dispatch<K, ELO, EHI, COMPACT>(e, sBlk, F, desc, yrow, &ok, &det, &quad, &hm, &hmap,
+                                                          &pmap);
                 if (!ok) {
                     const unsigned long long slot = atomicAdd(a.careful_count, 1ull);
                     a.careful_list[slot] = ((unsigned long long)u << 32) | (unsigned long long)v;
@@ -667,16 +732,23 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps) spin_pairs_frame(SpinTabl
                 const double det_g = __shfl_sync(0xffffffffu, det, owner);
                 const double quad_g = __shfl_sync(0xffffffffu, quad, owner);
                 const long long t_g = __shfl_sync(0xffffffffu, t, owner);
+                const unsigned hmap_g = __shfl_sync(0xffffffffu, hmap, owner);
+                const unsigned pmap_g = __shfl_sync(0xffffffffu, pmap, owner);
                 const bool ok_g = (okbits >> owner) & 1u;
-                const double* yr = yw + owner * KFS;
+                const double* yr = yw + owner * ROW;
                 double* rec = a.records + t_g * (long long)a.rec_stride;
+                // this lane's particle slots for the two k-steps of a hole block (b = tq, tq + 4)
+                const unsigned i0 = (pmap_g >> (4 * tq)) & 0xFu, i1 = (pmap_g >> (4 * (tq + 4))) & 0xFu;
+                // the trace from column 7 of each pair's first hole block (compact, level >= 1,
+                // at most 7 complement orbitals) instead of a separate k-step
+                const bool pad_trace = COMPACT && e >= 1 && a.n - K <= 7;
 #pragma unroll 1
                 for (int nt0 = 0; nt0 < NT; nt0 += 6) {
                     double acc[6][2];
 #pragma unroll
                     for (int j = 0; j < 6; ++j) acc[j][0] = acc[j][1] = 0.0;
-                    {
-                        const double af = yr[8 * K + tq];
+                    if (!pad_trace) {
+                        const double af = COMPACT ? ((tq == 0 && ok_g) ? 1.0 : 0.0) : yr[8 * K + tq];
 #pragma unroll
                         for (int j = 0; j < 6; ++j) {
                             const double bf = (nt0 + j < NT) ? sBlk[(8 * (nt0 + j) + g) * KFS + 8 * K + tq] : 0.0;
@@ -687,10 +759,18 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps) spin_pairs_frame(SpinTabl
                     while (rest) {
                         const int c = __ffs(rest) - 1;
                         rest &= rest - 1;
+                        const unsigned jh = (hmap_g >> (4 * c)) & 0xFu;
 #pragma unroll
                         for (int ks = 0; ks < 2; ++ks) {
                             const int col = 8 * c + 4 * ks + tq;
-                            const double af = yr[col];
+                            double af;
+                            if (COMPACT) {
+                                const unsigned ip = ks ? i1 : i0;
+                                af = (jh < (unsigned)e && ip < (unsigned)e) ? yr[jh * e + ip] : 0.0;
+                                if (pad_trace && ks == 1 && tq == 3) af = jh == 0 ? 1.0 : 0.0;
+                            } else {
+                                af = yr[col];
+                            }
 #pragma unroll
                             for (int j = 0; j < 6; ++j) {
                                 const double bf = (nt0 + j < NT) ? sBlk[(8 * (nt0 + j) + g) * KFS + col] : 0.0;
@@ -723,20 +803,28 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps) spin_pairs_frame(SpinTabl
 }
 
 template <int K>
-size_t frame_spin_smem(int n, int R, int warps = 4) {
-    return sizeof(double) * ((size_t)frame_layout(n, K, R).total + (size_t)warps * 32 * fr_kfs(K));
+size_t frame_spin_smem(int n, int R, int warps = 4, bool compact = false) {
+    return sizeof(double) * ((size_t)frame_layout(n, K, R).total + (size_t)warps * 32 * frame_row_doubles(K, compact));
+}
+
+// The larger of the two kernels' shared memory (8-warp compact, 4-warp dense).
+template <int K>
+size_t frame_spin_smem_max(int n, int R) {
+    const size_t c = frame_spin_smem<K>(n, R, 8, true);
+    const size_t d = K > kCompactEMax ? frame_spin_smem<K>(n, R, 1, false) : 0;
+    return c > d ? c : d;
 }
 
 size_t frame_spin_smem_rt(int n, int k, int R) {
     switch (k) {
-        case 1: return frame_spin_smem<1>(n, R);
-        case 2: return frame_spin_smem<2>(n, R);
-        case 3: return frame_spin_smem<3>(n, R);
-        case 4: return frame_spin_smem<4>(n, R);
-        case 5: return frame_spin_smem<5>(n, R);
-        case 6: return frame_spin_smem<6>(n, R);
-        case 7: return frame_spin_smem<7>(n, R);
-        case 8: return frame_spin_smem<8>(n, R);
+        case 1: return frame_spin_smem_max<1>(n, R);
+        case 2: return frame_spin_smem_max<2>(n, R);
+        case 3: return frame_spin_smem_max<3>(n, R);
+        case 4: return frame_spin_smem_max<4>(n, R);
+        case 5: return frame_spin_smem_max<5>(n, R);
+        case 6: return frame_spin_smem_max<6>(n, R);
+        case 7: return frame_spin_smem_max<7>(n, R);
+        case 8: return frame_spin_smem_max<8>(n, R);
         default: return ~size_t{0};
     }
 }
@@ -750,26 +838,38 @@ cudaError_t launch_tables(const SpinTableArgs& a, double* tables, cudaStream_t s
     return cudaGetLastError();
 }
 
-// Launch variants (the autotuner's choices): 0 = 4 warps per CTA, 1 = 2 warps, 2 = 8 warps; every
-// variant fills each SM with as many resident CTAs as fit.
+// Launch variants of the compact kernel (the autotuner's choices): 0 = 8 warps per CTA, 1 = 4,
+// 2 = 2; every variant fills each SM with as many resident CTAs as fit.  The dense kernel for
+// excitation levels 6 .. K (k >= 6 only) follows with one warp per CTA.
 constexpr int kFrameVariants = 3;
-constexpr int kFrameVariantWarps[kFrameVariants] = {4, 2, 8};
+constexpr int kFrameVariantWarps[kFrameVariants] = {8, 4, 2};
 
-template <int K>
-cudaError_t launch_frame(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int variant) {
-    const int warps = kFrameVariantWarps[variant];
-    const size_t smem = frame_spin_smem<K>(a.n, a.R, warps);
-    cudaError_t err = allow_dynamic_smem((const void*)spin_pairs_frame<K>, smem);
+template <int K, int ELO, int EHI, bool COMPACT>
+cudaError_t launch_frame_part(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int warps) {
+    const size_t smem = frame_spin_smem<K>(a.n, a.R, warps, COMPACT);
+    auto kernel = spin_pairs_frame<K, ELO, EHI, COMPACT>;
+    cudaError_t err = allow_dynamic_smem((const void*)kernel, smem);
     if (err != cudaSuccess) return err;
     int per_sm = 1, dev = 0, sms = 148;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_pairs_frame<K>, 32 * warps, smem);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * warps, smem);
     if (err != cudaSuccess) return err;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     long long blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (blocks > a.n_strings) blocks = a.n_strings;
     if (blocks < 1) blocks = 1;
-    spin_pairs_frame<K><<<(unsigned)blocks, 32 * warps, smem, stream>>>(a, tables);
+    kernel<<<(unsigned)blocks, 32 * warps, smem, stream>>>(a, tables);
     return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_frame(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int variant) {
+    constexpr int EL = K < kCompactEMax ? K : kCompactEMax;
+    cudaError_t err = launch_frame_part<K, 0, EL, true>(a, tables, stream, kFrameVariantWarps[variant]);
+    if (err != cudaSuccess) return err;
+    // the high levels have about one chunk per left string: one warp per CTA, so no warp of a CTA
+    // waits at the task barrier for another's chunk
+    if constexpr (K > kCompactEMax) err = launch_frame_part<K, kCompactEMax + 1, K, false>(a, tables, stream, 1);
+    return err;
 }
 
 template <int K>
@@ -818,9 +918,10 @@ cudaError_t launch_frame_tables(const SpinTableArgs& a, double* tables, cudaStre
 }
 
 int frame_pair_variants(int n, int k, int R) {
-    // the 8-warp variant only where its rows fit next to the table
-    const bool eight = frame_spin_smem_rt(n, k, R) + sizeof(double) * 4 * 32 * fr_kfs(k) <= 200 * 1024;
-    return eight ? kFrameVariants : kFrameVariants - 1;
+    (void)n;
+    (void)k;
+    (void)R;
+    return kFrameVariants;
 }
 
 cudaError_t launch_frame_pairs(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int variant) {
@@ -838,22 +939,29 @@ cudaError_t launch_frame_pairs(const SpinTableArgs& a, const double* tables, cud
     }
 }
 
+template <int K>
+cudaError_t preload_k() {
+    constexpr int EL = K < kCompactEMax ? K : kCompactEMax;
+    cudaFuncAttributes fa{};
+    cudaError_t err = cudaFuncGetAttributes(&fa, (const void*)sort_right_strings<K>);
+    if (err == cudaSuccess) err = cudaFuncGetAttributes(&fa, (const void*)frame_tables<K>);
+    if (err == cudaSuccess) err = cudaFuncGetAttributes(&fa, (const void*)spin_pairs_frame<K, 0, EL, true>);
+    if constexpr (K > kCompactEMax)
+        if (err == cudaSuccess)
+            err = cudaFuncGetAttributes(&fa, (const void*)spin_pairs_frame<K, kCompactEMax + 1, K, false>);
+    return err;
+}
+
 cudaError_t preload_frame_kernels() {
-    const void* fns[] = {
-        (const void*)sort_right_strings<1>, (const void*)sort_right_strings<2>, (const void*)sort_right_strings<3>,
-        (const void*)sort_right_strings<4>, (const void*)sort_right_strings<5>, (const void*)sort_right_strings<6>,
-        (const void*)sort_right_strings<7>, (const void*)sort_right_strings<8>, (const void*)frame_tables<1>,
-        (const void*)frame_tables<2>,       (const void*)frame_tables<3>,       (const void*)frame_tables<4>,
-        (const void*)frame_tables<5>,       (const void*)frame_tables<6>,       (const void*)frame_tables<7>,
-        (const void*)frame_tables<8>,       (const void*)spin_pairs_frame<1>,   (const void*)spin_pairs_frame<2>,
-        (const void*)spin_pairs_frame<3>,   (const void*)spin_pairs_frame<4>,   (const void*)spin_pairs_frame<5>,
-        (const void*)spin_pairs_frame<6>,   (const void*)spin_pairs_frame<7>,   (const void*)spin_pairs_frame<8>};
-    for (const void* f : fns) {
-        cudaFuncAttributes fa{};
-        const cudaError_t err = cudaFuncGetAttributes(&fa, f);
-        if (err != cudaSuccess) return err;
-    }
-    return cudaSuccess;
+    cudaError_t err = preload_k<1>();
+    if (err == cudaSuccess) err = preload_k<2>();
+    if (err == cudaSuccess) err = preload_k<3>();
+    if (err == cudaSuccess) err = preload_k<4>();
+    if (err == cudaSuccess) err = preload_k<5>();
+    if (err == cudaSuccess) err = preload_k<6>();
+    if (err == cudaSuccess) err = preload_k<7>();
+    if (err == cudaSuccess) err = preload_k<8>();
+    return err;
 }
 
 }  // namespace vbcore
