@@ -405,6 +405,21 @@ vb_status vb_active_transform_ri_precision(vb_context* ctx, const double* B_pack
 vb_status vb_active_transform_ri_adjoint(vb_context* ctx, const double* one_index, const double* dL, int n_aux,
                                          int n_bf, int n_act, int mem_space, double* dC);
 
+/* RI pair factors in a new orbital frame, replacing transform_ri_pair_factors (mode 0),
+ * transform_ri_pair_factor_direction (mode 1) and transform_ri_pair_factor_direction_from_orthogonal
+ * (mode 2) of src/integrals/active/ri_transform.cpp:178-211 (declared in ri_transform.hpp:24-60).
+ * factors / factor_direction: [n_aux x n(n+1)/2] column-major, row P packing the symmetric n x n
+ * factor B_P at (i, j), i >= j, i (i+1)/2 + j; frame Q and frame_direction: n x n column-major.
+ *   mode 0: out = Q^T B Q                                  (factor_direction, frame_direction unused)
+ *   mode 1: out = Q^T dB Q + dQ^T B Q + Q^T B dQ           (factors = B, factor_direction = dB,
+ *                                                           frame_direction = dQ)
+ *   mode 2: out = Q^T dB Q - K^T Bbar - Bbar K             (factors = Bbar = Q^T B Q,
+ *                                                           factor_direction = dB, frame_direction = K)
+ * Same packed layout out.  n <= 64. */
+vb_status vb_ri_pair_factors_frame(vb_context* ctx, int mode, const double* factors, const double* factor_direction,
+                                   int n_aux, int n, const double* frame, const double* frame_direction,
+                                   int mem_space, double* out);
+
 /* ---- launch-schedule autotuner ---------------------------------------------------------------- */
 
 /* No counterpart in the reference.  The first evaluation of a shape (electrons per string, active

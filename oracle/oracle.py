@@ -225,6 +225,36 @@ def ri_transform(B_packed: np.ndarray, C: np.ndarray, threads: int = 0):
     return L.T.copy(), K
 
 
+def ri_pair_factors_frame(factors, frame, mode=0, factor_direction=None, frame_direction=None):
+    """RI pair factors in a new orbital frame, restating transform_ri_pair_factors and its
+    directional forms (src/integrals/active/ri_transform.cpp:98-211): rows of `factors`
+    [n_aux, n(n+1)/2] pack symmetric n x n factors at i(i+1)/2 + j (i >= j).  mode 0: Q^T B Q;
+    mode 1: Q^T dB Q + dQ^T B Q + Q^T B dQ; mode 2 (factors already in the frame, dQ = -Q K):
+    Q^T dB Q - K^T Bbar - Bbar K."""
+    F = np.asarray(factors, dtype=np.float64)
+    n_aux, npair = F.shape
+    n = int(round((np.sqrt(8 * npair + 1) - 1) / 2))
+    hi, lo = np.tril_indices(n)
+    pk = np.zeros((n, n), dtype=np.int64)
+    pk[hi, lo] = np.arange(npair)
+    pk[lo, hi] = np.arange(npair)
+
+    def expand(M):
+        return np.asarray(M)[:, pk]  # [n_aux, n, n]
+
+    Q = np.asarray(frame, dtype=np.float64)
+    if mode == 0:
+        X = np.einsum("ki,pkl,lj->pij", Q, expand(F), Q)
+    elif mode == 1:
+        B, dB, dQ = expand(F), expand(factor_direction), np.asarray(frame_direction)
+        X = (np.einsum("ki,pkl,lj->pij", Q, dB, Q) + np.einsum("ki,pkl,lj->pij", dQ, B, Q)
+             + np.einsum("ki,pkl,lj->pij", Q, B, dQ))
+    else:
+        Bb, dB, K = expand(F), expand(factor_direction), np.asarray(frame_direction)
+        X = np.einsum("ki,pkl,lj->pij", Q, dB, Q) - np.einsum("ki,pkj->pij", K, Bb) - np.einsum("pik,kj->pij", Bb, K)
+    return X[:, hi, lo]
+
+
 def ri_one_index(B_packed: np.ndarray, C: np.ndarray) -> np.ndarray:
     """One-index RI factors T [(n_act n_aux), n_bf], row a*n_aux + P:
     T[(a, P), mu] = sum_nu B_P(mu, nu) C(nu, a) (transform_ri_one_index,

@@ -164,3 +164,23 @@ def test_cached_algorithm_equals_direct_oracle(n, keyword, mult, overlap):
     # a row-limited call evaluates only those determinant rows: the timing sample
     _, _, part = O.cached_structure_matrices(n, ex, S, h, eri, threads=4, det_rows=2)
     assert part["pairs"] == 2 * ex.n_determinants
+
+
+def test_ri_pair_factor_frame_restatement():
+    """The oracle's frame transform of packed RI pair factors: identity frame, an explicit
+    single-row check, and the orthogonal directional form equal to the raw one at dQ = -Q K."""
+    rng = np.random.default_rng(3)
+    n, n_aux = 5, 7
+    B = rng.standard_normal((n_aux, n * (n + 1) // 2))
+    dB = rng.standard_normal(B.shape)
+    Q = np.eye(n) + 0.3 * rng.standard_normal((n, n))
+    K = rng.standard_normal((n, n))
+    assert np.allclose(O.ri_pair_factors_frame(B, np.eye(n)), B, atol=0, rtol=0)
+    hi, lo = np.tril_indices(n)
+    M = np.zeros((n, n))
+    M[hi, lo] = B[2]
+    M[lo, hi] = B[2]
+    assert np.allclose(O.ri_pair_factors_frame(B, Q)[2], (Q.T @ M @ Q)[hi, lo], rtol=1e-14, atol=1e-14)
+    a = O.ri_pair_factors_frame(O.ri_pair_factors_frame(B, Q), Q, 2, dB, K)
+    b = O.ri_pair_factors_frame(B, Q, 1, dB, -Q @ K)
+    assert np.abs(a - b).max() < 1e-12

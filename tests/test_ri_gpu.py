@@ -116,3 +116,38 @@ def test_rejects_too_many_active_orbitals(ctx):
     with pytest.raises(vbcore.VbError) as e:
         vbcore.active_transform_ri(ctx, B, C)
     assert e.value.status == 5
+
+
+@pytest.mark.parametrize("n,n_aux", [(1, 3), (6, 40), (14, 42), (16, 257)])
+def test_pair_factors_in_a_new_frame(ctx, n, n_aux):
+    """transform_ri_pair_factors and its two directional forms (ri_transform.cpp:98-211) against
+    the oracle, a non-orthogonal frame; the raw direction against a central difference of the
+    forward transform, and the orthogonal form against the raw one with dQ = -Q K."""
+    rng = np.random.default_rng(n * 1000 + n_aux)
+    npair = n * (n + 1) // 2
+    B = rng.standard_normal((n_aux, npair))
+    dB = rng.standard_normal((n_aux, npair))
+    Q = np.eye(n) + 0.3 * rng.standard_normal((n, n))
+    dQ = rng.standard_normal((n, n))
+    K = rng.standard_normal((n, n))
+    fwd = vbcore.ri_pair_factors_frame(ctx, B, Q)
+    ref = O.ri_pair_factors_frame(B, Q)
+    scale = max(1.0, np.abs(ref).max())
+    assert np.abs(fwd - ref).max() <= 1e-13 * scale
+    raw = vbcore.ri_pair_factors_frame(ctx, B, Q, mode=1, factor_direction=dB, frame_direction=dQ)
+    assert np.abs(raw - O.ri_pair_factors_frame(B, Q, 1, dB, dQ)).max() <= 1e-13 * max(1.0, np.abs(raw).max())
+    # the transform is cubic along the line (B + t dB, Q + t dQ): Richardson's combination of two
+    # central differences is exact for a cubic up to rounding
+    def central(h):
+        return (O.ri_pair_factors_frame(B + h * dB, Q + h * dQ) - O.ri_pair_factors_frame(B - h * dB, Q - h * dQ)) / (2 * h)
+
+    fd = (4.0 * central(5e-4) - central(1e-3)) / 3.0
+    assert np.abs(raw - fd).max() <= 1e-9 * max(1.0, np.abs(fd).max())
+    orth = vbcore.ri_pair_factors_frame(ctx, fwd, Q, mode=2, factor_direction=dB, frame_direction=K)
+    via_raw = vbcore.ri_pair_factors_frame(ctx, B, Q, mode=1, factor_direction=dB, frame_direction=-Q @ K)
+    assert np.abs(orth - via_raw).max() <= 1e-12 * max(1.0, np.abs(via_raw).max())
+
+
+def test_pair_factors_frame_rejects_bad_input(ctx):
+    with pytest.raises(vbcore.VbError):
+        vbcore.ri_pair_factors_frame(ctx, np.zeros((2, 3)), np.eye(2), mode=1)

@@ -103,7 +103,7 @@ EXPORTED_SYMBOLS = (
     "vb_engine_evaluate_instances", "vb_engine_submit_scf", "vb_engine_poll", "vb_engine_pending",
     "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_create_from_integrals", "vb_scf_problem_destroy",
     "vb_scf_problem_sizes", "vb_scf_ao_integrals", "vb_scf_energy_gradient", "vb_solve_scf",
-    "vb_autotune_report", "vb_autotune_clear",
+    "vb_autotune_report", "vb_autotune_clear", "vb_ri_pair_factors_frame",
 )
 
 PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
@@ -127,6 +127,7 @@ def load_library(path: str = LIB_PATH):
     lib.vb_context_synchronize.argtypes = [P]
     lib.vb_context_set_barrier_spin_limit.argtypes = [P, c.c_longlong]
     lib.vb_autotune_report.argtypes = [c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
+    lib.vb_ri_pair_factors_frame.argtypes = [P, c.c_int, P, P, c.c_int, c.c_int, P, P, c.c_int, P]
     lib.vb_autotune_clear.argtypes = []
     lib.vb_last_error.argtypes = [P]
     lib.vb_last_error.restype = c.c_char_p
@@ -515,6 +516,24 @@ def _scf_integral_input(ints, pattern, n_electrons, multiplicity, structures, ke
                              vals.size, _ptr(rows).value, _ptr(cols).value, _ptr(vals).value,
                              float(ints["nuclear_repulsion"]), len(pattern), _ptr(offsets).value,
                              _ptr(funcs).value if funcs.size else None, n_electrons, multiplicity, kw)
+
+
+def ri_pair_factors_frame(ctx: "Context", factors, frame, mode: int = 0, factor_direction=None,
+                          frame_direction=None):
+    """RI pair factors [n_aux, n(n+1)/2] in the frame Q (mode 0: Q^T B Q; mode 1: the raw
+    directional derivative; mode 2: the direction from factors already in the frame); host arrays."""
+    F = np.asarray(factors, dtype=np.float64)
+    n_aux, npair = F.shape
+    n = int(round((np.sqrt(8 * npair + 1) - 1) / 2))
+    Ff = _c(F.T, np.float64)  # column-major [n_aux x np]
+    Qf = _c(np.asarray(frame).T, np.float64)
+    Gf = _c(np.asarray(factor_direction).T, np.float64) if factor_direction is not None else None
+    Df = _c(np.asarray(frame_direction).T, np.float64) if frame_direction is not None else None
+    out = np.empty(n_aux * npair)
+    _check(load_library().vb_ri_pair_factors_frame(ctx.handle, mode, _ptr(Ff), _ptr(Gf) if Gf is not None else None,
+                                                   n_aux, n, _ptr(Qf), _ptr(Df) if Df is not None else None,
+                                                   VB_MEM_HOST, _ptr(out)), ctx.handle)
+    return out.reshape(npair, n_aux).T.copy()
 
 
 def autotune_report() -> str:
