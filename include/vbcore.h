@@ -149,11 +149,12 @@ vb_status vb_hs_plan_stats(const vb_hs_plan* plan, vb_hs_stats* stats);
 /* Phase timing with CUDA events on the context stream (the device counterpart of the
  * reference's XMVB_PHASE_TIMING scoped phases, src/core/timing.hpp:411).  When enabled, every
  * execute records events around its phases; vb_hs_plan_phase_times synchronizes and returns
- * the milliseconds of the last execute per phase: [0] integral tables, [1] spin-pair records
- * (fast + exact kernels), [2] determinant pairs (all bands), [3] band reduction,
- * [4] structure reduction + symmetrization.  Phases [2] and [3] sum over bands. */
+ * the milliseconds of the last execute per phase: [0] integral tables (pair-kernel factorization
+ * and the per-left-string frame tables), [1] spin-pair records of the register path (frame
+ * kernel), [2] determinant pairs (all bands), [3] band reduction, [4] structure reduction +
+ * symmetrization, [5] spin-pair records of the exact path (listed blocks).  Phases [2] and [3] sum over bands. */
 enum { VB_PHASE_TABLES = 0, VB_PHASE_SPIN_PAIRS = 1, VB_PHASE_DETERMINANT_PAIRS = 2, VB_PHASE_BAND_REDUCE = 3,
-       VB_PHASE_STRUCTURE_REDUCE = 4, VB_PHASE_COUNT = 5 };
+       VB_PHASE_STRUCTURE_REDUCE = 4, VB_PHASE_EXACT_PAIRS = 5, VB_PHASE_COUNT = 6 };
 vb_status vb_hs_plan_enable_phase_timing(vb_hs_plan* plan, int enable);
 vb_status vb_hs_plan_phase_times(vb_hs_plan* plan, double* milliseconds, int count);
 

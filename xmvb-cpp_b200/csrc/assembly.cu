@@ -19,16 +19,13 @@ namespace {
 
 constexpr int kPad = kBandReduceColumns + 1;
 
-constexpr int kTileRows = 64;  // band rows staged in shared memory per step
-
-// One CTA per (32 band columns, structure chunk of at most 64 structures).  The CTA walks the
-// band's rows in tiles of 64: the tile of H and S (64 rows x 32 columns, upper-triangle mask
-// applied) is staged in shared memory once, then every warp consumes the (determinant,
-// structure, coefficient) triples of its structures whose determinant falls in the tile (they
-// are sorted by determinant), so each band element is read from memory once per CTA however
-// many structures its determinant belongs to.  Warp w owns the chunk's structures bucketed to it
-// (local structure index = w mod warps): each shared-memory accumulator has exactly one writer
-// and the sum order is fixed.
+// One CTA per (32 band columns, structure chunk of at most 64 structures): every chunk's
+// triples stream the band rows they need, and the small per-chunk accumulators let several
+// CTAs share an SM.  Warp w owns the chunk's structures bucketed to it (local structure index
+// = w mod warps), so each shared-memory accumulator has exactly one writer and the sum order is
+// fixed.  A warp walks its (determinant, structure, coefficient) triples, sorted by
+// determinant, 32 at a time: lane j fetches triple j, then the warp broadcasts them one by one;
+// the band loads of consecutive triples are independent, which keeps many loads in flight.
 __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(BandReduceArgs a) {
     extern __shared__ double zsm[];
     const int chunk = blockIdx.y;
@@ -36,59 +33,60 @@ __global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(Band
     const long long* wbegin = a.wbegin + (size_t)chunk * (kBandReduceWarps + 1);
     double* zh = zsm;
     double* zs = zsm + (size_t)struct_count * kPad;
-    double* th = zs + (size_t)struct_count * kPad;   // [kTileRows][kPad]
-    double* ts = th + (size_t)kTileRows * kPad;
     for (int i = threadIdx.x; i < struct_count * kPad; i += blockDim.x) {
         zh[i] = 0.0;
         zs[i] = 0.0;
     }
+    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long j0 = (long long)blockIdx.x * kBandReduceColumns;
-    long long row_end = a.e0 + j0 + kBandReduceColumns;  // rows d <= e of this column block
+    const long long j = (long long)blockIdx.x * kBandReduceColumns + lane;
+    const bool valid = j < a.width;
+    const long long e = a.e0 + j;
+    long long row_end = a.e0 + (long long)blockIdx.x * kBandReduceColumns + kBandReduceColumns;
     if (row_end > a.e0 + a.width) row_end = a.e0 + a.width;
-    const long long t_end = wbegin[warp + 1];
-    long long pos = wbegin[warp];
-    for (long long r0 = 0; r0 < row_end; r0 += kTileRows) {
-        __syncthreads();
-        for (int i = threadIdx.x; i < kTileRows * kBandReduceColumns; i += blockDim.x) {
-            const int r = i / kBandReduceColumns, c = i % kBandReduceColumns;
-            const long long d = r0 + r, jj = j0 + c;
-            const bool use = d < row_end && jj < a.width && d <= a.e0 + jj;
-            const long long o = use ? d * a.width + jj : 0;
-            th[r * kPad + c] = use ? __ldg(a.Hb + o) : 0.0;
-            ts[r * kPad + c] = use ? __ldg(a.Sb + o) : 0.0;
+    const long long t_begin = wbegin[warp], t_end = wbegin[warp + 1];
+    for (long long base = t_begin; base < t_end; base += 32) {
+        const long long mine = base + lane;
+        int d_l = 0x7fffffff, I_l = 0;
+        double c_l = 0.0;
+        if (mine < t_end) {
+            d_l = __ldg(a.wdet + mine);
+            I_l = __ldg(a.wstruct + mine);
+            c_l = __ldg(a.wcoef + mine);
         }
-        __syncthreads();
-        const long long tile_end = r0 + kTileRows < row_end ? r0 + kTileRows : row_end;
-        while (pos < t_end) {
-            const long long mine = pos + lane;
-            int d_l = 0x7fffffff, I_l = 0;
-            double c_l = 0.0;
-            if (mine < t_end) {
-                d_l = __ldg(a.wdet + mine);
-                I_l = __ldg(a.wstruct + mine);
-                c_l = __ldg(a.wcoef + mine);
+        const int first = __shfl_sync(0xffffffffu, d_l, 0);
+        if (first >= row_end) break;
+        // eight independent band loads in flight per batch
+#pragma unroll
+        for (int q0 = 0; q0 < 32; q0 += 8) {
+            int d[8], I[8];
+            double c[8], hv[8], sv[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                d[i] = __shfl_sync(0xffffffffu, d_l, q0 + i);
+                I[i] = __shfl_sync(0xffffffffu, I_l, q0 + i);
+                c[i] = __shfl_sync(0xffffffffu, c_l, q0 + i);
             }
-            // triples of this tile: a prefix of the sorted batch
-            const unsigned in_tile = __ballot_sync(0xffffffffu, (long long)d_l < tile_end);
-            const int cnt = __popc(in_tile);
-            for (int q = 0; q < cnt; ++q) {
-                const int d = __shfl_sync(0xffffffffu, d_l, q);
-                const int I = __shfl_sync(0xffffffffu, I_l, q);
-                const double c = __shfl_sync(0xffffffffu, c_l, q);
-                const int r = d - (int)r0;
-                zh[I * kPad + lane] = fma(c, th[r * kPad + lane], zh[I * kPad + lane]);
-                zs[I * kPad + lane] = fma(c, ts[r * kPad + lane], zs[I * kPad + lane]);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const bool use = valid && d[i] <= e && d[i] < row_end;
+                const long long o = use ? (long long)d[i] * a.width + j : 0;
+                hv[i] = use ? __ldg(a.Hb + o) : 0.0;
+                sv[i] = use ? __ldg(a.Sb + o) : 0.0;
             }
-            pos += cnt;
-            if (cnt < 32) break;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (d[i] >= row_end) continue;  // padding triples and rows past this column block
+                zh[I[i] * kPad + lane] = fma(c[i], hv[i], zh[I[i] * kPad + lane]);
+                zs[I[i] * kPad + lane] = fma(c[i], sv[i], zs[I[i] * kPad + lane]);
+            }
         }
     }
     __syncthreads();
-    const long long col0 = a.e0 + j0;
+    const long long col0 = a.e0 + (long long)blockIdx.x * kBandReduceColumns;
     for (int i = threadIdx.x; i < struct_count * kBandReduceColumns; i += blockDim.x) {
         const int I = i % struct_count, l = i / struct_count;
-        if (j0 + l >= a.width) continue;
+        if ((long long)blockIdx.x * kBandReduceColumns + l >= a.width) continue;
         const long long col = col0 + l;
         a.Zh[col * a.n_str + struct_begin + I] = zh[I * kPad + l];
         a.Zs[col * a.n_str + struct_begin + I] = zs[I * kPad + l];
@@ -125,11 +123,9 @@ __global__ void symmetrize_kernel(int n, const double* __restrict__ Wh, const do
 
 }  // namespace
 
-size_t band_reduce_smem_bytes(int struct_count) {
-    return sizeof(double) * 2 * ((size_t)struct_count + kTileRows) * kPad;
-}
+size_t band_reduce_smem_bytes(int struct_count) { return sizeof(double) * 2 * (size_t)struct_count * kPad; }
 
-// 64 structures per chunk: 33.8 KB of accumulators and 33.8 KB of band tile, three CTAs per SM.
+// 64 structures per chunk: 33.8 KB of accumulators, six CTAs per SM.
 int band_reduce_max_structures() { return 64; }
 
 cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches) {

@@ -489,6 +489,16 @@ vb_status prepare_spin_records(vb_hs_plan* p, const double* S, const double* h, 
         err = launch_spin_pairs(table_args(p, true, *dS, *dh, *deri), p->tables_b.as<double>(), s, launches);
         if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs (beta)");
     }
+    spin.close();
+    PhaseMark exact(p, VB_PHASE_EXACT_PAIRS);
+    if (p->ka > 0) {
+        err = launch_spin_pairs_exact(table_args(p, false, *dS, *dh, *deri), s, launches);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs exact (alpha)");
+    }
+    if (p->kb > 0 && !p->shared_tables) {
+        err = launch_spin_pairs_exact(table_args(p, true, *dS, *dh, *deri), s, launches);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "spin_pairs exact (beta)");
+    }
     p->records_current = mem == VB_MEM_HOST;
     return VB_OK;
 }

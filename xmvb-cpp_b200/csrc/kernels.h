@@ -119,9 +119,12 @@ cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work,
                                       double* lf, int ld, int* meta, cudaStream_t stream);
 // Spin-pair records of one string table: the per-left-string frame tables first
 // (launch_spin_tables, nothing when the register path does not apply), then launch_spin_pairs
-// (the frame kernel and the exact path for the blocks it lists, or the exact path for all).
+// (the frame kernel, listing the blocks it cannot certify) and launch_spin_pairs_exact.
 cudaError_t launch_spin_tables(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches);
 cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream_t stream, int* launches);
+// The exact path of one string table: the blocks launch_spin_pairs listed, or every block when the
+// register path does not apply.
+cudaError_t launch_spin_pairs_exact(const SpinTableArgs& a, cudaStream_t stream, int* launches);
 // Frame kernels (spin_frame.cu): per-left-string block size, the envelope of the register path,
 // the once-per-table bucketing of right strings, and the table and pair launches.
 size_t frame_table_doubles(int n, int k, int R);

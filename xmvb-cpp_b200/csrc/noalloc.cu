@@ -227,6 +227,7 @@ extern "C" vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, in
     err = launch_spin_tables(a, reinterpret_cast<double*>(b + o_tables), s, &launches);
     if (err != cudaSuccess) return cuda_error(nullptr, err, "spin tables");
     err = launch_spin_pairs(a, reinterpret_cast<double*>(b + o_tables), s, &launches);
+    if (err == cudaSuccess) err = launch_spin_pairs_exact(a, s, &launches);
     if (err != cudaSuccess) return cuda_error(nullptr, err, "spin_pairs");
     long long blocks = (n_pairs + 255) / 256;
     if (blocks > 4096) blocks = 4096;

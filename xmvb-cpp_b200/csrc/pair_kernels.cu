@@ -299,34 +299,78 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
             // is (r1 c1 | r2 c2) - (r1 c2 | r2 c1)
             if (__shfl_sync(0xffffffffu, (int)regular, j)) {
                 double part = 0.0;
-                for (int q = lane; q < cp * cp; q += 32) {
-                    const int rp = q / cp, cq = q % cp;
-                    int r2 = 1;
-                    while ((r2 + 1) * r2 / 2 <= rp) ++r2;
-                    const int r1 = rp - r2 * (r2 - 1) / 2;
-                    int c2 = 1;
-                    while ((c2 + 1) * c2 / 2 <= cq) ++c2;
-                    const int c1 = cq - c2 * (c2 - 1) / 2;
-                    const double g = __ldg(a.gamma + (long long)dev::anti_index(occ_byte(orr, r1), occ_byte(orr, r2)) * gd +
-                                           dev::anti_index(occ_byte(ol, c1), occ_byte(ol, c2)));
-                    part = fma(g, cj[c1 * k + r1] * cj[c2 * k + r2] - cj[c2 * k + r1] * cj[c1 * k + r2], part);
+                if constexpr (KC > 0) {
+                    // k fixed: every lane's terms unrolled, occupations from registers, loads batched
+                    constexpr int CPK = KC * (KC - 1) / 2;
+                    constexpr int PER = (CPK * CPK + 31) / 32;
+                    const uint64_t wl = __ldg(ol), wr = __ldg(orr);
+#pragma unroll 2
+                    for (int t = 0; t < PER; ++t) {
+                        const int q = lane + 32 * t;
+                        if (q < CPK * CPK) {
+                            const int rp = q / CPK, cq = q % CPK;
+                            int r2 = 1;
+                            while ((r2 + 1) * r2 / 2 <= rp) ++r2;
+                            const int r1 = rp - r2 * (r2 - 1) / 2;
+                            int c2 = 1;
+                            while ((c2 + 1) * c2 / 2 <= cq) ++c2;
+                            const int c1 = cq - c2 * (c2 - 1) / 2;
+                            const int R1 = (int)((wr >> (8 * r1)) & 0xFFu), R2 = (int)((wr >> (8 * r2)) & 0xFFu);
+                            const int L1 = (int)((wl >> (8 * c1)) & 0xFFu), L2 = (int)((wl >> (8 * c2)) & 0xFFu);
+                            const double g = __ldg(a.gamma + (long long)dev::anti_index(R1, R2) * gd + dev::anti_index(L1, L2));
+                            part = fma(g, cj[c1 * KC + r1] * cj[c2 * KC + r2] - cj[c2 * KC + r1] * cj[c1 * KC + r2], part);
+                        }
+                    }
+                } else {
+                    for (int q = lane; q < cp * cp; q += 32) {
+                        const int rp = q / cp, cq = q % cp;
+                        int r2 = 1;
+                        while ((r2 + 1) * r2 / 2 <= rp) ++r2;
+                        const int r1 = rp - r2 * (r2 - 1) / 2;
+                        int c2 = 1;
+                        while ((c2 + 1) * c2 / 2 <= cq) ++c2;
+                        const int c1 = cq - c2 * (c2 - 1) / 2;
+                        const double g = __ldg(a.gamma + (long long)dev::anti_index(occ_byte(orr, r1), occ_byte(orr, r2)) * gd +
+                                               dev::anti_index(occ_byte(ol, c1), occ_byte(ol, c2)));
+                        part = fma(g, cj[c1 * k + r1] * cj[c2 * k + r2] - cj[c2 * k + r1] * cj[c1 * k + r2], part);
+                    }
                 }
                 for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
                 if (lane == j) h2 = part / det;
             }
             // u-vectors: u_m = sum_{c,r} A(r,c) l_m[pair(R_r, L_c)]
             double* rec = a.records + record_index(uj, vj, N) * (long long)a.rec_stride;
-            for (int m = lane; m < a.R; m += 32) {
-                double acc = 0.0;
-                for (int c = 0; c < k; ++c) {
-                    const int lc = occ_byte(ol, c);
-                    for (int r = 0; r < k; ++r) {
-                        const double cv = cj[c * k + r];
-                        if (cv != 0.0)
-                            acc = fma(cv, __ldg(a.lf + (long long)dev::pair_index(occ_byte(orr, r), lc) * a.ld + m), acc);
+            if constexpr (KC > 0) {
+                // k fixed: the k^2 factor-row loads of a column issued together
+                const uint64_t wl = __ldg(ol), wr = __ldg(orr);
+                for (int m = lane; m < a.R; m += 32) {
+                    double acc = 0.0;
+#pragma unroll 1
+                    for (int c = 0; c < KC; ++c) {
+                        const int lc = (int)((wl >> (8 * c)) & 0xFFu);
+                        double v[KC];
+#pragma unroll
+                        for (int r = 0; r < KC; ++r)
+                            v[r] = __ldg(a.lf + (long long)dev::pair_index((int)((wr >> (8 * r)) & 0xFFu), lc) * a.ld + m);
+#pragma unroll
+                        for (int r = 0; r < KC; ++r) acc = fma(cj[c * KC + r], v[r], acc);
                     }
+                    rec[m] = acc;
                 }
-                rec[m] = acc;
+            } else {
+                for (int m = lane; m < a.R; m += 32) {
+                    double acc = 0.0;
+                    for (int c = 0; c < k; ++c) {
+                        const int lc = occ_byte(ol, c);
+                        for (int r = 0; r < k; ++r) {
+                            const double cv = cj[c * k + r];
+                            if (cv != 0.0)
+                                acc = fma(cv, __ldg(a.lf + (long long)dev::pair_index(occ_byte(orr, r), lc) * a.ld + m),
+                                          acc);
+                        }
+                    }
+                    rec[m] = acc;
+                }
             }
         }
         if (valid) {
@@ -511,10 +555,9 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream
         const int tuned = autotune_run(
             key, frame_pair_variants(a.n, a.k, a.R), stream, [&](int v) { return launch_frame_pairs(a, tables, stream, v); },
             [&]() {
-                // the listed-pair counter and both kernels' task counters (compact at +0, dense at +2)
+                // the listed-pair counter and the task counter
                 cudaError_t e = cudaMemsetAsync(a.careful_count, 0, sizeof(unsigned long long), stream);
                 if (e == cudaSuccess) e = cudaMemsetAsync(a.task_counter, 0, sizeof(unsigned long long), stream);
-                if (e == cudaSuccess) e = cudaMemsetAsync(a.task_counter + 2, 0, sizeof(unsigned long long), stream);
                 return e;
             },
             &err);
@@ -522,6 +565,13 @@ cudaError_t launch_spin_pairs(const SpinTableArgs& a, double* tables, cudaStream
         if (err != cudaSuccess) return err;
         ++*launches;
     }
+    return cudaSuccess;
+}
+
+cudaError_t launch_spin_pairs_exact(const SpinTableArgs& a, cudaStream_t stream, int* launches) {
+    if (a.n_pairs <= 0 || a.k <= 0) return cudaSuccess;
+    cudaError_t err = cudaSuccess;
+    const bool fast_ok = !a.all_careful && frame_spin_supported(a.n, a.k, a.R);
     SpinTableArgs b = a;
     b.all_careful = fast_ok ? 0 : 1;
     auto exact = a.k == 7 ? spin_pairs_exact<7, 7> : (a.k <= 8 ? spin_pairs_exact<8, 0> : spin_pairs_exact<dev::KMAX, 0>);

@@ -60,7 +60,7 @@ struct vb_hs_plan {
     // phase timing: per phase a pool of (start, stop) event pairs, `used` pairs this execute
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[VB_PHASE_COUNT];
-    int used[VB_PHASE_COUNT] = {0, 0, 0, 0, 0};
+    int used[VB_PHASE_COUNT] = {};
     ~vb_hs_plan() {
         if (meta_host) cudaFreeHost(meta_host);
         for (auto& v : events)

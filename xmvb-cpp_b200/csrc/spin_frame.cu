@@ -591,14 +591,50 @@ __device__ __forceinline__ void frame_pair(const double* __restrict__ blk, const
     *hm_out = hm;
 }
 
+// Compact slots: W of an E <= 5 pair (25 doubles; stride 26 spreads a tile's pairs over banks).
+// Higher levels use fewer pairs per chunk with E^2 + 1 doubles per slot in the same 32 x 26
+// doubles of the warp: 16 pairs for E = 6, 7, 8 pairs for E = 8.
+constexpr int kCompactEMax = 5;
+constexpr int kCompactSlot = 26;
+
+__host__ __device__ constexpr int compact_chunk_pairs(int e) { return e <= kCompactEMax ? 32 : (e <= 7 ? 16 : 8); }
+__host__ __device__ constexpr int compact_slot(int e) { return e <= kCompactEMax ? kCompactSlot : e * e + 1; }
+
+// The high excitation levels (E > kCompactEMax, about 1.5 % of the pairs at K = 7) out of line:
+// their E x E registers do not count against the register budget of the common levels.
+struct PairOut {
+    double det, quad;
+    unsigned hm, hmap, pmap;
+    bool ok;
+};
+
+template <int K, int E>
+__device__ __noinline__ PairOut frame_pair_out_of_line(const double* __restrict__ blk, const FrameLayout* F,
+                                                       unsigned desc, double* __restrict__ yrow) {
+    PairOut o;
+    frame_pair<K, E, true>(blk, *F, desc, yrow, &o.ok, &o.det, &o.quad, &o.hm, &o.hmap, &o.pmap);
+    return o;
+}
+
 template <int K, int ELO, int EHI, bool COMPACT>
 __device__ __forceinline__ void frame_pair_dispatch(int e, const double* blk, const FrameLayout& F, unsigned desc,
                                                     double* yrow, bool* ok, double* det, double* quad, unsigned* hm,
                                                     unsigned* hmap, unsigned* pmap) {
 #define VB_FRAME_CASE(E_)                                                                             \
     case E_:                                                                                          \
-        if constexpr (E_ >= ELO && E_ <= EHI && E_ <= K)                                              \
-            frame_pair<K, E_, COMPACT>(blk, F, desc, yrow, ok, det, quad, hm, hmap, pmap);             \
+        if constexpr (E_ >= ELO && E_ <= EHI && E_ <= K) {                                            \
+            if constexpr (COMPACT && E_ > kCompactEMax) {                                             \
+                const PairOut o = frame_pair_out_of_line<K, E_>(blk, &F, desc, yrow);                 \
+                *ok = o.ok;                                                                           \
+                *det = o.det;                                                                         \
+                *quad = o.quad;                                                                       \
+                *hm = o.hm;                                                                           \
+                *hmap = o.hmap;                                                                       \
+                *pmap = o.pmap;                                                                       \
+            } else {                                                                                  \
+                frame_pair<K, E_, COMPACT>(blk, F, desc, yrow, ok, det, quad, hm, hmap, pmap);         \
+            }                                                                                         \
+        }                                                                                             \
         break;
     switch (e) {
         VB_FRAME_CASE(0)
@@ -615,9 +651,6 @@ __device__ __forceinline__ void frame_pair_dispatch(int e, const double* blk, co
 #undef VB_FRAME_CASE
 }
 
-// Compact slots: W of an E <= 5 pair (25 doubles; stride 26 spreads a tile's pairs over banks).
-constexpr int kCompactEMax = 5;
-constexpr int kCompactSlot = 26;
 
 __host__ __device__ constexpr int frame_row_doubles(int K, bool compact) { return compact ? kCompactSlot : fr_kfs(K); }
 
@@ -656,7 +689,10 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps, COMPACT ? 2 : 1)
         for (int e = 0; e < K + 2; ++e) bound[e] = __ldg(eb + e);
         int nchunks = 0;
 #pragma unroll
-        for (int e = ELO; e <= EHI && e <= K; ++e) nchunks += (bound[e + 1] - bound[e] + 31) >> 5;
+        for (int e = ELO; e <= EHI && e <= K; ++e) {
+            const int cs = COMPACT ? compact_chunk_pairs(e) : 32;
+            nchunks += (bound[e + 1] - bound[e] + cs - 1) / cs;
+        }
         if (nchunks == 0) {
             __syncthreads();
             continue;
@@ -678,11 +714,12 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps, COMPACT ? 2 : 1)
             int e = -1, start = 0, cnt = 0, left = ch;
 #pragma unroll
             for (int ee = (EHI < K ? EHI : K); ee >= ELO; --ee) {
-                const int c = (bound[ee + 1] - bound[ee] + 31) >> 5;
+                const int cs = COMPACT ? compact_chunk_pairs(ee) : 32;
+                const int c = (bound[ee + 1] - bound[ee] + cs - 1) / cs;
                 if (left >= 0 && left < c) {
                     e = ee;
-                    start = bound[ee] + 32 * left;
-                    cnt = min(32, bound[ee + 1] - start);
+                    start = bound[ee] + cs * left;
+                    cnt = min(cs, bound[ee + 1] - start);
                 }
                 left -= c;
             }
@@ -708,7 +745,8 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps, COMPACT ? 2 : 1)
                 for (int f = lane; f < 16 * KFS; f += 32) z[f] = make_double2(0.0, 0.0);
                 __syncwarp();
             }
-            double* yrow = yw + lane * ROW;
+            const int slot = COMPACT ? compact_slot(e) : ROW;
+            double* yrow = yw + lane * slot;
             bool ok = false;
             double det = 0.0, quad = 0.0;
             unsigned hm = 0, hmap = 0xFFFFFFFFu, pmap = 0xFFFFFFFFu;
@@ -724,8 +762,9 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps, COMPACT ? 2 : 1)
             const unsigned okbits = __ballot_sync(0xffffffffu, ok);
             __syncwarp();
             // phase B, one 8-pair tile at a time
+            const int tiles = COMPACT ? compact_chunk_pairs(e) / 8 : 4;
 #pragma unroll 1
-            for (int mt = 0; mt < 4; ++mt) {
+            for (int mt = 0; mt < tiles; ++mt) {
                 const unsigned uh = __reduce_or_sync(0xffffffffu, ((lane >> 3) == mt && ok) ? hm : 0u);
                 if (((okbits >> (8 * mt)) & 0xFFu) == 0) continue;
                 const int owner = 8 * mt + g;
@@ -735,7 +774,7 @@ __global__ void __launch_bounds__(32 * kFrameMaxWarps, COMPACT ? 2 : 1)
                 const unsigned hmap_g = __shfl_sync(0xffffffffu, hmap, owner);
                 const unsigned pmap_g = __shfl_sync(0xffffffffu, pmap, owner);
                 const bool ok_g = (okbits >> owner) & 1u;
-                const double* yr = yw + owner * ROW;
+                const double* yr = yw + owner * slot;
                 double* rec = a.records + t_g * (long long)a.rec_stride;
                 // this lane's particle slots for the two k-steps of a hole block (b = tq, tq + 4)
                 const unsigned i0 = (pmap_g >> (4 * tq)) & 0xFu, i1 = (pmap_g >> (4 * (tq + 4))) & 0xFu;
@@ -807,12 +846,10 @@ size_t frame_spin_smem(int n, int R, int warps = 4, bool compact = false) {
     return sizeof(double) * ((size_t)frame_layout(n, K, R).total + (size_t)warps * 32 * frame_row_doubles(K, compact));
 }
 
-// The larger of the two kernels' shared memory (8-warp compact, 4-warp dense).
+// Shared memory of the largest launch variant (8 warps per CTA).
 template <int K>
 size_t frame_spin_smem_max(int n, int R) {
-    const size_t c = frame_spin_smem<K>(n, R, 8, true);
-    const size_t d = K > kCompactEMax ? frame_spin_smem<K>(n, R, 1, false) : 0;
-    return c > d ? c : d;
+    return frame_spin_smem<K>(n, R, 8, true);
 }
 
 size_t frame_spin_smem_rt(int n, int k, int R) {
@@ -838,9 +875,8 @@ cudaError_t launch_tables(const SpinTableArgs& a, double* tables, cudaStream_t s
     return cudaGetLastError();
 }
 
-// Launch variants of the compact kernel (the autotuner's choices): 0 = 8 warps per CTA, 1 = 4,
-// 2 = 2; every variant fills each SM with as many resident CTAs as fit.  The dense kernel for
-// excitation levels 6 .. K (k >= 6 only) follows with one warp per CTA.
+// Launch variants of the pair kernel (the autotuner's choices): 0 = 8 warps per CTA, 1 = 4,
+// 2 = 2; every variant fills each SM with as many resident CTAs as fit.
 constexpr int kFrameVariants = 3;
 constexpr int kFrameVariantWarps[kFrameVariants] = {8, 4, 2};
 
@@ -863,13 +899,7 @@ cudaError_t launch_frame_part(const SpinTableArgs& a, const double* tables, cuda
 
 template <int K>
 cudaError_t launch_frame(const SpinTableArgs& a, const double* tables, cudaStream_t stream, int variant) {
-    constexpr int EL = K < kCompactEMax ? K : kCompactEMax;
-    cudaError_t err = launch_frame_part<K, 0, EL, true>(a, tables, stream, kFrameVariantWarps[variant]);
-    if (err != cudaSuccess) return err;
-    // the high levels have about one chunk per left string: one warp per CTA, so no warp of a CTA
-    // waits at the task barrier for another's chunk
-    if constexpr (K > kCompactEMax) err = launch_frame_part<K, kCompactEMax + 1, K, false>(a, tables, stream, 1);
-    return err;
+    return launch_frame_part<K, 0, K, true>(a, tables, stream, kFrameVariantWarps[variant]);
 }
 
 template <int K>
@@ -941,14 +971,10 @@ cudaError_t launch_frame_pairs(const SpinTableArgs& a, const double* tables, cud
 
 template <int K>
 cudaError_t preload_k() {
-    constexpr int EL = K < kCompactEMax ? K : kCompactEMax;
     cudaFuncAttributes fa{};
     cudaError_t err = cudaFuncGetAttributes(&fa, (const void*)sort_right_strings<K>);
     if (err == cudaSuccess) err = cudaFuncGetAttributes(&fa, (const void*)frame_tables<K>);
-    if (err == cudaSuccess) err = cudaFuncGetAttributes(&fa, (const void*)spin_pairs_frame<K, 0, EL, true>);
-    if constexpr (K > kCompactEMax)
-        if (err == cudaSuccess)
-            err = cudaFuncGetAttributes(&fa, (const void*)spin_pairs_frame<K, kCompactEMax + 1, K, false>);
+    if (err == cudaSuccess) err = cudaFuncGetAttributes(&fa, (const void*)spin_pairs_frame<K, 0, K, true>);
     return err;
 }
 

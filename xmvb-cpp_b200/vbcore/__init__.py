@@ -106,7 +106,7 @@ EXPORTED_SYMBOLS = (
     "vb_autotune_report", "vb_autotune_clear", "vb_ri_pair_factors_frame",
 )
 
-PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce")
+PHASES = ("tables", "spin_pairs", "determinant_pairs", "band_reduce", "structure_reduce", "exact_pairs")
 
 _lib = None
 
