@@ -426,6 +426,7 @@ def run_vbcore(args):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": stats["kernel_launches"] * args.steps,
             "careful_spin_pairs": stats["careful_spin_pairs"],
+            "factor_columns": stats["factor_columns"],
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

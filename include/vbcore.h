@@ -137,12 +137,14 @@ vb_status vb_hs_plan_execute(vb_hs_plan* plan, const double* ovlp_act, const dou
 
 /* Diagnostics of the last execute: spin pairs evaluated, pairs routed to the exact
  * full-pivot/SVD path, unordered determinant pairs evaluated (with alpha/beta-exchange
- * symmetry one pair per orbit {(d, e), (flip d, flip e)}), kernel launches. */
+ * symmetry one pair per orbit {(d, e), (flip d, flip e)}), kernel launches, and the number of
+ * columns of the pivoted LDL^T factorization of the pair kernel (ij|kl) (its numerical rank). */
 typedef struct {
     int64_t spin_pairs;
     int64_t careful_spin_pairs;
     int64_t determinant_pairs;
     int64_t kernel_launches;
+    int64_t factor_columns;
 } vb_hs_stats;
 vb_status vb_hs_plan_stats(const vb_hs_plan* plan, vb_hs_stats* stats);
 

@@ -55,6 +55,8 @@ def test_structure_matrices_match_oracle(ctx, kw, n, seed):
     assert np.array_equal(H, H.T) and np.array_equal(So, So.T)
     st = plan.stats()
     assert st["spin_pairs"] > 0 and st["kernel_launches"] >= 5
+    # (ij|kl) = sum_P B_ij^P B_kl^P with 3n auxiliary functions: the factorization stops at that rank
+    assert st["factor_columns"] == min(3 * n, n * (n + 1) // 2)
     if n <= 8:
         # one evaluation per orbit {(d, e), (flip d, flip e)} of unordered pairs (brute force)
         n_det = ex.n_determinants

@@ -9,7 +9,11 @@
 //   W  = Z T             (n_str x n_str; structure_reduce)
 //   H  = W + W^T         (symmetrize)
 // Every sum runs in a fixed order (no atomics), so results are bitwise reproducible.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+
+#include <mutex>
 
 #include "internal.h"
 #include "kernels.h"
@@ -17,79 +21,194 @@
 namespace vbcore {
 namespace {
 
-constexpr int kPad = kBandReduceColumns + 1;
+constexpr int kTileBytes = kBandTileRows * kBandColumns * 8;  // one band tile (H or S)
+constexpr int kZPad = kBandColumns + 1;
 
-// One CTA per (32 band columns, structure chunk of at most 64 structures): every chunk's
-// triples stream the band rows they need, and the small per-chunk accumulators let several
-// CTAs share an SM.  Warp w owns the chunk's structures bucketed to it (local structure index
-// = w mod warps), so each shared-memory accumulator has exactly one writer and the sum order is
-// fixed.  A warp walks its (determinant, structure, coefficient) triples, sorted by
-// determinant, 32 at a time: lane j fetches triple j, then the warp broadcasts them one by one;
-// the band loads of consecutive triples are independent, which keeps many loads in flight.
-__global__ void __launch_bounds__(kBandReduceWarps * 32) band_reduce_kernel(BandReduceArgs a) {
-    extern __shared__ double zsm[];
-    const int chunk = blockIdx.y;
-    const int struct_begin = __ldg(a.chunk_begin + chunk), struct_count = __ldg(a.chunk_count + chunk);
-    const long long* wbegin = a.wbegin + (size_t)chunk * (kBandReduceWarps + 1);
-    double* zh = zsm;
-    double* zs = zsm + (size_t)struct_count * kPad;
-    for (int i = threadIdx.x; i < struct_count * kPad; i += blockDim.x) {
-        zh[i] = 0.0;
-        zs[i] = 0.0;
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// One poll of the phase with the given parity; the thread may sleep up to ~1 us inside it.
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 1000;\n selp.u32 %0, 1, 0, "
+        "p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for the phase of `bar` with the given parity: false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
+    for (long long i = 0; i < limit; ++i)
+        if (mbar_test(bar, parity)) return true;
+    return false;
+}
+
+// TMA: a [kBandTileRows x kBandColumns] box of the band at (column x, row y); rows past n_det
+// and columns past the band width arrive as zeros.
+__device__ __forceinline__ void tma_band_tile(void* dst, const CUtensorMap* map, int x, int y,
+                                              unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Contiguous bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// One CTA per (32 band columns, structure group of kBandGroup), heaviest column blocks first
+// (a column block needs the band rows d <= its last column).  The rows stream through two
+// shared-memory stages, each filled by TMA (the H and S tiles) and bulk copies (the tile's
+// terms of this structure group), completion tracked by one mbarrier per stage.  Lane l owns
+// band column l; warp w accumulates the kBandSlots structures s * kBandWarps + w of the group in
+// registers, walking each structure's terms of the tile in determinant order, two per step.
+// Tiles that reach below the diagonal have their entries d > e zeroed in shared memory first,
+// so the term loop carries no mask.  The accumulators then pass through shared memory so that
+// Z is written in coalesced runs of structures.
+__global__ void __launch_bounds__(kBandWarps * 32, 3)
+    band_reduce_kernel(const __grid_constant__ CUtensorMap map_h, const __grid_constant__ CUtensorMap map_s,
+                       BandReduceArgs a, int stage_bytes) {
+    extern __shared__ __align__(1024) unsigned char bsm_raw[];
+    __shared__ __align__(8) unsigned long long full[2];
+    // stages start on 1024-byte boundaries (TMA destinations; the launch adds the slack)
+    unsigned char* bsm = bsm_raw + ((1024u - (smem_addr(bsm_raw) & 1023u)) & 1023u);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int G = a.n_groups;
+    const long long nb = (a.width + kBandColumns - 1) / kBandColumns;
+    const long long b = nb - 1 - (long long)blockIdx.x / G;
+    const int g = (int)(blockIdx.x % G);
+    const long long col0 = b * kBandColumns;
+    long long rows = a.e0 + col0 + kBandColumns;
+    if (rows > a.n_det) rows = a.n_det;
+    const int ntiles = (int)((rows + kBandTileRows - 1) / kBandTileRows);
+    const int seg_max = a.seg_max;
+
+    auto issue = [&](int t, int st) {
+        unsigned char* base = bsm + (size_t)st * stage_bytes;
+        const long long seg = (long long)g * a.n_tiles + t;
+        const long long o0 = a.seg_off[seg];
+        const unsigned len = (unsigned)(a.seg_off[seg + 1] - o0);
+        mbar_expect_tx(&full[st], 2u * kTileBytes + 9u * len + kBandMetaBytes);
+        tma_band_tile(base, &map_h, (int)col0, t * kBandTileRows, &full[st]);
+        tma_band_tile(base + kTileBytes, &map_s, (int)col0, t * kBandTileRows, &full[st]);
+        if (len) {
+            bulk_load(base + 2 * kTileBytes, a.term_c + o0, 8u * len, &full[st]);
+            bulk_load(base + 2 * kTileBytes + 8 * seg_max, a.term_d + o0, len, &full[st]);
+        }
+        bulk_load(base + 2 * kTileBytes + 9 * seg_max, a.seg_meta + seg * kBandMetaBytes, kBandMetaBytes, &full[st]);
+    };
+
+    if (tid == 0) {
+        mbar_init(&full[0]);
+        mbar_init(&full[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long j = (long long)blockIdx.x * kBandReduceColumns + lane;
-    const bool valid = j < a.width;
-    const long long e = a.e0 + j;
-    long long row_end = a.e0 + (long long)blockIdx.x * kBandReduceColumns + kBandReduceColumns;
-    if (row_end > a.e0 + a.width) row_end = a.e0 + a.width;
-    const long long t_begin = wbegin[warp], t_end = wbegin[warp + 1];
-    for (long long base = t_begin; base < t_end; base += 32) {
-        const long long mine = base + lane;
-        int d_l = 0x7fffffff, I_l = 0;
-        double c_l = 0.0;
-        if (mine < t_end) {
-            d_l = __ldg(a.wdet + mine);
-            I_l = __ldg(a.wstruct + mine);
-            c_l = __ldg(a.wcoef + mine);
+    int issued = 0;  // tiles issued so far (thread 0)
+    if (tid == 0) {
+        issue(0, 0);
+        if (ntiles > 1) issue(1, 1);
+        issued = ntiles > 1 ? 2 : 1;
+    }
+    double acc_h[kBandSlots], acc_s[kBandSlots];
+#pragma unroll
+    for (int s = 0; s < kBandSlots; ++s) acc_h[s] = acc_s[s] = 0.0;
+
+    // One barrier per tile: after computing tile t every thread waits for tile t + 1, and the
+    // barrier then both releases stage t & 1 for refilling and confirms tile t + 1 landed.
+    const long long limit = a.spin_limit / 16 > 0 ? a.spin_limit / 16 : 1;  // polls of <= ~1 us
+    bool ok = __syncthreads_and(mbar_wait(&full[0], 0u, limit)) != 0;
+    int t = 0;
+    for (; ok && t < ntiles; ++t) {
+        const int st = t & 1;
+        unsigned char* base = bsm + (size_t)st * stage_bytes;
+        const long long r0 = (long long)t * kBandTileRows;
+        if (r0 + kBandTileRows - 1 > a.e0 + col0) {
+            // rows below the diagonal of this column block hold no data: zero them
+            double* zH = reinterpret_cast<double*>(base);
+            double* zS = zH + kBandTileRows * kBandColumns;
+            for (int i = tid; i < kBandTileRows * kBandColumns; i += blockDim.x) {
+                const int dl = i / kBandColumns, l = i % kBandColumns;
+                if (r0 + dl > a.e0 + col0 + l) {
+                    zH[i] = 0.0;
+                    zS[i] = 0.0;
+                }
+            }
+            // these generic-proxy writes precede the stage's next TMA fill
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
         }
-        const int first = __shfl_sync(0xffffffffu, d_l, 0);
-        if (first >= row_end) break;
-        // eight independent band loads in flight per batch
+        const double* tH = reinterpret_cast<const double*>(base);
+        const double* tS = reinterpret_cast<const double*>(base + kTileBytes);
+        const double* tc = reinterpret_cast<const double*>(base + 2 * kTileBytes);
+        const unsigned char* td = base + 2 * kTileBytes + 8 * seg_max;
+        const unsigned char* cnt = td + seg_max;
+        int q = reinterpret_cast<const unsigned short*>(cnt + kBandWarps * kBandSlots)[warp];
 #pragma unroll
-        for (int q0 = 0; q0 < 32; q0 += 8) {
-            int d[8], I[8];
-            double c[8], hv[8], sv[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                d[i] = __shfl_sync(0xffffffffu, d_l, q0 + i);
-                I[i] = __shfl_sync(0xffffffffu, I_l, q0 + i);
-                c[i] = __shfl_sync(0xffffffffu, c_l, q0 + i);
+        for (int s = 0; s < kBandSlots; ++s) {
+            const int n = cnt[warp * kBandSlots + s];
+            for (int i = 0; i < n; i += 2, q += 2) {
+                const bool two = i + 1 < n;
+                const int d0 = td[q], d1 = two ? td[q + 1] : d0;
+                const double c0 = tc[q], c1 = two ? tc[q + 1] : 0.0;
+                const double h0 = tH[d0 * kBandColumns + lane], h1 = tH[d1 * kBandColumns + lane];
+                const double s0 = tS[d0 * kBandColumns + lane], s1 = tS[d1 * kBandColumns + lane];
+                acc_h[s] = fma(c1, h1, fma(c0, h0, acc_h[s]));
+                acc_s[s] = fma(c1, s1, fma(c0, s0, acc_s[s]));
             }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const bool use = valid && d[i] <= e && d[i] < row_end;
-                const long long o = use ? (long long)d[i] * a.width + j : 0;
-                hv[i] = use ? __ldg(a.Hb + o) : 0.0;
-                sv[i] = use ? __ldg(a.Sb + o) : 0.0;
-            }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (d[i] >= row_end) continue;  // padding triples and rows past this column block
-                zh[I[i] * kPad + lane] = fma(c[i], hv[i], zh[I[i] * kPad + lane]);
-                zs[I[i] * kPad + lane] = fma(c[i], sv[i], zs[I[i] * kPad + lane]);
-            }
+            q -= (n & 1);
+        }
+        const bool next = t + 1 >= ntiles || mbar_wait(&full[st ^ 1], (unsigned)((t + 1) >> 1) & 1u, limit);
+        ok = __syncthreads_and(next) != 0;
+        if (ok && tid == 0 && t + 2 < ntiles) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(t + 2, st);
+            ++issued;
         }
     }
+    if (!ok) {
+        // a tile never landed: flag it, let the copies still in flight land, and leave
+        if (tid == 0) {
+            atomicExch(a.error, 1);
+            for (int u = t; u < issued; ++u) mbar_wait(&full[u & 1], (unsigned)(u >> 1) & 1u, limit);
+        }
+        __syncthreads();
+        return;
+    }
+    double* zh = reinterpret_cast<double*>(bsm);
+    double* zs = zh + kBandGroup * kZPad;
+#pragma unroll
+    for (int s = 0; s < kBandSlots; ++s) {
+        const int li = s * kBandWarps + warp;
+        zh[li * kZPad + lane] = acc_h[s];
+        zs[li * kZPad + lane] = acc_s[s];
+    }
     __syncthreads();
-    const long long col0 = a.e0 + (long long)blockIdx.x * kBandReduceColumns;
-    for (int i = threadIdx.x; i < struct_count * kBandReduceColumns; i += blockDim.x) {
-        const int I = i % struct_count, l = i / struct_count;
-        if ((long long)blockIdx.x * kBandReduceColumns + l >= a.width) continue;
-        const long long col = col0 + l;
-        a.Zh[col * a.n_str + struct_begin + I] = zh[I * kPad + l];
-        a.Zs[col * a.n_str + struct_begin + I] = zs[I * kPad + l];
+    const int gbegin = g * kBandGroup;
+    const int gcount = min(kBandGroup, a.n_str - gbegin);
+    for (int i = tid; i < gcount * kBandColumns; i += blockDim.x) {
+        const int l = i / gcount, li = i - l * gcount;
+        if (col0 + l >= a.width) break;
+        const long long col = a.e0 + col0 + l;
+        a.Zh[col * a.n_str + gbegin + li] = zh[li * kZPad + l];
+        a.Zs[col * a.n_str + gbegin + li] = zs[li * kZPad + l];
     }
 }
 
@@ -123,17 +242,55 @@ __global__ void symmetrize_kernel(int n, const double* __restrict__ Wh, const do
 
 }  // namespace
 
-size_t band_reduce_smem_bytes(int struct_count) { return sizeof(double) * 2 * (size_t)struct_count * kPad; }
+static int band_stage_bytes(int seg_max) { return (2 * kTileBytes + 9 * seg_max + kBandMetaBytes + 1023) / 1024 * 1024; }
 
-// 64 structures per chunk: 33.8 KB of accumulators, six CTAs per SM.
-int band_reduce_max_structures() { return 64; }
+size_t band_reduce_smem_bytes(int seg_max) {
+    const size_t stages = 2 * (size_t)band_stage_bytes(seg_max);
+    const size_t z = 2 * sizeof(double) * kBandGroup * kZPad;
+    return (stages > z ? stages : z) + 1024;  // + alignment slack
+}
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+bool band_tensor_map(CUtensorMap* map, const double* band, long long width, long long n_det, long long ldb) {
+    auto encode = tensor_map_encoder();
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)n_det};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldb * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)kBandColumns, (cuuint32_t)kBandTileRows};
+    const cuuint32_t elem[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(band), dims, strides, box, elem,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
 
 cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int* launches) {
-    const size_t smem = band_reduce_smem_bytes(a.max_count);
-    cudaError_t err = allow_dynamic_smem((const void*)band_reduce_kernel, (int)smem);
+    if (a.width <= 0 || a.n_str <= 0) return cudaSuccess;
+    if (a.ldb % 2 != 0 || (reinterpret_cast<uintptr_t>(a.Hb) & 15) || (reinterpret_cast<uintptr_t>(a.Sb) & 15))
+        return cudaErrorInvalidValue;
+    CUtensorMap mh, ms;
+    if (!band_tensor_map(&mh, a.Hb, a.width, a.n_det, a.ldb) || !band_tensor_map(&ms, a.Sb, a.width, a.n_det, a.ldb))
+        return cudaErrorInvalidValue;
+    const size_t smem = band_reduce_smem_bytes(a.seg_max);
+    cudaError_t err = allow_dynamic_smem((const void*)band_reduce_kernel, smem);
     if (err != cudaSuccess) return err;
-    const long long blocks = (a.width + kBandReduceColumns - 1) / kBandReduceColumns;
-    band_reduce_kernel<<<dim3((unsigned)blocks, (unsigned)a.n_chunks), kBandReduceWarps * 32, smem, stream>>>(a);
+    const long long blocks = (a.width + kBandColumns - 1) / kBandColumns * a.n_groups;
+    band_reduce_kernel<<<(unsigned)blocks, kBandWarps * 32, smem, stream>>>(mh, ms, a, band_stage_bytes(a.seg_max));
     ++*launches;
     return cudaGetLastError();
 }

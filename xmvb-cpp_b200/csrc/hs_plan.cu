@@ -206,7 +206,7 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
         if ((st = b->allocate(ctx, sizeof(double) * p->np * p->np)) != VB_OK) return fail(st);
     if ((st = p->fsigns.allocate(ctx, sizeof(int) * p->np)) != VB_OK) return fail(st);
     if ((st = p->fmeta.allocate(ctx, sizeof(int) * 2)) != VB_OK) return fail(st);
-    if (cudaMallocHost(&p->meta_host, sizeof(int) * 2) != cudaSuccess) return fail(set_error(ctx, VB_ERR_CUDA, "cudaMallocHost"));
+    if (cudaMallocHost(&p->meta_host, sizeof(int) * 4) != cudaSuccess) return fail(set_error(ctx, VB_ERR_CUDA, "cudaMallocHost"));
 
     // spin-flip map: determinant with the alpha and beta strings exchanged; usable when every
     // determinant's image exists and carries the same structure coefficients
@@ -269,6 +269,7 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     long long width = (long long)(band_cap / (16 * (size_t)p->n_det));
     width = std::max(32LL, std::min(width, p->n_det));
     p->band_width = width;
+    p->band_ld = (width + 31) / 32 * 32;
     // the bands and the structure-reduce buffers (Z, W) are the context's execute scratch
     const size_t wbytes = sizeof(double) * (size_t)p->n_str * p->n_str;
     for (DeviceBuffer* b : {&p->Hout, &p->Sout})
@@ -292,47 +293,52 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     if ((st = upload(ctx, p->str_coef, scoef.data(), sizeof(double) * std::max<size_t>(1, scoef.size()))) != VB_OK)
         return fail(st);
 
-    // per structure chunk and warp bucket ((structure - begin) mod warps): triples
-    // (determinant, local structure, coefficient) sorted by determinant, concatenated over chunks
+    // band-reduction term segments: for every (structure group, row tile) the terms (row in the
+    // tile, coefficient) of the group's structures ordered by (warp, slot, determinant)
     {
-        const int max_chunk = band_reduce_max_structures();
-        std::vector<int> cbegin, ccount;
-        std::vector<long long> wbegin;
-        std::vector<int> wdet, wstruct;
-        std::vector<double> wcoef;
-        for (int begin = 0; begin < p->n_str; begin += max_chunk) {
-            const int count = std::min(max_chunk, p->n_str - begin);
-            cbegin.push_back(begin);
-            ccount.push_back(count);
-            for (int w = 0; w < kBandReduceWarps; ++w) {
-                wbegin.push_back((long long)wdet.size());
-                for (long long d = 0; d < p->n_det; ++d)
-                    for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t) {
-                        const int I = ex->term_structure[t];
-                        if (I >= begin && I < begin + count && (I - begin) % kBandReduceWarps == w) {
-                            wdet.push_back((int)d);
-                            wstruct.push_back(I - begin);
-                            wcoef.push_back(ex->term_coefficient[t]);
-                        }
+        BandSegments& b = p->segments;
+        b.n_groups = (p->n_str + kBandGroup - 1) / kBandGroup;
+        b.n_tiles = (int)((p->n_det + kBandTileRows - 1) / kBandTileRows);
+        const size_t nseg = (size_t)b.n_groups * b.n_tiles;
+        std::vector<long long> off(nseg + 1, 0);
+        std::vector<unsigned char> meta(nseg * kBandMetaBytes, 0);
+        std::vector<double> coef;
+        std::vector<unsigned char> row;
+        std::vector<long long> cur(soff.begin(), soff.end() - 1);  // next term of each structure
+        for (int g = 0; g < b.n_groups; ++g)
+            for (int t = 0; t < b.n_tiles; ++t) {
+                const size_t seg = (size_t)g * b.n_tiles + t;
+                off[seg] = (long long)coef.size();
+                unsigned char* m = meta.data() + seg * kBandMetaBytes;
+                const long long r0 = (long long)t * kBandTileRows, r1 = r0 + kBandTileRows;
+                int within = 0;
+                for (int w = 0; w < kBandWarps; ++w) {
+                    const unsigned short start = (unsigned short)within;
+                    std::memcpy(m + kBandWarps * kBandSlots + 2 * w, &start, 2);
+                    for (int sl = 0; sl < kBandSlots; ++sl) {
+                        const int I = g * kBandGroup + sl * kBandWarps + w;
+                        int cnt = 0;
+                        if (I < p->n_str)
+                            for (; cur[I] < soff[I + 1] && sdet[cur[I]] < r1; ++cur[I], ++cnt) {
+                                row.push_back((unsigned char)(sdet[cur[I]] - r0));
+                                coef.push_back(scoef[cur[I]]);
+                            }
+                        m[w * kBandSlots + sl] = (unsigned char)cnt;
+                        within += cnt;
                     }
+                }
+                while (coef.size() % 16) {
+                    coef.push_back(0.0);
+                    row.push_back(0);
+                }
+                b.seg_max = std::max(b.seg_max, (int)((long long)coef.size() - off[seg]));
             }
-            wbegin.push_back((long long)wdet.size());
-            p->chunks.max_count = std::max(p->chunks.max_count, count);
-        }
-        p->chunks.n = (int)cbegin.size();
-        StructureChunks& c = p->chunks;
-        if ((st = upload(ctx, c.begin, cbegin.data(), sizeof(int) * std::max<size_t>(1, cbegin.size()))) != VB_OK)
+        off[nseg] = (long long)coef.size();
+        if ((st = upload(ctx, b.off, off.data(), sizeof(long long) * off.size())) != VB_OK) return fail(st);
+        if ((st = upload(ctx, b.meta, meta.data(), std::max<size_t>(16, meta.size()))) != VB_OK) return fail(st);
+        if ((st = upload(ctx, b.coef, coef.data(), sizeof(double) * std::max<size_t>(1, coef.size()))) != VB_OK)
             return fail(st);
-        if ((st = upload(ctx, c.count, ccount.data(), sizeof(int) * std::max<size_t>(1, ccount.size()))) != VB_OK)
-            return fail(st);
-        if ((st = upload(ctx, c.wbegin, wbegin.data(), sizeof(long long) * std::max<size_t>(1, wbegin.size()))) != VB_OK)
-            return fail(st);
-        if ((st = upload(ctx, c.wdet, wdet.data(), sizeof(int) * std::max<size_t>(1, wdet.size()))) != VB_OK)
-            return fail(st);
-        if ((st = upload(ctx, c.wstruct, wstruct.data(), sizeof(int) * std::max<size_t>(1, wstruct.size()))) != VB_OK)
-            return fail(st);
-        if ((st = upload(ctx, c.wcoef, wcoef.data(), sizeof(double) * std::max<size_t>(1, wcoef.size()))) != VB_OK)
-            return fail(st);
+        if ((st = upload(ctx, b.row, row.data(), std::max<size_t>(16, row.size()))) != VB_OK) return fail(st);
     }
     cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
     if (e2 != cudaSuccess) return fail(cuda_error(ctx, e2, "plan upload"));
@@ -523,7 +529,7 @@ vb_status execute_impl(vb_hs_plan* p, const double* S, const double* h, const do
     // execute scratch of the context: bands [n_det x width] and Z [n_det x n_str] (H, S), W [n_str^2] (H, S)
     double* scr[6];
     {
-        const size_t band = sizeof(double) * (size_t)p->n_det * p->band_width;
+        const size_t band = sizeof(double) * (size_t)p->n_det * p->band_ld;
         const size_t zb = sizeof(double) * (size_t)p->n_str * p->n_det;
         const size_t wb = sizeof(double) * (size_t)p->n_str * p->n_str;
         const size_t sizes[6] = {band, band, zb, zb, wb, wb};
@@ -540,6 +546,7 @@ vb_status execute_impl(vb_hs_plan* p, const double* S, const double* h, const do
         fa.e0 = e0;
         fa.e1 = e1;
         fa.n_items = e0 * B + B * (B + 1) / 2;
+        fa.ldb = p->band_ld;
         fa.Hb = scr[0];
         fa.Sb = scr[1];
         PhaseMark pairs(p, VB_PHASE_DETERMINANT_PAIRS);
@@ -555,14 +562,16 @@ vb_status execute_impl(vb_hs_plan* p, const double* S, const double* h, const do
             ba.width = B;
             ba.Hb = fa.Hb;
             ba.Sb = fa.Sb;
-            ba.n_chunks = p->chunks.n;
-            ba.max_count = p->chunks.max_count;
-            ba.chunk_begin = p->chunks.begin.as<int>();
-            ba.chunk_count = p->chunks.count.as<int>();
-            ba.wbegin = p->chunks.wbegin.as<long long>();
-            ba.wdet = p->chunks.wdet.as<int>();
-            ba.wstruct = p->chunks.wstruct.as<int>();
-            ba.wcoef = p->chunks.wcoef.as<double>();
+            ba.ldb = p->band_ld;
+            ba.n_groups = p->segments.n_groups;
+            ba.n_tiles = p->segments.n_tiles;
+            ba.seg_max = p->segments.seg_max;
+            ba.seg_off = p->segments.off.as<long long>();
+            ba.seg_meta = p->segments.meta.as<unsigned char>();
+            ba.term_c = p->segments.coef.as<double>();
+            ba.term_d = p->segments.row.as<unsigned char>();
+            ba.error = reinterpret_cast<int*>(p->counters.as<unsigned long long>() + 7);
+            ba.spin_limit = ctx->barrier_spin_limit > 0 ? ctx->barrier_spin_limit : (1ll << 26);
             ba.Zh = scr[2];
             ba.Zs = scr[3];
             err = launch_band_reduce(ba, s, &launches);
@@ -590,13 +599,29 @@ vb_status execute_impl(vb_hs_plan* p, const double* S, const double* h, const do
         const size_t wbytes = sizeof(double) * (size_t)p->n_str * p->n_str;
         err = cudaMemcpyAsync(H_out, Hdst, wbytes, cudaMemcpyDeviceToHost, s);
         if (err == cudaSuccess) err = cudaMemcpyAsync(S_out, Sdst, wbytes, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(p->meta_host + 2, p->counters.as<unsigned long long>() + 7, sizeof(int),
+                                  cudaMemcpyDeviceToHost, s);
         if (err == cudaSuccess) err = cudaStreamSynchronize(s);
         if (err != cudaSuccess) return cuda_error(ctx, err, "result download");
+        if (p->meta_host[2]) return set_error(ctx, VB_ERR_TIMEOUT, "band_reduce: a tile wait timed out");
     }
     p->stats.spin_pairs = p->npairs_a + p->npairs_b;
     p->stats.determinant_pairs = p->det_pair_evaluations;
     p->stats.kernel_launches = launches;
+    p->stats.factor_columns = p->R;
     p->evaluated = true;
+    return VB_OK;
+}
+
+// Reads the band reduction's timeout flag of the last execute (synchronizes the stream).
+vb_status band_status(vb_hs_plan* p) {
+    cudaStream_t s = p->ctx->stream;
+    cudaError_t err = cudaMemcpyAsync(p->meta_host + 2, p->counters.as<unsigned long long>() + 7, sizeof(int),
+                                      cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_error(p->ctx, err, "band status");
+    if (p->meta_host[2]) return set_error(p->ctx, VB_ERR_TIMEOUT, "band_reduce: a tile wait timed out");
     return VB_OK;
 }
 
@@ -619,6 +644,7 @@ vb_status vb_hs_plan_root_gradient(vb_hs_plan* p, const double* S, const double*
     if (!S || !h || !eri || !energy)
         return set_error(ctx, VB_ERR_INVALID, "vb_hs_plan_root_gradient: null pointer");
     vb_status st = execute_impl(p, S, h, eri, VB_MEM_HOST, nullptr, nullptr);
+    if (st == VB_OK) st = band_status(p);
     if (st != VB_OK) return st;
     const int ns = p->n_str;
     std::vector<double> c(ns);
@@ -683,10 +709,11 @@ vb_status vb_hs_plan_stats(const vb_hs_plan* p, vb_hs_stats* stats) {
     if (!p || !stats) return VB_ERR_INVALID;
     vb_hs_stats s = p->stats;
     if (p->evaluated) {
-        unsigned long long c[4] = {0, 0, 0, 0};
+        unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         cudaError_t err = cudaMemcpyAsync(c, p->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, p->ctx->stream);
         if (err == cudaSuccess) err = cudaStreamSynchronize(p->ctx->stream);
         if (err != cudaSuccess) return cuda_error(p->ctx, err, "stats download");
+        if ((int)c[7]) return set_error(p->ctx, VB_ERR_TIMEOUT, "band_reduce: a tile wait timed out");
         auto all_exact = [&](int k) { return !frame_spin_supported(p->n, k, p->R); };
         const bool all_a = p->ka > 0 && all_exact(p->ka);
         const bool all_b = p->kb > 0 && !p->shared_tables && all_exact(p->kb);

@@ -59,29 +59,36 @@ struct FullPairArgs {
     int R, r_pos;         // factor columns, positive-sign columns
     long long e0, e1;     // band columns [e0, e1)
     long long n_items;    // determinant pairs (d <= e) in the band
-    double* Hb;           // band, row-major: Hb[d * (e1 - e0) + (e - e0)], valid for d <= e
+    long long ldb;        // band row stride (elements, even: rows start on 16-byte boundaries)
+    double* Hb;           // band, row-major: Hb[d * ldb + (e - e0)], valid for d <= e
     double* Sb;
     const int* flip;      // spin-flip permutation of determinants (nullptr: no folding)
 };
 
+// Band reduction Z = T^T U' (structure-major weights T, band U' upper triangle).  Rows of the
+// band are streamed in tiles of kBandTileRows; for every (structure group g, row tile t) the plan
+// holds one segment of (row-in-tile, coefficient) terms ordered by (warp, slot, determinant):
+// seg_off[g T + t] (a multiple of 16) indexes term_c / term_d, and seg_meta holds 144 bytes per
+// segment: the term count of each (warp, slot) (kBandWarps x kBandSlots bytes) followed by the
+// start of each warp's terms within the segment (kBandWarps uint16).  Structure of group g, warp
+// w, slot s: I = g * kBandGroup + s * kBandWarps + w.
 struct BandReduceArgs {
     long long n_det;
     int n_str;
-    long long e0, width;      // band columns
+    long long e0, width;      // band columns [e0, e0 + width)
+    long long ldb;            // band row stride (elements, even)
     const double* Hb;
     const double* Sb;
-    // structure chunks (grid.y): chunk c covers structures [chunk_begin[c], + chunk_count[c]);
-    // its warp w owns the triples [wbegin[c (W + 1) + w], wbegin[c (W + 1) + w + 1]) of the
-    // concatenated lists, sorted by determinant: (determinant, local structure, coefficient)
-    int n_chunks, max_count;
-    const int* chunk_begin;
-    const int* chunk_count;
-    const long long* wbegin;
-    const int* wdet;
-    const int* wstruct;
-    const double* wcoef;
+    int n_groups, n_tiles;
+    int seg_max;              // longest segment (terms, a multiple of 16)
+    const long long* seg_off;
+    const unsigned char* seg_meta;
+    const double* term_c;
+    const unsigned char* term_d;
     double* Zh;  // n_str x n_det column-major: Z[e * n_str + I]
     double* Zs;
+    int* error;  // set to 1 when a tile wait gives up (the results are then incomplete)
+    long long spin_limit;
 };
 
 struct StructureReduceArgs {
@@ -104,8 +111,12 @@ struct StructureReduceArgs {
 // so these blocks are full rank under the reference semantics.  Others take the exact path.
 constexpr double kCertificate2 = 1.0e16;
 
-constexpr int kBandReduceWarps = 8;
-constexpr int kBandReduceColumns = 32;
+constexpr int kBandWarps = 8;        // warps per band-reduction CTA
+constexpr int kBandSlots = 8;        // structures per warp (register accumulators)
+constexpr int kBandGroup = kBandWarps * kBandSlots;
+constexpr int kBandColumns = 32;     // band columns per CTA (one per lane)
+constexpr int kBandTileRows = 64;    // band rows per staged tile
+constexpr int kBandMetaBytes = kBandWarps * kBandSlots + 2 * kBandWarps;
 constexpr int kSpinBlock = 128;    // right strings per fast-kernel item (threads per CTA)
 
 // Per-thread stack frames of the exact-path kernels instantiated for k <= 8 (reserved when a
@@ -158,7 +169,7 @@ cudaError_t launch_factor_project(int np, int R, const double* lf, int ld, const
                                   long long cnt, double* C, long long ldC, cudaStream_t stream);
 cudaError_t launch_factor_outer(int np, int R, const double* Y, long long ldY, const double* Z, long long ldZ,
                                 long long cnt, double* G, long long ldG, double* partial, cudaStream_t stream);
-size_t band_reduce_smem_bytes(int struct_count);
-int band_reduce_max_structures();
+// Dynamic shared memory of the band reduction for segments of at most seg_max terms.
+size_t band_reduce_smem_bytes(int seg_max);
 
 }  // namespace vbcore

@@ -32,7 +32,10 @@ namespace vbcore {
 namespace {
 
 constexpr double kThreshold = 1.0e-12;
-constexpr double kFactorTolerance = 1.0e-15;  // relative pivot cut of the pair-kernel factorization
+// Relative pivot cut of the pair-kernel factorization.  Once the numerical rank is exhausted the
+// Schur complement holds rounding noise of about (steps) * eps * max|K_pp|, so a cut of 8 np eps
+// (at least 1e-15) ends the factorization there instead of emitting columns of noise.
+double factor_tolerance(int np) { return fmax(1.0e-15, 8.0 * np * 2.220446049250313e-16); }
 constexpr int kSms = 148;
 
 __device__ __forceinline__ int occ_byte(const uint64_t* row, int i) {
@@ -69,38 +72,42 @@ __global__ void prepare_tables_kernel(int n, const double* __restrict__ eri, dou
     }
 }
 
-// Pivoted LDL^T of the unpacked pair kernel with diagonal (complete) pivoting, one CTA.
+// Pivoted LDL^T of the unpacked pair kernel with diagonal (complete) pivoting, one CTA, in the
+// left-looking form: step m picks the largest remaining |diagonal| p, forms the Schur-complement
+// column K[:, p] - sum_{m' < m} sigma_m' l_m'[p] l_m' (one dot product of length m per row) and
+// updates the diagonal, so each step costs two barriers and O(np m) work.
 // Stops when the largest remaining |diagonal| falls to rel_tol times the largest initial one;
 // the dropped remainder then perturbs any opposite-spin energy by at most
 // rel_tol * max|K_pp| * ||p_a||_1 ||p_b||_1.  Columns are emitted positive-sign first.
-// The working matrix lives in shared memory when it fits (in_smem), else in `work`; the current
-// column is always in shared memory.  Two barriers per step: the warp that updates a row also
-// reports the row's new diagonal, so the next pivot search is a reduction over per-warp maxima.
-__global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* __restrict__ kfull,
-                                                          double* __restrict__ work_g, double* __restrict__ cols,
-                                                          int* __restrict__ signs, double* __restrict__ lf, int ld,
-                                                          int* __restrict__ meta, double rel_tol, int in_smem) {
+// The factor columns l_m live in shared memory when np^2 doubles fit (in_smem), else in `cols`
+// (row i of column m at cols[m np + i]); `work_g` is not used.
+__global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double* __restrict__ kfull,
+                                                           double* __restrict__ work_g, double* __restrict__ cols,
+                                                           int* __restrict__ signs, double* __restrict__ lf, int ld,
+                                                           int* __restrict__ meta, double rel_tol, int in_smem) {
+    (void)work_g;
     extern __shared__ double fsm[];
-    double* work = in_smem ? fsm : work_g;
-    double* lc = in_smem ? fsm + (size_t)np * np : fsm;  // current column
-    int* used = reinterpret_cast<int*>(lc + np);
-    int* slot_col = used + np;  // emission map: output slot -> column
-    __shared__ double red_v[32];
-    __shared__ int red_i[32];
+    double* diag = fsm;                                      // np
+    double* sig = diag + np;                                 // np signs as doubles
+    int* used = reinterpret_cast<int*>(sig + np);            // np
+    int* slot_col = used + np;                               // np (emission map)
+    double* L = in_smem ? reinterpret_cast<double*>(slot_col + np) : cols;
+    __shared__ int pivot, stop;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int warp = tid >> 5, lane = tid & 31, nwarps = nt >> 5;
-    const long long n2 = (long long)np * np;
-    for (long long i = tid; i < n2; i += nt) work[i] = kfull[i];
-    for (int i = tid; i < np; i += nt) used[i] = 0;
+    const int lane = tid & 31;
+    for (int i = tid; i < np; i += nt) {
+        diag[i] = __ldg(kfull + (long long)i * np + i);
+        used[i] = 0;
+    }
     __syncthreads();
-    // per-warp (max |diagonal|, row) over the warp's rows i = warp, warp + nwarps, ...
-    auto warp_best = [&](int exclude) {
+    // largest |diagonal| among the unused rows (smallest index on ties), by warp 0
+    auto argmax = [&](double* best_out) {
         double best = -1.0;
         int bi = -1;
-        for (int i = warp + nwarps * lane; i < np; i += nwarps * 32)
-            if (!used[i] && i != exclude) {
-                const double v = fabs(work[(long long)i * np + i]);
-                if (v > best || (v == best && i < bi)) {
+        for (int i = lane; i < np; i += 32)
+            if (!used[i]) {
+                const double v = fabs(diag[i]);
+                if (v > best) {
                     best = v;
                     bi = i;
                 }
@@ -113,74 +120,68 @@ __global__ void __launch_bounds__(512) factor_pair_kernel(int np, const double* 
                 bi = oi;
             }
         }
-        if (lane == 0) {
-            red_v[warp] = best;
-            red_i[warp] = bi;
-        }
+        *best_out = best;
+        return bi;
     };
-    auto block_best = [&](double* v_out, int* i_out) {
-        double v = -1.0;
-        int vi = -1;
-        for (int w = 0; w < nwarps; ++w) {
-            const double ov = red_v[w];
-            const int oi = red_i[w];
-            if (ov > v || (ov == v && oi >= 0 && (vi < 0 || oi < vi))) {
-                v = ov;
-                vi = oi;
-            }
-        }
-        *v_out = v;
-        *i_out = vi;
-    };
-    warp_best(-1);
-    __syncthreads();
-    double dmax = 0.0;
-    int p0 = -1;
-    block_best(&dmax, &p0);
-    const double cut = rel_tol * fmax(dmax, 0.0);
+    double cut = 0.0;
+    if (tid < 32) {
+        double dmax;
+        argmax(&dmax);
+        cut = rel_tol * fmax(dmax, 0.0);
+    }
     int m = 0;
     for (; m < np; ++m) {
-        double best;
-        int p;
-        block_best(&best, &p);
-        const double piv = p >= 0 ? work[(long long)p * np + p] : 0.0;
-        if (p < 0 || !(fabs(piv) > cut) || fabs(piv) == 0.0) break;
+        if (tid < 32) {
+            double best;
+            const int p = argmax(&best);
+            if (lane == 0) {
+                pivot = p;
+                stop = (p < 0 || !(fabs(diag[p]) > cut) || diag[p] == 0.0) ? 1 : 0;
+            }
+        }
+        __syncthreads();
+        if (stop) break;
+        const int p = pivot;
+        const double piv = diag[p];
         const double inv = 1.0 / sqrt(fabs(piv));
-        const int sgn = piv > 0.0 ? 1 : -1;
-        double* l = cols + (long long)m * np;
+        const double sgn = piv > 0.0 ? 1.0 : -1.0;
+        double* lm = L + (long long)m * np;
         for (int i = tid; i < np; i += nt) {
-            const double v = used[i] ? 0.0 : work[(long long)i * np + p] * inv;
-            lc[i] = v;
-            l[i] = v;
+            double v = 0.0;
+            if (!used[i]) {
+                double acc0 = __ldg(kfull + (long long)p * np + i), acc1 = 0.0;
+                int q = 0;
+                for (; q + 1 < m; q += 2) {
+                    const double* l0 = L + (long long)q * np;
+                    acc0 = fma(-sig[q] * l0[p], l0[i], acc0);
+                    acc1 = fma(-sig[q + 1] * l0[np + p], l0[np + i], acc1);
+                }
+                if (q < m) acc0 = fma(-sig[q] * L[(long long)q * np + p], L[(long long)q * np + i], acc0);
+                v = (acc0 + acc1) * inv;
+                if (i != p) diag[i] = fma(-sgn * v, v, diag[i]);
+            }
+            lm[i] = v;
         }
-        if (tid == 0) signs[m] = sgn;
-        __syncthreads();  // the column is complete; every thread has read red_v / red_i
-        // rank-1 update of the remaining block (pivot row and column excluded), one warp per row;
-        // the updated diagonals feed the next pivot search
-        for (int i = warp; i < np; i += nwarps) {
-            if (used[i] || i == p) continue;
-            const double li = (double)sgn * lc[i];
-            double* row = work + (long long)i * np;
-            for (int j = lane; j < np; j += 32)
-                if (!used[j] && j != p) row[j] = fma(-li, lc[j], row[j]);
+        if (tid == 0) {
+            sig[m] = sgn;
+            signs[m] = (int)sgn;
+            used[p] = 1;
         }
-        __syncwarp();
-        if (tid == 0) used[p] = 1;
-        warp_best(p);
         __syncthreads();
     }
     if (tid == 0) {
         int pos = 0;
-        for (int c = 0; c < m; ++c) pos += signs[c] > 0 ? 1 : 0;
+        for (int c = 0; c < m; ++c) pos += sig[c] > 0.0 ? 1 : 0;
         int ip = 0, in = pos;
-        for (int c = 0; c < m; ++c) slot_col[signs[c] > 0 ? ip++ : in++] = c;
+        for (int c = 0; c < m; ++c) slot_col[sig[c] > 0.0 ? ip++ : in++] = c;
         meta[0] = pos;
         meta[1] = m - pos;
     }
     __syncthreads();
+    const int warp = tid >> 5, nwarps = nt >> 5;
     for (int q = warp; q < np; q += nwarps)
         for (int slot = lane; slot < ld; slot += 32)
-            lf[(long long)q * ld + slot] = slot < m ? cols[(long long)slot_col[slot] * np + q] : 0.0;
+            lf[(long long)q * ld + slot] = slot < m ? L[(long long)slot_col[slot] * np + q] : 0.0;
 }
 
 // Listed blocks (or all blocks): one thread per block resolves it by the exact path; its first
@@ -206,10 +207,14 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
     const long long N = a.n_strings;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long base = warp * 32; base < count; base += nwarps * 32) {
+    // blocks per warp: 32 (one per lane) when there are enough, fewer so that a short list
+    // spreads over as many warps as it has blocks
+    long long chunk = (count + nwarps - 1) / nwarps;
+    chunk = chunk < 1 ? 1 : (chunk > 32 ? 32 : chunk);
+    for (long long base = warp * chunk; base < count; base += nwarps * chunk) {
         const long long idx = base + lane;
         long long u = 0, v = 0;
-        const bool valid = idx < count;
+        const bool valid = lane < chunk && idx < count;
         double det = 0.0, h1 = 0.0, h2 = 0.0;
         int nullity = 3;
         bool regular = false;  // two-electron sum done by the warp
@@ -288,7 +293,7 @@ __global__ void __launch_bounds__(64) spin_pairs_exact(SpinTableArgs a) {
                 for (int i = 0; i < kk; ++i) cof[i] = 0.0;
         }
         __syncwarp();
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < chunk; ++j) {
             const long long jdx = base + j;
             if (jdx >= count) break;
             const long long uj = __shfl_sync(0xffffffffu, u, j), vj = __shfl_sync(0xffffffffu, v, j);
@@ -418,7 +423,6 @@ __device__ __forceinline__ double pair_weight(const int* flip, long long d, long
 }
 
 __global__ void __launch_bounds__(512) full_pairs_kernel(FullPairArgs a) {
-    const long long B = a.e1 - a.e0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < a.n_items; t += stride) {
         long long d, e;
@@ -430,9 +434,70 @@ __global__ void __launch_bounds__(512) full_pairs_kernel(FullPairArgs a) {
             H *= w;
             S *= w;
         }
-        const long long o = d * B + (e - a.e0);
+        const long long o = d * a.ldb + (e - a.e0);
         a.Hb[o] = H;
         a.Sb[o] = S;
+    }
+}
+
+// Same band, G lanes per determinant pair: the group reads the pair's two records as contiguous
+// 16-byte slices (G x 16 bytes per load), so every fetched sector is used, then reduces the
+// opposite-spin dot product across the group.  Records start on 16-byte boundaries (even stride).
+template <int G>
+__global__ void __launch_bounds__(256) full_pairs_group_kernel(FullPairArgs a) {
+    const int lane = threadIdx.x & 31, sub = lane & (G - 1);
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int R = a.R, r_pos = a.r_pos;
+    for (long long t0 = warp * (32 / G); t0 < a.n_items; t0 += nwarps * (32 / G)) {
+        const long long t = t0 + lane / G;
+        const bool valid = t < a.n_items;
+        long long d = 0, e = 0;
+        double w = 0.0;
+        if (valid) {
+            band_decode(t, a.e0, a.e1, &d, &e);
+            w = pair_weight(a.flip, d, e);
+        }
+        const double* ra = nullptr;
+        const double* rb = nullptr;
+        double sa = 1.0, hsa = 0.0, sb = 1.0, hsb = 0.0, dot = 0.0;
+        if (w != 0.0) {
+            if (a.ka > 0) {
+                const int ia = __ldg(a.det_alpha + d), ja = __ldg(a.det_alpha + e);
+                ra = a.rec_a + record_index(min(ia, ja), max(ia, ja), a.Na) * a.stride_a;
+                sa = ra[R];
+                hsa = ra[R + 1];
+            }
+            if (a.kb > 0) {
+                const int ib = __ldg(a.det_beta + d), jb = __ldg(a.det_beta + e);
+                rb = a.rec_b + record_index(min(ib, jb), max(ib, jb), a.Nb) * a.stride_b;
+                sb = rb[R];
+                hsb = rb[R + 1];
+            }
+            if (ra && rb) {
+                int m = 2 * sub;
+#pragma unroll 4
+                for (; m + 1 < R; m += 2 * G) {
+                    const double2 x = *reinterpret_cast<const double2*>(ra + m);
+                    const double2 y = *reinterpret_cast<const double2*>(rb + m);
+                    dot = fma(m < r_pos ? x.x : -x.x, y.x, dot);
+                    dot = fma(m + 1 < r_pos ? x.y : -x.y, y.y, dot);
+                }
+                if (m == R - 1) dot = fma(m < r_pos ? ra[m] : -ra[m], rb[m], dot);
+            }
+        }
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+        if (valid && sub == 0) {
+            double H = 0.0, S = 0.0;
+            if (w != 0.0) {
+                H = w * fma(hsa, sb, fma(hsb, sa, dot));
+                S = w * (sa * sb);
+            }
+            const long long o = d * a.ldb + (e - a.e0);
+            a.Hb[o] = H;
+            a.Sb[o] = S;
+        }
     }
 }
 
@@ -496,13 +561,16 @@ __global__ void same_spin_list_kernel(int n, int k, long long batch, const int* 
 
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs, double* lf,
                                       int ld, int* meta, cudaStream_t stream) {
-    const size_t aux_bytes = sizeof(double) * (size_t)np + sizeof(int) * 2 * (size_t)np;
-    const size_t in_smem_bytes = sizeof(double) * (size_t)np * np + aux_bytes;
-    const int in_smem = in_smem_bytes <= 200 * 1024 ? 1 : 0;
+    const size_t aux_bytes = sizeof(double) * 2 * (size_t)np + sizeof(int) * 2 * ((size_t)np + 1);
+    const size_t in_smem_bytes = aux_bytes + sizeof(double) * (size_t)np * np;
+    const int in_smem = in_smem_bytes <= 160 * 1024 ? 1 : 0;
     const size_t smem = in_smem ? in_smem_bytes : aux_bytes;
     cudaError_t err = allow_dynamic_smem((const void*)factor_pair_kernel, (int)smem);
     if (err != cudaSuccess) return err;
-    factor_pair_kernel<<<1, 512, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, kFactorTolerance, in_smem);
+    int threads = (np + 31) / 32 * 32;
+    threads = threads < 64 ? 64 : (threads > 1024 ? 1024 : threads);
+    factor_pair_kernel<<<1, threads, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, factor_tolerance(np),
+                                                     in_smem);
     return cudaGetLastError();
 }
 
@@ -588,18 +656,25 @@ cudaError_t launch_spin_pairs_exact(const SpinTableArgs& a, cudaStream_t stream,
 cudaError_t launch_full_pairs(const FullPairArgs& a, cudaStream_t stream, int* launches) {
     if (a.n_items <= 0) return cudaSuccess;
     // launch variants (block size, CTAs per SM), chosen by the autotuner per band shape
-    constexpr int kVariants = 4;
-    constexpr int threads[kVariants] = {256, 128, 256, 512};
-    constexpr int per_sm[kVariants] = {16, 16, 8, 4};
+    // (variants 0-3: one thread per pair; 4-5: groups of 4 and 8 lanes per pair)
+    constexpr int kVariants = 6;
+    constexpr int threads[kVariants] = {256, 128, 256, 512, 256, 256};
+    constexpr int per_sm[kVariants] = {16, 16, 8, 4, 8, 8};
+    constexpr int group[kVariants] = {1, 1, 1, 1, 4, 8};
     const std::string key = "full_pairs_kernel R=" + std::to_string(a.R) + " ndet=" + std::to_string(a.n_det) +
                             " items=" + std::to_string(a.n_items) + " flip=" + std::to_string(a.flip ? 1 : 0);
     cudaError_t err = cudaSuccess;
     autotune_run(
         key, kVariants, stream,
         [&](int v) {
-            long long blocks = (a.n_items + threads[v] - 1) / threads[v];
+            long long blocks = (a.n_items * group[v] + threads[v] - 1) / threads[v];
             if (blocks > (long long)kSms * per_sm[v]) blocks = (long long)kSms * per_sm[v];
-            full_pairs_kernel<<<(unsigned)blocks, threads[v], 0, stream>>>(a);
+            if (group[v] == 4)
+                full_pairs_group_kernel<4><<<(unsigned)blocks, threads[v], 0, stream>>>(a);
+            else if (group[v] == 8)
+                full_pairs_group_kernel<8><<<(unsigned)blocks, threads[v], 0, stream>>>(a);
+            else
+                full_pairs_kernel<<<(unsigned)blocks, threads[v], 0, stream>>>(a);
             return cudaGetLastError();
         },
         {}, &err);

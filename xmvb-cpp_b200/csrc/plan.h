@@ -11,10 +11,10 @@
 
 using namespace vbcore;
 
-// Structure chunks of the band reduction, all in one launch (see BandReduceArgs).
-struct StructureChunks {
-    int n = 0, max_count = 0;
-    DeviceBuffer begin, count, wbegin, wdet, wstruct, wcoef;
+// Term segments of the band reduction per (structure group, row tile) (see BandReduceArgs).
+struct BandSegments {
+    int n_groups = 0, n_tiles = 0, seg_max = 0;
+    DeviceBuffer off, meta, coef, row;
 };
 
 struct vb_hs_plan {
@@ -29,7 +29,8 @@ struct vb_hs_plan {
     int stride_a = 0, stride_b = 0;
     long long npairs_a = 0, npairs_b = 0;
     // counters: [0, 1] listed (exact-path) spin pairs alpha/beta, [2, 3] the gradient's listed
-    // pairs, [4, 5] the frame kernel's task counters alpha/beta
+    // pairs, [4, 5] the frame kernel's task counters alpha/beta, [7] the band reduction's
+    // timeout flag
     DeviceBuffer counters, list_a, list_b;
     // right strings of each left string bucketed by hole set (see SpinTableArgs::rlist)
     DeviceBuffer rlist_a, rlist_b, rdesc_a, rdesc_b, ebound_a, ebound_b;
@@ -40,6 +41,7 @@ struct vb_hs_plan {
     int* meta_host = nullptr;
     int R = 0, r_pos = 0;
     long long band_width = 0;  // determinant columns per band (bands live in the context scratch)
+    long long band_ld = 0;     // band row stride (band_width rounded up to 32 elements)
     DeviceBuffer Hout, Sout;
     DeviceBuffer str_off, str_det, str_coef;
     // structure incidence by determinant (CSR) and the gradient's adjoint scratch
@@ -48,7 +50,7 @@ struct vb_hs_plan {
     // host inputs of the last host-pointer evaluation whose records are still resident
     std::vector<double> last_inputs;
     bool records_current = false;
-    StructureChunks chunks;
+    BandSegments segments;
     // spin-flip map of the determinant list (folds the determinant-pair work in half)
     DeviceBuffer flip;
     // determinants by alpha string (CSR: alpha_off[i] .. alpha_off[i + 1] index alpha_dets)

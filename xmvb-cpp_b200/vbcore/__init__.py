@@ -86,7 +86,8 @@ class _ScfResult(ctypes.Structure):
 
 class _HsStats(ctypes.Structure):
     _fields_ = [("spin_pairs", ctypes.c_int64), ("careful_spin_pairs", ctypes.c_int64),
-                ("determinant_pairs", ctypes.c_int64), ("kernel_launches", ctypes.c_int64)]
+                ("determinant_pairs", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+                ("factor_columns", ctypes.c_int64)]
 
 
 # every symbol include/vbcore.h declares
@@ -886,7 +887,8 @@ class HsPlan:
         st = _HsStats()
         _check(load_library().vb_hs_plan_stats(self._h, ctypes.byref(st)), self.ctx.handle)
         return dict(spin_pairs=st.spin_pairs, careful_spin_pairs=st.careful_spin_pairs,
-                    determinant_pairs=st.determinant_pairs, kernel_launches=st.kernel_launches)
+                    determinant_pairs=st.determinant_pairs, kernel_launches=st.kernel_launches,
+                    factor_columns=st.factor_columns)
 
     def enable_phase_timing(self, enable: bool = True):
         _check(load_library().vb_hs_plan_enable_phase_timing(self._h, int(enable)), self.ctx.handle)
