@@ -212,20 +212,53 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
     }
 }
 
-// W[I, J] = sum_{(e, c) in J} c Z[I, e]; one CTA per J, threads over I.
-__global__ void structure_reduce_kernel(StructureReduceArgs a) {
+// W[I, J] = sum_{(e, c) in J} c Z[I, e]; one CTA per J, threads over I.  The terms of J are
+// staged in shared memory 256 at a time, and each thread keeps eight Z loads in flight.
+constexpr int kReduceTerms = 256;
+
+__global__ void __launch_bounds__(512) structure_reduce_kernel(StructureReduceArgs a) {
+    __shared__ long long se[kReduceTerms];
+    __shared__ double sc[kReduceTerms];
     const int J = blockIdx.x;
     const long long t0 = a.str_off[J], t1 = a.str_off[J + 1];
-    for (int I = threadIdx.x; I < a.n_str; I += blockDim.x) {
-        double wh = 0.0, ws = 0.0;
-        for (long long t = t0; t < t1; ++t) {
-            const long long e = __ldg(a.str_det + t);
-            const double c = __ldg(a.str_coef + t);
-            wh = fma(c, __ldg(a.Zh + e * a.n_str + I), wh);
-            ws = fma(c, __ldg(a.Zs + e * a.n_str + I), ws);
+    for (int I0 = 0; I0 < a.n_str; I0 += blockDim.x) {
+        const int I = I0 + threadIdx.x;
+        const bool valid = I < a.n_str;
+        double wh0 = 0.0, wh1 = 0.0, ws0 = 0.0, ws1 = 0.0;
+        for (long long c0 = t0; c0 < t1; c0 += kReduceTerms) {
+            const int n = (int)(t1 - c0 < kReduceTerms ? t1 - c0 : kReduceTerms);
+            __syncthreads();
+            for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                se[q] = __ldg(a.str_det + c0 + q) * a.n_str;
+                sc[q] = __ldg(a.str_coef + c0 + q);
+            }
+            __syncthreads();
+            if (!valid) continue;
+            int q = 0;
+            for (; q + 8 <= n; q += 8) {
+                double zh[8], zs[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    zh[u] = __ldg(a.Zh + se[q + u] + I);
+                    zs[u] = __ldg(a.Zs + se[q + u] + I);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                    wh0 = fma(sc[q + u], zh[u], wh0);
+                    ws0 = fma(sc[q + u], zs[u], ws0);
+                    wh1 = fma(sc[q + u + 1], zh[u + 1], wh1);
+                    ws1 = fma(sc[q + u + 1], zs[u + 1], ws1);
+                }
+            }
+            for (; q < n; ++q) {
+                wh0 = fma(sc[q], __ldg(a.Zh + se[q] + I), wh0);
+                ws0 = fma(sc[q], __ldg(a.Zs + se[q] + I), ws0);
+            }
         }
-        a.Wh[(long long)J * a.n_str + I] = wh;
-        a.Ws[(long long)J * a.n_str + I] = ws;
+        if (valid) {
+            a.Wh[(long long)J * a.n_str + I] = wh0 + wh1;
+            a.Ws[(long long)J * a.n_str + I] = ws0 + ws1;
+        }
     }
 }
 
@@ -297,7 +330,9 @@ cudaError_t launch_band_reduce(const BandReduceArgs& a, cudaStream_t stream, int
 
 cudaError_t launch_structure_reduce(const StructureReduceArgs& a, double* H, double* S, cudaStream_t stream,
                                     int* launches) {
-    structure_reduce_kernel<<<a.n_str, 128, 0, stream>>>(a);
+    int threads = (a.n_str + 31) / 32 * 32;
+    threads = threads > 512 ? 512 : threads;
+    structure_reduce_kernel<<<a.n_str, threads, 0, stream>>>(a);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     const long long total = (long long)a.n_str * a.n_str;

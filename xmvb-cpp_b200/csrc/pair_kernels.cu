@@ -73,83 +73,104 @@ __global__ void prepare_tables_kernel(int n, const double* __restrict__ eri, dou
 }
 
 // Pivoted LDL^T of the unpacked pair kernel with diagonal (complete) pivoting, one CTA, in the
-// left-looking form: step m picks the largest remaining |diagonal| p, forms the Schur-complement
-// column K[:, p] - sum_{m' < m} sigma_m' l_m'[p] l_m' (one dot product of length m per row) and
-// updates the diagonal, so each step costs two barriers and O(np m) work.
+// left-looking form.  Thread t owns rows t, t + nt, ... (at most kFactorRows) and keeps their
+// diagonal in registers.  Step m: with the pivot p and its value known, every owned row forms its
+// entry of the Schur-complement column, K[i, p] - sum_{m' < m} sigma_m' l_m'[p] l_m'[i], scales it
+// into l_m[i] and updates its diagonal; each warp then reduces its rows' largest |diagonal| and
+// one barrier publishes the warp results, from which every thread picks the next pivot.
 // Stops when the largest remaining |diagonal| falls to rel_tol times the largest initial one;
 // the dropped remainder then perturbs any opposite-spin energy by at most
 // rel_tol * max|K_pp| * ||p_a||_1 ||p_b||_1.  Columns are emitted positive-sign first.
-// The factor columns l_m live in shared memory when np^2 doubles fit (in_smem), else in `cols`
-// (row i of column m at cols[m np + i]); `work_g` is not used.
+// K and the columns l_m (l_m[i] at [m np + i]) sit in shared memory when they fit (in_smem),
+// else K is read from `kfull` and the columns live in `cols`.  `work_g` is not used.
+constexpr int kFactorRows = 4;
+
 __global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double* __restrict__ kfull,
                                                            double* __restrict__ work_g, double* __restrict__ cols,
                                                            int* __restrict__ signs, double* __restrict__ lf, int ld,
                                                            int* __restrict__ meta, double rel_tol, int in_smem) {
     (void)work_g;
     extern __shared__ double fsm[];
-    double* diag = fsm;                                      // np
-    double* sig = diag + np;                                 // np signs as doubles
-    int* used = reinterpret_cast<int*>(sig + np);            // np
-    int* slot_col = used + np;                               // np (emission map)
-    double* L = in_smem ? reinterpret_cast<double*>(slot_col + np) : cols;
-    __shared__ int pivot, stop;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31;
-    for (int i = tid; i < np; i += nt) {
-        diag[i] = __ldg(kfull + (long long)i * np + i);
-        used[i] = 0;
+    double* sig = fsm;                                        // np
+    int* slot_col = reinterpret_cast<int*>(sig + np);         // np (+1 pad)
+    double* Ks = sig + np + (np + 2) / 2;                     // np^2 when in_smem
+    const double* K = in_smem ? Ks : kfull;
+    double* L = in_smem ? Ks + (size_t)np * np : cols;
+    __shared__ double red_v[2][32], red_d[2][32];
+    __shared__ int red_i[2][32];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    if (in_smem)
+        for (long long i = tid; i < (long long)np * np; i += nt) Ks[i] = __ldg(kfull + i);
+    double dg[kFactorRows];
+    bool used[kFactorRows];
+#pragma unroll
+    for (int r = 0; r < kFactorRows; ++r) {
+        const int i = tid + r * nt;
+        dg[r] = i < np ? __ldg(kfull + (long long)i * np + i) : 0.0;
+        used[r] = i >= np;
     }
-    __syncthreads();
-    // largest |diagonal| among the unused rows (smallest index on ties), by warp 0
-    auto argmax = [&](double* best_out) {
-        double best = -1.0;
+    // publishes this thread's best unused row to the warp slots of buffer b (largest |diagonal|,
+    // smallest index on ties)
+    auto publish = [&](int b) {
+        double best = -1.0, bd = 0.0;
         int bi = -1;
-        for (int i = lane; i < np; i += 32)
-            if (!used[i]) {
-                const double v = fabs(diag[i]);
-                if (v > best) {
-                    best = v;
-                    bi = i;
-                }
+#pragma unroll
+        for (int r = 0; r < kFactorRows; ++r)
+            if (!used[r] && fabs(dg[r]) > best) {
+                best = fabs(dg[r]);
+                bd = dg[r];
+                bi = tid + r * nt;
             }
         for (int o = 16; o > 0; o >>= 1) {
             const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            const double od = __shfl_xor_sync(0xffffffffu, bd, o);
             const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
             if (ov > best || (ov == best && oi >= 0 && (bi < 0 || oi < bi))) {
                 best = ov;
+                bd = od;
                 bi = oi;
             }
         }
-        *best_out = best;
-        return bi;
+        if (lane == 0) {
+            red_v[b][warp] = best;
+            red_d[b][warp] = bd;
+            red_i[b][warp] = bi;
+        }
     };
-    double cut = 0.0;
-    if (tid < 32) {
-        double dmax;
-        argmax(&dmax);
-        cut = rel_tol * fmax(dmax, 0.0);
-    }
-    int m = 0;
-    for (; m < np; ++m) {
-        if (tid < 32) {
-            double best;
-            const int p = argmax(&best);
-            if (lane == 0) {
-                pivot = p;
-                stop = (p < 0 || !(fabs(diag[p]) > cut) || diag[p] == 0.0) ? 1 : 0;
+    auto pick = [&](int b, int* p, double* piv) {
+        double best = -1.0, bd = 0.0;
+        int bi = -1;
+        for (int w = 0; w < nwarps; ++w) {
+            const double ov = red_v[b][w];
+            const int oi = red_i[b][w];
+            if (ov > best || (ov == best && oi >= 0 && (bi < 0 || oi < bi))) {
+                best = ov;
+                bd = red_d[b][w];
+                bi = oi;
             }
         }
-        __syncthreads();
-        if (stop) break;
-        const int p = pivot;
-        const double piv = diag[p];
+        *p = bi;
+        *piv = bd;
+    };
+    publish(0);
+    __syncthreads();
+    int p;
+    double piv;
+    pick(0, &p, &piv);
+    const double cut = rel_tol * fmax(fabs(piv), 0.0);
+    int m = 0;
+    for (; m < np; ++m) {
+        if (p < 0 || !(fabs(piv) > cut) || piv == 0.0) break;
         const double inv = 1.0 / sqrt(fabs(piv));
         const double sgn = piv > 0.0 ? 1.0 : -1.0;
         double* lm = L + (long long)m * np;
-        for (int i = tid; i < np; i += nt) {
+#pragma unroll
+        for (int r = 0; r < kFactorRows; ++r) {
+            const int i = tid + r * nt;
+            if (i >= np) continue;
             double v = 0.0;
-            if (!used[i]) {
-                double acc0 = __ldg(kfull + (long long)p * np + i), acc1 = 0.0;
+            if (!used[r]) {
+                double acc0 = K[(long long)p * np + i], acc1 = 0.0;
                 int q = 0;
                 for (; q + 1 < m; q += 2) {
                     const double* l0 = L + (long long)q * np;
@@ -158,16 +179,20 @@ __global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double*
                 }
                 if (q < m) acc0 = fma(-sig[q] * L[(long long)q * np + p], L[(long long)q * np + i], acc0);
                 v = (acc0 + acc1) * inv;
-                if (i != p) diag[i] = fma(-sgn * v, v, diag[i]);
+                if (i == p)
+                    used[r] = true;
+                else
+                    dg[r] = fma(-sgn * v, v, dg[r]);
             }
             lm[i] = v;
         }
         if (tid == 0) {
             sig[m] = sgn;
             signs[m] = (int)sgn;
-            used[p] = 1;
         }
+        publish((m + 1) & 1);
         __syncthreads();
+        pick((m + 1) & 1, &p, &piv);
     }
     if (tid == 0) {
         int pos = 0;
@@ -178,7 +203,6 @@ __global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double*
         meta[1] = m - pos;
     }
     __syncthreads();
-    const int warp = tid >> 5, nwarps = nt >> 5;
     for (int q = warp; q < np; q += nwarps)
         for (int slot = lane; slot < ld; slot += 32)
             lf[(long long)q * ld + slot] = slot < m ? L[(long long)slot_col[slot] * np + q] : 0.0;
@@ -561,14 +585,15 @@ __global__ void same_spin_list_kernel(int n, int k, long long batch, const int* 
 
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs, double* lf,
                                       int ld, int* meta, cudaStream_t stream) {
-    const size_t aux_bytes = sizeof(double) * 2 * (size_t)np + sizeof(int) * 2 * ((size_t)np + 1);
-    const size_t in_smem_bytes = aux_bytes + sizeof(double) * (size_t)np * np;
-    const int in_smem = in_smem_bytes <= 160 * 1024 ? 1 : 0;
+    int threads = (np + 31) / 32 * 32;
+    threads = threads < 64 ? 64 : (threads > 1024 ? 1024 : threads);
+    if (np > threads * kFactorRows) return cudaErrorInvalidValue;
+    const size_t aux_bytes = sizeof(double) * ((size_t)np + (np + 2) / 2);
+    const size_t in_smem_bytes = aux_bytes + 2 * sizeof(double) * (size_t)np * np;
+    const int in_smem = in_smem_bytes <= 200 * 1024 ? 1 : 0;
     const size_t smem = in_smem ? in_smem_bytes : aux_bytes;
     cudaError_t err = allow_dynamic_smem((const void*)factor_pair_kernel, (int)smem);
     if (err != cudaSuccess) return err;
-    int threads = (np + 31) / 32 * 32;
-    threads = threads < 64 ? 64 : (threads > 1024 ? 1024 : threads);
     factor_pair_kernel<<<1, threads, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, factor_tolerance(np),
                                                      in_smem);
     return cudaGetLastError();
