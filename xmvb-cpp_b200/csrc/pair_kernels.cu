@@ -85,10 +85,11 @@ __global__ void prepare_tables_kernel(int n, const double* __restrict__ eri, dou
 // else K is read from `kfull` and the columns live in `cols`.  `work_g` is not used.
 constexpr int kFactorRows = 4;
 
+template <bool in_smem>  // compile-time, so that the shared-memory path uses shared loads
 __global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double* __restrict__ kfull,
                                                            double* __restrict__ work_g, double* __restrict__ cols,
                                                            int* __restrict__ signs, double* __restrict__ lf, int ld,
-                                                           int* __restrict__ meta, double rel_tol, int in_smem) {
+                                                           int* __restrict__ meta, double rel_tol) {
     (void)work_g;
     extern __shared__ double fsm[];
     double* sig = fsm;                                        // np
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double*
     int m = 0;
     for (; m < np; ++m) {
         if (p < 0 || !(fabs(piv) > cut) || piv == 0.0) break;
-        const double inv = 1.0 / sqrt(fabs(piv));
+        const double inv = rsqrt(fabs(piv));
         const double sgn = piv > 0.0 ? 1.0 : -1.0;
         double* lm = L + (long long)m * np;
 #pragma unroll
@@ -170,15 +171,17 @@ __global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double*
             if (i >= np) continue;
             double v = 0.0;
             if (!used[r]) {
-                double acc0 = K[(long long)p * np + i], acc1 = 0.0;
+                double acc0 = K[(long long)p * np + i], acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
                 int q = 0;
-                for (; q + 1 < m; q += 2) {
+                for (; q + 3 < m; q += 4) {
                     const double* l0 = L + (long long)q * np;
                     acc0 = fma(-sig[q] * l0[p], l0[i], acc0);
                     acc1 = fma(-sig[q + 1] * l0[np + p], l0[np + i], acc1);
+                    acc2 = fma(-sig[q + 2] * l0[2 * np + p], l0[2 * np + i], acc2);
+                    acc3 = fma(-sig[q + 3] * l0[3 * np + p], l0[3 * np + i], acc3);
                 }
-                if (q < m) acc0 = fma(-sig[q] * L[(long long)q * np + p], L[(long long)q * np + i], acc0);
-                v = (acc0 + acc1) * inv;
+                for (; q < m; ++q) acc0 = fma(-sig[q] * L[(long long)q * np + p], L[(long long)q * np + i], acc0);
+                v = ((acc0 + acc1) + (acc2 + acc3)) * inv;
                 if (i == p)
                     used[r] = true;
                 else
@@ -592,10 +595,16 @@ cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work,
     const size_t in_smem_bytes = aux_bytes + 2 * sizeof(double) * (size_t)np * np;
     const int in_smem = in_smem_bytes <= 200 * 1024 ? 1 : 0;
     const size_t smem = in_smem ? in_smem_bytes : aux_bytes;
-    cudaError_t err = allow_dynamic_smem((const void*)factor_pair_kernel, (int)smem);
+    cudaError_t err = allow_dynamic_smem(in_smem ? (const void*)factor_pair_kernel<true>
+                                                 : (const void*)factor_pair_kernel<false>,
+                                         (int)smem);
     if (err != cudaSuccess) return err;
-    factor_pair_kernel<<<1, threads, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta, factor_tolerance(np),
-                                                     in_smem);
+    if (in_smem)
+        factor_pair_kernel<true><<<1, threads, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta,
+                                                               factor_tolerance(np));
+    else
+        factor_pair_kernel<false><<<1, threads, smem, stream>>>(np, kfull, work, cols, signs, lf, ld, meta,
+                                                                factor_tolerance(np));
     return cudaGetLastError();
 }
 
@@ -619,7 +628,8 @@ size_t exact_stack_bytes() {
 
 cudaError_t preload_spin_pair_kernels() {
     // cudaFuncGetAttributes loads a function that lazy module loading has not loaded yet
-    const void* fns[] = {(const void*)prepare_tables_kernel, (const void*)factor_pair_kernel,
+    const void* fns[] = {(const void*)prepare_tables_kernel, (const void*)factor_pair_kernel<true>,
+                         (const void*)factor_pair_kernel<false>,
                          (const void*)spin_pairs_exact<7, 7>, (const void*)spin_pairs_exact<8, 0>,
                          (const void*)spin_pairs_exact<dev::KMAX, 0>};
     for (const void* f : fns) {
