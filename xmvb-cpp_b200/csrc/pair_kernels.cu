@@ -467,67 +467,6 @@ __global__ void __launch_bounds__(512) full_pairs_kernel(FullPairArgs a) {
     }
 }
 
-// Same band, G lanes per determinant pair: the group reads the pair's two records as contiguous
-// 16-byte slices (G x 16 bytes per load), so every fetched sector is used, then reduces the
-// opposite-spin dot product across the group.  Records start on 16-byte boundaries (even stride).
-template <int G>
-__global__ void __launch_bounds__(256) full_pairs_group_kernel(FullPairArgs a) {
-    const int lane = threadIdx.x & 31, sub = lane & (G - 1);
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int R = a.R, r_pos = a.r_pos;
-    for (long long t0 = warp * (32 / G); t0 < a.n_items; t0 += nwarps * (32 / G)) {
-        const long long t = t0 + lane / G;
-        const bool valid = t < a.n_items;
-        long long d = 0, e = 0;
-        double w = 0.0;
-        if (valid) {
-            band_decode(t, a.e0, a.e1, &d, &e);
-            w = pair_weight(a.flip, d, e);
-        }
-        const double* ra = nullptr;
-        const double* rb = nullptr;
-        double sa = 1.0, hsa = 0.0, sb = 1.0, hsb = 0.0, dot = 0.0;
-        if (w != 0.0) {
-            if (a.ka > 0) {
-                const int ia = __ldg(a.det_alpha + d), ja = __ldg(a.det_alpha + e);
-                ra = a.rec_a + record_index(min(ia, ja), max(ia, ja), a.Na) * a.stride_a;
-                sa = ra[R];
-                hsa = ra[R + 1];
-            }
-            if (a.kb > 0) {
-                const int ib = __ldg(a.det_beta + d), jb = __ldg(a.det_beta + e);
-                rb = a.rec_b + record_index(min(ib, jb), max(ib, jb), a.Nb) * a.stride_b;
-                sb = rb[R];
-                hsb = rb[R + 1];
-            }
-            if (ra && rb) {
-                int m = 2 * sub;
-#pragma unroll 4
-                for (; m + 1 < R; m += 2 * G) {
-                    const double2 x = *reinterpret_cast<const double2*>(ra + m);
-                    const double2 y = *reinterpret_cast<const double2*>(rb + m);
-                    dot = fma(m < r_pos ? x.x : -x.x, y.x, dot);
-                    dot = fma(m + 1 < r_pos ? x.y : -x.y, y.y, dot);
-                }
-                if (m == R - 1) dot = fma(m < r_pos ? ra[m] : -ra[m], rb[m], dot);
-            }
-        }
-#pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-        if (valid && sub == 0) {
-            double H = 0.0, S = 0.0;
-            if (w != 0.0) {
-                H = w * fma(hsa, sb, fma(hsb, sa, dot));
-                S = w * (sa * sb);
-            }
-            const long long o = d * a.ldb + (e - a.e0);
-            a.Hb[o] = H;
-            a.Sb[o] = S;
-        }
-    }
-}
-
 // Listed determinant pairs (d, e) in any order.
 __global__ void listed_pairs_kernel(FullPairArgs a, long long n_pairs, const long long* __restrict__ pairs,
                                     double* __restrict__ h_out, double* __restrict__ s_out) {
@@ -691,25 +630,18 @@ cudaError_t launch_spin_pairs_exact(const SpinTableArgs& a, cudaStream_t stream,
 cudaError_t launch_full_pairs(const FullPairArgs& a, cudaStream_t stream, int* launches) {
     if (a.n_items <= 0) return cudaSuccess;
     // launch variants (block size, CTAs per SM), chosen by the autotuner per band shape
-    // (variants 0-3: one thread per pair; 4-5: groups of 4 and 8 lanes per pair)
-    constexpr int kVariants = 6;
-    constexpr int threads[kVariants] = {256, 128, 256, 512, 256, 256};
-    constexpr int per_sm[kVariants] = {16, 16, 8, 4, 8, 8};
-    constexpr int group[kVariants] = {1, 1, 1, 1, 4, 8};
+    constexpr int kVariants = 4;
+    constexpr int threads[kVariants] = {256, 128, 256, 512};
+    constexpr int per_sm[kVariants] = {16, 16, 8, 4};
     const std::string key = "full_pairs_kernel R=" + std::to_string(a.R) + " ndet=" + std::to_string(a.n_det) +
                             " items=" + std::to_string(a.n_items) + " flip=" + std::to_string(a.flip ? 1 : 0);
     cudaError_t err = cudaSuccess;
     autotune_run(
         key, kVariants, stream,
         [&](int v) {
-            long long blocks = (a.n_items * group[v] + threads[v] - 1) / threads[v];
+            long long blocks = (a.n_items + threads[v] - 1) / threads[v];
             if (blocks > (long long)kSms * per_sm[v]) blocks = (long long)kSms * per_sm[v];
-            if (group[v] == 4)
-                full_pairs_group_kernel<4><<<(unsigned)blocks, threads[v], 0, stream>>>(a);
-            else if (group[v] == 8)
-                full_pairs_group_kernel<8><<<(unsigned)blocks, threads[v], 0, stream>>>(a);
-            else
-                full_pairs_kernel<<<(unsigned)blocks, threads[v], 0, stream>>>(a);
+            full_pairs_kernel<<<(unsigned)blocks, threads[v], 0, stream>>>(a);
             return cudaGetLastError();
         },
         {}, &err);

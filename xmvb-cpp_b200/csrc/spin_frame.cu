@@ -203,39 +203,61 @@ __global__ void __launch_bounds__(kFrameThreads) sort_right_strings(int N, const
     }
 }
 
-constexpr int kTableThreads = 128;
-constexpr int kTableSources = 48;  // pair-kernel sources (h and factor columns) staged per pass
+constexpr int kTableThreads = 128;  // four warps
+constexpr int kTableWarps = kTableThreads / 32;
+constexpr int kTableSources = 20;   // pair-kernel sources (h and factor columns) staged per pass
+constexpr int kZS = 129;            // shared-memory stride of one staged source (odd: no conflicts)
+constexpr int kXS = 20;             // stride of one Vt entry over the sources (>= kTableSources,
+                                    // = 4 mod 16: fragment loads without bank conflicts)
 
 __host__ __device__ inline int table_sources(int R) { return R + 1 < kTableSources ? R + 1 : kTableSources; }
 
 // Per-left-string tables, one CTA per string u (dynamic shared memory: frame_tables_smem).  With
-// Y_s = Z_s[:, L] Sinv (n x K) for each source s (Z_0 = h, Z_{1+m} = B_m):
-//   Vt_s = Y_s[Lbar, :] - P Y_s[L, :],  tr T_s = tr Y_s[L, :],  tr T_s^2 = tr (Y_s[L, :])^2,
-//   V_s T_s Sinv = Vt_s Y_s[L, :],
-// so every quantity is a small dense product over staged rows, one thread per output element.
+// Y_s = Z_s[:, L] Sinv for each source s (Z_0 = h, Z_{1+m} = B_m), taken on the rows L (YL_s) and
+// Lbar (YB_s):
+//   Vt_s = YB_s - P YL_s,  tr T_s = tr YL_s,  tr T_s^2 = tr YL_s^2,  V_s T_s Sinv = Vt_s YL_s,
+// every product is an 8 x 8 tile (K, the complement and the hole positions are at most 8) on the
+// FP64 tensor cores (mma.sync m8n8k4): per source, Y_s from the staged rows [L; Lbar] of Z_s
+// (two row tiles), Vt_s with the accumulator started at YB_s, and Vt_s YL_s; the linear table
+// accumulates sigma_s (tr T_s Vt_s - Vt_s YL_s) in each warp's accumulator fragments.  The
+// quadratic table needs M = sum_s sigma_s x_s x_s^T over x_s = vec Vt_s (64 x 64, its 36 upper
+// tiles spread over the warps, k-steps over four sources at a time):
+//   Q(b b', c c') = M[(b c), (b' c')] - M[(b c'), (b' c)].
 template <int K>
 __global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a, double* __restrict__ tables) {
     constexpr int NBM = fr_nbmax(K);
     constexpr int CP = fr_cp(K);
     constexpr int BP = fr_bp(K);
     constexpr int KFS = fr_kfs(K);
-    constexpr int NQ = BP * CP;            // quadratic entries
-    constexpr int NE = NQ + NBM * K + 1;   // + linear entries + constant
-    constexpr int PER = (NE + kTableThreads - 1) / kTableThreads;
+    constexpr int NQ = BP * CP;
+    constexpr int MT = 36;                                     // upper 8 x 8 tiles of M
+    constexpr int MT_W = (MT + kTableWarps - 1) / kTableWarps;  // tiles per warp
     extern __shared__ double dsm[];
     const int n = a.n, R = a.R;
     const int nb = n - K;
     const int SC = table_sources(R);
     const FrameLayout F = frame_layout(n, K, R);
+    __shared__ int sL[8], sLb[8];
+    __shared__ double sM[K][2 * K], sF[K], sSinv[64], sP[64], sDet;
+    __shared__ double sE2[kTableWarps];
+    __shared__ int sOff[128];  // per staged slot (row, column): offset of its pair row in lf / in h
+    // Shared-memory layouts are chosen so that every fragment load of the tensor-core steps reads
+    // 32 consecutive doubles (lane order) or an odd stride, i.e. without bank conflicts:
+    //  sZ  [SC][kZS]: rows [L; Lbar] of Z_s as (k half, row, k mod 4): h * 64 + row * 4 + c % 4,
+    //                 then M (64 x 64) at the end
+    //  sX  [64][kXS]: Vt_s entry (b * 8 + c), source fastest
+    //  sYL [warps][64]: YL_s as a B operand (k half, column, k mod 4)
+    //  sVA [warps][64]: Vt_s as an A operand (k half, row, k mod 4)
+    double* sZ = dsm;
+    double* sX = sZ + (SC * kZS > 4096 ? SC * kZS : 4096);
+    double* sYL = sX + 64 * kXS;
+    double* sVA = sYL + kTableWarps * 64;
+    double* sLin = sVA + kTableWarps * 64;                  // [warps][64] linear-table partials
     const long long u = blockIdx.x;
     if (u >= a.n_strings) return;
     double* blk = tables + u * (long long)F.total;
-    __shared__ int sL[K], sLb[NBM];
-    __shared__ double sM[K][2 * K], sF[K], sSinv[K * K], sP[NBM * K], sDet;
-    double* sZ = dsm;                            // [SC][n][K]: Z_s, then Y_s in place
-    double* sVt = sZ + (size_t)SC * n * K;       // [SC][NBM][K]
-    double* sTr = sVt + (size_t)SC * NBM * K;    // [SC][2]: tr T_s, tr T_s^2
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gr = lane >> 2, gc = lane & 3;  // fragment row / column-in-group
     const uint64_t w0 = a.occ[2 * u];
     for (int i = tid; i < F.total; i += kTableThreads) blk[i] = 0.0;
     if (tid == 0) {
@@ -243,12 +265,51 @@ __global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a
         int q = 0;
         for (int i = 0; i < n && q < NBM; ++i)
             if (!((mask >> i) & 1)) sLb[q++] = i;
-        for (; q < NBM; ++q) sLb[q] = 0;
+        for (; q < 8; ++q) sLb[q] = -1;
     }
-    if (tid < K) sL[tid] = (int)((w0 >> (8 * tid)) & 0xFFu);
+    if (tid < 8) sL[tid] = tid < K ? (int)((w0 >> (8 * tid)) & 0xFFu) : -1;
+    for (int e = tid; e < 64; e += kTableThreads) {
+        sSinv[e] = 0.0;
+        sP[e] = 0.0;
+    }
     __syncthreads();
+    // slot (r, c) of a staged source holds Z_s(i, L_c) for i = L_r (r < 8) or Lbar_{r - 8}
+    for (int rc = tid; rc < 128; rc += kTableThreads) {
+        const int r = rc >> 3, c = rc & 7;
+        const int i = r < 8 ? sL[r] : sLb[r - 8];
+        sOff[rc] = (c < K && i >= 0) ? (int)((long long)dev::pair_index(i, sL[c]) * a.ld) : -1;
+    }
+    __syncthreads();
+    // stage sources [s0, s0 + sc) (lanes over sources, so factor columns read coalesced; the
+    // smem stride kZS is odd) by the warps [w_first, kTableWarps), eight loads in flight
+    auto stage = [&](int s0, int sc, int w_first) {
+        const int nw = kTableWarps - w_first, s = s0 + lane;
+        for (int rc0 = warp - w_first; rc0 < 128; rc0 += 8 * nw) {
+            double v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int rc = rc0 + j * nw;
+                v[j] = 0.0;
+                if (rc < 128 && lane < sc) {
+                    const int o = sOff[rc];
+                    if (o >= 0) {
+                        const int i = (rc >> 3) < 8 ? sL[rc >> 3] : sLb[(rc >> 3) - 8];
+                        v[j] = s == 0 ? __ldg(a.h + i * n + sL[rc & 7]) : __ldg(a.lf + o + (s - 1));
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int rc = rc0 + j * nw;
+                if (rc < 128 && lane < sc)
+                    sZ[lane * kZS + ((rc & 7) >> 2) * 64 + (rc >> 3) * 4 + (rc & 3)] = v[j];
+            }
+        }
+    };
     // S_LL^-1 by Gauss-Jordan on [S_LL | I] (S_LL is a principal block of an SPD matrix: the
-    // diagonal pivots are positive), warp 0 over the augmented entries
+    // diagonal pivots are positive), warp 0 over the augmented entries, while the other warps
+    // stage the first sources
+    if (warp != 0) stage(0, min(SC, R + 1), 1);
     if (warp == 0) {
         for (int e = lane; e < K * 2 * K; e += 32) {
             const int r = e / (2 * K), c = e % (2 * K);
@@ -259,9 +320,10 @@ __global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a
         for (int st = 0; st < K; ++st) {
             const double piv = sM[st][st];
             det *= piv;
+            const double inv = 1.0 / piv;
             if (lane < K) sF[lane] = sM[lane][st];
             __syncwarp();
-            for (int c = lane; c < 2 * K; c += 32) sM[st][c] /= piv;
+            for (int c = lane; c < 2 * K; c += 32) sM[st][c] *= inv;
             __syncwarp();
             for (int e = lane; e < K * 2 * K; e += 32) {
                 const int r = e / (2 * K), c = e % (2 * K);
@@ -269,7 +331,7 @@ __global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a
             }
             __syncwarp();
         }
-        for (int e = lane; e < K * K; e += 32) sSinv[e] = sM[e / K][K + e % K];
+        for (int e = lane; e < K * K; e += 32) sSinv[(e / K) * 8 + e % K] = sM[e / K][K + e % K];
         if (lane == 0) sDet = det;
     }
     __syncthreads();
@@ -279,8 +341,8 @@ __global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a
         double acc = 0.0;
         if (b < nb)
 #pragma unroll
-            for (int t = 0; t < K; ++t) acc = fma(__ldg(a.S + sLb[b] * n + sL[t]), sSinv[t * K + c], acc);
-        sP[e] = acc;
+            for (int t = 0; t < K; ++t) acc = fma(__ldg(a.S + sLb[b] * n + sL[t]), sSinv[t * 8 + c], acc);
+        sP[b * 8 + c] = acc;
         blk[F.o_p + e] = acc;
     }
     for (int e = tid; e < K + NBM; e += kTableThreads) {
@@ -297,7 +359,7 @@ __global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a
     }
     if (tid == kTableThreads - 1) {
         double s2 = 0.0, x2 = 0.0;
-        for (int e = 0; e < K * K; ++e) s2 = fma(sSinv[e], sSinv[e], s2);
+        for (int e = 0; e < 64; ++e) s2 = fma(sSinv[e], sSinv[e], s2);
         for (int c = 0; c < K; ++c)
             for (int t = 0; t < K; ++t) {
                 const double v = __ldg(a.S + sL[c] * n + sL[t]);
@@ -311,130 +373,167 @@ __global__ void __launch_bounds__(kTableThreads, 4) frame_tables(SpinTableArgs a
     if (tid < NBM) {
         double acc = 0.0;
 #pragma unroll
-        for (int c = 0; c < K; ++c) acc = fma(sP[tid * K + c], sP[tid * K + c], acc);
+        for (int c = 0; c < K; ++c) acc = fma(sP[tid * 8 + c], sP[tid * 8 + c], acc);
         blk[F.o_prow2 + tid] = acc;
     }
-    double acc[PER];
+    // per-lane fragments that do not change with the source: Sinv as B (k x n), -P as A (m x k)
+    double sinv_b[2], negp_a[2];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) acc[q] = 0.0;
+    for (int ks = 0; ks < 2; ++ks) {
+        sinv_b[ks] = sSinv[(4 * ks + gc) * 8 + gr];
+        negp_a[ks] = -sP[gr * 8 + 4 * ks + gc];
+    }
+    double lin[2] = {0.0, 0.0}, e2 = 0.0;
+    double mq[MT_W][2];
+#pragma unroll
+    for (int t = 0; t < MT_W; ++t) mq[t][0] = mq[t][1] = 0.0;
+    double* yl = sYL + warp * 64;
+    double* va = sVA + warp * 64;
     for (int s0 = 0; s0 < R + 1; s0 += SC) {
         const int sc = min(SC, R + 1 - s0);
-        // stage Z_s(i, L_c) for every orbital i; source fastest, so factor columns read coalesced
-        for (int e = tid; e < sc * n * K; e += kTableThreads) {
-            const int sl = e % sc, ic = e / sc, i = ic / K, c = ic % K, s = s0 + sl;
-            const double v = s == 0 ? __ldg(a.h + i * n + sL[c])
-                                    : __ldg(a.lf + (long long)dev::pair_index(i, sL[c]) * a.ld + (s - 1));
-            sZ[((size_t)sl * n + i) * K + c] = v;
+        if (s0 > 0) {
+            stage(s0, sc, 0);
+            __syncthreads();
         }
-        __syncthreads();
-        // Y_s = Z_s Sinv, one row per thread, in place
-        for (int e = tid; e < sc * n; e += kTableThreads) {
-            double* row = sZ + (size_t)e * K;
-            double z[K];
-#pragma unroll
-            for (int t = 0; t < K; ++t) z[t] = row[t];
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                double x = 0.0;
-#pragma unroll
-                for (int t = 0; t < K; ++t) x = fma(z[t], sSinv[t * K + c], x);
-                row[c] = x;
-            }
-        }
-        __syncthreads();
-        // Vt_s and the traces; table rows (row 0 = h, row 1 + s = factor column s - 1)
-        for (int e = tid; e < sc * NBM * K; e += kTableThreads) {
-            const int sl = e / (NBM * K), bc = e % (NBM * K), b = bc / K, c = bc % K;
-            const double* Y = sZ + (size_t)sl * n * K;
-            double x = 0.0;
-            if (b < nb) {
-                x = Y[sLb[b] * K + c];
-#pragma unroll
-                for (int t = 0; t < K; ++t) x = fma(-sP[b * K + t], Y[sL[t] * K + c], x);
-                const int s = s0 + sl;
-                blk[(long long)(s == 0 ? 0 : s + 1) * KFS + c * 8 + b] = x;
-            }
-            sVt[e] = x;
-        }
-        for (int sl = tid; sl < sc; sl += kTableThreads) {
-            const double* Y = sZ + (size_t)sl * n * K;
-            double tr = 0.0, tr2 = 0.0;
-            for (int r = 0; r < K; ++r) {
-                tr += Y[sL[r] * K + r];
-                for (int t = 0; t < K; ++t) tr2 = fma(Y[sL[r] * K + t], Y[sL[t] * K + r], tr2);
-            }
-            sTr[2 * sl] = tr;
-            sTr[2 * sl + 1] = tr2;
+        for (int sl = warp; sl < sc; sl += kTableWarps) {
             const int s = s0 + sl;
+            const double* z = sZ + (size_t)sl * kZS;
+            // Y' = [L; Lbar] rows of Z_s times Sinv: tile 0 = YL, tile 1 = YB
+            double y0[2] = {0.0, 0.0}, y1[2] = {0.0, 0.0};
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                mma_f64(y0, z[ks * 64 + lane], sinv_b[ks]);
+                mma_f64(y1, z[ks * 64 + 32 + lane], sinv_b[ks]);
+            }
+            // YL(r, c) at (r / 4) * 32 + c * 4 + r % 4
+#pragma unroll
+            for (int h = 0; h < 2; ++h) yl[(gr >> 2) * 32 + (2 * gc + h) * 4 + (gr & 3)] = y0[h];
+            __syncwarp();
+            // Vt = YB - P YL (accumulator started at YB)
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) mma_f64(y1, negp_a[ks], yl[ks * 32 + lane]);
+            // Vt to the source's column of sX and, as an A operand, to va
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = 2 * gc + h;
+                sX[(gr * 8 + c) * kXS + sl] = y1[h];
+                va[(c >> 2) * 32 + gr * 4 + (c & 3)] = y1[h];
+            }
+            // traces of YL and YL^2
+            double tr = 0.0, tr2 = 0.0;
+            if (lane < K) {
+                auto YL = [&](int r, int c) { return yl[(r >> 2) * 32 + c * 4 + (r & 3)]; };
+                tr = YL(lane, lane);
+#pragma unroll
+                for (int t = 0; t < K; ++t) tr2 = fma(YL(lane, t), YL(t, lane), tr2);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                tr += __shfl_xor_sync(0xffffffffu, tr, o);
+                tr2 += __shfl_xor_sync(0xffffffffu, tr2, o);
+            }
+            // table row of this source: Vt on the (hole position c, complement b) grid, trace
             double* row = blk + (long long)(s == 0 ? 0 : s + 1) * KFS;
-            row[8 * K] = tr;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int b = gr, c = 2 * gc + h;
+                if (c < K && b < nb) row[c * 8 + b] = y1[h];
+            }
+            if (lane == 0) row[8 * K] = tr;
             // with at most 7 complement orbitals, column 7 of every hole block is free: the trace
             // there lets a pair with holes pick it up in its first hole block (no trace k-step)
-            if (nb <= 7)
-                for (int c = 0; c < K; ++c) row[c * 8 + 7] = tr;
-        }
-        __syncthreads();
-        // two-electron constant, linear and quadratic tables over the factor sources
+            if (nb <= 7 && lane < K) row[lane * 8 + 7] = tr;
+            __syncwarp();
+            if (s > 0) {
+                const double sg = (s - 1) < a.r_pos ? 1.0 : -1.0;
+                // V T Sinv = Vt YL
+                double vts[2] = {0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            const int e = tid + kTableThreads * q;
-            if (e >= NE) continue;
-            double x = acc[q];
-            if (e < NQ) {
-                constexpr int CPD = CP > 0 ? CP : 1;
-                const int bp = e / CPD, cp = e % CPD;
-                int b2 = 1;
-                while ((b2 + 1) * b2 / 2 <= bp) ++b2;
-                const int b1 = bp - b2 * (b2 - 1) / 2;
-                int c2 = 1;
-                while ((c2 + 1) * c2 / 2 <= cp) ++c2;
-                const int c1 = cp - c2 * (c2 - 1) / 2;
-                for (int sl = (s0 == 0 ? 1 : 0); sl < sc; ++sl) {
-                    const double* V = sVt + (size_t)sl * NBM * K;
-                    const double sg = (s0 + sl - 1) < a.r_pos ? 1.0 : -1.0;
-                    x = fma(sg, V[b1 * K + c1] * V[b2 * K + c2] - V[b1 * K + c2] * V[b2 * K + c1], x);
-                }
-            } else if (e < NE - 1) {
-                const int bc = e - NQ, b = bc / K, c = bc % K;
-                for (int sl = (s0 == 0 ? 1 : 0); sl < sc; ++sl) {
-                    const double* V = sVt + (size_t)sl * NBM * K;
-                    const double* Y = sZ + (size_t)sl * n * K;
-                    const double sg = (s0 + sl - 1) < a.r_pos ? 1.0 : -1.0;
-                    double vts = 0.0;
-#pragma unroll
-                    for (int t = 0; t < K; ++t) vts = fma(V[b * K + t], Y[sL[t] * K + c], vts);
-                    x = fma(sg, sTr[2 * sl] * V[bc] - vts, x);
-                }
-            } else {
-                for (int sl = (s0 == 0 ? 1 : 0); sl < sc; ++sl) {
-                    const double sg = (s0 + sl - 1) < a.r_pos ? 1.0 : -1.0;
-                    x = fma(sg, sTr[2 * sl] * sTr[2 * sl] - sTr[2 * sl + 1], x);
-                }
+                for (int ks = 0; ks < 2; ++ks) mma_f64(vts, va[ks * 32 + lane], yl[ks * 32 + lane]);
+                lin[0] = fma(sg, fma(tr, y1[0], -vts[0]), lin[0]);
+                lin[1] = fma(sg, fma(tr, y1[1], -vts[1]), lin[1]);
+                e2 = fma(sg, tr * tr - tr2, e2);
             }
-            acc[q] = x;
+            __syncwarp();
         }
         __syncthreads();
-    }
+        // M += sum_s sigma_s x_s x_s^T over this pass's sources, four per k-step
+        for (int k0 = 0; k0 < sc; k0 += 4) {
+            const int sl = k0 + gc, s = s0 + sl;
+            const bool ok = sl < sc && s > 0;
+            const double sg = ok ? ((s - 1) < a.r_pos ? 1.0 : -1.0) : 0.0;
+            const double* x = sX + (ok ? sl : 0);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int e = tid + kTableThreads * q;
-        if (e >= NE) continue;
-        if (e < NQ) {
-            blk[F.o_q + e] = acc[q];
-        } else if (e < NE - 1) {
-            const int bc = e - NQ, b = bc / K, c = bc % K;
-            if (b < nb) blk[1 * KFS + c * 8 + b] = acc[q];
-        } else {
-            blk[1 * KFS + 8 * K] = 0.5 * acc[q];
-            if (nb <= 7)
-                for (int c = 0; c < K; ++c) blk[1 * KFS + c * 8 + 7] = 0.5 * acc[q];
+            for (int t = 0; t < MT_W; ++t) {
+                const int tile = warp + kTableWarps * t;
+                if (tile >= MT) break;
+                int ti = 0, rem = tile;
+                while (rem >= 8 - ti) {
+                    rem -= 8 - ti;
+                    ++ti;
+                }
+                const int tj = ti + rem;
+                mma_f64(mq[t], sg * x[(ti * 8 + gr) * kXS], ok ? x[(tj * 8 + gr) * kXS] : 0.0);
+            }
         }
+    }
+    // combine the warps' partial linear tables, the constant, and M
+    sLin[warp * 64 + gr * 8 + 2 * gc] = lin[0];
+    sLin[warp * 64 + gr * 8 + 2 * gc + 1] = lin[1];
+    if (lane == 0) sE2[warp] = e2;
+    double* sMq = sZ;  // 64 x 64
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < MT_W; ++t) {
+        const int tile = warp + kTableWarps * t;
+        if (tile >= MT) break;
+        int ti = 0, rem = tile;
+        while (rem >= 8 - ti) {
+            rem -= 8 - ti;
+            ++ti;
+        }
+        const int tj = ti + rem;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = ti * 8 + gr, c = tj * 8 + 2 * gc + h;
+            sMq[r * 64 + c] = mq[t][h];
+            if (ti != tj) sMq[c * 64 + r] = mq[t][h];
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < 64; e += kTableThreads) {
+        const int b = e >> 3, c = e & 7;
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < kTableWarps; ++w) x += sLin[w * 64 + e];
+        if (c < K && b < nb) blk[1 * KFS + c * 8 + b] = x;
+    }
+    if (tid == 0) {
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < kTableWarps; ++w) x += sE2[w];
+        blk[1 * KFS + 8 * K] = 0.5 * x;
+        if (nb <= 7)
+            for (int c = 0; c < K; ++c) blk[1 * KFS + c * 8 + 7] = 0.5 * x;
+    }
+    for (int e = tid; e < NQ; e += kTableThreads) {
+        constexpr int CPD = CP > 0 ? CP : 1;
+        const int bp = e / CPD, cp = e % CPD;
+        int b2 = 1;
+        while ((b2 + 1) * b2 / 2 <= bp) ++b2;
+        const int b1 = bp - b2 * (b2 - 1) / 2;
+        int c2 = 1;
+        while ((c2 + 1) * c2 / 2 <= cp) ++c2;
+        const int c1 = cp - c2 * (c2 - 1) / 2;
+        blk[F.o_q + e] = sMq[(b1 * 8 + c1) * 64 + b2 * 8 + c2] - sMq[(b1 * 8 + c2) * 64 + b2 * 8 + c1];
     }
 }
 
 template <int K>
 size_t frame_tables_smem(int n, int R) {
-    return sizeof(double) * (size_t)table_sources(R) * ((size_t)n * K + (size_t)fr_nbmax(K) * K + 2);
+    (void)n;
+    const size_t sc = (size_t)table_sources(R);
+    return sizeof(double) * ((sc * kZS > 4096 ? sc * kZS : 4096) + 64 * kXS + 3 * (size_t)kTableWarps * 64);
 }
 
 // Phase A of one pair at excitation level E (compile time).  Writes the pair's Y' row and
