@@ -220,6 +220,112 @@ __global__ void __launch_bounds__(32 * kPipeWarps, 2) one_index_pipelined_kernel
     }
 }
 
+// FP64 tensor-core variant (mma.sync m8n8k4, the FP64 tensor path of sm_100a) for even n_aux
+// and n_bf <= kDmmaMaxBf: T_mu[P, a] = sum_nu B[P, pair(mu, nu)] C[nu, a] is, per AO index mu,
+// a (64 auxiliary rows) x (16 active) x (n_bf) product.  Persistent CTAs of eight warps stage C
+// once ([nu][20], padded so the B-fragment loads are conflict-free) and loop over (8 AO indices,
+// 64 auxiliary rows) items; each warp streams its mu's columns through a private 3-stage
+// cp.async ring of 8 columns x 64 rows (row stride 68: conflict-free A-fragment loads) and keeps
+// 8 x 2 accumulator tiles in registers.  Items run with the auxiliary tile fastest, so the
+// CTAs resident together read whole packed columns.  The sum over nu runs in a fixed order.
+constexpr int kDmmaWarps = 8;
+constexpr int kDmmaRows = 64;      // auxiliary rows per item (8 M tiles)
+constexpr int kDmmaNu = 8;         // columns per ring stage (two k-steps)
+constexpr int kDmmaStages = 3;
+constexpr int kDmmaRing = 68;      // ring row stride (doubles; = 4 mod 16)
+constexpr int kDmmaCt = 20;        // staged C stride (doubles; = 4 mod 16)
+constexpr int kDmmaMaxBf = 768;   // shared memory: C staging plus the rings
+
+size_t dmma_smem_bytes(int n_bf) {
+    return sizeof(double) * ((size_t)n_bf * kDmmaCt + (size_t)kDmmaWarps * kDmmaStages * kDmmaNu * kDmmaRing);
+}
+
+__device__ __forceinline__ void dmma_f64(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(32 * kDmmaWarps, 1) one_index_dmma_kernel(const double* __restrict__ B, int n_aux,
+                                                                            int n_bf, const double* __restrict__ Ct,
+                                                                            int n_act, double* __restrict__ T) {
+    extern __shared__ __align__(16) double smem[];
+    double* sC = smem;                                       // [n_bf][kDmmaCt]
+    double* ring_all = smem + (size_t)n_bf * kDmmaCt;       // [warp][stage][nu][kDmmaRing]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gr = lane >> 2, gc = lane & 3;
+    for (int e = threadIdx.x; e < n_bf * kDmmaCt; e += blockDim.x) {
+        const int nu = e / kDmmaCt, a = e % kDmmaCt;
+        sC[e] = a < kMaxActive ? __ldg(Ct + (size_t)nu * kMaxActive + a) : 0.0;
+    }
+    __syncthreads();
+    double* ring = ring_all + (size_t)warp * kDmmaStages * kDmmaNu * kDmmaRing;
+    const int mu_blocks = (n_bf + kDmmaWarps - 1) / kDmmaWarps;
+    const int aux_tiles = (n_aux + kDmmaRows - 1) / kDmmaRows;
+    const int n_steps = (n_bf + kDmmaNu - 1) / kDmmaNu;
+    const long long ld = (long long)n_act * n_aux;
+    for (long long item = blockIdx.x; item < (long long)mu_blocks * aux_tiles; item += gridDim.x) {
+        const int mu = (int)(item / aux_tiles) * kDmmaWarps + warp;
+        const int aux0 = (int)(item % aux_tiles) * kDmmaRows;
+        if (mu >= n_bf) continue;  // warp-private work below: no CTA-wide barrier
+        auto issue = [&](int step) {
+            if (step < n_steps) {
+                double* stage = ring + (step % kDmmaStages) * kDmmaNu * kDmmaRing;
+#pragma unroll
+                for (int h = 0; h < kDmmaNu; ++h) {
+                    // lane's 16-byte chunk: column h of the stage, rows 2 lane and 2 lane + 1
+                    const int nu = step * kDmmaNu + h, r = 2 * lane;
+                    const bool ok = nu < n_bf && aux0 + r < n_aux;
+                    const double* src = ok ? B + ao_pair(mu, nu) * n_aux + aux0 + r : B;
+                    cp_async16(stage + h * kDmmaRing + r, src, ok ? 16 : 0);
+                }
+            }
+            cp_async_commit();
+        };
+#pragma unroll
+        for (int st = 0; st < kDmmaStages - 1; ++st) issue(st);
+        double acc[8][2][2];
+#pragma unroll
+        for (int m = 0; m < 8; ++m)
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) acc[m][nt][0] = acc[m][nt][1] = 0.0;
+        for (int step = 0; step < n_steps; ++step) {
+            issue(step + kDmmaStages - 1);
+            cp_async_wait<kDmmaStages - 1>();
+            __syncwarp();
+            const double* stage = ring + (step % kDmmaStages) * kDmmaNu * kDmmaRing;
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                const int v = 4 * ks + gc;  // column of this lane's A (and row of its B) element
+                const int nu = step * kDmmaNu + v;
+                const double* cb = sC + (size_t)(nu < n_bf ? nu : 0) * kDmmaCt + gr;
+                const double b0 = nu < n_bf ? cb[0] : 0.0, b1 = nu < n_bf ? cb[8] : 0.0;
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    const double a = stage[v * kDmmaRing + 8 * m + gr];
+                    dmma_f64(acc[m][0], a, b0);
+                    dmma_f64(acc[m][1], a, b1);
+                }
+            }
+            __syncwarp();
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int P = aux0 + 8 * m + gr;
+            if (P >= n_aux) continue;
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int a = 8 * nt + 2 * gc + h;
+                    if (a < n_act) T[(long long)a * n_aux + P + (long long)mu * ld] = acc[m][nt][h];
+                }
+        }
+    }
+}
+
 constexpr int kSplitWarps = 8;   // AO indices per CTA
 constexpr int kSplitRows = 16;   // auxiliary rows per warp (one M tile)
 constexpr int kSplitFlush = 4;   // K steps between flushes of the leading-order FP32 accumulator
@@ -686,12 +792,28 @@ vb_status vb_active_transform_ri_precision(vb_context* ctx, const double* B_pack
             transpose_coefficients_kernel<<<(n_bf * kMaxActive + 255) / 256, 256, 0, s>>>(dC, n_bf, n_act, Ct);
             err = cudaGetLastError();
             const size_t smem = pipelined_smem_bytes(n_bf);
+            if (n_bf <= kDmmaMaxBf) {
+                // FP64 tensor cores, persistent CTAs (one per SM)
+                const size_t dsmem = dmma_smem_bytes(n_bf);
+                if (err == cudaSuccess) err = allow_dynamic_smem((const void*)one_index_dmma_kernel, (int)dsmem);
+                int dev = 0, sms = 0;
+                if (err == cudaSuccess) err = cudaGetDevice(&dev);
+                if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                const long long items = (long long)((n_bf + kDmmaWarps - 1) / kDmmaWarps) *
+                                        ((n_aux + kDmmaRows - 1) / kDmmaRows);
+                const long long grid = items < sms ? items : sms;
+                if (err == cudaSuccess) {
+                    one_index_dmma_kernel<<<(unsigned)grid, 32 * kDmmaWarps, dsmem, s>>>(dB, n_aux, n_bf, Ct, n_act, dT);
+                    err = cudaGetLastError();
+                }
+            } else {
             if (err == cudaSuccess)
                 err = allow_dynamic_smem((const void*)one_index_pipelined_kernel, (int)smem);
             if (err == cudaSuccess) {
                 const dim3 pgrid((n_bf + kPipeWarps - 1) / kPipeWarps, (n_aux + kAuxTile - 1) / kAuxTile);
                 one_index_pipelined_kernel<<<pgrid, 32 * kPipeWarps, smem, s>>>(dB, n_aux, n_bf, Ct, n_act, dT);
                 err = cudaGetLastError();
+            }
             }
         } else {
             one_index_kernel<<<grid, 32 * kWarpsPerCta, 0, s>>>(dB, n_aux, n_bf, dC, n_act, dT);
