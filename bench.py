@@ -671,9 +671,9 @@ def run_ri(args):
                                "[1600 x 80,200] (1.027 GB), C ~ N(0, 1/sqrt(400)); outputs one-index factors, "
                                "L [1600 x 136], packed K", "flops_model": flops, "l2": "256 MiB write between steps "
                                "(B alone is 1.03 GB)"},
-        "roofline": {"bound": "fp64", "kernel": "one_index_pipelined_kernel (+ second index, packing)",
+        "roofline": {"bound": "fp64", "kernel": "one_index_dmma_kernel (+ second index, packing)",
                      "achieved": flops / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
-                     "frac": flops / (ms * 1e-3) / 1e12 / peak, "traffic": read_profile_traffic("one_index_pipelined_kernel"),
+                     "frac": flops / (ms * 1e-3) / 1e12 / peak, "traffic": read_profile_traffic("one_index_dmma_kernel"),
                      "hbm_gbs": bytes_b / (ms * 1e-3) / 1e9,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured)"},
         "errors_vs_fp64_oracle": {"max_abs": err_abs, "rel": err_rel, "rows_checked": int(len(rows))},
