@@ -17,6 +17,7 @@
 #include <algorithm>
 
 #include "internal.h"
+#include "kernels.h"
 
 namespace vbcore {
 namespace {
@@ -55,10 +56,20 @@ __global__ void __launch_bounds__(128) factor_project_kernel(int np, int R, cons
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const long long c0 = t * kProjCols;
         __syncthreads();
-        for (int e = tid; e < KR * kProjCols; e += 128) {
-            const int cc = e / KR, m = e % KR;  // m fastest: contiguous reads of each column
-            const long long c = c0 + cc;
-            sY[m * YS + cc] = (m < R && c < cnt) ? __ldg(Y + c * ldY + m) : 0.0;
+        // m fastest: contiguous reads of each column; eight loads in flight per thread
+        for (int e0 = tid; e0 < KR * kProjCols; e0 += 8 * 128) {
+            double v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int e = e0 + 128 * j, cc = e / KR, m = e % KR;
+                const long long c = c0 + cc;
+                v[j] = (e < KR * kProjCols && m < R && c < cnt) ? __ldg(Y + c * ldY + m) : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int e = e0 + 128 * j;
+                if (e < KR * kProjCols) sY[(e % KR) * YS + e / KR] = v[j];
+            }
         }
         __syncthreads();
         // this warp's 16 columns: B fragments for every k-step, kept in registers
@@ -122,13 +133,34 @@ __global__ void __launch_bounds__(32 * kOuterWarps) factor_outer_kernel(int np, 
     const long long c_begin = blockIdx.x * per, c_end = min(cnt, c_begin + per);
     for (long long c0 = c_begin; c0 < c_end; c0 += kOuterChunk) {
         __syncthreads();
-        for (int e = tid; e < (MR + NQ) * kOuterChunk; e += 32 * kOuterWarps) {
-            const int cc = e / (MR + NQ), r = e % (MR + NQ);  // row fastest: contiguous column reads
-            const long long c = c0 + cc;
-            if (r < MR)
-                sY[r * CS + cc] = (r < R && c < c_end) ? __ldg(Y + c * ldY + r) : 0.0;
-            else
-                sZ[(r - MR) * CS + cc] = (r - MR < np && c < c_end) ? __ldg(Z + c * ldZ + (r - MR)) : 0.0;
+        // row fastest: contiguous column reads; eight loads in flight per thread
+        const int tot = (MR + NQ) * kOuterChunk;
+        for (int e0 = tid; e0 < tot; e0 += 8 * 32 * kOuterWarps) {
+            double v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int e = e0 + 32 * kOuterWarps * j;
+                const int cc = e / (MR + NQ), r = e % (MR + NQ);
+                const long long c = c0 + cc;
+                v[j] = 0.0;
+                if (e < tot && c < c_end) {
+                    if (r < MR) {
+                        if (r < R) v[j] = __ldg(Y + c * ldY + r);
+                    } else if (r - MR < np) {
+                        v[j] = __ldg(Z + c * ldZ + (r - MR));
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int e = e0 + 32 * kOuterWarps * j;
+                if (e >= tot) break;
+                const int cc = e / (MR + NQ), r = e % (MR + NQ);
+                if (r < MR)
+                    sY[r * CS + cc] = v[j];
+                else
+                    sZ[(r - MR) * CS + cc] = v[j];
+            }
         }
         __syncthreads();
 #pragma unroll
@@ -222,7 +254,8 @@ size_t factor_project_smem(int np, int R) {
 
 bool factor_contractions_supported(int np, int R) {
     // register-resident k-steps (R <= 144) and tile blocks (12 per warp: R, np <= 192)
-    return R <= 144 && np <= 192 && factor_project_smem(np, R) <= 200 * 1024;
+    return R <= 144 && np <= 192 && factor_project_smem(np, R) <= 200 * 1024 &&
+           sizeof(double) * (size_t)(up8(R) + up8(np)) * (kOuterChunk + 1) <= 200 * 1024;
 }
 
 cudaError_t launch_factor_project(int np, int R, const double* lf, int ld, const double* Y, long long ldY,
@@ -251,8 +284,10 @@ cudaError_t launch_factor_project(int np, int R, const double* lf, int ld, const
     return cudaGetLastError();
 }
 
+// Split-K parts of factor_outer: up to kOuterMaxParts CTAs (four per SM, so that enough column
+// loads are in flight), at least 256 spin pairs each.
 int factor_outer_parts(long long cnt) {
-    return (int)std::max<long long>(1, std::min<long long>(148, (cnt + 255) / 256));
+    return (int)std::max<long long>(1, std::min<long long>(kOuterMaxParts, (cnt + 255) / 256));
 }
 
 cudaError_t launch_factor_outer(int np, int R, const double* Y, long long ldY, const double* Z, long long ldZ,

@@ -873,7 +873,7 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
     }
     // split-K partials of the factor-column adjoint (one R x np block per CTA of factor_outer)
     DeviceBuffer partial;
-    if (err == cudaSuccess && (st = partial.allocate(ctx, sizeof(double) * 148 * (size_t)std::max(1, R) * np)) != VB_OK)
+    if (err == cudaSuccess && (st = partial.allocate(ctx, sizeof(double) * kOuterMaxParts * (size_t)std::max(1, R) * np)) != VB_OK)
         return st;
     // backward through each distinct spin table
     for (int beta = 0; beta < 2 && err == cudaSuccess; ++beta) {

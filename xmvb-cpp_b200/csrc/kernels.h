@@ -68,8 +68,8 @@ struct FullPairArgs {
 // Band reduction Z = T^T U' (structure-major weights T, band U' upper triangle).  Rows of the
 // band are streamed in tiles of kBandTileRows; for every (structure group g, row tile t) the plan
 // holds one segment of (row-in-tile, coefficient) terms ordered by (warp, slot, determinant):
-// seg_off[g T + t] (a multiple of 16) indexes term_c / term_d, and seg_meta holds 144 bytes per
-// segment: the term count of each (warp, slot) (kBandWarps x kBandSlots bytes) followed by the
+// seg_off[g T + t] (a multiple of 16) indexes term_c / term_d, and seg_meta holds kBandMetaBytes
+// per segment: the term count of each (warp, slot) (kBandWarps x kBandSlots bytes) followed by the
 // start of each warp's terms within the segment (kBandWarps uint16).  Structure of group g, warp
 // w, slot s: I = g * kBandGroup + s * kBandWarps + w.
 struct BandReduceArgs {
@@ -163,10 +163,11 @@ cudaError_t launch_same_spin_list(int n, int k, long long batch, const int* occ_
 // FP64 tensor-core contractions over the pair-kernel factor columns (dgemm.cu):
 //   launch_factor_project: C[q + c ldC] = sum_m lf[q ld + m] Y[m + c ldY]     (np x cnt)
 //   launch_factor_outer:   G[m + q ldG] += sum_c Y[m + c ldY] Z[q + c ldZ]    (R x np); `partial`
-//   holds 148 R np doubles of split-K partials, summed in a fixed order.
+//   holds kOuterMaxParts R np doubles of split-K partials, summed in a fixed order.
 bool factor_contractions_supported(int np, int R);
 cudaError_t launch_factor_project(int np, int R, const double* lf, int ld, const double* Y, long long ldY,
                                   long long cnt, double* C, long long ldC, cudaStream_t stream);
+constexpr int kOuterMaxParts = 4 * 148;
 cudaError_t launch_factor_outer(int np, int R, const double* Y, long long ldY, const double* Z, long long ldZ,
                                 long long cnt, double* G, long long ldG, double* partial, cudaStream_t stream);
 // Dynamic shared memory of the band reduction for segments of at most seg_max terms.
