@@ -242,3 +242,26 @@ def test_spin_pair_records_every_electron_count(n, k):
             assert int(got[t, 3]) == ref["nullity"]
             for col, key in ((0, "det"), (1, "h1"), (2, "htot")):
                 assert abs(got[t, col] - ref[key]) <= REL * max(1.0, abs(ref[key])), (n, k, t, key)
+
+
+def test_band_reduction_wait_timeout_is_reported_and_the_plan_recovers():
+    """The band reduction's tile waits are bounded: with a one-poll limit the first wait gives up,
+    the CTAs flag it and leave after their copies in flight land, and the execute returns
+    VB_ERR_TIMEOUT (no trap, no hang); with the default limit restored the same plan evaluates
+    the structure matrices."""
+    n = 8
+    S, h, eri = workloads.active_space(n, 3 * n, 21)
+    c = vbcore.Context(0)
+    try:
+        plan, ex = _plan(c, "COV", n, n)
+        c.set_barrier_spin_limit(1)
+        with pytest.raises(vbcore.VbError) as e:
+            plan.execute(S, h, eri)
+        assert e.value.status == 6 and "band_reduce" in str(e.value)
+        c.set_barrier_spin_limit(0)
+        H, So = plan.execute(S, h, eri)
+        Hr, Sr, _ = O.structure_matrices(n, ex, S, h, eri)
+        assert _rel(H, Hr) < REL and _rel(So, Sr) < REL
+        plan.close()
+    finally:
+        c.close()

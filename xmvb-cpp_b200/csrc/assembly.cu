@@ -22,6 +22,7 @@ namespace vbcore {
 namespace {
 
 constexpr int kTileBytes = kBandTileRows * kBandColumns * 8;  // one band tile (H or S)
+constexpr long long kDrainPolls = 1ll << 22;  // bound on waiting for copies in flight (~seconds)
 constexpr int kZPad = kBandColumns + 1;
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -133,7 +134,9 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
 
     // One barrier per tile: after computing tile t every thread waits for tile t + 1, and the
     // barrier then both releases stage t & 1 for refilling and confirms tile t + 1 landed.
-    const long long limit = a.spin_limit / 16 > 0 ? a.spin_limit / 16 : 1;  // polls of <= ~1 us
+    // polls of up to ~1 us each (0 when the context's limit is below 16: the first wait gives up
+    // at once, which is how the timeout path is exercised)
+    const long long limit = a.spin_limit / 16;
     bool ok = __syncthreads_and(mbar_wait(&full[0], 0u, limit)) != 0;
     int t = 0;
     for (; ok && t < ntiles; ++t) {
@@ -184,10 +187,11 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
         }
     }
     if (!ok) {
-        // a tile never landed: flag it, let the copies still in flight land, and leave
+        // a tile never landed: flag it, let the copies still in flight land (a generous bound of
+        // its own: no copy may outlive the CTA), and leave
         if (tid == 0) {
             atomicExch(a.error, 1);
-            for (int u = t; u < issued; ++u) mbar_wait(&full[u & 1], (unsigned)(u >> 1) & 1u, limit);
+            for (int u = t; u < issued; ++u) mbar_wait(&full[u & 1], (unsigned)(u >> 1) & 1u, kDrainPolls);
         }
         __syncthreads();
         return;
