@@ -103,25 +103,48 @@ __global__ void __launch_bounds__(256) det_pair_adjoint_flip_kernel(AdjArgs a, c
         const double pair_w = i == j ? 1.0 : 2.0;
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         double acc_det = 0.0, acc_h = 0.0;
-        for (int p = i0; p < i1; ++p) {
-            const int d = __ldg(adets + p);
-            const double wd = __ldg(a.w + d) * pair_w;
-            if (wd == 0.0) continue;
-            const int bd = __ldg(a.f.det_beta + d);
-            for (int q = j0; q < j1; ++q) {
-                const int e = __ldg(adets + q);
-                const double omega = wd * __ldg(a.w + e);
-                if (omega == 0.0) continue;
-                const int be = __ldg(a.f.det_beta + e);
-                const double* rb = a.f.rec_b + record_index(min(bd, be), max(bd, be), a.f.Nb) * a.f.stride_b;
-#pragma unroll
-                for (int qq = 0; qq < 4; ++qq) {
-                    const int m = lane + 32 * qq;
-                    if (m < R) acc[qq] = fma(omega, m < a.f.r_pos ? __ldg(rb + m) : -__ldg(rb + m), acc[qq]);
+        // 32 determinants of each side at a time: lanes load their indices, weights and beta
+        // strings together, then the warp walks the pairs with shuffled operands, so the record
+        // loads of consecutive pairs do not wait on one another
+        for (int qc = j0; qc < j1; qc += 32) {
+            const int nq = min(32, j1 - qc);
+            int be_l = 0;
+            double we_l = 0.0;
+            if (lane < nq) {
+                const int e = __ldg(adets + qc + lane);
+                we_l = __ldg(a.w + e);
+                be_l = __ldg(a.f.det_beta + e);
+            }
+            for (int pc = i0; pc < i1; pc += 32) {
+                const int np_ = min(32, i1 - pc);
+                int bd_l = 0;
+                double wd_l = 0.0;
+                if (lane < np_) {
+                    const int d = __ldg(adets + pc + lane);
+                    wd_l = __ldg(a.w + d) * pair_w;
+                    bd_l = __ldg(a.f.det_beta + d);
                 }
-                const double sb = __ldg(rb + R), hb = __ldg(rb + R + 1);
-                acc_det = fma(omega, hb - a.lambda * sb, acc_det);
-                acc_h = fma(omega, sb, acc_h);
+                for (int pp = 0; pp < np_; ++pp) {
+                    const double wd = __shfl_sync(0xffffffffu, wd_l, pp);
+                    const int bd = __shfl_sync(0xffffffffu, bd_l, pp);
+                    if (wd == 0.0) continue;
+#pragma unroll 4
+                    for (int qq = 0; qq < nq; ++qq) {
+                        const double omega = wd * __shfl_sync(0xffffffffu, we_l, qq);
+                        const int be = __shfl_sync(0xffffffffu, be_l, qq);
+                        if (omega == 0.0) continue;
+                        const double* rb =
+                            a.f.rec_b + record_index(min(bd, be), max(bd, be), a.f.Nb) * a.f.stride_b;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int m = lane + 32 * u;
+                            if (m < R) acc[u] = fma(omega, m < a.f.r_pos ? __ldg(rb + m) : -__ldg(rb + m), acc[u]);
+                        }
+                        const double sb = __ldg(rb + R), hb = __ldg(rb + R + 1);
+                        acc_det = fma(omega, hb - a.lambda * sb, acc_det);
+                        acc_h = fma(omega, sb, acc_h);
+                    }
+                }
             }
         }
         double* adj = a.adj_a + t * a.adj_stride;
