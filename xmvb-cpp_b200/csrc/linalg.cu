@@ -125,6 +125,23 @@ struct Shared {
     int flag;
 };
 
+// FP64 tensor-core step (mma.sync m8n8k4): this lane's fragment (row lane / 4, columns
+// 2 (lane % 4) + {0, 1}) of the 8 x 8 output tile (mt, nt) of a 32 x 32 product, accumulated over
+// k < 32 with A(r, k) = fa(r, k) and B(k, c) = fb(k, c).  Eight warps cover the 16 output tiles
+// of a 32 x 32 tile two at a time (tiles warp and warp + 8).
+__device__ __forceinline__ void dmma8(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+template <class FA, class FB>
+__device__ __forceinline__ void mma_tile32(double (&acc)[2], FA fa, FB fb, int mt, int nt) {
+    const int lane = threadIdx.x & 31, gr = lane >> 2, gc = lane & 3;
+#pragma unroll
+    for (int k0 = 0; k0 < kTile; k0 += 4) dmma8(acc, fa(8 * mt + gr, k0 + gc), fb(k0 + gc, 8 * nt + gr));
+}
+
 // ---------------------------------------------------------------------------------------
 // Cholesky, S = U^T U (upper), right-looking with 32-column panels.
 template <class Sync>
@@ -220,18 +237,21 @@ __device__ bool cholesky(const EighArgs& a, const Sync& sync, Shared& sh, int ct
                 sh.b[k][i] = (k < jb && cj < n) ? ld(U + (j0 + k) + (long long)cj * n) : 0.0;
             }
             __syncthreads();
-            const int i = tid & 31, jq = tid >> 5;
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int k = 0; k < jb; ++k) {
-                const double av = sh.a[k][i];
+            // A22 tile -= U12(:, ti)^T U12(:, tj) on the FP64 tensor cores (rows of the panel past
+            // jb are zero in sh.a / sh.b)
+            const int warp = tid >> 5, lane = tid & 31;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(av, sh.b[k][jq + 8 * q], acc[q]);
-            }
-            const int r = j1 + ti * kTile + i;
+            for (int q = 0; q < 2; ++q) {
+                const int ot = warp + 8 * q, mt = ot & 3, nt = ot >> 2;
+                double acc[2] = {0.0, 0.0};
+                mma_tile32(
+                    acc, [&](int r, int k) { return sh.a[k][r]; }, [&](int k, int c) { return sh.b[k][c]; }, mt, nt);
+                const int r = j1 + ti * kTile + 8 * mt + (lane >> 2);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int c = j1 + tj * kTile + jq + 8 * q;
-                if (r < n && c < n && r <= c) U[r + (long long)c * n] -= acc[q];
+                for (int h = 0; h < 2; ++h) {
+                    const int c = j1 + tj * kTile + 8 * nt + 2 * (lane & 3) + h;
+                    if (r < n && c < n && r <= c) U[r + (long long)c * n] -= acc[h];
+                }
             }
             __syncthreads();
         }
@@ -279,8 +299,9 @@ __device__ bool triangular_inverse(const EighArgs& a, const Sync& sync, Shared& 
         for (int I = cta; I + dgl < nb; I += ncta) {
             const int J = I + dgl;
             const int r0 = I * kTile, c0 = J * kTile;
-            const int i = tid & 31, jq = tid >> 5;
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            const int warp = tid >> 5, lane = tid & 31, gr = lane >> 2, gc = lane & 3;
+            // P = sum_K U[I][K] Ui[K][J] and Ui[I][J] = -Ui[I][I] P on the FP64 tensor cores
+            double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
             for (int K = I + 1; K <= J; ++K) {
                 const int k0 = K * kTile;
                 for (int e = tid; e < kTile * kTile; e += blockDim.x) {
@@ -289,32 +310,38 @@ __device__ bool triangular_inverse(const EighArgs& a, const Sync& sync, Shared& 
                     sh.b[r][c] = (k0 + r < n && c0 + c < n) ? ld(Ui + (k0 + r) + (long long)(c0 + c) * n) : 0.0;
                 }
                 __syncthreads();
-#pragma unroll 8
-                for (int k = 0; k < kTile; ++k) {
-                    const double av = sh.a[i][k];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[q] = fma(av, sh.b[k][jq + 8 * q], acc[q]);
+                for (int q = 0; q < 2; ++q) {
+                    const int ot = warp + 8 * q;
+                    mma_tile32(
+                        acc[q], [&](int r, int k) { return sh.a[r][k]; }, [&](int k, int c) { return sh.b[k][c]; },
+                        ot & 3, ot >> 2);
                 }
                 __syncthreads();
             }
-            // Ui[I][J] = -Ui[I][I] P
 #pragma unroll
-            for (int q = 0; q < 4; ++q) sh.b[i][jq + 8 * q] = acc[q];
+            for (int q = 0; q < 2; ++q) {
+                const int ot = warp + 8 * q, mt = ot & 3, nt = ot >> 2;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) sh.b[8 * mt + gr][8 * nt + 2 * gc + h] = acc[q][h];
+            }
             for (int e = tid; e < kTile * kTile; e += blockDim.x) {
                 const int r = e % kTile, c = e / kTile;
                 sh.a[r][c] = (r0 + r < n && r0 + c < n) ? ld(Ui + (r0 + r) + (long long)(r0 + c) * n) : 0.0;
             }
             __syncthreads();
-            double out[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int k = 0; k < kTile; ++k) {
-                const double av = sh.a[i][k];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) out[q] = fma(av, sh.b[k][jq + 8 * q], out[q]);
-            }
+            for (int q = 0; q < 2; ++q) {
+                const int ot = warp + 8 * q, mt = ot & 3, nt = ot >> 2;
+                double out[2] = {0.0, 0.0};
+                mma_tile32(
+                    out, [&](int r, int k) { return sh.a[r][k]; }, [&](int k, int c) { return sh.b[k][c]; }, mt, nt);
+                const int r = r0 + 8 * mt + gr;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = r0 + i, c = c0 + jq + 8 * q;
-                if (r < n && c < n) Ui[r + (long long)c * n] = -out[q];
+                for (int h = 0; h < 2; ++h) {
+                    const int c = c0 + 8 * nt + 2 * gc + h;
+                    if (r < n && c < n) Ui[r + (long long)c * n] = -out[h];
+                }
             }
             __syncthreads();
         }
