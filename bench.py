@@ -481,15 +481,33 @@ def run_scf(args):
         shells = [(int(a), mol.shell_exponents[o:o + n], mol.shell_coefficients[o:o + n])
                   for a, n, o in zip(mol.shell_atom, mol.shell_nprim, offs)]
         orc = O.VbscfOracle(mol.charges, mol.coords, shells, pattern, 6)
-        t0 = time.perf_counter()
         Er, Cr, _ = orc.solve(C0, gtol=1e-9)
-        dt = time.perf_counter() - t0
-        base = {"value": 1.0 / dt, "unit": "solves/s", "cores": 1, "kind": "port",
-                "sample": f"one oracle solve (scipy L-BFGS-B over the 12 HAO coefficients, gradients by "
-                          f"Richardson central differences of the oracle energy), {dt:.1f} s"}
+        # CPU baseline: the oracle's energy evaluation (structure H/S from the per-pair restatement,
+        # dense eigensolver) timed per call, times the GPU solve's evaluation count; the oracle has
+        # no analytic gradient, so this is a lower bound on a CPU solve's cost
+        reps = 20
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            orc.energy(C)
+        t_eval = (time.perf_counter() - t0) / reps
+        per_solve = t_eval * statistics.mean(evals)
+        base = {"value": 1.0 / per_solve, "unit": "solves/s", "cores": 1, "kind": "port",
+                "sample": f"oracle energy evaluation {1e3 * t_eval:.2f} ms (mean of {reps}) x "
+                          f"{statistics.mean(evals):.0f} evaluations per GPU solve (energy only: no gradient)"}
         E, G = prob.energy_gradient(C)
         parity = {"energy_gpu": res["energy"], "energy_oracle": Er, "abs_diff_Eh": abs(res["energy"] - Er),
                   "gradient_inf_at_solution": float(np.abs(G).max())}
+    # the split-precision RI transform layered onto the solve (FP64 finish below the switch)
+    prob_sp = vbcore.ScfProblem(ctx, mol, pattern, 6)
+    prob_sp.set_precision("bf16x3", 1e-4)
+    res_sp, _ = prob_sp.solve(C0, gradient_tolerance=1e-7)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res_sp, _ = prob_sp.solve(C0, gradient_tolerance=1e-7)
+    split = {"solves_per_s": args.steps / (time.perf_counter() - t0), "switch_gradient": 1e-4,
+             "evaluations": res_sp["evaluations"], "split_evaluations": res_sp["split_evaluations"],
+             "energy_minus_fp64_Eh": res_sp["energy"] - res["energy"], "converged": res_sp["converged"]}
+    prob_sp.close()
     line = {
         "metric": "VBSCF solves/s (H6 6-31G, energy+gradient to convergence)", "value": args.steps / total,
         "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -503,7 +521,7 @@ def run_scf(args):
         "roofline": {"bound": "latency", "note": "20 determinants and 5 structures per evaluation: every kernel "
                      "is launch/latency-bound; time per evaluation "
                      f"{1e3 * total / max(1, sum(evals)):.3f} ms"},
-        "cpu_baseline": base, "parity": parity,
+        "cpu_baseline": base, "parity": parity, "split_precision_solve": split,
         "e2e": {"value": args.steps / total, "unit": "solves/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None},
         "clocks": clocks,

@@ -341,6 +341,15 @@ vb_status vb_scf_energy_gradient(vb_scf_problem* problem, const double* coeffici
  * (run_plbfgs_backend, src/vbscf/optimization/backends/plbfgs.cpp:19-228). */
 vb_status vb_solve_scf(vb_scf_problem* problem, const double* initial_coefficients, const vb_scf_options* options,
                        vb_scf_result* result, double* coefficients_out);
+/* Precision of the per-evaluation RI transform in vb_solve_scf (no counterpart in the reference,
+ * which is FP64 only).  VB_PRECISION_BF16X3: the solve evaluates with the split-precision
+ * transform (vb_active_transform_ri_precision) while the gradient's infinity norm is above
+ * switch_gradient, then re-evaluates the current point in FP64, drops its secant history and
+ * finishes in FP64, so the converged point and energy are those of an FP64 solve to the
+ * gradient tolerance.  VB_PRECISION_FP64 (default) uses FP64 throughout.  *split_evaluations
+ * (vb_scf_problem_split_evaluations) counts the split-precision evaluations of the last solve. */
+vb_status vb_scf_problem_set_precision(vb_scf_problem* problem, int precision, double switch_gradient);
+vb_status vb_scf_problem_split_evaluations(const vb_scf_problem* problem, int32_t* split_evaluations);
 
 /* ---- batched and served work ------------------------------------------------------------------ */
 

@@ -72,6 +72,30 @@ def test_solve_converges_to_the_oracle_minimum(ctx, h6):
     prob.close()
 
 
+def test_split_precision_solve_reaches_the_fp64_minimum(ctx, h6):
+    """The split-precision RI transform layered onto the solve: split-precision evaluations while
+    the gradient is above the switch, then an FP64 finish, so the converged energy is the FP64
+    solve's (1e-9 Eh) and the split evaluations did part of the work."""
+    mol, pattern, oracle = h6
+    C0 = molecules.hao_guess(mol, pattern)
+    ref = vbcore.ScfProblem(ctx, mol, pattern, 6)
+    r64, C64 = ref.solve(C0, max_iterations=300, gradient_tolerance=1e-7)
+    ref.close()
+    prob = vbcore.ScfProblem(ctx, mol, pattern, 6)
+    prob.set_precision("bf16x3", 1e-4)
+    res, C = prob.solve(C0, max_iterations=300, gradient_tolerance=1e-7)
+    assert res["converged"], res
+    assert res["split_evaluations"] > 0 and res["split_evaluations"] < res["evaluations"]
+    assert abs(res["energy"] - r64["energy"]) < 1e-9, (res["energy"], r64["energy"])
+    assert abs(res["energy"] - oracle.energy(C)) < 1e-9
+    # the FP64 evaluation path is restored after the solve
+    E, G = prob.energy_gradient(C)
+    assert abs(E - res["energy"]) < 1e-12 and np.abs(G).max() < 1e-6
+    with pytest.raises(vbcore.VbError):
+        prob.set_precision("bf16x3", -1.0)
+    prob.close()
+
+
 @pytest.mark.parametrize("threshold", [0.0, 1e-12])
 def test_integral_input_matches_shell_input(ctx, h6, threshold):
     """The problem built from AO integrals the caller already has (an AO pair graph's unique

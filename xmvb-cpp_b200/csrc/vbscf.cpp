@@ -289,6 +289,11 @@ struct vb_scf_problem {
     std::vector<double> term_coef;
     vb_hs_plan* plan = nullptr;
     int n_str = 0;
+    // RI transform precision of vb_solve_scf (split until the gradient falls to precision_switch)
+    int precision = VB_PRECISION_FP64;
+    double precision_switch = 0.0;
+    bool split_now = false;
+    int split_evaluations = 0;
     ~vb_scf_problem() {
         if (plan) vb_hs_plan_destroy(plan);
     }
@@ -326,8 +331,15 @@ vb_status evaluate(vb_scf_problem* pr, const std::vector<double>& C, double* ene
             hact[a + (size_t)b * na] = hacc;
         }
     std::vector<double> L((size_t)nc * P), K((size_t)P * (P + 1) / 2), T((size_t)na * nc * nbf);
-    vb_status st = vb_active_transform_ri(pr->ctx, pr->chol.data(), nc, nbf, C.data(), na, VB_MEM_HOST,
-                                          grad ? T.data() : nullptr, L.data(), K.data());
+    vb_status st;
+    if (pr->split_now) {
+        st = vb_active_transform_ri_precision(pr->ctx, pr->chol.data(), nc, nbf, C.data(), na, VB_PRECISION_BF16X3,
+                                              VB_MEM_HOST, grad ? T.data() : nullptr, L.data(), K.data());
+        ++pr->split_evaluations;
+    } else {
+        st = vb_active_transform_ri(pr->ctx, pr->chol.data(), nc, nbf, C.data(), na, VB_MEM_HOST,
+                                    grad ? T.data() : nullptr, L.data(), K.data());
+    }
     if (st != VB_OK) return st;
     const int ns = pr->n_str;
     std::vector<double> Hs((size_t)ns * ns), Ss((size_t)ns * ns);
@@ -611,6 +623,12 @@ vb_status vb_solve_scf(vb_scf_problem* pr, const double* initial_coefficients, c
     };
     std::vector<double> x = pack(C), gfull;
     double f = 0.0;
+    pr->split_evaluations = 0;
+    pr->split_now = pr->precision == VB_PRECISION_BF16X3;
+    struct SplitOff {  // no split evaluation outlives the solve
+        vb_scf_problem* p;
+        ~SplitOff() { p->split_now = false; }
+    } split_off{pr};
     vb_status st = evaluate(pr, unpack(x), &f, &gfull, nullptr, nullptr);
     if (st != VB_OK) return st;
     std::vector<double> g = pack(gfull);
@@ -621,7 +639,17 @@ vb_status vb_solve_scf(vb_scf_problem* pr, const double* initial_coefficients, c
     const int history = std::max(1, opt->history_size);
     const double c1 = opt->armijo > 0.0 ? opt->armijo : 1.0e-4;
     for (int it = 0; it < opt->max_iterations; ++it) {
-        if (inf_norm(g) <= opt->gradient_tolerance) {
+        if (pr->split_now && inf_norm(g) <= std::max(pr->precision_switch, opt->gradient_tolerance)) {
+            // leave split precision: the same point in FP64, a fresh secant history
+            pr->split_now = false;
+            st = evaluate(pr, unpack(x), &f, &gfull, nullptr, nullptr);
+            ++evaluations;
+            if (st != VB_OK) return st;
+            g = pack(gfull);
+            S_hist.clear();
+            Y_hist.clear();
+        }
+        if (!pr->split_now && inf_norm(g) <= opt->gradient_tolerance) {
             res->converged = 1;
             break;
         }
@@ -687,6 +715,14 @@ vb_status vb_solve_scf(vb_scf_problem* pr, const double* initial_coefficients, c
         g = gn;
         f = fn;
     }
+    if (pr->split_now) {
+        // stopped while still in split precision: report the FP64 energy and gradient there
+        pr->split_now = false;
+        st = evaluate(pr, unpack(x), &f, &gfull, nullptr, nullptr);
+        ++evaluations;
+        if (st != VB_OK) return st;
+        g = pack(gfull);
+    }
     if (!res->converged && inf_norm(g) <= opt->gradient_tolerance) res->converged = 1;
     res->energy = f;
     res->gradient_inf = inf_norm(g);
@@ -695,6 +731,21 @@ vb_status vb_solve_scf(vb_scf_problem* pr, const double* initial_coefficients, c
         std::vector<double> full = unpack(x);
         std::copy(full.begin(), full.end(), coefficients_out);
     }
+    return VB_OK;
+}
+
+vb_status vb_scf_problem_set_precision(vb_scf_problem* pr, int precision, double switch_gradient) {
+    if (!pr) return VB_ERR_INVALID;
+    if ((precision != VB_PRECISION_FP64 && precision != VB_PRECISION_BF16X3) || !(switch_gradient >= 0.0))
+        return set_error(pr->ctx, VB_ERR_INVALID, "vb_scf_problem_set_precision: bad arguments");
+    pr->precision = precision;
+    pr->precision_switch = switch_gradient;
+    return VB_OK;
+}
+
+vb_status vb_scf_problem_split_evaluations(const vb_scf_problem* pr, int32_t* split_evaluations) {
+    if (!pr || !split_evaluations) return VB_ERR_INVALID;
+    *split_evaluations = pr->split_evaluations;
     return VB_OK;
 }
 

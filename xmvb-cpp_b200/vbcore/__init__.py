@@ -104,6 +104,7 @@ EXPORTED_SYMBOLS = (
     "vb_engine_evaluate_instances", "vb_engine_submit_scf", "vb_engine_poll", "vb_engine_pending",
     "vb_ao_integrals_s", "vb_scf_problem_create", "vb_scf_problem_create_from_integrals", "vb_scf_problem_destroy",
     "vb_scf_problem_sizes", "vb_scf_ao_integrals", "vb_scf_energy_gradient", "vb_solve_scf",
+    "vb_scf_problem_set_precision", "vb_scf_problem_split_evaluations",
     "vb_autotune_report", "vb_autotune_clear", "vb_ri_pair_factors_frame",
 )
 
@@ -168,6 +169,8 @@ def load_library(path: str = LIB_PATH):
     lib.vb_scf_ao_integrals.argtypes = [P, P, P, P]
     lib.vb_scf_energy_gradient.argtypes = [P, P, c.POINTER(c.c_double), P, P, P]
     lib.vb_solve_scf.argtypes = [P, P, c.POINTER(_ScfOptions), c.POINTER(_ScfResult), P]
+    lib.vb_scf_problem_set_precision.argtypes = [P, c.c_int, c.c_double]
+    lib.vb_scf_problem_split_evaluations.argtypes = [P, c.POINTER(c.c_int32)]
     lib.vb_hs_plan_gradient.argtypes = [P, P, P, P, c.c_int, P, c.c_double, P, P, P, P, c.c_int, P]
     lib.vb_active_transform_ri.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, P, P, P]
     lib.vb_active_transform_ri_precision.argtypes = [P, P, c.c_int, c.c_int, P, c.c_int, c.c_int, c.c_int, P, P, P]
@@ -631,9 +634,17 @@ class ScfProblem:
         res = _ScfResult()
         _check(load_library().vb_solve_scf(self._h, _ptr(Cf), ctypes.byref(opt), ctypes.byref(res), _ptr(out)),
                self.ctx.handle)
+        split = ctypes.c_int32()
+        _check(load_library().vb_scf_problem_split_evaluations(self._h, ctypes.byref(split)), self.ctx.handle)
         return ({"energy": res.energy, "gradient_inf": res.gradient_inf, "iterations": res.iterations,
-                 "evaluations": res.evaluations, "converged": bool(res.converged)},
+                 "evaluations": res.evaluations, "split_evaluations": split.value, "converged": bool(res.converged)},
                 out.reshape(self.n_active, self.n_basis).T.copy())
+
+    def set_precision(self, precision: str = "fp64", switch_gradient: float = 1e-4):
+        """RI transform precision of solve(): "bf16x3" evaluates in split precision until the
+        gradient's infinity norm falls to switch_gradient, then finishes in FP64."""
+        _check(load_library().vb_scf_problem_set_precision(self._h, PRECISIONS[precision], switch_gradient),
+               self.ctx.handle)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
