@@ -285,9 +285,9 @@ cudaError_t launch_factor_project(int np, int R, const double* lf, int ld, const
 }
 
 // Split-K parts of factor_outer: up to kOuterMaxParts CTAs (four per SM, so that enough column
-// loads are in flight), at least 256 spin pairs each.
+// loads are in flight), at least 64 spin pairs (two staged chunks) each.
 int factor_outer_parts(long long cnt) {
-    return (int)std::max<long long>(1, std::min<long long>(kOuterMaxParts, (cnt + 255) / 256));
+    return (int)std::max<long long>(1, std::min<long long>(kOuterMaxParts, (cnt + 63) / 64));
 }
 
 cudaError_t launch_factor_outer(int np, int R, const double* Y, long long ldY, const double* Z, long long ldZ,

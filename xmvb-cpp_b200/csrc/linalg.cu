@@ -672,6 +672,155 @@ __device__ void eigh_body(const EighArgs& a, const Sync& sync, Shared& sh, int c
     }
 }
 
+// Small generalized eigenproblems (n <= kTinyProblem, the structure problems of small active
+// spaces): one warp, everything in shared memory.  Cholesky S = U^T U (lane j owns column j),
+// U^-1, A = U^-T H U^-1, cyclic Jacobi on A with the rotations accumulated in V (lane i updates
+// row/column i of each rotation), then eigenvalues ascending and C = U^-1 V.  Same outputs and
+// info semantics as the cooperative kernel (ctl->info = order of the first non-positive leading
+// minor of S, ctl->sweeps).
+constexpr int kTinyProblem = 32;
+
+__global__ void __launch_bounds__(32) eigh_tiny_kernel(EighArgs a) {
+    __shared__ double sU[kTinyProblem][kTinyProblem + 1];   // S, then U (upper), then U^-1
+    __shared__ double sA[kTinyProblem][kTinyProblem + 1];   // H, then A
+    __shared__ double sV[kTinyProblem][kTinyProblem + 1];
+    __shared__ double sT[kTinyProblem][kTinyProblem + 1];
+    __shared__ double sw[kTinyProblem];
+    __shared__ int sorder[kTinyProblem];
+    const int n = a.n, lane = threadIdx.x;
+    for (int e = lane; e < n * n; e += 32) {
+        const int r = e % n, c = e / n;
+        sU[r][c] = r <= c ? a.S[e] : a.S[c + (long long)r * n];
+        sA[r][c] = r <= c ? a.H[e] : a.H[c + (long long)r * n];
+        sV[r][c] = r == c ? 1.0 : 0.0;
+    }
+    __syncwarp();
+    // Cholesky, right-looking on the upper triangle
+    for (int k = 0; k < n; ++k) {
+        const double d = sU[k][k];
+        if (!(d > 0.0) || !isfinite(d)) {
+            if (lane == 0) a.ctl->info = k + 1;
+            return;
+        }
+        const double u = sqrt(d);
+        __syncwarp();
+        if (lane == k) sU[k][k] = u;
+        if (lane > k && lane < n) sU[k][lane] /= u;
+        __syncwarp();
+        if (lane > k && lane < n)
+            for (int i = k + 1; i <= lane; ++i) sU[i][lane] = fma(-sU[k][i], sU[k][lane], sU[i][lane]);
+        __syncwarp();
+    }
+    for (int e = lane; e < n * n; e += 32) {
+        const int r = e % n, c = e / n;
+        if (r > c) sU[r][c] = 0.0;
+    }
+    __syncwarp();
+    // U^-1 by columns (lane j: column j, back substitution), into sT then back to sU
+    if (lane < n) {
+        const int j = lane;
+        for (int i = n - 1; i >= 0; --i) {
+            double x = i == j ? 1.0 : 0.0;
+            for (int k = i + 1; k <= j; ++k) x = fma(-sU[i][k], sT[k][j], x);
+            sT[i][j] = i <= j ? x / sU[i][i] : 0.0;
+        }
+    }
+    __syncwarp();
+    for (int e = lane; e < n * n; e += 32) sU[e % n][e / n] = sT[e % n][e / n];
+    __syncwarp();
+    // A = U^-T H U^-1 (T = H U^-1, then U^-T T), lane j: column j
+    if (lane < n) {
+        const int j = lane;
+        for (int i = 0; i < n; ++i) {
+            double x = 0.0;
+            for (int k = 0; k <= j; ++k) x = fma(sA[i][k], sU[k][j], x);
+            sT[i][j] = x;
+        }
+    }
+    __syncwarp();
+    if (lane < n) {
+        const int j = lane;
+        for (int i = 0; i < n; ++i) {
+            double x = 0.0;
+            for (int k = 0; k <= i; ++k) x = fma(sU[k][i], sT[k][j], x);
+            sV[i][j] = x;  // A in sV for now
+        }
+    }
+    __syncwarp();
+    for (int e = lane; e < n * n; e += 32) {
+        const int r = e % n, c = e / n;
+        sA[r][c] = 0.5 * (sV[r][c] + sV[c][r]);
+    }
+    __syncwarp();
+    for (int e = lane; e < n * n; e += 32) sV[e % n][e / n] = (e % n) == (e / n) ? 1.0 : 0.0;
+    __syncwarp();
+    // cyclic Jacobi
+    // (an off-diagonal entry below eps sqrt|a_pp a_qq|, or below 1e-17 ||A||_F, is set to zero
+    // instead of rotated; the iteration ends after a sweep without rotations)
+    double fro = 0.0;
+    for (int e = lane; e < n * n; e += 32) fro = fma(sA[e % n][e / n], sA[e % n][e / n], fro);
+    for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
+    const double floor_abs = 1.0e-17 * sqrt(fro);
+    int sweep = 0;
+    for (; sweep < kMaxSweeps; ++sweep) {
+        int rotations = 0;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = sA[p][q];
+                const double app = sA[p][p], aqq = sA[q][q];
+                if (fabs(apq) <= fmax(2.220446049250313e-16 * sqrt(fabs(app * aqq)), floor_abs)) {
+                    __syncwarp();
+                    if (lane == 0) sA[p][q] = sA[q][p] = 0.0;
+                    __syncwarp();
+                    continue;
+                }
+                ++rotations;
+                const double tau = (aqq - app) / (2.0 * apq);
+                const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                const double cs = 1.0 / sqrt(1.0 + t * t), sn = t * cs;
+                __syncwarp();
+                // columns p, q of A and V (lane i: row i)
+                if (lane < n) {
+                    const double aip = sA[lane][p], aiq = sA[lane][q];
+                    sA[lane][p] = cs * aip - sn * aiq;
+                    sA[lane][q] = sn * aip + cs * aiq;
+                    const double vip = sV[lane][p], viq = sV[lane][q];
+                    sV[lane][p] = cs * vip - sn * viq;
+                    sV[lane][q] = sn * vip + cs * viq;
+                }
+                __syncwarp();
+                // rows p, q of A (lane i: column i)
+                if (lane < n) {
+                    const double api = sA[p][lane], aqi = sA[q][lane];
+                    sA[p][lane] = cs * api - sn * aqi;
+                    sA[q][lane] = sn * api + cs * aqi;
+                }
+                __syncwarp();
+            }
+        if (rotations == 0) break;
+    }
+    if (lane == 0) a.ctl->sweeps = sweep;
+    // eigenvalues ascending (rank by comparison, ties by index), C = U^-1 V
+    if (lane < n) {
+        const double li = sA[lane][lane];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+            const double lj = sA[j][j];
+            rank += (lj < li || (lj == li && j < lane)) ? 1 : 0;
+        }
+        sorder[rank] = lane;
+        sw[rank] = li;
+    }
+    __syncwarp();
+    if (lane < n) a.evals[lane] = sw[lane];
+    for (int e = lane; e < n * n; e += 32) {
+        const int r = e % n, c = e / n, src = sorder[c];
+        double x = 0.0;
+        for (int k = r; k < n; ++k) x = fma(sU[r][k], sV[k][src], x);
+        a.evecs[r + (long long)c * n] = x;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) eigh_grid_kernel(EighArgs a) {
     __shared__ Shared sh;
     GridSync sync{a.ctl, gridDim.x, a.spin_limit};
@@ -766,6 +915,11 @@ EighArgs args_for(unsigned char* base, const Layout& L, int n, int mode, const d
 std::mutex g_cooperative;
 
 cudaError_t launch_single(const EighArgs& a, cudaStream_t s, int* grid_out) {
+    if (a.mode == 1 && a.n <= kTinyProblem) {
+        *grid_out = 1;
+        eigh_tiny_kernel<<<1, 32, 0, s>>>(a);
+        return cudaGetLastError();
+    }
     if (a.n <= kSmallProblem) {
         // one CTA: the grid barrier of a one-block launch never waits
         void* params[] = {const_cast<EighArgs*>(&a)};
