@@ -211,6 +211,74 @@ __global__ void __launch_bounds__(1024) factor_pair_kernel(int np, const double*
             lf[(long long)q * ld + slot] = slot < m ? L[(long long)slot_col[slot] * np + q] : 0.0;
 }
 
+// The same factorization for np <= 32 (active spaces of up to 7 orbitals) in one warp: lane i
+// owns row i, the pivot search is a shuffle reduction and the steps need no block barrier.
+__global__ void __launch_bounds__(32) factor_pair_warp_kernel(int np, const double* __restrict__ kfull,
+                                                             int* __restrict__ signs, double* __restrict__ lf,
+                                                             int ld, int* __restrict__ meta, double rel_tol) {
+    __shared__ double sL[32][33];  // column m of the factor in sL[m][.]
+    __shared__ double sig[32];
+    __shared__ int slot_col[32];
+    const int lane = threadIdx.x;
+    double dg = lane < np ? __ldg(kfull + (long long)lane * np + lane) : 0.0;
+    bool used = lane >= np;
+    auto argmax = [&](int* p, double* piv) {
+        double best = used ? -1.0 : fabs(dg), bd = dg;
+        int bi = used ? -1 : lane;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            const double od = __shfl_xor_sync(0xffffffffu, bd, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi >= 0 && (bi < 0 || oi < bi))) {
+                best = ov;
+                bd = od;
+                bi = oi;
+            }
+        }
+        *p = bi;
+        *piv = bd;
+    };
+    int p;
+    double piv;
+    argmax(&p, &piv);
+    const double cut = rel_tol * fmax(fabs(piv), 0.0);
+    int m = 0;
+    for (; m < np; ++m) {
+        if (p < 0 || !(fabs(piv) > cut) || piv == 0.0) break;
+        const double inv = rsqrt(fabs(piv));
+        const double sgn = piv > 0.0 ? 1.0 : -1.0;
+        double v = 0.0;
+        if (!used) {
+            double acc = __ldg(kfull + (long long)p * np + lane);
+            for (int q = 0; q < m; ++q) acc = fma(-sig[q] * sL[q][p], sL[q][lane], acc);
+            v = acc * inv;
+            if (lane == p)
+                used = true;
+            else
+                dg = fma(-sgn * v, v, dg);
+        }
+        sL[m][lane] = v;
+        if (lane == 0) {
+            sig[m] = sgn;
+            signs[m] = (int)sgn;
+        }
+        __syncwarp();
+        argmax(&p, &piv);
+    }
+    if (lane == 0) {
+        int pos = 0;
+        for (int c = 0; c < m; ++c) pos += sig[c] > 0.0 ? 1 : 0;
+        int ip = 0, in = pos;
+        for (int c = 0; c < m; ++c) slot_col[sig[c] > 0.0 ? ip++ : in++] = c;
+        meta[0] = pos;
+        meta[1] = m - pos;
+    }
+    __syncwarp();
+    for (int q = 0; q < np; ++q)
+        for (int slot = lane; slot < ld; slot += 32)
+            lf[(long long)q * ld + slot] = slot < m ? sL[slot_col[slot]][q] : 0.0;
+}
+
 // Listed blocks (or all blocks): one thread per block resolves it by the exact path; its first
 // cofactors A go to the lane's shared slot (k^2 doubles).  The warp then treats its 32 blocks one
 // at a time: the u-vectors of the records with the factor columns split over lanes, and, for
@@ -527,6 +595,10 @@ __global__ void same_spin_list_kernel(int n, int k, long long batch, const int* 
 
 cudaError_t launch_factor_pair_kernel(int np, const double* kfull, double* work, double* cols, int* signs, double* lf,
                                       int ld, int* meta, cudaStream_t stream) {
+    if (np <= 32) {
+        factor_pair_warp_kernel<<<1, 32, 0, stream>>>(np, kfull, signs, lf, ld, meta, factor_tolerance(np));
+        return cudaGetLastError();
+    }
     int threads = (np + 31) / 32 * 32;
     threads = threads < 64 ? 64 : (threads > 1024 ? 1024 : threads);
     if (np > threads * kFactorRows) return cudaErrorInvalidValue;
@@ -568,7 +640,7 @@ size_t exact_stack_bytes() {
 cudaError_t preload_spin_pair_kernels() {
     // cudaFuncGetAttributes loads a function that lazy module loading has not loaded yet
     const void* fns[] = {(const void*)prepare_tables_kernel, (const void*)factor_pair_kernel<true>,
-                         (const void*)factor_pair_kernel<false>,
+                         (const void*)factor_pair_kernel<false>, (const void*)factor_pair_warp_kernel,
                          (const void*)spin_pairs_exact<7, 7>, (const void*)spin_pairs_exact<8, 0>,
                          (const void*)spin_pairs_exact<dev::KMAX, 0>};
     for (const void* f : fns) {

@@ -342,30 +342,55 @@ vb_status evaluate(vb_scf_problem* pr, const std::vector<double>& C, double* ene
     }
     if (st != VB_OK) return st;
     const int ns = pr->n_str;
-    std::vector<double> Hs((size_t)ns * ns), Ss((size_t)ns * ns);
-    st = vb_hs_plan_execute(pr->plan, Sact.data(), hact.data(), K.data(), VB_MEM_HOST, Hs.data(), Ss.data());
-    if (st != VB_OK) return st;
-    std::vector<double> w(ns), V((size_t)ns * ns);
-    int info = 0;
-    if (ns <= kDenseStructureLimit) {
-        st = vb_generalized_eigh(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, w.data(), V.data(), &info);
-    } else {
-        int its = 0;
-        st = vb_lowest_root(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, 1.0e-11, 2000, w.data(), V.data(), &its);
+    std::vector<double> F;  // pair factors F = L^T (P x n_chol), the gradient's RI input
+    if (grad) {
+        F.resize((size_t)P * nc);
+        for (int c = 0; c < nc; ++c)
+            for (int q = 0; q < P; ++q) F[q + (size_t)c * P] = L[c + (size_t)nc * q];
     }
-    if (st != VB_OK) return st;
-    *energy = w[0] + pr->ao.enuc;
-    if (Hs_out) *Hs_out = Hs;
-    if (Ss_out) *Ss_out = Ss;
-    if (!grad) return VB_OK;
-    // gradient with respect to S_act, h_act and the pair factors F = L^T (P x n_chol)
-    std::vector<double> F((size_t)P * nc);
-    for (int c = 0; c < nc; ++c)
-        for (int q = 0; q < P; ++q) F[q + (size_t)c * P] = L[c + (size_t)nc * q];
-    std::vector<double> gS((size_t)na * na), gh((size_t)na * na), gF((size_t)P * nc);
-    st = vb_hs_plan_gradient(pr->plan, Sact.data(), hact.data(), K.data(), VB_MEM_HOST, V.data(), w[0], gS.data(),
-                             gh.data(), nullptr, F.data(), nc, gF.data());
-    if (st != VB_OK) return st;
+    std::vector<double> gS, gh, gF;
+    double root = 0.0;
+    if (!Hs_out && !Ss_out) {
+        // structure H/S stay on the device: root and gradient in one call
+        if (grad) {
+            gS.resize((size_t)na * na);
+            gh.resize((size_t)na * na);
+            gF.resize((size_t)P * nc);
+        }
+        st = vb_hs_plan_root_gradient(pr->plan, Sact.data(), hact.data(), K.data(), 1.0e-11, &root, nullptr,
+                                      grad ? gS.data() : nullptr, grad ? gh.data() : nullptr,
+                                      grad ? F.data() : nullptr, nc, grad ? gF.data() : nullptr);
+        if (st != VB_OK) return st;
+        *energy = root + pr->ao.enuc;
+        if (!grad) return VB_OK;
+    }
+    std::vector<double> Hs, Ss;
+    if (Hs_out || Ss_out) {
+        Hs.resize((size_t)ns * ns);
+        Ss.resize((size_t)ns * ns);
+        st = vb_hs_plan_execute(pr->plan, Sact.data(), hact.data(), K.data(), VB_MEM_HOST, Hs.data(), Ss.data());
+        if (st != VB_OK) return st;
+        std::vector<double> w(ns), V((size_t)ns * ns);
+        int info = 0;
+        if (ns <= kDenseStructureLimit) {
+            st = vb_generalized_eigh(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, w.data(), V.data(), &info);
+        } else {
+            int its = 0;
+            st = vb_lowest_root(pr->ctx, Hs.data(), Ss.data(), ns, VB_MEM_HOST, 1.0e-11, 2000, w.data(), V.data(), &its);
+        }
+        if (st != VB_OK) return st;
+        *energy = w[0] + pr->ao.enuc;
+        if (Hs_out) *Hs_out = Hs;
+        if (Ss_out) *Ss_out = Ss;
+        if (!grad) return VB_OK;
+        // gradient with respect to S_act, h_act and the pair factors F
+        gS.resize((size_t)na * na);
+        gh.resize((size_t)na * na);
+        gF.resize((size_t)P * nc);
+        st = vb_hs_plan_gradient(pr->plan, Sact.data(), hact.data(), K.data(), VB_MEM_HOST, V.data(), w[0], gS.data(),
+                                 gh.data(), nullptr, F.data(), nc, gF.data());
+        if (st != VB_OK) return st;
+    }
     // dE/dC = 2 S_ao C G_S + 2 h_ao C G_h + RI adjoint of dE/dL
     std::vector<double> gL((size_t)nc * P), gC((size_t)nbf * na);
     for (int c = 0; c < nc; ++c)
