@@ -270,15 +270,36 @@ def expand_structures(rows: np.ndarray, n_active_electrons: int, spin_multiplici
 # device context and the H/S plan
 
 
+_LIVE_CONTEXTS = None
+
+
+def _close_live_contexts():
+    """At interpreter exit: close every open context and the objects built on it, children first,
+    while the native library and the CUDA runtime are still up."""
+    for ctx in list(_LIVE_CONTEXTS or ()):
+        try:
+            ctx.close()
+        except Exception:
+            pass
+
+
 class Context:
     """One device, one stream, an HBM budget (xmvb::cuda::Context of the reference)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        global _LIVE_CONTEXTS
         lib = load_library()
         h = ctypes.c_void_p()
         _check(lib.vb_context_create(device, hbm_budget_bytes, ctypes.byref(h)))
         self._h = h
         self.device = device
+        if _LIVE_CONTEXTS is None:
+            import atexit
+            import weakref
+
+            _LIVE_CONTEXTS = weakref.WeakSet()
+            atexit.register(_close_live_contexts)
+        _LIVE_CONTEXTS.add(self)
 
     @property
     def handle(self):
