@@ -44,7 +44,7 @@ def test_structure_matrices_match_golden(ctx, name):
 
 
 @pytest.mark.parametrize("kw,n,seed", [("COV", 8, 1), ("COV", 10, 2), ("COV", 12, 3), ("COV ION(1)", 8, 4),
-                                       ("COV ION(1)", 6, 5), ("FULL", 6, 6)])
+                                       ("COV ION(1)", 6, 5), ("FULL", 6, 6), ("COV ION(1)", 10, 7)])
 def test_structure_matrices_match_oracle(ctx, kw, n, seed):
     S, h, eri = workloads.active_space(n, 3 * n, seed)
     plan, ex = _plan(ctx, kw, n, n)
