@@ -466,9 +466,9 @@ vb_status vb_autotune_clear(void);
  * call: it raises the device's stack limit to what the exact-path kernels need (later calls
  * then never make the runtime grow the local-memory reservation), loads every kernel a call may
  * launch (lazy module loading then places no code in device memory during a later call) and
- * looks up the scratch array's address (cudaGetSymbolAddress).  Make that first call before
- * any stream capture.  Calls share the array and keep its last contents;
- * calls that overlap on the GPU race on it. */
+ * looks up the scratch array's address (cudaGetSymbolAddress).  No call can be recorded into
+ * a CUDA graph: each one synchronizes its stream.  Calls share the array and keep its last
+ * contents; calls that overlap on the GPU race on it. */
 vb_status vb_spin_pairs_noalloc(void* cuda_stream, int n_orbitals, int k, int n_strings, const uint64_t* strings,
                                 const double* ovlp_act, const double* h1e_act, const double* eri_packed,
                                 double* out_scalars);
