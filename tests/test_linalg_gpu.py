@@ -160,7 +160,8 @@ def test_lowest_root_random(ctx):
 def test_grid_barrier_timeout_is_reported_and_the_context_stays_usable():
     """The cooperative solver's grid barrier gives up after a bounded number of polls: with a
     one-poll limit the waits run out, the kernel ends and the call returns VB_ERR_TIMEOUT (no
-    trap, no hang); after the default limit is restored the same context solves the problem."""
+    trap, no hang); after the default limit is restored the same context solves the problem.
+    The blocked Cholesky above the one-CTA size has no grid barrier: the limit does not touch it."""
     c = vbcore.Context(0)
     try:
         n = 200  # above the one-CTA size: a grid-wide cooperative launch with a grid barrier
@@ -170,9 +171,8 @@ def test_grid_barrier_timeout_is_reported_and_the_context_stays_usable():
         with pytest.raises(vbcore.VbError) as e:
             vbcore.generalized_eigh(c, H, S)
         assert e.value.status == 6 and "grid barrier timed out" in str(e.value)
-        with pytest.raises(vbcore.VbError) as e:
-            vbcore.metric_cholesky(c, S)
-        assert e.value.status == 6
+        U = vbcore.metric_cholesky(c, S)
+        assert np.abs(U - O.metric_cholesky(S)).max() < 1e-12
         c.set_barrier_spin_limit(0)
         w, _ = vbcore.generalized_eigh(c, H, S)
         wr, _ = O.generalized_eigh(H, S)

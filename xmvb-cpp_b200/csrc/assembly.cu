@@ -100,8 +100,24 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
     if (rows > a.n_det) rows = a.n_det;
     const int ntiles = (int)((rows + kBandTileRows - 1) / kBandTileRows);
     const int seg_max = a.seg_max;
+    // the group's row tiles with terms (ascending), up to the last one this column block reaches
+    const int* tl = a.seg_tiles + a.seg_tile_off[g];
+    int nt = a.seg_tile_off[g + 1] - a.seg_tile_off[g];
+    {
+        int lo = 0, hi = nt;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (tl[mid] < ntiles)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        nt = lo;
+    }
 
-    auto issue = [&](int t, int st) {
+    // stage st <- the i-th listed tile
+    auto issue = [&](int i, int st) {
+        const int t = tl[i];
         unsigned char* base = bsm + (size_t)st * stage_bytes;
         const long long seg = (long long)g * a.n_tiles + t;
         const long long o0 = a.seg_off[seg];
@@ -123,10 +139,10 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
     }
     __syncthreads();
     int issued = 0;  // tiles issued so far (thread 0)
-    if (tid == 0) {
+    if (tid == 0 && nt > 0) {
         issue(0, 0);
-        if (ntiles > 1) issue(1, 1);
-        issued = ntiles > 1 ? 2 : 1;
+        if (nt > 1) issue(1, 1);
+        issued = nt > 1 ? 2 : 1;
     }
     double acc_h[kBandSlots], acc_s[kBandSlots];
 #pragma unroll
@@ -137,12 +153,12 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
     // polls of up to ~1 us each (0 when the context's limit is below 16: the first wait gives up
     // at once, which is how the timeout path is exercised)
     const long long limit = a.spin_limit / 16;
-    bool ok = __syncthreads_and(mbar_wait(&full[0], 0u, limit)) != 0;
-    int t = 0;
-    for (; ok && t < ntiles; ++t) {
-        const int st = t & 1;
+    bool ok = nt == 0 || __syncthreads_and(mbar_wait(&full[0], 0u, limit)) != 0;
+    int i = 0;
+    for (; ok && i < nt; ++i) {
+        const int st = i & 1;
         unsigned char* base = bsm + (size_t)st * stage_bytes;
-        const long long r0 = (long long)t * kBandTileRows;
+        const long long r0 = (long long)tl[i] * kBandTileRows;
         if (r0 + kBandTileRows - 1 > a.e0 + col0) {
             // rows below the diagonal of this column block hold no data: zero them
             double* zH = reinterpret_cast<double*>(base);
@@ -178,11 +194,11 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
             }
             q -= (n & 1);
         }
-        const bool next = t + 1 >= ntiles || mbar_wait(&full[st ^ 1], (unsigned)((t + 1) >> 1) & 1u, limit);
+        const bool next = i + 1 >= nt || mbar_wait(&full[st ^ 1], (unsigned)((i + 1) >> 1) & 1u, limit);
         ok = __syncthreads_and(next) != 0;
-        if (ok && tid == 0 && t + 2 < ntiles) {
+        if (ok && tid == 0 && i + 2 < nt) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(t + 2, st);
+            issue(i + 2, st);
             ++issued;
         }
     }
@@ -191,7 +207,7 @@ __global__ void __launch_bounds__(kBandWarps * 32, 3)
         // its own: no copy may outlive the CTA), and leave
         if (tid == 0) {
             atomicExch(a.error, 1);
-            for (int u = t; u < issued; ++u) mbar_wait(&full[u & 1], (unsigned)(u >> 1) & 1u, kDrainPolls);
+            for (int u = i; u < issued; ++u) mbar_wait(&full[u & 1], (unsigned)(u >> 1) & 1u, kDrainPolls);
         }
         __syncthreads();
         return;

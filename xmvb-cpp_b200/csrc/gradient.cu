@@ -11,7 +11,10 @@
 //   1. det_pair_adjoint_kernel: every determinant pair (d <= e) scatters its weight onto the
 //      two spin-pair records it was built from (H_de = H_a S_b + H_b S_a + sum_m s_m u_a u_b):
 //      adj(det_a) += w (H_b - lambda S_b), adj(H_a) += w S_b, adj(u_a[m]) += w s_m u_b[m], and
-//      the same with a <-> b.
+//      the same with a <-> b.  With a spin-flip symmetric determinant list the scatter is grouped
+//      by alpha record (det_pair_adjoint_flip_kernel, no atomics), and in two stages through a
+//      per-alpha-string table in shared memory when alpha strings carry several determinants
+//      (det_pair_adjoint_two_stage_kernel).
 //   2. spin_backward_kernel<K>: per spin pair, with X = S[R, L], B = X^-1 and d = det X:
 //      det = d, A = d B^T, H_1 = <h[R, L], A>, H_2 = d q(B) (q: the same-spin two-electron form
 //      in B), u[m] = <l_m[pair(R, L)], A>.  The adjoint with respect to X is
@@ -24,8 +27,8 @@
 //      block's singular value decomposition (products of singular values only, no inverse;
 //      see svd_frame_adjoint).
 // The two contractions over the R factor columns (adj_u . l_m at each packed pair, and the
-// factor-column adjoint sum_t adj_u (x) A-scatter) run as FP64 GEMMs (cuBLAS) over chunks of
-// records around the backward kernel, which walks left-string work items like the forward
+// factor-column adjoint sum_t adj_u (x) A-scatter) run on the FP64 tensor cores (dgemm.cu) over
+// chunks of records around the backward kernel, which walks left-string work items like the forward
 // kernel and accumulates the two-electron table per left string in shared memory.  The host
 // then maps the two-electron table and factor-column adjoints onto the packed integrals
 // (full-rank pair kernel) or onto caller-supplied RI factors.
@@ -158,6 +161,92 @@ __global__ void __launch_bounds__(256) det_pair_adjoint_flip_kernel(AdjArgs a, c
             adj[R + 1] += 2.0 * acc_h;
         }
     }
+}
+
+// Determinant weights and beta strings in alpha-string order (the order of alpha_dets).
+__global__ void alpha_order_kernel(long long n_det, const int* __restrict__ adets, const double* __restrict__ w,
+                                   const int* __restrict__ det_beta, double* __restrict__ ws, int* __restrict__ bs) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n_det;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int d = __ldg(adets + k);
+        ws[k] = __ldg(w + d);
+        bs[k] = __ldg(det_beta + d);
+    }
+}
+
+// The record adjoint of det_pair_adjoint_flip_kernel in two stages per alpha string i, for plans
+// whose alpha strings carry several determinants each (D = n_det / Na of them on average: the
+// one-stage form gathers D^2 beta records per alpha record, this one about 2 D):
+//   T_i[b][c] = sum_{d in D_i} w_d val_c(rec(beta_d, b))                for every beta string b,
+//   adj[(i, j)][c] += 2 pair_w sum_{e in D_j} w_e T_i[beta_e][c]        for every j >= i,
+// with val_m = s_m u[m] (m < R), val_R = H - lambda S, val_{R+1} = S.  T_i lives in shared
+// memory; one CTA per (alpha string i, chunk of CC record components), every adjoint entry is
+// written by one thread and every sum runs in a fixed order.  ws / bs: weights and beta strings in
+// alpha_dets order (alpha_order_kernel).
+template <int CC>
+__global__ void __launch_bounds__(256) det_pair_adjoint_two_stage_kernel(AdjArgs a, const int* __restrict__ aoff,
+                                                                         const double* __restrict__ ws,
+                                                                         const int* __restrict__ bs) {
+    extern __shared__ double sT[];  // Nb x CC
+    const int i = blockIdx.x;
+    const int c0 = blockIdx.y * CC;
+    const int R = a.f.R, r_pos = a.f.r_pos;
+    const int ncomp = R + 2;
+    const int Nb = a.f.Nb;
+    const int i0 = __ldg(aoff + i), i1 = __ldg(aoff + i + 1);
+    if (i0 == i1) return;
+    for (int t = threadIdx.x; t < Nb * CC; t += blockDim.x) {
+        const int b = t / CC, c = c0 + t % CC;
+        double acc = 0.0;
+        if (c < ncomp) {
+            const double sign = c < r_pos ? 1.0 : -1.0;
+#pragma unroll 4
+            for (int k = i0; k < i1; ++k) {
+                const int bd = __ldg(bs + k);
+                const double* rb = a.f.rec_b + record_index(min(bd, b), max(bd, b), Nb) * a.f.stride_b;
+                double v;
+                if (c < R)
+                    v = sign * __ldg(rb + c);
+                else if (c == R)
+                    v = __ldg(rb + R + 1) - a.lambda * __ldg(rb + R);
+                else
+                    v = __ldg(rb + R);
+                acc = fma(__ldg(ws + k), v, acc);
+            }
+        }
+        sT[t] = acc;
+    }
+    __syncthreads();
+    const long long Na = a.f.Na;
+    const long long items = (Na - i) * CC;
+    for (long long t = threadIdx.x; t < items; t += blockDim.x) {
+        const int j = i + (int)(t / CC), cl = (int)(t % CC), c = c0 + cl;
+        if (c >= ncomp) continue;
+        const int j0 = __ldg(aoff + j), j1 = __ldg(aoff + j + 1);
+        double acc = 0.0;
+        for (int k = j0; k < j1; ++k) acc = fma(__ldg(ws + k), sT[__ldg(bs + k) * CC + cl], acc);
+        const double pair_w = j == i ? 1.0 : 2.0;
+        double* adj = a.adj_a + record_index(i, j, Na) * a.adj_stride;
+        adj[c] += 2.0 * pair_w * acc;
+    }
+}
+
+// Record-component chunk of the two-stage adjoint for Nb beta strings (shared memory Nb x CC
+// doubles, at most 100 KB so that two CTAs share an SM), 0 when even 4 components do not fit.
+int two_stage_chunk(long long Nb) {
+    for (int cc : {16, 8, 4})
+        if ((size_t)Nb * cc * sizeof(double) <= 100u * 1024u) return cc;
+    return 0;
+}
+
+template <int CC>
+cudaError_t launch_two_stage(const AdjArgs& a, const int* aoff, const double* ws, const int* bs, cudaStream_t s) {
+    const size_t smem = sizeof(double) * (size_t)a.f.Nb * CC;
+    cudaError_t err = allow_dynamic_smem((const void*)det_pair_adjoint_two_stage_kernel<CC>, smem);
+    if (err != cudaSuccess) return err;
+    const dim3 grid((unsigned)a.f.Na, (unsigned)((a.f.R + 2 + CC - 1) / CC));
+    det_pair_adjoint_two_stage_kernel<CC><<<grid, 256, smem, s>>>(a, aoff, ws, bs);
+    return cudaGetLastError();
 }
 
 __global__ void __launch_bounds__(256) det_pair_adjoint_kernel(AdjArgs a) {
@@ -858,13 +947,21 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
     // scratch: w, coefficients, adjoint records, gradient accumulators
     const size_t n_gS = (size_t)n * n, n_gG = (size_t)std::max(gd, 1) * std::max(gd, 1), n_gL = (size_t)np * np;
     const size_t acc_doubles = 2 * n_gS + n_gG + n_gL;
-    if ((st = p->grad_acc.allocate(ctx, sizeof(double) * (acc_doubles + p->n_det + p->n_str))) != VB_OK) return st;
+    // the two-stage record adjoint when alpha strings carry four or more determinants on average
+    const bool flip_adjoint = p->has_flip && p->shared_tables && p->ka > 0 && p->R <= 128;
+    const int chunk = flip_adjoint && p->n_det >= 4LL * p->Na ? two_stage_chunk(p->Nb) : 0;
+    const size_t order_doubles = chunk ? (size_t)p->n_det + ((size_t)p->n_det + 1) / 2 : 0;
+    if ((st = p->grad_acc.allocate(ctx, sizeof(double) * (acc_doubles + p->n_det + p->n_str + order_doubles))) !=
+        VB_OK)
+        return st;
     double* gS = p->grad_acc.as<double>();
     double* gh = gS + n_gS;
     double* gG = gh + n_gS;
     double* gL = gG + n_gG;
     double* w = gL + n_gL;
     double* cdev = w + p->n_det;
+    double* ws = cdev + p->n_str;
+    int* bs = reinterpret_cast<int*>(ws + p->n_det);
     const long long adj_a_n = std::max(1LL, p->npairs_a) * adj_stride;
     const long long adj_b_n = p->shared_tables ? 0 : std::max(1LL, p->npairs_b) * adj_stride;
     if ((st = p->adj_a.allocate(ctx, sizeof(double) * adj_a_n)) != VB_OK) return st;
@@ -888,11 +985,24 @@ extern "C" vb_status vb_hs_plan_gradient(vb_hs_plan* p, const double* S, const d
     aa.adj_b = p->shared_tables ? p->adj_a.as<double>() : p->adj_b.as<double>();
     aa.adj_stride = adj_stride;
     if (err == cudaSuccess) {
-        if (p->has_flip && p->shared_tables && p->ka > 0 && p->R <= 128)
-            det_pair_adjoint_flip_kernel<<<148 * 8, 256, 0, s>>>(aa, p->alpha_off.as<int>(), p->alpha_dets.as<int>());
-        else
-            det_pair_adjoint_kernel<<<148 * 8, 256, 0, s>>>(aa);
-        err = cudaGetLastError();
+        if (chunk) {
+            alpha_order_kernel<<<(unsigned)std::min<long long>(4096, (p->n_det + 255) / 256), 256, 0, s>>>(
+                p->n_det, p->alpha_dets.as<int>(), w, p->det_beta.as<int>(), ws, bs);
+            err = cudaGetLastError();
+            if (err == cudaSuccess) {
+                const int* aoff = p->alpha_off.as<int>();
+                err = chunk == 16 ? launch_two_stage<16>(aa, aoff, ws, bs, s)
+                      : chunk == 8 ? launch_two_stage<8>(aa, aoff, ws, bs, s)
+                                   : launch_two_stage<4>(aa, aoff, ws, bs, s);
+            }
+        } else {
+            if (flip_adjoint)
+                det_pair_adjoint_flip_kernel<<<148 * 8, 256, 0, s>>>(aa, p->alpha_off.as<int>(),
+                                                                     p->alpha_dets.as<int>());
+            else
+                det_pair_adjoint_kernel<<<148 * 8, 256, 0, s>>>(aa);
+            err = cudaGetLastError();
+        }
     }
     // split-K partials of the factor-column adjoint (one R x np block per CTA of factor_outer)
     DeviceBuffer partial;

@@ -36,6 +36,18 @@ vb_status upload(vb_context* ctx, DeviceBuffer& buf, const void* src, size_t byt
 
 namespace {
 
+// Determinant indices of the caller's list -> the plan's order (indices outside the list pass
+// through unchanged, as they would without a reorder).
+__global__ void translate_pairs_kernel(long long count, const long long* __restrict__ in,
+                                       const long long* __restrict__ position, long long n_det,
+                                       long long* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long d = in[i];
+        out[i] = (d >= 0 && d < n_det) ? position[d] : d;
+    }
+}
+
 std::vector<uint64_t> occupation_rows(const uint64_t* masks, int count, int k, int n, std::string* error) {
     std::vector<uint64_t> rows(2 * (size_t)count, ~uint64_t{0});
     for (int s = 0; s < count; ++s) {
@@ -144,6 +156,71 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
     for (long long t = 0; t < n_terms; ++t)
         if (ex->term_structure[t] < 0 || ex->term_structure[t] >= p->n_str)
             return fail(set_error(ctx, VB_ERR_INVALID, "term structure index out of range"));
+
+    // Determinant order.  Structures that share few determinants (ionic structures: determinants
+    // cluster by occupation pattern) leave each band-reduction structure group reading a row tile
+    // for a handful of its rows.  Placing every determinant at the first structure that uses it
+    // makes the determinants of consecutive structures contiguous; the reorder is taken when it at
+    // least halves the (structure group, row tile) segments.  Everything the plan computes is per
+    // structure or per spin string, so only vb_hs_plan_determinant_pairs translates indices.
+    std::vector<int32_t> r_alpha, r_beta, r_str;
+    std::vector<int64_t> r_off;
+    std::vector<double> r_coef;
+    vb_expansion reordered;
+    {
+        const long long nd = p->n_det;
+        std::vector<long long> first(nd, (long long)p->n_str);
+        for (long long d = 0; d < nd; ++d)
+            for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t)
+                first[d] = std::min<long long>(first[d], ex->term_structure[t]);
+        std::vector<long long> order(nd);
+        for (long long d = 0; d < nd; ++d) order[d] = d;
+        // within a structure group's range, determinants stay in alpha-major order (the spin-pair
+        // records of neighbouring determinant pairs stay neighbours)
+        std::stable_sort(order.begin(), order.end(), [&](long long x, long long y) {
+            const long long gx = first[x] / kBandGroup, gy = first[y] / kBandGroup;
+            if (gx != gy) return gx < gy;
+            if (ex->det_alpha[x] != ex->det_alpha[y]) return ex->det_alpha[x] < ex->det_alpha[y];
+            return ex->det_beta[x] < ex->det_beta[y];
+        });
+        std::vector<long long> pos(nd);
+        for (long long i = 0; i < nd; ++i) pos[order[i]] = i;
+        const long long tiles = (nd + kBandTileRows - 1) / kBandTileRows;
+        auto segments = [&](bool moved) {
+            std::vector<long long> keys;
+            keys.reserve((size_t)n_terms);
+            for (long long d = 0; d < nd; ++d)
+                for (long long t = ex->term_offsets[d]; t < ex->term_offsets[d + 1]; ++t)
+                    keys.push_back((long long)(ex->term_structure[t] / kBandGroup) * tiles +
+                                   (moved ? pos[d] : d) / kBandTileRows);
+            std::sort(keys.begin(), keys.end());
+            return (long long)(std::unique(keys.begin(), keys.end()) - keys.begin());
+        };
+        if (2 * segments(true) <= segments(false)) {
+            r_alpha.resize(nd);
+            r_beta.resize(nd);
+            r_off.assign(nd + 1, 0);
+            r_str.resize(n_terms);
+            r_coef.resize(n_terms);
+            for (long long i = 0; i < nd; ++i) {
+                const long long d = order[i];
+                r_alpha[i] = ex->det_alpha[d];
+                r_beta[i] = ex->det_beta[d];
+                const long long t0 = ex->term_offsets[d], cnt = ex->term_offsets[d + 1] - t0;
+                std::copy(ex->term_structure + t0, ex->term_structure + t0 + cnt, r_str.begin() + r_off[i]);
+                std::copy(ex->term_coefficient + t0, ex->term_coefficient + t0 + cnt, r_coef.begin() + r_off[i]);
+                r_off[i + 1] = r_off[i] + cnt;
+            }
+            reordered = *ex;
+            reordered.det_alpha = r_alpha.data();
+            reordered.det_beta = r_beta.data();
+            reordered.term_offsets = r_off.data();
+            reordered.term_structure = r_str.data();
+            reordered.term_coefficient = r_coef.data();
+            ex = &reordered;
+            p->det_position = std::move(pos);
+        }
+    }
 
     std::string err;
     std::vector<uint64_t> occa, occb;
@@ -305,6 +382,7 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
         std::vector<double> coef;
         std::vector<unsigned char> row;
         std::vector<long long> cur(soff.begin(), soff.end() - 1);  // next term of each structure
+        std::vector<int> tiles, tile_off(b.n_groups + 1, 0);
         for (int g = 0; g < b.n_groups; ++g)
             for (int t = 0; t < b.n_tiles; ++t) {
                 const size_t seg = (size_t)g * b.n_tiles + t;
@@ -327,6 +405,8 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
                         within += cnt;
                     }
                 }
+                if (within > 0) tiles.push_back(t);
+                tile_off[g + 1] = (int)tiles.size();
                 while (coef.size() % 16) {
                     coef.push_back(0.0);
                     row.push_back(0);
@@ -334,6 +414,9 @@ vb_status vb_hs_plan_create(vb_context* ctx, const vb_expansion* ex, vb_hs_plan*
                 b.seg_max = std::max(b.seg_max, (int)((long long)coef.size() - off[seg]));
             }
         off[nseg] = (long long)coef.size();
+        if ((st = upload(ctx, b.tiles, tiles.data(), sizeof(int) * std::max<size_t>(1, tiles.size()))) != VB_OK)
+            return fail(st);
+        if ((st = upload(ctx, b.tile_off, tile_off.data(), sizeof(int) * tile_off.size())) != VB_OK) return fail(st);
         if ((st = upload(ctx, b.off, off.data(), sizeof(long long) * off.size())) != VB_OK) return fail(st);
         if ((st = upload(ctx, b.meta, meta.data(), std::max<size_t>(16, meta.size()))) != VB_OK) return fail(st);
         if ((st = upload(ctx, b.coef, coef.data(), sizeof(double) * std::max<size_t>(1, coef.size()))) != VB_OK)
@@ -570,6 +653,8 @@ vb_status execute_impl(vb_hs_plan* p, const double* S, const double* h, const do
             ba.seg_meta = p->segments.meta.as<unsigned char>();
             ba.term_c = p->segments.coef.as<double>();
             ba.term_d = p->segments.row.as<unsigned char>();
+            ba.seg_tiles = p->segments.tiles.as<int>();
+            ba.seg_tile_off = p->segments.tile_off.as<int>();
             ba.error = reinterpret_cast<int*>(p->counters.as<unsigned long long>() + 7);
             ba.spin_limit = ctx->barrier_spin_limit > 0 ? ctx->barrier_spin_limit : (1ll << 26);
             ba.Zh = scr[2];
@@ -742,6 +827,25 @@ vb_status vb_hs_plan_determinant_pairs(vb_hs_plan* p, const double* S, const dou
     DeviceBuffer dp, dh_o, ds_o;
     const long long* pp = reinterpret_cast<const long long*>(pairs);
     double *ho = h_out, *so = s_out;
+    std::vector<int64_t> moved;
+    if (mem == VB_MEM_HOST && !p->det_position.empty()) {
+        // the caller's determinant indices -> the plan's order
+        moved.resize((size_t)(2 * n_pairs));
+        for (int64_t i = 0; i < 2 * n_pairs; ++i) moved[i] = p->det_position[pairs[i]];
+        pairs = moved.data();
+    }
+    if (mem == VB_MEM_DEVICE && !p->det_position.empty() && n_pairs > 0) {
+        if (!p->det_position_dev.ptr &&
+            (st = upload(ctx, p->det_position_dev, p->det_position.data(), sizeof(long long) * p->n_det)) != VB_OK)
+            return st;
+        if ((st = dp.allocate(ctx, sizeof(int64_t) * 2 * n_pairs)) != VB_OK) return st;
+        translate_pairs_kernel<<<(unsigned)std::min<long long>(4096, (2 * n_pairs + 255) / 256), 256, 0, s>>>(
+            2 * n_pairs, reinterpret_cast<const long long*>(pairs), p->det_position_dev.as<long long>(), p->n_det,
+            dp.as<long long>());
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return cuda_error(ctx, err, "vb_hs_plan_determinant_pairs");
+        pp = dp.as<long long>();
+    }
     if (mem == VB_MEM_HOST) {
         if ((st = upload(ctx, dp, pairs, sizeof(int64_t) * 2 * std::max<int64_t>(1, n_pairs))) != VB_OK) return st;
         if ((st = dh_o.allocate(ctx, sizeof(double) * std::max<int64_t>(1, n_pairs))) != VB_OK) return st;

@@ -66,6 +66,13 @@ cudaError_t reserve_kernel_stack();
 // leading minor of that order is not positive definite.  Synchronizes the context stream.
 vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double* Ui_out, int* info);
 
+// Blocked Cholesky on the FP64 tensor cores (cholesky_blocked.cu): U (and U^-1 when Ui is not
+// null) of the device matrix M, upper triangle read, lower triangles written as zeros; `work`
+// holds blocked_cholesky_workspace(n, Ui != nullptr) bytes; *info = order of the first failing
+// pivot (0 on success).  Synchronizes the stream.
+size_t blocked_cholesky_workspace(int n, bool inverse);
+cudaError_t blocked_cholesky(const double* M, int n, double* U, double* Ui, void* work, int* info, cudaStream_t s);
+
 // Lets `kernel` launch with up to `bytes` of dynamic shared memory on the current device.  The
 // limit is a process-wide function attribute, so it is raised once per kernel and device to the
 // opt-in maximum (never lowered) under a lock: threads launching the same kernel with different

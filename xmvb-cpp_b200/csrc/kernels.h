@@ -85,6 +85,8 @@ struct BandReduceArgs {
     const unsigned char* seg_meta;
     const double* term_c;
     const unsigned char* term_d;
+    const int* seg_tiles;     // row tiles whose segment has terms, per group ascending
+    const int* seg_tile_off;  // group g: seg_tiles[seg_tile_off[g] .. seg_tile_off[g + 1])
     double* Zh;  // n_str x n_det column-major: Z[e * n_str + I]
     double* Zs;
     int* error;  // set to 1 when a tile wait gives up (the results are then incomplete)

@@ -945,6 +945,39 @@ using namespace vbcore;
 
 namespace {
 
+// Cholesky factor of a matrix above the one-CTA size: blocked panels, no grid barrier.
+vb_status run_blocked_cholesky(vb_context* ctx, const double* S, int n, bool host, double* U_out, int* info,
+                               const char* name) {
+    cudaStream_t s = ctx->stream;
+    const size_t m2 = sizeof(double) * (size_t)n * n;
+    DeviceBuffer ws;
+    vb_status st = ws.allocate(ctx, (host ? 2 * m2 : 0) + blocked_cholesky_workspace(n, false));
+    if (st != VB_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ws.ptr);
+    const double* dS = S;
+    double* dU = U_out;
+    cudaError_t err = cudaSuccess;
+    if (host) {
+        err = cudaMemcpyAsync(base, S, m2, cudaMemcpyHostToDevice, s);
+        dS = reinterpret_cast<const double*>(base);
+        dU = reinterpret_cast<double*>(base + m2);
+    }
+    int bad = 0;
+    if (err == cudaSuccess) err = blocked_cholesky(dS, n, dU, nullptr, base + (host ? 2 * m2 : 0), &bad, s);
+    if (err == cudaSuccess && host && !bad) {
+        err = cudaMemcpyAsync(U_out, dU, m2, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    }
+    if (err != cudaSuccess) return cuda_error(ctx, err, name);
+    if (bad) {
+        if (info) *info = bad;
+        return set_error(ctx, VB_ERR_NUMERIC,
+                         std::string(name) + ": matrix is not positive definite (leading minor " +
+                             std::to_string(bad) + ")");
+    }
+    return VB_OK;
+}
+
 vb_status run_single(vb_context* ctx, int mode, const double* H, const double* S, int n, int mem, double* evals,
                      double* evecs, double* U_out, int* info, const char* name) {
     if (!ctx) return VB_ERR_INVALID;
@@ -955,6 +988,7 @@ vb_status run_single(vb_context* ctx, int mode, const double* H, const double* S
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     const bool host = mem == VB_MEM_HOST;
+    if (mode == 0 && n > kSmallProblem) return run_blocked_cholesky(ctx, S, n, host, U_out, info, name);
     const Layout L = layout_for(n, mode, host, host);
     DeviceBuffer ws;
     vb_status st = ws.allocate(ctx, L.total);
@@ -1022,6 +1056,18 @@ namespace vbcore {
 vb_status factor_inverse_device(vb_context* ctx, const double* M, int n, double* Ui_out, int* info) {
     *info = 0;
     cudaStream_t s = ctx->stream;
+    if (n > kSmallProblem) {
+        // stream-ordered panels and tensor-core products, no grid barrier
+        DeviceBuffer ws;
+        const size_t u_bytes = sizeof(double) * (size_t)n * n;
+        vb_status st = ws.allocate(ctx, u_bytes + blocked_cholesky_workspace(n, true));
+        if (st != VB_OK) return st;
+        unsigned char* base = static_cast<unsigned char*>(ws.ptr);
+        const cudaError_t err =
+            blocked_cholesky(M, n, reinterpret_cast<double*>(base), Ui_out, base + u_bytes, info, s);
+        if (err != cudaSuccess) return cuda_error(ctx, err, "factor_inverse_device");
+        return VB_OK;
+    }
     const Layout L = layout_for(n, 2, false, false);
     DeviceBuffer ws;
     vb_status st = ws.allocate(ctx, L.total);

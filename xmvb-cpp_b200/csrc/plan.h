@@ -15,6 +15,8 @@ using namespace vbcore;
 struct BandSegments {
     int n_groups = 0, n_tiles = 0, seg_max = 0;
     DeviceBuffer off, meta, coef, row;
+    // row tiles with terms, per group ascending (CSR: tile_off[g] .. tile_off[g + 1] index tiles)
+    DeviceBuffer tiles, tile_off;
 };
 
 struct vb_hs_plan {
@@ -56,6 +58,10 @@ struct vb_hs_plan {
     // determinants by alpha string (CSR: alpha_off[i] .. alpha_off[i + 1] index alpha_dets)
     DeviceBuffer alpha_off, alpha_dets;
     bool has_flip = false;
+    // internal position of each determinant of the caller's list when the plan reorders them
+    // (empty: the caller's order), host copy and device copy
+    std::vector<long long> det_position;
+    DeviceBuffer det_position_dev;
     long long det_pair_evaluations = 0;  // unordered determinant pairs evaluated (orbit representatives)
     vb_hs_stats stats{};
     bool evaluated = false;
