@@ -159,21 +159,39 @@ __global__ void bc_init_kernel(const double* __restrict__ M, double* __restrict_
 }
 
 // Panel j0: Cholesky of the (updated) diagonal block, rows beyond the matrix padded with the
-// identity.  Thread (g, c) keeps rows 16 g .. 16 g + 15 of column c in registers; pivot k is
-// published through a double-buffered row in shared memory (one barrier per pivot), eliminated
-// without scaling (row k keeps p_k u_k^T), and row r is divided by sqrt(p_r) at the end.  The
-// inverse of the triangular block follows the same way, pivots from the last up (X = I;
-// X[k, :] /= u_kk; X[r, :] -= u_rk X[k, :] for r < k).  Writes U_JJ into U, its inverse into Ub
-// (64 x 64, column-major) and, when Ui is given, onto Ui's diagonal block.
+// identity.  Thread (g, c) keeps rows 16 g .. 16 g + 15 of column c in registers.  Pivot k is
+// published through a double-buffered row in shared memory (one barrier per pivot): entries
+// a[k][c] for c > k (zeros elsewhere), 1 / p_k and p_k, so the update a[r][c] -= a[k][r] a[k][c] / p_k
+// needs no row or column test (rows r <= k and columns c <= k see zeros; the lower triangle takes
+// values that are never read and is cleared at the end).  Row r is divided by sqrt(p_r) at the
+// end.  The inverse of the triangular block follows the same way, pivots from the last up
+// (X = I; X[k, :] /= u_kk; X[r, :] -= u_rk X[k, :] for r < k), with u held transposed in shared
+// memory so that a thread's 16 entries of column k are 8 vector loads.  Writes U_JJ into U, its
+// inverse into Ub (64 x 64, column-major) and, when Ui is given, onto Ui's diagonal block.
 constexpr int kPanelRows = kNB / (kThreadsB / kNB);  // rows per thread (16)
-constexpr size_t kPanelSmem = sizeof(double) * (kNB * (kNB + 1) + 3 * kNB);
+constexpr int kUtStride = kNB + 2;                   // even: rows of the transposed factor stay 16-byte aligned
+constexpr int kPrStride = kNB + 2;                   // published row: kNB entries, 1 / p, p
+constexpr size_t kPanelSmem = sizeof(double) * (kNB * kUtStride + 2 * kPrStride + kNB);
+
+// v[kk] by a tree of selects on the bits of kk (depth 4, no dynamic register index)
+__device__ __forceinline__ double pick(const double (&v)[kPanelRows], int kk) {
+    static_assert(kPanelRows == 16, "four select levels");
+    double l1[8], l2[4], l3[2];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) l1[i] = (kk & 1) ? v[2 * i + 1] : v[2 * i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) l2[i] = (kk & 2) ? l1[2 * i + 1] : l1[2 * i];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) l3[i] = (kk & 4) ? l2[2 * i + 1] : l2[2 * i];
+    return (kk & 8) ? l3[1] : l3[0];
+}
 
 __global__ void __launch_bounds__(kThreadsB) bc_panel_kernel(double* __restrict__ U, double* __restrict__ Ub,
                                                              double* __restrict__ Ui, int n, int j0, int* status) {
-    extern __shared__ double psm[];
-    double(*a)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(psm);  // the factor, for the inverse
-    double* prow = psm + kNB * (kNB + 1);                              // 2 x kNB published rows
-    double* piv = prow + 2 * kNB;                                      // pivots p_k
+    extern __shared__ __align__(16) double psm[];
+    double* ut = psm;                          // ut[c * kUtStride + r] = u[r][c]
+    double* prow = psm + kNB * kUtStride;      // 2 x kPrStride
+    double* piv = prow + 2 * kPrStride;        // pivots p_k
     if (failed(status)) return;
     const int t = threadIdx.x, c = t & (kNB - 1), g = t / kNB;
     const int jb = min(kNB, n - j0);
@@ -189,22 +207,33 @@ __global__ void __launch_bounds__(kThreadsB) bc_panel_kernel(double* __restrict_
         }
         v[i] = x;
     }
-#pragma unroll
+    // the pivot loops stay rolled (a short body that stays in the instruction cache); a thread's
+    // row k % kPanelRows is picked from its registers by selects, not by a dynamic index
+#pragma unroll 1
     for (int k = 0; k < kNB; ++k) {
-        double* pr = prow + (k & 1) * kNB;
-        if (g == k / kPanelRows) pr[c] = v[k % kPanelRows];
+        double* pr = prow + (k & 1) * kPrStride;
+        if (g == k / kPanelRows) {
+            const double x = pick(v, k % kPanelRows);  // a[k][c]
+            pr[c] = c > k ? x : 0.0;
+            if (c == k) {
+                pr[kNB] = 1.0 / x;
+                pr[kNB + 1] = x;
+            }
+        }
         __syncthreads();
-        const double p = pr[k];
+        const double p = pr[kNB + 1];
         if (k < jb && (!(p > 0.0) || !isfinite(p))) {  // the same decision in every thread
             if (t == 0) atomicCAS(status, 0, j0 + k + 1);
             return;
         }
         if (t == 0) piv[k] = p;
-        const double f = pr[c] * (1.0 / p);
+        const double f = pr[c] * pr[kNB];
+        const double2* q2 = reinterpret_cast<const double2*>(pr + kPanelRows * g);
 #pragma unroll
-        for (int i = 0; i < kPanelRows; ++i) {
-            const int r = kPanelRows * g + i;
-            if (r > k && r <= c) v[i] = fma(-pr[r], f, v[i]);
+        for (int i = 0; i < kPanelRows / 2; ++i) {
+            const double2 q = q2[i];
+            v[2 * i] = fma(-q.x, f, v[2 * i]);
+            v[2 * i + 1] = fma(-q.y, f, v[2 * i + 1]);
         }
     }
     __syncthreads();
@@ -213,25 +242,36 @@ __global__ void __launch_bounds__(kThreadsB) bc_panel_kernel(double* __restrict_
         const int r = kPanelRows * g + i;
         const double d = sqrt(piv[r]);
         v[i] = r < c ? v[i] / d : (r == c ? d : 0.0);
-        a[r][c] = v[i];
+        ut[c * kUtStride + r] = v[i];
         if (r <= c && c < jb) U[(j0 + r) + (long long)(j0 + c) * n] = v[i];
     }
     __syncthreads();
+    if (t < kNB) piv[t] = 1.0 / ut[t * kUtStride + t];  // 1 / u_kk, off the pivot chain
+    __syncthreads();
 #pragma unroll
     for (int i = 0; i < kPanelRows; ++i) v[i] = (kPanelRows * g + i == c) ? 1.0 : 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int k = kNB - 1; k >= 0; --k) {
-        double* pr = prow + (k & 1) * kNB;
-        if (g == k / kPanelRows) {
-            v[k % kPanelRows] /= a[k][k];
-            pr[c] = v[k % kPanelRows];
+        double* pr = prow + (k & 1) * kPrStride;
+        const bool owner = g == k / kPanelRows;
+        const int kk = k % kPanelRows;
+        double own = 0.0;
+        if (owner) {
+            own = pick(v, kk) * piv[k];
+            pr[c] = own;
         }
         __syncthreads();
         const double xk = pr[c];
+        const double2* u2 = reinterpret_cast<const double2*>(ut + k * kUtStride + kPanelRows * g);  // u[r][k]
 #pragma unroll
-        for (int i = 0; i < kPanelRows; ++i) {
-            const int r = kPanelRows * g + i;
-            if (r < k) v[i] = fma(-a[r][k], xk, v[i]);
+        for (int i = 0; i < kPanelRows / 2; ++i) {
+            const double2 q = u2[i];
+            v[2 * i] = fma(-q.x, xk, v[2 * i]);
+            v[2 * i + 1] = fma(-q.y, xk, v[2 * i + 1]);
+        }
+        if (owner) {
+#pragma unroll
+            for (int i = 0; i < kPanelRows; ++i) v[i] = i == kk ? own : v[i];
         }
     }
 #pragma unroll

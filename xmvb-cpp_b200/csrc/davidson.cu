@@ -30,7 +30,7 @@ namespace {
 constexpr int kMaxSubspace = 48;
 constexpr int kKeep = 12;  // Ritz vectors kept at a restart
 constexpr int kDiagonalPhase = 24;  // iterations with the diagonal preconditioner
-constexpr int kSplits = 16;
+constexpr int kSplits = 64;  // column ranges of the matrix-vector partial sums (parallelism for the HBM stream)
 
 // y_h = H x, y_s = S x (column-major n x n), partial sums over kSplits column ranges.
 __global__ void __launch_bounds__(256) gemv2_partial_kernel(const double* __restrict__ H, const double* __restrict__ S,
@@ -64,21 +64,27 @@ __global__ void gemv2_reduce_kernel(int n, const double* __restrict__ part_h, co
     ys[i] = as;
 }
 
-// out[c] = sum_i A[i + c n] * y[i] for c < k (one CTA per column, fixed reduction order).
+// out[b] = sum_i A[i + c n] * y[i] with c = b for blocks b < k and, when y2 is given, c = b - k and
+// y2 in place of y for blocks k .. 2k - 1; y == nullptr: column c with itself.  One CTA per dot,
+// fixed reduction order.
 __global__ void __launch_bounds__(256) multi_dot_kernel(const double* __restrict__ A, int n, int k,
-                                                        const double* __restrict__ y, double* __restrict__ out) {
+                                                        const double* __restrict__ y, const double* __restrict__ y2,
+                                                        double* __restrict__ out) {
     __shared__ double red[256];
-    const int c = blockIdx.x;
-    if (c >= k) return;
+    const int b = blockIdx.x;
+    const int c = b < k ? b : b - k;
+    const double* a = A + (long long)c * n;
+    const double* v = b < k ? y : y2;
+    if (!v) v = a;
     double acc = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) acc = fma(A[i + (long long)c * n], y[i], acc);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc = fma(a[i], v[i], acc);
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
         if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[c] = red[0];
+    if (threadIdx.x == 0) out[b] = red[0];
 }
 
 // y[i] = sum_c A[i + c n] coef[c] (+ beta * y[i])
@@ -111,20 +117,21 @@ __global__ void diag_kernel(int n, const double* __restrict__ H, const double* _
     sd[i] = S[i + (long long)i * n];
 }
 
-// y = A^T x (one warp per column of A, coalesced down the column)
+// y = A^T x for upper-triangular A (one warp per column, coalesced down the column's rows <= col)
 __global__ void __launch_bounds__(256) gemv_t_kernel(const double* __restrict__ A, int n, const double* __restrict__ x,
                                                      double* __restrict__ y) {
     const int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (col >= n) return;
     const double* a = A + (long long)col * n;
     double acc = 0.0;
-    for (int i = lane; i < n; i += 32) acc = fma(__ldg(a + i), __ldg(x + i), acc);
+    for (int i = lane; i <= col; i += 32) acc = fma(__ldg(a + i), __ldg(x + i), acc);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) y[col] = acc;
 }
 
-// y = A x, column-split partial sums (same scheme as gemv2)
+// y = A x for upper-triangular A, column-split partial sums (same scheme as gemv2; row i reads
+// only its columns j >= i)
 __global__ void __launch_bounds__(256) gemv_partial_kernel(const double* __restrict__ A, int n,
                                                            const double* __restrict__ x, double* __restrict__ part) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -133,7 +140,7 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double* __restr
     const int j0 = split * chunk, j1 = min(n, j0 + chunk);
     if (i >= n) return;
     double acc = 0.0;
-    for (int j = j0; j < j1; ++j) acc = fma(__ldg(A + i + (long long)j * n), __ldg(x + j), acc);
+    for (int j = max(j0, i); j < j1; ++j) acc = fma(__ldg(A + i + (long long)j * n), __ldg(x + j), acc);
     part[(long long)split * n + i] = acc;
 }
 
@@ -265,7 +272,7 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
     const int kmax = std::min(kMaxSubspace, n);
     // workspace: [H S (host mode)] V HV SV (n x kmax) parts (2 x splits x n) vectors (8 n) coef
     const size_t ws_doubles = (host ? 2 * (size_t)n * n : 0) + 3 * (size_t)n * kmax + 2 * (size_t)kSplits * n +
-                              8 * (size_t)n + 2 * kMaxSubspace + 3 * (size_t)kKeep * n;
+                              8 * (size_t)n + 3 * kMaxSubspace + 3 * (size_t)kKeep * n;
     DeviceBuffer ws;
     vb_status st = ws.allocate(ctx, sizeof(double) * ws_doubles);
     if (st != VB_OK) return st;
@@ -295,7 +302,7 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
     double* st_vec = t + n;
     double* coef = st_vec + n;
     double* dots = coef + kMaxSubspace;
-    double* restart = dots + kMaxSubspace;  // 3 kKeep columns
+    double* restart = dots + 2 * kMaxSubspace;  // 3 kKeep columns (dots: up to 2 kMaxSubspace)
     const int tb = 256, nb = (n + tb - 1) / tb;
     auto check = [&](const char* what) -> vb_status {
         if (err == cudaSuccess) err = cudaGetLastError();
@@ -306,10 +313,14 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
         gemv2_partial_kernel<<<dim3(nb, kSplits), tb, 0, s>>>(dH, dS, n, in, ph, ps);
         gemv2_reduce_kernel<<<nb, tb, 0, s>>>(n, ph, ps, yh, ys);
     };
-    auto dots_of = [&](const double* A, int k, const double* y, std::vector<double>* out) {
-        multi_dot_kernel<<<k, 256, 0, s>>>(A, n, k, y, dots);
-        out->resize(k);
-        err = cudaMemcpyAsync(out->data(), dots, sizeof(double) * k, cudaMemcpyDeviceToHost, s);
+    // dots of the k columns of A with y (and, when y2 is given, then with y2; y == nullptr: each
+    // column with itself), read back in one synchronization
+    auto dots_of = [&](const double* A, int k, const double* y, std::vector<double>* out,
+                       const double* y2 = nullptr) {
+        const int m = y2 ? 2 * k : k;
+        multi_dot_kernel<<<m, 256, 0, s>>>(A, n, k, y, y2, dots);
+        out->resize(m);
+        err = cudaMemcpyAsync(out->data(), dots, sizeof(double) * m, cudaMemcpyDeviceToHost, s);
         if (err == cudaSuccess) err = cudaStreamSynchronize(s);
     };
     diag_kernel<<<nb, tb, 0, s>>>(n, dH, dS, hd, sd);
@@ -336,14 +347,12 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
     // here unless the caller already stored them in HV and SV)
     auto add_column = [&](int c, bool have_images) -> vb_status {
         if (!have_images) gemv2(V + (size_t)c * n, HV + (size_t)c * n, SV + (size_t)c * n);
-        std::vector<double> hcol, scol;
-        dots_of(V, c + 1, HV + (size_t)c * n, &hcol);
-        if ((st = check("vb_lowest_root")) != VB_OK) return st;
-        dots_of(V, c + 1, SV + (size_t)c * n, &scol);
+        std::vector<double> cols;
+        dots_of(V, c + 1, HV + (size_t)c * n, &cols, SV + (size_t)c * n);
         if ((st = check("vb_lowest_root")) != VB_OK) return st;
         for (int i = 0; i <= c; ++i) {
-            Hs[i + c * kmax] = Hs[c + i * kmax] = hcol[i];
-            Ss[i + c * kmax] = Ss[c + i * kmax] = scol[i];
+            Hs[i + c * kmax] = Hs[c + i * kmax] = cols[i];
+            Ss[i + c * kmax] = Ss[c + i * kmax] = cols[c + 1 + i];
         }
         return VB_OK;
     };
@@ -368,12 +377,12 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
         combine_kernel<<<nb, tb, 0, s>>>(HV, n, k, coef, 0.0, hx);
         combine_kernel<<<nb, tb, 0, s>>>(SV, n, k, coef, 0.0, sx);
         residual_kernel<<<nb, tb, 0, s>>>(n, hx, sx, theta, hd, sd, r, t);
-        std::vector<double> rr, hh, ss;
-        dots_of(r, 1, r, &rr);
-        dots_of(hx, 1, hx, &hh);
-        dots_of(sx, 1, sx, &ss);
+        // |H x|^2, |S x|^2, |r|^2 (hx, sx and r are consecutive vectors)
+        std::vector<double> norms;
+        dots_of(hx, 3, nullptr, &norms);
         if ((st = check("vb_lowest_root")) != VB_OK) return st;
-        if (std::sqrt(rr[0]) <= tolerance * (std::sqrt(hh[0]) + std::fabs(theta) * std::sqrt(ss[0]))) {
+        std::vector<double> rr{norms[2]};
+        if (std::sqrt(rr[0]) <= tolerance * (std::sqrt(norms[0]) + std::fabs(theta) * std::sqrt(norms[1]))) {
             converged = true;
             break;
         }
