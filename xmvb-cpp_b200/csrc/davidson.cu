@@ -87,11 +87,14 @@ __global__ void __launch_bounds__(256) multi_dot_kernel(const double* __restrict
     if (threadIdx.x == 0) out[b] = red[0];
 }
 
-// y[i] = sum_c A[i + c n] coef[c] (+ beta * y[i])
+// y[i] = sum_c A[i + c n] coef[c] (+ beta * y[i]); grid row b (blockIdx.y) applies the same
+// coefficients to A + b a_step into y + b y_step (the basis and its two images in one launch)
 __global__ void combine_kernel(const double* __restrict__ A, int n, int k, const double* __restrict__ coef,
-                               double beta, double* __restrict__ y) {
+                               double beta, double* __restrict__ y, long long a_step = 0, long long y_step = 0) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    A += blockIdx.y * a_step;
+    y += blockIdx.y * y_step;
     double acc = beta == 0.0 ? 0.0 : beta * y[i];
     for (int c = 0; c < k; ++c) acc = fma(A[i + (long long)c * n], coef[c], acc);
     y[i] = acc;
@@ -373,9 +376,8 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
         y.assign(Y.begin(), Y.begin() + k);
         scale = std::max(1.0, std::fabs(theta));
         err = cudaMemcpyAsync(coef, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s);
-        combine_kernel<<<nb, tb, 0, s>>>(V, n, k, coef, 0.0, x);
-        combine_kernel<<<nb, tb, 0, s>>>(HV, n, k, coef, 0.0, hx);
-        combine_kernel<<<nb, tb, 0, s>>>(SV, n, k, coef, 0.0, sx);
+        // x, hx, sx (consecutive vectors) from V, HV, SV (consecutive n x kmax blocks)
+        combine_kernel<<<dim3(nb, 3), tb, 0, s>>>(V, n, k, coef, 0.0, x, (long long)n * kmax, n);
         residual_kernel<<<nb, tb, 0, s>>>(n, hx, sx, theta, hd, sd, r, t);
         // |H x|^2, |S x|^2, |r|^2 (hx, sx and r are consecutive vectors)
         std::vector<double> norms;
@@ -417,9 +419,8 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
             std::vector<double> nv((size_t)n * keep), nh((size_t)n * keep), ns((size_t)n * keep);
             for (int j = 0; j < keep; ++j) {
                 err = cudaMemcpyAsync(coef, Y.data() + (size_t)j * k, sizeof(double) * k, cudaMemcpyHostToDevice, s);
-                combine_kernel<<<nb, tb, 0, s>>>(V, n, k, coef, 0.0, restart + (size_t)j * n);
-                combine_kernel<<<nb, tb, 0, s>>>(HV, n, k, coef, 0.0, restart + (size_t)(keep + j) * n);
-                combine_kernel<<<nb, tb, 0, s>>>(SV, n, k, coef, 0.0, restart + (size_t)(2 * keep + j) * n);
+                combine_kernel<<<dim3(nb, 3), tb, 0, s>>>(V, n, k, coef, 0.0, restart + (size_t)j * n,
+                                                          (long long)n * kmax, (long long)keep * n);
                 err = cudaStreamSynchronize(s);  // coef is reused by the next column
             }
             err = cudaMemcpyAsync(V, restart, v1 * keep, cudaMemcpyDeviceToDevice, s);
