@@ -44,7 +44,7 @@ def test_cholesky_reads_upper_triangle_only(ctx):
     assert np.abs(vbcore.metric_cholesky(ctx, Sl) - O.metric_cholesky(S)).max() < 1e-12
 
 
-@pytest.mark.parametrize("n,bad", [(10, 4), (70, 40), (150, 1)])
+@pytest.mark.parametrize("n,bad", [(10, 4), (70, 40), (150, 1), (300, 200)])
 def test_cholesky_reports_the_failing_minor(ctx, n, bad):
     S = O.conditioned_metric(n, 1e2, seed=n)
     S[bad - 1, bad - 1] = -1.0  # leading minor of order `bad` is the first that is not positive

@@ -107,6 +107,32 @@ def test_determinant_pairs_match_oracle(ctx):
     assert np.abs(so - Sd[pairs[:, 0], pairs[:, 1]]).max() < REL * max(1.0, np.abs(Sd).max())
 
 
+def test_determinant_pairs_in_device_memory_use_the_callers_order(ctx):
+    # this covalent + ionic list is reordered inside the plan (determinants grouped by the first
+    # structure group using them); pair indices in device memory are mapped like host ones
+    import ctypes
+    import torch
+    n = 8
+    S, h, eri = workloads.active_space(n, 24, 7)
+    plan, ex = _plan(ctx, "COV ION(1)", n, n)
+    rng = np.random.default_rng(1)
+    pairs = rng.integers(0, ex.n_determinants, size=(3000, 2)).astype(np.int64)
+    ho, so = plan.determinant_pairs(S, h, eri, pairs)
+    dev = torch.device("cuda", 0)
+    dS = torch.tensor(np.ascontiguousarray(S.T), device=dev)
+    dh = torch.tensor(np.ascontiguousarray(h.T), device=dev)
+    de = torch.tensor(np.ascontiguousarray(eri, dtype=np.float64), device=dev)
+    dp = torch.tensor(pairs, device=dev)
+    dho = torch.zeros(len(pairs), dtype=torch.float64, device=dev)
+    dso = torch.zeros(len(pairs), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    st = vbcore.load_library().vb_hs_plan_determinant_pairs(plan._h, p(dS), p(dh), p(de), len(pairs), p(dp),
+                                                            vbcore.VB_MEM_DEVICE, p(dho), p(dso))
+    assert st == 0
+    assert np.array_equal(dho.cpu().numpy(), ho) and np.array_equal(dso.cpu().numpy(), so)
+
+
 @pytest.mark.parametrize("k", [1, 2, 3, 4, 6, 7, 9])
 def test_resolve_overlaps_reference_semantics(ctx, k):
     rng = np.random.default_rng(k)

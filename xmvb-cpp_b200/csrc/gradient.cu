@@ -195,14 +195,26 @@ __global__ void __launch_bounds__(256) det_pair_adjoint_two_stage_kernel(AdjArgs
     const int Nb = a.f.Nb;
     const int i0 = __ldg(aoff + i), i1 = __ldg(aoff + i + 1);
     if (i0 == i1) return;
+    // the determinants of alpha string i (weights, beta strings) in shared memory when they fit, so
+    // that the record gathers of consecutive determinants do not wait on index loads
+    constexpr int kStaged = 512;
+    __shared__ double s_w[kStaged];
+    __shared__ int s_b[kStaged];
+    const bool staged = i1 - i0 <= kStaged;
+    if (staged)
+        for (int q = threadIdx.x; q < i1 - i0; q += blockDim.x) {
+            s_w[q] = __ldg(ws + i0 + q);
+            s_b[q] = __ldg(bs + i0 + q);
+        }
+    __syncthreads();
     for (int t = threadIdx.x; t < Nb * CC; t += blockDim.x) {
         const int b = t / CC, c = c0 + t % CC;
         double acc = 0.0;
         if (c < ncomp) {
             const double sign = c < r_pos ? 1.0 : -1.0;
-#pragma unroll 4
+#pragma unroll 8
             for (int k = i0; k < i1; ++k) {
-                const int bd = __ldg(bs + k);
+                const int bd = staged ? s_b[k - i0] : __ldg(bs + k);
                 const double* rb = a.f.rec_b + record_index(min(bd, b), max(bd, b), Nb) * a.f.stride_b;
                 double v;
                 if (c < R)
@@ -211,7 +223,7 @@ __global__ void __launch_bounds__(256) det_pair_adjoint_two_stage_kernel(AdjArgs
                     v = __ldg(rb + R + 1) - a.lambda * __ldg(rb + R);
                 else
                     v = __ldg(rb + R);
-                acc = fma(__ldg(ws + k), v, acc);
+                acc = fma(staged ? s_w[k - i0] : __ldg(ws + k), v, acc);
             }
         }
         sT[t] = acc;
