@@ -345,6 +345,7 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
     std::vector<double> y;
     double scale = 1.0;
     int it = 0;
+    std::vector<double> ritz;  // lowest Ritz value of every iteration
     bool converged = false;
     // projected matrices are kept with the basis; column c is new (its H v and S v are computed
     // here unless the caller already stored them in HV and SV)
@@ -373,6 +374,7 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
         if (!small_eigs(k, A, Bm, &thetas, &Y))
             return set_error(ctx, VB_ERR_NUMERIC, "vb_lowest_root: projected overlap is not positive definite");
         theta = thetas[0];
+        ritz.push_back(theta);
         y.assign(Y.begin(), Y.begin() + k);
         scale = std::max(1.0, std::fabs(theta));
         err = cudaMemcpyAsync(coef, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s);
@@ -391,7 +393,23 @@ extern "C" vb_status vb_lowest_root(vb_context* ctx, const double* H, const doub
         if (!Ui && it + 1 >= kDiagonalPhase) {
             // switch to the shift-invert preconditioner (H - sigma S)^-1 with sigma below the
             // lowest root: the factorization only holds (positive definite) there
+            // shift below the root: by default from the residual, which overstates the distance to
+            // the root by orders of magnitude on non-orthogonal structures (a shift far below it
+            // leaves a weak preconditioner); when the Ritz values of the last eight iterations
+            // decrease at a slowing rate, the root is estimated by Aitken's delta-squared
+            // extrapolation of theta_{it-8}, theta_{it-4}, theta_it and the shift is 1.5 times the
+            // estimated distance plus a tenth of the Ritz gap.  A shift that proves to lie above the
+            // root fails the factorization and is widened below.
             double delta = std::max(1.0e-2 * scale, 10.0 * std::sqrt(rr[0]));
+            const size_t nr = ritz.size();
+            if (nr > 8) {
+                const double d1 = ritz[nr - 5] - ritz[nr - 9], d2 = ritz[nr - 1] - ritz[nr - 5];
+                if (d1 < 0.0 && d2 < 0.0 && d2 > d1) {
+                    const double below = d2 * d2 / (d2 - d1);  // theta - estimated root
+                    const double gap = thetas.size() > 1 ? thetas[1] - thetas[0] : 0.0;
+                    delta = 1.5 * below + std::max(0.1 * gap, 1.0e-4 * scale);
+                }
+            }
             if ((st = mbuf.allocate(ctx, m2)) != VB_OK) return st;
             if ((st = uibuf.allocate(ctx, m2)) != VB_OK) return st;
             int info = 1;
