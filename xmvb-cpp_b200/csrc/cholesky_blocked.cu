@@ -303,8 +303,8 @@ __global__ void __launch_bounds__(kThreadsB) bc_panel_row_kernel(double* __restr
 }
 
 // A_22 -= U_12^T U_12 on the upper 64 x 64 tiles (ti <= tj) of the trailing matrix.
-__global__ void __launch_bounds__(kThreadsB) bc_trailing_kernel(double* __restrict__ U, int n, int j0,
-                                                                const int* status) {
+__global__ void __launch_bounds__(kThreadsB, 2) bc_trailing_kernel(double* __restrict__ U, int n, int j0,
+                                                                   const int* status) {
     extern __shared__ double smem[];
     if (failed(status)) return;
     const int jb = min(kNB, n - j0), j1 = j0 + jb;
@@ -315,6 +315,17 @@ __global__ void __launch_bounds__(kThreadsB) bc_trailing_kernel(double* __restri
     const int ti = (int)(b - (long long)tj * (tj + 1) / 2);
     const int r0 = j1 + kNB * ti, c0 = j1 + kNB * tj;
     const Opnd P{U + j0, n, n, jb};
+    // the tile's current entries are loaded first, so that their latency overlaps the product
+    double cur[2][4][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = r0 + out_row(i), c = c0 + out_col(j, h);
+                cur[i][j][h] = (r <= c && c < n) ? U[r + (long long)c * n] : 0.0;
+            }
     double acc[2][4][2] = {};
     tile_product<true, true>(P, P, r0, c0, 0, jb, smem, acc);
 #pragma unroll
@@ -324,7 +335,7 @@ __global__ void __launch_bounds__(kThreadsB) bc_trailing_kernel(double* __restri
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int r = r0 + out_row(i), c = c0 + out_col(j, h);
-                if (r <= c && c < n) U[r + (long long)c * n] -= acc[i][j][h];
+                if (r <= c && c < n) U[r + (long long)c * n] = cur[i][j][h] - acc[i][j][h];
             }
 }
 
