@@ -21,6 +21,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <vector>
 
 #include "internal.h"
 
@@ -303,12 +305,13 @@ __global__ void __launch_bounds__(kThreadsB) bc_panel_row_kernel(double* __restr
 }
 
 // A_22 -= U_12^T U_12 on the upper 64 x 64 tiles (ti <= tj) of the trailing matrix.
+// Tiles first .. first + gridDim.x - 1 of the upper-tile enumeration (t = tj (tj + 1) / 2 + ti).
 __global__ void __launch_bounds__(kThreadsB, 2) bc_trailing_kernel(double* __restrict__ U, int n, int j0,
-                                                                   const int* status) {
+                                                                   const int* status, int first) {
     extern __shared__ double smem[];
     if (failed(status)) return;
     const int jb = min(kNB, n - j0), j1 = j0 + jb;
-    const long long b = blockIdx.x;
+    const long long b = (long long)blockIdx.x + first;
     int tj = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
     while ((long long)tj * (tj + 1) / 2 > b) --tj;
     while ((long long)(tj + 1) * (tj + 2) / 2 <= b) ++tj;
@@ -390,6 +393,52 @@ size_t blocked_cholesky_workspace(int n, bool inverse) {
 // U (n x n, device, column-major; the lower triangle is written with zeros) and, when Ui is not
 // null, U^-1 (same layout) of the device matrix M; `work` holds blocked_cholesky_workspace(n, Ui)
 // bytes.  *info: order of the first failing pivot, 0 on success.  Synchronizes the stream.
+namespace {
+
+// High-priority auxiliary streams (with their two events) for the look-ahead panels, pooled per
+// device: a call takes one for its duration, so concurrent calls from several host threads never
+// share one.
+struct AuxStream {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t block_ready = nullptr, panel_done = nullptr;
+};
+std::mutex g_aux_mutex;
+std::vector<AuxStream> g_aux_free;
+
+cudaError_t acquire_aux(AuxStream* out) {
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) return err;
+    {
+        std::lock_guard<std::mutex> lock(g_aux_mutex);
+        for (size_t i = 0; i < g_aux_free.size(); ++i)
+            if (g_aux_free[i].device == device) {
+                *out = g_aux_free[i];
+                g_aux_free.erase(g_aux_free.begin() + (long)i);
+                return cudaSuccess;
+            }
+    }
+    AuxStream a;
+    a.device = device;
+    int least = 0, greatest = 0;
+    err = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (err == cudaSuccess) err = cudaStreamCreateWithPriority(&a.stream, cudaStreamNonBlocking, greatest);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&a.block_ready, cudaEventDisableTiming);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&a.panel_done, cudaEventDisableTiming);
+    if (err != cudaSuccess) return err;
+    // a fresh event counts as complete, so the first waits on it return at once
+    *out = a;
+    return cudaSuccess;
+}
+
+void release_aux(const AuxStream& a) {
+    std::lock_guard<std::mutex> lock(g_aux_mutex);
+    g_aux_free.push_back(a);
+}
+
+}  // namespace
+
 cudaError_t blocked_cholesky(const double* M, int n, double* U, double* Ui, void* work, int* info,
                              cudaStream_t s) {
     *info = 0;
@@ -407,17 +456,33 @@ cudaError_t blocked_cholesky(const double* M, int n, double* U, double* Ui, void
     if (err != cudaSuccess) return err;
     const long long total = (long long)n * n;
     bc_init_kernel<<<(unsigned)std::min<long long>(4096, (total + 255) / 256), 256, 0, s>>>(M, U, n);
+    // Look-ahead: after the panel row, the trailing update's first tile (the next panel's
+    // diagonal block) runs alone, then the next panel's factorization goes to a high-priority
+    // auxiliary stream while the other tiles run on s, so that the one-CTA panel takes an SM as
+    // soon as a trailing CTA retires; the next panel row waits for it.
+    AuxStream aux;
+    if ((err = acquire_aux(&aux)) != cudaSuccess) return err;
+    bc_panel_kernel<<<1, kThreadsB, kPanelSmem, s>>>(U, Ub, Ui, n, 0, status);
     for (int j0 = 0; j0 < n && err == cudaSuccess; j0 += kNB) {
         const int j1 = std::min(n, j0 + kNB);
-        bc_panel_kernel<<<1, kThreadsB, kPanelSmem, s>>>(U, Ub, Ui, n, j0, status);
-        if (j1 < n) {
-            const int m = n - j1, nt = (m + kNB - 1) / kNB;
-            bc_panel_row_kernel<<<nt, kThreadsB, kProductSmem, s>>>(U, Ub, n, j0, status);
-            bc_trailing_kernel<<<(unsigned)((long long)nt * (nt + 1) / 2), kThreadsB, kProductSmem, s>>>(U, n, j0,
-                                                                                                      status);
-        }
+        if (j1 >= n) break;
+        const int m = n - j1, nt = (m + kNB - 1) / kNB;
+        const long long tiles = (long long)nt * (nt + 1) / 2;
+        if (j0 > 0 && (err = cudaStreamWaitEvent(s, aux.panel_done, 0)) != cudaSuccess) break;
+        bc_panel_row_kernel<<<nt, kThreadsB, kProductSmem, s>>>(U, Ub, n, j0, status);
+        bc_trailing_kernel<<<1, kThreadsB, kProductSmem, s>>>(U, n, j0, status, 0);
+        if ((err = cudaEventRecord(aux.block_ready, s)) != cudaSuccess) break;
+        if ((err = cudaStreamWaitEvent(aux.stream, aux.block_ready, 0)) != cudaSuccess) break;
+        bc_panel_kernel<<<1, kThreadsB, kPanelSmem, aux.stream>>>(U, Ub, Ui, n, j1, status);
+        if ((err = cudaEventRecord(aux.panel_done, aux.stream)) != cudaSuccess) break;
+        if (tiles > 1)
+            bc_trailing_kernel<<<(unsigned)(tiles - 1), kThreadsB, kProductSmem, s>>>(U, n, j0, status, 1);
         err = cudaGetLastError();
     }
+    // join: the last panel on the auxiliary stream precedes the rest of s
+    const cudaError_t join = cudaStreamWaitEvent(s, aux.panel_done, 0);
+    if (err == cudaSuccess) err = join;
+    release_aux(aux);
     if (Ui) {
         for (int b = kNB; b < n && err == cudaSuccess; b *= 2) {
             const int pairs = (n + 2 * b - 1) / (2 * b);
