@@ -680,6 +680,30 @@ def run_ri(args):
         U = dU.view(nS, nS).T.cpu().numpy()
         chol.append({"cond": cond, "ms": statistics.median(ct),
                      "backward_error": float(np.linalg.norm(U.T @ U - Sm) / np.linalg.norm(Sm))})
+    # larger metrics (the Davidson preconditioner's sizes): blocked Cholesky, FP64 tensor cores
+    chol_large = []
+    for nL in (2048, 5676):
+        rngL = np.random.default_rng(nL)
+        AL = rngL.standard_normal((nL, nL))
+        SL = AL @ AL.T / nL + np.eye(nL)
+        dS = torch.tensor(SL, device=device)
+        dU = torch.empty(nL * nL, dtype=torch.float64, device=device)
+        info = ctypes.c_int(0)
+        ct = []
+        for rep in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lib.vb_metric_cholesky(ctx.handle, ctypes.c_void_p(dS.data_ptr()), nL, 1, ctypes.c_void_p(dU.data_ptr()),
+                                   ctypes.byref(info))
+            e1.record(stream)
+            e1.synchronize()
+            if rep:
+                ct.append(e0.elapsed_time(e1))
+        U = dU.view(nL, nL).T.cpu().numpy()
+        msL = statistics.median(ct)
+        chol_large.append({"n": nL, "ms": msL, "tflops": nL ** 3 / 3.0 / (msL * 1e-3) / 1e12,
+                           "backward_error": float(np.linalg.norm(U.T @ U - SL) / np.linalg.norm(SL))})
+        del dS, dU
     line = {
         "metric": "RI AO->active transform throughput (FP64)", "value": flops / (ms * 1e-3) / 1e9,
         "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -697,6 +721,7 @@ def run_ri(args):
         "errors_vs_fp64_oracle": {"max_abs": err_abs, "rel": err_rel, "rows_checked": int(len(rows))},
         "split_precision": split,
         "cholesky_429": chol,
+        "cholesky_large": chol_large,
         "cpu_baseline": {"value": flops * len(rows) / n_aux / dt_cpu / 1e9, "unit": "GFLOP/s",
                          "cores": os.cpu_count() or 1, "kind": "port",
                          "sample": f"oracle transform of {len(rows)} of {n_aux} auxiliary rows, {dt_cpu:.2f} s"},

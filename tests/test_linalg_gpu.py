@@ -25,7 +25,7 @@ def _random_symmetric(n, seed):
     return 0.5 * (a + a.T)
 
 
-@pytest.mark.parametrize("n", [1, 2, 5, 31, 32, 33, 64, 97, 200, 429])
+@pytest.mark.parametrize("n", [1, 2, 5, 31, 32, 33, 64, 97, 200, 429, 1000])
 @pytest.mark.parametrize("cond", [1e2, 1e6, 1e10])
 def test_cholesky_matches_lapack(ctx, n, cond):
     S = O.conditioned_metric(n, cond, seed=n)
