@@ -55,8 +55,9 @@ vb_status vb_context_destroy(vb_context* ctx);
  * stream order). */
 vb_status vb_context_set_stream(vb_context* ctx, void* cuda_stream);
 vb_status vb_context_synchronize(vb_context* ctx);
-/* Polls a grid-barrier wait of the cooperative eigensolver kernels (vb_metric_cholesky,
- * vb_generalized_eigh, the Davidson shift-invert factor) makes before it gives up: the kernel
+/* Polls a grid-barrier wait of the cooperative eigensolver kernels (vb_generalized_eigh, and
+ * vb_metric_cholesky up to n = 96; the blocked Cholesky used above that size and for the Davidson
+ * shift-invert factor has no grid barrier) makes before it gives up: the kernel
  * then ends and the call returns VB_ERR_TIMEOUT, with the context still usable.  0 restores the
  * built-in default (2^26 polls, seconds).  No reference counterpart: the reference's solvers are
  * library calls (dsygvd) without a device-side wait. */
