@@ -9,6 +9,9 @@
 //      inverse of the resulting triangular block;
 //   2. bc_panel_row_kernel: U_12 = U_11^-T A_12;
 //   3. bc_trailing_kernel: A_22 -= U_12^T U_12 over the upper 64 x 64 tiles.
+// Look-ahead: the trailing update's first tile (the next panel's diagonal block) runs first, then
+// the next panel's factorization on a high-priority auxiliary stream while the remaining tiles run
+// on the caller's stream.
 // Inverse U^-1 (optional): the panel kernels leave U_JJ^-1 on the diagonal blocks; then for block
 // sizes b = 64, 128, ... consecutive diagonal blocks are paired,
 //   [[A, B], [0, C]]^-1 = [[A^-1, -A^-1 B C^-1], [0, C^-1]],
